@@ -1,0 +1,284 @@
+"""Benchmark of the B200 JW step (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): N = 1024 rows,
+65 536 complex right-hand sides in strided XXII layout, a 5-band matvec fused
+ahead of the tridiagonal solve (PfSolve jw_type 13, upperBanded 2) and the
+XXII -> packed conversion (block 7) fused behind it: one kernel per step.
+Synthetic seeded inputs with the named shapes and distributions; inputs are
+2 GiB (larger than the 126 MB L2), so no L2 flush is needed between steps.
+
+value  : complex RHS/s over the whole job (all ranks), inputs resident in HBM.
+e2e    : same metric through the C ABI with host buffers: pinned H2D of the
+         step's input, the fused kernel, D2H of the step's output.
+roofline: algorithmic bytes (read XXII + write packed: 2*N*16 B per complex RHS,
+         plus bands once) / kernel time, against MEASURED_PEAKS.json hbm_gbs.
+--impl reference: the reference's CPU verification algorithm (sequential
+         band matvec + Thomas per RHS, restated in C) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M_ROWS = 1024
+N_CPLX = 65536
+METRIC = "JW-step RHS/s (N=1024, 65536 complex RHS, 5-band matvec + tridiagonal solve, XXII->packed), FP64"
+UNIT = "complex RHS/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(target_s=12.0, threads=None):
+    """Time the reference's CPU verification path (port) on a bounded sample of
+    the workload; returns (complex RHS/s, cores, sample description)."""
+    from oracle import oracle as O
+    from pfsolve_b200 import workloads as WL
+    threads = threads or os.cpu_count() or 1
+    probe = 64
+    wl = WL.config2(B=probe)
+    M = wl.M
+
+    def run(ncplx, rhs):
+        c1 = O.Case(M=M, batch=2 * ncplx, LDA=5, KU=2, KL=2, jw_type=0)
+        y = O.dgbmv(c1, wl.dgbmv, rhs, mode="d", nthreads=threads)
+        c2 = O.Case(M=M, batch=2 * ncplx, upperBanded=2, jw_type=13)
+        O.jw_step(c2, wl.jw_bands, y, mode="d", nthreads=threads)
+
+    t0 = time.perf_counter()
+    run(probe, wl.rhs)
+    t = time.perf_counter() - t0
+    n = int(min(N_CPLX, max(probe, probe * target_s / max(t, 1e-6))))
+    rng = np.random.default_rng(1)
+    rhs = rng.standard_normal(2 * M * n)
+    t0 = time.perf_counter()
+    run(n, rhs)
+    t = time.perf_counter() - t0
+    return n / t, threads, f"{n} of {N_CPLX} complex RHS (N=1024), double, {threads} OpenMP threads, {t:.1f} s"
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    vals = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_reference_sample(target_s=2.0)
+    for _ in range(args.steps):
+        v, cores, desc = cpu_reference_sample(target_s=8.0)
+        vals.append(v)
+        info = (cores, desc)
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_CPLX / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, N(0,1) complex RHS, dominant tridiagonal, U(-1,1) 5-band)",
+            "config": {"workload": "config2: N=1024, 65536 complex RHS, XXII in -> packed out, dgbmv(5) + "
+                                   "tridiagonal JW step (jw_type 13)", "rhs_per_gpu": N_CPLX},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info[0], "kind": "port", "sample": info[1]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App, append_chain, launch_count
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = WL.config2(seed=1 + rank, B=N_CPLX)
+    M = wl.M
+    tA = torch.from_numpy(wl.dgbmv).to(dev)
+    tb = torch.from_numpy(wl.jw_bands).to(dev)
+    rhs = torch.from_numpy(wl.rhs).to(dev)  # XXII, 1 GiB
+    out = torch.empty(2 * M * N_CPLX, dtype=torch.float64, device=dev)
+    del wl
+    dg = App(device=local, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * N_CPLX), LDA=5, KU=2, KL=2,
+             doublePrecision=1)
+    jw = App(device=local, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * N_CPLX), upperBanded=2, jw_type=13,
+             doublePrecision=1)
+    bl = App(device=local, buffer=rhs, outputBuffer=out, M_size=M, size=(M, N_CPLX), block=7, doublePrecision=1)
+    lps = [dg.launch_params(), jw.launch_params(), bl.launch_params()]
+    apps = [dg, jw, bl]
+
+    def step():
+        append_chain(apps, lps)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    n0 = launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = launch_count() - n0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * N_CPLX / (ms_max * 1e-3)
+    bytes_alg = 2.0 * M * 16 * N_CPLX + (5 + 3) * M * 8
+    achieved = bytes_alg / (ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+
+    # ---- e2e through the C ABI with host buffers (pinned), copies inside the timed region
+    host_in = torch.empty(2 * M * N_CPLX, dtype=torch.float64, pin_memory=True)
+    host_in.copy_(rhs.cpu())
+    host_out = torch.empty(2 * M * N_CPLX, dtype=torch.float64, pin_memory=True)
+    e_steps = max(2, min(args.steps, 5))
+    for _ in range(2):
+        rhs.copy_(host_in, non_blocking=True)
+        step()
+        host_out.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record()
+    for _ in range(e_steps):
+        rhs.copy_(host_in, non_blocking=True)
+        step()
+        host_out.copy_(out, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e_steps
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * N_CPLX / (float(t.item()) * 1e-3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, cores, desc = cpu_reference_sample(target_s=12.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded, N(0,1) complex RHS, dominant tridiagonal, U(-1,1) 5-band)",
+                "config": {"workload": "config2: N=1024, 65536 complex RHS per GPU, XXII in -> packed out, "
+                                       "dgbmv(5) + tridiagonal JW step (jw_type 13) fused, one kernel per step",
+                           "rhs_per_gpu": N_CPLX, "l2": "inputs 2 GiB > L2, no flush",
+                           "parallelism": f"replicas x{world} (independent RHS shards, no collective)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                             "bytes_per_launch": bytes_alg},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * N_CPLX * 8,
+                        "d2h_bytes_per_step": 2 * M * N_CPLX * 8},
+                "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            gpu_arm(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

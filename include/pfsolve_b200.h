@@ -1,0 +1,265 @@
+/*
+ * pfsolve_b200.h -- C ABI of the B200-native Jones-Worland step library.
+ *
+ * This header is the drop-in boundary for PfSolve's JW path.  It keeps the
+ * reference's type names, field names, bitfield values and result codes for
+ * the Jones-Worland, dgbmv and block applications, so code written against
+ * PfSolve's public API (PfSolve/pfSolve.h) compiles against it for that path:
+ *
+ *   initializePfSolve  <- PfSolve/pfSolve_AppManagement/pfSolve_InitializeApp.h:1480
+ *   PfSolveAppend      <- PfSolve/pfSolve_AppManagement/pfSolve_RunApp.h:80
+ *   PfSolveSync        <- PfSolve/pfSolve_AppManagement/pfSolve_RunApp.h:28
+ *   deletePfSolve      <- PfSolve/pfSolve_AppManagement/pfSolve_DeleteApp.h:28
+ *   PfSolveConfiguration / PfSolveLaunchParams / PfSolveResult
+ *                      <- PfSolve/pfSolve_Structs/pfSolve_Structs.h:119-543
+ *   app library (checkLibrary_* / addToLibrary_*)
+ *                      <- PfSolve/pfSolve_AppCollectionManager.hpp:29-148
+ *
+ * Only the fields the JW / dgbmv / block applications read are present.
+ * The kernels are precompiled for sm_100a; there is no runtime code generation.
+ * Entry points marked "extension" have no counterpart in the reference.
+ *
+ * Everything is plain C: pointers, integers, doubles.  Device buffers are
+ * caller-owned; the library never frees them.
+ */
+#ifndef PFSOLVE_B200_H
+#define PFSOLVE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PFSOLVE_API __attribute__((visibility("default")))
+#else
+#define PFSOLVE_API
+#endif
+
+/* Same types as cuda.h / cuda_runtime_api.h declare (identical redeclaration). */
+typedef int CUdevice;
+typedef struct CUstream_st* cudaStream_t;
+
+/* jw_control_bitmask: which values come from PfSolveLaunchParams at launch
+ * (pfSolve_Structs.h:73-81). */
+#define RUNTIME_MSIZE 1
+#define RUNTIME_OFFSETM 2
+#define RUNTIME_OFFSETV 4
+#define RUNTIME_OFFSETSOLUTION 8
+#define RUNTIME_INPUTZEROPAD 16
+#define RUNTIME_OUTPUTZEROPAD 32
+#define RUNTIME_SCALEC 64
+#define RUNTIME_INPUTBUFFERSTRIDE 128
+#define RUNTIME_OUTPUTBUFFERSTRIDE 256
+
+/* block kernel selector (pfSolve_Structs.h:83-94). */
+#define BLOCK_READ_REAL_WRITE_REAL 1
+#define BLOCK_READ_COMPLEX_R_WRITE_REAL 2
+#define BLOCK_READ_COMPLEX_I_WRITE_REAL 3
+#define BLOCK_READ_COMPLEX_STRIDED_WRITE_COMPLEX_PACKED 4
+#define BLOCK_READ_REAL_WRITE_COMPLEX_R 5
+#define BLOCK_READ_REAL_WRITE_COMPLEX_I 6
+#define BLOCK_READ_COMPLEX_PACKED_WRITE_COMPLEX_STRIDED 7
+#define BLOCK_ADD_OUTPUTBUFFER_VALUES 20
+#define BLOCK_SCALEC 100
+#define BLOCK_SCALED 200
+#define BLOCK_SCALESPHLAPLA 300
+#define BLOCK_SCALESPHLAPLB 400
+
+/* jw_type digits (pfSolve_Structs.h:96-99). */
+#define JWT_DISABLE_TRIDIAGONAL_SOLVE 1
+#define JWT_DISABLE_MATVECMUL_SOLVE 2
+#define JWT_DIAGONAL_MATVECMUL 3
+#define JWT_USE_PARALLEL_THOMAS 10
+
+typedef enum PfSolveResult {
+    PFSOLVE_SUCCESS = 0,
+    PFSOLVE_ERROR_MALLOC_FAILED = 1,
+    PFSOLVE_ERROR_INSUFFICIENT_CODE_BUFFER = 2,
+    PFSOLVE_ERROR_INSUFFICIENT_TEMP_BUFFER = 3,
+    PFSOLVE_ERROR_PLAN_NOT_INITIALIZED = 4,
+    PFSOLVE_ERROR_NULL_TEMP_PASSED = 5,
+    PFSOLVE_ERROR_MATH_FAILED = 6,
+    PFSOLVE_ERROR_INVALID_PHYSICAL_DEVICE = 1001,
+    PFSOLVE_ERROR_INVALID_DEVICE = 1002,
+    PFSOLVE_ERROR_INVALID_CONTEXT = 1008,
+    PFSOLVE_ERROR_EMPTY_FFTdim = 2001,
+    PFSOLVE_ERROR_EMPTY_size = 2002,
+    PFSOLVE_ERROR_EMPTY_bufferSize = 2003,
+    PFSOLVE_ERROR_EMPTY_buffer = 2004,
+    PFSOLVE_ERROR_EMPTY_outputBufferSize = 2009,
+    PFSOLVE_ERROR_EMPTY_outputBuffer = 2010,
+    PFSOLVE_ERROR_EMPTY_kernel = 2012,
+    PFSOLVE_ERROR_UNSUPPORTED_RADIX = 3001,
+    PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH = 3002,
+    PFSOLVE_ERROR_FAILED_TO_ALLOCATE = 4001,
+    PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE = 4028,
+    PFSOLVE_ERROR_FAILED_TO_COPY = 4029,
+    PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL = 4039,
+    PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD = 4040,
+    PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE = 4051,
+    /* extension codes (no counterpart in the reference) */
+    PFSOLVE_ERROR_UNSUPPORTED_COMBINATION = 5001, /* parameter combination the reference leaves undefined */
+    PFSOLVE_ERROR_INVALID_ARGUMENT = 5002,        /* NULL pointer, negative size, misaligned buffer */
+    PFSOLVE_ERROR_CAPACITY = 5003,                /* request exceeds a stated fixed capacity */
+    PFSOLVE_ERROR_DEVICE_FAULT = 5004             /* a kernel reported an error status */
+} PfSolveResult;
+
+/* Plan-time parameters.  Field names, types and meaning follow
+ * PfSolveConfiguration (pfSolve_Structs.h:119-381) for the JW / dgbmv / block
+ * applications.  Zero-initialise, then set what you need. */
+typedef struct {
+    uint64_t FFTdim;      /* must be 1 */
+    uint64_t size[3];     /* size[0] = system length (or block row length), size[1] = batch */
+
+    CUdevice* device;     /* device ordinal holder, required */
+    cudaStream_t* stream; /* streams to launch on (NULL: default stream) */
+    uint64_t num_streams; /* launches rotate over num_streams streams when > 1 */
+
+    uint64_t* bufferSize;       /* optional */
+    uint64_t* outputBufferSize; /* optional */
+    uint64_t* kernelSize;       /* optional */
+    void** buffer;              /* bands (JW, dgbmv) or input (block); may be set at launch */
+    void** outputBuffer;        /* right-hand sides, solved in place (JW, dgbmv) or block output */
+    void** kernel;              /* temporary buffer (unused by single-upload plans) */
+
+    int upperBanded;      /* 0: lower-banded V / upper M, 1: upper-banded V / lower M, 2: tridiagonal */
+    int jw_type;          /* >= 10 selects the JW application; jw_type % 10: 0 matvec+solve,
+                             1 matvec only, 2 solve only, 3 diagonal matvec + solve */
+    int block;            /* > 0 selects the block application (BLOCK_* sum) */
+    int lshift;           /* harmonic degree shift used by the Scale operators */
+    int LDA;              /* > 0 selects the dgbmv application: LDA = KL + KU + 1 bands */
+    int KU;
+    int KL;
+    int ALT_dgbmv;        /* not supported: must be 0 */
+    uint64_t Msplit[3];   /* multi-upload split (accepted, single upload used for M <= 4352) */
+
+    int64_t jw_control_bitmask; /* RUNTIME_* bits */
+    int64_t M_size;
+    int64_t offsetM;
+    int64_t offsetV;
+    int64_t offsetSolution;
+    int64_t inputZeropad[2];
+    int64_t outputZeropad[2];
+    double scaleC;
+
+    uint64_t doublePrecision;                       /* FP64 storage and arithmetic */
+    uint64_t quadDoubleDoublePrecision;             /* double-double storage and arithmetic */
+    uint64_t quadDoubleDoublePrecisionDoubleMemory; /* double-double arithmetic, FP64 storage */
+    uint64_t halfPrecision;                         /* not supported: must be 0 */
+    uint64_t doublePrecisionFloatMemory;            /* FP64 arithmetic, FP32 storage */
+
+    uint64_t inputBufferStride[3];
+    uint64_t outputBufferStride[3];
+    uint64_t isInputFormatted;
+    uint64_t isOutputFormatted;
+
+    uint64_t keepShaderCode;    /* accepted; there is no generated code to print */
+    uint64_t printMemoryLayout; /* accepted */
+    int disableCaching;         /* accepted; plans are never cached on disk */
+    uint64_t disableSetLocale;  /* accepted */
+    uint64_t useUint64;         /* accepted; addressing is always 64-bit */
+
+    int numConsecutiveJWIterations; /* K; 1 supported */
+    int useMultipleInputBuffers;    /* bands of step k in buffer[k] */
+
+    /* --- extensions (0 keeps the reference behaviour) --- */
+    int mixedPrecisionRefinement; /* > 0 with doublePrecision: FP32 solve + this many (<= 3)
+                                     FP64 residual refinement sweeps, FP64 storage */
+    int rowsPerThread;            /* 0: autotuned; else 2, 4, 8 or 16 */
+} PfSolveConfiguration;
+
+/* Launch-time values (pfSolve_Structs.h:383-449). */
+typedef struct {
+    void** buffer;       /* bands / block input; NULL keeps the plan's */
+    void** outputBuffer; /* right-hand sides / block output; NULL keeps the plan's */
+    void** kernel;
+
+    uint64_t M_size;
+    uint64_t offsetM;
+    uint64_t offsetV;
+    uint64_t offsetSolution;
+    uint64_t inputZeropad[2];
+    uint64_t outputZeropad[2];
+    long double scaleC;
+    uint64_t inputBufferStride;
+    uint64_t outputBufferStride;
+    uint64_t batchSize; /* > 0 replaces size[1] for this and later launches */
+} PfSolveLaunchParams;
+
+/* Opaque plan state lives behind `internal`; `configuration` is the copy
+ * initializePfSolve validated (pfSolve_Structs.h:1292-1341 holds the
+ * reference's larger struct). */
+typedef struct PfSolveApplication {
+    PfSolveConfiguration configuration;
+    void* internal;
+} PfSolveApplication;
+
+/* Validate `configuration` (passed by value, as in the reference), pick the
+ * kernel variant and launch shape, and query the device.  On failure the app
+ * is released and the error returned. */
+PFSOLVE_API PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration configuration);
+
+/* Enqueue one application launch on the plan's stream; never synchronises.
+ * `inverse` is ignored, as in the reference. */
+PFSOLVE_API PfSolveResult PfSolveAppend(PfSolveApplication* app, int inverse, PfSolveLaunchParams* launchParams);
+
+/* Wait for the plan's streams when num_streams > 1 (no-op otherwise). */
+PFSOLVE_API PfSolveResult PfSolveSync(PfSolveApplication* app);
+
+/* Release the plan's host and device state (never the user's buffers). */
+PFSOLVE_API void deletePfSolve(PfSolveApplication* app);
+
+PFSOLVE_API const char* getPfSolveErrorString(PfSolveResult result);
+PFSOLVE_API int PfSolveGetVersion(void);
+
+/* ---- App library (kernel reuse cache), pfSolve_AppCollectionManager.hpp ---- */
+typedef struct PfSolve_MapKey_JonesWorland {
+    int64_t size[2];
+    int64_t upperBanded;
+    int64_t outputBufferStride;
+    int64_t type;
+} PfSolve_MapKey_JonesWorland;
+typedef struct PfSolve_MapKey_dgbmv {
+    int64_t size[2];
+    int64_t outputBufferStride;
+    int64_t LDA;
+    int64_t KU;
+    int64_t KL;
+} PfSolve_MapKey_dgbmv;
+typedef struct PfSolve_MapKey_block {
+    int64_t size[2];
+    int64_t inputBufferStride;
+    int64_t outputBufferStride;
+    int64_t type;
+    int64_t lshift;
+} PfSolve_MapKey_block;
+
+typedef struct PfSolve_AppLibrary PfSolve_AppLibrary;
+
+PFSOLVE_API PfSolve_AppLibrary* PfSolveAppLibraryCreate(void);                 /* extension: C handle */
+PFSOLVE_API void PfSolveAppLibraryDestroy(PfSolve_AppLibrary* lib);            /* extension: deletes the apps it holds */
+PFSOLVE_API PfSolveResult checkLibrary_JonesWorland(PfSolve_AppLibrary* lib, PfSolve_MapKey_JonesWorland key, PfSolveApplication** app);
+PFSOLVE_API PfSolveResult addToLibrary_JonesWorland(PfSolve_AppLibrary* lib, PfSolve_MapKey_JonesWorland key, PfSolveApplication* app);
+PFSOLVE_API PfSolveResult checkLibrary_dgbmv(PfSolve_AppLibrary* lib, PfSolve_MapKey_dgbmv key, PfSolveApplication** app);
+PFSOLVE_API PfSolveResult addToLibrary_dgbmv(PfSolve_AppLibrary* lib, PfSolve_MapKey_dgbmv key, PfSolveApplication* app);
+PFSOLVE_API PfSolveResult checkLibrary_block(PfSolve_AppLibrary* lib, PfSolve_MapKey_block key, PfSolveApplication** app);
+PFSOLVE_API PfSolveResult addToLibrary_block(PfSolve_AppLibrary* lib, PfSolve_MapKey_block key, PfSolveApplication* app);
+
+/* ---- Fused chain (extension) ----
+ * Runs apps[0..n-1] as if appended one after the other on the same data, in
+ * one kernel when the chain is [dgbmv] -> JW -> [block] over the same systems.
+ * Intermediate results are not written back to memory.  Returns
+ * PFSOLVE_ERROR_UNSUPPORTED_COMBINATION when the chain cannot be fused and
+ * `allowUnfused` is 0; with allowUnfused the apps run one by one. */
+PFSOLVE_API PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveLaunchParams** launchParams, int n,
+                                 int allowUnfused);
+
+/* Number of kernel launches this library has enqueued since load (all apps). */
+PFSOLVE_API uint64_t PfSolveLaunchCount(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFSOLVE_B200_H */

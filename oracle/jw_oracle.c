@@ -1,0 +1,457 @@
+/*
+ * jw_oracle.c -- CPU restatement of PfSolve's Jones-Worland step (see jw_oracle.h).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for parity tests, smoke() and the CPU
+ * baseline of bench.py.  Not part of the product; nothing in libpfsolve_b200.so
+ * links or calls it.
+ *
+ * File references are relative to the PfSolve project root.
+ */
+#include "jw_oracle.h"
+
+#include <math.h>
+#include <quadmath.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef __float128 q_t;
+
+/* ------------------------------------------------------------------------- */
+/* Register-major band layout.
+ * reorder_i0 (pfSolve_Plan_JonesWorland.h:66-142): the kernel gives each lane
+ * r = ceil(M / T) consecutive rows (T = 32 below 512 rows, else 64*ceil(M/1024);
+ * pfSolve_Plan_JonesWorland.h:311-346) and loads band register j of every lane
+ * with one coalesced access, so row t*r + j is stored at S_j + t where S_j
+ * counts the rows held by registers 0..j-1 (ceil(M/r) lanes for j < M%r, else
+ * floor(M/r)).  Systems longer than 4352 rows are split into Msplit0-row
+ * pieces, each permuted on its own. */
+int64_t pfo_reorder_i0(int64_t i, int64_t M, int64_t Msplit0)
+{
+    if (Msplit0 == 0) Msplit0 = 256;
+    int64_t size0 = M, size1 = M;
+    if (M > 4352) { size0 = Msplit0; size1 = Msplit0; }
+    int64_t warp = 64 * ((size1 + 1023) / 1024);
+    if (size1 < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    int64_t r = (size1 + warp - 1) / warp;
+    int64_t piece = (i / size0) * size0;
+    int64_t li = i % size0;
+    if (((i / size0) + 1) * size0 > M) size0 = M % size0;
+    int64_t t = li / r, j = li % r;
+    int64_t m = size0 % r, ceil_n = (size0 + r - 1) / r, floor_n = size0 / r;
+    int64_t pos = t;
+    if (j < m) pos += j * ceil_n;
+    else pos += m * ceil_n + (j - m) * floor_n;
+    return pos + piece;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Resolution of plan-time vs launch-time values (pfSolve_Plan_JonesWorland.h:387-526). */
+static int64_t rv(const pfo_params* p, int64_t bit, int64_t cfg, int64_t run)
+{
+    return (p->bitmask & bit) ? run : cfg;
+}
+
+/* Keep-window test of PfConfigureZeropad (pfSolve_KernelsLevel0/pfSolve_Zeropad.h:306-377):
+ * launch-time windows keep [z0, z1); plan-time windows treat 0 as "no bound". */
+static int keep(int64_t i, int64_t z0, int64_t z1, int runtime)
+{
+    if (runtime) return (i >= z0) && (i < z1);
+    if (z0) return (i >= z0) && ((z1 == 0) || (i < z1));
+    if (z1) return i < z1;
+    return 1;
+}
+
+typedef struct {
+    int mv, sv;
+    int64_t off_md, off_mo, off_sl, off_su; /* band offsets (elements) */
+} jw_layout;
+
+/* Band offsets for K = 1 (pfSolve_JonesWorland.h:117-207 for the matvec
+ * operand, :269-353 for the solve operand).  Plan-time offsetM/offsetV are
+ * not added by the reference (the additions are commented out at :161-162,
+ * :191-192, :291-295, :321-324); only the RUNTIME_OFFSETM/V forms move the
+ * bands, and with the runtime forms the two matvec bands swap places
+ * (:156-157 and :186-187). */
+static int jw_resolve(const pfo_params* p, jw_layout* L)
+{
+    const int64_t M = p->M;
+    const int jwt = p->jw_type % 10;
+    const int rtM = (p->bitmask & PFO_RUNTIME_OFFSETM) != 0;
+    const int rtV = (p->bitmask & PFO_RUNTIME_OFFSETV) != 0;
+    const int64_t oM = p->run_offsetM, oV = p->run_offsetV;
+    memset(L, 0, sizeof(*L));
+    if (p->upperBanded == 2) {
+        /* tridiagonal: ld at 0, md at M, ud at 2M (:117-131) */
+        L->off_md = M; L->off_sl = 0; L->off_su = 2 * M;
+        if (jwt == 3) { L->mv = PFO_MV_DIAG; L->sv = PFO_SV_TRI; return 0; }
+        if (jwt == 2) { L->mv = PFO_MV_NONE; L->sv = PFO_SV_TRI; return 0; }
+        return -1;
+    }
+    if (jwt == 2) L->mv = PFO_MV_NONE;
+    else if (jwt == 3) {
+        /* jw_type%10 == 3 flips upperBanded while the matvec offsets are
+         * chosen (:133-136, :203-206); the matvec is then md-only (:241-245). */
+        L->mv = PFO_MV_DIAG;
+        if (p->upperBanded == 1) L->off_md = rtM ? oM : M;
+        else L->off_md = rtM ? oM + M : 0;
+    } else if (p->upperBanded == 1) {
+        L->mv = PFO_MV_UPPER;
+        L->off_md = rtM ? oM + M : 0;
+        L->off_mo = rtM ? oM : M;
+    } else {
+        L->mv = PFO_MV_LOWER;
+        L->off_md = rtM ? oM : M;
+        L->off_mo = rtM ? oM + M : 0;
+    }
+    if (jwt == 1) L->sv = PFO_SV_NONE;
+    else if (p->upperBanded == 1) { L->sv = PFO_SV_LOWER; L->off_sl = rtV ? oV : 2 * M; }
+    else { L->sv = PFO_SV_UPPER; L->off_su = rtV ? oV : 2 * M; }
+    return 0;
+}
+
+static int64_t band_pos(const pfo_params* p, int64_t i)
+{
+    return p->bandsPermuted ? pfo_reorder_i0(i, p->M, 0) : i;
+}
+
+int pfo_jw_operator(const pfo_params* p, const double* bands, int* mv_kind, int* sv_kind,
+                    double* mv_d, double* mv_o, double* sv_l, double* sv_u)
+{
+    jw_layout L;
+    if (jw_resolve(p, &L)) return -1;
+    *mv_kind = L.mv; *sv_kind = L.sv;
+    for (int64_t i = 0; i < p->M; i++) {
+        int64_t k = band_pos(p, i);
+        if (L.mv != PFO_MV_NONE && mv_d) mv_d[i] = bands[L.off_md + k];
+        if ((L.mv == PFO_MV_UPPER || L.mv == PFO_MV_LOWER) && mv_o) mv_o[i] = bands[L.off_mo + k];
+        if ((L.sv == PFO_SV_LOWER || L.sv == PFO_SV_TRI) && sv_l) sv_l[i] = bands[L.off_sl + k];
+        if ((L.sv == PFO_SV_UPPER || L.sv == PFO_SV_TRI) && sv_u) sv_u[i] = bands[L.off_su + k];
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* One system in type T: matvec (pfSolve_MatVecMul.h:28-133), unit-diagonal
+ * bi-/tridiagonal solve (pfSolve_TridiagonalSolve.h:1578-1929), scaleC on
+ * solution row 0 (:1918-1927).  Rows outside [0, M) read as zero, so
+ * ld[0] and ud[M-1] never contribute. */
+#define DEFINE_SYSTEM(NAME, T)                                                           \
+    static void NAME(int mv, int sv, int64_t M, const T* md, const T* mo, const T* sl,   \
+                     const T* su, T scaleC, T* b, T* g, T* w)                            \
+    {                                                                                    \
+        for (int64_t i = 0; i < M; i++) {                                                \
+            T v = b[i];                                                                  \
+            if (mv == PFO_MV_DIAG) v = md[i] * b[i];                                     \
+            else if (mv == PFO_MV_UPPER)                                                 \
+                v = md[i] * b[i] + ((i + 1 < M) ? mo[i] * b[i + 1] : (T)0);              \
+            else if (mv == PFO_MV_LOWER)                                                 \
+                v = md[i] * b[i] + ((i > 0) ? mo[i] * b[i - 1] : (T)0);                  \
+            g[i] = v;                                                                    \
+        }                                                                                \
+        if (sv == PFO_SV_LOWER) {                                                        \
+            for (int64_t i = 1; i < M; i++) g[i] = g[i] - sl[i] * g[i - 1];              \
+        } else if (sv == PFO_SV_UPPER) {                                                 \
+            for (int64_t i = M - 2; i >= 0; i--) g[i] = g[i] - su[i] * g[i + 1];         \
+        } else if (sv == PFO_SV_TRI) {                                                   \
+            /* Thomas, sample_0_benchmark_VkFFT_single.cpp:437-460, unit diagonal */     \
+            w[0] = su[0];                                                                \
+            for (int64_t i = 1; i < M; i++) {                                            \
+                T den = (T)1 - sl[i] * w[i - 1];                                         \
+                w[i] = su[i] / den;                                                      \
+                g[i] = (g[i] - sl[i] * g[i - 1]) / den;                                  \
+            }                                                                            \
+            for (int64_t i = M - 2; i >= 0; i--) g[i] = g[i] - w[i] * g[i + 1];          \
+        }                                                                                \
+        if (sv != PFO_SV_NONE && M > 0) g[0] = g[0] * scaleC;                            \
+    }
+DEFINE_SYSTEM(system_q, q_t)
+DEFINE_SYSTEM(system_d, double)
+
+typedef struct {
+    int64_t offS, oStride;
+    int64_t iz0, iz1, oz0, oz1;
+    int rtIZ, rtOZ;
+    double scaleC;
+} rhs_layout;
+
+static void rhs_resolve(const pfo_params* p, rhs_layout* R)
+{
+    R->offS = rv(p, PFO_RUNTIME_OFFSETSOLUTION, p->cfg_offsetSolution, p->run_offsetSolution);
+    R->oStride = rv(p, PFO_RUNTIME_OUTPUTBUFFERSTRIDE, p->cfg_outputBufferStride, p->run_outputBufferStride);
+    R->rtIZ = (p->bitmask & PFO_RUNTIME_INPUTZEROPAD) != 0;
+    R->rtOZ = (p->bitmask & PFO_RUNTIME_OUTPUTZEROPAD) != 0;
+    R->iz0 = R->rtIZ ? p->run_inputZeropad[0] : p->cfg_inputZeropad[0];
+    R->iz1 = R->rtIZ ? p->run_inputZeropad[1] : p->cfg_inputZeropad[1];
+    R->oz0 = R->rtOZ ? p->run_outputZeropad[0] : p->cfg_outputZeropad[0];
+    R->oz1 = R->rtOZ ? p->run_outputZeropad[1] : p->cfg_outputZeropad[1];
+    R->scaleC = (p->bitmask & PFO_RUNTIME_SCALEC) ? p->run_scaleC : p->cfg_scaleC;
+}
+
+/* Storage kinds for the generic driver. */
+enum { ST_F64 = 0, ST_F32 = 1, ST_DD = 2 };
+
+static q_t load_q(const void* a, int st, int64_t k)
+{
+    if (st == ST_F64) return (q_t)((const double*)a)[k];
+    if (st == ST_F32) return (q_t)((const float*)a)[k];
+    const double* d = (const double*)a;
+    return (q_t)d[2 * k] + (q_t)d[2 * k + 1];
+}
+
+static void store_q(void* a, int st, int64_t k, q_t v)
+{
+    if (st == ST_F64) ((double*)a)[k] = (double)v;
+    else if (st == ST_F32) ((float*)a)[k] = (float)v;
+    else {
+        double hi = (double)v;
+        double lo = (double)(v - (q_t)hi);
+        ((double*)a)[2 * k] = hi;
+        ((double*)a)[2 * k + 1] = lo;
+    }
+}
+
+static int jw_step_q_generic(const pfo_params* p, const void* bands, void* rhs, int st, int nthreads)
+{
+    jw_layout L;
+    if (jw_resolve(p, &L)) return -1;
+    rhs_layout R;
+    rhs_resolve(p, &R);
+    const int64_t M = p->M;
+    q_t* md = (q_t*)calloc((size_t)M + 1, sizeof(q_t));
+    q_t* mo = (q_t*)calloc((size_t)M + 1, sizeof(q_t));
+    q_t* sl = (q_t*)calloc((size_t)M + 1, sizeof(q_t));
+    q_t* su = (q_t*)calloc((size_t)M + 1, sizeof(q_t));
+    if (!md || !mo || !sl || !su) { free(md); free(mo); free(sl); free(su); return -1; }
+    for (int64_t i = 0; i < M; i++) {
+        int64_t k = band_pos(p, i);
+        if (L.mv != PFO_MV_NONE) md[i] = load_q(bands, st, L.off_md + k);
+        if (L.mv == PFO_MV_UPPER || L.mv == PFO_MV_LOWER) mo[i] = load_q(bands, st, L.off_mo + k);
+        if (L.sv == PFO_SV_LOWER || L.sv == PFO_SV_TRI) sl[i] = load_q(bands, st, L.off_sl + k);
+        if (L.sv == PFO_SV_UPPER || L.sv == PFO_SV_TRI) su[i] = load_q(bands, st, L.off_su + k);
+    }
+    q_t sC = (st == ST_F32) ? (q_t)(float)R.scaleC : (q_t)R.scaleC;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        q_t* b = (q_t*)malloc(sizeof(q_t) * (size_t)(M + 1));
+        q_t* g = (q_t*)malloc(sizeof(q_t) * (size_t)(M + 1));
+        q_t* w = (q_t*)malloc(sizeof(q_t) * (size_t)(M + 1));
+#pragma omp for schedule(static)
+        for (int64_t y = 0; y < p->batch; y++) {
+            int64_t base = R.offS + y * R.oStride;
+            for (int64_t i = 0; i < M; i++)
+                b[i] = keep(i, R.iz0, R.iz1, R.rtIZ) ? load_q(rhs, st, base + i) : (q_t)0;
+            system_q(L.mv, L.sv, M, md, mo, sl, su, sC, b, g, w);
+            for (int64_t i = 0; i < M; i++)
+                if (keep(i, R.oz0, R.oz1, R.rtOZ)) store_q(rhs, st, base + i, g[i]);
+        }
+        free(b); free(g); free(w);
+    }
+    free(md); free(mo); free(sl); free(su);
+    return 0;
+}
+
+int pfo_jw_step_q(const pfo_params* p, const double* bands, double* rhs, int nthreads)
+{
+    return jw_step_q_generic(p, bands, rhs, ST_F64, nthreads);
+}
+int pfo_jw_step_q_f32(const pfo_params* p, const float* bands, float* rhs, int nthreads)
+{
+    return jw_step_q_generic(p, bands, rhs, ST_F32, nthreads);
+}
+int pfo_jw_step_q_dd(const pfo_params* p, const double* bands_dd, double* rhs_dd, int nthreads)
+{
+    return jw_step_q_generic(p, bands_dd, rhs_dd, ST_DD, nthreads);
+}
+
+int pfo_jw_step_d(const pfo_params* p, const double* bands, double* rhs, int nthreads)
+{
+    jw_layout L;
+    if (jw_resolve(p, &L)) return -1;
+    rhs_layout R;
+    rhs_resolve(p, &R);
+    const int64_t M = p->M;
+    double* md = (double*)calloc((size_t)M + 1, sizeof(double));
+    double* mo = (double*)calloc((size_t)M + 1, sizeof(double));
+    double* sl = (double*)calloc((size_t)M + 1, sizeof(double));
+    double* su = (double*)calloc((size_t)M + 1, sizeof(double));
+    if (!md || !mo || !sl || !su) { free(md); free(mo); free(sl); free(su); return -1; }
+    for (int64_t i = 0; i < M; i++) {
+        int64_t k = band_pos(p, i);
+        if (L.mv != PFO_MV_NONE) md[i] = bands[L.off_md + k];
+        if (L.mv == PFO_MV_UPPER || L.mv == PFO_MV_LOWER) mo[i] = bands[L.off_mo + k];
+        if (L.sv == PFO_SV_LOWER || L.sv == PFO_SV_TRI) sl[i] = bands[L.off_sl + k];
+        if (L.sv == PFO_SV_UPPER || L.sv == PFO_SV_TRI) su[i] = bands[L.off_su + k];
+    }
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        double* b = (double*)malloc(sizeof(double) * (size_t)(M + 1));
+        double* g = (double*)malloc(sizeof(double) * (size_t)(M + 1));
+        double* w = (double*)malloc(sizeof(double) * (size_t)(M + 1));
+#pragma omp for schedule(static)
+        for (int64_t y = 0; y < p->batch; y++) {
+            int64_t base = R.offS + y * R.oStride;
+            for (int64_t i = 0; i < M; i++) b[i] = keep(i, R.iz0, R.iz1, R.rtIZ) ? rhs[base + i] : 0.0;
+            system_d(L.mv, L.sv, M, md, mo, sl, su, R.scaleC, b, g, w);
+            for (int64_t i = 0; i < M; i++)
+                if (keep(i, R.oz0, R.oz1, R.rtOZ)) rhs[base + i] = g[i];
+        }
+        free(b); free(g); free(w);
+    }
+    free(md); free(mo); free(sl); free(su);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* dgbmv: y_r = sum_j A[offsetM + j*M + c] x_c, c = r + KU - j, 0 <= c < M
+ * (pfSolve_MatVecMul.h:389-443).  The plan-time offsetM is honoured here
+ * (pfSolve_dgbmv.h:79-87), unlike the JW kernel. */
+#define DEFINE_DGBMV(NAME, T)                                                              \
+    int NAME(const pfo_params* p, const double* A, double* rhs, int nthreads)              \
+    {                                                                                      \
+        rhs_layout R;                                                                      \
+        rhs_resolve(p, &R);                                                                \
+        const int64_t M = p->M;                                                            \
+        const int64_t offM = rv(p, PFO_RUNTIME_OFFSETM, p->cfg_offsetM, p->run_offsetM);   \
+        if (p->LDA <= 0 || p->KU < 0 || p->KU >= p->LDA) return -1;                        \
+        _Pragma("omp parallel num_threads(nthreads > 0 ? nthreads : 1)")                   \
+        {                                                                                  \
+            T* x = (T*)malloc(sizeof(T) * (size_t)(M + 1));                                \
+            _Pragma("omp for schedule(static)")                                            \
+            for (int64_t y = 0; y < p->batch; y++) {                                       \
+                int64_t base = R.offS + y * R.oStride;                                     \
+                for (int64_t i = 0; i < M; i++)                                            \
+                    x[i] = keep(i, R.iz0, R.iz1, R.rtIZ) ? (T)rhs[base + i] : (T)0;        \
+                for (int64_t r = 0; r < M; r++) {                                          \
+                    T acc = 0;                                                             \
+                    for (int64_t j = 0; j < p->LDA; j++) {                                 \
+                        int64_t c = r + p->KU - j;                                         \
+                        if (c < 0 || c >= M) continue;                                     \
+                        acc += (T)A[offM + j * M + c] * x[c];                              \
+                    }                                                                      \
+                    if (keep(r, R.oz0, R.oz1, R.rtOZ)) rhs[base + r] = (double)acc;        \
+                }                                                                          \
+            }                                                                              \
+            free(x);                                                                       \
+        }                                                                                  \
+        return 0;                                                                          \
+    }
+DEFINE_DGBMV(pfo_dgbmv_q, q_t)
+DEFINE_DGBMV(pfo_dgbmv_d, double)
+
+/* ------------------------------------------------------------------------- */
+/* Scale operators, runtime-scaleC branch (pfSolve_RegistersScaleC.h:27-201);
+ * x is the row index inside the system, L = lshift, s = scaleC. */
+static q_t scale_factor_q(int kind, int64_t x, int L, q_t s)
+{
+    q_t X = (q_t)x;
+    switch (kind) {
+    case 1: return s;
+    case 2: return (q_t)2 * (X + L + 1) * sqrtq((X + 1) / (X + s + L + (q_t)1.5));
+    case 3:
+        return (q_t)4 * (X + L + 2) * (X + L + 3) *
+               sqrtq((X + 1) * (X + 2) / ((X + s + L + (q_t)2.5) * (X + s + L + (q_t)3.5)));
+    case 4: return ((q_t)4 * L + 6) * (X + L + 1) * sqrtq((X + 1) / (X + s + L + (q_t)1.5));
+    default: return (q_t)1;
+    }
+}
+
+double pfo_scale_factor(int kind, int64_t x, int lshift, double s)
+{
+    return (double)scale_factor_q(kind, x, lshift, (q_t)s);
+}
+
+/* Block kernel: element (x = e mod size0, y = e div size0); read at
+ * offsetM + y*inputStride + x, write at offsetSolution + y*outputStride + x
+ * (pfSolve_ReadWrite.h:2293-2317).  block%10 picks the layout conversion
+ * (XXII = per-row real block then imaginary block, pfSolve_ReadWrite.h:2313-2354,
+ * with the in/out types of pfSolve_KernelStartEnd.h:1089-1097), block/10%10 == 2
+ * accumulates into the output (:2320-2329), block/100 picks the Scale
+ * operator.  Scale operators multiply both components of a complex value by
+ * the real factor.  block/100 == 1 with a plan-time scaleC of 0 writes zeros
+ * without reading (pfSolve_block.h:82). */
+int pfo_block_q(const pfo_params* p, const double* in, double* out)
+{
+    const int bt = p->block % 10, acc = ((p->block / 10) % 10) == 2, sk = p->block / 100;
+    if (bt < 1 || bt > 7 || sk > 4) return -1;
+    if (acc && bt == 4) return -1; /* reads a real into a complex register: undefined */
+    rhs_layout R;
+    rhs_resolve(p, &R);
+    const int64_t offM = rv(p, PFO_RUNTIME_OFFSETM, p->cfg_offsetM, p->run_offsetM);
+    const int64_t iS = rv(p, PFO_RUNTIME_INPUTBUFFERSTRIDE, p->cfg_inputBufferStride, p->run_inputBufferStride);
+    const int64_t oS = R.oStride, offS = R.offS;
+    const int rtC = (p->bitmask & PFO_RUNTIME_SCALEC) != 0;
+    const int skip = (sk == 1) && !rtC && (p->cfg_scaleC == 0.0);
+    const q_t s = (q_t)R.scaleC;
+    for (int64_t y = 0; y < p->size1; y++) {
+        for (int64_t x = 0; x < p->size0; x++) {
+            q_t vr = 0, vi = 0;
+            if (!skip) {
+                if (keep(x, R.iz0, R.iz1, R.rtIZ)) {
+                    int64_t ii = offM + y * iS;
+                    switch (bt) {
+                    case 1: vr = in[ii + x]; break;
+                    case 2: case 3: case 4: vr = in[2 * (ii + x)]; vi = in[2 * (ii + x) + 1]; break;
+                    case 5: vr = in[ii + x]; break;
+                    case 6: vi = in[ii + x]; break;
+                    case 7: vr = in[2 * ii + x]; vi = in[2 * ii + x + iS]; break;
+                    }
+                }
+                if (sk) {
+                    q_t f = scale_factor_q(sk, x, p->lshift, s);
+                    vr *= f; vi *= f;
+                }
+            }
+            if (!keep(x, R.oz0, R.oz1, R.rtOZ)) continue;
+            int64_t oi = offS + y * oS;
+            switch (bt) {
+            case 1: case 2:
+                if (acc) vr += out[oi + x];
+                out[oi + x] = (double)vr;
+                break;
+            case 3:
+                if (acc) vi += out[oi + x];
+                out[oi + x] = (double)vi;
+                break;
+            case 4:
+                out[2 * oi + x] = (double)vr;
+                out[2 * oi + x + oS] = (double)vi;
+                break;
+            default:
+                if (acc) { vr += out[2 * (oi + x)]; vi += out[2 * (oi + x) + 1]; }
+                out[2 * (oi + x)] = (double)vr;
+                out[2 * (oi + x) + 1] = (double)vi;
+                break;
+            }
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+void pfo_rel_errors(const double* a, const double* ref, int64_t M, int64_t batch, int64_t stride,
+                    int64_t offset, double* rel_l2_max, double* rel_max)
+{
+    double worst_l2 = 0, dmax = 0, rmax = 0;
+    for (int64_t y = 0; y < batch; y++) {
+        const double* pa = a + offset + y * stride;
+        const double* pr = ref + offset + y * stride;
+        q_t num = 0, den = 0;
+        for (int64_t i = 0; i < M; i++) {
+            q_t d = (q_t)pa[i] - (q_t)pr[i];
+            num += d * d;
+            den += (q_t)pr[i] * (q_t)pr[i];
+            double ad = fabs((double)d), ar = fabs(pr[i]);
+            if (ad > dmax) dmax = ad;
+            if (ar > rmax) rmax = ar;
+        }
+        double e = (den > 0) ? (double)sqrtq(num / den) : (double)sqrtq(num);
+        if (e > worst_l2) worst_l2 = e;
+    }
+    *rel_l2_max = worst_l2;
+    *rel_max = (rmax > 0) ? dmax / rmax : dmax;
+}

@@ -1,0 +1,157 @@
+"""ctypes binding of the C ABI in ``include/pfsolve_b200.h``.
+
+The structures mirror the header field for field; ``tests/test_abi.py`` checks
+their sizes against the compiled library's own view.  The library is the
+in-tree ``pfsolve_b200/libpfsolve_b200.so``; importing this module never falls
+back to anything else -- a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfsolve_b200.so")
+
+RUNTIME_MSIZE = 1
+RUNTIME_OFFSETM = 2
+RUNTIME_OFFSETV = 4
+RUNTIME_OFFSETSOLUTION = 8
+RUNTIME_INPUTZEROPAD = 16
+RUNTIME_OUTPUTZEROPAD = 32
+RUNTIME_SCALEC = 64
+RUNTIME_INPUTBUFFERSTRIDE = 128
+RUNTIME_OUTPUTBUFFERSTRIDE = 256
+
+BLOCK_READ_REAL_WRITE_REAL = 1
+BLOCK_READ_COMPLEX_R_WRITE_REAL = 2
+BLOCK_READ_COMPLEX_I_WRITE_REAL = 3
+BLOCK_READ_COMPLEX_STRIDED_WRITE_COMPLEX_PACKED = 4
+BLOCK_READ_REAL_WRITE_COMPLEX_R = 5
+BLOCK_READ_REAL_WRITE_COMPLEX_I = 6
+BLOCK_READ_COMPLEX_PACKED_WRITE_COMPLEX_STRIDED = 7
+BLOCK_ADD_OUTPUTBUFFER_VALUES = 20
+BLOCK_SCALEC = 100
+BLOCK_SCALED = 200
+BLOCK_SCALESPHLAPLA = 300
+BLOCK_SCALESPHLAPLB = 400
+
+PFSOLVE_SUCCESS = 0
+PFSOLVE_ERROR_INVALID_DEVICE = 1002
+PFSOLVE_ERROR_EMPTY_FFTdim = 2001
+PFSOLVE_ERROR_EMPTY_size = 2002
+PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH = 3002
+PFSOLVE_ERROR_UNSUPPORTED_COMBINATION = 5001
+PFSOLVE_ERROR_INVALID_ARGUMENT = 5002
+PFSOLVE_ERROR_CAPACITY = 5003
+
+u64 = ctypes.c_uint64
+i64 = ctypes.c_int64
+c_int = ctypes.c_int
+vpp = ctypes.POINTER(ctypes.c_void_p)
+
+
+class PfSolveConfiguration(ctypes.Structure):
+    _fields_ = [
+        ("FFTdim", u64), ("size", u64 * 3),
+        ("device", ctypes.POINTER(c_int)), ("stream", ctypes.POINTER(ctypes.c_void_p)), ("num_streams", u64),
+        ("bufferSize", ctypes.POINTER(u64)), ("outputBufferSize", ctypes.POINTER(u64)),
+        ("kernelSize", ctypes.POINTER(u64)),
+        ("buffer", vpp), ("outputBuffer", vpp), ("kernel", vpp),
+        ("upperBanded", c_int), ("jw_type", c_int), ("block", c_int), ("lshift", c_int),
+        ("LDA", c_int), ("KU", c_int), ("KL", c_int), ("ALT_dgbmv", c_int),
+        ("Msplit", u64 * 3),
+        ("jw_control_bitmask", i64), ("M_size", i64), ("offsetM", i64), ("offsetV", i64),
+        ("offsetSolution", i64), ("inputZeropad", i64 * 2), ("outputZeropad", i64 * 2),
+        ("scaleC", ctypes.c_double),
+        ("doublePrecision", u64), ("quadDoubleDoublePrecision", u64),
+        ("quadDoubleDoublePrecisionDoubleMemory", u64), ("halfPrecision", u64),
+        ("doublePrecisionFloatMemory", u64),
+        ("inputBufferStride", u64 * 3), ("outputBufferStride", u64 * 3),
+        ("isInputFormatted", u64), ("isOutputFormatted", u64),
+        ("keepShaderCode", u64), ("printMemoryLayout", u64), ("disableCaching", c_int),
+        ("disableSetLocale", u64), ("useUint64", u64),
+        ("numConsecutiveJWIterations", c_int), ("useMultipleInputBuffers", c_int),
+        ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int),
+    ]
+
+
+class PfSolveLaunchParams(ctypes.Structure):
+    _fields_ = [
+        ("buffer", vpp), ("outputBuffer", vpp), ("kernel", vpp),
+        ("M_size", u64), ("offsetM", u64), ("offsetV", u64), ("offsetSolution", u64),
+        ("inputZeropad", u64 * 2), ("outputZeropad", u64 * 2),
+        ("scaleC", ctypes.c_longdouble),
+        ("inputBufferStride", u64), ("outputBufferStride", u64), ("batchSize", u64),
+    ]
+
+
+class PfSolveApplication(ctypes.Structure):
+    _fields_ = [("configuration", PfSolveConfiguration), ("internal", ctypes.c_void_p)]
+
+
+class MapKeyJW(ctypes.Structure):
+    _fields_ = [("size", i64 * 2), ("upperBanded", i64), ("outputBufferStride", i64), ("type", i64)]
+
+
+class MapKeyDgbmv(ctypes.Structure):
+    _fields_ = [("size", i64 * 2), ("outputBufferStride", i64), ("LDA", i64), ("KU", i64), ("KL", i64)]
+
+
+class MapKeyBlock(ctypes.Structure):
+    _fields_ = [("size", i64 * 2), ("inputBufferStride", i64), ("outputBufferStride", i64), ("type", i64),
+                ("lshift", i64)]
+
+
+# Every function the header declares, with its ctypes signature.
+_APP_P = ctypes.POINTER(PfSolveApplication)
+_LP_P = ctypes.POINTER(PfSolveLaunchParams)
+SIGNATURES = {
+    "initializePfSolve": (c_int, [_APP_P, PfSolveConfiguration]),
+    "PfSolveAppend": (c_int, [_APP_P, c_int, _LP_P]),
+    "PfSolveSync": (c_int, [_APP_P]),
+    "deletePfSolve": (None, [_APP_P]),
+    "getPfSolveErrorString": (ctypes.c_char_p, [c_int]),
+    "PfSolveGetVersion": (c_int, []),
+    "PfSolveAppLibraryCreate": (ctypes.c_void_p, []),
+    "PfSolveAppLibraryDestroy": (None, [ctypes.c_void_p]),
+    "checkLibrary_JonesWorland": (c_int, [ctypes.c_void_p, MapKeyJW, ctypes.POINTER(_APP_P)]),
+    "addToLibrary_JonesWorland": (c_int, [ctypes.c_void_p, MapKeyJW, _APP_P]),
+    "checkLibrary_dgbmv": (c_int, [ctypes.c_void_p, MapKeyDgbmv, ctypes.POINTER(_APP_P)]),
+    "addToLibrary_dgbmv": (c_int, [ctypes.c_void_p, MapKeyDgbmv, _APP_P]),
+    "checkLibrary_block": (c_int, [ctypes.c_void_p, MapKeyBlock, ctypes.POINTER(_APP_P)]),
+    "addToLibrary_block": (c_int, [ctypes.c_void_p, MapKeyBlock, _APP_P]),
+    "PfSolveAppendChain": (c_int, [ctypes.POINTER(_APP_P), ctypes.POINTER(_LP_P), c_int, c_int]),
+    "PfSolveLaunchCount": (u64, []),
+}
+
+_lib = None
+
+
+def load():
+    """Load the in-tree library; raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C pfsolve_b200` "
+                           "(or __graft_entry__.build()); there is no fallback implementation")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+class PfSolveError(RuntimeError):
+    def __init__(self, code, what=""):
+        s = load().getPfSolveErrorString(code).decode()
+        super().__init__(f"{what}: {s} ({code})")
+        self.code = code
+
+
+def check(code, what=""):
+    if code != PFSOLVE_SUCCESS:
+        raise PfSolveError(code, what)

@@ -1,0 +1,674 @@
+// api.cpp -- the C ABI of include/pfsolve_b200.h: plan creation, launch, apps
+// library and fused chains.  Host logic mirrors PfSolve's plan/application
+// layer for the JW path (PfSolve/pfSolve_AppManagement/*,
+// PfSolve/pfSolve_PlanManagement/pfSolve_Plans/pfSolve_Plan_JonesWorland.h)
+// without runtime code generation: every kernel variant is precompiled.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <tuple>
+
+#include "../../include/pfsolve_b200.h"
+#include "jw_variants.h"
+
+using namespace pfb;
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+
+enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3 };
+
+constexpr int64_t kMaxRows = 4096;  // single-upload limit of this build (<= 8 warps x 32 x 16 rows)
+
+struct AppState {
+    AppKind kind;
+    int num_sms = 0;
+    int device = 0;
+    // JW / dgbmv plan
+    int R = 0, W = 1, G = 1;
+    int mvj = MVJ_NONE, sv = SV_NONE, KL = 0, KU = 0;
+    const JwVariant* variant = nullptr;
+    int max_blocks = 0;  // resident CTAs over the whole GPU
+    // reference band permutation parameters (reorder_i0 inputs)
+    int64_t perm_r = 1, perm_m = 0, perm_ceil = 0, perm_floor = 0;
+    // streams
+    uint64_t stream_counter = 0;
+    cudaEvent_t* events = nullptr;
+};
+
+AppState* st(PfSolveApplication* app) { return static_cast<AppState*>(app->internal); }
+
+// Rows per lane of the reference's register-major band order
+// (pfSolve_Plan_JonesWorland.h:311-346 and reorder_i0, :66-142).
+void reference_band_order(int64_t M, int64_t& r, int64_t& m, int64_t& ceil_n, int64_t& floor_n)
+{
+    int64_t warp = 64 * ((M + 1023) / 1024);
+    if (M < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    r = (M + warp - 1) / warp;
+    if (r < 1) r = 1;
+    m = M % r;
+    ceil_n = (M + r - 1) / r;
+    floor_n = M / r;
+}
+
+// Keep-window of PfConfigureZeropad (pfSolve_KernelsLevel0/pfSolve_Zeropad.h:306-377)
+// as a half-open row range.  Launch-time windows keep [z0, z1); plan-time
+// windows treat 0 as "unbounded".
+void keep_window(bool runtime, int64_t z0, int64_t z1, int64_t& lo, int64_t& hi)
+{
+    const int64_t BIG = INT64_MAX / 4;
+    if (runtime) { lo = z0; hi = z1; return; }
+    lo = z0 ? z0 : 0;
+    hi = z1 ? z1 : BIG;
+}
+
+int pick_rows_per_thread(int64_t M, int requested)
+{
+    if (requested == 2 || requested == 4 || requested == 8 || requested == 16) return requested;
+    if (M <= 64) return 2;
+    if (M <= 128) return 4;
+    if (M <= 2048) return 8;
+    return 16;
+}
+
+PfSolveResult configure_launch_shape(AppState* s, int64_t M)
+{
+    // W warps per system: enough for M rows at R rows per thread, at most 8.
+    int R = s->R;
+    int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+    while (W > 8 && R < 16) {
+        R *= 2;
+        W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+    }
+    if (W > 8) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+    if (W < 1) W = 1;
+    s->R = R;
+    s->W = (int)W;
+    s->G = std::max(1, 8 / s->W);  // 256-thread CTAs
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    PfSolveResult r = configure_launch_shape(s, M);
+    if (r != PFSOLVE_SUCCESS) return r;
+    const JwVariant* v = find_jw_variant(s->R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+    if (!v) {
+        for (int R : {8, 4, 16, 2}) {
+            if (R == s->R) continue;
+            const JwVariant* c = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+            if (!c) continue;
+            AppState t = *s;
+            t.R = R;
+            if (configure_launch_shape(&t, M) != PFSOLVE_SUCCESS) continue;
+            if (t.R != R) continue;
+            *s = t;
+            v = c;
+            break;
+        }
+    }
+    if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    s->variant = v;
+    const size_t smem = v->smem_bytes(s->W, s->G);
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    }
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * s->W * s->G, smem) != cudaSuccess ||
+        blocks < 1)
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    s->max_blocks = blocks * s->num_sms;
+    return PFSOLVE_SUCCESS;
+}
+
+// JW operator kinds for K = 1 (pfSolve_JonesWorland.h:117-353): which matvec,
+// which solve, and where the bands sit.  Returns false for combinations the
+// reference leaves undefined (upperBanded 2 with jw_type % 10 in {0, 1}).
+struct JwLayout {
+    int mvj, sv;
+    int64_t off_md, off_mo, off_sl, off_su;
+};
+
+bool jw_layout(const PfSolveConfiguration& c, bool rtM, bool rtV, int64_t oM, int64_t oV, JwLayout& L)
+{
+    const int64_t M = c.M_size;
+    const int jwt = c.jw_type % 10;
+    L = JwLayout{MVJ_NONE, SV_NONE, 0, 0, 0, 0};
+    if (c.upperBanded == 2) {
+        L.off_md = M; L.off_sl = 0; L.off_su = 2 * M;
+        if (jwt == 3) { L.mvj = MVJ_DIAG; L.sv = SV_TRI; return true; }
+        if (jwt == 2) { L.mvj = MVJ_NONE; L.sv = SV_TRI; return true; }
+        return false;
+    }
+    if (jwt == 2) L.mvj = MVJ_NONE;
+    else if (jwt == 3) {
+        L.mvj = MVJ_DIAG;  // offsets chosen with upperBanded flipped (:133-136, :203-206)
+        L.off_md = (c.upperBanded == 1) ? (rtM ? oM : M) : (rtM ? oM + M : 0);
+    } else if (c.upperBanded == 1) {
+        L.mvj = MVJ_UPPER;
+        L.off_md = rtM ? oM + M : 0;
+        L.off_mo = rtM ? oM : M;
+    } else {
+        L.mvj = MVJ_LOWER;
+        L.off_md = rtM ? oM : M;
+        L.off_mo = rtM ? oM + M : 0;
+    }
+    if (jwt == 1) L.sv = SV_NONE;
+    else if (c.upperBanded == 1) { L.sv = SV_LOWER; L.off_sl = rtV ? oV : 2 * M; }
+    else { L.sv = SV_UPPER; L.off_su = rtV ? oV : 2 * M; }
+    return true;
+}
+
+cudaStream_t pick_stream(PfSolveApplication* app)
+{
+    PfSolveConfiguration& c = app->configuration;
+    AppState* s = st(app);
+    if (!c.stream || c.num_streams == 0) return nullptr;
+    if (c.num_streams == 1) return c.stream[0];
+    const uint64_t id = s->stream_counter % c.num_streams;
+    s->stream_counter++;
+    return c.stream[id];
+}
+
+void record_stream_event(PfSolveApplication* app, cudaStream_t stream)
+{
+    PfSolveConfiguration& c = app->configuration;
+    AppState* s = st(app);
+    if (c.num_streams > 1 && s->events) {
+        const uint64_t id = (s->stream_counter + c.num_streams - 1) % c.num_streams;
+        cudaEventRecord(s->events[id], stream);
+    }
+}
+
+struct Resolved {
+    void* bands;
+    void* rhs;
+    int64_t offM, offV, offS, iS, oS;
+    int64_t iz0, iz1, oz0, oz1;
+    double scaleC;
+    int64_t batch;
+};
+
+PfSolveResult resolve(PfSolveApplication* app, const PfSolveLaunchParams* lp, Resolved& r)
+{
+    PfSolveConfiguration& c = app->configuration;
+    const int64_t bm = c.jw_control_bitmask;
+    if (lp && lp->batchSize > 0) c.size[1] = lp->batchSize;  // persists, as in the reference
+    r.bands = (lp && lp->buffer) ? lp->buffer[0] : (c.buffer ? c.buffer[0] : nullptr);
+    r.rhs = (lp && lp->outputBuffer) ? lp->outputBuffer[0] : (c.outputBuffer ? c.outputBuffer[0] : nullptr);
+    if (!r.rhs) return PFSOLVE_ERROR_EMPTY_outputBuffer;
+    auto pick = [&](int64_t bit, int64_t cfgv, uint64_t runv) -> int64_t {
+        return (bm & bit) ? (lp ? (int64_t)runv : 0) : cfgv;
+    };
+    r.offM = pick(RUNTIME_OFFSETM, c.offsetM, lp ? lp->offsetM : 0);
+    r.offV = pick(RUNTIME_OFFSETV, c.offsetV, lp ? lp->offsetV : 0);
+    r.offS = pick(RUNTIME_OFFSETSOLUTION, c.offsetSolution, lp ? lp->offsetSolution : 0);
+    r.iS = pick(RUNTIME_INPUTBUFFERSTRIDE, (int64_t)c.inputBufferStride[0], lp ? lp->inputBufferStride : 0);
+    r.oS = pick(RUNTIME_OUTPUTBUFFERSTRIDE, (int64_t)c.outputBufferStride[0], lp ? lp->outputBufferStride : 0);
+    const bool rtIZ = (bm & RUNTIME_INPUTZEROPAD) != 0, rtOZ = (bm & RUNTIME_OUTPUTZEROPAD) != 0;
+    keep_window(rtIZ, rtIZ ? (lp ? (int64_t)lp->inputZeropad[0] : 0) : c.inputZeropad[0],
+                rtIZ ? (lp ? (int64_t)lp->inputZeropad[1] : 0) : c.inputZeropad[1], r.iz0, r.iz1);
+    keep_window(rtOZ, rtOZ ? (lp ? (int64_t)lp->outputZeropad[0] : 0) : c.outputZeropad[0],
+                rtOZ ? (lp ? (int64_t)lp->outputZeropad[1] : 0) : c.outputZeropad[1], r.oz0, r.oz1);
+    r.scaleC = (bm & RUNTIME_SCALEC) ? (lp ? (double)lp->scaleC : 0.0) : c.scaleC;
+    r.batch = (int64_t)c.size[1] * (int64_t)(c.size[2] ? c.size[2] : 1);
+    return PFSOLVE_SUCCESS;
+}
+
+void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator& op)
+{
+    memset(&op, 0, sizeof(op));
+    op.M = c.M_size;
+    op.perm = 1;
+    op.perm_r = s->perm_r;
+    op.perm_m = s->perm_m;
+    op.perm_ceil = s->perm_ceil;
+    op.perm_floor = s->perm_floor;
+    op.scaleC = 1.0;
+}
+
+PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
+{
+    if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    const int64_t want = (io.nsys + s->G - 1) / s->G;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->max_blocks));
+    const size_t smem = s->variant->smem_bytes(s->W, s->G);
+    s->variant->launch(dim3((unsigned)grid), dim3(32 * s->W * s->G), smem, stream, op, io, s->W);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult append_jw(PfSolveApplication* app, const PfSolveLaunchParams* lp, cudaStream_t stream)
+{
+    AppState* s = st(app);
+    const PfSolveConfiguration& c = app->configuration;
+    Resolved r;
+    PfSolveResult res = resolve(app, lp, r);
+    if (res != PFSOLVE_SUCCESS) return res;
+    if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
+    JwLayout L;
+    jw_layout(c, (c.jw_control_bitmask & RUNTIME_OFFSETM) != 0, (c.jw_control_bitmask & RUNTIME_OFFSETV) != 0,
+              r.offM, r.offV, L);
+    JwOperator op;
+    fill_operator_common(s, c, op);
+    op.bands = static_cast<const double*>(r.bands);
+    op.off_md = L.off_md;
+    op.off_mo = L.off_mo;
+    op.off_sl = L.off_sl;
+    op.off_su = L.off_su;
+    op.mvj = L.mvj;
+    op.scaleC = r.scaleC;
+    JwIO io;
+    memset(&io, 0, sizeof(io));
+    io.in = static_cast<const double*>(r.rhs);
+    io.out = static_cast<double*>(r.rhs);
+    io.in_off = io.out_off = r.offS;
+    io.in_stride = io.out_stride = r.oS;  // the JW kernel addresses rows with outputBufferStride
+    io.iz0 = r.iz0; io.iz1 = r.iz1; io.oz0 = r.oz0; io.oz1 = r.oz1;
+    io.nsys = r.batch;
+    io.M = c.M_size;
+    return launch_jw_variant(s, op, io, stream);
+}
+
+PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* lp, cudaStream_t stream)
+{
+    AppState* s = st(app);
+    const PfSolveConfiguration& c = app->configuration;
+    Resolved r;
+    PfSolveResult res = resolve(app, lp, r);
+    if (res != PFSOLVE_SUCCESS) return res;
+    if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
+    if (s->variant) {
+        JwOperator op;
+        fill_operator_common(s, c, op);
+        op.bands = static_cast<const double*>(r.bands);  // unused by MVJ_NONE
+        op.mvj = MVJ_NONE;
+        op.dgbmv = static_cast<const double*>(r.bands);
+        op.dg_off = r.offM;
+        op.dg_lda = c.LDA;
+        op.dg_ku = c.KU;
+        JwIO io;
+        memset(&io, 0, sizeof(io));
+        io.in = static_cast<const double*>(r.rhs);
+        io.out = static_cast<double*>(r.rhs);
+        io.in_off = io.out_off = r.offS;
+        io.in_stride = io.out_stride = r.oS;
+        io.iz0 = r.iz0; io.iz1 = r.iz1; io.oz0 = r.oz0; io.oz1 = r.oz1;
+        io.nsys = r.batch;
+        io.M = c.M_size;
+        return launch_jw_variant(s, op, io, stream);
+    }
+    DgbmvArgs a;
+    a.A = static_cast<const double*>(r.bands);
+    a.x = static_cast<double*>(r.rhs);
+    a.M = c.M_size;
+    a.nsys = r.batch;
+    a.off_A = r.offM;
+    a.off_x = r.offS;
+    a.stride = r.oS;
+    a.lda = c.LDA;
+    a.ku = c.KU;
+    a.iz0 = r.iz0; a.iz1 = r.iz1; a.oz0 = r.oz0; a.oz1 = r.oz1;
+    launch_dgbmv_generic(a, stream, s->num_sms);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL; }
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult append_block(PfSolveApplication* app, const PfSolveLaunchParams* lp, cudaStream_t stream)
+{
+    AppState* s = st(app);
+    const PfSolveConfiguration& c = app->configuration;
+    Resolved r;
+    PfSolveResult res = resolve(app, lp, r);
+    if (res != PFSOLVE_SUCCESS) return res;
+    if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
+    BlockArgs a;
+    a.in = static_cast<const double*>(r.bands);
+    a.out = static_cast<double*>(r.rhs);
+    a.size0 = (int64_t)c.size[0];
+    a.size1 = r.batch;
+    a.in_off = r.offM;
+    a.in_stride = r.iS;
+    a.out_off = r.offS;
+    a.out_stride = r.oS;
+    a.iz0 = r.iz0; a.iz1 = r.iz1; a.oz0 = r.oz0; a.oz1 = r.oz1;
+    a.layout = c.block % 10;
+    a.accumulate = ((c.block / 10) % 10) == 2;
+    a.scale_kind = c.block / 100;
+    a.lshift = c.lshift;
+    a.s = r.scaleC;
+    a.skip_read = (a.scale_kind == 1) && !(c.jw_control_bitmask & RUNTIME_SCALEC) && c.scaleC == 0.0;
+    launch_block(a, stream, s->num_sms);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL; }
+    return PFSOLVE_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* getPfSolveErrorString(PfSolveResult result)
+{
+    switch (result) {
+    case PFSOLVE_SUCCESS: return "PFSOLVE_SUCCESS";
+    case PFSOLVE_ERROR_MALLOC_FAILED: return "PFSOLVE_ERROR_MALLOC_FAILED";
+    case PFSOLVE_ERROR_PLAN_NOT_INITIALIZED: return "PFSOLVE_ERROR_PLAN_NOT_INITIALIZED";
+    case PFSOLVE_ERROR_INVALID_DEVICE: return "PFSOLVE_ERROR_INVALID_DEVICE";
+    case PFSOLVE_ERROR_EMPTY_FFTdim: return "PFSOLVE_ERROR_EMPTY_FFTdim";
+    case PFSOLVE_ERROR_EMPTY_size: return "PFSOLVE_ERROR_EMPTY_size";
+    case PFSOLVE_ERROR_EMPTY_buffer: return "PFSOLVE_ERROR_EMPTY_buffer";
+    case PFSOLVE_ERROR_EMPTY_outputBuffer: return "PFSOLVE_ERROR_EMPTY_outputBuffer";
+    case PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH: return "PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH";
+    case PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE: return "PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE";
+    case PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL: return "PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL";
+    case PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE: return "PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE";
+    case PFSOLVE_ERROR_UNSUPPORTED_COMBINATION: return "PFSOLVE_ERROR_UNSUPPORTED_COMBINATION";
+    case PFSOLVE_ERROR_INVALID_ARGUMENT: return "PFSOLVE_ERROR_INVALID_ARGUMENT";
+    case PFSOLVE_ERROR_CAPACITY: return "PFSOLVE_ERROR_CAPACITY";
+    case PFSOLVE_ERROR_DEVICE_FAULT: return "PFSOLVE_ERROR_DEVICE_FAULT";
+    default: return "PFSOLVE_ERROR_UNKNOWN";
+    }
+}
+
+int PfSolveGetVersion(void) { return 102; }
+
+uint64_t PfSolveLaunchCount(void) { return g_launches.load(); }
+
+PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cfg)
+{
+    if (!app) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    memset(app, 0, sizeof(*app));
+    app->configuration = cfg;
+    PfSolveConfiguration& c = app->configuration;
+    if (c.FFTdim != 1) return PFSOLVE_ERROR_EMPTY_FFTdim;
+    if (!c.device) return PFSOLVE_ERROR_INVALID_DEVICE;
+    if (c.size[0] == 0) return PFSOLVE_ERROR_EMPTY_size;
+    if (c.size[1] == 0) c.size[1] = 1;
+    if (c.size[2] == 0) c.size[2] = 1;
+    if (c.M_size == 0) c.M_size = (int64_t)c.size[0];
+    if (c.inputBufferStride[0] == 0) c.inputBufferStride[0] = c.size[0];
+    if (c.outputBufferStride[0] == 0) c.outputBufferStride[0] = c.size[0];
+    if (c.halfPrecision || c.ALT_dgbmv) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+
+    AppState* s = new (std::nothrow) AppState();
+    if (!s) return PFSOLVE_ERROR_MALLOC_FAILED;
+    app->internal = s;
+    s->device = *c.device;
+    if (cudaSetDevice(s->device) != cudaSuccess) { deletePfSolve(app); return PFSOLVE_ERROR_INVALID_DEVICE; }
+    if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess) {
+        deletePfSolve(app);
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    }
+    if (c.num_streams > 1) {
+        if (!c.stream) { deletePfSolve(app); return PFSOLVE_ERROR_INVALID_ARGUMENT; }
+        s->events = new (std::nothrow) cudaEvent_t[c.num_streams];
+        if (!s->events) { deletePfSolve(app); return PFSOLVE_ERROR_MALLOC_FAILED; }
+        for (uint64_t i = 0; i < c.num_streams; i++) {
+            if (cudaEventCreateWithFlags(&s->events[i], cudaEventDisableTiming) != cudaSuccess) {
+                deletePfSolve(app);
+                return PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD;
+            }
+        }
+    }
+    // Precision: this build runs the FP64 path; other storage modes are
+    // rejected until their kernels are selected here.
+    const bool fp64 = c.doublePrecision && !c.quadDoubleDoublePrecision && !c.quadDoubleDoublePrecisionDoubleMemory &&
+                      !c.doublePrecisionFloatMemory;
+    PfSolveResult r = PFSOLVE_SUCCESS;
+    if (c.jw_type >= 10) {
+        s->kind = APP_JW;
+        if (!fp64 || c.mixedPrecisionRefinement) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.numConsecutiveJWIterations > 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (((c.jw_type / 100) % 10) == 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // ALT mode
+        else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.M_size > kMaxRows || c.M_size < 1) r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+        else {
+            JwLayout L;
+            if (!jw_layout(c, false, false, 0, 0, L)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            else {
+                s->mvj = L.mvj;
+                s->sv = L.sv;
+                s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
+                s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
+                s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
+                reference_band_order(c.M_size, s->perm_r, s->perm_m, s->perm_ceil, s->perm_floor);
+                r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
+            }
+        }
+    } else if (c.LDA > 0) {
+        s->kind = APP_DGBMV;
+        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.KU < 0 || c.KU >= c.LDA) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
+        else {
+            const int kl = c.LDA - 1 - c.KU;
+            if (kl <= 2 && c.KU <= 2 && c.M_size <= kMaxRows) {
+                s->KL = kl;
+                s->KU = c.KU;
+                s->sv = SV_NONE;
+                s->mvj = MVJ_NONE;
+                s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
+                if (s->R < 4) s->R = 4;
+                r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
+            }
+            // wider bands use the generic kernel (variant stays null)
+        }
+    } else if (c.block > 0) {
+        s->kind = APP_BLOCK;
+        const int bt = c.block % 10, acc = (c.block / 10) % 10, sk = c.block / 100;
+        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (bt < 1 || bt > 7 || (acc != 0 && acc != 2) || sk > 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (acc == 2 && bt == 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    } else {
+        r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    }
+    if (r != PFSOLVE_SUCCESS) {
+        deletePfSolve(app);
+        return r;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveAppend(PfSolveApplication* app, int inverse, PfSolveLaunchParams* launchParams)
+{
+    (void)inverse;
+    if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    AppState* s = st(app);
+    cudaStream_t stream = pick_stream(app);
+    PfSolveResult r;
+    switch (s->kind) {
+    case APP_JW: r = append_jw(app, launchParams, stream); break;
+    case APP_DGBMV: r = append_dgbmv(app, launchParams, stream); break;
+    case APP_BLOCK: r = append_block(app, launchParams, stream); break;
+    default: r = PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    }
+    if (r == PFSOLVE_SUCCESS) record_stream_event(app, stream);
+    return r;
+}
+
+PfSolveResult PfSolveSync(PfSolveApplication* app)
+{
+    if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    AppState* s = st(app);
+    const PfSolveConfiguration& c = app->configuration;
+    if (c.num_streams > 1 && s->events) {
+        for (uint64_t i = 0; i < c.num_streams; i++)
+            if (cudaEventSynchronize(s->events[i]) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE;
+        s->stream_counter = 0;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
+void deletePfSolve(PfSolveApplication* app)
+{
+    if (!app) return;
+    AppState* s = st(app);
+    if (s) {
+        if (s->events) {
+            for (uint64_t i = 0; i < app->configuration.num_streams; i++)
+                if (s->events[i]) cudaEventDestroy(s->events[i]);
+            delete[] s->events;
+        }
+        delete s;
+    }
+    app->internal = nullptr;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Fused chains: [dgbmv] -> JW -> [block] over the same systems, one kernel.
+namespace {
+
+bool trivial_window(int64_t lo, int64_t hi, int64_t M) { return lo <= 0 && hi >= M; }
+
+PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchParams* dlp, PfSolveApplication* jw,
+                                 const PfSolveLaunchParams* jlp, PfSolveApplication* bl,
+                                 const PfSolveLaunchParams* blp, cudaStream_t stream)
+{
+    AppState* sj = st(jw);
+    const PfSolveConfiguration& cj = jw->configuration;
+    const int64_t M = cj.M_size;
+    Resolved rj;
+    PfSolveResult res = resolve(jw, jlp, rj);
+    if (res != PFSOLVE_SUCCESS) return res;
+    if (!rj.bands) return PFSOLVE_ERROR_EMPTY_buffer;
+    JwLayout L;
+    jw_layout(cj, (cj.jw_control_bitmask & RUNTIME_OFFSETM) != 0, (cj.jw_control_bitmask & RUNTIME_OFFSETV) != 0,
+              rj.offM, rj.offV, L);
+    int KL = (L.mvj == MVJ_LOWER) ? 1 : 0, KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
+    JwOperator op;
+    fill_operator_common(sj, cj, op);
+    op.bands = static_cast<const double*>(rj.bands);
+    op.off_md = L.off_md; op.off_mo = L.off_mo; op.off_sl = L.off_sl; op.off_su = L.off_su;
+    op.mvj = L.mvj;
+    op.scaleC = rj.scaleC;
+    JwIO io;
+    memset(&io, 0, sizeof(io));
+    io.M = M;
+    io.in = static_cast<const double*>(rj.rhs);
+    io.in_off = rj.offS;
+    io.in_stride = rj.oS;
+    io.iz0 = rj.iz0; io.iz1 = rj.iz1;
+    io.oz0 = rj.oz0; io.oz1 = rj.oz1;
+    io.out = static_cast<double*>(rj.rhs);
+    io.out_off = rj.offS;
+    io.out_stride = rj.oS;
+    io.nsys = rj.batch;
+    int LIN = LAY_REAL, LOUT = LAY_REAL, SCALE = 0;
+    if (dg) {
+        const PfSolveConfiguration& cd = dg->configuration;
+        Resolved rd;
+        if ((res = resolve(dg, dlp, rd)) != PFSOLVE_SUCCESS) return res;
+        if (cd.M_size != M || rd.rhs != rj.rhs || rd.offS != rj.offS || rd.oS != rj.oS || rd.batch != rj.batch)
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (!trivial_window(rd.oz0, rd.oz1, M) || !trivial_window(rj.iz0, rj.iz1, M))
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        const int kla = cd.LDA - 1 - cd.KU;
+        op.dgbmv = static_cast<const double*>(rd.bands);
+        op.dg_off = rd.offM;
+        op.dg_lda = cd.LDA;
+        op.dg_ku = cd.KU;
+        KL += kla;
+        KU += cd.KU;
+        io.iz0 = rd.iz0;  // the chain reads b through the dgbmv's input window
+        io.iz1 = rd.iz1;
+    }
+    if (bl) {
+        const PfSolveConfiguration& cb = bl->configuration;
+        Resolved rb;
+        if ((res = resolve(bl, blp, rb)) != PFSOLVE_SUCCESS) return res;
+        const int bt = cb.block % 10, sk = cb.block / 100;
+        if ((int64_t)cb.size[0] != M || rb.bands != rj.rhs) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (!trivial_window(rj.oz0, rj.oz1, M) || !trivial_window(rb.iz0, rb.iz1, M))
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (sk == 1 && !(cb.jw_control_bitmask & RUNTIME_SCALEC) && cb.scaleC == 0.0)
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (bt == 1) {
+            if (rb.offM != rj.offS || rb.iS != rj.oS || rb.batch != rj.batch) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            LOUT = LAY_REAL;
+        } else if (bt == 7) {
+            // XXII pairs (real rows 2y, 2y+1 of the JW batch) -> packed complex y
+            if (2 * rb.offM != rj.offS || rb.iS != rj.oS || 2 * rb.batch != rj.batch)
+                return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            LIN = LAY_XXII;
+            LOUT = LAY_PACKED;
+            io.in_off = rj.offS;
+            io.nsys = rb.batch;
+        } else {
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        }
+        io.out = static_cast<double*>(rb.rhs);
+        io.out_off = rb.offS;
+        io.out_stride = rb.oS;
+        io.oz0 = rb.oz0;
+        io.oz1 = rb.oz1;
+        io.accumulate = ((cb.block / 10) % 10) == 2;
+        if (sk) {
+            SCALE = 1;
+            op.scale_kind = sk;
+            op.lshift = cb.lshift;
+            op.scale_s = rb.scaleC;
+        }
+    }
+    // plan for the fused variant
+    AppState t = *sj;
+    t.KL = KL;
+    t.KU = KU;
+    t.sv = L.sv;
+    t.events = nullptr;
+    t.R = pick_rows_per_thread(M, cj.rowsPerThread);
+    if (t.R < 4) t.R = 4;
+    if (finish_variant(&t, M, LIN, LOUT, SCALE) != PFSOLVE_SUCCESS) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    return launch_jw_variant(&t, op, io, stream);
+}
+
+}  // namespace
+
+extern "C" PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveLaunchParams** lps, int n,
+                                            int allowUnfused)
+{
+    if (!apps || n < 1) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    for (int i = 0; i < n; i++)
+        if (!apps[i] || !apps[i]->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    PfSolveApplication *dg = nullptr, *jw = nullptr, *bl = nullptr;
+    const PfSolveLaunchParams *dlp = nullptr, *jlp = nullptr, *blp = nullptr;
+    bool pattern = true;
+    int i = 0;
+    if (i < n && st(apps[i])->kind == APP_DGBMV) { dg = apps[i]; dlp = lps ? lps[i] : nullptr; i++; }
+    if (i < n && st(apps[i])->kind == APP_JW) { jw = apps[i]; jlp = lps ? lps[i] : nullptr; i++; }
+    else pattern = false;
+    if (i < n && st(apps[i])->kind == APP_BLOCK) { bl = apps[i]; blp = lps ? lps[i] : nullptr; i++; }
+    if (i != n) pattern = false;
+    PfSolveResult r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (pattern && (dg || bl)) {
+        cudaStream_t stream = pick_stream(jw);
+        r = append_chain_fused(dg, dlp, jw, jlp, bl, blp, stream);
+        if (r == PFSOLVE_SUCCESS) record_stream_event(jw, stream);
+    } else if (pattern && n == 1) {
+        r = PfSolveAppend(jw, 0, lps ? lps[0] : nullptr);
+    }
+    if (r == PFSOLVE_ERROR_UNSUPPORTED_COMBINATION && allowUnfused) {
+        for (int k = 0; k < n; k++) {
+            r = PfSolveAppend(apps[k], 0, lps ? lps[k] : nullptr);
+            if (r != PFSOLVE_SUCCESS) return r;
+        }
+    }
+    return r;
+}

@@ -1,0 +1,101 @@
+// common.cuh -- device helpers shared by the JW-step kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pfb {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- value types: real systems use double, complex systems double2 (re, im
+// of one complex right-hand side share the real matrix).
+template <class V> struct VOps;
+
+template <> struct VOps<double> {
+    static __device__ __forceinline__ double zero() { return 0.0; }
+    static __device__ __forceinline__ double mul(double a, double v) { return a * v; }
+    // a*v + w
+    static __device__ __forceinline__ double fma(double a, double v, double w) { return __fma_rn(a, v, w); }
+    static __device__ __forceinline__ double add(double v, double w) { return v + w; }
+    static __device__ __forceinline__ double shfl_up(double v, int d) { return __shfl_up_sync(FULL, v, d); }
+    static __device__ __forceinline__ double shfl_down(double v, int d) { return __shfl_down_sync(FULL, v, d); }
+};
+
+template <> struct VOps<double2> {
+    static __device__ __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
+    static __device__ __forceinline__ double2 mul(double a, double2 v) { return make_double2(a * v.x, a * v.y); }
+    static __device__ __forceinline__ double2 fma(double a, double2 v, double2 w)
+    {
+        return make_double2(__fma_rn(a, v.x, w.x), __fma_rn(a, v.y, w.y));
+    }
+    static __device__ __forceinline__ double2 add(double2 v, double2 w) { return make_double2(v.x + w.x, v.y + w.y); }
+    static __device__ __forceinline__ double2 shfl_up(double2 v, int d)
+    {
+        return make_double2(__shfl_up_sync(FULL, v.x, d), __shfl_up_sync(FULL, v.y, d));
+    }
+    static __device__ __forceinline__ double2 shfl_down(double2 v, int d)
+    {
+        return make_double2(__shfl_down_sync(FULL, v.x, d), __shfl_down_sync(FULL, v.y, d));
+    }
+};
+
+template <int R> struct Log2 { static constexpr int v = (R <= 1) ? 0 : 1 + Log2<R / 2>::v; };
+template <> struct Log2<1> { static constexpr int v = 0; };
+
+// ---- Shared-memory swizzle for a warp segment of 32*R rows.
+// Lanes write the segment coalesced (row q = 32k + lane) and read it blocked
+// (lane t reads rows R*t .. R*t+R-1).  XORing the low bits of the element
+// index with the chunk index keeps both patterns free of bank conflicts:
+// 8-byte elements are served 16 lanes per wavefront (16 bank pairs), 16-byte
+// elements 8 lanes per wavefront (8 bank quads).
+template <int R, bool CPLX>
+__device__ __forceinline__ int swz(int e)
+{
+    if constexpr (R == 1) {
+        return e;
+    } else {
+        constexpr int L2 = Log2<R>::v;
+        constexpr int MASK = CPLX ? 7 : 15;
+        return e ^ ((e >> L2) & MASK);
+    }
+}
+
+// ---- cp.async (global -> shared, bypassing registers); bytes beyond
+// src_size are zero-filled, which implements out-of-range and zeropad rows.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid)
+{
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int src = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid)
+{
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int src = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ---- Named barrier over the `nthreads` threads of one system group.
+__device__ __forceinline__ void group_bar(int id, int nthreads)
+{
+    asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// ---- Exact power-of-two renormalisation of a 2x2 matrix (keeps continuant
+// products in range without rounding).
+__device__ __forceinline__ void renorm2x2(double& a, double& b, double& c, double& d)
+{
+    double m = fmax(fmax(fabs(a), fabs(b)), fmax(fabs(c), fabs(d)));
+    if (m > 0.0 && isfinite(m)) {
+        int e = ilogb(m);
+        a = scalbn(a, -e);
+        b = scalbn(b, -e);
+        c = scalbn(c, -e);
+        d = scalbn(d, -e);
+    }
+}
+
+}  // namespace pfb

@@ -1,0 +1,40 @@
+// jw_types.h -- host/device descriptors of one fused JW step launch.
+#pragma once
+#include <cstdint>
+
+namespace pfb {
+
+enum : int { SV_NONE = 0, SV_LOWER = 1, SV_UPPER = 2, SV_TRI = 3 };
+enum : int { LAY_REAL = 0, LAY_XXII = 1, LAY_PACKED = 2 };
+enum : int { MVJ_NONE = 0, MVJ_DIAG = 1, MVJ_UPPER = 2, MVJ_LOWER = 3 };
+
+// The matrix side of a JW step: where the bands live and how to read them.
+struct JwOperator {
+    const double* bands;  // JW band buffer (FP64)
+    int64_t off_md, off_mo, off_sl, off_su;  // band offsets in elements (resolved on the host)
+    int mvj;                                 // JW matvec kind (MVJ_*)
+    int perm;                                // 1: bands in the reference's register-major order
+    int64_t perm_r, perm_m, perm_ceil, perm_floor;
+    const double* dgbmv;  // fused general band matrix (band-major), or nullptr
+    int64_t dg_off;
+    int dg_lda, dg_ku;
+    int scale_kind, lshift;  // fused block Scale operator (0: none)
+    double scale_s;
+    double scaleC;  // multiplies solution row 0 when a solve runs
+    int64_t M;
+};
+
+// The data side: systems, layouts, keep-windows.
+struct JwIO {
+    const double* in;
+    double* out;
+    int64_t in_off, in_stride;    // elements (see LAY_*)
+    int64_t out_off, out_stride;  // elements of the output type (double or double2)
+    int64_t iz0, iz1;             // rows read as data: [iz0, iz1); others read as 0
+    int64_t oz0, oz1;             // rows written: [oz0, oz1)
+    int64_t nsys;                 // systems (real, or complex pairs)
+    int64_t M;
+    int accumulate;               // output += result
+};
+
+}  // namespace pfb

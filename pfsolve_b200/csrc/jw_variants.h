@@ -1,0 +1,49 @@
+// jw_variants.h -- host-side table of precompiled JW-step kernel variants.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "jw_types.h"
+
+namespace pfb {
+
+using JwKernelFn = void (*)(JwOperator, JwIO, int);
+
+struct JwVariant {
+    int R, KL, KU, SV, LIN, LOUT, SCALE;
+    const void* func;                  // __global__ entry (for attributes / occupancy)
+    size_t (*smem_bytes)(int W, int G);
+    void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op, const JwIO& io, int W);
+};
+
+// Find a variant; nullptr when that combination was not compiled.
+const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE);
+// All compiled variants (for tests and the autotuner).
+const JwVariant* jw_variants(int* count);
+
+// Standalone kernels of the block and generic-bandwidth dgbmv applications.
+struct BlockArgs {
+    const double* in;
+    double* out;
+    int64_t size0, size1;
+    int64_t in_off, in_stride, out_off, out_stride;
+    int64_t iz0, iz1, oz0, oz1;
+    int layout;  // block % 10
+    int accumulate;
+    int scale_kind, lshift;
+    double s;
+    int skip_read;
+};
+void launch_block(const BlockArgs& a, cudaStream_t st, int num_sms);
+
+struct DgbmvArgs {
+    const double* A;
+    double* x;
+    int64_t M, nsys, off_A, off_x, stride;
+    int lda, ku;
+    int64_t iz0, iz1, oz0, oz1;
+};
+void launch_dgbmv_generic(const DgbmvArgs& a, cudaStream_t st, int num_sms);
+
+}  // namespace pfb

@@ -1,0 +1,126 @@
+"""Seeded synthetic inputs with the shapes and distributions of the JW-step
+workloads this library is measured on, plus the reference's band layout.
+
+Band layout: PfSolve's JW kernel reads band arrays in a register-major order
+(reorder_i0, PfSolve/pfSolve_PlanManagement/pfSolve_Plans/pfSolve_Plan_JonesWorland.h:66-142):
+row ``t*r + j`` of a band is stored at ``S_j + t`` where ``r = ceil(M/T)``
+rows per lane (``T`` = 32 lanes below 512 rows, else ``64*ceil(M/1024)``) and
+``S_j`` counts the rows held by registers ``0..j-1``.  Callers of the
+reference pre-permute bands this way (sample_0_benchmark_VkFFT_single.cpp:306-310);
+this library reads the same layout so the buffers are interchangeable.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+def reference_band_order(M: int) -> np.ndarray:
+    """perm[i] = storage position of logical row i (single upload, M <= 4352)."""
+    warp = 64 * ((M + 1023) // 1024)
+    if M < 512:
+        warp = 32
+    warp = max(warp, 32)
+    if warp % 32:
+        warp = 32 * ((warp + 31) // 32)
+    r = max(1, (M + warp - 1) // warp)
+    i = np.arange(M, dtype=np.int64)
+    t, j = i // r, i % r
+    m = M % r
+    ceil_n, floor_n = (M + r - 1) // r, M // r
+    return t + np.where(j < m, j * ceil_n, m * ceil_n + (j - m) * floor_n)
+
+
+def permute_bands(natural: np.ndarray, M: int) -> np.ndarray:
+    """Natural-order bands (band k occupies [k*M, (k+1)*M)) -> reference layout."""
+    natural = np.asarray(natural)
+    out = np.empty_like(natural)
+    perm = reference_band_order(M)
+    for k in range(natural.shape[0] // M):
+        out[k * M + perm] = natural[k * M:(k + 1) * M]
+    return out
+
+
+def tridiagonal(rng, M, dominance=None):
+    """(a, d, c): a_0 = c_{M-1} = 0.  d = |a|+|c|+U(1,2), or dominance*(|a|+|c|)."""
+    a = rng.uniform(-1.0, 1.0, M)
+    c = rng.uniform(-1.0, 1.0, M)
+    a[0] = 0.0
+    c[-1] = 0.0
+    if dominance is None:
+        d = np.abs(a) + np.abs(c) + rng.uniform(1.0, 2.0, M)
+    else:
+        d = dominance * (np.abs(a) + np.abs(c))
+        d[d == 0] = 1.0
+    return a, d, c
+
+
+def tri_bands(a, d, c):
+    """JW tridiagonal bands in natural order: ld = a/d at [0,M), md = 1/d at
+    [M,2M), ud = c/d at [2M,3M) (host normalisation of sample_0...cpp:306-310)."""
+    return np.concatenate([a / d, 1.0 / d, c / d])
+
+
+def upper_bidiag_bands(d, s):
+    """Bands of an upperBanded=0, jw_type%10=3 step solving (diag d, super s):
+    md = 1/d at [0,M), ud = s/d at [2M,3M)."""
+    M = d.shape[0]
+    s = s.copy()
+    s[-1] = 0.0
+    return np.concatenate([1.0 / d, np.zeros(M), s / d])
+
+
+def band_major(rng, M, KL, KU, low=-1.0, high=1.0):
+    """dgbmv band-major storage A[j*M + c] (j = 0..KL+KU), U(low, high)."""
+    return rng.uniform(low, high, (KL + KU + 1) * M)
+
+
+@dataclass
+class Workload:
+    name: str
+    M: int
+    nrhs: int          # right-hand sides (complex ones count once)
+    complex: bool
+    jw_bands: np.ndarray   # reference layout
+    dgbmv: np.ndarray | None
+    rhs: np.ndarray        # real rows (XXII for complex)
+    desc: dict
+
+
+def config1(seed=0, M=256, B=512) -> Workload:
+    """Plain FP64 JW step, test-1 form: 3-band V then upper-bidiagonal M
+    (diag ~U(1,2), super ~U(-0.5,0.5)), B real RHS ~U(-1,1), stride M."""
+    rng = np.random.default_rng(seed)
+    d = rng.uniform(1.0, 2.0, M)
+    s = rng.uniform(-0.5, 0.5, M)
+    A = band_major(rng, M, 1, 1)
+    rhs = rng.uniform(-1.0, 1.0, M * B)
+    return Workload("config1", M, B, False, permute_bands(upper_bidiag_bands(d, s), M), A, rhs,
+                    dict(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1))
+
+
+def config2(seed=1, M=1024, B=65536) -> Workload:
+    """Batched FP64 tridiagonal solve fused with a 5-band matvec: N=1024, B
+    complex RHS ~N(0,1) in XXII layout, written packed.  a,c ~U(-1,1),
+    d = |a|+|c|+U(1,2); band matrix ~U(-1,1)."""
+    rng = np.random.default_rng(seed)
+    a, d, c = tridiagonal(rng, M)
+    A = band_major(rng, M, 2, 2)
+    rhs = rng.standard_normal(2 * M * B)
+    return Workload("config2", M, B, True, permute_bands(tri_bands(a, d, c), M), A, rhs,
+                    dict(upperBanded=2, jw_type=13, LDA=5, KU=2, KL=2, block=7))
+
+
+def config3(seed=2, M=512, B=131072) -> Workload:
+    """Weakly dominant tridiagonal (d = 1.05(|a|+|c|)), B real RHS ~U(-1,1)."""
+    rng = np.random.default_rng(seed)
+    a, d, c = tridiagonal(rng, M, dominance=1.05)
+    rhs = rng.uniform(-1.0, 1.0, M * B)
+    return Workload("config3", M, B, False, permute_bands(tri_bands(a, d, c), M), None, rhs,
+                    dict(upperBanded=2, jw_type=13))
+
+
+def config4_sizes(lmax=511, Nmax=512):
+    ls = np.arange(lmax + 1)
+    return ls, Nmax - ls // 2, 2 * ls + 1

@@ -1,0 +1,186 @@
+"""Generate golden vectors from the reference's own GPU kernels.
+
+Runs ``oracle/_ref/pfsolve_ref`` (the unmodified PfSolve library, compiled from
+its sources by ``make -C oracle ref``) on seeded inputs and stores inputs plus
+the reference's outputs as ``tests/golden/<case>.npz``.  Needs a CUDA GPU; run
+it as ``python tests/golden/make_golden.py --out gpurun_out/golden`` and copy the
+fixtures into ``tests/golden/``.  ``--time`` also times the reference's JW
+kernel on the full-size configurations and writes ``ref_timing.json``.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import traceback
+from dataclasses import asdict
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from pfsolve_b200 import workloads as WL  # noqa: E402
+
+RT = O
+
+
+def jw_cases():
+    """(name, Case, bands, rhs, precision) for the JW application."""
+    out = []
+    for ub, jwt in [(2, 13), (1, 10), (1, 11), (1, 12), (1, 13), (0, 10), (0, 11), (0, 12), (0, 13)]:
+        for M in ([7, 33, 100, 256, 513, 1024] if (ub, jwt) in [(2, 13), (1, 10), (0, 10)] else [33, 300]):
+            rng = np.random.default_rng(7000 + 100 * ub + jwt + M)
+            if ub == 2:
+                a, d, c = WL.tridiagonal(rng, M)
+                nat = WL.tri_bands(a, d, c)
+            else:
+                nat = np.concatenate([rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)])
+            bands = WL.permute_bands(nat, M)
+            case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=jwt)
+            rhs = rng.uniform(-1, 1, case.rhs_len())
+            out.append((f"jw_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
+    # runtime values: offsets, strides, zeropads, scaleC (sample_0 form: stride N+128)
+    M = 200
+    bm = (RT.RUNTIME_OFFSETSOLUTION | RT.RUNTIME_INPUTZEROPAD | RT.RUNTIME_OUTPUTZEROPAD | RT.RUNTIME_SCALEC |
+          RT.RUNTIME_OUTPUTBUFFERSTRIDE)
+    for ub, jwt in [(2, 13), (1, 10), (0, 13)]:
+        rng = np.random.default_rng(8000 + ub)
+        nat = (WL.tri_bands(*WL.tridiagonal(rng, M)) if ub == 2 else
+               np.concatenate([rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)]))
+        case = O.Case(M=M, batch=4, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetSolution=6,
+                      run_inputZeropad=(3, 190), run_outputZeropad=(5, 180), run_scaleC=0.625,
+                      run_outputBufferStride=M + 128)
+        rhs = rng.uniform(-1, 1, case.rhs_len() + 8)
+        out.append((f"jw_runtime_ub{ub}_t{jwt}", case, WL.permute_bands(nat, M), rhs, "f64"))
+    # runtime offsetM / offsetV (band order swap)
+    for ub in (0, 1):
+        rng = np.random.default_rng(8100 + ub)
+        md, mo, sv = rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)
+        perm = WL.reference_band_order(M)
+        big = np.zeros(5 * M)
+        oM, oV = M + 3, 4 * M - 7
+        first, second = (mo, md) if ub == 1 else (md, mo)
+        big[oM + perm] = first
+        big[oM + M + perm] = second
+        big[oV + perm] = sv
+        case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=10, bitmask=RT.RUNTIME_OFFSETM | RT.RUNTIME_OFFSETV,
+                      run_offsetM=oM, run_offsetV=oV)
+        rhs = rng.uniform(-1, 1, case.rhs_len())
+        out.append((f"jw_offsetMV_ub{ub}", case, big, rhs, "f64"))
+    # plan-time values (compile-time windows, scaleC, offsetSolution)
+    rng = np.random.default_rng(8200)
+    case = O.Case(M=M, batch=3, upperBanded=2, jw_type=13, cfg_offsetSolution=4, cfg_outputBufferStride=M + 16,
+                  cfg_inputZeropad=(4, 0), cfg_outputZeropad=(0, 150), cfg_scaleC=2.0)
+    out.append(("jw_plantime", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
+                rng.uniform(-1, 1, case.rhs_len()), "f64"))
+    # double-double storage (test-0 form, quad emulation)
+    for M in (64, 256):
+        rng = np.random.default_rng(8300 + M)
+        bands = WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M)
+        case = O.Case(M=M, batch=2, upperBanded=2, jw_type=13)
+        rhs = rng.uniform(-1, 1, case.rhs_len())
+        bdd = np.stack([bands, np.zeros_like(bands)], -1).ravel()
+        rdd = np.stack([rhs, np.zeros_like(rhs)], -1).ravel()
+        out.append((f"jw_dd_M{M}", case, bdd, rdd, "dd"))
+    # FP32 (the reference's default precision)
+    rng = np.random.default_rng(8400)
+    M = 256
+    case = O.Case(M=M, batch=3, upperBanded=2, jw_type=13)
+    out.append(("jw_f32_M256", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
+                rng.uniform(-1, 1, case.rhs_len()), "f32"))
+    # the reference leaves bands unloaded for upperBanded=2, jw_type=12 (recorded to document it)
+    rng = np.random.default_rng(8500)
+    M = 64
+    case = O.Case(M=M, batch=2, upperBanded=2, jw_type=12)
+    out.append(("jw_undefined_ub2_t12", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
+                rng.uniform(-1, 1, case.rhs_len()), "f64"))
+    return out
+
+
+def dgbmv_cases():
+    out = []
+    for M, KL, KU in [(33, 1, 1), (128, 2, 2), (100, 0, 2), (64, 3, 1)]:
+        rng = np.random.default_rng(9000 + M + KL)
+        A = WL.band_major(rng, M, KL, KU)
+        case = O.Case(M=M, batch=2, LDA=KL + KU + 1, KU=KU, KL=KL, jw_type=0)
+        out.append((f"dgbmv_M{M}_kl{KL}_ku{KU}", case, A, rng.uniform(-1, 1, case.rhs_len()), "f64"))
+    return out
+
+
+def block_cases():
+    out = []
+    N, Y = 40, 3
+    for block in (1, 2, 3, 4, 5, 6, 7, 21, 27, 101, 201, 301, 401):
+        rng = np.random.default_rng(9500 + block)
+        bt = block % 10
+        nin = (2 if bt in (2, 3, 4, 7) else 1) * N * Y
+        nout = (2 if bt in (4, 5, 6, 7) else 1) * N * Y
+        case = O.Case(M=N, batch=Y, block=block, lshift=2, jw_type=0, bitmask=RT.RUNTIME_SCALEC, run_scaleC=0.5)
+        out.append((f"block_{block}", case, rng.standard_normal(nin), rng.standard_normal(nout), "f64"))
+    return out
+
+
+def run_case(tmp, name, case, buf, rhs, prec):
+    d = os.path.join(tmp, name)
+    if case.block:
+        O.write_reference_case(d, case, None, rhs, precision=prec, inp=buf)
+    else:
+        O.write_reference_case(d, case, buf, rhs, precision=prec)
+    path, _ = O.run_reference(d)
+    dt = np.float32 if prec == "f32" else np.float64
+    return np.fromfile(path, dtype=dt)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--time", action="store_true")
+    args = ap.parse_args()
+    os.makedirs(args.out, exist_ok=True)
+    tmp = os.path.join(args.out, "_cases")
+    summary = {}
+    for name, case, buf, rhs, prec in jw_cases() + dgbmv_cases() + block_cases():
+        try:
+            ref = run_case(tmp, name, case, buf, rhs, prec)
+            np.savez_compressed(os.path.join(args.out, name + ".npz"), params=json.dumps(asdict(case)),
+                                precision=prec, buffer=buf, rhs=rhs, ref_out=ref)
+            summary[name] = "ok"
+        except Exception as e:  # record and continue: one failing case must not hide the others
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
+    if args.time:
+        timing = {}
+        for label, M, B in [("config3_jw_t13_N512_B131072", 512, 131072),
+                            ("config2_jw_t13_N1024_B131072real", 1024, 131072),
+                            ("config1_jw_ub0_t13_N256_B512", 256, 512)]:
+            rng = np.random.default_rng(1)
+            ub = 0 if "ub0" in label else 2
+            nat = (WL.tri_bands(*WL.tridiagonal(rng, M)) if ub == 2 else
+                   WL.upper_bidiag_bands(rng.uniform(1, 2, M), rng.uniform(-.5, .5, M)))
+            case = O.Case(M=M, batch=B, upperBanded=ub, jw_type=13)
+            d = os.path.join(tmp, label)
+            os.makedirs(d, exist_ok=True)
+            O.write_reference_case(d, case, WL.permute_bands(nat, M), np.zeros(1), precision="f64", iters=20)
+            os.remove(os.path.join(d, "rhs.bin"))
+            with open(os.path.join(d, "params.txt"), "a") as f:
+                f.write(f"rhs_bytes={8 * M * B}\n")
+            try:
+                _, ms = O.run_reference(d, timeout=300)
+                bytes_alg = 2 * 8 * M * B
+                timing[label] = dict(ms=ms, rhs_per_s=B / (ms * 1e-3), gbs=bytes_alg / (ms * 1e-3) / 1e9)
+            except Exception as e:
+                timing[label] = dict(error=str(e))
+        with open(os.path.join(args.out, "ref_timing.json"), "w") as f:
+            json.dump(timing, f, indent=1)
+        print(json.dumps(timing, indent=1))
+    with open(os.path.join(args.out, "summary.json"), "w") as f:
+        json.dump(summary, f, indent=1)
+    bad = [k for k, v in summary.items() if v != "ok"]
+    print(f"{len(summary) - len(bad)} ok, {len(bad)} failed: {bad}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,56 @@
+"""Shared helpers: run one PfSolve application through the C ABI on the GPU and
+compare with the oracle."""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def case_fields(case: O.Case, **extra):
+    """PfSolveConfiguration fields of an oracle Case."""
+    f = dict(M_size=case.M, size=(case.size0, case.size1 if case.block else case.batch),
+             upperBanded=case.upperBanded, jw_type=case.jw_type, jw_control_bitmask=case.bitmask,
+             offsetM=case.cfg_offsetM, offsetV=case.cfg_offsetV, offsetSolution=case.cfg_offsetSolution,
+             inputZeropad=case.cfg_inputZeropad, outputZeropad=case.cfg_outputZeropad,
+             scaleC=case.cfg_scaleC, inputBufferStride=case.cfg_inputBufferStride,
+             outputBufferStride=case.cfg_outputBufferStride, LDA=case.LDA, KU=case.KU, KL=case.KL,
+             block=case.block, lshift=case.lshift, doublePrecision=1)
+    f.update(extra)
+    return f
+
+
+def launch_fields(case: O.Case):
+    return dict(offsetM=case.run_offsetM, offsetV=case.run_offsetV, offsetSolution=case.run_offsetSolution,
+                inputZeropad=case.run_inputZeropad, outputZeropad=case.run_outputZeropad,
+                scaleC=case.run_scaleC, inputBufferStride=case.run_inputBufferStride,
+                outputBufferStride=case.run_outputBufferStride)
+
+
+def run_app(case: O.Case, buffer: np.ndarray, out: np.ndarray, **extra):
+    """Initialise + append one app; returns the output buffer after the launch."""
+    import torch
+
+    from pfsolve_b200.api import App
+    tb = torch.from_numpy(np.ascontiguousarray(buffer, dtype=np.float64)).cuda()
+    to = torch.from_numpy(np.array(out, dtype=np.float64, copy=True)).cuda()
+    app = App(buffer=tb, outputBuffer=to, **case_fields(case, **extra))
+    app.append(**launch_fields(case))
+    torch.cuda.synchronize()
+    res = to.cpu().numpy()
+    app.close()
+    return res
+
+
+def rel_err(x, ref, case: O.Case):
+    return O.rel_errors(x, ref, case.M, case.batch, case.out_stride, case.offset_solution)
+
+
+def random_bands(rng, M, ub):
+    """Natural-order JW bands for the given orientation."""
+    if ub == 2:
+        a = rng.uniform(-1, 1, M)
+        c = rng.uniform(-1, 1, M)
+        a[0] = 0
+        c[-1] = 0
+        d = np.abs(a) + np.abs(c) + rng.uniform(1, 2, M)
+        return np.concatenate([a / d, 1 / d, c / d])
+    return np.concatenate([rng.uniform(1, 2, M), rng.uniform(-0.5, 0.5, M), rng.uniform(-0.5, 0.5, M)])

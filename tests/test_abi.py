@@ -1,0 +1,136 @@
+"""The C-ABI library loads, exports every entry point its header declares, and
+the ctypes mirror has the C layout (CPU only; no kernel runs)."""
+import ctypes
+import glob
+import os
+import re
+import subprocess
+
+import pytest
+
+from pfsolve_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = sorted(glob.glob(os.path.join(ROOT, "include", "*.h")))
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        text = open(h).read()
+        for m in re.finditer(r"PFSOLVE_API\s+[\w\s\*]+?\b(\w+)\s*\(", text):
+            names.append(m.group(1))
+    return names
+
+
+def test_library_builds_and_loads():
+    assert os.path.exists(capi.LIB_PATH), "run make -C pfsolve_b200"
+    lib = capi.load()
+    assert lib.PfSolveGetVersion() == 102
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 16
+    lib = ctypes.CDLL(capi.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/ but not exported"
+    assert set(names) == set(capi.SIGNATURES), "capi.SIGNATURES must cover exactly the header's functions"
+
+
+PROBE = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "pfsolve_b200.h"
+#define F(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
+int main(void) {
+  printf("cfg %zu\nlp %zu\napp %zu\nkjw %zu\nkdg %zu\nkbl %zu\n", sizeof(PfSolveConfiguration),
+         sizeof(PfSolveLaunchParams), sizeof(PfSolveApplication), sizeof(PfSolve_MapKey_JonesWorland),
+         sizeof(PfSolve_MapKey_dgbmv), sizeof(PfSolve_MapKey_block));
+  F(PfSolveConfiguration, jw_type) F(PfSolveConfiguration, jw_control_bitmask)
+  F(PfSolveConfiguration, scaleC) F(PfSolveConfiguration, doublePrecision)
+  F(PfSolveConfiguration, outputBufferStride) F(PfSolveConfiguration, numConsecutiveJWIterations)
+  F(PfSolveConfiguration, rowsPerThread)
+  F(PfSolveLaunchParams, scaleC) F(PfSolveLaunchParams, batchSize)
+  return 0;
+}
+"""
+
+
+def test_ctypes_layout_matches_c(tmp_path):
+    src = tmp_path / "probe.c"
+    src.write_text(PROBE)
+    exe = tmp_path / "probe"
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                               check=True).stdout.strip().splitlines())
+    assert int(out["cfg"]) == ctypes.sizeof(capi.PfSolveConfiguration)
+    assert int(out["lp"]) == ctypes.sizeof(capi.PfSolveLaunchParams)
+    assert int(out["app"]) == ctypes.sizeof(capi.PfSolveApplication)
+    assert int(out["kjw"]) == ctypes.sizeof(capi.MapKeyJW)
+    assert int(out["kdg"]) == ctypes.sizeof(capi.MapKeyDgbmv)
+    assert int(out["kbl"]) == ctypes.sizeof(capi.MapKeyBlock)
+    for key, val in out.items():
+        if "." in key:
+            T, f = key.split(".")
+            cls = capi.PfSolveConfiguration if T == "PfSolveConfiguration" else capi.PfSolveLaunchParams
+            assert getattr(cls, f).offset == int(val), key
+
+
+def _init(**fields):
+    lib = capi.load()
+    cfg = capi.PfSolveConfiguration()
+    dev = ctypes.c_int(0)
+    cfg.device = ctypes.pointer(dev)
+    cfg.FFTdim = 1
+    for k, v in fields.items():
+        if k == "size":
+            for i, x in enumerate(v):
+                cfg.size[i] = x
+        else:
+            setattr(cfg, k, v)
+    app = capi.PfSolveApplication()
+    return lib.initializePfSolve(ctypes.byref(app), cfg), app
+
+
+def test_validation_errors_before_device_use():
+    assert _init(FFTdim=0, size=(8, 1), jw_type=13)[0] == capi.PFSOLVE_ERROR_EMPTY_FFTdim
+    assert _init(size=(0, 1), jw_type=13)[0] == capi.PFSOLVE_ERROR_EMPTY_size
+    lib = capi.load()
+    cfg = capi.PfSolveConfiguration()
+    cfg.FFTdim = 1
+    cfg.size[0] = 8
+    app = capi.PfSolveApplication()
+    assert lib.initializePfSolve(ctypes.byref(app), cfg) == capi.PFSOLVE_ERROR_INVALID_DEVICE
+    assert lib.initializePfSolve(None, cfg) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT
+    # an uninitialised app is rejected, not dereferenced
+    assert lib.PfSolveAppend(ctypes.byref(capi.PfSolveApplication()), 0, None) == 4
+
+
+def test_error_strings():
+    lib = capi.load()
+    assert lib.getPfSolveErrorString(0) == b"PFSOLVE_SUCCESS"
+    assert lib.getPfSolveErrorString(5001) == b"PFSOLVE_ERROR_UNSUPPORTED_COMBINATION"
+
+
+def test_app_library_keys_order_and_lookup():
+    lib = capi.load()
+    L = lib.PfSolveAppLibraryCreate()
+    try:
+        k = capi.MapKeyJW()
+        k.size[0], k.size[1], k.upperBanded, k.outputBufferStride, k.type = 256, 512, 2, 256, 13
+        out = ctypes.POINTER(capi.PfSolveApplication)()
+        assert lib.checkLibrary_JonesWorland(L, k, ctypes.byref(out)) == 0
+        assert not out  # miss
+        app = capi.PfSolveApplication()
+        app.configuration.M_size = 256
+        assert lib.addToLibrary_JonesWorland(L, k, ctypes.byref(app)) == 0
+        assert lib.checkLibrary_JonesWorland(L, k, ctypes.byref(out)) == 0
+        assert out and out.contents.configuration.M_size == 256
+        k2 = capi.MapKeyJW()
+        k2.size[0], k2.size[1], k2.upperBanded, k2.outputBufferStride, k2.type = 256, 512, 2, 256, 12
+        assert lib.checkLibrary_JonesWorland(L, k2, ctypes.byref(out)) == 0
+        assert not out
+    finally:
+        lib.PfSolveAppLibraryDestroy(L)
