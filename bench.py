@@ -156,21 +156,22 @@ def gpu_arm(args, rank, world):
     from pfsolve_b200 import workloads as WL
     from pfsolve_b200.api import App, append_chain, launch_count
 
+    nc = args.ncplx
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    wl = WL.config2(seed=1 + rank, B=N_CPLX)
+    wl = WL.config2(seed=1 + rank, B=nc)
     M = wl.M
     tA = torch.from_numpy(wl.dgbmv).to(dev)
     tb = torch.from_numpy(wl.jw_bands).to(dev)
     rhs = torch.from_numpy(wl.rhs).to(dev)  # XXII, 1 GiB
-    out = torch.empty(2 * M * N_CPLX, dtype=torch.float64, device=dev)
+    out = torch.empty(2 * M * nc, dtype=torch.float64, device=dev)
     del wl
-    dg = App(device=local, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * N_CPLX), LDA=5, KU=2, KL=2,
+    dg = App(device=local, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), LDA=5, KU=2, KL=2,
              doublePrecision=1)
-    jw = App(device=local, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * N_CPLX), upperBanded=2, jw_type=13,
-             doublePrecision=1)
-    bl = App(device=local, buffer=rhs, outputBuffer=out, M_size=M, size=(M, N_CPLX), block=7, doublePrecision=1)
+    jw = App(device=local, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), upperBanded=2, jw_type=13,
+             doublePrecision=1, scaleC=1.0)
+    bl = App(device=local, buffer=rhs, outputBuffer=out, M_size=M, size=(M, nc), block=7, doublePrecision=1)
     lps = [dg.launch_params(), jw.launch_params(), bl.launch_params()]
     apps = [dg, jw, bl]
 
@@ -201,15 +202,20 @@ def gpu_arm(args, rank, world):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = world * N_CPLX / (ms_max * 1e-3)
-    bytes_alg = 2.0 * M * 16 * N_CPLX + (5 + 3) * M * 8
+    value = world * nc / (ms_max * 1e-3)
+    bytes_alg = 2.0 * M * 16 * nc + (5 + 3) * M * 8
     achieved = bytes_alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
 
     # ---- e2e through the C ABI with host buffers (pinned), copies inside the timed region
-    host_in = torch.empty(2 * M * N_CPLX, dtype=torch.float64, pin_memory=True)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_case": True, "ncplx": nc, "ms_per_step": ms_max, "gbs": achieved,
+                              "gpu_launches": int(launches)}), flush=True)
+        return
+    host_in = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
     host_in.copy_(rhs.cpu())
-    host_out = torch.empty(2 * M * N_CPLX, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
     e_steps = max(2, min(args.steps, 5))
     for _ in range(2):
         rhs.copy_(host_in, non_blocking=True)
@@ -229,7 +235,7 @@ def gpu_arm(args, rank, world):
     t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * N_CPLX / (float(t.item()) * 1e-3)
+    e2e_value = world * nc / (float(t.item()) * 1e-3)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -242,13 +248,13 @@ def gpu_arm(args, rank, world):
                 "data": "synthetic (seeded, N(0,1) complex RHS, dominant tridiagonal, U(-1,1) 5-band)",
                 "config": {"workload": "config2: N=1024, 65536 complex RHS per GPU, XXII in -> packed out, "
                                        "dgbmv(5) + tridiagonal JW step (jw_type 13) fused, one kernel per step",
-                           "rhs_per_gpu": N_CPLX, "l2": "inputs 2 GiB > L2, no flush",
+                           "rhs_per_gpu": nc, "l2": "inputs 2 GiB > L2, no flush",
                            "parallelism": f"replicas x{world} (independent RHS shards, no collective)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                              "bytes_per_launch": bytes_alg},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * N_CPLX * 8,
-                        "d2h_bytes_per_step": 2 * M * N_CPLX * 8},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * nc * 8,
+                        "d2h_bytes_per_step": 2 * M * nc * 8},
                 "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
 
@@ -260,7 +266,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ncplx", type=int, default=N_CPLX, help="complex RHS per GPU (profiling cases only)")
+    ap.add_argument("--profile", action="store_true", help="kernel steps only: no e2e leg, no CPU baseline")
     args = ap.parse_args()
+    if args.profile:
+        args.no_cpu = True
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1 and args.impl == "ours":

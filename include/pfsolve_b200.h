@@ -165,8 +165,8 @@ typedef struct {
     int useMultipleInputBuffers;    /* bands of step k in buffer[k] */
 
     /* --- extensions (0 keeps the reference behaviour) --- */
-    int mixedPrecisionRefinement; /* > 0 with doublePrecision: FP32 solve + this many (<= 3)
-                                     FP64 residual refinement sweeps, FP64 storage */
+    int mixedPrecisionRefinement; /* 1..3 with doublePrecision: FP32 factor-solve plus this many
+                                     FP64 residual refinement sweeps, FP64 storage (0: plain FP64) */
     int rowsPerThread;            /* 0: autotuned; else 2, 4, 8 or 16 */
 } PfSolveConfiguration;
 

@@ -86,19 +86,30 @@ static int jw_resolve(const pfo_params* p, jw_layout* L)
     const int64_t oM = p->run_offsetM, oV = p->run_offsetV;
     memset(L, 0, sizeof(*L));
     if (p->upperBanded == 2) {
-        /* tridiagonal: ld at 0, md at M, ud at 2M (:117-131) */
+        /* tridiagonal: ld at 0, md at M, ud at 2M (:117-131).  Only jw_type%10
+         * == 3 is defined: with %10 == 2 the bands are loaded only by the
+         * matvec (:228-235, :269), so the reference's "solve" is the identity. */
         L->off_md = M; L->off_sl = 0; L->off_su = 2 * M;
         if (jwt == 3) { L->mv = PFO_MV_DIAG; L->sv = PFO_SV_TRI; return 0; }
-        if (jwt == 2) { L->mv = PFO_MV_NONE; L->sv = PFO_SV_TRI; return 0; }
         return -1;
     }
     if (jwt == 2) L->mv = PFO_MV_NONE;
     else if (jwt == 3) {
         /* jw_type%10 == 3 flips upperBanded while the matvec offsets are
-         * chosen (:133-136, :203-206); the matvec is then md-only (:241-245). */
+         * chosen (:133-136, :203-206); the matvec is then md-only (:241-245),
+         * and the solve reuses the off-diagonal band loaded with it: the solve
+         * bands are not reloaded when performTriSolve == 2 (:337-344). */
         L->mv = PFO_MV_DIAG;
-        if (p->upperBanded == 1) L->off_md = rtM ? oM : M;
-        else L->off_md = rtM ? oM + M : 0;
+        if (p->upperBanded == 1) {
+            L->off_md = rtM ? oM : M;
+            L->sv = PFO_SV_LOWER;
+            L->off_sl = rtM ? oM + M : 0;
+        } else {
+            L->off_md = rtM ? oM + M : 0;
+            L->sv = PFO_SV_UPPER;
+            L->off_su = rtM ? oM : M;
+        }
+        return 0;
     } else if (p->upperBanded == 1) {
         L->mv = PFO_MV_UPPER;
         L->off_md = rtM ? oM + M : 0;

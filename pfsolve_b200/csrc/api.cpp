@@ -35,6 +35,8 @@ struct AppState {
     // JW / dgbmv plan
     int R = 0, W = 1, G = 1;
     int mvj = MVJ_NONE, sv = SV_NONE, KL = 0, KU = 0;
+    int prec = 0;           // 0: FP64, 1: FP32 solve + FP64 refinement
+    int refine_sweeps = 1;  // FP32 solves per system in the mixed mode
     const JwVariant* variant = nullptr;
     int max_blocks = 0;  // resident CTAs over the whole GPU
     // reference band permutation parameters (reorder_i0 inputs)
@@ -102,11 +104,11 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
 {
     PfSolveResult r = configure_launch_shape(s, M);
     if (r != PFSOLVE_SUCCESS) return r;
-    const JwVariant* v = find_jw_variant(s->R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+    const JwVariant* v = find_jw_variant(s->R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
     if (!v) {
         for (int R : {8, 4, 16, 2}) {
             if (R == s->R) continue;
-            const JwVariant* c = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+            const JwVariant* c = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
             if (!c) continue;
             AppState t = *s;
             t.R = R;
@@ -146,15 +148,28 @@ bool jw_layout(const PfSolveConfiguration& c, bool rtM, bool rtV, int64_t oM, in
     const int jwt = c.jw_type % 10;
     L = JwLayout{MVJ_NONE, SV_NONE, 0, 0, 0, 0};
     if (c.upperBanded == 2) {
+        // Only jw_type%10 == 3 is defined: with %10 == 2 the reference loads
+        // the bands only for the matvec (:228-235, :269) and its solve is the identity.
         L.off_md = M; L.off_sl = 0; L.off_su = 2 * M;
         if (jwt == 3) { L.mvj = MVJ_DIAG; L.sv = SV_TRI; return true; }
-        if (jwt == 2) { L.mvj = MVJ_NONE; L.sv = SV_TRI; return true; }
         return false;
     }
     if (jwt == 2) L.mvj = MVJ_NONE;
     else if (jwt == 3) {
-        L.mvj = MVJ_DIAG;  // offsets chosen with upperBanded flipped (:133-136, :203-206)
-        L.off_md = (c.upperBanded == 1) ? (rtM ? oM : M) : (rtM ? oM + M : 0);
+        // Offsets chosen with upperBanded flipped (:133-136, :203-206); the
+        // solve reuses the off-diagonal band loaded with the matvec (no reload
+        // when performTriSolve == 2, :337-344).
+        L.mvj = MVJ_DIAG;
+        if (c.upperBanded == 1) {
+            L.off_md = rtM ? oM : M;
+            L.sv = SV_LOWER;
+            L.off_sl = rtM ? oM + M : 0;
+        } else {
+            L.off_md = rtM ? oM + M : 0;
+            L.sv = SV_UPPER;
+            L.off_su = rtM ? oM : M;
+        }
+        return true;
     } else if (c.upperBanded == 1) {
         L.mvj = MVJ_UPPER;
         L.off_md = rtM ? oM + M : 0;
@@ -236,6 +251,7 @@ void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator
     op.perm_ceil = s->perm_ceil;
     op.perm_floor = s->perm_floor;
     op.scaleC = 1.0;
+    op.refine_sweeps = s->refine_sweeps;
 }
 
 PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
@@ -434,7 +450,8 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
     PfSolveResult r = PFSOLVE_SUCCESS;
     if (c.jw_type >= 10) {
         s->kind = APP_JW;
-        if (!fp64 || c.mixedPrecisionRefinement) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
         else if (c.numConsecutiveJWIterations > 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (((c.jw_type / 100) % 10) == 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // ALT mode
         else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
@@ -445,6 +462,8 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
             else {
                 s->mvj = L.mvj;
                 s->sv = L.sv;
+                s->prec = (c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? 1 : 0;
+                s->refine_sweeps = 1 + c.mixedPrecisionRefinement;
                 s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
                 s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);

@@ -39,6 +39,42 @@ template <> struct VOps<double2> {
     }
 };
 
+template <> struct VOps<float> {
+    static __device__ __forceinline__ float zero() { return 0.0f; }
+    static __device__ __forceinline__ float mul(float a, float v) { return a * v; }
+    static __device__ __forceinline__ float fma(float a, float v, float w) { return __fmaf_rn(a, v, w); }
+    static __device__ __forceinline__ float add(float v, float w) { return v + w; }
+    static __device__ __forceinline__ float shfl_up(float v, int d) { return __shfl_up_sync(FULL, v, d); }
+    static __device__ __forceinline__ float shfl_down(float v, int d) { return __shfl_down_sync(FULL, v, d); }
+};
+
+template <> struct VOps<float2> {
+    static __device__ __forceinline__ float2 zero() { return make_float2(0.0f, 0.0f); }
+    static __device__ __forceinline__ float2 mul(float a, float2 v) { return make_float2(a * v.x, a * v.y); }
+    static __device__ __forceinline__ float2 fma(float a, float2 v, float2 w)
+    {
+        return make_float2(__fmaf_rn(a, v.x, w.x), __fmaf_rn(a, v.y, w.y));
+    }
+    static __device__ __forceinline__ float2 add(float2 v, float2 w) { return make_float2(v.x + w.x, v.y + w.y); }
+    static __device__ __forceinline__ float2 shfl_up(float2 v, int d)
+    {
+        return make_float2(__shfl_up_sync(FULL, v.x, d), __shfl_up_sync(FULL, v.y, d));
+    }
+    static __device__ __forceinline__ float2 shfl_down(float2 v, int d)
+    {
+        return make_float2(__shfl_down_sync(FULL, v.x, d), __shfl_down_sync(FULL, v.y, d));
+    }
+};
+
+// FP64 <-> FP32 value conversions (round to nearest).
+__device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v); }
+__device__ __forceinline__ float2 to_f32(double2 v) { return make_float2(__double2float_rn(v.x), __double2float_rn(v.y)); }
+__device__ __forceinline__ double to_f64(float v) { return (double)v; }
+__device__ __forceinline__ double2 to_f64(float2 v) { return make_double2((double)v.x, (double)v.y); }
+template <class V> struct Lower;
+template <> struct Lower<double> { using type = float; };
+template <> struct Lower<double2> { using type = float2; };
+
 template <int R> struct Log2 { static constexpr int v = (R <= 1) ? 0 : 1 + Log2<R / 2>::v; };
 template <> struct Log2<1> { static constexpr int v = 0; };
 

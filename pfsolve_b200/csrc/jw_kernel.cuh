@@ -31,30 +31,49 @@
 //    the zeropad keep-window and out-of-range rows for free), double-buffered
 //    per warp, into an XOR-swizzled layout that is conflict-free for both the
 //    coalesced write and the blocked (per-thread chunk) read.
+//  * PREC_MIXED: FP64 storage, the solve factors rounded to FP32 and applied
+//    in FP32; the residual r = V*A*b - M*x and the correction accumulation run
+//    in FP64 (iterative refinement, all on chip: b is never re-read).
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "jw_types.h"
 
 namespace pfb {
 
-template <int R, int KL, int KU, int SV, int LIN, int LOUT, bool SCALE>
+enum : int { PREC_F64 = 0, PREC_MIXED = 1 };
+
+template <int R, int KL, int KU, int SV, int LIN, int LOUT, bool SCALE, int PREC = PREC_F64>
 struct JwCfg {
-    static constexpr int kR = R, kKL = KL, kKU = KU, kSV = SV, kLIN = LIN, kLOUT = LOUT;
+    static constexpr int kR = R, kKL = KL, kKU = KU, kSV = SV, kLIN = LIN, kLOUT = LOUT, kPrec = PREC;
     static constexpr bool kScale = SCALE;
     static constexpr bool kCplx = (LIN != LAY_REAL);
     using V = typename std::conditional<kCplx, double2, double>::type;
+    using VF = typename Lower<V>::type;
     static constexpr int NB = KL + KU + 1;
     static constexpr int SEG = 32 * R + KL + KU;  // elements per warp buffer
     static constexpr bool kFwd = (SV == SV_LOWER || SV == SV_TRI);
     static constexpr bool kBwd = (SV == SV_UPPER || SV == SV_TRI);
+    static constexpr bool kMixed = (PREC == PREC_MIXED) && (SV != SV_NONE);
+    static constexpr int NF = kFwd ? R : 1;
+    static constexpr int NBW = kBwd ? R : 1;
 };
 
-// Shared memory per warp: two segment buffers (16-byte aligned).  The scan
-// scratch (16 doubles per warp) follows all warp buffers.
+constexpr int kScratchPerWarp = 32;  // doubles
+
+// Shared memory per warp: two segment buffers (16-byte aligned).  The scratch
+// (kScratchPerWarp doubles per warp) follows all warp buffers.
 template <class C>
 __host__ __device__ constexpr size_t jw_smem_per_warp()
 {
     return ((2 * (size_t)C::SEG * sizeof(typename C::V)) + 15) / 16 * 16;
+}
+
+template <class C>
+__host__ size_t jw_smem_bytes(int W, int G)
+{
+    return (size_t)G * W * jw_smem_per_warp<C>() + (size_t)G * W * kScratchPerWarp * sizeof(double);
 }
 
 __device__ __forceinline__ int64_t band_pos(const JwOperator& op, int64_t i)
@@ -84,35 +103,53 @@ __device__ __forceinline__ double scale_factor(int kind, int64_t x, int L, doubl
     }
 }
 
-// Per-thread coefficients of one matrix.
+// Per-thread coefficients of one matrix.  FP64 path: the solve scaling is
+// folded into w.  Mixed path: w stays unscaled (it forms g = V*A*b), the
+// solve factors live in FP32 and the unit-diagonal solve bands in FP64 for the
+// residual.
 template <class C>
 struct JwCoef {
-    double w[C::NB][C::kR];  // matvec weights, offsets -KL..KU, solve scaling folded in
-    double l[C::kFwd ? C::kR : 1];
-    double F[C::kFwd ? C::kR : 1];
-    double h[C::kBwd ? C::kR : 1];
-    double G[C::kBwd ? C::kR : 1];
+    using S = typename std::conditional<C::kMixed, float, double>::type;
+    double w[C::NB][C::kR];
+    S m[C::kMixed ? C::kR : 1];
+    S l[C::NF];
+    S F[C::NF];
+    S h[C::NBW];
+    S G[C::NBW];
+    double al[C::kMixed ? C::NF : 1];   // M's sub-diagonal (residual)
+    double cu[C::kMixed ? C::NBW : 1];  // M's super-diagonal (residual)
     double sc[C::kScale ? C::kR : 1];
 };
 
-// Scan scratch: 16 doubles per warp, [direction*8 + parity*4 + {A, -, B.x, B.y}].
-// Alternating the parity per system keeps a fast warp from overwriting an
-// aggregate a slower warp of the same group has not read yet.
+// Cross-warp scratch: kScratchPerWarp doubles per warp,
+//   [0, 8)   forward scan aggregates  (2 slots x {A, -, B.x, B.y})
+//   [8, 16)  backward scan aggregates
+//   [16, 24) neighbour exchange       (2 slots x {first.x, first.y, last.x, last.y})
+//   [24, 28) factorisation scan (2x2 matrix)
+// Every cross-warp operation bumps `seq` and uses slot seq & 1: a warp can only
+// rewrite a slot after passing the barrier of the next operation, which every
+// other warp reaches after reading the slot.
 struct GroupCtx {
-    int lane, wg, W, nthr, bar_id, par;
-    double* scratch;  // scratch of warp 0 of this group; warp w at scratch + 16*w
+    int lane, wg, W, nthr, bar_id, seq;
+    double* scratch;  // scratch of warp 0 of this group; warp w at scratch + kScratchPerWarp*w
+    __device__ __forceinline__ double* warp_area(int w) const { return scratch + kScratchPerWarp * w; }
 };
 
+template <class V>
+__device__ __forceinline__ void store_v(double* p, V v) { *reinterpret_cast<V*>(p) = v; }
+template <class V>
+__device__ __forceinline__ V load_v(const double* p) { return *reinterpret_cast<const V*>(p); }
+
 // Exclusive scan of affine maps y = B + A*x over the group, in row order
-// (forward) or reverse row order (backward).  Returns the incoming value of
-// this thread.  `in0` is the value entering the first (last) thread.
-template <class V, bool FORWARD>
-__device__ __forceinline__ V group_affine_scan(const GroupCtx& g, double A, V B)
+// (forward) or reverse row order (backward).  Returns the value entering this
+// thread's chunk; the value entering the whole system is zero.
+template <class V, class S, bool FORWARD>
+__device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
 {
     using O = VOps<V>;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        double Ap = FORWARD ? __shfl_up_sync(FULL, A, d) : __shfl_down_sync(FULL, A, d);
+        S Ap = FORWARD ? __shfl_up_sync(FULL, A, d) : __shfl_down_sync(FULL, A, d);
         V Bp = FORWARD ? O::shfl_up(B, d) : O::shfl_down(B, d);
         bool take = FORWARD ? (g.lane >= d) : (g.lane + d < 32);
         if (take) {
@@ -120,44 +157,67 @@ __device__ __forceinline__ V group_affine_scan(const GroupCtx& g, double A, V B)
             A = A * Ap;
         }
     }
-    // exclusive map of this lane within its warp
-    double Ae = FORWARD ? __shfl_up_sync(FULL, A, 1) : __shfl_down_sync(FULL, A, 1);
+    S Ae = FORWARD ? __shfl_up_sync(FULL, A, 1) : __shfl_down_sync(FULL, A, 1);
     V Be = FORWARD ? O::shfl_up(B, 1) : O::shfl_down(B, 1);
     const bool first = FORWARD ? (g.lane == 0) : (g.lane == 31);
     if (first) {
-        Ae = 1.0;
+        Ae = S(1);
         Be = O::zero();
     }
     V win = O::zero();
     if (g.W > 1) {
-        // warp aggregate = inclusive map of the warp's last (first) lane
-        const int slot = (FORWARD ? 0 : 8) + 4 * g.par;
-        double* my = g.scratch + 16 * g.wg + slot;
+        const int slot = (FORWARD ? 0 : 8) + 4 * (g.seq & 1);
         const bool agg = FORWARD ? (g.lane == 31) : (g.lane == 0);
         if (agg) {
-            my[0] = A;
-            *reinterpret_cast<V*>(my + 2) = B;
+            double* my = g.warp_area(g.wg) + slot;
+            my[0] = (double)A;
+            store_v<V>(my + 2, B);
         }
         __syncwarp();
         group_bar(g.bar_id, g.nthr);
         if (FORWARD) {
             for (int w = 0; w < g.wg; ++w) {
-                const double* o = g.scratch + 16 * w + slot;
-                win = O::fma(o[0], win, *reinterpret_cast<const V*>(o + 2));
+                const double* o = g.warp_area(w) + slot;
+                win = O::fma((S)o[0], win, load_v<V>(o + 2));
             }
         } else {
             for (int w = g.W - 1; w > g.wg; --w) {
-                const double* o = g.scratch + 16 * w + slot;
-                win = O::fma(o[0], win, *reinterpret_cast<const V*>(o + 2));
+                const double* o = g.warp_area(w) + slot;
+                win = O::fma((S)o[0], win, load_v<V>(o + 2));
             }
         }
+        g.seq++;
     }
     return O::fma(Ae, win, Be);
 }
 
+// Values of the rows around this thread's chunk: x[s-1] (prev) and x[s+R]
+// (next); zero outside the system.
+template <class V>
+__device__ __forceinline__ void group_neighbours(GroupCtx& g, V first, V last, V& prev, V& next)
+{
+    using O = VOps<V>;
+    prev = O::shfl_up(last, 1);
+    next = O::shfl_down(first, 1);
+    if (g.W > 1) {
+        const int slot = 16 + 4 * (g.seq & 1);
+        double* my = g.warp_area(g.wg) + slot;
+        if (g.lane == 0) store_v<V>(my, first);
+        if (g.lane == 31) store_v<V>(my + 2, last);
+        __syncwarp();
+        group_bar(g.bar_id, g.nthr);
+        if (g.lane == 0) prev = (g.wg > 0) ? load_v<V>(g.warp_area(g.wg - 1) + slot + 2) : O::zero();
+        if (g.lane == 31) next = (g.wg < g.W - 1) ? load_v<V>(g.warp_area(g.wg + 1) + slot) : O::zero();
+        g.seq++;
+    } else {
+        if (g.lane == 0) prev = O::zero();
+        if (g.lane == 31) next = O::zero();
+    }
+}
+
 // Exclusive scan of 2x2 matrix products P_t * ... * P_0 (row order) used by
 // the tridiagonal factorisation.  Returns the product of all preceding chunks.
-__device__ __forceinline__ void group_matrix_scan(const GroupCtx& g, double& a, double& b, double& c, double& d)
+__device__ __forceinline__ void group_matrix_scan(GroupCtx& g, double& a, double& b, double& c, double& d)
 {
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
@@ -175,18 +235,18 @@ __device__ __forceinline__ void group_matrix_scan(const GroupCtx& g, double& a, 
     if (g.lane == 0) { ea = 1; eb = 0; ec = 0; ed = 1; }
     double wa = 1, wb = 0, wc = 0, wd = 1;  // product of preceding warps
     if (g.W > 1) {
-        double* my = g.scratch + 16 * g.wg;
+        double* my = g.warp_area(g.wg) + 24;
         if (g.lane == 31) { my[0] = a; my[1] = b; my[2] = c; my[3] = d; }
         __syncwarp();
         group_bar(g.bar_id, g.nthr);
         for (int w = 0; w < g.wg; ++w) {
-            const double* o = g.scratch + 16 * w;
+            const double* o = g.warp_area(w) + 24;
             double na = o[0] * wa + o[1] * wc, nb = o[0] * wb + o[1] * wd;
             double nc = o[2] * wa + o[3] * wc, nd = o[2] * wb + o[3] * wd;
             wa = na; wb = nb; wc = nc; wd = nd;
             renorm2x2(wa, wb, wc, wd);
         }
-        group_bar(g.bar_id, g.nthr);  // scratch is reused by the next scan
+        group_bar(g.bar_id, g.nthr);
     }
     a = ea * wa + eb * wc;
     b = ea * wb + eb * wd;
@@ -196,9 +256,10 @@ __device__ __forceinline__ void group_matrix_scan(const GroupCtx& g, double& a, 
 
 // Build the per-thread coefficients for rows s .. s+R-1 of operator `op`.
 template <class C>
-__device__ __forceinline__ void jw_prologue(const JwOperator& op, const GroupCtx& g, int64_t s, JwCoef<C>& cf)
+__device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, int64_t s, JwCoef<C>& cf)
 {
     constexpr int R = C::kR, KL = C::kKL, KU = C::kKU;
+    using S = typename JwCoef<C>::S;
     const int64_t M = op.M;
     // (1) effective matvec weights of V*A for each row
 #pragma unroll
@@ -234,7 +295,10 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, const GroupCtx
             }
         }
     }
-    // (2) solve coefficients
+    // (2) solve coefficients in FP64
+    double l64[R], h64[R], m64[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) { l64[j] = 0.0; h64[j] = 0.0; m64[j] = 1.0; }
     if constexpr (C::kSV == SV_TRI) {
         // Moebius product of this chunk: v_i = [[1, -a_i c_{i-1}], [1, 0]] v_{i-1}
         double a = 1, b = 0, c = 0, d = 1;
@@ -249,7 +313,6 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, const GroupCtx
                 ac = ai * cim1;
             }
             acs[j] = ac;
-            // [[1,-ac],[1,0]] * [[a,b],[c,d]]
             const double na = a - ac * c, nb = b - ac * d;
             c = a; d = b; a = na; b = nb;
             renorm2x2(a, b, c, d);
@@ -265,38 +328,54 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, const GroupCtx
             dprev = dp;
             const double ai = (i >= 1 && i < M) ? band(op, op.off_sl, i) : 0.0;
             const double ci = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
-            cf.l[j] = ai * dinv;
-            cf.h[j] = ci * dinv;
-#pragma unroll
-            for (int k = 0; k < C::NB; ++k) cf.w[k][j] *= dinv;
+            l64[j] = ai * dinv;
+            h64[j] = ci * dinv;
+            m64[j] = dinv;
+            if constexpr (C::kMixed) {
+                cf.al[j] = ai;
+                cf.cu[j] = ci;
+            }
         }
     } else if constexpr (C::kSV == SV_LOWER) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int64_t i = s + j;
-            cf.l[j] = (i >= 1 && i < M) ? band(op, op.off_sl, i) : 0.0;
+            l64[j] = (i >= 1 && i < M) ? band(op, op.off_sl, i) : 0.0;
+            if constexpr (C::kMixed) cf.al[j] = l64[j];
         }
     } else if constexpr (C::kSV == SV_UPPER) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int64_t i = s + j;
-            cf.h[j] = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
+            h64[j] = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
+            if constexpr (C::kMixed) cf.cu[j] = h64[j];
         }
+    }
+    if constexpr (C::kMixed) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) cf.m[j] = (S)m64[j];
+    } else {
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+#pragma unroll
+            for (int k = 0; k < C::NB; ++k) cf.w[k][j] *= m64[j];
     }
     if constexpr (C::kFwd) {
         double p = 1.0;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            p = -cf.l[j] * p;
-            cf.F[j] = p;
+            p = -l64[j] * p;
+            cf.l[j] = (S)l64[j];
+            cf.F[j] = (S)p;
         }
     }
     if constexpr (C::kBwd) {
         double p = 1.0;
 #pragma unroll
         for (int j = R - 1; j >= 0; --j) {
-            p = -cf.h[j] * p;
-            cf.G[j] = p;
+            p = -h64[j] * p;
+            cf.h[j] = (S)h64[j];
+            cf.G[j] = (S)p;
         }
     }
     if constexpr (C::kScale) {
@@ -390,41 +469,86 @@ __device__ __forceinline__ void store_segment(const JwIO& io, int64_t sys, int64
     }
 }
 
-// ---- Solve one system whose chunk values are in x (after the matvec).
-template <class C>
-__device__ __forceinline__ void jw_solve_chunk(const GroupCtx& g, const JwCoef<C>& cf, typename C::V (&x)[C::kR])
+// ---- Unit-diagonal solve of one chunk given the coefficient arrays.
+// Forward: z_j = x_j - l_j z_{j-1}; backward: x_j = z_j - h_j x_{j+1};
+// chunk-boundary couplings through the affine scans (F, G are the in-chunk
+// products of -l and -h).
+template <int R, int SV, class V, class S, int NF, int NBW>
+__device__ __forceinline__ void chunk_solve(GroupCtx& g, const S (&l)[NF], const S (&F)[NF], const S (&h)[NBW],
+                                            const S (&G)[NBW], V (&x)[R])
 {
-    using V = typename C::V;
     using O = VOps<V>;
-    constexpr int R = C::kR;
-    if constexpr (C::kFwd) {
+    constexpr bool FWD = (SV == SV_LOWER || SV == SV_TRI);
+    constexpr bool BWD = (SV == SV_UPPER || SV == SV_TRI);
+    if constexpr (FWD) {
         V z[R];
         z[0] = x[0];
 #pragma unroll
-        for (int j = 1; j < R; ++j) z[j] = O::fma(-cf.l[j], z[j - 1], x[j]);
-        const V pin = group_affine_scan<V, true>(g, cf.F[R - 1], z[R - 1]);
-        if constexpr (C::kSV == SV_LOWER) {
+        for (int j = 1; j < R; ++j) z[j] = O::fma(-l[j], z[j - 1], x[j]);
+        const V pin = group_affine_scan<V, S, true>(g, F[R - 1], z[R - 1]);
+        if constexpr (SV == SV_LOWER) {
 #pragma unroll
-            for (int j = 0; j < R; ++j) x[j] = O::fma(cf.F[j], pin, z[j]);
+            for (int j = 0; j < R; ++j) x[j] = O::fma(F[j], pin, z[j]);
         } else {
-            x[R - 1] = O::fma(cf.F[R - 1], pin, z[R - 1]);
+            x[R - 1] = O::fma(F[R - 1], pin, z[R - 1]);
 #pragma unroll
-            for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-cf.h[j], x[j + 1], O::fma(cf.F[j], pin, z[j]));
+            for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-h[j], x[j + 1], O::fma(F[j], pin, z[j]));
         }
-    } else if constexpr (C::kSV == SV_UPPER) {
+    } else if constexpr (SV == SV_UPPER) {
 #pragma unroll
-        for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-cf.h[j], x[j + 1], x[j]);
+        for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-h[j], x[j + 1], x[j]);
     }
-    if constexpr (C::kBwd) {
-        const V q = group_affine_scan<V, false>(g, cf.G[0], x[0]);
+    if constexpr (BWD) {
+        const V q = group_affine_scan<V, S, false>(g, G[0], x[0]);
 #pragma unroll
-        for (int j = 0; j < R; ++j) x[j] = O::fma(cf.G[j], q, x[j]);
+        for (int j = 0; j < R; ++j) x[j] = O::fma(G[j], q, x[j]);
+    }
+}
+
+// Mixed precision: x = M^{-1} g with FP32 solves and FP64 residuals
+// (`sweeps` FP32 solves: one initial, sweeps-1 refinements).
+template <class C>
+__device__ __forceinline__ void mixed_solve(GroupCtx& g, const JwCoef<C>& cf, int sweeps, typename C::V (&x)[C::kR])
+{
+    using V = typename C::V;
+    using VF = typename C::VF;
+    using O = VOps<V>;
+    using OF = VOps<VF>;
+    constexpr int R = C::kR, SV = C::kSV;
+    V gv[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        gv[j] = x[j];
+        x[j] = O::zero();
+    }
+    for (int it = 0; it < sweeps; ++it) {
+        V r[R];
+        if (it == 0) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) r[j] = gv[j];
+        } else {
+            V prev, next;
+            group_neighbours<V>(g, x[0], x[R - 1], prev, next);
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                V mx = x[j];
+                if constexpr (C::kFwd) mx = O::fma(cf.al[j], j > 0 ? x[j - 1] : prev, mx);
+                if constexpr (C::kBwd) mx = O::fma(cf.cu[j], j < R - 1 ? x[j + 1] : next, mx);
+                r[j] = O::fma(-1.0, mx, gv[j]);
+            }
+        }
+        VF d[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) d[j] = OF::mul(cf.m[j], to_f32(r[j]));
+        chunk_solve<R, SV, VF, float, C::NF, C::NBW>(g, cf.l, cf.F, cf.h, cf.G, d);
+#pragma unroll
+        for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
     }
 }
 
 // ---- Process systems sys0, sys0+step, ... with the group's coefficients.
 template <class C>
-__device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO& io, GroupCtx g,
+__device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO& io, GroupCtx& g,
                                                const JwCoef<C>& cf, typename C::V* buf0, typename C::V* buf1,
                                                int64_t sys0, int64_t step)
 {
@@ -439,13 +563,18 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
     cp_async_commit();
     int it = 0;
     for (int64_t sys = sys0; sys < io.nsys; sys += step, ++it) {
-        g.par = it & 1;
         V* cur = (it & 1) ? buf1 : buf0;
         V* nxt = (it & 1) ? buf0 : buf1;
         if (sys + step < io.nsys) issue_segment_load<C>(io, sys + step, r0, g.lane, nxt);
         cp_async_commit();
         cp_async_wait<1>();
         __syncwarp();
+        // In place, a warp's halo rows belong to its neighbour warps: every
+        // warp of the group must hold this system's input before any warp
+        // stores results.  Solves get that ordering from their scan barriers.
+        if constexpr (C::kSV == SV_NONE && (KL + KU) > 0) {
+            if (g.W > 1) group_bar(g.bar_id, g.nthr);
+        }
         // chunk rows s-KL .. s+R+KU-1
         V be[R + KL + KU];
 #pragma unroll
@@ -465,7 +594,11 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
             for (int k = 1; k < C::NB; ++k) acc = O::fma(cf.w[k][j], be[j + k], acc);
             x[j] = acc;
         }
-        jw_solve_chunk<C>(g, cf, x);
+        if constexpr (C::kMixed) {
+            mixed_solve<C>(g, cf, op.refine_sweeps, x);
+        } else if constexpr (C::kSV != SV_NONE) {
+            chunk_solve<R, C::kSV, V, double, C::NF, C::NBW>(g, cf.l, cf.F, cf.h, cf.G, x);
+        }
         if (C::kSV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
         if constexpr (C::kScale) {
 #pragma unroll
@@ -495,11 +628,11 @@ __global__ void __launch_bounds__(256) jw_step_kernel(const JwOperator op, const
     g.W = W;
     g.nthr = 32 * W;
     g.bar_id = 1 + grp;
-    g.par = 0;
+    g.seq = 0;
     constexpr size_t per_warp = jw_smem_per_warp<C>();
     V* buf0 = reinterpret_cast<V*>(smem_raw + (size_t)warp * per_warp);
     V* buf1 = buf0 + C::SEG;
-    g.scratch = reinterpret_cast<double*>(smem_raw + (size_t)G * W * per_warp) + (size_t)grp * W * 16;
+    g.scratch = reinterpret_cast<double*>(smem_raw + (size_t)G * W * per_warp) + (size_t)grp * W * kScratchPerWarp;
 
     const int64_t s = (int64_t)(g.wg * 32 + g.lane) * C::kR;
     JwCoef<C> cf;
@@ -507,12 +640,6 @@ __global__ void __launch_bounds__(256) jw_step_kernel(const JwOperator op, const
     const int64_t sys0 = (int64_t)blockIdx.x * G + grp;
     const int64_t step = (int64_t)gridDim.x * G;
     jw_run_systems<C>(op, io, g, cf, buf0, buf1, sys0, step);
-}
-
-template <class C>
-__host__ size_t jw_smem_bytes(int W, int G)
-{
-    return (size_t)G * W * jw_smem_per_warp<C>() + (size_t)G * W * 16 * sizeof(double);
 }
 
 }  // namespace pfb

@@ -22,6 +22,7 @@ struct JwOperator {
     double scale_s;
     double scaleC;  // multiplies solution row 0 when a solve runs
     int64_t M;
+    int refine_sweeps;  // mixed precision: FP32 solves in total (1 + refinements)
 };
 
 // The data side: systems, layouts, keep-windows.

@@ -19,20 +19,24 @@ static void launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const
     jw_step_kernel<C><<<grid, block, smem, st>>>(op, io, W);
 }
 
-#define PFB_V(R, KL, KU, SV, LIN, LOUT, SC)                                                              \
-    JwVariant{R, KL, KU, SV, LIN, LOUT, SC, (const void*)&jw_step_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC>>, \
-              &smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC>>, &launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC>>}
+#define PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, P)                                                         \
+    JwVariant{R, KL, KU, SV, LIN, LOUT, SC, P,                                                           \
+              (const void*)&jw_step_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>,                     \
+              &smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>, &launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>}
+#define PFB_V(R, KL, KU, SV, LIN, LOUT, SC) PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, PREC_F64)
 
 // Rows-per-thread choices for the single-application (drop-in) variants.
 #define PFB_R4(KL, KU, SV, LIN, LOUT, SC) \
     PFB_V(2, KL, KU, SV, LIN, LOUT, SC), PFB_V(4, KL, KU, SV, LIN, LOUT, SC), PFB_V(8, KL, KU, SV, LIN, LOUT, SC), \
         PFB_V(16, KL, KU, SV, LIN, LOUT, SC)
 #define PFB_R2(KL, KU, SV, LIN, LOUT, SC) PFB_V(4, KL, KU, SV, LIN, LOUT, SC), PFB_V(8, KL, KU, SV, LIN, LOUT, SC)
+#define PFB_M2(KL, KU, SV, LIN, LOUT, SC) \
+    PFB_VP(4, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED), PFB_VP(8, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED)
 
 static const JwVariant kVariants[] = {
     // JW application, real systems in place (upperBanded 2: tridiagonal;
     // 1: upper V / lower M; 0: lower V / upper M), by jw_type % 10.
-    PFB_R4(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),    // ub 2, jwt 3 / 2
+    PFB_R4(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),    // ub 2, jwt 3
     PFB_R4(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),  // ub 1, jwt 0
     PFB_R4(0, 1, SV_NONE, LAY_REAL, LAY_REAL, false),   // ub 1, jwt 1
     PFB_R4(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),  // ub 1, jwt 2 / 3
@@ -42,8 +46,6 @@ static const JwVariant kVariants[] = {
     // dgbmv application (band matvec only), KL, KU <= 2
     PFB_R2(1, 1, SV_NONE, LAY_REAL, LAY_REAL, false),
     PFB_R2(2, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(0, 1, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(1, 0, SV_NONE, LAY_REAL, LAY_REAL, false),
     PFB_R2(0, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
     PFB_R2(2, 0, SV_NONE, LAY_REAL, LAY_REAL, false),
     PFB_R2(1, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
@@ -58,17 +60,26 @@ static const JwVariant kVariants[] = {
     PFB_R2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, true),
     // fused chains on complex XXII right-hand sides -> packed complex output
     PFB_R2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
+    PFB_R2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true),
     PFB_R2(0, 0, SV_TRI, LAY_XXII, LAY_PACKED, false),
     PFB_R2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true),
     PFB_R2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, false),
     PFB_R2(0, 0, SV_UPPER, LAY_XXII, LAY_PACKED, true),
+    // mixed precision (FP32 solve + FP64 refinement), real
+    PFB_M2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),
+    PFB_M2(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),
+    PFB_M2(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),
+    PFB_M2(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_M2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_M2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_M2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
 };
 
-const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE)
+const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)
 {
     for (const JwVariant& v : kVariants)
         if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
-            v.SCALE == (SCALE ? 1 : 0))
+            v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC)
             return &v;
     return nullptr;
 }

@@ -64,11 +64,13 @@ def tri_bands(a, d, c):
 
 def upper_bidiag_bands(d, s):
     """Bands of an upperBanded=0, jw_type%10=3 step solving (diag d, super s):
-    md = 1/d at [0,M), ud = s/d at [2M,3M)."""
+    md = 1/d at [0,M) and ud = s/d at [M,2M) -- with jw_type%10 == 3 the
+    reference's solve reuses the band loaded next to md (pfSolve_JonesWorland.h:
+    133-206, 337-344); [2M,3M) is unused."""
     M = d.shape[0]
     s = s.copy()
     s[-1] = 0.0
-    return np.concatenate([1.0 / d, np.zeros(M), s / d])
+    return np.concatenate([1.0 / d, s / d, np.zeros(M)])
 
 
 def band_major(rng, M, KL, KU, low=-1.0, high=1.0):

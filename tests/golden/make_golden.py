@@ -27,18 +27,26 @@ from pfsolve_b200 import workloads as WL  # noqa: E402
 RT = O
 
 
+def jw_bands(rng, M, ub):
+    """Natural-order bands; out-of-range couplings zero (reference convention)."""
+    if ub == 2:
+        return WL.tri_bands(*WL.tridiagonal(rng, M))
+    # each band is the solve band in some jw_type: |entries| < 1/2 keeps the
+    # unit-diagonal recurrences stable
+    bands = [rng.uniform(-.5, .5, M) for _ in range(3)]
+    for k in range(3):
+        bands[k][0] = 0.0
+        bands[k][-1] = 0.0
+    return np.concatenate(bands)
+
+
 def jw_cases():
     """(name, Case, bands, rhs, precision) for the JW application."""
     out = []
     for ub, jwt in [(2, 13), (1, 10), (1, 11), (1, 12), (1, 13), (0, 10), (0, 11), (0, 12), (0, 13)]:
         for M in ([7, 33, 100, 256, 513, 1024] if (ub, jwt) in [(2, 13), (1, 10), (0, 10)] else [33, 300]):
             rng = np.random.default_rng(7000 + 100 * ub + jwt + M)
-            if ub == 2:
-                a, d, c = WL.tridiagonal(rng, M)
-                nat = WL.tri_bands(a, d, c)
-            else:
-                nat = np.concatenate([rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)])
-            bands = WL.permute_bands(nat, M)
+            bands = WL.permute_bands(jw_bands(rng, M, ub), M)
             case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=jwt)
             rhs = rng.uniform(-1, 1, case.rhs_len())
             out.append((f"jw_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
@@ -48,8 +56,7 @@ def jw_cases():
           RT.RUNTIME_OUTPUTBUFFERSTRIDE)
     for ub, jwt in [(2, 13), (1, 10), (0, 13)]:
         rng = np.random.default_rng(8000 + ub)
-        nat = (WL.tri_bands(*WL.tridiagonal(rng, M)) if ub == 2 else
-               np.concatenate([rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)]))
+        nat = jw_bands(rng, M, ub)
         case = O.Case(M=M, batch=4, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetSolution=6,
                       run_inputZeropad=(3, 190), run_outputZeropad=(5, 180), run_scaleC=0.625,
                       run_outputBufferStride=M + 128)
@@ -58,7 +65,8 @@ def jw_cases():
     # runtime offsetM / offsetV (band order swap)
     for ub in (0, 1):
         rng = np.random.default_rng(8100 + ub)
-        md, mo, sv = rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)
+        md, mo, sv = rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)
+        mo[0] = mo[-1] = sv[0] = sv[-1] = 0.0
         perm = WL.reference_band_order(M)
         big = np.zeros(5 * M)
         oM, oV = M + 3, 4 * M - 7
@@ -91,12 +99,6 @@ def jw_cases():
     case = O.Case(M=M, batch=3, upperBanded=2, jw_type=13)
     out.append(("jw_f32_M256", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
                 rng.uniform(-1, 1, case.rhs_len()), "f32"))
-    # the reference leaves bands unloaded for upperBanded=2, jw_type=12 (recorded to document it)
-    rng = np.random.default_rng(8500)
-    M = 64
-    case = O.Case(M=M, batch=2, upperBanded=2, jw_type=12)
-    out.append(("jw_undefined_ub2_t12", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
-                rng.uniform(-1, 1, case.rhs_len()), "f64"))
     return out
 
 
@@ -123,8 +125,18 @@ def block_cases():
     return out
 
 
+REF_BIN_FP128 = os.path.join(ROOT, "oracle", "_ref", "pfsolve_ref_fp128")
+
+
 def run_case(tmp, name, case, buf, rhs, prec):
     d = os.path.join(tmp, name)
+    if prec == "dd" and os.path.exists(REF_BIN_FP128):
+        O.write_reference_case(d, case, buf, rhs, precision=prec)
+        import subprocess
+        r = subprocess.run([REF_BIN_FP128, d], capture_output=True, text=True, timeout=120)
+        if r.returncode != 0:
+            raise RuntimeError(f"pfsolve_ref_fp128 failed ({r.returncode}): {r.stderr.strip()}")
+        return np.fromfile(os.path.join(d, "out.bin"), dtype=np.float64)
     if case.block:
         O.write_reference_case(d, case, None, rhs, precision=prec, inp=buf)
     else:

@@ -45,7 +45,11 @@ def rel_err(x, ref, case: O.Case):
 
 
 def random_bands(rng, M, ub):
-    """Natural-order JW bands for the given orientation."""
+    """Natural-order JW bands for the given orientation.  Off-diagonal entries
+    that couple to rows outside the system (row 0 of a lower band, row M-1 of
+    an upper band) are zero, as in the reference's own inputs
+    (sample_0_benchmark_VkFFT_single.cpp:191-192): the reference reads an
+    unrelated register value for such a neighbour."""
     if ub == 2:
         a = rng.uniform(-1, 1, M)
         c = rng.uniform(-1, 1, M)
@@ -53,4 +57,10 @@ def random_bands(rng, M, ub):
         c[-1] = 0
         d = np.abs(a) + np.abs(c) + rng.uniform(1, 2, M)
         return np.concatenate([a / d, 1 / d, c / d])
-    return np.concatenate([rng.uniform(1, 2, M), rng.uniform(-0.5, 0.5, M), rng.uniform(-0.5, 0.5, M)])
+    # Any of the three bands is the solve band in some jw_type: |entries| < 1/2
+    # keeps every unit-diagonal recurrence stable.
+    bands = [rng.uniform(-0.5, 0.5, M) for _ in range(3)]
+    for k in range(3):
+        bands[k][0] = 0.0
+        bands[k][-1] = 0.0
+    return np.concatenate(bands)

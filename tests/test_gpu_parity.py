@@ -26,7 +26,7 @@ def jw_case(rng, M, B, ub, jwt, **kw):
     return case, bands, rhs
 
 
-@pytest.mark.parametrize("ub,jwt", [(2, 13), (2, 12), (1, 10), (1, 11), (1, 12), (1, 13),
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (1, 11), (1, 12), (1, 13),
                                     (0, 10), (0, 11), (0, 12), (0, 13)])
 @pytest.mark.parametrize("M", [1, 7, 32, 33, 100, 256, 257, 512, 1000, 1024])
 def test_jw_modes_and_sizes(ub, jwt, M):
@@ -58,7 +58,7 @@ def test_runtime_offsets_strides_zeropad_scaleC():
           capi.RUNTIME_OUTPUTZEROPAD | capi.RUNTIME_SCALEC | capi.RUNTIME_OUTPUTBUFFERSTRIDE)
     for ub, jwt in [(1, 10), (0, 10), (1, 13), (0, 13), (2, 13)]:
         nat = J.random_bands(rng, M, ub)
-        perm = WL.permute_bands(nat, M)
+        perm = WL.permute_bands(nat, M)  # md = perm[:M], mo = perm[M:2M], solve band = perm[2M:]
         # bands placed at runtime offsets: offsetM region holds the two matvec bands, offsetV the solve band
         big = np.full(8 * M, np.nan)
         oM, oV = 2 * M + 5, 6 * M + 3
@@ -66,18 +66,21 @@ def test_runtime_offsets_strides_zeropad_scaleC():
             big[:3 * M] = perm
         else:
             md, mo, sv = perm[:M], perm[M:2 * M], perm[2 * M:]
-            if jwt % 10 == 3:
+            if jwt % 10 == 3:  # the solve reuses the band loaded beside md
                 if ub == 1:
                     big[oM:oM + M] = md
+                    big[oM + M:oM + 2 * M] = sv
                 else:
                     big[oM + M:oM + 2 * M] = md
-            elif ub == 1:
-                big[oM + M:oM + 2 * M] = md
-                big[oM:oM + M] = mo
+                    big[oM:oM + M] = sv
             else:
-                big[oM:oM + M] = md
-                big[oM + M:oM + 2 * M] = mo
-            big[oV:oV + M] = sv
+                if ub == 1:
+                    big[oM + M:oM + 2 * M] = md
+                    big[oM:oM + M] = mo
+                else:
+                    big[oM:oM + M] = md
+                    big[oM + M:oM + 2 * M] = mo
+                big[oV:oV + M] = sv
         big = np.nan_to_num(big, nan=1e300)  # any stray read would blow the error up
         case = O.Case(M=M, batch=B, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetM=oM, run_offsetV=oV,
                       run_offsetSolution=17, run_inputZeropad=(3, 280), run_outputZeropad=(10, 250),
@@ -116,6 +119,7 @@ def test_unsupported_combinations_return_codes():
     b = torch.zeros(3 * 64, dtype=torch.float64, device="cuda")
     r = torch.zeros(64, dtype=torch.float64, device="cuda")
     for fields, code in [(dict(upperBanded=2, jw_type=10), capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION),
+                         (dict(upperBanded=2, jw_type=12), capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION),
                          (dict(upperBanded=2, jw_type=13, numConsecutiveJWIterations=2),
                           capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION)]:
         with pytest.raises(capi.PfSolveError) as ei:
@@ -170,8 +174,8 @@ def test_chain_dgbmv_jw_config1_form():
     tA = torch.from_numpy(wl.dgbmv).cuda()
     tb = torch.from_numpy(wl.jw_bands).cuda()
     tr = torch.from_numpy(wl.rhs.copy()).cuda()
-    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1)
-    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1)
+    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1, scaleC=1.0)
+    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1, scaleC=1.0)
     append_chain([dg, jw], [dg.launch_params(), jw.launch_params()])
     torch.cuda.synchronize()
     x = tr.cpu().numpy()
@@ -183,8 +187,8 @@ def test_chain_dgbmv_jw_config1_form():
     assert e <= TOL
     # unfused chain gives the same answer within rounding
     tr2 = torch.from_numpy(wl.rhs.copy()).cuda()
-    dg2 = App(buffer=tA, outputBuffer=tr2, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1)
-    jw2 = App(buffer=tb, outputBuffer=tr2, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1)
+    dg2 = App(buffer=tA, outputBuffer=tr2, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1, scaleC=1.0)
+    jw2 = App(buffer=tb, outputBuffer=tr2, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1, scaleC=1.0)
     dg2.append()
     jw2.append()
     torch.cuda.synchronize()
@@ -202,8 +206,8 @@ def _config2_chain(wl, ncplx, scale_block=7, lshift=0):
     rhs = wl.rhs[:2 * M * ncplx].copy()
     tr = torch.from_numpy(rhs).cuda()
     tout = torch.zeros(2 * M * ncplx, dtype=torch.float64, device="cuda")
-    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, 2 * ncplx), LDA=5, KU=2, KL=2, doublePrecision=1)
-    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, 2 * ncplx), upperBanded=2, jw_type=13, doublePrecision=1)
+    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, 2 * ncplx), LDA=5, KU=2, KL=2, doublePrecision=1, scaleC=1.0)
+    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, 2 * ncplx), upperBanded=2, jw_type=13, doublePrecision=1, scaleC=1.0)
     bl = App(buffer=tr, outputBuffer=tout, M_size=M, size=(M, ncplx), block=scale_block, lshift=lshift,
              jw_control_bitmask=capi.RUNTIME_SCALEC, doublePrecision=1)
     append_chain([dg, jw, bl], [dg.launch_params(), jw.launch_params(), bl.launch_params(scaleC=0.5)])
@@ -241,7 +245,7 @@ def test_config3_full_size_sampled():
     M, B = wl.M, wl.nrhs
     tb = torch.from_numpy(wl.jw_bands).cuda()
     tr = torch.from_numpy(wl.rhs).cuda()
-    app = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1)
+    app = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1, scaleC=1.0)
     app.append()
     torch.cuda.synchronize()
     x = tr.view(B, M)
@@ -264,3 +268,58 @@ def test_config3_full_size_sampled():
     r[:, :-1] -= ud[:-1] * x[:, 1:]
     rel = (r.norm(dim=1) / (md * b).norm(dim=1)).max().item()
     assert rel <= 1e-13
+
+
+# ---------------------------------------------------------------------------
+# Mixed precision: FP32 factor-solve + FP64 residual refinement (FP64 storage).
+# Bound: 1e-12 relative L2 against the __float128 oracle after 2 refinement
+# sweeps on the weakly dominant config-3 system; one sweep
+# is allowed 1e-10.
+
+@pytest.mark.parametrize("refine,tol", [(1, 1e-10), (2, 1e-12), (3, 1e-12)])
+def test_mixed_precision_config3(refine, tol):
+    import torch
+
+    from pfsolve_b200.api import App
+    wl = WL.config3(B=512)
+    M, B = wl.M, wl.nrhs
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    tr = torch.from_numpy(wl.rhs.copy()).cuda()
+    app = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
+              scaleC=1.0, mixedPrecisionRefinement=refine)
+    app.append()
+    torch.cuda.synchronize()
+    case = O.Case(M=M, batch=B, upperBanded=2, jw_type=13)
+    ref = O.jw_step(case, wl.jw_bands, wl.rhs, "q")
+    e, _ = O.rel_errors(tr.cpu().numpy(), ref, M, B, M)
+    assert e <= tol, e
+
+
+@pytest.mark.parametrize("ub,jwt", [(1, 10), (0, 10), (1, 12), (0, 12), (1, 13), (0, 13)])
+@pytest.mark.parametrize("M", [100, 300, 1000])
+def test_mixed_precision_bidiagonal(ub, jwt, M):
+    rng = np.random.default_rng(500 + 10 * ub + jwt + M)
+    case, bands, rhs = jw_case(rng, M, 23, ub, jwt)
+    x = J.run_app(case, bands, rhs, mixedPrecisionRefinement=2)
+    e, _ = J.rel_err(x, O.jw_step(case, bands, rhs, "q"), case)
+    assert e <= 1e-12, e
+
+
+def test_mixed_precision_chain_config1_form():
+    import torch
+
+    from pfsolve_b200.api import App, append_chain
+    wl = WL.config1(B=128)
+    M, B = wl.M, wl.nrhs
+    tA = torch.from_numpy(wl.dgbmv).cuda()
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    tr = torch.from_numpy(wl.rhs.copy()).cuda()
+    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1)
+    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1,
+             scaleC=1.0, mixedPrecisionRefinement=2)
+    append_chain([dg, jw], [dg.launch_params(), jw.launch_params()])
+    torch.cuda.synchronize()
+    y = O.dgbmv(O.Case(M=M, batch=B, LDA=3, KU=1, KL=1, jw_type=0), wl.dgbmv, wl.rhs)
+    ref = O.jw_step(O.Case(M=M, batch=B, upperBanded=0, jw_type=13), wl.jw_bands, y, "q")
+    e, _ = O.rel_errors(tr.cpu().numpy(), ref, M, B, M)
+    assert e <= 1e-12, e

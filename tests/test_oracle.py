@@ -67,7 +67,9 @@ def _jw_dense(ub, jwt, md, mo, sl, su, M):
 @pytest.mark.parametrize("M", [40, 257])
 def test_bidiagonal_modes_match_dense(ub, jwt, M):
     rng = np.random.default_rng(ub * 100 + jwt + M)
-    nat = np.concatenate([rng.uniform(1, 2, M), rng.uniform(-.5, .5, M), rng.uniform(-.5, .5, M)])
+    # every band may act as a solve band in some mode: |entries| < 1/2 keeps the
+    # unit-diagonal recurrences stable
+    nat = rng.uniform(-.5, .5, 3 * M)
     bands = WL.permute_bands(nat, M)
     B = 2
     rhs = rng.uniform(-1, 1, M * B)
@@ -92,15 +94,19 @@ def test_operator_offsets_follow_code_not_readme():
                   run_offsetM=0, run_offsetV=2 * M)
     mv, sv, md, mo, sl, su = O.jw_operator(case, bands)
     assert md[0] == 3.0 and mo[0] == 2.0 and sl[0] == 5.0
-    # jw_type%10 == 3 with upperBanded=1 takes md from [M,2M) (flipped orientation)
+    # jw_type%10 == 3 with upperBanded=1 takes md from [M,2M) (flipped
+    # orientation) and solves with the band at [0,M) loaded beside it
     mv, sv, md, mo, sl, su = O.jw_operator(O.Case(M=M, batch=1, upperBanded=1, jw_type=13), bands)
-    assert mv == O.MV_DIAG and md[0] == 3.0
+    assert (mv, sv) == (O.MV_DIAG, O.SV_LOWER) and md[0] == 3.0 and sl[0] == 2.0
+    mv, sv, md, mo, sl, su = O.jw_operator(O.Case(M=M, batch=1, upperBanded=0, jw_type=13), bands)
+    assert (mv, sv) == (O.MV_DIAG, O.SV_UPPER) and md[0] == 2.0 and su[0] == 3.0
 
 
-def test_undefined_combination_rejected():
+@pytest.mark.parametrize("jwt", [10, 11, 12])
+def test_undefined_combination_rejected(jwt):
     M = 16
     with pytest.raises(ValueError):
-        O.jw_step(O.Case(M=M, batch=1, upperBanded=2, jw_type=10), np.ones(3 * M), np.ones(M))
+        O.jw_step(O.Case(M=M, batch=1, upperBanded=2, jw_type=jwt), np.ones(3 * M), np.ones(M))
 
 
 def test_zeropad_keep_windows_and_scaleC():
