@@ -170,7 +170,7 @@ def gpu_arm(args, rank, world):
     dg = App(device=local, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), LDA=5, KU=2, KL=2,
              doublePrecision=1)
     jw = App(device=local, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), upperBanded=2, jw_type=13,
-             doublePrecision=1, scaleC=1.0)
+             doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows)
     bl = App(device=local, buffer=rhs, outputBuffer=out, M_size=M, size=(M, nc), block=7, doublePrecision=1)
     lps = [dg.launch_params(), jw.launch_params(), bl.launch_params()]
     apps = [dg, jw, bl]
@@ -256,7 +256,83 @@ def gpu_arm(args, rank, world):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * nc * 8,
                         "d2h_bytes_per_step": 2 * M * nc * 8},
                 "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
+        if not args.no_extras:
+            line["extras"] = extras_arm(args)
         print(json.dumps(line), flush=True)
+
+
+def extras_arm(args):
+    """Other parts of the metric, measured on the same GPU: config 3 (N=512,
+    131072 real RHS, weakly dominant) in FP64 and in mixed precision (FP32
+    solve + 2 FP64 refinement sweeps) with the mixed result's error against
+    FP64, and config 4 (one spectral timestep, l = 0..511, one persistent
+    launch, captured CUDA graph, autotuned shape)."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App, Batch
+    out = {}
+    wl = WL.config3()
+    M, B = wl.M, wl.nrhs
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    base = torch.from_numpy(wl.rhs).cuda()
+    bytes_alg = 2.0 * M * 8 * B + 3 * M * 8
+    res = {}
+    for name, refine in (("fp64", 0), ("mixed", 2)):
+        x = base.clone()
+        app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
+                  scaleC=1.0, mixedPrecisionRefinement=refine)
+        app.append()
+        torch.cuda.synchronize()
+        res[name] = x.clone()
+        for _ in range(3):
+            app.append()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            app.append()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[f"config3_{name}"] = {"rhs_per_s": B / (ms * 1e-3), "ms": ms, "gbs": bytes_alg / (ms * 1e-3) / 1e9}
+        app.close()
+        del x
+    d = (res["mixed"] - res["fp64"]).view(B, M).norm(dim=1) / res["fp64"].view(B, M).norm(dim=1)
+    out["config3_mixed_vs_fp64_rel_l2_max"] = float(d.max().item())
+    out["config3_mixed_speedup"] = out["config3_fp64"]["ms"] / out["config3_mixed"]["ms"]
+    del res, base
+    step = WL.config4()
+    dev = torch.device("cuda")
+    inp = torch.from_numpy(step.rhs).to(dev)
+    outb = torch.zeros_like(inp)
+    keep, entries = [], []
+    for k, (l, N, ns) in enumerate(zip(step.ls, step.Ns, step.nsys)):
+        tj = torch.from_numpy(step.jw_bands[k]).to(dev)
+        ta = torch.from_numpy(step.dgbmv[k]).to(dev)
+        keep += [tj, ta]
+        off = int(step.rhs_offsets[k])
+        entries.append(dict(M=int(N), nsys=int(ns), bands=tj, dgbmvBands=ta, input=inp.data_ptr() + 8 * off,
+                            output=outb.data_ptr() + 8 * off, inputStride=int(N), outputStride=int(N),
+                            lshift=int(l), scaleS=step.scale_s, scaleC=1.0))
+    batch = Batch(entries, upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=307)
+    st = torch.cuda.Stream()
+    batch.autotune(st, iterations=3)
+    batch.capture(st)
+    for _ in range(3):
+        batch.append(st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(10):
+        batch.append(st)
+    e1.record(st)
+    st.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    rows = int((step.Ns * step.nsys).sum())
+    out["config4_uneven_step"] = {"complex_rhs_per_s": int(step.nsys.sum()) / (ms * 1e-3), "ms": ms,
+                                  "gbs": 2.0 * rows * 16 / (ms * 1e-3) / 1e9, "shape": batch.shape(),
+                                  "graph": True, "launches_per_step": 1}
+    batch.close()
+    return out
 
 
 def main():
@@ -268,6 +344,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ncplx", type=int, default=N_CPLX, help="complex RHS per GPU (profiling cases only)")
     ap.add_argument("--profile", action="store_true", help="kernel steps only: no e2e leg, no CPU baseline")
+    ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu = True

@@ -256,6 +256,61 @@ PFSOLVE_API PfSolveResult addToLibrary_block(PfSolve_AppLibrary* lib, PfSolve_Ma
 PFSOLVE_API PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveLaunchParams** launchParams, int n,
                                  int allowUnfused);
 
+/* ---- Uneven batch (extension) ----
+ * One JW step over many groups of systems of different sizes (one group per
+ * harmonic degree of a spectral timestep), in ONE persistent launch: groups
+ * of warps take (entry, system range) items from a device work queue,
+ * largest first, and refactor the matrix when the entry changes.  The step is
+ * the chain [dgbmv] -> JW -> [block] of the apps with the same fields.
+ * Every entry uses plan-time band offsets: JW bands at 0, M, 2M of `bands`
+ * (reference register-major order for its own M), dgbmv bands band-major. */
+typedef struct {
+    int64_t M;               /* rows of this entry's systems (<= 4096) */
+    int64_t nsys;            /* systems (complex ones count once) */
+    const void* bands;       /* JW bands of this entry (device) */
+    const void* dgbmvBands;  /* band-major matrix of the fused dgbmv (device), or NULL */
+    const void* input;       /* system y: input + y*inputStride (XXII: rows 2y and 2y+1) */
+    void* output;            /* system y: output + y*outputStride (packed complex: in complex elements) */
+    int64_t inputStride;
+    int64_t outputStride;
+    int lshift;              /* Scale operator's harmonic degree */
+    double scaleS;           /* Scale operator's s (its scaleC) */
+    double scaleC;           /* JW scaleC on solution row 0 */
+} PfSolveBatchEntry;
+
+typedef struct {
+    int upperBanded;              /* JW step of every entry */
+    int jw_type;
+    int LDA, KU, KL;              /* fused dgbmv (LDA = 0: none) */
+    int block;                    /* fused block epilogue: 0, 1 (real) or 7 (XXII -> packed) plus
+                                     100 * Scale kind (BLOCK_SCALEC ... BLOCK_SCALESPHLAPLB) */
+    int mixedPrecisionRefinement; /* as in PfSolveConfiguration */
+    int rowsPerThread;            /* 0: default / autotuned */
+    int systemsPerItem;           /* work-queue item size (0: default / autotuned) */
+} PfSolveBatchDesc;
+
+typedef struct PfSolveBatch PfSolveBatch;
+
+/* Build a batch plan: copies the entry descriptors and the work list to the
+ * device (owned by the plan). */
+PFSOLVE_API PfSolveResult PfSolveBatchCreate(PfSolveBatch** batch, CUdevice device, const PfSolveBatchDesc* desc,
+                                             const PfSolveBatchEntry* entries, int nentries);
+/* Enqueue the whole batch: a work-queue reset and one persistent kernel (or
+ * the captured graph of exactly that). */
+PFSOLVE_API PfSolveResult PfSolveBatchAppend(PfSolveBatch* batch, cudaStream_t stream);
+/* Capture the batch's launch into a CUDA graph on `stream` (a non-default
+ * stream); later PfSolveBatchAppend calls launch the graph. */
+PFSOLVE_API PfSolveResult PfSolveBatchCaptureGraph(PfSolveBatch* batch, cudaStream_t stream);
+/* Time every compiled rows-per-thread / item-size candidate on the batch's
+ * own buffers (`iterations` launches each) and keep the fastest; drops a
+ * captured graph.  Entries must be out of place (input != output). */
+PFSOLVE_API PfSolveResult PfSolveBatchAutotune(PfSolveBatch* batch, cudaStream_t stream, int iterations);
+/* Chosen shape: rows per thread, warps per system, systems per item, work
+ * items, and the autotuner's best time (ms, 0 when not tuned). */
+PFSOLVE_API PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* batch, int* rowsPerThread, int* warpsPerSystem,
+                                               int* systemsPerItem, int* items, double* tunedMs);
+PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
+
 /* Number of kernel launches this library has enqueued since load (all apps). */
 PFSOLVE_API uint64_t PfSolveLaunchCount(void);
 

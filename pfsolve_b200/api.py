@@ -121,3 +121,71 @@ def append_chain(apps: Sequence[App], lps: Sequence[capi.PfSolveLaunchParams], a
 
 def launch_count() -> int:
     return int(capi.load().PfSolveLaunchCount())
+
+
+class Batch:
+    """One uneven batch plan (``PfSolveBatchCreate``): a JW step over many
+    groups of systems of different sizes in one persistent launch.
+
+    ``entries`` is a list of dicts with the ``PfSolveBatchEntry`` fields; device
+    buffers may be torch tensors or raw pointers.
+    """
+
+    def __init__(self, entries, *, device: int = 0, **desc_fields):
+        self._lib = capi.load()
+        self._keep = entries
+        d = capi.PfSolveBatchDesc()
+        for k, v in desc_fields.items():
+            setattr(d, k, int(v))
+        arr = (capi.PfSolveBatchEntry * max(1, len(entries)))()
+        for i, e in enumerate(entries):
+            a = arr[i]
+            a.M, a.nsys = int(e["M"]), int(e["nsys"])
+            a.bands = _ptr(e["bands"])
+            a.dgbmvBands = _ptr(e.get("dgbmvBands"))
+            a.input = _ptr(e["input"])
+            a.output = _ptr(e["output"])
+            a.inputStride = int(e["inputStride"])
+            a.outputStride = int(e["outputStride"])
+            a.lshift = int(e.get("lshift", 0))
+            a.scaleS = float(e.get("scaleS", 0.0))
+            a.scaleC = float(e.get("scaleC", 1.0))
+        self.handle = ctypes.c_void_p()
+        check(self._lib.PfSolveBatchCreate(ctypes.byref(self.handle), int(device), ctypes.byref(d), arr,
+                                           len(entries)), "PfSolveBatchCreate")
+
+    def append(self, stream=None):
+        check(self._lib.PfSolveBatchAppend(self.handle, _stream(stream)), "PfSolveBatchAppend")
+
+    def capture(self, stream):
+        check(self._lib.PfSolveBatchCaptureGraph(self.handle, _stream(stream)), "PfSolveBatchCaptureGraph")
+
+    def autotune(self, stream=None, iterations=3):
+        check(self._lib.PfSolveBatchAutotune(self.handle, _stream(stream), int(iterations)), "PfSolveBatchAutotune")
+
+    def shape(self):
+        r, w, spi, items = (ctypes.c_int() for _ in range(4))
+        ms = ctypes.c_double()
+        check(self._lib.PfSolveBatchGetShape(self.handle, ctypes.byref(r), ctypes.byref(w), ctypes.byref(spi),
+                                             ctypes.byref(items), ctypes.byref(ms)), "PfSolveBatchGetShape")
+        return dict(rowsPerThread=r.value, warpsPerSystem=w.value, systemsPerItem=spi.value, items=items.value,
+                    tunedMs=ms.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.PfSolveBatchDestroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return int(s.cuda_stream)

@@ -103,6 +103,18 @@ class MapKeyBlock(ctypes.Structure):
                 ("lshift", i64)]
 
 
+class PfSolveBatchEntry(ctypes.Structure):
+    _fields_ = [("M", i64), ("nsys", i64), ("bands", ctypes.c_void_p), ("dgbmvBands", ctypes.c_void_p),
+                ("input", ctypes.c_void_p), ("output", ctypes.c_void_p), ("inputStride", i64),
+                ("outputStride", i64), ("lshift", c_int), ("scaleS", ctypes.c_double), ("scaleC", ctypes.c_double)]
+
+
+class PfSolveBatchDesc(ctypes.Structure):
+    _fields_ = [("upperBanded", c_int), ("jw_type", c_int), ("LDA", c_int), ("KU", c_int), ("KL", c_int),
+                ("block", c_int), ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int),
+                ("systemsPerItem", c_int)]
+
+
 # Every function the header declares, with its ctypes signature.
 _APP_P = ctypes.POINTER(PfSolveApplication)
 _LP_P = ctypes.POINTER(PfSolveLaunchParams)
@@ -123,6 +135,13 @@ SIGNATURES = {
     "addToLibrary_block": (c_int, [ctypes.c_void_p, MapKeyBlock, _APP_P]),
     "PfSolveAppendChain": (c_int, [ctypes.POINTER(_APP_P), ctypes.POINTER(_LP_P), c_int, c_int]),
     "PfSolveLaunchCount": (u64, []),
+    "PfSolveBatchCreate": (c_int, [ctypes.POINTER(ctypes.c_void_p), c_int, ctypes.POINTER(PfSolveBatchDesc),
+                                   ctypes.POINTER(PfSolveBatchEntry), c_int]),
+    "PfSolveBatchAppend": (c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "PfSolveBatchCaptureGraph": (c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "PfSolveBatchAutotune": (c_int, [ctypes.c_void_p, ctypes.c_void_p, c_int]),
+    "PfSolveBatchGetShape": (c_int, [ctypes.c_void_p] + [ctypes.POINTER(c_int)] * 4 + [ctypes.POINTER(ctypes.c_double)]),
+    "PfSolveBatchDestroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None

@@ -36,6 +36,7 @@ struct AppState {
     int R = 0, W = 1, G = 1;
     int mvj = MVJ_NONE, sv = SV_NONE, KL = 0, KU = 0;
     int prec = 0;           // 0: FP64, 1: FP32 solve + FP64 refinement
+    bool R_fixed = false;   // rows per thread requested by the caller
     int refine_sweeps = 1;  // FP32 solves per system in the mixed mode
     const JwVariant* variant = nullptr;
     int max_blocks = 0;  // resident CTAs over the whole GPU
@@ -74,64 +75,78 @@ void keep_window(bool runtime, int64_t z0, int64_t z1, int64_t& lo, int64_t& hi)
     hi = z1 ? z1 : BIG;
 }
 
+// Default rows per thread: 4 keeps the data of a coefficient-table variant
+// within 128 registers (two 256-thread groups per SM); longer systems need
+// more rows per thread to stay within 8 warps per system.
 int pick_rows_per_thread(int64_t M, int requested)
 {
     if (requested == 2 || requested == 4 || requested == 8 || requested == 16) return requested;
     if (M <= 64) return 2;
-    if (M <= 128) return 4;
+    if (M <= 1024) return 4;
     if (M <= 2048) return 8;
     return 16;
 }
 
-PfSolveResult configure_launch_shape(AppState* s, int64_t M)
+// Groups per CTA for variant v at W warps per system: the count that keeps the
+// most groups resident per SM (shared memory, registers and the variant's
+// launch bound permitting).  Returns false when nothing fits.
+bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, int& max_blocks)
 {
-    // W warps per system: enough for M rows at R rows per thread, at most 8.
-    int R = s->R;
-    int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
-    while (W > 8 && R < 16) {
-        R *= 2;
-        W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
-    }
-    if (W > 8) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
-    if (W < 1) W = 1;
-    s->R = R;
-    s->W = (int)W;
-    s->G = std::max(1, 8 / s->W);  // 256-thread CTAs
-    return PFSOLVE_SUCCESS;
-}
-
-PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
-{
-    PfSolveResult r = configure_launch_shape(s, M);
-    if (r != PFSOLVE_SUCCESS) return r;
-    const JwVariant* v = find_jw_variant(s->R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
-    if (!v) {
-        for (int R : {8, 4, 16, 2}) {
-            if (R == s->R) continue;
-            const JwVariant* c = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
-            if (!c) continue;
-            AppState t = *s;
-            t.R = R;
-            if (configure_launch_shape(&t, M) != PFSOLVE_SUCCESS) continue;
-            if (t.R != R) continue;
-            *s = t;
-            v = c;
+    int best = 0, bestG = 0, bestBlocks = 0;
+    size_t bestSmem = 0;
+    for (int G = 1; 32 * W * G <= v->max_threads; ++G) {
+        const size_t smem = v->smem_bytes(W, G);
+        if (smem > 227 * 1024) break;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             break;
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess)
+            break;
+        if (blocks * G > best) {
+            best = blocks * G;
+            bestG = G;
+            bestBlocks = blocks;
+            bestSmem = smem;
         }
     }
-    if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-    s->variant = v;
-    const size_t smem = v->smem_bytes(s->W, s->G);
-    if (smem > 48 * 1024) {
-        if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    if (best == 0) return false;
+    if (bestSmem > 48 * 1024 &&
+        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bestSmem) != cudaSuccess)
+        return false;
+    G_out = bestG;
+    max_blocks = bestBlocks * num_sms;
+    return true;
+}
+
+// Pick the kernel variant and launch shape for M rows: coefficient-table
+// variants first (FP64), then register variants; rows per thread from the
+// caller's choice (s->R) first, then the other compiled choices.
+PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    const int order[4] = {s->R, 8, 4, 16};
+    for (int tbl = (s->prec == 0 ? 1 : 0); tbl >= 0; --tbl) {
+        for (int oi = 0; oi < 4; ++oi) {
+            const int R = order[oi];
+            if (oi > 0 && (R == s->R || s->R_fixed)) continue;
+            const JwVariant* v = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, tbl);
+            if (!v) continue;
+            const int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+            if (W < 1 || W > 8 || 32 * W > v->max_threads) continue;
+            int G = 0, maxb = 0;
+            if (!choose_groups(v, (int)W, s->num_sms, G, maxb)) continue;
+            s->variant = v;
+            s->R = R;
+            s->W = (int)W;
+            s->G = G;
+            s->max_blocks = maxb;
+            return PFSOLVE_SUCCESS;
+        }
     }
-    int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * s->W * s->G, smem) != cudaSuccess ||
-        blocks < 1)
-        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
-    s->max_blocks = blocks * s->num_sms;
-    return PFSOLVE_SUCCESS;
+    // nothing compiled fits: distinguish "too long" from "not compiled"
+    for (int R : {2, 4, 8, 16})
+        if ((M + 32 * (int64_t)R - 1) / (32 * (int64_t)R) <= 8) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
 }
 
 // JW operator kinds for K = 1 (pfSolve_JonesWorland.h:117-353): which matvec,
@@ -467,6 +482,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
                 s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
+                s->R_fixed = c.rowsPerThread != 0;
                 reference_band_order(c.M_size, s->perm_r, s->perm_m, s->perm_ceil, s->perm_floor);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
@@ -691,3 +707,326 @@ extern "C" PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveLa
     }
     return r;
 }
+
+// ---------------------------------------------------------------------------
+// Uneven batches: many matrices of different sizes, one persistent launch.
+#include <vector>
+
+struct PfSolveBatch {
+    PfSolveBatchDesc desc;
+    int device = 0, num_sms = 0;
+    int KL = 0, KU = 0, SV = 0, LIN = 0, LOUT = 0, SCALE = 0, PREC = 0;
+    int64_t Mmax = 0;
+    int R = 8, W = 1, G = 1, spi = 64;
+    int max_blocks = 0;
+    const BatchVariant* variant = nullptr;
+    std::vector<BatchEntryDev> entries;
+    std::vector<WorkItem> items;
+    BatchEntryDev* d_entries = nullptr;
+    WorkItem* d_items = nullptr;
+    size_t d_items_cap = 0;
+    unsigned int* d_counter = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double tuned_ms = 0.0;
+};
+
+namespace {
+
+void batch_drop_graph(PfSolveBatch* b)
+{
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+}
+
+PfSolveResult batch_build_items(PfSolveBatch* b, int spi)
+{
+    b->items.clear();
+    for (size_t e = 0; e < b->entries.size(); ++e) {
+        const int64_t n = b->entries[e].io.nsys;
+        for (int64_t y0 = 0; y0 < n; y0 += spi) {
+            WorkItem w;
+            w.entry = (int)e;
+            w.pad = 0;
+            w.y0 = y0;
+            w.y1 = std::min<int64_t>(n, y0 + spi);
+            b->items.push_back(w);
+        }
+    }
+    // largest work first (bytes ~ rows x systems), ties by entry for locality
+    std::stable_sort(b->items.begin(), b->items.end(), [&](const WorkItem& x, const WorkItem& y) {
+        const int64_t cx = b->entries[x.entry].op.M * (x.y1 - x.y0);
+        const int64_t cy = b->entries[y.entry].op.M * (y.y1 - y.y0);
+        return cx > cy;
+    });
+    if (b->items.size() > b->d_items_cap) {
+        if (b->d_items) cudaFree(b->d_items);
+        b->d_items = nullptr;
+        if (cudaMalloc(&b->d_items, b->items.size() * sizeof(WorkItem)) != cudaSuccess)
+            return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
+        b->d_items_cap = b->items.size();
+    }
+    if (!b->items.empty() &&
+        cudaMemcpy(b->d_items, b->items.data(), b->items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+        return PFSOLVE_ERROR_FAILED_TO_COPY;
+    b->spi = spi;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult batch_configure(PfSolveBatch* b, int R)
+{
+    int64_t W = (b->Mmax + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+    if (W < 1) W = 1;
+    if (W > 8) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+    const BatchVariant* v = find_batch_variant(R, b->KL, b->KU, b->SV, b->LIN, b->LOUT, b->SCALE, b->PREC);
+    if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const int G = std::max(1, 8 / (int)W);
+    const size_t smem = v->smem_bytes((int)W, G);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * (int)W * G, smem) != cudaSuccess ||
+        blocks < 1)
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    b->variant = v;
+    b->R = R;
+    b->W = (int)W;
+    b->G = G;
+    b->max_blocks = blocks * b->num_sms;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult batch_launch(PfSolveBatch* b, cudaStream_t stream)
+{
+    const int nitems = (int)b->items.size();
+    if (nitems == 0) return PFSOLVE_SUCCESS;
+    if (cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned int), stream) != cudaSuccess)
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    const int64_t want = (nitems + b->G - 1) / b->G;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, b->max_blocks));
+    const size_t smem = b->variant->smem_bytes(b->W, b->G);
+    b->variant->launch(dim3((unsigned)grid), dim3(32 * b->W * b->G), smem, stream, b->d_entries, b->d_items, nitems,
+                       b->d_counter, b->W);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+PfSolveResult PfSolveBatchCreate(PfSolveBatch** out, CUdevice device, const PfSolveBatchDesc* desc,
+                                 const PfSolveBatchEntry* entries, int nentries)
+{
+    if (!out || !desc || (nentries > 0 && !entries) || nentries < 0) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    *out = nullptr;
+    PfSolveBatch* b = new (std::nothrow) PfSolveBatch();
+    if (!b) return PFSOLVE_ERROR_MALLOC_FAILED;
+    b->desc = *desc;
+    b->device = device;
+    auto fail = [&](PfSolveResult r) {
+        PfSolveBatchDestroy(b);
+        return r;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(PFSOLVE_ERROR_INVALID_DEVICE);
+    if (cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return fail(PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE);
+    if (desc->mixedPrecisionRefinement < 0 || desc->mixedPrecisionRefinement > 3)
+        return fail(PFSOLVE_ERROR_INVALID_ARGUMENT);
+    const int bt = desc->block % 10, sk = desc->block / 100;
+    if (!(bt == 0 || bt == 1 || bt == 7) || ((desc->block / 10) % 10 != 0 && (desc->block / 10) % 10 != 2) || sk > 4)
+        return fail(PFSOLVE_ERROR_UNSUPPORTED_COMBINATION);
+    if (bt == 0 && desc->block != 0) return fail(PFSOLVE_ERROR_UNSUPPORTED_COMBINATION);
+    PfSolveConfiguration c;
+    memset(&c, 0, sizeof(c));
+    c.upperBanded = desc->upperBanded;
+    c.jw_type = desc->jw_type;
+    c.M_size = 16;
+    JwLayout L0;
+    if (desc->jw_type < 10 || !jw_layout(c, false, false, 0, 0, L0)) return fail(PFSOLVE_ERROR_UNSUPPORTED_COMBINATION);
+    b->SV = L0.sv;
+    b->KL = (L0.mvj == MVJ_LOWER) ? 1 : 0;
+    b->KU = (L0.mvj == MVJ_UPPER) ? 1 : 0;
+    if (desc->LDA > 0) {
+        if (desc->KU < 0 || desc->KU >= desc->LDA) return fail(PFSOLVE_ERROR_INVALID_ARGUMENT);
+        b->KL += desc->LDA - 1 - desc->KU;
+        b->KU += desc->KU;
+    }
+    b->LIN = (bt == 7) ? LAY_XXII : LAY_REAL;
+    b->LOUT = (bt == 7) ? LAY_PACKED : LAY_REAL;
+    b->SCALE = sk ? 1 : 0;
+    b->PREC = (desc->mixedPrecisionRefinement > 0 && b->SV != SV_NONE) ? 1 : 0;
+    for (int e = 0; e < nentries; ++e) {
+        const PfSolveBatchEntry& en = entries[e];
+        if (en.M < 1 || en.M > kMaxRows || en.nsys < 0 || !en.bands || !en.input || !en.output)
+            return fail(PFSOLVE_ERROR_INVALID_ARGUMENT);
+        if (desc->LDA > 0 && !en.dgbmvBands) return fail(PFSOLVE_ERROR_INVALID_ARGUMENT);
+        c.M_size = en.M;
+        JwLayout L;
+        jw_layout(c, false, false, 0, 0, L);
+        BatchEntryDev d;
+        memset(&d, 0, sizeof(d));
+        AppState tmp;
+        reference_band_order(en.M, tmp.perm_r, tmp.perm_m, tmp.perm_ceil, tmp.perm_floor);
+        tmp.refine_sweeps = 1 + desc->mixedPrecisionRefinement;
+        fill_operator_common(&tmp, c, d.op);
+        d.op.bands = static_cast<const double*>(en.bands);
+        d.op.off_md = L.off_md;
+        d.op.off_mo = L.off_mo;
+        d.op.off_sl = L.off_sl;
+        d.op.off_su = L.off_su;
+        d.op.mvj = L.mvj;
+        d.op.scaleC = en.scaleC;
+        if (desc->LDA > 0) {
+            d.op.dgbmv = static_cast<const double*>(en.dgbmvBands);
+            d.op.dg_off = 0;
+            d.op.dg_lda = desc->LDA;
+            d.op.dg_ku = desc->KU;
+        }
+        d.op.scale_kind = sk;
+        d.op.lshift = en.lshift;
+        d.op.scale_s = en.scaleS;
+        d.io.in = static_cast<const double*>(en.input);
+        d.io.out = static_cast<double*>(en.output);
+        d.io.in_stride = en.inputStride;
+        d.io.out_stride = en.outputStride;
+        d.io.iz0 = 0;
+        d.io.iz1 = INT64_MAX / 4;
+        d.io.oz0 = 0;
+        d.io.oz1 = INT64_MAX / 4;
+        d.io.nsys = en.nsys;
+        d.io.M = en.M;
+        d.io.accumulate = ((desc->block / 10) % 10) == 2;
+        b->entries.push_back(d);
+        b->Mmax = std::max<int64_t>(b->Mmax, en.M);
+    }
+    if (cudaMalloc(&b->d_counter, sizeof(unsigned int)) != cudaSuccess) return fail(PFSOLVE_ERROR_FAILED_TO_ALLOCATE);
+    if (!b->entries.empty()) {
+        if (cudaMalloc(&b->d_entries, b->entries.size() * sizeof(BatchEntryDev)) != cudaSuccess)
+            return fail(PFSOLVE_ERROR_FAILED_TO_ALLOCATE);
+        if (cudaMemcpy(b->d_entries, b->entries.data(), b->entries.size() * sizeof(BatchEntryDev),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(PFSOLVE_ERROR_FAILED_TO_COPY);
+    }
+    int R = desc->rowsPerThread ? desc->rowsPerThread : 8;
+    PfSolveResult r = batch_configure(b, R);
+    if (r != PFSOLVE_SUCCESS && !desc->rowsPerThread) r = batch_configure(b, 4);
+    if (r != PFSOLVE_SUCCESS) return fail(r);
+    int spi = desc->systemsPerItem;
+    if (spi <= 0) {
+        // about 4 items per resident group keeps the queue balanced
+        int64_t total = 0;
+        for (const auto& e : b->entries) total += e.io.nsys;
+        const int64_t groups = std::max<int64_t>(1, (int64_t)b->max_blocks * b->G);
+        spi = (int)std::max<int64_t>(8, std::min<int64_t>(256, total / (4 * groups) + 1));
+    }
+    if ((r = batch_build_items(b, spi)) != PFSOLVE_SUCCESS) return fail(r);
+    *out = b;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveBatchAppend(PfSolveBatch* b, cudaStream_t stream)
+{
+    if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    if (b->graph_exec) {
+        if (cudaGraphLaunch(b->graph_exec, stream) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        return PFSOLVE_SUCCESS;
+    }
+    return batch_launch(b, stream);
+}
+
+PfSolveResult PfSolveBatchCaptureGraph(PfSolveBatch* b, cudaStream_t stream)
+{
+    if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    if (!stream) return PFSOLVE_ERROR_INVALID_ARGUMENT;  // the legacy default stream cannot be captured
+    batch_drop_graph(b);
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    const uint64_t before = g_launches.load();
+    PfSolveResult r = batch_launch(b, stream);
+    g_launches.store(before);  // capturing enqueues nothing
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+    if (r != PFSOLVE_SUCCESS || ce != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        return r != PFSOLVE_SUCCESS ? r : PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    if (cudaGraphInstantiate(&b->graph_exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        b->graph_exec = nullptr;
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    b->graph = graph;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int iterations)
+{
+    if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    for (const auto& e : b->entries)
+        if ((const void*)e.io.in == (const void*)e.io.out) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    if (iterations < 1) iterations = 3;
+    batch_drop_graph(b);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int bestR = b->R, bestSpi = b->spi;
+    for (int R : {4, 8, 16, 2}) {
+        if (batch_configure(b, R) != PFSOLVE_SUCCESS) continue;
+        for (int spi : {16, 32, 64, 128}) {
+            if (batch_build_items(b, spi) != PFSOLVE_SUCCESS) continue;
+            if (batch_launch(b, stream) != PFSOLVE_SUCCESS) continue;  // warm-up
+            cudaEventRecord(e0, stream);
+            for (int it = 0; it < iterations; ++it) batch_launch(b, stream);
+            cudaEventRecord(e1, stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double per = ms / iterations;
+            if (per < best) {
+                best = per;
+                bestR = R;
+                bestSpi = spi;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    PfSolveResult r = batch_configure(b, bestR);
+    if (r == PFSOLVE_SUCCESS) r = batch_build_items(b, bestSpi);
+    if (r == PFSOLVE_SUCCESS) b->tuned_ms = best;
+    return r;
+}
+
+PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* b, int* R, int* W, int* spi, int* items, double* ms)
+{
+    if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    if (R) *R = b->R;
+    if (W) *W = b->W;
+    if (spi) *spi = b->spi;
+    if (items) *items = (int)b->items.size();
+    if (ms) *ms = b->tuned_ms;
+    return PFSOLVE_SUCCESS;
+}
+
+void PfSolveBatchDestroy(PfSolveBatch* b)
+{
+    if (!b) return;
+    batch_drop_graph(b);
+    if (b->d_entries) cudaFree(b->d_entries);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_counter) cudaFree(b->d_counter);
+    delete b;
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// batch_variants.cu -- instantiations of the persistent uneven-batch kernel.
+#include "jw_kernel.cuh"
+#include "jw_variants.h"
+
+namespace pfb {
+
+template <class C>
+static size_t batch_smem_fn(int W, int G)
+{
+    return jw_batch_smem_bytes<C>(W, G);
+}
+
+template <class C>
+static void batch_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const BatchEntryDev* entries,
+                            const WorkItem* items, int nitems, unsigned int* counter, int W)
+{
+    jw_batch_kernel<C><<<grid, block, smem, st>>>(entries, items, nitems, counter, W);
+}
+
+#define PFB_BV(R, KL, KU, SV, LIN, LOUT, SC, P)                                                   \
+    BatchVariant{R, KL, KU, SV, LIN, LOUT, SC, P,                                                 \
+                 (const void*)&jw_batch_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>,           \
+                 &batch_smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>,                          \
+                 &batch_launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>}
+#define PFB_BV2(KL, KU, SV, LIN, LOUT, SC, P) PFB_BV(4, KL, KU, SV, LIN, LOUT, SC, P), PFB_BV(8, KL, KU, SV, LIN, LOUT, SC, P)
+
+static const BatchVariant kBatchVariants[] = {
+    // one spectral timestep: 3-band V + upper-bidiagonal M, SphLaplA, XXII -> packed
+    PFB_BV2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true, PREC_F64),
+    PFB_BV2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, false, PREC_F64),
+    // request batches of the serving loop (real systems, in place)
+    PFB_BV2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_F64),
+    PFB_BV2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_MIXED),
+    PFB_BV2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false, PREC_F64),
+    PFB_BV2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false, PREC_MIXED),
+    PFB_BV2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_F64),
+};
+
+const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)
+{
+    for (const BatchVariant& v : kBatchVariants)
+        if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
+            v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC)
+            return &v;
+    return nullptr;
+}
+
+}  // namespace pfb

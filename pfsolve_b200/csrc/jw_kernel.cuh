@@ -44,7 +44,7 @@ namespace pfb {
 
 enum : int { PREC_F64 = 0, PREC_MIXED = 1 };
 
-template <int R, int KL, int KU, int SV, int LIN, int LOUT, bool SCALE, int PREC = PREC_F64>
+template <int R, int KL, int KU, int SV, int LIN, int LOUT, bool SCALE, int PREC = PREC_F64, bool TBL = false>
 struct JwCfg {
     static constexpr int kR = R, kKL = KL, kKU = KU, kSV = SV, kLIN = LIN, kLOUT = LOUT, kPrec = PREC;
     static constexpr bool kScale = SCALE;
@@ -58,6 +58,14 @@ struct JwCfg {
     static constexpr bool kMixed = (PREC == PREC_MIXED) && (SV != SV_NONE);
     static constexpr int NF = kFwd ? R : 1;
     static constexpr int NBW = kBwd ? R : 1;
+    // Coefficients in a CTA-shared table: planes w[0..NB), l, h, sc, each
+    // [R][T] doubles (T threads per group) -- lane-contiguous, conflict-free.
+    static constexpr bool kTbl = TBL && !kMixed;
+    static constexpr int P_L = NB, P_H = NB + (kFwd ? 1 : 0), P_SC = P_H + (kBwd ? 1 : 0);
+    static constexpr int NPLANES = P_SC + (SCALE ? 1 : 0);
+    // Register-resident coefficients need up to 255 registers: 256-thread
+    // CTAs.  Table variants keep data only: up to 512 threads (<= 128 regs).
+    static constexpr int kMaxThreads = kTbl ? 512 : 256;
 };
 
 constexpr int kScratchPerWarp = 32;  // doubles
@@ -71,9 +79,16 @@ __host__ __device__ constexpr size_t jw_smem_per_warp()
 }
 
 template <class C>
+__host__ __device__ constexpr size_t jw_table_bytes(int W)
+{
+    return C::kTbl ? (size_t)C::NPLANES * C::kR * 32 * W * sizeof(double) : 0;
+}
+
+template <class C>
 __host__ size_t jw_smem_bytes(int W, int G)
 {
-    return (size_t)G * W * jw_smem_per_warp<C>() + (size_t)G * W * kScratchPerWarp * sizeof(double);
+    return jw_table_bytes<C>(W) + (size_t)G * W * jw_smem_per_warp<C>() +
+           (size_t)G * W * kScratchPerWarp * sizeof(double);
 }
 
 __device__ __forceinline__ int64_t band_pos(const JwOperator& op, int64_t i)
@@ -103,22 +118,46 @@ __device__ __forceinline__ double scale_factor(int kind, int64_t x, int L, doubl
     }
 }
 
-// Per-thread coefficients of one matrix.  FP64 path: the solve scaling is
-// folded into w.  Mixed path: w stays unscaled (it forms g = V*A*b), the
-// solve factors live in FP32 and the unit-diagonal solve bands in FP64 for the
-// residual.
+// Per-thread coefficients of one matrix, in registers or in the CTA-shared
+// table.  FP64 path: the solve scaling is folded into w.  Mixed path: w stays
+// unscaled (it forms g = V*A*b), the solve factors live in FP32 and the
+// unit-diagonal solve bands in FP64 for the residual.  The in-chunk products of
+// the recurrences (-l and -h) are formed on the fly by the solve.
 template <class C>
 struct JwCoef {
     using S = typename std::conditional<C::kMixed, float, double>::type;
-    double w[C::NB][C::kR];
-    S m[C::kMixed ? C::kR : 1];
-    S l[C::NF];
-    S F[C::NF];
-    S h[C::NBW];
-    S G[C::NBW];
-    double al[C::kMixed ? C::NF : 1];   // M's sub-diagonal (residual)
-    double cu[C::kMixed ? C::NBW : 1];  // M's super-diagonal (residual)
-    double sc[C::kScale ? C::kR : 1];
+    static constexpr int RR = C::kTbl ? 1 : C::kR;
+    double w_[C::NB][RR];
+    S m_[C::kMixed ? C::kR : 1];
+    S l_[C::kTbl ? 1 : C::NF];
+    S h_[C::kTbl ? 1 : C::NBW];
+    double al_[C::kMixed ? C::NF : 1];   // M's sub-diagonal (residual)
+    double cu_[C::kMixed ? C::NBW : 1];  // M's super-diagonal (residual)
+    double sc_[(C::kScale && !C::kTbl) ? C::kR : 1];
+    const double* tbl;  // table mode: plane p, row j of thread tt at tbl[(p*R + j)*T + tt]
+    int T, tt;
+
+    __device__ __forceinline__ double t_(int p, int j) const { return tbl[(p * C::kR + j) * T + tt]; }
+    __device__ __forceinline__ double w(int k, int j) const
+    {
+        if constexpr (C::kTbl) return t_(k, j);
+        else return w_[k][j];
+    }
+    __device__ __forceinline__ S l(int j) const
+    {
+        if constexpr (C::kTbl) return t_(C::P_L, j);
+        else return l_[j];
+    }
+    __device__ __forceinline__ S h(int j) const
+    {
+        if constexpr (C::kTbl) return t_(C::P_H, j);
+        else return h_[j];
+    }
+    __device__ __forceinline__ double sc(int j) const
+    {
+        if constexpr (C::kTbl) return t_(C::P_SC, j);
+        else return sc_[j];
+    }
 };
 
 // Cross-warp scratch: kScratchPerWarp doubles per warp,
@@ -254,18 +293,21 @@ __device__ __forceinline__ void group_matrix_scan(GroupCtx& g, double& a, double
     d = ec * wb + ed * wd;
 }
 
-// Build the per-thread coefficients for rows s .. s+R-1 of operator `op`.
+// Build the coefficients for rows s .. s+R-1 of operator `op` (every thread
+// of the group), then keep them in registers or write them to the table.
 template <class C>
-__device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, int64_t s, JwCoef<C>& cf)
+__device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, int64_t s, JwCoef<C>& cf,
+                                            double* table = nullptr)
 {
     constexpr int R = C::kR, KL = C::kKL, KU = C::kKU;
     using S = typename JwCoef<C>::S;
     const int64_t M = op.M;
+    double w[C::NB][R];
     // (1) effective matvec weights of V*A for each row
 #pragma unroll
     for (int j = 0; j < R; ++j) {
 #pragma unroll
-        for (int k = 0; k < C::NB; ++k) cf.w[k][j] = 0.0;
+        for (int k = 0; k < C::NB; ++k) w[k][j] = 0.0;
         const int64_t i = s + j;
         if (i < M) {
             double vl = 0, vd = 1, vu = 0;
@@ -273,9 +315,9 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, i
             if (op.mvj == MVJ_UPPER && i + 1 < M) vu = band(op, op.off_mo, i);
             if (op.mvj == MVJ_LOWER && i >= 1) vl = band(op, op.off_mo, i);
             if (op.dgbmv == nullptr) {
-                if constexpr (KL >= 1) cf.w[KL - 1][j] = vl;
-                cf.w[KL][j] = vd;
-                if constexpr (KU >= 1) cf.w[KL + 1][j] = vu;
+                if constexpr (KL >= 1) w[KL - 1][j] = vl;
+                w[KL][j] = vd;
+                if constexpr (KU >= 1) w[KL + 1][j] = vu;
             } else {
                 const int kla = op.dg_lda - 1 - op.dg_ku;
                 for (int pv = -1; pv <= 1; ++pv) {
@@ -289,16 +331,16 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, i
                         const int64_t k = c - i;  // within [-KL, KU] by construction of the plan
 #pragma unroll
                         for (int q = 0; q < C::NB; ++q)
-                            if (q - KL == (int)k) cf.w[q][j] = __fma_rn(vp, a, cf.w[q][j]);
+                            if (q - KL == (int)k) w[q][j] = __fma_rn(vp, a, w[q][j]);
                     }
                 }
             }
         }
     }
     // (2) solve coefficients in FP64
-    double l64[R], h64[R], m64[R];
+    double l64[R], h64[R], m64[R], a64[R], c64[R];
 #pragma unroll
-    for (int j = 0; j < R; ++j) { l64[j] = 0.0; h64[j] = 0.0; m64[j] = 1.0; }
+    for (int j = 0; j < R; ++j) { l64[j] = 0.0; h64[j] = 0.0; m64[j] = 1.0; a64[j] = 0.0; c64[j] = 0.0; }
     if constexpr (C::kSV == SV_TRI) {
         // Moebius product of this chunk: v_i = [[1, -a_i c_{i-1}], [1, 0]] v_{i-1}
         double a = 1, b = 0, c = 0, d = 1;
@@ -331,56 +373,57 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, i
             l64[j] = ai * dinv;
             h64[j] = ci * dinv;
             m64[j] = dinv;
-            if constexpr (C::kMixed) {
-                cf.al[j] = ai;
-                cf.cu[j] = ci;
-            }
+            a64[j] = ai;
+            c64[j] = ci;
         }
     } else if constexpr (C::kSV == SV_LOWER) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int64_t i = s + j;
             l64[j] = (i >= 1 && i < M) ? band(op, op.off_sl, i) : 0.0;
-            if constexpr (C::kMixed) cf.al[j] = l64[j];
+            a64[j] = l64[j];
         }
     } else if constexpr (C::kSV == SV_UPPER) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int64_t i = s + j;
             h64[j] = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
-            if constexpr (C::kMixed) cf.cu[j] = h64[j];
+            c64[j] = h64[j];
         }
     }
-    if constexpr (C::kMixed) {
-#pragma unroll
-        for (int j = 0; j < R; ++j) cf.m[j] = (S)m64[j];
-    } else {
+    if constexpr (!C::kMixed) {
 #pragma unroll
         for (int j = 0; j < R; ++j)
 #pragma unroll
-            for (int k = 0; k < C::NB; ++k) cf.w[k][j] *= m64[j];
+            for (int k = 0; k < C::NB; ++k) w[k][j] *= m64[j];
     }
-    if constexpr (C::kFwd) {
-        double p = 1.0;
+    double sc[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) sc[j] = C::kScale ? scale_factor(op.scale_kind, s + j, op.lshift, op.scale_s) : 1.0;
+    if constexpr (C::kTbl) {
+        const int T = cf.T, tt = cf.tt;
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            p = -l64[j] * p;
-            cf.l[j] = (S)l64[j];
-            cf.F[j] = (S)p;
-        }
-    }
-    if constexpr (C::kBwd) {
-        double p = 1.0;
 #pragma unroll
-        for (int j = R - 1; j >= 0; --j) {
-            p = -h64[j] * p;
-            cf.h[j] = (S)h64[j];
-            cf.G[j] = (S)p;
+            for (int k = 0; k < C::NB; ++k) table[(k * R + j) * T + tt] = w[k][j];
+            if constexpr (C::kFwd) table[(C::P_L * R + j) * T + tt] = l64[j];
+            if constexpr (C::kBwd) table[(C::P_H * R + j) * T + tt] = h64[j];
+            if constexpr (C::kScale) table[(C::P_SC * R + j) * T + tt] = sc[j];
         }
-    }
-    if constexpr (C::kScale) {
+    } else {
 #pragma unroll
-        for (int j = 0; j < R; ++j) cf.sc[j] = scale_factor(op.scale_kind, s + j, op.lshift, op.scale_s);
+        for (int j = 0; j < R; ++j) {
+#pragma unroll
+            for (int k = 0; k < C::NB; ++k) cf.w_[k][j] = w[k][j];
+            if constexpr (C::kFwd) cf.l_[j] = (S)l64[j];
+            if constexpr (C::kBwd) cf.h_[j] = (S)h64[j];
+            if constexpr (C::kScale) cf.sc_[j] = sc[j];
+            if constexpr (C::kMixed) {
+                cf.m_[j] = (S)m64[j];
+                if constexpr (C::kFwd) cf.al_[j] = a64[j];
+                if constexpr (C::kBwd) cf.cu_[j] = c64[j];
+            }
+        }
     }
 }
 
@@ -469,39 +512,48 @@ __device__ __forceinline__ void store_segment(const JwIO& io, int64_t sys, int64
     }
 }
 
-// ---- Unit-diagonal solve of one chunk given the coefficient arrays.
-// Forward: z_j = x_j - l_j z_{j-1}; backward: x_j = z_j - h_j x_{j+1};
-// chunk-boundary couplings through the affine scans (F, G are the in-chunk
-// products of -l and -h).
-template <int R, int SV, class V, class S, int NF, int NBW>
-__device__ __forceinline__ void chunk_solve(GroupCtx& g, const S (&l)[NF], const S (&F)[NF], const S (&h)[NBW],
-                                            const S (&G)[NBW], V (&x)[R])
+// ---- Unit-diagonal solve of one chunk.
+// Forward: z_j = x_j - l_j z_{j-1}; backward: x_j = z_j - h_j x_{j+1}.  The
+// chunk-boundary couplings go through the affine scans; the in-chunk products
+// F_j = prod_{k<=j}(-l_k) and G_j = prod_{k>=j}(-h_k) are rebuilt on the fly.
+template <int R, int SV, class V, class S, class LF, class HF>
+__device__ __forceinline__ void chunk_solve(GroupCtx& g, LF lget, HF hget, V (&x)[R])
 {
     using O = VOps<V>;
     constexpr bool FWD = (SV == SV_LOWER || SV == SV_TRI);
     constexpr bool BWD = (SV == SV_UPPER || SV == SV_TRI);
     if constexpr (FWD) {
-        V z[R];
-        z[0] = x[0];
+        // in place: x holds z after the local forward pass
+        S A = -lget(0);
 #pragma unroll
-        for (int j = 1; j < R; ++j) z[j] = O::fma(-l[j], z[j - 1], x[j]);
-        const V pin = group_affine_scan<V, S, true>(g, F[R - 1], z[R - 1]);
-        if constexpr (SV == SV_LOWER) {
-#pragma unroll
-            for (int j = 0; j < R; ++j) x[j] = O::fma(F[j], pin, z[j]);
-        } else {
-            x[R - 1] = O::fma(F[R - 1], pin, z[R - 1]);
-#pragma unroll
-            for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-h[j], x[j + 1], O::fma(F[j], pin, z[j]));
+        for (int j = 1; j < R; ++j) {
+            const S lj = lget(j);
+            x[j] = O::fma(-lj, x[j - 1], x[j]);
+            A = -lj * A;
         }
-    } else if constexpr (SV == SV_UPPER) {
+        const V pin = group_affine_scan<V, S, true>(g, A, x[R - 1]);
+        S p = S(1);
 #pragma unroll
-        for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-h[j], x[j + 1], x[j]);
+        for (int j = 0; j < R; ++j) {
+            p = -lget(j) * p;
+            x[j] = O::fma(p, pin, x[j]);
+        }
+    }
+    if constexpr (SV == SV_UPPER || SV == SV_TRI) {
+#pragma unroll
+        for (int j = R - 2; j >= 0; --j) x[j] = O::fma(-hget(j), x[j + 1], x[j]);
     }
     if constexpr (BWD) {
-        const V q = group_affine_scan<V, S, false>(g, G[0], x[0]);
+        S Ab = S(1);
 #pragma unroll
-        for (int j = 0; j < R; ++j) x[j] = O::fma(G[j], q, x[j]);
+        for (int j = 0; j < R; ++j) Ab = -hget(j) * Ab;
+        const V q = group_affine_scan<V, S, false>(g, Ab, x[0]);
+        S p = S(1);
+#pragma unroll
+        for (int j = R - 1; j >= 0; --j) {
+            p = -hget(j) * p;
+            x[j] = O::fma(p, q, x[j]);
+        }
     }
 }
 
@@ -532,15 +584,15 @@ __device__ __forceinline__ void mixed_solve(GroupCtx& g, const JwCoef<C>& cf, in
 #pragma unroll
             for (int j = 0; j < R; ++j) {
                 V mx = x[j];
-                if constexpr (C::kFwd) mx = O::fma(cf.al[j], j > 0 ? x[j - 1] : prev, mx);
-                if constexpr (C::kBwd) mx = O::fma(cf.cu[j], j < R - 1 ? x[j + 1] : next, mx);
+                if constexpr (C::kFwd) mx = O::fma(cf.al_[j], j > 0 ? x[j - 1] : prev, mx);
+                if constexpr (C::kBwd) mx = O::fma(cf.cu_[j], j < R - 1 ? x[j + 1] : next, mx);
                 r[j] = O::fma(-1.0, mx, gv[j]);
             }
         }
         VF d[R];
 #pragma unroll
-        for (int j = 0; j < R; ++j) d[j] = OF::mul(cf.m[j], to_f32(r[j]));
-        chunk_solve<R, SV, VF, float, C::NF, C::NBW>(g, cf.l, cf.F, cf.h, cf.G, d);
+        for (int j = 0; j < R; ++j) d[j] = OF::mul(cf.m_[j], to_f32(r[j]));
+        chunk_solve<R, SV, VF, float>(g, [&](int j) { return cf.l_[j]; }, [&](int j) { return cf.h_[j]; }, d);
 #pragma unroll
         for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
     }
@@ -589,20 +641,20 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
         V x[R];
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-            V acc = O::mul(cf.w[0][j], be[j]);
+            V acc = O::mul(cf.w(0, j), be[j]);
 #pragma unroll
-            for (int k = 1; k < C::NB; ++k) acc = O::fma(cf.w[k][j], be[j + k], acc);
+            for (int k = 1; k < C::NB; ++k) acc = O::fma(cf.w(k, j), be[j + k], acc);
             x[j] = acc;
         }
         if constexpr (C::kMixed) {
             mixed_solve<C>(g, cf, op.refine_sweeps, x);
         } else if constexpr (C::kSV != SV_NONE) {
-            chunk_solve<R, C::kSV, V, double, C::NF, C::NBW>(g, cf.l, cf.F, cf.h, cf.G, x);
+            chunk_solve<R, C::kSV, V, double>(g, [&](int j) { return cf.l(j); }, [&](int j) { return cf.h(j); }, x);
         }
         if (C::kSV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
         if constexpr (C::kScale) {
 #pragma unroll
-            for (int j = 0; j < R; ++j) x[j] = O::mul(cf.sc[j], x[j]);
+            for (int j = 0; j < R; ++j) x[j] = O::mul(cf.sc(j), x[j]);
         }
         __syncwarp();  // every lane has read `cur`
 #pragma unroll
@@ -615,7 +667,54 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
 }
 
 template <class C>
-__global__ void __launch_bounds__(256) jw_step_kernel(const JwOperator op, const JwIO io, const int W)
+__global__ void __launch_bounds__(C::kMaxThreads) jw_step_kernel(const JwOperator op, const JwIO io, const int W)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using V = typename C::V;
+    const int warp = threadIdx.x >> 5;
+    const int G = blockDim.x / (32 * W);
+    const int grp = warp / W;
+    GroupCtx g;
+    g.lane = threadIdx.x & 31;
+    g.wg = warp - grp * W;
+    g.W = W;
+    g.nthr = 32 * W;
+    g.bar_id = 1 + grp;
+    g.seq = 0;
+    constexpr size_t per_warp = jw_smem_per_warp<C>();
+    double* table = reinterpret_cast<double*>(smem_raw);
+    unsigned char* data = smem_raw + jw_table_bytes<C>(W);
+    V* buf0 = reinterpret_cast<V*>(data + (size_t)warp * per_warp);
+    V* buf1 = buf0 + C::SEG;
+    g.scratch = reinterpret_cast<double*>(data + (size_t)G * W * per_warp) + (size_t)grp * W * kScratchPerWarp;
+
+    const int64_t s = (int64_t)(g.wg * 32 + g.lane) * C::kR;
+    JwCoef<C> cf;
+    cf.tbl = table;
+    cf.T = 32 * W;
+    cf.tt = g.wg * 32 + g.lane;
+    if constexpr (C::kTbl) {
+        // every group of the CTA solves with the same matrix: group 0 builds
+        // the shared table once
+        if (grp == 0) jw_prologue<C>(op, g, s, cf, table);
+        __syncthreads();
+    } else {
+        jw_prologue<C>(op, g, s, cf);
+    }
+    const int64_t sys0 = (int64_t)blockIdx.x * G + grp;
+    const int64_t step = (int64_t)gridDim.x * G;
+    jw_run_systems<C>(op, io, g, cf, buf0, buf1, sys0, step);
+}
+
+// ---- Uneven batch: one persistent launch over many matrices of different
+// sizes.  Each group takes (entry, system range) items from a global counter
+// (largest items first), refactors when the entry changes and streams the
+// item's systems.  Item fetch: the group leader's atomicAdd is broadcast
+// through two alternating shared slots, one barrier per fetch.
+template <class C>
+__global__ void __launch_bounds__(256) jw_batch_kernel(const BatchEntryDev* __restrict__ entries,
+                                                      const WorkItem* __restrict__ items, const int nitems,
+                                                      unsigned int* __restrict__ counter, const int W)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using V = typename C::V;
@@ -632,14 +731,43 @@ __global__ void __launch_bounds__(256) jw_step_kernel(const JwOperator op, const
     constexpr size_t per_warp = jw_smem_per_warp<C>();
     V* buf0 = reinterpret_cast<V*>(smem_raw + (size_t)warp * per_warp);
     V* buf1 = buf0 + C::SEG;
-    g.scratch = reinterpret_cast<double*>(smem_raw + (size_t)G * W * per_warp) + (size_t)grp * W * kScratchPerWarp;
-
+    double* scratch_all = reinterpret_cast<double*>(smem_raw + (size_t)G * W * per_warp);
+    g.scratch = scratch_all + (size_t)grp * W * kScratchPerWarp;
+    int* slots = reinterpret_cast<int*>(scratch_all + (size_t)G * W * kScratchPerWarp) + 2 * grp;
     const int64_t s = (int64_t)(g.wg * 32 + g.lane) * C::kR;
+
     JwCoef<C> cf;
-    jw_prologue<C>(op, g, s, cf);
-    const int64_t sys0 = (int64_t)blockIdx.x * G + grp;
-    const int64_t step = (int64_t)gridDim.x * G;
-    jw_run_systems<C>(op, io, g, cf, buf0, buf1, sys0, step);
+    int cur_entry = -1;
+    int par = 0;
+    for (;;) {
+        int it = 0;
+        if (W == 1) {
+            if (g.lane == 0) it = (int)atomicAdd(counter, 1u);
+            it = __shfl_sync(FULL, it, 0);
+        } else {
+            if (g.wg == 0 && g.lane == 0) slots[par] = (int)atomicAdd(counter, 1u);
+            __syncwarp();
+            group_bar(g.bar_id, g.nthr);
+            it = slots[par];
+            par ^= 1;
+        }
+        if (it >= nitems) break;
+        const WorkItem wi = items[it];
+        const JwOperator op = entries[wi.entry].op;
+        JwIO io = entries[wi.entry].io;
+        io.nsys = wi.y1;
+        if (wi.entry != cur_entry) {
+            jw_prologue<C>(op, g, s, cf);
+            cur_entry = wi.entry;
+        }
+        jw_run_systems<C>(op, io, g, cf, buf0, buf1, wi.y0, 1);
+    }
+}
+
+template <class C>
+__host__ size_t jw_batch_smem_bytes(int W, int G)
+{
+    return jw_smem_bytes<C>(W, G) + (size_t)G * 2 * sizeof(int);
 }
 
 }  // namespace pfb

@@ -38,4 +38,16 @@ struct JwIO {
     int accumulate;               // output += result
 };
 
+// Uneven batches: one descriptor per entry (systems sharing one matrix) and
+// a work list of (entry, system range) items consumed through a counter.
+struct BatchEntryDev {
+    JwOperator op;
+    JwIO io;
+};
+struct WorkItem {
+    int entry;
+    int pad;
+    int64_t y0, y1;  // systems [y0, y1) of the entry
+};
+
 }  // namespace pfb

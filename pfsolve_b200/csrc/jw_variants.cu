@@ -19,11 +19,15 @@ static void launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const
     jw_step_kernel<C><<<grid, block, smem, st>>>(op, io, W);
 }
 
-#define PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, P)                                                         \
-    JwVariant{R, KL, KU, SV, LIN, LOUT, SC, P,                                                           \
-              (const void*)&jw_step_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>,                     \
-              &smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>, &launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P>>}
+#define PFB_VT(R, KL, KU, SV, LIN, LOUT, SC, P, T)                                                     \
+    JwVariant{R, KL, KU, SV, LIN, LOUT, SC, P, T, JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>::kMaxThreads,  \
+              (const void*)&jw_step_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>,                    \
+              &smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>, &launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>}
+#define PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, P) PFB_VT(R, KL, KU, SV, LIN, LOUT, SC, P, false)
 #define PFB_V(R, KL, KU, SV, LIN, LOUT, SC) PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, PREC_F64)
+// coefficient-table variants (FP64), rows per thread 4 and 8
+#define PFB_T2(KL, KU, SV, LIN, LOUT, SC) \
+    PFB_VT(4, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true), PFB_VT(8, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true)
 
 // Rows-per-thread choices for the single-application (drop-in) variants.
 #define PFB_R4(KL, KU, SV, LIN, LOUT, SC) \
@@ -73,13 +77,23 @@ static const JwVariant kVariants[] = {
     PFB_M2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
     PFB_M2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
     PFB_M2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
+    // coefficient-table variants for the single-matrix launches
+    PFB_T2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),
+    PFB_T2(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),
+    PFB_T2(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),
+    PFB_T2(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_T2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_T2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
+    PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
+    PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true),
+    PFB_T2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true),
 };
 
-const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)
+const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC, int TBL)
 {
     for (const JwVariant& v : kVariants)
         if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
-            v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC)
+            v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC && v.TBL == (TBL ? 1 : 0))
             return &v;
     return nullptr;
 }

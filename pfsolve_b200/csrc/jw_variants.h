@@ -11,16 +11,28 @@ namespace pfb {
 using JwKernelFn = void (*)(JwOperator, JwIO, int);
 
 struct JwVariant {
-    int R, KL, KU, SV, LIN, LOUT, SCALE, PREC;
+    int R, KL, KU, SV, LIN, LOUT, SCALE, PREC, TBL;
+    int max_threads;                   // launch bound of the entry
     const void* func;                  // __global__ entry (for attributes / occupancy)
     size_t (*smem_bytes)(int W, int G);
     void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op, const JwIO& io, int W);
 };
 
 // Find a variant; nullptr when that combination was not compiled.
-const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC = 0);
+const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC = 0,
+                                int TBL = 0);
 // All compiled variants (for tests and the autotuner).
 const JwVariant* jw_variants(int* count);
+
+// Persistent uneven-batch kernels (one per operator shape).
+struct BatchVariant {
+    int R, KL, KU, SV, LIN, LOUT, SCALE, PREC;
+    const void* func;
+    size_t (*smem_bytes)(int W, int G);
+    void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const BatchEntryDev* entries,
+                   const WorkItem* items, int nitems, unsigned int* counter, int W);
+};
+const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC);
 
 // Standalone kernels of the block and generic-bandwidth dgbmv applications.
 struct BlockArgs {

@@ -126,3 +126,36 @@ def config3(seed=2, M=512, B=131072) -> Workload:
 def config4_sizes(lmax=511, Nmax=512):
     ls = np.arange(lmax + 1)
     return ls, Nmax - ls // 2, 2 * ls + 1
+
+
+@dataclass
+class UnevenStep:
+    """One spectral timestep: harmonic degrees l = 0..lmax, N_l rows and
+    2l+1 complex RHS per degree; coefficients as config 1 per degree."""
+    ls: np.ndarray
+    Ns: np.ndarray
+    nsys: np.ndarray
+    jw_bands: list      # per degree, reference layout
+    dgbmv: list         # per degree, band-major (3 bands)
+    rhs_offsets: np.ndarray  # per degree, element offset of its XXII block in `rhs`
+    rhs: np.ndarray     # all degrees' XXII right-hand sides, concatenated
+    scale_s: float
+
+
+def config4(seed=3, lmax=511, Nmax=512, scale_s=-0.5, rhs=True) -> UnevenStep:
+    """Uneven batch of one timestep: N_l = Nmax - floor(l/2), 2l+1 complex RHS
+    ~N(0,1) per degree (XXII), V 3-band ~U(-1,1) and upper-bidiagonal M
+    (diag ~U(1,2), super ~U(-0.5,0.5)) per degree; SphLaplA with lshift = l."""
+    rng = np.random.default_rng(seed)
+    ls, Ns, nsys = config4_sizes(lmax, Nmax)
+    jw, dg, offs = [], [], []
+    off = 0
+    for l, N, ns in zip(ls, Ns, nsys):
+        d = rng.uniform(1.0, 2.0, N)
+        s = rng.uniform(-0.5, 0.5, N)
+        jw.append(permute_bands(upper_bidiag_bands(d, s), N))
+        dg.append(band_major(rng, N, 1, 1))
+        offs.append(off)
+        off += 2 * N * ns
+    data = rng.standard_normal(off) if rhs else np.zeros(0)
+    return UnevenStep(ls, Ns, nsys, jw, dg, np.array(offs, dtype=np.int64), data, scale_s)

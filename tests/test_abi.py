@@ -44,9 +44,10 @@ PROBE = r"""
 #include "pfsolve_b200.h"
 #define F(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
 int main(void) {
-  printf("cfg %zu\nlp %zu\napp %zu\nkjw %zu\nkdg %zu\nkbl %zu\n", sizeof(PfSolveConfiguration),
-         sizeof(PfSolveLaunchParams), sizeof(PfSolveApplication), sizeof(PfSolve_MapKey_JonesWorland),
-         sizeof(PfSolve_MapKey_dgbmv), sizeof(PfSolve_MapKey_block));
+  printf("cfg %zu\nlp %zu\napp %zu\nkjw %zu\nkdg %zu\nkbl %zu\nbent %zu\nbdesc %zu\n",
+         sizeof(PfSolveConfiguration), sizeof(PfSolveLaunchParams), sizeof(PfSolveApplication),
+         sizeof(PfSolve_MapKey_JonesWorland), sizeof(PfSolve_MapKey_dgbmv), sizeof(PfSolve_MapKey_block),
+         sizeof(PfSolveBatchEntry), sizeof(PfSolveBatchDesc));
   F(PfSolveConfiguration, jw_type) F(PfSolveConfiguration, jw_control_bitmask)
   F(PfSolveConfiguration, scaleC) F(PfSolveConfiguration, doublePrecision)
   F(PfSolveConfiguration, outputBufferStride) F(PfSolveConfiguration, numConsecutiveJWIterations)
@@ -71,6 +72,8 @@ def test_ctypes_layout_matches_c(tmp_path):
     assert int(out["kjw"]) == ctypes.sizeof(capi.MapKeyJW)
     assert int(out["kdg"]) == ctypes.sizeof(capi.MapKeyDgbmv)
     assert int(out["kbl"]) == ctypes.sizeof(capi.MapKeyBlock)
+    assert int(out["bent"]) == ctypes.sizeof(capi.PfSolveBatchEntry)
+    assert int(out["bdesc"]) == ctypes.sizeof(capi.PfSolveBatchDesc)
     for key, val in out.items():
         if "." in key:
             T, f = key.split(".")
