@@ -466,3 +466,28 @@ void pfo_rel_errors(const double* a, const double* ref, int64_t M, int64_t batch
     *rel_l2_max = worst_l2;
     *rel_max = (rmax > 0) ? dmax / rmax : dmax;
 }
+
+/* Relative errors for double-double storage ({hi, lo} pairs), in __float128. */
+void pfo_rel_errors_dd(const double* a, const double* ref, int64_t M, int64_t batch, int64_t stride,
+                       int64_t offset, double* rel_l2_max, double* rel_max)
+{
+    double worst = 0, dmax = 0, rmax = 0;
+    for (int64_t y = 0; y < batch; y++) {
+        q_t num = 0, den = 0;
+        for (int64_t i = 0; i < M; i++) {
+            const int64_t k = offset + y * stride + i;
+            const q_t va = (q_t)a[2 * k] + (q_t)a[2 * k + 1];
+            const q_t vr = (q_t)ref[2 * k] + (q_t)ref[2 * k + 1];
+            const q_t d = va - vr;
+            num += d * d;
+            den += vr * vr;
+            const double ad = fabs((double)d), ar = fabs((double)vr);
+            if (ad > dmax) dmax = ad;
+            if (ar > rmax) rmax = ar;
+        }
+        const double e = (den > 0) ? (double)sqrtq(num / den) : (double)sqrtq(num);
+        if (e > worst) worst = e;
+    }
+    *rel_l2_max = worst;
+    *rel_max = (rmax > 0) ? dmax / rmax : dmax;
+}

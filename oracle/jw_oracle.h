@@ -114,6 +114,10 @@ double pfo_scale_factor(int kind, int64_t x, int lshift, double s);
 void pfo_rel_errors(const double* a, const double* ref, int64_t M, int64_t batch, int64_t stride,
                     int64_t offset, double* rel_l2_max, double* rel_max);
 
+/* Same for double-double storage: every value a {hi, lo} pair. */
+void pfo_rel_errors_dd(const double* a, const double* ref, int64_t M, int64_t batch, int64_t stride,
+                       int64_t offset, double* rel_l2_max, double* rel_max);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,6 +173,8 @@ def lib():
     L.pfo_rel_errors.argtypes = [dp, dp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                  dp, dp]
     L.pfo_rel_errors.restype = None
+    L.pfo_rel_errors_dd.argtypes = L.pfo_rel_errors.argtypes
+    L.pfo_rel_errors_dd.restype = None
     _lib = L
     return L
 
@@ -265,6 +267,22 @@ def rel_errors(a, ref, M, batch, stride, offset=0):
     e2 = ctypes.c_double()
     lib().pfo_rel_errors(_dptr(a), _dptr(r), M, batch, stride, offset, ctypes.byref(e1), ctypes.byref(e2))
     return e1.value, e2.value
+
+
+def rel_errors_dd(a, ref, M, batch, stride, offset=0):
+    """rel_errors for double-double arrays ({hi, lo} pairs), evaluated in __float128."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    r = np.ascontiguousarray(ref, dtype=np.float64)
+    e1 = ctypes.c_double()
+    e2 = ctypes.c_double()
+    lib().pfo_rel_errors_dd(_dptr(a), _dptr(r), M, batch, stride, offset, ctypes.byref(e1), ctypes.byref(e2))
+    return e1.value, e2.value
+
+
+def to_dd(x):
+    """FP64 array -> double-double pairs {x, 0}."""
+    x = np.asarray(x, dtype=np.float64)
+    return np.stack([x, np.zeros_like(x)], -1).ravel()
 
 
 # --------------------------------------------------------------------------

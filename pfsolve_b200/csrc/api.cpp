@@ -344,6 +344,7 @@ PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* l
         io.M = c.M_size;
         return launch_jw_variant(s, op, io, stream);
     }
+    if (s->prec) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     DgbmvArgs a;
     a.A = static_cast<const double*>(r.bands);
     a.x = static_cast<double*>(r.rhs);
@@ -458,10 +459,13 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
             }
         }
     }
-    // Precision: this build runs the FP64 path; other storage modes are
-    // rejected until their kernels are selected here.
-    const bool fp64 = c.doublePrecision && !c.quadDoubleDoublePrecision && !c.quadDoubleDoublePrecisionDoubleMemory &&
-                      !c.doublePrecisionFloatMemory;
+    // Precision: FP64 (doublePrecision, optionally with FP32-solve refinement),
+    // double-double storage (quadDoubleDoublePrecision) or double-double
+    // arithmetic on FP64 storage (quadDoubleDoublePrecisionDoubleMemory).
+    const bool ddmem = c.quadDoubleDoublePrecision != 0;
+    const bool ddf64 = !ddmem && c.quadDoubleDoublePrecisionDoubleMemory != 0;
+    const bool fp64 = (c.doublePrecision && !ddmem && !ddf64 && !c.doublePrecisionFloatMemory) || ddmem || ddf64;
+    const int dd_prec = ddmem ? 2 : (ddf64 ? 3 : 0);
     PfSolveResult r = PFSOLVE_SUCCESS;
     if (c.jw_type >= 10) {
         s->kind = APP_JW;
@@ -477,7 +481,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
             else {
                 s->mvj = L.mvj;
                 s->sv = L.sv;
-                s->prec = (c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? 1 : 0;
+                s->prec = dd_prec ? dd_prec : ((c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? 1 : 0);
                 s->refine_sweeps = 1 + c.mixedPrecisionRefinement;
                 s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
                 s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
@@ -493,11 +497,13 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
         else if (c.KU < 0 || c.KU >= c.LDA) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
         else {
             const int kl = c.LDA - 1 - c.KU;
-            if (kl <= 2 && c.KU <= 2 && c.M_size <= kMaxRows) {
+            if (dd_prec && !(kl == 1 && c.KU == 1)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            else if (kl <= 2 && c.KU <= 2 && c.M_size <= kMaxRows) {
                 s->KL = kl;
                 s->KU = c.KU;
                 s->sv = SV_NONE;
                 s->mvj = MVJ_NONE;
+                s->prec = dd_prec;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
                 if (s->R < 4) s->R = 4;
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
@@ -507,7 +513,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
     } else if (c.block > 0) {
         s->kind = APP_BLOCK;
         const int bt = c.block % 10, acc = (c.block / 10) % 10, sk = c.block / 100;
-        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (!fp64 || dd_prec) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (bt < 1 || bt > 7 || (acc != 0 && acc != 2) || sk > 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (acc == 2 && bt == 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     } else {

@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "dd.cuh"
+
 namespace pfb {
 
 constexpr unsigned FULL = 0xffffffffu;
@@ -65,6 +67,27 @@ template <> struct VOps<float2> {
         return make_float2(__shfl_down_sync(FULL, v.x, d), __shfl_down_sync(FULL, v.y, d));
     }
 };
+
+template <> struct VOps<dd> {
+    static __device__ __forceinline__ dd zero() { return dd(0.0, 0.0); }
+    static __device__ __forceinline__ dd mul(dd a, dd v) { return a * v; }
+    static __device__ __forceinline__ dd fma(dd a, dd v, dd w) { return dd_fma(a, v, w); }
+    static __device__ __forceinline__ dd add(dd v, dd w) { return v + w; }
+    static __device__ __forceinline__ dd shfl_up(dd v, int d)
+    {
+        return dd(__shfl_up_sync(FULL, v.hi, d), __shfl_up_sync(FULL, v.lo, d));
+    }
+    static __device__ __forceinline__ dd shfl_down(dd v, int d)
+    {
+        return dd(__shfl_down_sync(FULL, v.hi, d), __shfl_down_sync(FULL, v.lo, d));
+    }
+};
+
+// Shuffles of the scan multiplier type (double, float or dd).
+template <class S> __device__ __forceinline__ S shfl_up_s(S v, int d) { return __shfl_up_sync(FULL, v, d); }
+template <class S> __device__ __forceinline__ S shfl_down_s(S v, int d) { return __shfl_down_sync(FULL, v, d); }
+template <> __device__ __forceinline__ dd shfl_up_s<dd>(dd v, int d) { return VOps<dd>::shfl_up(v, d); }
+template <> __device__ __forceinline__ dd shfl_down_s<dd>(dd v, int d) { return VOps<dd>::shfl_down(v, d); }
 
 // FP64 <-> FP32 value conversions (round to nearest).
 __device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v); }

@@ -188,7 +188,7 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
     using O = VOps<V>;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        S Ap = FORWARD ? __shfl_up_sync(FULL, A, d) : __shfl_down_sync(FULL, A, d);
+        S Ap = FORWARD ? shfl_up_s<S>(A, d) : shfl_down_s<S>(A, d);
         V Bp = FORWARD ? O::shfl_up(B, d) : O::shfl_down(B, d);
         bool take = FORWARD ? (g.lane >= d) : (g.lane + d < 32);
         if (take) {
@@ -196,7 +196,7 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
             A = A * Ap;
         }
     }
-    S Ae = FORWARD ? __shfl_up_sync(FULL, A, 1) : __shfl_down_sync(FULL, A, 1);
+    S Ae = FORWARD ? shfl_up_s<S>(A, 1) : shfl_down_s<S>(A, 1);
     V Be = FORWARD ? O::shfl_up(B, 1) : O::shfl_down(B, 1);
     const bool first = FORWARD ? (g.lane == 0) : (g.lane == 31);
     if (first) {
@@ -209,7 +209,7 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
         const bool agg = FORWARD ? (g.lane == 31) : (g.lane == 0);
         if (agg) {
             double* my = g.warp_area(g.wg) + slot;
-            my[0] = (double)A;
+            store_v<S>(my, A);
             store_v<V>(my + 2, B);
         }
         __syncwarp();
@@ -217,12 +217,12 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
         if (FORWARD) {
             for (int w = 0; w < g.wg; ++w) {
                 const double* o = g.warp_area(w) + slot;
-                win = O::fma((S)o[0], win, load_v<V>(o + 2));
+                win = O::fma(load_v<S>(o), win, load_v<V>(o + 2));
             }
         } else {
             for (int w = g.W - 1; w > g.wg; --w) {
                 const double* o = g.warp_area(w) + slot;
-                win = O::fma((S)o[0], win, load_v<V>(o + 2));
+                win = O::fma(load_v<S>(o), win, load_v<V>(o + 2));
             }
         }
         g.seq++;

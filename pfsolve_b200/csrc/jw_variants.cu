@@ -2,6 +2,7 @@
 // standalone block / generic dgbmv kernels.
 #include <vector>
 
+#include "dd_kernel.cuh"
 #include "jw_kernel.cuh"
 #include "jw_variants.h"
 
@@ -28,6 +29,26 @@ static void launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const
 // coefficient-table variants (FP64), rows per thread 4 and 8
 #define PFB_T2(KL, KU, SV, LIN, LOUT, SC) \
     PFB_VT(4, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true), PFB_VT(8, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true)
+
+// double-double variants: PREC 2 = dd storage, PREC 3 = dd arithmetic on FP64 storage
+template <class C>
+static size_t dd_smem_fn(int W, int G)
+{
+    return dd_smem_bytes<C>(W, G);
+}
+template <class C>
+static void dd_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op, const JwIO& io,
+                         int W)
+{
+    jw_dd_kernel<C><<<grid, block, smem, st>>>(op, io, W);
+}
+#define PFB_DDV(R, KL, KU, SV, MEM)                                                                     \
+    JwVariant{R, KL, KU, SV, LAY_REAL, LAY_REAL, 0, (MEM) ? 2 : 3, 0, 256,                              \
+              (const void*)&jw_dd_kernel<DdCfg<R, KL, KU, SV, MEM>>, &dd_smem_fn<DdCfg<R, KL, KU, SV, MEM>>, \
+              &dd_launch_fn<DdCfg<R, KL, KU, SV, MEM>>}
+#define PFB_DD(KL, KU, SV) \
+    PFB_DDV(4, KL, KU, SV, true), PFB_DDV(8, KL, KU, SV, true), PFB_DDV(4, KL, KU, SV, false), \
+        PFB_DDV(8, KL, KU, SV, false)
 
 // Rows-per-thread choices for the single-application (drop-in) variants.
 #define PFB_R4(KL, KU, SV, LIN, LOUT, SC) \
@@ -87,6 +108,16 @@ static const JwVariant kVariants[] = {
     PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
     PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true),
     PFB_T2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true),
+    // double-double (quad emulation), real systems
+    PFB_DD(0, 0, SV_TRI),
+    PFB_DD(0, 1, SV_LOWER),
+    PFB_DD(0, 1, SV_NONE),
+    PFB_DD(0, 0, SV_LOWER),
+    PFB_DD(1, 0, SV_UPPER),
+    PFB_DD(1, 0, SV_NONE),
+    PFB_DD(0, 0, SV_UPPER),
+    PFB_DD(1, 1, SV_UPPER),
+    PFB_DD(1, 1, SV_NONE),
 };
 
 const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC, int TBL)
