@@ -170,7 +170,7 @@ def gpu_arm(args, rank, world):
     dg = App(device=local, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), LDA=5, KU=2, KL=2,
              doublePrecision=1)
     jw = App(device=local, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * nc), upperBanded=2, jw_type=13,
-             doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows)
+             doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows, kernelPath=args.path)
     bl = App(device=local, buffer=rhs, outputBuffer=out, M_size=M, size=(M, nc), block=7, doublePrecision=1)
     lps = [dg.launch_params(), jw.launch_params(), bl.launch_params()]
     apps = [dg, jw, bl]
@@ -211,7 +211,7 @@ def gpu_arm(args, rank, world):
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_case": True, "ncplx": nc, "ms_per_step": ms_max, "gbs": achieved,
-                              "gpu_launches": int(launches)}), flush=True)
+                              "gpu_launches": int(launches), "kernel": jw.shape()}), flush=True)
         return
     host_in = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
     host_in.copy_(rhs.cpu())
@@ -248,7 +248,7 @@ def gpu_arm(args, rank, world):
                 "data": "synthetic (seeded, N(0,1) complex RHS, dominant tridiagonal, U(-1,1) 5-band)",
                 "config": {"workload": "config2: N=1024, 65536 complex RHS per GPU, XXII in -> packed out, "
                                        "dgbmv(5) + tridiagonal JW step (jw_type 13) fused, one kernel per step",
-                           "rhs_per_gpu": nc, "l2": "inputs 2 GiB > L2, no flush",
+                           "rhs_per_gpu": nc, "l2": "inputs 2 GiB > L2, no flush", "kernel": jw.shape(),
                            "parallelism": f"replicas x{world} (independent RHS shards, no collective)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
@@ -346,6 +346,8 @@ def main():
     ap.add_argument("--profile", action="store_true", help="kernel steps only: no e2e leg, no CPU baseline")
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1],
+                    help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu = True

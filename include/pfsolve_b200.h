@@ -167,7 +167,9 @@ typedef struct {
     /* --- extensions (0 keeps the reference behaviour) --- */
     int mixedPrecisionRefinement; /* 1..3 with doublePrecision: FP32 factor-solve plus this many
                                      FP64 residual refinement sweeps, FP64 storage (0: plain FP64) */
-    int rowsPerThread;            /* 0: autotuned; else 2, 4, 8 or 16 */
+    int rowsPerThread;            /* 0: autotuned; else 2, 4, 8, 16 or 32 (32: streaming kernel only) */
+    int kernelPath;               /* 0: streaming kernel wherever a launch allows it, else the group
+                                     kernel; 1: group kernel only */
 } PfSolveConfiguration;
 
 /* Launch-time values (pfSolve_Structs.h:383-449). */
@@ -313,6 +315,22 @@ PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
 
 /* Number of kernel launches this library has enqueued since load (all apps). */
 PFSOLVE_API uint64_t PfSolveLaunchCount(void);
+
+/* Status of the bounded completion waits inside this library's kernels on
+ * the current device since the previous call: PFSOLVE_SUCCESS, or
+ * PFSOLVE_ERROR_DEVICE_FAULT when a wait ran out and a kernel stopped early
+ * (its output is incomplete).  Synchronises with the device.  No counterpart
+ * in the reference, whose generated kernels have no such waits. */
+PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
+
+/* Kernel shape a JW or dgbmv plan chose: streaming = 1 when its launches use
+ * the TMA-staged streaming kernel wherever their buffers allow it, with
+ * rowsPerThread x warpsPerSystem rows per group and groupsPerCTA groups;
+ * streaming = 0: the group kernel's shape.  No counterpart in the reference. */
+PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
+                                          int* warpsPerSystem, int* groupsPerCTA);
+/* Launches that ran on the streaming kernel since load (all apps). */
+PFSOLVE_API uint64_t PfSolveStreamingLaunchCount(void);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,13 @@ class App:
     def sync(self):
         check(self._lib.PfSolveSync(ctypes.byref(self.app)), "PfSolveSync")
 
+    def shape(self) -> dict:
+        """Kernel shape of this plan (``PfSolveGetShape``)."""
+        v = [ctypes.c_int() for _ in range(4)]
+        check(self._lib.PfSolveGetShape(ctypes.byref(self.app), *[ctypes.byref(x) for x in v]), "PfSolveGetShape")
+        return dict(streaming=v[0].value, rowsPerThread=v[1].value, warpsPerSystem=v[2].value,
+                    groupsPerCTA=v[3].value)
+
     def close(self):
         if getattr(self, "alive", False):
             self._lib.deletePfSolve(ctypes.byref(self.app))
@@ -108,6 +115,16 @@ class App:
             self.close()
         except Exception:
             pass
+
+
+def streaming_launch_count() -> int:
+    """Launches that ran on the streaming kernel (``PfSolveStreamingLaunchCount``)."""
+    return int(capi.load().PfSolveStreamingLaunchCount())
+
+
+def device_status() -> int:
+    """``PfSolveGetDeviceStatus``: 0, or PFSOLVE_ERROR_DEVICE_FAULT after a bounded wait ran out."""
+    return int(capi.load().PfSolveGetDeviceStatus())
 
 
 def append_chain(apps: Sequence[App], lps: Sequence[capi.PfSolveLaunchParams], allow_unfused: bool = False):

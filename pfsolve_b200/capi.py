@@ -72,7 +72,7 @@ class PfSolveConfiguration(ctypes.Structure):
         ("keepShaderCode", u64), ("printMemoryLayout", u64), ("disableCaching", c_int),
         ("disableSetLocale", u64), ("useUint64", u64),
         ("numConsecutiveJWIterations", c_int), ("useMultipleInputBuffers", c_int),
-        ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int),
+        ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int), ("kernelPath", c_int),
     ]
 
 
@@ -135,6 +135,9 @@ SIGNATURES = {
     "addToLibrary_block": (c_int, [ctypes.c_void_p, MapKeyBlock, _APP_P]),
     "PfSolveAppendChain": (c_int, [ctypes.POINTER(_APP_P), ctypes.POINTER(_LP_P), c_int, c_int]),
     "PfSolveLaunchCount": (u64, []),
+    "PfSolveGetDeviceStatus": (c_int, []),
+    "PfSolveGetShape": (c_int, [_APP_P] + [ctypes.POINTER(c_int)] * 4),
+    "PfSolveStreamingLaunchCount": (u64, []),
     "PfSolveBatchCreate": (c_int, [ctypes.POINTER(ctypes.c_void_p), c_int, ctypes.POINTER(PfSolveBatchDesc),
                                    ctypes.POINTER(PfSolveBatchEntry), c_int]),
     "PfSolveBatchAppend": (c_int, [ctypes.c_void_p, ctypes.c_void_p]),

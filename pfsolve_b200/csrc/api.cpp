@@ -14,6 +14,7 @@
 #include <map>
 #include <new>
 #include <tuple>
+#include <vector>
 
 #include "../../include/pfsolve_b200.h"
 #include "jw_variants.h"
@@ -23,6 +24,7 @@ using namespace pfb;
 namespace {
 
 std::atomic<uint64_t> g_launches{0};
+std::atomic<uint64_t> g_stream_launches{0};
 
 enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3 };
 
@@ -40,6 +42,21 @@ struct AppState {
     int refine_sweeps = 1;  // FP32 solves per system in the mixed mode
     const JwVariant* variant = nullptr;
     int max_blocks = 0;  // resident CTAs over the whole GPU
+    // streaming variant (FP64, TMA-staged systems), used when a launch's
+    // buffers allow it; `variant` serves the other launches
+    const StreamVariant* stream_v = nullptr;
+    int stream_G = 0, stream_max_blocks = 0;
+    int R_req = 0;           // caller's rows per thread (0: choose)
+    bool no_stream = false;  // kernelPath 1
+    // fused-chain plans made with this JW app, by operator shape
+    struct ChainPlan {
+        int KL, KU, sv, LIN, LOUT, SCALE;
+        const JwVariant* variant;
+        int R, W, G, max_blocks;
+        const StreamVariant* stream_v;
+        int stream_G, stream_max_blocks;
+    };
+    std::vector<ChainPlan> chain_plans;
     // reference band permutation parameters (reorder_i0 inputs)
     int64_t perm_r = 1, perm_m = 0, perm_ceil = 0, perm_floor = 0;
     // streams
@@ -119,6 +136,54 @@ bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, int& max_
     return true;
 }
 
+// Streaming variant for M rows: rows per thread R (the caller's choice, else
+// the compiled R whose groups leave the fewest idle rows, 16 first), W warps
+// per system, and the most groups per CTA that fit shared memory.
+bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    s->stream_v = nullptr;
+    if (s->prec != 0 || s->no_stream) return false;
+    int cand[3][2];
+    int n = 0;
+    const int prefs[3] = {16, 32, 8};
+    for (int R : prefs) {
+        if (s->R_req && R != s->R_req) continue;
+        const int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+        if (M % R != 0 || !(W == 1 || W == 2 || W == 4)) continue;
+        cand[n][0] = R;
+        cand[n][1] = (int)W;
+        n++;
+    }
+    // fewest idle rows first (stable: keeps the preference order on ties)
+    for (int i = 1; i < n; ++i)
+        for (int j = i; j > 0; --j) {
+            const int64_t a = 32LL * cand[j][1] * cand[j][0] - M, b = 32LL * cand[j - 1][1] * cand[j - 1][0] - M;
+            if (a >= b) break;
+            std::swap(cand[j], cand[j - 1]);
+        }
+    for (int i = 0; i < n; ++i) {
+        const StreamVariant* v = find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+        if (!v) continue;
+        const int T = 32 * v->W;
+        for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
+            const size_t smem = v->smem_bytes(G);
+            if (smem > 227 * 1024) continue;
+            if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                continue;
+            int blocks = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, T * G, smem) != cudaSuccess ||
+                blocks < 1)
+                continue;
+            s->stream_v = v;
+            s->stream_G = G;
+            s->stream_max_blocks = blocks * s->num_sms;
+            return true;
+        }
+    }
+    cudaGetLastError();
+    return false;
+}
+
 // Pick the kernel variant and launch shape for M rows: coefficient-table
 // variants first (FP64), then register variants; rows per thread from the
 // caller's choice (s->R) first, then the other compiled choices.
@@ -136,6 +201,7 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
             int G = 0, maxb = 0;
             if (!choose_groups(v, (int)W, s->num_sms, G, maxb)) continue;
             s->variant = v;
+            choose_stream(s, M, LIN, LOUT, SCALE);
             s->R = R;
             s->W = (int)W;
             s->G = G;
@@ -269,9 +335,63 @@ void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator
     op.refine_sweeps = s->refine_sweeps;
 }
 
+// Tensor maps of recent launches (encoding is host work; steady-state
+// launches repeat the same buffers).
+struct MapCacheEntry {
+    const StreamVariant* v;
+    JwIO io;
+    CUtensorMap in, out;
+    bool valid;
+};
+thread_local MapCacheEntry g_map_cache[8];
+thread_local unsigned g_map_next = 0;
+
+bool same_io(const JwIO& a, const JwIO& b)
+{
+    return a.in == b.in && a.out == b.out && a.in_off == b.in_off && a.in_stride == b.in_stride &&
+           a.out_off == b.out_off && a.out_stride == b.out_stride && a.nsys == b.nsys && a.M == b.M;
+}
+
+const MapCacheEntry* stream_maps(const StreamVariant* v, const JwIO& io)
+{
+    for (const MapCacheEntry& e : g_map_cache)
+        if (e.valid && e.v == v && same_io(e.io, io)) return &e;
+    MapCacheEntry& e = g_map_cache[g_map_next++ % 8];
+    e.valid = false;
+    if (!encode_stream_maps(v, io, &e.in, &e.out)) return nullptr;
+    e.v = v;
+    e.io = io;
+    e.valid = true;
+    return &e;
+}
+
+// Launch on the streaming variant when the plan has one and this launch's
+// buffers allow it (no accumulation, full output window, TMA-encodable rows).
+bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
+{
+    const StreamVariant* v = s->stream_v;
+    if (!v || io.accumulate || io.oz0 > 0 || io.oz1 < io.M) return false;
+    const MapCacheEntry* e = stream_maps(v, io);
+    if (!e) return false;
+    const int64_t want = (io.nsys + s->stream_G - 1) / s->stream_G;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->stream_max_blocks));
+    v->launch(dim3((unsigned)grid), dim3(32 * v->W * s->stream_G), v->smem_bytes(s->stream_G), stream, &e->in, &e->out,
+              op, io);
+    return true;
+}
+
 PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
 {
     if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    if (launch_stream(s, op, io, stream)) {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        g_stream_launches.fetch_add(1, std::memory_order_relaxed);
+        if (cudaPeekAtLastError() != cudaSuccess) {
+            cudaGetLastError();
+            return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+        }
+        return PFSOLVE_SUCCESS;
+    }
     const int64_t want = (io.nsys + s->G - 1) / s->G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->max_blocks));
     const size_t smem = s->variant->smem_bytes(s->W, s->G);
@@ -423,6 +543,21 @@ int PfSolveGetVersion(void) { return 102; }
 
 uint64_t PfSolveLaunchCount(void) { return g_launches.load(); }
 
+uint64_t PfSolveStreamingLaunchCount(void) { return g_stream_launches.load(); }
+
+PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread, int* warpsPerSystem,
+                              int* groupsPerCTA)
+{
+    if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    const AppState* s = static_cast<const AppState*>(app->internal);
+    const bool sm = s->stream_v != nullptr;
+    if (streaming) *streaming = sm ? 1 : 0;
+    if (rowsPerThread) *rowsPerThread = sm ? s->stream_v->R : s->R;
+    if (warpsPerSystem) *warpsPerSystem = sm ? s->stream_v->W : s->W;
+    if (groupsPerCTA) *groupsPerCTA = sm ? s->stream_G : s->G;
+    return PFSOLVE_SUCCESS;
+}
+
 PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cfg)
 {
     if (!app) return PFSOLVE_ERROR_INVALID_ARGUMENT;
@@ -486,7 +621,9 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
                 s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
-                s->R_fixed = c.rowsPerThread != 0;
+                s->R_fixed = c.rowsPerThread != 0 && c.rowsPerThread != 32;
+                s->R_req = c.rowsPerThread;
+                s->no_stream = c.kernelPath == 1;
                 reference_band_order(c.M_size, s->perm_r, s->perm_m, s->perm_ceil, s->perm_floor);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
@@ -506,6 +643,8 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->prec = dd_prec;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
                 if (s->R < 4) s->R = 4;
+                s->R_req = c.rowsPerThread;
+                s->no_stream = c.kernelPath == 1;
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
             // wider bands use the generic kernel (variant stays null)
@@ -541,6 +680,13 @@ PfSolveResult PfSolveAppend(PfSolveApplication* app, int inverse, PfSolveLaunchP
     }
     if (r == PFSOLVE_SUCCESS) record_stream_event(app, stream);
     return r;
+}
+
+PfSolveResult PfSolveGetDeviceStatus(void)
+{
+    const unsigned v = stream_status_fetch_clear();
+    if (v == ~0u) return PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE;
+    return v ? PFSOLVE_ERROR_DEVICE_FAULT : PFSOLVE_SUCCESS;
 }
 
 PfSolveResult PfSolveSync(PfSolveApplication* app)
@@ -669,14 +815,37 @@ PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchPara
         }
     }
     // plan for the fused variant
-    AppState t = *sj;
+    for (const AppState::ChainPlan& cp : sj->chain_plans) {
+        if (cp.KL != KL || cp.KU != KU || cp.sv != L.sv || cp.LIN != LIN || cp.LOUT != LOUT || cp.SCALE != SCALE)
+            continue;
+        AppState t;
+        t.num_sms = sj->num_sms;
+        t.variant = cp.variant;
+        t.R = cp.R;
+        t.W = cp.W;
+        t.G = cp.G;
+        t.max_blocks = cp.max_blocks;
+        t.stream_v = cp.stream_v;
+        t.stream_G = cp.stream_G;
+        t.stream_max_blocks = cp.stream_max_blocks;
+        return launch_jw_variant(&t, op, io, stream);
+    }
+    AppState t;
+    t.num_sms = sj->num_sms;
+    t.device = sj->device;
+    t.prec = sj->prec;
+    t.refine_sweeps = sj->refine_sweeps;
     t.KL = KL;
     t.KU = KU;
     t.sv = L.sv;
-    t.events = nullptr;
     t.R = pick_rows_per_thread(M, cj.rowsPerThread);
     if (t.R < 4) t.R = 4;
+    t.R_fixed = cj.rowsPerThread != 0 && cj.rowsPerThread != 32;
+    t.R_req = cj.rowsPerThread;
+    t.no_stream = cj.kernelPath == 1;
     if (finish_variant(&t, M, LIN, LOUT, SCALE) != PFSOLVE_SUCCESS) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    sj->chain_plans.push_back(AppState::ChainPlan{KL, KU, L.sv, LIN, LOUT, SCALE, t.variant, t.R, t.W, t.G,
+                                                  t.max_blocks, t.stream_v, t.stream_G, t.stream_max_blocks});
     return launch_jw_variant(&t, op, io, stream);
 }
 

@@ -293,49 +293,63 @@ __device__ __forceinline__ void group_matrix_scan(GroupCtx& g, double& a, double
     d = ec * wb + ed * wd;
 }
 
+// Effective matvec weights of V*A for row i (0 <= i < M): w[q] multiplies
+// row i + q - KL.  Without a fused dgbmv, V alone.
+template <int KL, int NB>
+__device__ __forceinline__ void jw_row_weights(const JwOperator& op, int64_t i, double (&w)[NB])
+{
+    const int64_t M = op.M;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) w[k] = 0.0;
+    double vl = 0, vd = 1, vu = 0;
+    if (op.mvj != MVJ_NONE) vd = band(op, op.off_md, i);
+    if (op.mvj == MVJ_UPPER && i + 1 < M) vu = band(op, op.off_mo, i);
+    if (op.mvj == MVJ_LOWER && i >= 1) vl = band(op, op.off_mo, i);
+    if (op.dgbmv == nullptr) {
+        if constexpr (KL >= 1) w[KL - 1] = vl;
+        w[KL] = vd;
+        if constexpr (NB - KL - 1 >= 1) w[KL + 1] = vu;
+    } else {
+        const int kla = op.dg_lda - 1 - op.dg_ku;
+        for (int pv = -1; pv <= 1; ++pv) {
+            const double vp = (pv < 0) ? vl : (pv == 0 ? vd : vu);
+            const int64_t p = i + pv;
+            if (vp == 0.0 || p < 0 || p >= M) continue;
+            for (int kk = -kla; kk <= op.dg_ku; ++kk) {
+                const int64_t c = p + kk;
+                if (c < 0 || c >= M) continue;
+                const double a = __ldg(op.dgbmv + op.dg_off + (int64_t)(op.dg_ku - kk) * M + c);
+                const int64_t k = c - i;  // within [-KL, KU] by construction of the plan
+#pragma unroll
+                for (int q = 0; q < NB; ++q)
+                    if (q - KL == (int)k) w[q] = __fma_rn(vp, a, w[q]);
+            }
+        }
+    }
+}
+
 // Build the coefficients for rows s .. s+R-1 of operator `op` (every thread
 // of the group), then keep them in registers or write them to the table.
 template <class C>
 __device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, int64_t s, JwCoef<C>& cf,
                                             double* table = nullptr)
 {
-    constexpr int R = C::kR, KL = C::kKL, KU = C::kKU;
+    constexpr int R = C::kR;
     using S = typename JwCoef<C>::S;
     const int64_t M = op.M;
     double w[C::NB][R];
     // (1) effective matvec weights of V*A for each row
 #pragma unroll
     for (int j = 0; j < R; ++j) {
+        double wr[C::NB];
+        if (s + j < M) {
+            jw_row_weights<C::kKL, C::NB>(op, s + j, wr);
+        } else {
 #pragma unroll
-        for (int k = 0; k < C::NB; ++k) w[k][j] = 0.0;
-        const int64_t i = s + j;
-        if (i < M) {
-            double vl = 0, vd = 1, vu = 0;
-            if (op.mvj != MVJ_NONE) vd = band(op, op.off_md, i);
-            if (op.mvj == MVJ_UPPER && i + 1 < M) vu = band(op, op.off_mo, i);
-            if (op.mvj == MVJ_LOWER && i >= 1) vl = band(op, op.off_mo, i);
-            if (op.dgbmv == nullptr) {
-                if constexpr (KL >= 1) w[KL - 1][j] = vl;
-                w[KL][j] = vd;
-                if constexpr (KU >= 1) w[KL + 1][j] = vu;
-            } else {
-                const int kla = op.dg_lda - 1 - op.dg_ku;
-                for (int pv = -1; pv <= 1; ++pv) {
-                    const double vp = (pv < 0) ? vl : (pv == 0 ? vd : vu);
-                    const int64_t p = i + pv;
-                    if (vp == 0.0 || p < 0 || p >= M) continue;
-                    for (int kk = -kla; kk <= op.dg_ku; ++kk) {
-                        const int64_t c = p + kk;
-                        if (c < 0 || c >= M) continue;
-                        const double a = __ldg(op.dgbmv + op.dg_off + (int64_t)(op.dg_ku - kk) * M + c);
-                        const int64_t k = c - i;  // within [-KL, KU] by construction of the plan
-#pragma unroll
-                        for (int q = 0; q < C::NB; ++q)
-                            if (q - KL == (int)k) w[q][j] = __fma_rn(vp, a, w[q][j]);
-                    }
-                }
-            }
+            for (int k = 0; k < C::NB; ++k) wr[k] = 0.0;
         }
+#pragma unroll
+        for (int k = 0; k < C::NB; ++k) w[k][j] = wr[k];
     }
     // (2) solve coefficients in FP64
     double l64[R], h64[R], m64[R], a64[R], c64[R];

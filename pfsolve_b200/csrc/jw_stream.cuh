@@ -1,0 +1,512 @@
+// jw_stream.cuh -- the streaming JW-step kernel: whole systems staged by TMA.
+//
+// Same operator as jw_step_kernel (x = diag(s) M^{-1} V A b, x[0] *= scaleC;
+// PfSolve/pfSolve_CodeGen/pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:38-408),
+// organised for throughput on long runs of systems that share one matrix:
+//
+//  * One CTA per SM, G groups of W warps; a group owns one system at a time,
+//    thread t of the group owns the R consecutive rows [R t, R t + R).
+//  * Right-hand sides move global -> shared with TMA tensor loads
+//    (cp.async.bulk.tensor, 3-D view {row-in-chunk, chunk, system}) into a
+//    swizzled layout in which both the TMA write and the per-thread chunk read
+//    are free of bank conflicts; results go back with TMA tensor stores from
+//    the same buffer.  Two buffers per group: the next system's load is in
+//    flight while the current one is solved.  One elected lane per warp
+//    issues all copies, so moving data costs a handful of instructions per
+//    system instead of one per element.
+//  * The coefficients (V A folded with the LU scaling, -l, -h, Scale factors)
+//    are built once per CTA, by all its threads, into a shared table read with
+//    16-byte loads; the products of -l and -h over each chunk (the scan
+//    multipliers) are formed once per thread.
+//  * The chunk-boundary couplings are resolved with the affine scans of the
+//    group kernel (warp shuffles, then shared memory across warps).
+//  * Completion waits are bounded: a wait that exceeds its limit records
+//    kStatusWaitTimeout in the device status word and the CTA stops.
+#pragma once
+#include <cuda.h>
+
+#include "jw_kernel.cuh"
+
+namespace pfb {
+
+constexpr unsigned kStatusWaitTimeout = 1u;
+static __device__ unsigned int g_stream_status;
+
+template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_>
+struct StCfg {
+    static constexpr int R = R_, W = W_, KL = KL_, KU = KU_, SV = SV_, LIN = LIN_, LOUT = LOUT_;
+    static constexpr bool SCALE = SCALE_;
+    static constexpr bool CPLX = (LIN != LAY_REAL);
+    using V = typename std::conditional<CPLX, double2, double>::type;
+    static constexpr int T = 32 * W;  // chunks (threads) per group
+    static constexpr int NB = KL + KU + 1;
+    static constexpr bool FWD = (SV == SV_LOWER || SV == SV_TRI);
+    static constexpr bool BWD = (SV == SV_UPPER || SV == SV_TRI);
+    // coefficient table planes: NB weights, -l, -h, Scale factor
+    static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0), P_SC = P_NH + (BWD ? 1 : 0);
+    static constexpr int NPL = P_SC + (SCALE ? 1 : 0);
+    // Input: NPIN planes of 8-byte rows; a chunk holds U 16-byte units per
+    // plane, stored as H swizzle rows of IB units (TMA box inner extent).
+    static constexpr int NPIN = CPLX ? 2 : 1;
+    static constexpr int U = R / 2;
+    static constexpr int IB = U < 8 ? U : 8;
+    static constexpr int H = U / IB;
+    static constexpr int SWB = Log2<IB>::v;
+    // Output: packed complex (16-byte rows) or planes of 8-byte rows.
+    static constexpr bool OPK = (LOUT == LAY_PACKED);
+    static constexpr int NPOUT = OPK ? 1 : (LOUT == LAY_XXII ? 2 : 1);
+    static constexpr int UO = OPK ? R : R / 2;
+    static constexpr int IBO = UO < 8 ? UO : 8;
+    static constexpr int HO = UO / IBO;
+    static constexpr int SWBO = Log2<IBO>::v;
+    static constexpr size_t BUF = (size_t)T * R * (CPLX ? 16 : 8);  // bytes of one system
+    static constexpr size_t TBL = (size_t)NPL * U * T * 16;
+    // A warp's input and output bytes coincide when both layouts have the same
+    // swizzle rows; otherwise a warp's staging overlaps its neighbours' input.
+    static constexpr bool kSameRows = (IB == IBO) && (NPIN * H == NPOUT * HO);
+    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2);
+    static constexpr int kMaxThreads = kDataRegs >= 64 ? 256 : 512;
+    static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
+    static_assert(KL <= 2 && KU <= 2, "halo of at most two rows");
+    static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");
+    static_assert(W == 1 || kSameRows, "multi-warp groups need matching input/output rows");
+};
+
+template <class C>
+__host__ __device__ constexpr size_t st_fixed_bytes(int G)
+{
+    return C::TBL + (size_t)G * C::W * kScratchPerWarp * sizeof(double) + (size_t)G * 2 * sizeof(uint64_t);
+}
+
+// Dynamic shared memory: table | scratch | mbarriers | (align 1024) | buffers.
+template <class C>
+__host__ __device__ constexpr size_t st_smem_bytes(int G)
+{
+    return st_fixed_bytes<C>(G) + 1024 + (size_t)G * 2 * C::BUF;
+}
+
+// ---- TMA, mbarrier and bulk-group primitives (PTX).
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for phase `parity` of `bar`, giving up after about two seconds.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > 4000000000LL) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, uint32_t src)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z), "r"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// AND of `pred` over the `nthreads` threads of named barrier `id`.
+__device__ __forceinline__ bool group_and(int id, int nthreads, bool pred)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
+// XOR pattern of the TMA swizzle for a row of 2^B 16-byte units: unit u of
+// swizzle row t lands at unit u ^ ((t >> (3 - B)) & (2^B - 1)).
+template <int B>
+__device__ __forceinline__ int swz_row(int t)
+{
+    if constexpr (B == 0) return 0;
+    else return (t >> (3 - B)) & ((1 << B) - 1);
+}
+
+// ---- Coefficient table, built once per CTA by all of its threads.
+// Plane p, row i = R*tt + j (tt: thread of a group) is the double at
+// [((p*U + j/2)*T + tt)*2 + (j&1)]: thread tt reads rows 2u, 2u+1 of a plane
+// as one 16-byte word, lanes on consecutive words.
+template <class C>
+__device__ void st_prologue(const JwOperator& op, double* table, double* scratch_all)
+{
+    constexpr int R = C::R, T = C::T, U = C::U, NB = C::NB;
+    const int64_t M = op.M;
+    const int rows = T * R;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int Rp = (rows + nthr - 1) / nthr;
+    const int64_t s = (int64_t)tid * Rp;
+    GroupCtx g;
+    g.lane = tid & 31;
+    g.wg = tid >> 5;
+    g.W = nthr >> 5;
+    g.nthr = nthr;
+    g.bar_id = 1;
+    g.seq = 0;
+    g.scratch = scratch_all;
+    double dprev = 1.0;
+    if constexpr (C::SV == SV_TRI) {
+        // Moebius product of this thread's rows, then the CTA-wide scan gives
+        // the pivot entering them (same recurrence as jw_prologue).
+        double a = 1, b = 0, c = 0, d = 1;
+        for (int j = 0; j < Rp; ++j) {
+            const int64_t i = s + j;
+            double ac = 0.0;
+            if (i >= 1 && i < M) ac = band(op, op.off_sl, i) * band(op, op.off_su, i - 1);
+            const double na = a - ac * c, nb = b - ac * d;
+            c = a;
+            d = b;
+            a = na;
+            b = nb;
+            renorm2x2(a, b, c, d);
+        }
+        group_matrix_scan(g, a, b, c, d);
+        dprev = (s == 0) ? 1.0 : a / c;
+    }
+    for (int j = 0; j < Rp; ++j) {
+        const int64_t i = s + j;
+        if (i >= rows) break;
+        double w[NB];
+        double nl = 0.0, nh = 0.0, sc = 0.0;
+        if (i < M) {
+            jw_row_weights<C::KL, NB>(op, i, w);
+            double m = 1.0;
+            if constexpr (C::SV == SV_TRI) {
+                const double ai = (i >= 1) ? band(op, op.off_sl, i) : 0.0;
+                const double ci = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
+                const double ac = (i >= 1) ? ai * band(op, op.off_su, i - 1) : 0.0;
+                const double dp = (i == 0) ? 1.0 : 1.0 - ac / dprev;
+                m = 1.0 / dp;
+                dprev = dp;
+                nl = -(ai * m);
+                nh = -(ci * m);
+            } else if constexpr (C::SV == SV_LOWER) {
+                nl = (i >= 1) ? -band(op, op.off_sl, i) : 0.0;
+            } else if constexpr (C::SV == SV_UPPER) {
+                nh = (i < M - 1) ? -band(op, op.off_su, i) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) w[k] *= m;
+            if constexpr (C::SCALE) sc = scale_factor(op.scale_kind, i, op.lshift, op.scale_s);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NB; ++k) w[k] = 0.0;
+        }
+        const int tt = (int)(i / R), jj = (int)(i % R);
+        auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * T + tt) * 2 + (jj & 1)] = v; };
+#pragma unroll
+        for (int k = 0; k < NB; ++k) put(k, w[k]);
+        if constexpr (C::FWD) put(C::P_NL, nl);
+        if constexpr (C::BWD) put(C::P_NH, nh);
+        if constexpr (C::SCALE) put(C::P_SC, sc);
+    }
+}
+
+// ---- The kernel.
+template <class C>
+__global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_constant__ CUtensorMap tm_in,
+                                                                  const __grid_constant__ CUtensorMap tm_out,
+                                                                  const JwOperator op, const JwIO io)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using V = typename C::V;
+    using O = VOps<V>;
+    constexpr int R = C::R, W = C::W, T = C::T, U = C::U, KL = C::KL, KU = C::KU, NB = C::NB;
+    constexpr int IB = C::IB, H = C::H, IBO = C::IBO, HO = C::HO;
+    const int G = blockDim.x / T;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = warp / W, wg = warp - grp * W;
+
+    double* table = reinterpret_cast<double*>(smem_raw);
+    double* scratch_all = reinterpret_cast<double*>(smem_raw + C::TBL);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::TBL + (size_t)G * W * kScratchPerWarp * sizeof(double));
+    unsigned char* after = reinterpret_cast<unsigned char*>(bars + 2 * G);
+    const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
+    unsigned char* buf0 = after + pad + (size_t)(2 * grp) * C::BUF;
+    unsigned char* buf1 = buf0 + C::BUF;
+    const uint32_t bar0 = smem_u32(&bars[2 * grp]), bar1 = smem_u32(&bars[2 * grp + 1]);
+
+    if ((int)threadIdx.x < 2 * G) mbar_init(smem_u32(&bars[threadIdx.x]), W);
+    mbar_init_fence();
+    st_prologue<C>(op, table, scratch_all);
+    __syncthreads();
+
+    GroupCtx g;
+    g.lane = lane;
+    g.wg = wg;
+    g.W = W;
+    g.nthr = T;
+    g.bar_id = 1 + grp;
+    g.seq = 0;
+    g.scratch = scratch_all + (size_t)grp * W * kScratchPerWarp;
+
+    const int t = wg * 32 + lane;
+    const int64_t s = (int64_t)t * R;
+    const double2* tb = reinterpret_cast<const double2*>(table) + t;  // pair (p, u) at tb[(p*U + u)*T]
+    auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * T]; };
+
+    // Scan multipliers: products of -l and -h over this thread's chunk.
+    double Af = 1.0, Ab = 1.0;
+    if constexpr (C::FWD) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 c = coef(C::P_NL, u);
+            Af = (u == 0) ? c.x : c.x * Af;
+            Af = c.y * Af;
+        }
+    }
+    if constexpr (C::BWD) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 c = coef(C::P_NH, u);
+            Ab = c.x * Ab;
+            Ab = c.y * Ab;
+        }
+    }
+
+    // Shared-memory byte offsets of 16-byte unit uu (< IB) of swizzle row h of
+    // plane p for chunk c: plane_row(p, h) * T * IB*16 + c * IB*16 + (uu ^ swz(c))*16.
+    constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
+    const int sw_me = swz_row<C::SWB>(t), sw_prev = swz_row<C::SWB>(t - 1), sw_next = swz_row<C::SWB>(t + 1);
+    const int swo_me = swz_row<C::SWBO>(t);
+    const bool has_prev = t > 0, has_next = t < T - 1;
+    auto unit_at = [&](const unsigned char* b, int p, int u, int c, int sw) -> double2 {
+        const int h = u / IB, uu = u % IB;
+        return *reinterpret_cast<const double2*>(b + (size_t)((p * H + h) * T + c) * ROWB + ((uu ^ sw) << 4));
+    };
+
+    const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
+    const int64_t nsys = io.nsys;
+    const int64_t step = (int64_t)gridDim.x * G;
+    int64_t sys = (int64_t)blockIdx.x * G + grp;
+
+    // lane 0 of each warp: load / store this warp's 32 chunks of one system
+    auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(C::NPIN * H * 32 * ROWB));
+#pragma unroll
+        for (int p = 0; p < C::NPIN; ++p)
+#pragma unroll
+            for (int h = 0; h < H; ++h)
+                tma_load_3d(smem_u32(b + (size_t)((p * H + h) * T + 32 * wg) * ROWB), &tm_in, h * IB * 2, 32 * wg,
+                            (int)(C::CPLX ? 2 * y + p : y), bar);
+    };
+    auto issue_store = [&](unsigned char* b, int64_t y) {
+#pragma unroll
+        for (int p = 0; p < C::NPOUT; ++p)
+#pragma unroll
+            for (int h = 0; h < HO; ++h)
+                tma_store_3d(&tm_out, h * IBO * 2, 32 * wg, (int)(C::NPOUT == 2 ? 2 * y + p : y),
+                             smem_u32(b + (size_t)((p * HO + h) * T + 32 * wg) * ROWBO));
+        bulk_commit();
+    };
+
+    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+    for (int k = 0; sys < nsys; ++k, sys += step) {
+        unsigned char* cur = (k & 1) ? buf1 : buf0;
+        unsigned char* nxt = (k & 1) ? buf0 : buf1;
+        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+        ok = (W == 1) ? (__all_sync(FULL, ok) != 0) : group_and(g.bar_id, g.nthr, ok);
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
+            break;
+        }
+
+        // rows s-KL .. s+R+KU-1 of this system
+        V be[R + KL + KU];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (C::CPLX) {
+                const double2 re = unit_at(cur, 0, u, t, sw_me), im = unit_at(cur, 1, u, t, sw_me);
+                be[KL + 2 * u] = make_double2(re.x, im.x);
+                be[KL + 2 * u + 1] = make_double2(re.y, im.y);
+            } else {
+                const double2 v = unit_at(cur, 0, u, t, sw_me);
+                be[KL + 2 * u] = v.x;
+                be[KL + 2 * u + 1] = v.y;
+            }
+        }
+        if constexpr (KL > 0) {
+            V pv[2] = {O::zero(), O::zero()};
+            if (has_prev) {
+                if constexpr (C::CPLX) {
+                    const double2 re = unit_at(cur, 0, U - 1, t - 1, sw_prev), im = unit_at(cur, 1, U - 1, t - 1, sw_prev);
+                    pv[0] = make_double2(re.x, im.x);
+                    pv[1] = make_double2(re.y, im.y);
+                } else {
+                    const double2 v = unit_at(cur, 0, U - 1, t - 1, sw_prev);
+                    pv[0] = v.x;
+                    pv[1] = v.y;
+                }
+            }
+            be[KL - 1] = pv[1];
+            if constexpr (KL > 1) be[0] = pv[0];
+        }
+        if constexpr (KU > 0) {
+            V nv[2] = {O::zero(), O::zero()};
+            if (has_next) {
+                if constexpr (C::CPLX) {
+                    const double2 re = unit_at(cur, 0, 0, t + 1, sw_next), im = unit_at(cur, 1, 0, t + 1, sw_next);
+                    nv[0] = make_double2(re.x, im.x);
+                    nv[1] = make_double2(re.y, im.y);
+                } else {
+                    const double2 v = unit_at(cur, 0, 0, t + 1, sw_next);
+                    nv[0] = v.x;
+                    nv[1] = v.y;
+                }
+            }
+            be[KL + R] = nv[0];
+            if constexpr (KU > 1) be[KL + R + 1] = nv[1];
+        }
+        if (win_partial) {
+#pragma unroll
+            for (int i = 0; i < R + KL + KU; ++i) {
+                const int64_t row = s - KL + i;
+                if (row < io.iz0 || row >= io.iz1) be[i] = O::zero();
+            }
+        }
+
+        // x = (V A b) scaled by the LU pivots, in place over be[0 .. R)
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            double2 wc[NB];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int j = 2 * u + e;
+                V acc = O::mul(e ? wc[0].y : wc[0].x, be[j]);
+#pragma unroll
+                for (int q = 1; q < NB; ++q) acc = O::fma(e ? wc[q].y : wc[q].x, be[j + q], acc);
+                be[j] = acc;
+            }
+        }
+        V (&x)[R + KL + KU] = be;
+
+        // The next system's load goes into the other buffer once this warp's
+        // stores from it have been read out of shared memory.
+        if (sys + step < nsys && lane == 0) {
+            bulk_wait_read_all();
+            issue_load(nxt, (k & 1) ? bar0 : bar1, sys + step);
+        }
+
+        if constexpr (C::FWD) {
+            // z_j = x_j - l_j z_{j-1} within the chunk, then add the coupling
+            // from the preceding chunks scaled by prod_{k<=j}(-l_k)
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 c = coef(C::P_NL, u);
+                if (u > 0) x[2 * u] = O::fma(c.x, x[2 * u - 1], x[2 * u]);
+                x[2 * u + 1] = O::fma(c.y, x[2 * u], x[2 * u + 1]);
+            }
+            const V pin = group_affine_scan<V, double, true>(g, Af, x[R - 1]);
+            double p = 1.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 c = coef(C::P_NL, u);
+                p = c.x * p;
+                x[2 * u] = O::fma(p, pin, x[2 * u]);
+                p = c.y * p;
+                x[2 * u + 1] = O::fma(p, pin, x[2 * u + 1]);
+            }
+        }
+        if constexpr (C::BWD) {
+#pragma unroll
+            for (int u = U - 1; u >= 0; --u) {
+                const double2 c = coef(C::P_NH, u);
+                if (u < U - 1) x[2 * u + 1] = O::fma(c.y, x[2 * u + 2], x[2 * u + 1]);
+                x[2 * u] = O::fma(c.x, x[2 * u + 1], x[2 * u]);
+            }
+            const V q = group_affine_scan<V, double, false>(g, Ab, x[0]);
+            double p = 1.0;
+#pragma unroll
+            for (int u = U - 1; u >= 0; --u) {
+                const double2 c = coef(C::P_NH, u);
+                p = c.y * p;
+                x[2 * u + 1] = O::fma(p, q, x[2 * u + 1]);
+                p = c.x * p;
+                x[2 * u] = O::fma(p, q, x[2 * u]);
+            }
+        }
+        if (C::SV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
+        if constexpr (C::SCALE) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 c = coef(C::P_SC, u);
+                x[2 * u] = O::mul(c.x, x[2 * u]);
+                x[2 * u + 1] = O::mul(c.y, x[2 * u + 1]);
+            }
+        }
+
+        // Stage the result in place.  Every thread of the group has read its
+        // input: the solve's scans are group barriers; without a solve, wait.
+        if constexpr (C::SV == SV_NONE) {
+            if (W > 1) group_bar(g.bar_id, g.nthr);
+        }
+        __syncwarp();
+        if constexpr (C::OPK) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const int h = j / IBO, uu = j % IBO;
+                *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) = x[j];
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int h = u / IBO, uu = u % IBO;
+                if constexpr (C::CPLX) {
+                    *reinterpret_cast<double2*>(cur + (size_t)((0 * HO + h) * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
+                        make_double2(x[2 * u].x, x[2 * u + 1].x);
+                    *reinterpret_cast<double2*>(cur + (size_t)((1 * HO + h) * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
+                        make_double2(x[2 * u].y, x[2 * u + 1].y);
+                } else {
+                    *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
+                        make_double2(x[2 * u], x[2 * u + 1]);
+                }
+            }
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) issue_store(cur, sys);
+    }
+    if (lane == 0) bulk_wait_all();
+}
+
+}  // namespace pfb

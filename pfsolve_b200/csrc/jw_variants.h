@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "jw_types.h"
@@ -33,6 +34,27 @@ struct BatchVariant {
                    const WorkItem* items, int nitems, unsigned int* counter, int W);
 };
 const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC);
+
+// Streaming variants (TMA-staged systems, R rows per thread, W warps per
+// system).  IB / IBO: 16-byte units per swizzle row of the input / output
+// layout (the TMA box's inner extent).
+struct StreamVariant {
+    int R, W, KL, KU, SV, LIN, LOUT, SCALE;
+    int max_threads;
+    const void* func;
+    size_t (*smem_bytes)(int G);
+    int IB, IBO;
+    void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
+                   const JwOperator& op, const JwIO& io);
+};
+const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE);
+const StreamVariant* stream_variants(int* count);
+// Tensor maps of a launch's input and output rows; false when the buffers'
+// alignment, strides or M do not allow the streaming layout.
+bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out);
+// Status word of the streaming kernels' bounded waits since the last call
+// (0: none timed out); reading it synchronises with the device.
+unsigned stream_status_fetch_clear();
 
 // Standalone kernels of the block and generic-bandwidth dgbmv applications.
 struct BlockArgs {
