@@ -332,7 +332,52 @@ def extras_arm(args):
                                   "gbs": 2.0 * rows * 16 / (ms * 1e-3) / 1e9, "shape": batch.shape(),
                                   "graph": True, "launches_per_step": 1}
     batch.close()
+    del inp, outb, keep
+    torch.cuda.empty_cache()
+    out["config5_serving"] = serving_leg()
     return out
+
+
+def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):
+    """Config 5: Poisson arrivals at `rate` of JW-step requests (N log-uniform
+    in [32, 1024], RHS log-uniform in [1, 4096], 80 % mixed precision, 20 %
+    double-double storage) through the serving engine; inputs device-resident
+    (a pool of `pool` distinct requests, reused cyclically).  Latency = submit
+    -> completion on the GPU, per request."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.serving import Server, run_load
+    specs = WL.config5_requests(pool, seed=4)
+    srv = Server(hbm_budget_bytes=16 << 30, streams=8, max_batch_requests=32, refine_sweeps=2)
+    ops, templ = {}, []
+    g = torch.Generator(device="cuda").manual_seed(4)
+    keep = []
+    for sp in specs:
+        if sp.M not in ops:
+            tb = torch.from_numpy(WL.serve_operator_bands(np.random.default_rng(sp.M), sp.M)).cuda()
+            keep.append(tb)
+            ops[sp.M] = srv.add_operator(sp.M, tb)
+        x = torch.rand(sp.M * sp.nrhs, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        if sp.precision == 2:
+            x = torch.stack([x, torch.zeros_like(x)], -1).reshape(-1)
+        templ.append((ops[sp.M], sp.precision, sp.nrhs, x, torch.empty_like(x)))
+    run_load(srv, [templ[i % pool] for i in range(warm)], WL.poisson_arrivals(warm, rate, seed=5))
+    n = int(rate * duration_s)
+    reqs = [templ[i % pool] for i in range(n)]
+    st0 = srv.stats()
+    lat, wall, lag = run_load(srv, reqs, WL.poisson_arrivals(n, rate, seed=4))
+    st1 = srv.stats()
+    srv.close()
+    lat = np.sort(np.asarray(lat))
+    rhs = sum(r[2] for r in reqs)
+    nbytes = sum(r[3].numel() * 8 * 2 for r in reqs)
+    return {"requests": n, "offered_rate_per_s": rate, "achieved_rate_per_s": n / wall,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat[-1]), "rhs_per_s": rhs / wall, "hbm_gbs_offered": nbytes / wall / 1e9,
+            "batches": st1["batches"] - st0["batches"], "submitter_max_lag_ms": 1e3 * lag,
+            "mix": "80% mixed (FP32 solve + 2 FP64 refinement sweeps), 20% double-double storage",
+            "streams": 8, "max_batch_requests": 32, "hbm_budget_bytes": 16 << 30}
 
 
 def main():
@@ -346,6 +391,7 @@ def main():
     ap.add_argument("--profile", action="store_true", help="kernel steps only: no e2e leg, no CPU baseline")
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
+    ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1],
                     help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
     args = ap.parse_args()
@@ -359,6 +405,9 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.serve:
+        print(json.dumps({"config5_serving": serving_leg()}), flush=True)
+        return
     try:
         if args.impl == "reference":
             reference_arm(args, rank, world)

@@ -332,6 +332,58 @@ PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* st
 /* Launches that ran on the streaming kernel since load (all apps). */
 PFSOLVE_API uint64_t PfSolveStreamingLaunchCount(void);
 
+/* ---- Serving engine.  No counterpart in the reference (whose callers drive
+ * one application at a time): JW-step requests of mixed size and precision are
+ * queued, admitted while the bytes of the requests on the device stay within
+ * an HBM budget, batched as they arrive and run on several streams at once, so
+ * requests that arrive while others run start without waiting for them.
+ * Operators (bands) are registered once and stay resident on the device. */
+typedef struct PfSolveServer PfSolveServer;
+
+typedef struct {
+    int device;
+    uint64_t hbmBudgetBytes;  /* in-flight request bytes (inputs + outputs) admitted at once */
+    int streams;              /* batches on the device at once (1..16) */
+    int maxBatchRequests;     /* requests per batch (1..256) */
+    int refineSweeps;         /* FP64 refinement sweeps of mixed-precision requests (1..3) */
+} PfSolveServerDesc;
+
+enum { PFSOLVE_SERVE_MIXED = 1, PFSOLVE_SERVE_DD = 2, PFSOLVE_SERVE_DD_FP64MEM = 3 };
+
+typedef struct {
+    int op;              /* operator id from PfSolveServerAddOperator */
+    int precision;       /* PFSOLVE_SERVE_*: FP32 solve + FP64 refinement (FP64 storage), double-double
+                            storage ({hi, lo} per value), double-double arithmetic on FP64 storage */
+    int64_t nrhs;        /* right-hand sides (systems) */
+    const void* input;   /* device, systems `stride` values apart */
+    void* output;        /* device; may equal input */
+    int64_t stride;      /* values between consecutive systems (0: M) */
+    double scaleC;       /* multiplies solution row 0 */
+} PfSolveRequest;
+
+typedef struct {
+    uint64_t submitted, completed, batches, rhs;
+    uint64_t peakInflightBytes;
+    double p50Ms, p99Ms, maxMs;  /* submit -> completion on the GPU, over completed requests */
+} PfSolveServerStats;
+
+PFSOLVE_API PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSolveServerDesc* desc);
+/* Register an operator: JW bands in the reference's layout (3*M doubles, device
+ * memory that stays valid while the server lives), upperBanded / jw_type as in
+ * PfSolveConfiguration.  A double-double copy is made on the device. */
+PFSOLVE_API PfSolveResult PfSolveServerAddOperator(PfSolveServer* server, int64_t M, const double* bands,
+                                                   int upperBanded, int jw_type, int* opId);
+/* Queue a request; returns at once.  PFSOLVE_ERROR_CAPACITY when the request
+ * alone exceeds the HBM budget. */
+PFSOLVE_API PfSolveResult PfSolveServerSubmit(PfSolveServer* server, const PfSolveRequest* request,
+                                              uint64_t* ticket);
+/* Block until the request is done; its latency (ms) when latencyMs != NULL.
+ * Each ticket is waited on once. */
+PFSOLVE_API PfSolveResult PfSolveServerWait(PfSolveServer* server, uint64_t ticket, double* latencyMs);
+PFSOLVE_API PfSolveResult PfSolveServerGetStats(PfSolveServer* server, PfSolveServerStats* stats);
+/* Drain every queued request, then free the server. */
+PFSOLVE_API void PfSolveServerDestroy(PfSolveServer* server);
+
 #ifdef __cplusplus
 }
 #endif

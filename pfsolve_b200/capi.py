@@ -115,6 +115,24 @@ class PfSolveBatchDesc(ctypes.Structure):
                 ("systemsPerItem", c_int)]
 
 
+class PfSolveServerDesc(ctypes.Structure):
+    _fields_ = [("device", c_int), ("hbmBudgetBytes", u64), ("streams", c_int), ("maxBatchRequests", c_int),
+                ("refineSweeps", c_int)]
+
+
+class PfSolveRequest(ctypes.Structure):
+    _fields_ = [("op", c_int), ("precision", c_int), ("nrhs", i64), ("input", ctypes.c_void_p),
+                ("output", ctypes.c_void_p), ("stride", i64), ("scaleC", ctypes.c_double)]
+
+
+class PfSolveServerStats(ctypes.Structure):
+    _fields_ = [("submitted", u64), ("completed", u64), ("batches", u64), ("rhs", u64),
+                ("peakInflightBytes", u64), ("p50Ms", ctypes.c_double), ("p99Ms", ctypes.c_double),
+                ("maxMs", ctypes.c_double)]
+
+
+PFSOLVE_SERVE_MIXED, PFSOLVE_SERVE_DD, PFSOLVE_SERVE_DD_FP64MEM = 1, 2, 3
+
 # Every function the header declares, with its ctypes signature.
 _APP_P = ctypes.POINTER(PfSolveApplication)
 _LP_P = ctypes.POINTER(PfSolveLaunchParams)
@@ -138,6 +156,13 @@ SIGNATURES = {
     "PfSolveGetDeviceStatus": (c_int, []),
     "PfSolveGetShape": (c_int, [_APP_P] + [ctypes.POINTER(c_int)] * 4),
     "PfSolveStreamingLaunchCount": (u64, []),
+    "PfSolveServerCreate": (c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PfSolveServerDesc)]),
+    "PfSolveServerAddOperator": (c_int, [ctypes.c_void_p, i64, ctypes.c_void_p, c_int, c_int,
+                                         ctypes.POINTER(c_int)]),
+    "PfSolveServerSubmit": (c_int, [ctypes.c_void_p, ctypes.POINTER(PfSolveRequest), ctypes.POINTER(u64)]),
+    "PfSolveServerWait": (c_int, [ctypes.c_void_p, u64, ctypes.POINTER(ctypes.c_double)]),
+    "PfSolveServerGetStats": (c_int, [ctypes.c_void_p, ctypes.POINTER(PfSolveServerStats)]),
+    "PfSolveServerDestroy": (None, [ctypes.c_void_p]),
     "PfSolveBatchCreate": (c_int, [ctypes.POINTER(ctypes.c_void_p), c_int, ctypes.POINTER(PfSolveBatchDesc),
                                    ctypes.POINTER(PfSolveBatchEntry), c_int]),
     "PfSolveBatchAppend": (c_int, [ctypes.c_void_p, ctypes.c_void_p]),

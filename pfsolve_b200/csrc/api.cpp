@@ -18,6 +18,7 @@
 
 #include "../../include/pfsolve_b200.h"
 #include "jw_variants.h"
+#include "plan.h"
 
 using namespace pfb;
 
@@ -66,20 +67,15 @@ struct AppState {
 
 AppState* st(PfSolveApplication* app) { return static_cast<AppState*>(app->internal); }
 
-// Rows per lane of the reference's register-major band order
-// (pfSolve_Plan_JonesWorland.h:311-346 and reorder_i0, :66-142).
-void reference_band_order(int64_t M, int64_t& r, int64_t& m, int64_t& ceil_n, int64_t& floor_n)
+}  // namespace
+
+void pfb::note_launch(bool streaming)
 {
-    int64_t warp = 64 * ((M + 1023) / 1024);
-    if (M < 512) warp = 32;
-    if (warp < 32) warp = 32;
-    if (warp % 32) warp = 32 * ((warp + 31) / 32);
-    r = (M + warp - 1) / warp;
-    if (r < 1) r = 1;
-    m = M % r;
-    ceil_n = (M + r - 1) / r;
-    floor_n = M / r;
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (streaming) g_stream_launches.fetch_add(1, std::memory_order_relaxed);
 }
+
+namespace {
 
 // Keep-window of PfConfigureZeropad (pfSolve_KernelsLevel0/pfSolve_Zeropad.h:306-377)
 // as a half-open row range.  Launch-time windows keep [z0, z1); plan-time
@@ -102,38 +98,6 @@ int pick_rows_per_thread(int64_t M, int requested)
     if (M <= 1024) return 4;
     if (M <= 2048) return 8;
     return 16;
-}
-
-// Groups per CTA for variant v at W warps per system: the count that keeps the
-// most groups resident per SM (shared memory, registers and the variant's
-// launch bound permitting).  Returns false when nothing fits.
-bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, int& max_blocks)
-{
-    int best = 0, bestG = 0, bestBlocks = 0;
-    size_t bestSmem = 0;
-    for (int G = 1; 32 * W * G <= v->max_threads; ++G) {
-        const size_t smem = v->smem_bytes(W, G);
-        if (smem > 227 * 1024) break;
-        if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            break;
-        int blocks = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess)
-            break;
-        if (blocks * G > best) {
-            best = blocks * G;
-            bestG = G;
-            bestBlocks = blocks;
-            bestSmem = smem;
-        }
-    }
-    if (best == 0) return false;
-    if (bestSmem > 48 * 1024 &&
-        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bestSmem) != cudaSuccess)
-        return false;
-    G_out = bestG;
-    max_blocks = bestBlocks * num_sms;
-    return true;
 }
 
 // Streaming variant for M rows: rows per thread R (the caller's choice, else
@@ -184,16 +148,19 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
     return false;
 }
 
-// Pick the kernel variant and launch shape for M rows: coefficient-table
-// variants first (FP64), then register variants; rows per thread from the
+// Pick the kernel variant and launch shape for M rows: register variants
+// first, then coefficient-table variants (FP64); rows per thread from the
 // caller's choice (s->R) first, then the other compiled choices.
 PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {
     const int order[4] = {s->R, 8, 4, 16};
-    for (int tbl = (s->prec == 0 ? 1 : 0); tbl >= 0; --tbl) {
+    // The caller's rows per thread first; when the group kernel has no such
+    // variant (the choice is then the streaming kernel's), any other.
+    for (int pass = 0; pass < 2; ++pass)
+    for (int tbl = 0; tbl <= (s->prec == 0 ? 1 : 0); ++tbl) {
         for (int oi = 0; oi < 4; ++oi) {
             const int R = order[oi];
-            if (oi > 0 && (R == s->R || s->R_fixed)) continue;
+            if (oi > 0 && (R == s->R || (s->R_fixed && pass == 0))) continue;
             const JwVariant* v = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, tbl);
             if (!v) continue;
             const int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
@@ -213,57 +180,6 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
     for (int R : {2, 4, 8, 16})
         if ((M + 32 * (int64_t)R - 1) / (32 * (int64_t)R) <= 8) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
-}
-
-// JW operator kinds for K = 1 (pfSolve_JonesWorland.h:117-353): which matvec,
-// which solve, and where the bands sit.  Returns false for combinations the
-// reference leaves undefined (upperBanded 2 with jw_type % 10 in {0, 1}).
-struct JwLayout {
-    int mvj, sv;
-    int64_t off_md, off_mo, off_sl, off_su;
-};
-
-bool jw_layout(const PfSolveConfiguration& c, bool rtM, bool rtV, int64_t oM, int64_t oV, JwLayout& L)
-{
-    const int64_t M = c.M_size;
-    const int jwt = c.jw_type % 10;
-    L = JwLayout{MVJ_NONE, SV_NONE, 0, 0, 0, 0};
-    if (c.upperBanded == 2) {
-        // Only jw_type%10 == 3 is defined: with %10 == 2 the reference loads
-        // the bands only for the matvec (:228-235, :269) and its solve is the identity.
-        L.off_md = M; L.off_sl = 0; L.off_su = 2 * M;
-        if (jwt == 3) { L.mvj = MVJ_DIAG; L.sv = SV_TRI; return true; }
-        return false;
-    }
-    if (jwt == 2) L.mvj = MVJ_NONE;
-    else if (jwt == 3) {
-        // Offsets chosen with upperBanded flipped (:133-136, :203-206); the
-        // solve reuses the off-diagonal band loaded with the matvec (no reload
-        // when performTriSolve == 2, :337-344).
-        L.mvj = MVJ_DIAG;
-        if (c.upperBanded == 1) {
-            L.off_md = rtM ? oM : M;
-            L.sv = SV_LOWER;
-            L.off_sl = rtM ? oM + M : 0;
-        } else {
-            L.off_md = rtM ? oM + M : 0;
-            L.sv = SV_UPPER;
-            L.off_su = rtM ? oM : M;
-        }
-        return true;
-    } else if (c.upperBanded == 1) {
-        L.mvj = MVJ_UPPER;
-        L.off_md = rtM ? oM + M : 0;
-        L.off_mo = rtM ? oM : M;
-    } else {
-        L.mvj = MVJ_LOWER;
-        L.off_md = rtM ? oM : M;
-        L.off_mo = rtM ? oM + M : 0;
-    }
-    if (jwt == 1) L.sv = SV_NONE;
-    else if (c.upperBanded == 1) { L.sv = SV_LOWER; L.off_sl = rtV ? oV : 2 * M; }
-    else { L.sv = SV_UPPER; L.off_su = rtV ? oV : 2 * M; }
-    return true;
 }
 
 cudaStream_t pick_stream(PfSolveApplication* app)

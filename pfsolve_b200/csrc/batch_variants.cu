@@ -34,6 +34,10 @@ static const BatchVariant kBatchVariants[] = {
     PFB_BV2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false, PREC_F64),
     PFB_BV2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false, PREC_MIXED),
     PFB_BV2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_F64),
+    PFB_BV2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_MIXED),
+    PFB_BV2(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false, PREC_MIXED),
+    PFB_BV2(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false, PREC_MIXED),
+    PFB_BV2(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, PREC_MIXED),
 };
 
 const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)

@@ -42,8 +42,6 @@
 
 namespace pfb {
 
-enum : int { PREC_F64 = 0, PREC_MIXED = 1 };
-
 template <int R, int KL, int KU, int SV, int LIN, int LOUT, bool SCALE, int PREC = PREC_F64, bool TBL = false>
 struct JwCfg {
     static constexpr int kR = R, kKL = KL, kKU = KU, kSV = SV, kLIN = LIN, kLOUT = LOUT, kPrec = PREC;

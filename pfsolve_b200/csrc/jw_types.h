@@ -7,6 +7,9 @@ namespace pfb {
 enum : int { SV_NONE = 0, SV_LOWER = 1, SV_UPPER = 2, SV_TRI = 3 };
 enum : int { LAY_REAL = 0, LAY_XXII = 1, LAY_PACKED = 2 };
 enum : int { MVJ_NONE = 0, MVJ_DIAG = 1, MVJ_UPPER = 2, MVJ_LOWER = 3 };
+// Arithmetic of a kernel variant: FP64; FP32 solve + FP64 refinement;
+// double-double on double-double storage; double-double on FP64 storage.
+enum : int { PREC_F64 = 0, PREC_MIXED = 1, PREC_DD = 2, PREC_DD_F64MEM = 3 };
 
 // The matrix side of a JW step: where the bands live and how to read them.
 struct JwOperator {

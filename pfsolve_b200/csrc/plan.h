@@ -1,0 +1,115 @@
+// plan.h -- host-side planning helpers shared by the application API and the
+// serving engine: band order, JW operator resolution, launch shapes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/pfsolve_b200.h"
+#include "jw_variants.h"
+
+namespace pfb {
+
+// Count one kernel launch in PfSolveLaunchCount (and in
+// PfSolveStreamingLaunchCount when it ran on the streaming kernel).
+void note_launch(bool streaming);
+
+// Rows per lane of the reference's register-major band order
+// (pfSolve_Plan_JonesWorland.h:311-346 and reorder_i0, :66-142).
+inline void reference_band_order(int64_t M, int64_t& r, int64_t& m, int64_t& ceil_n, int64_t& floor_n)
+{
+    int64_t warp = 64 * ((M + 1023) / 1024);
+    if (M < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    r = (M + warp - 1) / warp;
+    if (r < 1) r = 1;
+    m = M % r;
+    ceil_n = (M + r - 1) / r;
+    floor_n = M / r;
+}
+
+// JW operator kinds for K = 1 (pfSolve_JonesWorland.h:117-353): which matvec,
+// which solve, and where the bands sit.  Returns false for combinations the
+// reference leaves undefined (upperBanded 2 with jw_type % 10 in {0, 1}).
+struct JwLayout {
+    int mvj, sv;
+    int64_t off_md, off_mo, off_sl, off_su;
+};
+
+inline bool jw_layout(const PfSolveConfiguration& c, bool rtM, bool rtV, int64_t oM, int64_t oV, JwLayout& L)
+{
+    const int64_t M = c.M_size;
+    const int jwt = c.jw_type % 10;
+    L = JwLayout{MVJ_NONE, SV_NONE, 0, 0, 0, 0};
+    if (c.upperBanded == 2) {
+        // Only jw_type%10 == 3 is defined: with %10 == 2 the reference loads
+        // the bands only for the matvec (:228-235, :269) and its solve is the identity.
+        L.off_md = M; L.off_sl = 0; L.off_su = 2 * M;
+        if (jwt == 3) { L.mvj = MVJ_DIAG; L.sv = SV_TRI; return true; }
+        return false;
+    }
+    if (jwt == 2) L.mvj = MVJ_NONE;
+    else if (jwt == 3) {
+        // Offsets chosen with upperBanded flipped (:133-136, :203-206); the
+        // solve reuses the off-diagonal band loaded with the matvec (no reload
+        // when performTriSolve == 2, :337-344).
+        L.mvj = MVJ_DIAG;
+        if (c.upperBanded == 1) {
+            L.off_md = rtM ? oM : M;
+            L.sv = SV_LOWER;
+            L.off_sl = rtM ? oM + M : 0;
+        } else {
+            L.off_md = rtM ? oM + M : 0;
+            L.sv = SV_UPPER;
+            L.off_su = rtM ? oM : M;
+        }
+        return true;
+    } else if (c.upperBanded == 1) {
+        L.mvj = MVJ_UPPER;
+        L.off_md = rtM ? oM + M : 0;
+        L.off_mo = rtM ? oM : M;
+    } else {
+        L.mvj = MVJ_LOWER;
+        L.off_md = rtM ? oM : M;
+        L.off_mo = rtM ? oM + M : 0;
+    }
+    if (jwt == 1) L.sv = SV_NONE;
+    else if (c.upperBanded == 1) { L.sv = SV_LOWER; L.off_sl = rtV ? oV : 2 * M; }
+    else { L.sv = SV_UPPER; L.off_su = rtV ? oV : 2 * M; }
+    return true;
+}
+
+// Groups per CTA for variant v at W warps per system: the count that keeps the
+// most groups resident per SM (shared memory, registers and the variant's
+// launch bound permitting).  Returns false when nothing fits.
+inline bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, int& max_blocks)
+{
+    int best = 0, bestG = 0, bestBlocks = 0;
+    size_t bestSmem = 0;
+    for (int G = 1; 32 * W * G <= v->max_threads; ++G) {
+        const size_t smem = v->smem_bytes(W, G);
+        if (smem > 227 * 1024) break;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            break;
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess)
+            break;
+        if (blocks * G > best) {
+            best = blocks * G;
+            bestG = G;
+            bestBlocks = blocks;
+            bestSmem = smem;
+        }
+    }
+    if (best == 0) return false;
+    if (bestSmem > 48 * 1024 &&
+        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bestSmem) != cudaSuccess)
+        return false;
+    G_out = bestG;
+    max_blocks = bestBlocks * num_sms;
+    return true;
+}
+
+}  // namespace pfb

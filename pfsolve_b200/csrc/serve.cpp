@@ -1,0 +1,503 @@
+// serve.cpp -- the serving engine: JW-step requests of mixed size and
+// precision, admitted by HBM footprint and batched continuously.
+//
+// One worker thread owns dispatch.  A request joins the queue on submit; the
+// worker takes the queue head's precision class, gathers the queued requests
+// of that class that fit the HBM budget (bytes of every admitted, unfinished
+// request) up to maxBatchRequests, and launches them on a free stream:
+//   * mixed precision (FP32 solve + FP64 refinement): one persistent
+//     uneven-batch launch over all requests of the batch (jw_batch_kernel),
+//     descriptors copied from pinned staging on the same stream;
+//   * double-double: one JW-step launch per request (jw_dd_kernel).
+// Completion is signalled by a host function queued behind the batch, which
+// stamps the requests' completion time, releases their bytes and wakes the
+// worker and the waiters.  With `streams` batches in flight, requests that
+// arrive while others run are admitted as soon as a stream and bytes free up,
+// and their kernels overlap on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/pfsolve_b200.h"
+#include "plan.h"
+
+using namespace pfb;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeOp {
+    int64_t M;
+    const double* bands;
+    double* bands_dd;  // {hi, lo} copy (lo = 0), owned
+    JwLayout L;
+    int KL, KU;
+    int64_t perm_r, perm_m, perm_ceil, perm_floor;
+};
+
+struct Req {
+    uint64_t id;
+    PfSolveRequest r;
+    int64_t M;
+    uint64_t bytes;
+    int cls;  // batch class: precision class and operator kind (one kernel per batch)
+    Clock::time_point t_submit, t_done;
+    bool done = false;
+};
+
+struct Shape {
+    int G = 0, max_blocks = 0;
+    size_t smem = 0;
+};
+
+struct Flight {
+    PfSolveServer* srv = nullptr;
+    cudaStream_t stream = nullptr;
+    BatchEntryDev* h_entries = nullptr;  // pinned staging
+    WorkItem* h_items = nullptr;
+    BatchEntryDev* d_entries = nullptr;
+    WorkItem* d_items = nullptr;
+    unsigned int* d_counter = nullptr;
+    int items_cap = 0;
+    std::vector<Req*> reqs;
+    bool busy = false;
+};
+
+
+}  // namespace
+
+struct PfSolveServer {
+    PfSolveServerDesc desc;
+    int num_sms = 0;
+    std::deque<ServeOp> ops;  // references stay valid while operators are added
+    std::map<std::pair<const void*, int>, Shape> shapes;  // (kernel, W) -> groups, blocks
+    std::mutex mu;
+    std::condition_variable cv;       // worker
+    std::condition_variable done_cv;  // waiters
+    std::deque<Req*> pending;
+    std::unordered_map<uint64_t, Req*> reqs;
+    std::vector<Flight> flights;
+    uint64_t next_id = 1;
+    uint64_t inflight_bytes = 0, peak_inflight = 0;
+    uint64_t submitted = 0, completed = 0, batches = 0, rhs = 0;
+    std::vector<double> lat_ms;
+    bool stop = false;
+    std::thread worker;
+};
+
+namespace {
+
+double ms_between(Clock::time_point a, Clock::time_point b)
+{
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// Rows per thread and warps per system for systems of up to Mmax rows.
+void serve_rows(int64_t Mmax, int& R, int& W)
+{
+    R = (Mmax <= 128) ? 4 : 8;
+    W = (int)((Mmax + 32 * R - 1) / (32 * R));
+    int p = 1;
+    while (p < W) p <<= 1;
+    W = p;
+}
+
+bool batch_shape(PfSolveServer* s, const BatchVariant* v, int W, Shape& out)
+{
+    auto key = std::make_pair(v->func, W);
+    auto it = s->shapes.find(key);
+    if (it != s->shapes.end()) { out = it->second; return true; }
+    for (int G = std::max(1, 8 / W); G >= 1; --G) {
+        const size_t smem = v->smem_bytes(W, G);
+        if (smem > 227 * 1024) continue;
+        if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            continue;
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess ||
+            blocks < 1)
+            continue;
+        out.G = G;
+        out.max_blocks = blocks * s->num_sms;
+        out.smem = smem;
+        s->shapes[key] = out;
+        return true;
+    }
+    cudaGetLastError();
+    return false;
+}
+
+bool jw_shape(PfSolveServer* s, const JwVariant* v, int W, Shape& out)
+{
+    auto key = std::make_pair(v->func, W);
+    auto it = s->shapes.find(key);
+    if (it != s->shapes.end()) { out = it->second; return true; }
+    int G = 0, maxb = 0;
+    if (!choose_groups(v, W, s->num_sms, G, maxb)) { cudaGetLastError(); return false; }
+    out.G = G;
+    out.max_blocks = maxb;
+    out.smem = v->smem_bytes(W, G);
+    s->shapes[key] = out;
+    return true;
+}
+
+JwOperator make_operator(const PfSolveServer* s, const ServeOp& o, const PfSolveRequest& r)
+{
+    JwOperator op;
+    memset(&op, 0, sizeof(op));
+    op.bands = (r.precision == PFSOLVE_SERVE_DD) ? o.bands_dd : o.bands;
+    op.off_md = o.L.off_md;
+    op.off_mo = o.L.off_mo;
+    op.off_sl = o.L.off_sl;
+    op.off_su = o.L.off_su;
+    op.mvj = o.L.mvj;
+    op.perm = 1;
+    op.perm_r = o.perm_r;
+    op.perm_m = o.perm_m;
+    op.perm_ceil = o.perm_ceil;
+    op.perm_floor = o.perm_floor;
+    op.scaleC = r.scaleC;
+    op.M = o.M;
+    op.refine_sweeps = 1 + s->desc.refineSweeps;
+    return op;
+}
+
+JwIO make_io(const ServeOp& o, const PfSolveRequest& r)
+{
+    JwIO io;
+    memset(&io, 0, sizeof(io));
+    io.in = static_cast<const double*>(r.input);
+    io.out = static_cast<double*>(r.output);
+    io.in_stride = io.out_stride = r.stride ? r.stride : o.M;
+    io.iz0 = io.oz0 = 0;
+    io.iz1 = io.oz1 = INT64_MAX / 4;
+    io.nsys = r.nrhs;
+    io.M = o.M;
+    return io;
+}
+
+void CUDART_CB on_flight_done(void* p)
+{
+    Flight* fl = static_cast<Flight*>(p);
+    PfSolveServer* s = fl->srv;
+    const Clock::time_point now = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (Req* r : fl->reqs) {
+        r->t_done = now;
+        r->done = true;
+        s->inflight_bytes -= r->bytes;
+        s->completed++;
+        s->rhs += (uint64_t)r->r.nrhs;
+        s->lat_ms.push_back(ms_between(r->t_submit, now));
+    }
+    fl->reqs.clear();
+    fl->busy = false;
+    s->batches++;
+    s->cv.notify_all();
+    s->done_cv.notify_all();
+}
+
+// Enqueue the batch of flight `fl` (mixed: one uneven-batch launch; dd: one
+// launch per request), then its completion callback.
+void launch_flight(PfSolveServer* s, Flight& fl, int cls)
+{
+    if (cls == 0) {
+        int64_t Mmax = 0, S = 0;
+        for (Req* r : fl.reqs) {
+            Mmax = std::max(Mmax, r->M);
+            S += r->r.nrhs;
+        }
+        int R, W;
+        serve_rows(Mmax, R, W);
+        const ServeOp& o0 = s->ops[fl.reqs[0]->r.op];
+        const BatchVariant* v = find_batch_variant(R, o0.KL, o0.KU, o0.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED);
+        Shape sh;
+        if (v && batch_shape(s, v, W, sh)) {
+            // items: enough per group for balance, within the staging capacity
+            const int64_t groups = (int64_t)sh.max_blocks * sh.G;
+            int64_t spi = std::max<int64_t>(1, std::min<int64_t>(64, (S + 2 * groups - 1) / (2 * groups)));
+            int64_t nitems = 0;
+            for (;;) {
+                nitems = 0;
+                for (Req* r : fl.reqs) nitems += (r->r.nrhs + spi - 1) / spi;
+                if (nitems <= fl.items_cap) break;
+                spi *= 2;
+            }
+            int k = 0, e = 0;
+            for (Req* r : fl.reqs) {
+                const ServeOp& o = s->ops[r->r.op];
+                fl.h_entries[e].op = make_operator(s, o, r->r);
+                fl.h_entries[e].io = make_io(o, r->r);
+                for (int64_t y0 = 0; y0 < r->r.nrhs; y0 += spi) {
+                    fl.h_items[k].entry = e;
+                    fl.h_items[k].pad = 0;
+                    fl.h_items[k].y0 = y0;
+                    fl.h_items[k].y1 = std::min<int64_t>(r->r.nrhs, y0 + spi);
+                    ++k;
+                }
+                ++e;
+            }
+            cudaMemcpyAsync(fl.d_entries, fl.h_entries, e * sizeof(BatchEntryDev), cudaMemcpyHostToDevice, fl.stream);
+            cudaMemcpyAsync(fl.d_items, fl.h_items, k * sizeof(WorkItem), cudaMemcpyHostToDevice, fl.stream);
+            cudaMemsetAsync(fl.d_counter, 0, sizeof(unsigned int), fl.stream);
+            const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((k + sh.G - 1) / sh.G, sh.max_blocks));
+            v->launch(dim3((unsigned)grid), dim3(32 * W * sh.G), sh.smem, fl.stream, fl.d_entries, fl.d_items, k,
+                      fl.d_counter, W);
+            note_launch(false);
+        }
+    } else {
+        for (Req* r : fl.reqs) {
+            const ServeOp& o = s->ops[r->r.op];
+            int R, W;
+            serve_rows(o.M, R, W);
+            const int prec = (r->r.precision == PFSOLVE_SERVE_DD) ? 2 : 3;
+            const JwVariant* v = find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, prec, 0);
+            Shape sh;
+            if (!v || !jw_shape(s, v, W, sh)) continue;
+            const JwOperator op = make_operator(s, o, r->r);
+            const JwIO io = make_io(o, r->r);
+            const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((io.nsys + sh.G - 1) / sh.G, sh.max_blocks));
+            v->launch(dim3((unsigned)grid), dim3(32 * W * sh.G), sh.smem, fl.stream, op, io, W);
+            note_launch(false);
+        }
+    }
+    cudaLaunchHostFunc(fl.stream, on_flight_done, &fl);
+}
+
+int free_flight(PfSolveServer* s)
+{
+    for (size_t i = 0; i < s->flights.size(); ++i)
+        if (!s->flights[i].busy) return (int)i;
+    return -1;
+}
+
+void worker_loop(PfSolveServer* s)
+{
+    cudaSetDevice(s->desc.device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    const uint64_t budget = s->desc.hbmBudgetBytes;
+    for (;;) {
+        s->cv.wait(lk, [&] {
+            if (s->stop && s->pending.empty()) return true;
+            if (s->pending.empty() || free_flight(s) < 0) return false;
+            return s->inflight_bytes + s->pending.front()->bytes <= budget;
+        });
+        if (s->pending.empty()) break;  // stop requested and drained
+        Flight& fl = s->flights[free_flight(s)];
+        const int cls = s->pending.front()->cls;
+        uint64_t add = 0;
+        for (auto it = s->pending.begin(); it != s->pending.end() && (int)fl.reqs.size() < s->desc.maxBatchRequests;) {
+            Req* r = *it;
+            if (r->cls != cls) {
+                ++it;
+                continue;
+            }
+            if (s->inflight_bytes + add + r->bytes > budget) break;
+            fl.reqs.push_back(r);
+            add += r->bytes;
+            it = s->pending.erase(it);
+        }
+        s->inflight_bytes += add;
+        s->peak_inflight = std::max(s->peak_inflight, s->inflight_bytes);
+        fl.busy = true;
+        lk.unlock();
+        launch_flight(s, fl, cls / 1000);
+        lk.lock();
+    }
+}
+
+void free_flight_resources(Flight& fl)
+{
+    if (fl.stream) cudaStreamDestroy(fl.stream);
+    if (fl.h_entries) cudaFreeHost(fl.h_entries);
+    if (fl.h_items) cudaFreeHost(fl.h_items);
+    if (fl.d_entries) cudaFree(fl.d_entries);
+    if (fl.d_items) cudaFree(fl.d_items);
+    if (fl.d_counter) cudaFree(fl.d_counter);
+}
+
+}  // namespace
+
+extern "C" {
+
+PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSolveServerDesc* desc)
+{
+    if (!server || !desc) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    *server = nullptr;
+    if (desc->hbmBudgetBytes == 0 || desc->streams < 1 || desc->streams > 16 || desc->maxBatchRequests < 1 ||
+        desc->maxBatchRequests > 256 || desc->refineSweeps < 1 || desc->refineSweeps > 3)
+        return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    if (cudaSetDevice(desc->device) != cudaSuccess) return PFSOLVE_ERROR_INVALID_DEVICE;
+    PfSolveServer* s = new (std::nothrow) PfSolveServer();
+    if (!s) return PFSOLVE_ERROR_MALLOC_FAILED;
+    s->desc = *desc;
+    if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, desc->device) != cudaSuccess) {
+        delete s;
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    }
+    s->flights.resize(desc->streams);
+    const int cap = desc->maxBatchRequests * 64;
+    bool ok = true;
+    for (Flight& fl : s->flights) {
+        fl.srv = s;
+        fl.items_cap = cap;
+        ok = ok && cudaStreamCreateWithFlags(&fl.stream, cudaStreamNonBlocking) == cudaSuccess;
+        ok = ok && cudaMallocHost(&fl.h_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
+        ok = ok && cudaMallocHost(&fl.h_items, cap * sizeof(WorkItem)) == cudaSuccess;
+        ok = ok && cudaMalloc(&fl.d_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
+        ok = ok && cudaMalloc(&fl.d_items, cap * sizeof(WorkItem)) == cudaSuccess;
+        ok = ok && cudaMalloc(&fl.d_counter, sizeof(unsigned int)) == cudaSuccess;
+    }
+    if (!ok) {
+        for (Flight& fl : s->flights) free_flight_resources(fl);
+        delete s;
+        return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
+    }
+    s->worker = std::thread(worker_loop, s);
+    *server = s;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveServerAddOperator(PfSolveServer* s, int64_t M, const double* bands, int upperBanded, int jw_type,
+                                       int* opId)
+{
+    if (!s || !bands || !opId || M < 1 || M > 1024) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    PfSolveConfiguration c;
+    memset(&c, 0, sizeof(c));
+    c.M_size = M;
+    c.upperBanded = upperBanded;
+    c.jw_type = jw_type;
+    ServeOp o;
+    memset(&o, 0, sizeof(o));
+    o.M = M;
+    o.bands = bands;
+    if (upperBanded < 0 || upperBanded > 2 || jw_type < 10 || !jw_layout(c, false, false, 0, 0, o.L) ||
+        o.L.sv == SV_NONE)
+        return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    o.KL = (o.L.mvj == MVJ_LOWER) ? 1 : 0;
+    o.KU = (o.L.mvj == MVJ_UPPER) ? 1 : 0;
+    for (int R : {4, 8}) {
+        if (!find_batch_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED) ||
+            !find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, 2, 0) ||
+            !find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, 3, 0))
+            return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    }
+    reference_band_order(M, o.perm_r, o.perm_m, o.perm_ceil, o.perm_floor);
+    cudaSetDevice(s->desc.device);
+    if (cudaMalloc(&o.bands_dd, 3 * M * 2 * sizeof(double)) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
+    if (cudaMemset(o.bands_dd, 0, 3 * M * 2 * sizeof(double)) != cudaSuccess ||
+        cudaMemcpy2D(o.bands_dd, 2 * sizeof(double), bands, sizeof(double), sizeof(double), 3 * M,
+                     cudaMemcpyDeviceToDevice) != cudaSuccess) {
+        cudaFree(o.bands_dd);
+        return PFSOLVE_ERROR_FAILED_TO_COPY;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->ops.push_back(o);
+    *opId = (int)s->ops.size() - 1;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveServerSubmit(PfSolveServer* s, const PfSolveRequest* r, uint64_t* ticket)
+{
+    if (!s || !r || !ticket || !r->input || !r->output || r->nrhs < 1 || r->stride < 0) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    if (r->precision < PFSOLVE_SERVE_MIXED || r->precision > PFSOLVE_SERVE_DD_FP64MEM) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    Req* q = new (std::nothrow) Req();
+    if (!q) return PFSOLVE_ERROR_MALLOC_FAILED;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (r->op < 0 || r->op >= (int)s->ops.size()) {
+        delete q;
+        return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    }
+    q->r = *r;
+    const ServeOp& o = s->ops[r->op];
+    q->M = o.M;
+    q->cls = (r->precision == PFSOLVE_SERVE_MIXED ? 0 : 1000) + 100 * o.KL + 10 * o.KU + o.L.sv;
+    if (r->stride && r->stride < q->M) {
+        delete q;
+        return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    }
+    const uint64_t elem = (r->precision == PFSOLVE_SERVE_DD) ? 16 : 8;
+    q->bytes = (uint64_t)r->nrhs * (uint64_t)q->M * elem * (r->input == r->output ? 1 : 2);
+    if (q->bytes > s->desc.hbmBudgetBytes) {
+        delete q;
+        return PFSOLVE_ERROR_CAPACITY;
+    }
+    q->id = s->next_id++;
+    q->t_submit = Clock::now();
+    s->reqs[q->id] = q;
+    s->pending.push_back(q);
+    s->submitted++;
+    *ticket = q->id;
+    lk.unlock();
+    s->cv.notify_all();
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveServerWait(PfSolveServer* s, uint64_t ticket, double* latencyMs)
+{
+    if (!s) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    Req* q = it->second;
+    s->done_cv.wait(lk, [&] { return q->done; });
+    if (latencyMs) *latencyMs = ms_between(q->t_submit, q->t_done);
+    s->reqs.erase(it);
+    delete q;
+    return PFSOLVE_SUCCESS;
+}
+
+PfSolveResult PfSolveServerGetStats(PfSolveServer* s, PfSolveServerStats* out)
+{
+    if (!s || !out) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    std::vector<double> lat;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        out->submitted = s->submitted;
+        out->completed = s->completed;
+        out->batches = s->batches;
+        out->rhs = s->rhs;
+        out->peakInflightBytes = s->peak_inflight;
+        lat = s->lat_ms;
+    }
+    out->p50Ms = out->p99Ms = out->maxMs = 0.0;
+    if (!lat.empty()) {
+        std::sort(lat.begin(), lat.end());
+        auto q = [&](double f) { return lat[std::min(lat.size() - 1, (size_t)(f * (lat.size() - 1) + 0.5))]; };
+        out->p50Ms = q(0.50);
+        out->p99Ms = q(0.99);
+        out->maxMs = lat.back();
+    }
+    return PFSOLVE_SUCCESS;
+}
+
+void PfSolveServerDestroy(PfSolveServer* s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->desc.device);
+    for (Flight& fl : s->flights)
+        if (fl.stream) cudaStreamSynchronize(fl.stream);
+    for (Flight& fl : s->flights) free_flight_resources(fl);
+    for (ServeOp& o : s->ops)
+        if (o.bands_dd) cudaFree(o.bands_dd);
+    for (auto& kv : s->reqs) delete kv.second;
+    delete s;
+}
+
+}  // extern "C"

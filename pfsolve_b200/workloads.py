@@ -159,3 +159,40 @@ def config4(seed=3, lmax=511, Nmax=512, scale_s=-0.5, rhs=True) -> UnevenStep:
         off += 2 * N * ns
     data = rng.standard_normal(off) if rhs else np.zeros(0)
     return UnevenStep(ls, Ns, nsys, jw, dg, np.array(offs, dtype=np.int64), data, scale_s)
+
+
+def serve_operator_bands(rng, M):
+    """Test-0 form operator (upperBanded 2, jw_type 13: diagonal scale then unit
+    tridiagonal solve) with config-1 coefficient distributions: d ~ U(1,2),
+    a, c ~ U(-0.5, 0.5), a_0 = c_{M-1} = 0; normalised md = 1/d, ld = a/d,
+    ud = c/d and stored in the reference's band order."""
+    d = rng.uniform(1.0, 2.0, M)
+    a = rng.uniform(-0.5, 0.5, M)
+    c = rng.uniform(-0.5, 0.5, M)
+    a[0] = 0.0
+    c[-1] = 0.0
+    return permute_bands(np.concatenate([a / d, 1.0 / d, c / d]), M)
+
+
+@dataclass
+class ServeRequestSpec:
+    M: int
+    nrhs: int
+    precision: int  # 1 mixed, 2 double-double storage
+
+
+def config5_requests(n, seed=4, n_min=32, n_max=1024, r_min=1, r_max=4096, dd_fraction=0.2):
+    """Request mix of the serving loop: N log-uniform in [n_min, n_max], RHS
+    count log-uniform in [r_min, r_max], 80 % mixed precision, 20 %
+    double-double."""
+    rng = np.random.default_rng(seed)
+    Ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max + 1), n)).astype(np.int64).clip(n_min, n_max)
+    Rs = np.exp(rng.uniform(np.log(r_min), np.log(r_max + 1), n)).astype(np.int64).clip(r_min, r_max)
+    dd = rng.uniform(0, 1, n) < dd_fraction
+    return [ServeRequestSpec(int(N), int(R), 2 if d else 1) for N, R, d in zip(Ns, Rs, dd)]
+
+
+def poisson_arrivals(n, rate, seed=4):
+    """Arrival times (s) of n requests of a Poisson process of the given rate."""
+    rng = np.random.default_rng(seed + 1)
+    return np.cumsum(rng.exponential(1.0 / rate, n))

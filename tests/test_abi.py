@@ -48,6 +48,10 @@ int main(void) {
          sizeof(PfSolveConfiguration), sizeof(PfSolveLaunchParams), sizeof(PfSolveApplication),
          sizeof(PfSolve_MapKey_JonesWorland), sizeof(PfSolve_MapKey_dgbmv), sizeof(PfSolve_MapKey_block),
          sizeof(PfSolveBatchEntry), sizeof(PfSolveBatchDesc));
+  printf("sdesc %zu\nsreq %zu\nsstat %zu\n", sizeof(PfSolveServerDesc), sizeof(PfSolveRequest),
+         sizeof(PfSolveServerStats));
+  F(PfSolveRequest, nrhs) F(PfSolveRequest, scaleC) F(PfSolveServerDesc, hbmBudgetBytes)
+  F(PfSolveServerStats, p50Ms) F(PfSolveConfiguration, kernelPath)
   F(PfSolveConfiguration, jw_type) F(PfSolveConfiguration, jw_control_bitmask)
   F(PfSolveConfiguration, scaleC) F(PfSolveConfiguration, doublePrecision)
   F(PfSolveConfiguration, outputBufferStride) F(PfSolveConfiguration, numConsecutiveJWIterations)
@@ -74,10 +78,13 @@ def test_ctypes_layout_matches_c(tmp_path):
     assert int(out["kbl"]) == ctypes.sizeof(capi.MapKeyBlock)
     assert int(out["bent"]) == ctypes.sizeof(capi.PfSolveBatchEntry)
     assert int(out["bdesc"]) == ctypes.sizeof(capi.PfSolveBatchDesc)
+    assert int(out["sdesc"]) == ctypes.sizeof(capi.PfSolveServerDesc)
+    assert int(out["sreq"]) == ctypes.sizeof(capi.PfSolveRequest)
+    assert int(out["sstat"]) == ctypes.sizeof(capi.PfSolveServerStats)
     for key, val in out.items():
         if "." in key:
             T, f = key.split(".")
-            cls = capi.PfSolveConfiguration if T == "PfSolveConfiguration" else capi.PfSolveLaunchParams
+            cls = getattr(capi, T)
             assert getattr(cls, f).offset == int(val), key
 
 
@@ -137,3 +144,19 @@ def test_app_library_keys_order_and_lookup():
         assert not out
     finally:
         lib.PfSolveAppLibraryDestroy(L)
+
+
+def test_server_argument_checks_before_device_use():
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    assert lib.PfSolveServerCreate(ctypes.byref(h), None) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT
+    for bad in (dict(streams=0), dict(streams=17), dict(maxBatchRequests=0), dict(refineSweeps=4),
+                dict(hbmBudgetBytes=0)):
+        kw = dict(device=0, hbmBudgetBytes=1 << 20, streams=2, maxBatchRequests=4, refineSweeps=2)
+        kw.update(bad)
+        d = capi.PfSolveServerDesc(**kw)
+        assert lib.PfSolveServerCreate(ctypes.byref(h), ctypes.byref(d)) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT, bad
+    r = capi.PfSolveRequest()
+    t = ctypes.c_uint64()
+    assert lib.PfSolveServerSubmit(None, ctypes.byref(r), ctypes.byref(t)) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT
+    lib.PfSolveServerDestroy(None)
