@@ -153,6 +153,7 @@ def gpu_arm(args, rank, world):
     import torch
     import torch.distributed as dist
 
+    from pfsolve_b200 import replicas
     from pfsolve_b200 import workloads as WL
     from pfsolve_b200.api import App, append_chain, launch_count
 
@@ -198,11 +199,8 @@ def gpu_arm(args, rank, world):
     launches = launch_count() - n0
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * nc / (ms_max * 1e-3)
+    ms_max = replicas.max_over_ranks(ms, dev)
+    value = replicas.job_throughput(nc, ms_max, world)
     bytes_alg = 2.0 * M * 16 * nc + (5 + 3) * M * 8
     achieved = bytes_alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
@@ -232,10 +230,7 @@ def gpu_arm(args, rank, world):
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e_steps
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * nc / (float(t.item()) * 1e-3)
+    e2e_value = replicas.job_throughput(nc, replicas.max_over_ranks(e2e_ms, dev), world)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -256,7 +251,7 @@ def gpu_arm(args, rank, world):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * nc * 8,
                         "d2h_bytes_per_step": 2 * M * nc * 8},
                 "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
-        if not args.no_extras:
+        if not args.no_extras and world == 1:
             line["extras"] = extras_arm(args)
         print(json.dumps(line), flush=True)
 

@@ -160,3 +160,16 @@ def test_server_argument_checks_before_device_use():
     t = ctypes.c_uint64()
     assert lib.PfSolveServerSubmit(None, ctypes.byref(r), ctypes.byref(t)) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT
     lib.PfSolveServerDestroy(None)
+
+
+def test_integration_example_compiles_and_links(tmp_path):
+    """The C caller in INTEGRATION.md builds against the header and links the library."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    code = text.split("```c\n", 1)[1].split("```", 1)[0]
+    src = tmp_path / "jw_step.c"
+    src.write_text(code + "\nint main(void) { return 0; }\n")
+    cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+    libdir = os.path.dirname(capi.LIB_PATH)
+    subprocess.run([cc, "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", libdir, "-lpfsolve_b200", "-Wl,-rpath," + libdir, "-o", str(tmp_path / "jw_step")],
+                   check=True)
