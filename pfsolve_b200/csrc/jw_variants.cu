@@ -1,138 +1,35 @@
-// jw_variants.cu -- explicit instantiations of the JW-step kernel and the
-// standalone block / generic dgbmv kernels.
+// jw_variants.cu -- lookup over the kernel variant tables (jw_variants_*.cu)
+// and the standalone block / generic dgbmv kernels.
 #include <vector>
 
-#include "dd_kernel.cuh"
 #include "jw_kernel.cuh"
 #include "jw_variants.h"
 
 namespace pfb {
 
-template <class C>
-static size_t smem_fn(int W, int G)
-{
-    return jw_smem_bytes<C>(W, G);
-}
+const JwVariant* jw_variants_real(int* count);
+const JwVariant* jw_variants_chain(int* count);
+const JwVariant* jw_variants_mixed(int* count);
+const JwVariant* jw_variants_dd(int* count);
 
-template <class C>
-static void launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op, const JwIO& io, int W)
-{
-    jw_step_kernel<C><<<grid, block, smem, st>>>(op, io, W);
-}
-
-#define PFB_VT(R, KL, KU, SV, LIN, LOUT, SC, P, T)                                                     \
-    JwVariant{R, KL, KU, SV, LIN, LOUT, SC, P, T, JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>::kMaxThreads,  \
-              (const void*)&jw_step_kernel<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>,                    \
-              &smem_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>, &launch_fn<JwCfg<R, KL, KU, SV, LIN, LOUT, SC, P, T>>}
-#define PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, P) PFB_VT(R, KL, KU, SV, LIN, LOUT, SC, P, false)
-#define PFB_V(R, KL, KU, SV, LIN, LOUT, SC) PFB_VP(R, KL, KU, SV, LIN, LOUT, SC, PREC_F64)
-// coefficient-table variants (FP64), rows per thread 4 and 8
-#define PFB_T2(KL, KU, SV, LIN, LOUT, SC) \
-    PFB_VT(4, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true), PFB_VT(8, KL, KU, SV, LIN, LOUT, SC, PREC_F64, true)
-
-// double-double variants: PREC 2 = dd storage, PREC 3 = dd arithmetic on FP64 storage
-template <class C>
-static size_t dd_smem_fn(int W, int G)
-{
-    return dd_smem_bytes<C>(W, G);
-}
-template <class C>
-static void dd_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op, const JwIO& io,
-                         int W)
-{
-    jw_dd_kernel<C><<<grid, block, smem, st>>>(op, io, W);
-}
-#define PFB_DDV(R, KL, KU, SV, MEM)                                                                     \
-    JwVariant{R, KL, KU, SV, LAY_REAL, LAY_REAL, 0, (MEM) ? 2 : 3, 0, 256,                              \
-              (const void*)&jw_dd_kernel<DdCfg<R, KL, KU, SV, MEM>>, &dd_smem_fn<DdCfg<R, KL, KU, SV, MEM>>, \
-              &dd_launch_fn<DdCfg<R, KL, KU, SV, MEM>>}
-#define PFB_DD(KL, KU, SV) \
-    PFB_DDV(4, KL, KU, SV, true), PFB_DDV(8, KL, KU, SV, true), PFB_DDV(4, KL, KU, SV, false), \
-        PFB_DDV(8, KL, KU, SV, false)
-
-// Rows-per-thread choices for the single-application (drop-in) variants.
-#define PFB_R4(KL, KU, SV, LIN, LOUT, SC) \
-    PFB_V(2, KL, KU, SV, LIN, LOUT, SC), PFB_V(4, KL, KU, SV, LIN, LOUT, SC), PFB_V(8, KL, KU, SV, LIN, LOUT, SC), \
-        PFB_V(16, KL, KU, SV, LIN, LOUT, SC)
-#define PFB_R2(KL, KU, SV, LIN, LOUT, SC) PFB_V(4, KL, KU, SV, LIN, LOUT, SC), PFB_V(8, KL, KU, SV, LIN, LOUT, SC)
-#define PFB_M2(KL, KU, SV, LIN, LOUT, SC) \
-    PFB_VP(4, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED), PFB_VP(8, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED)
-
-static const JwVariant kVariants[] = {
-    // JW application, real systems in place (upperBanded 2: tridiagonal;
-    // 1: upper V / lower M; 0: lower V / upper M), by jw_type % 10.
-    PFB_R4(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),    // ub 2, jwt 3
-    PFB_R4(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),  // ub 1, jwt 0
-    PFB_R4(0, 1, SV_NONE, LAY_REAL, LAY_REAL, false),   // ub 1, jwt 1
-    PFB_R4(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),  // ub 1, jwt 2 / 3
-    PFB_R4(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),  // ub 0, jwt 0
-    PFB_R4(1, 0, SV_NONE, LAY_REAL, LAY_REAL, false),   // ub 0, jwt 1
-    PFB_R4(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),  // ub 0, jwt 2 / 3
-    // dgbmv application (band matvec only), KL, KU <= 2
-    PFB_R2(1, 1, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(2, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(0, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(2, 0, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(1, 2, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(2, 1, SV_NONE, LAY_REAL, LAY_REAL, false),
-    PFB_R2(0, 0, SV_NONE, LAY_REAL, LAY_REAL, false),
-    // fused chains: dgbmv -> JW (-> block), real
-    PFB_R2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_R2(1, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),
-    PFB_R2(1, 1, SV_TRI, LAY_REAL, LAY_REAL, false),
-    PFB_R2(2, 2, SV_TRI, LAY_REAL, LAY_REAL, false),
-    PFB_R2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, true),
-    PFB_R2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, true),
-    // fused chains on complex XXII right-hand sides -> packed complex output
-    PFB_R2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
-    PFB_R2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true),
-    PFB_R2(0, 0, SV_TRI, LAY_XXII, LAY_PACKED, false),
-    PFB_R2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true),
-    PFB_R2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, false),
-    PFB_R2(0, 0, SV_UPPER, LAY_XXII, LAY_PACKED, true),
-    // mixed precision (FP32 solve + FP64 refinement), real
-    PFB_M2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),
-    PFB_M2(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),
-    PFB_M2(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),
-    PFB_M2(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_M2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_M2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_M2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
-    // coefficient-table variants for the single-matrix launches
-    PFB_T2(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false),
-    PFB_T2(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false),
-    PFB_T2(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false),
-    PFB_T2(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_T2(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_T2(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false),
-    PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false),
-    PFB_T2(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true),
-    PFB_T2(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true),
-    // double-double (quad emulation), real systems
-    PFB_DD(0, 0, SV_TRI),
-    PFB_DD(0, 1, SV_LOWER),
-    PFB_DD(0, 1, SV_NONE),
-    PFB_DD(0, 0, SV_LOWER),
-    PFB_DD(1, 0, SV_UPPER),
-    PFB_DD(1, 0, SV_NONE),
-    PFB_DD(0, 0, SV_UPPER),
-    PFB_DD(1, 1, SV_UPPER),
-    PFB_DD(1, 1, SV_NONE),
-};
+namespace {
+using PartFn = const JwVariant* (*)(int*);
+const PartFn kParts[] = {jw_variants_real, jw_variants_chain, jw_variants_mixed, jw_variants_dd};
+}  // namespace
 
 const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC, int TBL)
 {
-    for (const JwVariant& v : kVariants)
-        if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
-            v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC && v.TBL == (TBL ? 1 : 0))
-            return &v;
+    for (PartFn part : kParts) {
+        int n = 0;
+        const JwVariant* vs = part(&n);
+        for (int i = 0; i < n; ++i) {
+            const JwVariant& v = vs[i];
+            if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
+                v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC && v.TBL == (TBL ? 1 : 0))
+                return &v;
+        }
+    }
     return nullptr;
-}
-
-const JwVariant* jw_variants(int* count)
-{
-    *count = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
-    return kVariants;
 }
 
 // ---------------------------------------------------------------------------

@@ -22,8 +22,6 @@ struct JwVariant {
 // Find a variant; nullptr when that combination was not compiled.
 const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC = 0,
                                 int TBL = 0);
-// All compiled variants (for tests and the autotuner).
-const JwVariant* jw_variants(int* count);
 
 // Persistent uneven-batch kernels (one per operator shape).
 struct BatchVariant {
