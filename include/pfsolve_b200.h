@@ -378,7 +378,8 @@ PFSOLVE_API PfSolveResult PfSolveServerAddOperator(PfSolveServer* server, int64_
 PFSOLVE_API PfSolveResult PfSolveServerSubmit(PfSolveServer* server, const PfSolveRequest* request,
                                               uint64_t* ticket);
 /* Block until the request is done; its latency (ms) when latencyMs != NULL.
- * Each ticket is waited on once. */
+ * Returns the request's status: PFSOLVE_SUCCESS, or the launch error that
+ * left its output unwritten.  Each ticket is waited on once. */
 PFSOLVE_API PfSolveResult PfSolveServerWait(PfSolveServer* server, uint64_t ticket, double* latencyMs);
 PFSOLVE_API PfSolveResult PfSolveServerGetStats(PfSolveServer* server, PfSolveServerStats* stats);
 /* Drain every queued request, then free the server. */

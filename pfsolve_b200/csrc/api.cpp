@@ -132,8 +132,7 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
             const size_t smem = v->smem_bytes(G);
             if (smem > 227 * 1024) continue;
-            if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-                continue;
+            if (!allow_max_smem(v->func)) continue;
             int blocks = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, T * G, smem) != cudaSuccess ||
                 blocks < 1)
@@ -876,9 +875,7 @@ PfSolveResult batch_configure(PfSolveBatch* b, int R)
     if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     const int G = std::max(1, 8 / (int)W);
     const size_t smem = v->smem_bytes((int)W, G);
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    if (smem > 48 * 1024 && !allow_max_smem(v->func)) return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * (int)W * G, smem) != cudaSuccess ||
         blocks < 1)

@@ -4,6 +4,7 @@
 
 #include "jw_kernel.cuh"
 #include "jw_variants.h"
+#include "plan.h"
 
 namespace pfb {
 
@@ -139,7 +140,7 @@ void launch_dgbmv_generic(const DgbmvArgs& a, cudaStream_t st, int num_sms)
     if (blocks < 1) blocks = 1;
     const size_t smem = (size_t)a.M * sizeof(double);
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(dgbmv_generic_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_max_smem((const void*)dgbmv_generic_kernel);
     dgbmv_generic_kernel<<<(unsigned)blocks, 256, smem, st>>>(a);
 }
 

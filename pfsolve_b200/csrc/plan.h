@@ -4,11 +4,33 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "../../include/pfsolve_b200.h"
 #include "jw_variants.h"
 
 namespace pfb {
+
+// Let `func` use the device's full opt-in shared memory per block.  Set once
+// per device and never lowered, so plans that launch one kernel with
+// different shared-memory sizes do not undo each other's setting.
+inline bool allow_max_smem(const void* func)
+{
+    static std::mutex mu;
+    static std::set<std::pair<int, const void*>> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({dev, func})) return true;
+    int maxopt = 0;
+    if (cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt) != cudaSuccess)
+        return false;
+    done.insert({dev, func});
+    return true;
+}
 
 // Count one kernel launch in PfSolveLaunchCount (and in
 // PfSolveStreamingLaunchCount when it ran on the streaming kernel).
@@ -86,13 +108,10 @@ inline bool jw_layout(const PfSolveConfiguration& c, bool rtM, bool rtV, int64_t
 inline bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, int& max_blocks)
 {
     int best = 0, bestG = 0, bestBlocks = 0;
-    size_t bestSmem = 0;
     for (int G = 1; 32 * W * G <= v->max_threads; ++G) {
         const size_t smem = v->smem_bytes(W, G);
         if (smem > 227 * 1024) break;
-        if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            break;
+        if (smem > 48 * 1024 && !allow_max_smem(v->func)) break;
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess)
             break;
@@ -100,13 +119,9 @@ inline bool choose_groups(const JwVariant* v, int W, int num_sms, int& G_out, in
             best = blocks * G;
             bestG = G;
             bestBlocks = blocks;
-            bestSmem = smem;
         }
     }
     if (best == 0) return false;
-    if (bestSmem > 48 * 1024 &&
-        cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bestSmem) != cudaSuccess)
-        return false;
     G_out = bestG;
     max_blocks = bestBlocks * num_sms;
     return true;

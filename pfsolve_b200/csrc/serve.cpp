@@ -52,6 +52,7 @@ struct Req {
     int64_t M;
     uint64_t bytes;
     int cls;  // batch class: precision class and operator kind (one kernel per batch)
+    PfSolveResult status = PFSOLVE_SUCCESS;
     Clock::time_point t_submit, t_done;
     bool done = false;
 };
@@ -121,8 +122,7 @@ bool batch_shape(PfSolveServer* s, const BatchVariant* v, int W, Shape& out)
     for (int G = std::max(1, 8 / W); G >= 1; --G) {
         const size_t smem = v->smem_bytes(W, G);
         if (smem > 227 * 1024) continue;
-        if (cudaFuncSetAttribute(v->func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            continue;
+        if (!allow_max_smem(v->func)) continue;
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * W * G, smem) != cudaSuccess ||
             blocks < 1)
@@ -222,7 +222,9 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
         const ServeOp& o0 = s->ops[fl.reqs[0]->r.op];
         const BatchVariant* v = find_batch_variant(R, o0.KL, o0.KU, o0.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED);
         Shape sh;
-        if (v && batch_shape(s, v, W, sh)) {
+        if (!v || !batch_shape(s, v, W, sh)) {
+            for (Req* r : fl.reqs) r->status = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        } else {
             // items: enough per group for balance, within the staging capacity
             const int64_t groups = (int64_t)sh.max_blocks * sh.G;
             int64_t spi = std::max<int64_t>(1, std::min<int64_t>(64, (S + 2 * groups - 1) / (2 * groups)));
@@ -254,6 +256,8 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
             v->launch(dim3((unsigned)grid), dim3(32 * W * sh.G), sh.smem, fl.stream, fl.d_entries, fl.d_items, k,
                       fl.d_counter, W);
             note_launch(false);
+            if (cudaGetLastError() != cudaSuccess)
+                for (Req* r : fl.reqs) r->status = PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
         }
     } else {
         for (Req* r : fl.reqs) {
@@ -263,12 +267,16 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
             const int prec = (r->r.precision == PFSOLVE_SERVE_DD) ? 2 : 3;
             const JwVariant* v = find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, prec, 0);
             Shape sh;
-            if (!v || !jw_shape(s, v, W, sh)) continue;
+            if (!v || !jw_shape(s, v, W, sh)) {
+                r->status = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+                continue;
+            }
             const JwOperator op = make_operator(s, o, r->r);
             const JwIO io = make_io(o, r->r);
             const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((io.nsys + sh.G - 1) / sh.G, sh.max_blocks));
             v->launch(dim3((unsigned)grid), dim3(32 * W * sh.G), sh.smem, fl.stream, op, io, W);
             note_launch(false);
+            if (cudaGetLastError() != cudaSuccess) r->status = PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
         }
     }
     cudaLaunchHostFunc(fl.stream, on_flight_done, &fl);
@@ -452,9 +460,10 @@ PfSolveResult PfSolveServerWait(PfSolveServer* s, uint64_t ticket, double* laten
     Req* q = it->second;
     s->done_cv.wait(lk, [&] { return q->done; });
     if (latencyMs) *latencyMs = ms_between(q->t_submit, q->t_done);
+    const PfSolveResult status = q->status;
     s->reqs.erase(it);
     delete q;
-    return PFSOLVE_SUCCESS;
+    return status;
 }
 
 PfSolveResult PfSolveServerGetStats(PfSolveServer* s, PfSolveServerStats* out)
