@@ -313,6 +313,29 @@ PFSOLVE_API PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* batch, int* r
                                                int* systemsPerItem, int* items, double* tunedMs);
 PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
 
+/* One uneven batch, as PfSolveBatchCreate + PfSolveBatchAppend +
+ * PfSolveBatchDestroy, that allocates nothing: no cudaMalloc, no cudaFree,
+ * no host heap.  For callers that must not reach the device allocator during
+ * their time loop -- code whose device memory is all owned by its own pool,
+ * or which cannot afford the implicit device synchronisation and the failure
+ * modes of cudaMalloc.  No counterpart in the reference.
+ * The work list, the entry descriptors and the work counter live in one fixed
+ * device array inside the library, sized for PFSOLVE_NOALLOC_MAX_ENTRIES
+ * entries and PFSOLVE_NOALLOC_MAX_ITEMS work items (ceil(nsys /
+ * systemsPerItem) per entry, systemsPerItem 0 meaning 64); larger calls return
+ * PFSOLVE_ERROR_CAPACITY.  The work counter must start at zero: each call
+ * clears it on `stream` before its launch.  All calls share the array, so two
+ * calls whose work overlaps in time (on other streams or from other threads)
+ * race; serialise them.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that call before any stream
+ * capture on the device.  Results equal PfSolveBatchAppend's for the same
+ * descriptor, rows per thread and systems per item. */
+#define PFSOLVE_NOALLOC_MAX_ENTRIES 1024
+#define PFSOLVE_NOALLOC_MAX_ITEMS 16384
+PFSOLVE_API PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolveBatchDesc* desc,
+                                                   const PfSolveBatchEntry* entries, int nentries,
+                                                   cudaStream_t stream);
+
 /* Number of kernel launches this library has enqueued since load (all apps). */
 PFSOLVE_API uint64_t PfSolveLaunchCount(void);
 

@@ -132,6 +132,7 @@ class PfSolveServerStats(ctypes.Structure):
 
 
 PFSOLVE_SERVE_MIXED, PFSOLVE_SERVE_DD, PFSOLVE_SERVE_DD_FP64MEM = 1, 2, 3
+PFSOLVE_NOALLOC_MAX_ENTRIES, PFSOLVE_NOALLOC_MAX_ITEMS = 1024, 16384
 
 # Every function the header declares, with its ctypes signature.
 _APP_P = ctypes.POINTER(PfSolveApplication)
@@ -170,6 +171,8 @@ SIGNATURES = {
     "PfSolveBatchAutotune": (c_int, [ctypes.c_void_p, ctypes.c_void_p, c_int]),
     "PfSolveBatchGetShape": (c_int, [ctypes.c_void_p] + [ctypes.POINTER(c_int)] * 4 + [ctypes.POINTER(ctypes.c_double)]),
     "PfSolveBatchDestroy": (None, [ctypes.c_void_p]),
+    "PfSolveBatchAppendNoAlloc": (c_int, [c_int, ctypes.POINTER(PfSolveBatchDesc), ctypes.POINTER(PfSolveBatchEntry),
+                                          c_int, ctypes.c_void_p]),
 }
 
 _lib = None
