@@ -106,7 +106,7 @@ int pick_rows_per_thread(int64_t M, int requested)
 bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {
     s->stream_v = nullptr;
-    if (s->prec != 0 || s->no_stream) return false;
+    if ((s->prec != PREC_F64 && s->prec != PREC_MIXED) || s->no_stream) return false;
     int cand[3][2];
     int n = 0;
     const int prefs[3] = {16, 32, 8};
@@ -126,7 +126,8 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
             std::swap(cand[j], cand[j - 1]);
         }
     for (int i = 0; i < n; ++i) {
-        const StreamVariant* v = find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE);
+        const StreamVariant* v =
+            find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
         if (!v) continue;
         const int T = 32 * v->W;
         for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
@@ -175,6 +176,10 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
             return PFSOLVE_SUCCESS;
         }
     }
+    // No group-kernel variant fits: a streaming-only plan, whose launches need
+    // buffers the streaming kernel can take.
+    s->variant = nullptr;
+    if (choose_stream(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
     // nothing compiled fits: distinguish "too long" from "not compiled"
     for (int R : {2, 4, 8, 16})
         if ((M + 32 * (int64_t)R - 1) / (32 * (int64_t)R) <= 8) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
@@ -307,6 +312,7 @@ PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& i
         }
         return PFSOLVE_SUCCESS;
     }
+    if (!s->variant) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // streaming-only plan
     const int64_t want = (io.nsys + s->G - 1) / s->G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->max_blocks));
     const size_t smem = s->variant->smem_bytes(s->W, s->G);

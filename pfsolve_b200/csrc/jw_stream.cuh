@@ -32,18 +32,26 @@ namespace pfb {
 constexpr unsigned kStatusWaitTimeout = 1u;
 static __device__ unsigned int g_stream_status;
 
-template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_>
+template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_, int PREC_ = PREC_F64>
 struct StCfg {
     static constexpr int R = R_, W = W_, KL = KL_, KU = KU_, SV = SV_, LIN = LIN_, LOUT = LOUT_;
     static constexpr bool SCALE = SCALE_;
     static constexpr bool CPLX = (LIN != LAY_REAL);
     using V = typename std::conditional<CPLX, double2, double>::type;
+    using VF = typename Lower<V>::type;
     static constexpr int T = 32 * W;  // chunks (threads) per group
     static constexpr int NB = KL + KU + 1;
     static constexpr bool FWD = (SV == SV_LOWER || SV == SV_TRI);
     static constexpr bool BWD = (SV == SV_UPPER || SV == SV_TRI);
-    // coefficient table planes: NB weights, -l, -h, Scale factor
-    static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0), P_SC = P_NH + (BWD ? 1 : 0);
+    static constexpr bool MIXED = (PREC_ == PREC_MIXED) && (SV != SV_NONE);
+    // Coefficient table planes, each 16 bytes per (row pair, thread).
+    // FP64: NB weights (scaled by the LU pivots), -l, -h, Scale factor.
+    // Mixed: NB weights (unscaled), the solve's sub- and super-diagonal in FP64
+    // (residual), FP32 packs {m, m', -l, -l'} and {-h, -h', 0, 0}, Scale factor.
+    static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0);  // FP64 path
+    static constexpr int P_AL = NB, P_CU = NB + (FWD ? 1 : 0);  // mixed path
+    static constexpr int P_F1 = P_CU + (BWD ? 1 : 0), P_F2 = P_F1 + 1;
+    static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0);
     static constexpr int NPL = P_SC + (SCALE ? 1 : 0);
     // Input: NPIN planes of 8-byte rows; a chunk holds U 16-byte units per
     // plane, stored as H swizzle rows of IB units (TMA box inner extent).
@@ -64,7 +72,7 @@ struct StCfg {
     // A warp's input and output bytes coincide when both layouts have the same
     // swizzle rows; otherwise a warp's staging overlaps its neighbours' input.
     static constexpr bool kSameRows = (IB == IBO) && (NPIN * H == NPOUT * HO);
-    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2);
+    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2) * (MIXED ? 2 : 1);
     static constexpr int kMaxThreads = kDataRegs >= 64 ? 256 : 512;
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
     static_assert(KL <= 2 && KU <= 2, "halo of at most two rows");
@@ -205,10 +213,9 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
         const int64_t i = s + j;
         if (i >= rows) break;
         double w[NB];
-        double nl = 0.0, nh = 0.0, sc = 0.0;
+        double nl = 0.0, nh = 0.0, sc = 0.0, m = 1.0, al = 0.0, cu = 0.0;
         if (i < M) {
             jw_row_weights<C::KL, NB>(op, i, w);
-            double m = 1.0;
             if constexpr (C::SV == SV_TRI) {
                 const double ai = (i >= 1) ? band(op, op.off_sl, i) : 0.0;
                 const double ci = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
@@ -218,13 +225,19 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
                 dprev = dp;
                 nl = -(ai * m);
                 nh = -(ci * m);
+                al = ai;
+                cu = ci;
             } else if constexpr (C::SV == SV_LOWER) {
-                nl = (i >= 1) ? -band(op, op.off_sl, i) : 0.0;
+                al = (i >= 1) ? band(op, op.off_sl, i) : 0.0;
+                nl = -al;
             } else if constexpr (C::SV == SV_UPPER) {
-                nh = (i < M - 1) ? -band(op, op.off_su, i) : 0.0;
+                cu = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
+                nh = -cu;
             }
+            if constexpr (!C::MIXED) {
 #pragma unroll
-            for (int k = 0; k < NB; ++k) w[k] *= m;
+                for (int k = 0; k < NB; ++k) w[k] *= m;
+            }
             if constexpr (C::SCALE) sc = scale_factor(op.scale_kind, i, op.lshift, op.scale_s);
         } else {
 #pragma unroll
@@ -232,10 +245,24 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
         }
         const int tt = (int)(i / R), jj = (int)(i % R);
         auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * T + tt) * 2 + (jj & 1)] = v; };
+        auto put32 = [&](int p, int k, double v) {
+            reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * T + tt) * 4 + k + (jj & 1)] = (float)v;
+        };
 #pragma unroll
         for (int k = 0; k < NB; ++k) put(k, w[k]);
-        if constexpr (C::FWD) put(C::P_NL, nl);
-        if constexpr (C::BWD) put(C::P_NH, nh);
+        if constexpr (C::MIXED) {
+            if constexpr (C::FWD) put(C::P_AL, al);
+            if constexpr (C::BWD) put(C::P_CU, cu);
+            put32(C::P_F1, 0, m);
+            put32(C::P_F1, 2, nl);
+            if constexpr (C::BWD) {
+                put32(C::P_F2, 0, nh);
+                put32(C::P_F2, 2, 0.0);
+            }
+        } else {
+            if constexpr (C::FWD) put(C::P_NL, nl);
+            if constexpr (C::BWD) put(C::P_NH, nh);
+        }
         if constexpr (C::SCALE) put(C::P_SC, sc);
     }
 }
@@ -283,9 +310,13 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     const double2* tb = reinterpret_cast<const double2*>(table) + t;  // pair (p, u) at tb[(p*U + u)*T]
     auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * T]; };
 
-    // Scan multipliers: products of -l and -h over this thread's chunk.
+    auto coef4 = [&](int p, int u) -> float4 { return reinterpret_cast<const float4*>(tb)[(p * U + u) * T]; };
+
+    // Scan multipliers: products of -l and -h over this thread's chunk (in the
+    // precision of the solve that uses them).
     double Af = 1.0, Ab = 1.0;
-    if constexpr (C::FWD) {
+    float Af32 = 1.0f, Ab32 = 1.0f;
+    if constexpr (C::FWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const double2 c = coef(C::P_NL, u);
@@ -293,12 +324,28 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             Af = c.y * Af;
         }
     }
-    if constexpr (C::BWD) {
+    if constexpr (C::BWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const double2 c = coef(C::P_NH, u);
             Ab = c.x * Ab;
             Ab = c.y * Ab;
+        }
+    }
+    if constexpr (C::FWD && C::MIXED) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const float4 c = coef4(C::P_F1, u);
+            Af32 = (u == 0) ? c.z : c.z * Af32;
+            Af32 = c.w * Af32;
+        }
+    }
+    if constexpr (C::BWD && C::MIXED) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const float4 c = coef4(C::P_F2, u);
+            Ab32 = c.x * Ab32;
+            Ab32 = c.y * Ab32;
         }
     }
 
@@ -427,7 +474,87 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             issue_load(nxt, (k & 1) ? bar0 : bar1, sys + step);
         }
 
-        if constexpr (C::FWD) {
+        if constexpr (C::MIXED) {
+            // x = M^{-1} g: FP32 solves of the residual, accumulated in FP64
+            // (one initial solve, refine_sweeps - 1 refinements).
+            using VF = typename C::VF;
+            using OF = VOps<VF>;
+            V gv[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                gv[j] = x[j];
+                x[j] = O::zero();
+            }
+            for (int it = 0; it < op.refine_sweeps; ++it) {
+                VF d[R];
+                if (it == 0) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const float4 f = coef4(C::P_F1, u);
+                        d[2 * u] = OF::mul(f.x, to_f32(gv[2 * u]));
+                        d[2 * u + 1] = OF::mul(f.y, to_f32(gv[2 * u + 1]));
+                    }
+                } else {
+                    // r = g - M x in FP64 (M: unit diagonal, sub al, super cu)
+                    V prev, next;
+                    group_neighbours<V>(g, x[0], x[R - 1], prev, next);
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const float4 f = coef4(C::P_F1, u);
+                        double2 al = make_double2(0.0, 0.0), cu = make_double2(0.0, 0.0);
+                        if constexpr (C::FWD) al = coef(C::P_AL, u);
+                        if constexpr (C::BWD) cu = coef(C::P_CU, u);
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int j = 2 * u + e;
+                            V mx = x[j];
+                            if constexpr (C::FWD) mx = O::fma(e ? al.y : al.x, j > 0 ? x[j - 1] : prev, mx);
+                            if constexpr (C::BWD) mx = O::fma(e ? cu.y : cu.x, j < R - 1 ? x[j + 1] : next, mx);
+                            d[j] = OF::mul(e ? f.y : f.x, to_f32(O::fma(-1.0, mx, gv[j])));
+                        }
+                    }
+                }
+                if constexpr (C::FWD) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const float4 f = coef4(C::P_F1, u);
+                        if (u > 0) d[2 * u] = OF::fma(f.z, d[2 * u - 1], d[2 * u]);
+                        d[2 * u + 1] = OF::fma(f.w, d[2 * u], d[2 * u + 1]);
+                    }
+                    const VF pin = group_affine_scan<VF, float, true>(g, Af32, d[R - 1]);
+                    float p = 1.0f;
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const float4 f = coef4(C::P_F1, u);
+                        p = f.z * p;
+                        d[2 * u] = OF::fma(p, pin, d[2 * u]);
+                        p = f.w * p;
+                        d[2 * u + 1] = OF::fma(p, pin, d[2 * u + 1]);
+                    }
+                }
+                if constexpr (C::BWD) {
+#pragma unroll
+                    for (int u = U - 1; u >= 0; --u) {
+                        const float4 f = coef4(C::P_F2, u);
+                        if (u < U - 1) d[2 * u + 1] = OF::fma(f.y, d[2 * u + 2], d[2 * u + 1]);
+                        d[2 * u] = OF::fma(f.x, d[2 * u + 1], d[2 * u]);
+                    }
+                    const VF q = group_affine_scan<VF, float, false>(g, Ab32, d[0]);
+                    float p = 1.0f;
+#pragma unroll
+                    for (int u = U - 1; u >= 0; --u) {
+                        const float4 f = coef4(C::P_F2, u);
+                        p = f.y * p;
+                        d[2 * u + 1] = OF::fma(p, q, d[2 * u + 1]);
+                        p = f.x * p;
+                        d[2 * u] = OF::fma(p, q, d[2 * u]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
+            }
+        }
+        if constexpr (C::FWD && !C::MIXED) {
             // z_j = x_j - l_j z_{j-1} within the chunk, then add the coupling
             // from the preceding chunks scaled by prod_{k<=j}(-l_k)
 #pragma unroll
@@ -447,7 +574,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 x[2 * u + 1] = O::fma(p, pin, x[2 * u + 1]);
             }
         }
-        if constexpr (C::BWD) {
+        if constexpr (C::BWD && !C::MIXED) {
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
                 const double2 c = coef(C::P_NH, u);

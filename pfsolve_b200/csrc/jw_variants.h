@@ -37,7 +37,7 @@ const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, i
 // system).  IB / IBO: 16-byte units per swizzle row of the input / output
 // layout (the TMA box's inner extent).
 struct StreamVariant {
-    int R, W, KL, KU, SV, LIN, LOUT, SCALE;
+    int R, W, KL, KU, SV, LIN, LOUT, SCALE, PREC;
     int max_threads;
     const void* func;
     size_t (*smem_bytes)(int G);
@@ -45,8 +45,8 @@ struct StreamVariant {
     void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
                    const JwOperator& op, const JwIO& io);
 };
-const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE);
-const StreamVariant* stream_variants(int* count);
+const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE,
+                                        int PREC);
 // Tensor maps of a launch's input and output rows; false when the buffers'
 // alignment, strides or M do not allow the streaming layout.
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out);

@@ -1,74 +1,30 @@
-// stream_variants.cu -- instantiations of the streaming JW-step kernel, the
-// TMA tensor maps that describe a launch's right-hand sides, and the device
-// status word of its bounded waits.
+// stream_variants.cu -- lookup over the streaming kernel variant tables
+// (stream_variants_*.cu), the TMA tensor maps that describe a launch's
+// right-hand sides, and the status of the kernels' bounded waits.
 #include <cuda.h>
 
-#include "jw_stream.cuh"
 #include "jw_variants.h"
 
 namespace pfb {
 
-template <class C>
-static size_t st_smem_fn(int G)
+const StreamVariant* stream_variants_f64(int* count);
+const StreamVariant* stream_variants_mixed(int* count);
+unsigned stream_status_f64();
+unsigned stream_status_mixed();
+
+const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)
 {
-    return st_smem_bytes<C>(G);
-}
-
-template <class C>
-static void st_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in,
-                         const CUtensorMap* out, const JwOperator& op, const JwIO& io)
-{
-    jw_stream_kernel<C><<<grid, block, smem, st>>>(*in, *out, op, io);
-}
-
-#define PFB_SV(R, W, KL, KU, SV, LIN, LOUT, SC)                                                               \
-    StreamVariant{R, W, KL, KU, SV, LIN, LOUT, SC, StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>::kMaxThreads,          \
-                  (const void*)&jw_stream_kernel<StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>>,                        \
-                  &st_smem_fn<StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>>, StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>::IB, \
-                  StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>::IBO, &st_launch_fn<StCfg<R, W, KL, KU, SV, LIN, LOUT, SC>>}
-// real systems: 8 rows per thread (M <= 256, 512, 1024), 16 (M <= 512, 1024,
-// 2048) and 32 (M <= 1024, 2048, 4096)
-#define PFB_SREAL(KL, KU, SV)                                                                                   \
-    PFB_SV(8, 1, KL, KU, SV, LAY_REAL, LAY_REAL, false), PFB_SV(8, 2, KL, KU, SV, LAY_REAL, LAY_REAL, false),   \
-        PFB_SV(8, 4, KL, KU, SV, LAY_REAL, LAY_REAL, false), PFB_SV(16, 1, KL, KU, SV, LAY_REAL, LAY_REAL, false), \
-        PFB_SV(16, 2, KL, KU, SV, LAY_REAL, LAY_REAL, false), PFB_SV(16, 4, KL, KU, SV, LAY_REAL, LAY_REAL, false), \
-        PFB_SV(32, 1, KL, KU, SV, LAY_REAL, LAY_REAL, false), PFB_SV(32, 2, KL, KU, SV, LAY_REAL, LAY_REAL, false), \
-        PFB_SV(32, 4, KL, KU, SV, LAY_REAL, LAY_REAL, false)
-// complex XXII right-hand sides written packed
-#define PFB_SCPLX(KL, KU, SV, SC)                                                                           \
-    PFB_SV(16, 1, KL, KU, SV, LAY_XXII, LAY_PACKED, SC), PFB_SV(16, 2, KL, KU, SV, LAY_XXII, LAY_PACKED, SC), \
-        PFB_SV(32, 1, KL, KU, SV, LAY_XXII, LAY_PACKED, SC), PFB_SV(32, 2, KL, KU, SV, LAY_XXII, LAY_PACKED, SC)
-
-static const StreamVariant kStreamVariants[] = {
-    // JW application on real systems (see kVariants for the operator kinds)
-    PFB_SREAL(0, 0, SV_TRI),
-    PFB_SREAL(0, 1, SV_LOWER),
-    PFB_SREAL(0, 1, SV_NONE),
-    PFB_SREAL(0, 0, SV_LOWER),
-    PFB_SREAL(1, 0, SV_UPPER),
-    PFB_SREAL(1, 0, SV_NONE),
-    PFB_SREAL(0, 0, SV_UPPER),
-    // fused chains
-    PFB_SREAL(1, 1, SV_UPPER),
-    PFB_SREAL(2, 2, SV_TRI),
-    PFB_SCPLX(2, 2, SV_TRI, false),
-    PFB_SCPLX(2, 2, SV_TRI, true),
-    PFB_SCPLX(1, 1, SV_UPPER, true),
-};
-
-const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE)
-{
-    for (const StreamVariant& v : kStreamVariants)
-        if (v.R == R && v.W == W && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
-            v.SCALE == (SCALE ? 1 : 0))
-            return &v;
+    for (auto part : {stream_variants_f64, stream_variants_mixed}) {
+        int n = 0;
+        const StreamVariant* vs = part(&n);
+        for (int i = 0; i < n; ++i) {
+            const StreamVariant& v = vs[i];
+            if (v.R == R && v.W == W && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
+                v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC)
+                return &v;
+        }
+    }
     return nullptr;
-}
-
-const StreamVariant* stream_variants(int* count)
-{
-    *count = (int)(sizeof(kStreamVariants) / sizeof(kStreamVariants[0]));
-    return kStreamVariants;
 }
 
 // ---- Tensor maps.  cuTensorMapEncodeTiled is a host-side driver entry
@@ -138,10 +94,9 @@ bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in,
 
 unsigned stream_status_fetch_clear()
 {
-    unsigned v = 0, zero = 0;
-    if (cudaMemcpyFromSymbol(&v, g_stream_status, sizeof(v)) != cudaSuccess) return ~0u;
-    if (v) cudaMemcpyToSymbol(g_stream_status, &zero, sizeof(zero));
-    return v;
+    const unsigned a = stream_status_f64(), b = stream_status_mixed();
+    if (a == ~0u || b == ~0u) return ~0u;
+    return a | b;
 }
 
 }  // namespace pfb

@@ -182,3 +182,48 @@ def test_streaming_chain_config2_form(R, block, lshift):
 def test_device_status_clean():
     from pfsolve_b200.api import device_status
     assert device_status() == 0
+
+
+# Mixed precision on the streaming kernel: FP32 solves with FP64 residual
+# refinement; <= 1e-12 relative L2 after two refinement sweeps (1e-10 after
+# one) against the __float128 oracle, as for the group kernel.
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (1, 12), (1, 13), (0, 10), (0, 12), (0, 13)])
+@pytest.mark.parametrize("M", [256, 512, 1024, 4096])
+def test_streaming_mixed_precision(ub, jwt, M):
+    rng = np.random.default_rng(8100 + 10 * ub + jwt + M)
+    case, bands, rhs = _case(rng, M, 129, ub, jwt)
+    ref = O.jw_step(case, bands, rhs, "q")
+    for refine, tol in ((1, 1e-10), (2, 1e-12)):
+        x, n = _run(case, bands, rhs, mixedPrecisionRefinement=refine)
+        assert n == 1, "the mixed launch did not run on the streaming kernel"
+        e, _ = J.rel_err(x, ref, case)
+        assert e <= tol, (refine, e)
+
+
+def test_streaming_mixed_config3_weakly_dominant():
+    wl = WL.config3(B=256)
+    case = O.Case(M=wl.M, batch=wl.nrhs, upperBanded=2, jw_type=13)
+    ref = O.jw_step(case, wl.jw_bands, wl.rhs, "q")
+    x, n = _run(case, wl.jw_bands, wl.rhs, mixedPrecisionRefinement=2)
+    assert n == 1
+    e, _ = J.rel_err(x, ref, case)
+    assert e <= 1e-12, e
+    xg, ng = _run(case, wl.jw_bands, wl.rhs, mixedPrecisionRefinement=2, kernelPath=1)
+    assert ng == 0
+    assert J.rel_err(xg, ref, case)[0] <= 1e-12
+
+
+def test_streaming_mixed_chain_config2_form():
+    wl = WL.config2(B=64)
+    M, Y = wl.M, 64
+    rhs, got, n = _chain(wl, Y, 7, 0, mixedPrecisionRefinement=2)
+    assert n == 1
+    c1 = O.Case(M=M, batch=2 * Y, LDA=5, KU=2, KL=2, jw_type=0)
+    y = O.dgbmv(c1, wl.dgbmv, rhs)
+    c2 = O.Case(M=M, batch=2 * Y, upperBanded=2, jw_type=13)
+    x = O.jw_step(c2, wl.jw_bands, y, "q")
+    cb = O.Case(M=M, batch=Y, block=7, jw_type=0, bitmask=O.RUNTIME_SCALEC, run_scaleC=0.5)
+    ref = O.block(cb, x, np.zeros(2 * M * Y)).reshape(Y, M, 2)
+    got = got.reshape(Y, M, 2)
+    e = max(np.linalg.norm(got[k] - ref[k]) / np.linalg.norm(ref[k]) for k in range(Y))
+    assert e <= 1e-12, e
