@@ -216,26 +216,55 @@ def gpu_arm(args, rank, world):
             print(json.dumps({"profile_case": True, "ncplx": nc, "ms_per_step": ms_max, "gbs": achieved,
                               "gpu_launches": int(launches), "kernel": jw.shape()}), flush=True)
         return
+    # Double-buffered on three streams: the H2D of step k+1 (PCIe up) overlaps
+    # the D2H of step k (PCIe down); each step still copies its whole input
+    # in and its whole result out inside the timed region.
     host_in = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
     host_in.copy_(rhs.cpu())
-    host_out = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
-    e_steps = max(2, min(args.steps, 5))
-    for _ in range(2):
-        rhs.copy_(host_in, non_blocking=True)
-        step()
-        host_out.copy_(out, non_blocking=True)
+    host_out = [torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    dev_in = [rhs, torch.empty_like(rhs)]
+    dev_out = [out, torch.empty_like(out)]
+    s_up, s_comp, s_down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    jw_e = App(device=local, stream=s_comp.cuda_stream, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * nc),
+               upperBanded=2, jw_type=13, doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows,
+               kernelPath=args.path)
+    apps_e = [dg, jw_e, bl]
+    lps_e = [[dg.launch_params(outputBuffer=dev_in[b]), jw_e.launch_params(outputBuffer=dev_in[b]),
+              bl.launch_params(buffer=dev_in[b], outputBuffer=dev_out[b])] for b in range(2)]
+    ev_up = [torch.cuda.Event() for _ in range(2)]
+    ev_comp = [torch.cuda.Event() for _ in range(2)]
+    ev_down = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_step(k):
+        b = k & 1
+        s_up.wait_event(ev_comp[b])  # the kernel of step k-2 has read dev_in[b]
+        with torch.cuda.stream(s_up):
+            dev_in[b].copy_(host_in, non_blocking=True)
+        ev_up[b].record(s_up)
+        s_comp.wait_event(ev_up[b])
+        s_comp.wait_event(ev_down[b])  # the D2H of step k-2 has read dev_out[b]
+        append_chain(apps_e, lps_e[b])
+        ev_comp[b].record(s_comp)
+        s_down.wait_event(ev_comp[b])
+        with torch.cuda.stream(s_down):
+            host_out[b].copy_(dev_out[b], non_blocking=True)
+        ev_down[b].record(s_down)
+
+    e_steps = max(4, min(args.steps, 10))
+    for k in range(2):
+        e2e_step(k)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    e0.record()
-    for _ in range(e_steps):
-        rhs.copy_(host_in, non_blocking=True)
-        step()
-        host_out.copy_(out, non_blocking=True)
-    e1.record()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(s_up)
+    for k in range(e_steps):
+        e2e_step(k)
+    t1.record(s_down)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e_steps
+    e2e_ms = t0.elapsed_time(t1) / e_steps
     e2e_value = replicas.job_throughput(nc, replicas.max_over_ranks(e2e_ms, dev), world)
+    jw_e.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -254,7 +283,9 @@ def gpu_arm(args, rank, world):
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                              "bytes_per_launch": bytes_alg},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * nc * 8,
-                        "d2h_bytes_per_step": 2 * M * nc * 8},
+                        "d2h_bytes_per_step": 2 * M * nc * 8, "steps": e_steps, "ms_per_step": e2e_ms,
+                        "pipeline": "pinned host buffers; H2D, kernel and D2H on three streams, double-buffered: "
+                                    "step k+1's upload overlaps step k's download"},
                 "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
         if not args.no_extras and world == 1:
             line["extras"] = extras_arm(args)
@@ -369,15 +400,53 @@ def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):
     lat, wall, lag = run_load(srv, reqs, WL.poisson_arrivals(n, rate, seed=4))
     st1 = srv.stats()
     srv.close()
-    lat = np.sort(np.asarray(lat))
+    lat_all = np.asarray(lat)
+    prec = np.asarray([r[1] for r in reqs])
+    slow = [dict(M=int(specs[i % pool].M), nrhs=int(reqs[i][2]), precision=int(reqs[i][1]), ms=float(lat_all[i]))
+            for i in np.argsort(-lat_all)[:8]]
+    by_prec = {("mixed" if p == 1 else "dd"): {"p50_ms": float(np.percentile(lat_all[prec == p], 50)),
+                                               "p99_ms": float(np.percentile(lat_all[prec == p], 99))}
+               for p in (1, 2) if (prec == p).any()}
+    lat = np.sort(lat_all)
     rhs = sum(r[2] for r in reqs)
     nbytes = sum(r[3].numel() * 8 * 2 for r in reqs)
     return {"requests": n, "offered_rate_per_s": rate, "achieved_rate_per_s": n / wall,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "max_ms": float(lat[-1]), "rhs_per_s": rhs / wall, "hbm_gbs_offered": nbytes / wall / 1e9,
             "batches": st1["batches"] - st0["batches"], "submitter_max_lag_ms": 1e3 * lag,
+            "server_p99_queue_ms": st1["p99QueueMs"], "server_p99_device_ms": st1["p99DeviceMs"],
+            "by_precision": by_prec, "slowest": slow,
             "mix": "80% mixed (FP32 solve + 2 FP64 refinement sweeps), 20% double-double storage",
             "streams": 8, "max_batch_requests": 32, "hbm_budget_bytes": 16 << 30}
+
+
+def config3_profile(args):
+    """Profiling case: config 3 (N = 512 real tridiagonal, weakly dominant),
+    `--ncplx` systems, FP64 or mixed precision (`--refine`), K timed steps;
+    prints one JSON line with the kernel time."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App
+    wl = WL.config3(B=args.ncplx)
+    M, B = wl.M, wl.nrhs
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    x = torch.from_numpy(wl.rhs).cuda()
+    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
+              scaleC=1.0, mixedPrecisionRefinement=args.refine, rowsPerThread=args.rows, kernelPath=args.path)
+    for _ in range(max(1, args.warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"profile_case": "config3", "rhs": B, "refine": args.refine, "ms_per_step": ms,
+                      "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9, "kernel": app.shape()}), flush=True)
+    app.close()
 
 
 def main():
@@ -392,6 +461,9 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3"],
+                    help="profiling case (--profile): the config 2 chain or config 3 (--ncplx real systems)")
+    ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1],
                     help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
     args = ap.parse_args()
@@ -407,6 +479,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     if args.serve:
         print(json.dumps({"config5_serving": serving_leg()}), flush=True)
+        return
+    if args.profile and args.workload == "config3":
+        config3_profile(args)
         return
     try:
         if args.impl == "reference":

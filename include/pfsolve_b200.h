@@ -388,6 +388,8 @@ typedef struct {
     uint64_t submitted, completed, batches, rhs;
     uint64_t peakInflightBytes;
     double p50Ms, p99Ms, maxMs;  /* submit -> completion on the GPU, over completed requests */
+    double p99QueueMs;           /* submit -> launch enqueued (queueing and admission) */
+    double p99DeviceMs;          /* launch enqueued -> completion (device time and completion signal) */
 } PfSolveServerStats;
 
 PFSOLVE_API PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSolveServerDesc* desc);

@@ -128,7 +128,7 @@ class PfSolveRequest(ctypes.Structure):
 class PfSolveServerStats(ctypes.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("batches", u64), ("rhs", u64),
                 ("peakInflightBytes", u64), ("p50Ms", ctypes.c_double), ("p99Ms", ctypes.c_double),
-                ("maxMs", ctypes.c_double)]
+                ("maxMs", ctypes.c_double), ("p99QueueMs", ctypes.c_double), ("p99DeviceMs", ctypes.c_double)]
 
 
 PFSOLVE_SERVE_MIXED, PFSOLVE_SERVE_DD, PFSOLVE_SERVE_DD_FP64MEM = 1, 2, 3

@@ -53,7 +53,7 @@ struct Req {
     uint64_t bytes;
     int cls;  // batch class: precision class and operator kind (one kernel per batch)
     PfSolveResult status = PFSOLVE_SUCCESS;
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_dispatch, t_done;
     bool done = false;
 };
 
@@ -83,6 +83,7 @@ struct PfSolveServer {
     int num_sms = 0;
     std::deque<ServeOp> ops;  // references stay valid while operators are added
     std::map<std::pair<const void*, int>, Shape> shapes;  // (kernel, W) -> groups, blocks
+    std::mutex shape_mu;                                   // guards `shapes`
     std::mutex mu;
     std::condition_variable cv;       // worker
     std::condition_variable done_cv;  // waiters
@@ -92,7 +93,7 @@ struct PfSolveServer {
     uint64_t next_id = 1;
     uint64_t inflight_bytes = 0, peak_inflight = 0;
     uint64_t submitted = 0, completed = 0, batches = 0, rhs = 0;
-    std::vector<double> lat_ms;
+    std::vector<double> lat_ms, queue_ms, device_ms;
     bool stop = false;
     std::thread worker;
 };
@@ -116,6 +117,7 @@ void serve_rows(int64_t Mmax, int& R, int& W)
 
 bool batch_shape(PfSolveServer* s, const BatchVariant* v, int W, Shape& out)
 {
+    std::lock_guard<std::mutex> lk(s->shape_mu);
     auto key = std::make_pair(v->func, W);
     auto it = s->shapes.find(key);
     if (it != s->shapes.end()) { out = it->second; return true; }
@@ -139,6 +141,7 @@ bool batch_shape(PfSolveServer* s, const BatchVariant* v, int W, Shape& out)
 
 bool jw_shape(PfSolveServer* s, const JwVariant* v, int W, Shape& out)
 {
+    std::lock_guard<std::mutex> lk(s->shape_mu);
     auto key = std::make_pair(v->func, W);
     auto it = s->shapes.find(key);
     if (it != s->shapes.end()) { out = it->second; return true; }
@@ -199,6 +202,8 @@ void CUDART_CB on_flight_done(void* p)
         s->completed++;
         s->rhs += (uint64_t)r->r.nrhs;
         s->lat_ms.push_back(ms_between(r->t_submit, now));
+        s->queue_ms.push_back(ms_between(r->t_submit, r->t_dispatch));
+        s->device_ms.push_back(ms_between(r->t_dispatch, now));
     }
     fl->reqs.clear();
     fl->busy = false;
@@ -318,6 +323,8 @@ void worker_loop(PfSolveServer* s)
         s->inflight_bytes += add;
         s->peak_inflight = std::max(s->peak_inflight, s->inflight_bytes);
         fl.busy = true;
+        const Clock::time_point now = Clock::now();
+        for (Req* r : fl.reqs) r->t_dispatch = now;
         lk.unlock();
         launch_flight(s, fl, cls / 1000);
         lk.lock();
@@ -409,6 +416,16 @@ PfSolveResult PfSolveServerAddOperator(PfSolveServer* s, int64_t M, const double
         cudaFree(o.bands_dd);
         return PFSOLVE_ERROR_FAILED_TO_COPY;
     }
+    // Resolve every launch shape this operator can need now, so that the
+    // worker never queries (and first loads) a kernel while serving.
+    for (int R : {4, 8}) {
+        for (int W = 1; W <= (R == 4 ? 1 : 4); W *= 2) {  // the shapes serve_rows picks for M <= 1024
+            Shape sh;
+            batch_shape(s, find_batch_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED), W, sh);
+            for (int prec : {PREC_DD, PREC_DD_F64MEM})
+                jw_shape(s, find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, prec, 0), W, sh);
+        }
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     s->ops.push_back(o);
     *opId = (int)s->ops.size() - 1;
@@ -469,7 +486,7 @@ PfSolveResult PfSolveServerWait(PfSolveServer* s, uint64_t ticket, double* laten
 PfSolveResult PfSolveServerGetStats(PfSolveServer* s, PfSolveServerStats* out)
 {
     if (!s || !out) return PFSOLVE_ERROR_INVALID_ARGUMENT;
-    std::vector<double> lat;
+    std::vector<double> lat, qm, dm;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         out->submitted = s->submitted;
@@ -478,15 +495,19 @@ PfSolveResult PfSolveServerGetStats(PfSolveServer* s, PfSolveServerStats* out)
         out->rhs = s->rhs;
         out->peakInflightBytes = s->peak_inflight;
         lat = s->lat_ms;
+        qm = s->queue_ms;
+        dm = s->device_ms;
     }
-    out->p50Ms = out->p99Ms = out->maxMs = 0.0;
-    if (!lat.empty()) {
-        std::sort(lat.begin(), lat.end());
-        auto q = [&](double f) { return lat[std::min(lat.size() - 1, (size_t)(f * (lat.size() - 1) + 0.5))]; };
-        out->p50Ms = q(0.50);
-        out->p99Ms = q(0.99);
-        out->maxMs = lat.back();
-    }
+    auto quantile = [](std::vector<double>& v, double f) {
+        if (v.empty()) return 0.0;
+        std::sort(v.begin(), v.end());
+        return v[std::min(v.size() - 1, (size_t)(f * (v.size() - 1) + 0.5))];
+    };
+    out->p50Ms = quantile(lat, 0.50);
+    out->p99Ms = quantile(lat, 0.99);
+    out->maxMs = lat.empty() ? 0.0 : lat.back();
+    out->p99QueueMs = quantile(qm, 0.99);
+    out->p99DeviceMs = quantile(dm, 0.99);
     return PFSOLVE_SUCCESS;
 }
 

@@ -51,7 +51,7 @@ int main(void) {
   printf("sdesc %zu\nsreq %zu\nsstat %zu\n", sizeof(PfSolveServerDesc), sizeof(PfSolveRequest),
          sizeof(PfSolveServerStats));
   F(PfSolveRequest, nrhs) F(PfSolveRequest, scaleC) F(PfSolveServerDesc, hbmBudgetBytes)
-  F(PfSolveServerStats, p50Ms) F(PfSolveConfiguration, kernelPath)
+  F(PfSolveServerStats, p50Ms) F(PfSolveServerStats, p99DeviceMs) F(PfSolveConfiguration, kernelPath)
   F(PfSolveConfiguration, jw_type) F(PfSolveConfiguration, jw_control_bitmask)
   F(PfSolveConfiguration, scaleC) F(PfSolveConfiguration, doublePrecision)
   F(PfSolveConfiguration, outputBufferStride) F(PfSolveConfiguration, numConsecutiveJWIterations)
