@@ -68,12 +68,20 @@ struct StCfg {
     static constexpr int HO = UO / IBO;
     static constexpr int SWBO = Log2<IBO>::v;
     static constexpr size_t BUF = (size_t)T * R * (CPLX ? 16 : 8);  // bytes of one system
-    static constexpr size_t TBL = (size_t)NPL * U * T * 16;
+    // Table rows of T 16-byte units, padded by one unit: the prologue's
+    // writes (consecutive threads on consecutive row pairs of one chunk) then
+    // fall on different banks; the loop's reads (consecutive threads on
+    // consecutive units of one row) are conflict-free either way.
+    static constexpr int TP = (W <= 2) ? T + 1 : T;  // 4-warp groups: no room to spare at N = 4096
+    static constexpr size_t TBL = (size_t)NPL * U * TP * 16;
     // A warp's input and output bytes coincide when both layouts have the same
     // swizzle rows; otherwise a warp's staging overlaps its neighbours' input.
     static constexpr bool kSameRows = (IB == IBO) && (NPIN * H == NPOUT * HO);
-    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2) * (MIXED ? 2 : 1);
-    static constexpr int kMaxThreads = kDataRegs >= 64 ? 256 : 512;
+    // Registers held by the right-hand-side data (mixed: x, g and the FP32
+    // solve vector); the launch bound leaves the compiler room for them:
+    // 512 threads cap at 128 registers, 384 at 170, 256 at 255.
+    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2) * (MIXED ? 3 : 1);
+    static constexpr int kMaxThreads = kDataRegs >= 96 ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
     static_assert(KL <= 2 && KU <= 2, "halo of at most two rows");
     static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");
@@ -244,9 +252,9 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
             for (int k = 0; k < NB; ++k) w[k] = 0.0;
         }
         const int tt = (int)(i / R), jj = (int)(i % R);
-        auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * T + tt) * 2 + (jj & 1)] = v; };
+        auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 2 + (jj & 1)] = v; };
         auto put32 = [&](int p, int k, double v) {
-            reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * T + tt) * 4 + k + (jj & 1)] = (float)v;
+            reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 4 + k + (jj & 1)] = (float)v;
         };
 #pragma unroll
         for (int k = 0; k < NB; ++k) put(k, w[k]);
@@ -308,9 +316,39 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     const int t = wg * 32 + lane;
     const int64_t s = (int64_t)t * R;
     const double2* tb = reinterpret_cast<const double2*>(table) + t;  // pair (p, u) at tb[(p*U + u)*T]
-    auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * T]; };
+    auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * C::TP]; };
 
-    auto coef4 = [&](int p, int u) -> float4 { return reinterpret_cast<const float4*>(tb)[(p * U + u) * T]; };
+    auto coef4 = [&](int p, int u) -> float4 { return reinterpret_cast<const float4*>(tb)[(p * U + u) * C::TP]; };
+    // Mixed precision, real systems of up to 16 rows per thread: the FP32 solve
+    // factors stay in registers for the whole kernel (every refinement sweep
+    // reuses them).
+    constexpr bool kHoist = C::MIXED && !C::CPLX && U <= 8;
+    float4 hf1[kHoist ? U : 1];
+    float2 hf2[kHoist ? U : 1];
+    if constexpr (kHoist) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            hf1[u] = coef4(C::P_F1, u);
+            if constexpr (C::BWD) {
+                const float4 f = coef4(C::P_F2, u);
+                hf2[u] = make_float2(f.x, f.y);
+            } else {
+                hf2[u] = make_float2(0.0f, 0.0f);
+            }
+        }
+    }
+    auto F1 = [&](int u) -> float4 {
+        if constexpr (kHoist) return hf1[u];
+        else return coef4(C::P_F1, u);
+    };
+    auto F2 = [&](int u) -> float2 {
+        if constexpr (kHoist) {
+            return hf2[u];
+        } else {
+            const float4 f = coef4(C::P_F2, u);
+            return make_float2(f.x, f.y);
+        }
+    };
 
     // Scan multipliers: products of -l and -h over this thread's chunk (in the
     // precision of the solve that uses them).
@@ -490,7 +528,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 if (it == 0) {
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        const float4 f = coef4(C::P_F1, u);
+                        const float4 f = F1(u);
                         d[2 * u] = OF::mul(f.x, to_f32(gv[2 * u]));
                         d[2 * u + 1] = OF::mul(f.y, to_f32(gv[2 * u + 1]));
                     }
@@ -500,7 +538,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                     group_neighbours<V>(g, x[0], x[R - 1], prev, next);
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        const float4 f = coef4(C::P_F1, u);
+                        const float4 f = F1(u);
                         double2 al = make_double2(0.0, 0.0), cu = make_double2(0.0, 0.0);
                         if constexpr (C::FWD) al = coef(C::P_AL, u);
                         if constexpr (C::BWD) cu = coef(C::P_CU, u);
@@ -517,7 +555,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 if constexpr (C::FWD) {
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        const float4 f = coef4(C::P_F1, u);
+                        const float4 f = F1(u);
                         if (u > 0) d[2 * u] = OF::fma(f.z, d[2 * u - 1], d[2 * u]);
                         d[2 * u + 1] = OF::fma(f.w, d[2 * u], d[2 * u + 1]);
                     }
@@ -525,7 +563,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                     float p = 1.0f;
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
-                        const float4 f = coef4(C::P_F1, u);
+                        const float4 f = F1(u);
                         p = f.z * p;
                         d[2 * u] = OF::fma(p, pin, d[2 * u]);
                         p = f.w * p;
@@ -535,7 +573,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 if constexpr (C::BWD) {
 #pragma unroll
                     for (int u = U - 1; u >= 0; --u) {
-                        const float4 f = coef4(C::P_F2, u);
+                        const float2 f = F2(u);
                         if (u < U - 1) d[2 * u + 1] = OF::fma(f.y, d[2 * u + 2], d[2 * u + 1]);
                         d[2 * u] = OF::fma(f.x, d[2 * u + 1], d[2 * u]);
                     }
@@ -543,7 +581,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                     float p = 1.0f;
 #pragma unroll
                     for (int u = U - 1; u >= 0; --u) {
-                        const float4 f = coef4(C::P_F2, u);
+                        const float2 f = F2(u);
                         p = f.y * p;
                         d[2 * u + 1] = OF::fma(p, q, d[2 * u + 1]);
                         p = f.x * p;

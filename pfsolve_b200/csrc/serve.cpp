@@ -73,6 +73,7 @@ struct Flight {
     int items_cap = 0;
     std::vector<Req*> reqs;
     bool busy = false;
+    int cls = 0;  // batch class of the requests in flight
 };
 
 
@@ -294,22 +295,53 @@ int free_flight(PfSolveServer* s)
     return -1;
 }
 
+// Double-double requests run one launch each, sequentially on their stream;
+// they may hold at most half of the streams, a few requests per batch, so
+// that mixed-precision batches always find a stream.
+constexpr int kDdBatch = 4;
+
+int dd_cap(const PfSolveServer* s) { return std::max(1, s->desc.streams / 2); }
+
+int busy_dd(const PfSolveServer* s)
+{
+    int n = 0;
+    for (const Flight& fl : s->flights)
+        if (fl.busy && fl.cls >= 1000) ++n;
+    return n;
+}
+
+// The request that opens the next batch: the first queued request whose class
+// may take a stream now; nullptr when none may (or its bytes do not fit yet:
+// admission is first come, first served within a class).
+Req* next_head(PfSolveServer* s)
+{
+    const bool dd_ok = busy_dd(s) < dd_cap(s);
+    for (Req* r : s->pending) {
+        if (r->cls >= 1000 && !dd_ok) continue;
+        return (s->inflight_bytes + r->bytes <= s->desc.hbmBudgetBytes) ? r : nullptr;
+    }
+    return nullptr;
+}
+
 void worker_loop(PfSolveServer* s)
 {
     cudaSetDevice(s->desc.device);
     std::unique_lock<std::mutex> lk(s->mu);
     const uint64_t budget = s->desc.hbmBudgetBytes;
     for (;;) {
+        Req* head = nullptr;
         s->cv.wait(lk, [&] {
             if (s->stop && s->pending.empty()) return true;
             if (s->pending.empty() || free_flight(s) < 0) return false;
-            return s->inflight_bytes + s->pending.front()->bytes <= budget;
+            head = next_head(s);
+            return head != nullptr;
         });
         if (s->pending.empty()) break;  // stop requested and drained
         Flight& fl = s->flights[free_flight(s)];
-        const int cls = s->pending.front()->cls;
+        const int cls = head->cls;
+        const int cap = (cls >= 1000) ? std::min(kDdBatch, s->desc.maxBatchRequests) : s->desc.maxBatchRequests;
         uint64_t add = 0;
-        for (auto it = s->pending.begin(); it != s->pending.end() && (int)fl.reqs.size() < s->desc.maxBatchRequests;) {
+        for (auto it = s->pending.begin(); it != s->pending.end() && (int)fl.reqs.size() < cap;) {
             Req* r = *it;
             if (r->cls != cls) {
                 ++it;
@@ -323,6 +355,7 @@ void worker_loop(PfSolveServer* s)
         s->inflight_bytes += add;
         s->peak_inflight = std::max(s->peak_inflight, s->inflight_bytes);
         fl.busy = true;
+        fl.cls = cls;
         const Clock::time_point now = Clock::now();
         for (Req* r : fl.reqs) r->t_dispatch = now;
         lk.unlock();
