@@ -397,7 +397,10 @@ def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):
     n = int(rate * duration_s)
     reqs = [templ[i % pool] for i in range(n)]
     st0 = srv.stats()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
     lat, wall, lag = run_load(srv, reqs, WL.poisson_arrivals(n, rate, seed=4))
+    clocks = sampler.stop()
     st1 = srv.stats()
     srv.close()
     lat_all = np.asarray(lat)
@@ -414,7 +417,7 @@ def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "max_ms": float(lat[-1]), "rhs_per_s": rhs / wall, "hbm_gbs_offered": nbytes / wall / 1e9,
             "batches": st1["batches"] - st0["batches"], "submitter_max_lag_ms": 1e3 * lag,
-            "server_p99_queue_ms": st1["p99QueueMs"], "server_p99_device_ms": st1["p99DeviceMs"],
+            "server_p99_queue_ms": st1["p99QueueMs"], "server_p99_device_ms": st1["p99DeviceMs"], "clocks": clocks,
             "by_precision": by_prec, "slowest": slow,
             "mix": "80% mixed (FP32 solve + 2 FP64 refinement sweeps), 20% double-double storage",
             "streams": 8, "max_batch_requests": 32, "hbm_budget_bytes": 16 << 30}

@@ -79,9 +79,11 @@ struct StCfg {
     static constexpr bool kSameRows = (IB == IBO) && (NPIN * H == NPOUT * HO);
     // Registers held by the right-hand-side data (mixed: x, g and the FP32
     // solve vector); the launch bound leaves the compiler room for them:
-    // 512 threads cap at 128 registers, 384 at 170, 256 at 255.
+    // 512 threads cap at 128 registers, 384 at 170, 256 at 255.  Complex
+    // variants stay at 256 (measured faster than 384 on the config 2 chain).
     static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2) * (MIXED ? 3 : 1);
-    static constexpr int kMaxThreads = kDataRegs >= 96 ? 256 : (kDataRegs >= 64 ? 384 : 512);
+    static constexpr int kMaxThreads =
+        (kDataRegs >= 96 || (CPLX && kDataRegs >= 64)) ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
     static_assert(KL <= 2 && KU <= 2, "halo of at most two rows");
     static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");

@@ -73,7 +73,8 @@ struct Flight {
     int items_cap = 0;
     std::vector<Req*> reqs;
     bool busy = false;
-    int cls = 0;  // batch class of the requests in flight
+    bool high = false;  // high-priority stream: mixed-precision batches only
+    int cls = 0;        // batch class of the requests in flight
 };
 
 
@@ -288,37 +289,38 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
     cudaLaunchHostFunc(fl.stream, on_flight_done, &fl);
 }
 
-int free_flight(PfSolveServer* s)
+// A free stream for a batch of class `cls`: mixed precision prefers the
+// high-priority streams, double-double only uses the low-priority ones.
+int free_flight(PfSolveServer* s, int cls)
 {
-    for (size_t i = 0; i < s->flights.size(); ++i)
-        if (!s->flights[i].busy) return (int)i;
+    const bool dd = cls >= 1000;
+    for (int pass = 0; pass < 2; ++pass)
+        for (size_t i = 0; i < s->flights.size(); ++i) {
+            const Flight& fl = s->flights[i];
+            if (fl.busy) continue;
+            if (dd && fl.high) continue;
+            if (!dd && pass == 0 && !fl.high) continue;
+            return (int)i;
+        }
     return -1;
 }
 
-// Double-double requests run one launch each, sequentially on their stream;
-// they may hold at most half of the streams, a few requests per batch, so
-// that mixed-precision batches always find a stream.
+// Double-double requests run one launch each, sequentially on their stream,
+// a few per batch and only on the low-priority streams, so that short
+// mixed-precision batches are never queued behind them.
 constexpr int kDdBatch = 4;
 
-int dd_cap(const PfSolveServer* s) { return std::max(1, s->desc.streams / 2); }
-
-int busy_dd(const PfSolveServer* s)
-{
-    int n = 0;
-    for (const Flight& fl : s->flights)
-        if (fl.busy && fl.cls >= 1000) ++n;
-    return n;
-}
-
 // The request that opens the next batch: the first queued request whose class
-// may take a stream now; nullptr when none may (or its bytes do not fit yet:
-// admission is first come, first served within a class).
-Req* next_head(PfSolveServer* s)
+// has a free stream; nullptr when none has (or its bytes do not fit yet:
+// admission is first come, first served).
+Req* next_head(PfSolveServer* s, int& flight)
 {
-    const bool dd_ok = busy_dd(s) < dd_cap(s);
     for (Req* r : s->pending) {
-        if (r->cls >= 1000 && !dd_ok) continue;
-        return (s->inflight_bytes + r->bytes <= s->desc.hbmBudgetBytes) ? r : nullptr;
+        const int f = free_flight(s, r->cls);
+        if (f < 0) continue;
+        if (s->inflight_bytes + r->bytes > s->desc.hbmBudgetBytes) return nullptr;
+        flight = f;
+        return r;
     }
     return nullptr;
 }
@@ -330,14 +332,15 @@ void worker_loop(PfSolveServer* s)
     const uint64_t budget = s->desc.hbmBudgetBytes;
     for (;;) {
         Req* head = nullptr;
+        int f = -1;
         s->cv.wait(lk, [&] {
             if (s->stop && s->pending.empty()) return true;
-            if (s->pending.empty() || free_flight(s) < 0) return false;
-            head = next_head(s);
+            if (s->pending.empty()) return false;
+            head = next_head(s, f);
             return head != nullptr;
         });
         if (s->pending.empty()) break;  // stop requested and drained
-        Flight& fl = s->flights[free_flight(s)];
+        Flight& fl = s->flights[f];
         const int cls = head->cls;
         const int cap = (cls >= 1000) ? std::min(kDdBatch, s->desc.maxBatchRequests) : s->desc.maxBatchRequests;
         uint64_t add = 0;
@@ -395,11 +398,17 @@ PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSolveServerDes
     }
     s->flights.resize(desc->streams);
     const int cap = desc->maxBatchRequests * 64;
+    int prio_low = 0, prio_high = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     bool ok = true;
-    for (Flight& fl : s->flights) {
+    for (size_t i = 0; i < s->flights.size(); ++i) {
+        Flight& fl = s->flights[i];
         fl.srv = s;
         fl.items_cap = cap;
-        ok = ok && cudaStreamCreateWithFlags(&fl.stream, cudaStreamNonBlocking) == cudaSuccess;
+        // one stream: shared by both classes; otherwise half high priority
+        fl.high = desc->streams > 1 && (int)i < desc->streams / 2;
+        ok = ok && cudaStreamCreateWithPriority(&fl.stream, cudaStreamNonBlocking, fl.high ? prio_high : prio_low) ==
+                       cudaSuccess;
         ok = ok && cudaMallocHost(&fl.h_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
         ok = ok && cudaMallocHost(&fl.h_items, cap * sizeof(WorkItem)) == cudaSuccess;
         ok = ok && cudaMalloc(&fl.d_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
