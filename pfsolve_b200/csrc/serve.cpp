@@ -9,11 +9,14 @@
 //     uneven-batch launch over all requests of the batch (jw_batch_kernel),
 //     descriptors copied from pinned staging on the same stream;
 //   * double-double: one JW-step launch per request (jw_dd_kernel).
-// Completion is signalled by a host function queued behind the batch, which
-// stamps the requests' completion time, releases their bytes and wakes the
-// worker and the waiters.  With `streams` batches in flight, requests that
-// arrive while others run are admitted as soon as a stream and bytes free up,
-// and their kernels overlap on the device.
+// An event is recorded behind every batch; the worker polls the events of
+// the batches in flight (at least every 20 us while any is), stamps the
+// requests' completion time, releases their bytes and wakes the waiters.
+// With `streams` batches in flight, requests that arrive while others run are
+// admitted as soon as a stream and bytes free up, and their kernels overlap on
+// the device.  Mixed-precision batches prefer high-priority streams;
+// double-double batches (one launch per request) use only the low-priority
+// ones and take at most kDdBatch requests.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -71,9 +74,11 @@ struct Flight {
     WorkItem* d_items = nullptr;
     unsigned int* d_counter = nullptr;
     int items_cap = 0;
+    cudaEvent_t done = nullptr;  // recorded behind the batch; the worker polls it
     std::vector<Req*> reqs;
     bool busy = false;
-    bool high = false;  // high-priority stream: mixed-precision batches only
+    bool launched = false;  // the batch (and its event) has been enqueued
+    bool high = false;      // high-priority stream: mixed-precision batches only
     int cls = 0;        // batch class of the requests in flight
 };
 
@@ -191,13 +196,11 @@ JwIO make_io(const ServeOp& o, const PfSolveRequest& r)
     return io;
 }
 
-void CUDART_CB on_flight_done(void* p)
+// Complete the requests of flight `fl` (its event has fired).  Called by the
+// worker with the server lock held.
+void complete_flight(PfSolveServer* s, Flight& fl, Clock::time_point now)
 {
-    Flight* fl = static_cast<Flight*>(p);
-    PfSolveServer* s = fl->srv;
-    const Clock::time_point now = Clock::now();
-    std::lock_guard<std::mutex> lk(s->mu);
-    for (Req* r : fl->reqs) {
+    for (Req* r : fl.reqs) {
         r->t_done = now;
         r->done = true;
         s->inflight_bytes -= r->bytes;
@@ -207,11 +210,28 @@ void CUDART_CB on_flight_done(void* p)
         s->queue_ms.push_back(ms_between(r->t_submit, r->t_dispatch));
         s->device_ms.push_back(ms_between(r->t_dispatch, now));
     }
-    fl->reqs.clear();
-    fl->busy = false;
+    fl.reqs.clear();
+    fl.busy = false;
     s->batches++;
-    s->cv.notify_all();
-    s->done_cv.notify_all();
+}
+
+// Complete every flight whose work has finished; true when any did.
+bool reap_flights(PfSolveServer* s)
+{
+    bool any = false;
+    const Clock::time_point now = Clock::now();
+    for (Flight& fl : s->flights) {
+        if (!fl.busy || !fl.launched) continue;
+        const cudaError_t e = cudaEventQuery(fl.done);
+        if (e == cudaErrorNotReady) continue;
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            for (Req* r : fl.reqs) r->status = PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE;
+        }
+        complete_flight(s, fl, now);
+        any = true;
+    }
+    return any;
 }
 
 // Enqueue the batch of flight `fl` (mixed: one uneven-batch launch; dd: one
@@ -280,13 +300,15 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
             }
             const JwOperator op = make_operator(s, o, r->r);
             const JwIO io = make_io(o, r->r);
-            const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((io.nsys + sh.G - 1) / sh.G, sh.max_blocks));
+            // one system per group (no persistent CTAs): short CTAs let the
+            // high-priority streams' blocks in between
+            const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((io.nsys + sh.G - 1) / sh.G, INT32_MAX));
             v->launch(dim3((unsigned)grid), dim3(32 * W * sh.G), sh.smem, fl.stream, op, io, W);
             note_launch(false);
             if (cudaGetLastError() != cudaSuccess) r->status = PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
         }
     }
-    cudaLaunchHostFunc(fl.stream, on_flight_done, &fl);
+    cudaEventRecord(fl.done, fl.stream);
 }
 
 // A free stream for a batch of class `cls`: mixed precision prefers the
@@ -331,15 +353,19 @@ void worker_loop(PfSolveServer* s)
     std::unique_lock<std::mutex> lk(s->mu);
     const uint64_t budget = s->desc.hbmBudgetBytes;
     for (;;) {
+        if (reap_flights(s)) s->done_cv.notify_all();
         Req* head = nullptr;
         int f = -1;
-        s->cv.wait(lk, [&] {
-            if (s->stop && s->pending.empty()) return true;
-            if (s->pending.empty()) return false;
-            head = next_head(s, f);
-            return head != nullptr;
-        });
-        if (s->pending.empty()) break;  // stop requested and drained
+        if (!s->pending.empty()) head = next_head(s, f);
+        if (!head) {
+            bool busy = false;
+            for (const Flight& fl : s->flights) busy = busy || fl.busy;
+            if (s->stop && s->pending.empty() && !busy) break;  // drained
+            // sleep until a submission, or poll the flights in flight again shortly
+            if (busy) s->cv.wait_for(lk, std::chrono::microseconds(20));
+            else s->cv.wait(lk);
+            continue;
+        }
         Flight& fl = s->flights[f];
         const int cls = head->cls;
         const int cap = (cls >= 1000) ? std::min(kDdBatch, s->desc.maxBatchRequests) : s->desc.maxBatchRequests;
@@ -358,18 +384,21 @@ void worker_loop(PfSolveServer* s)
         s->inflight_bytes += add;
         s->peak_inflight = std::max(s->peak_inflight, s->inflight_bytes);
         fl.busy = true;
+        fl.launched = false;
         fl.cls = cls;
         const Clock::time_point now = Clock::now();
         for (Req* r : fl.reqs) r->t_dispatch = now;
         lk.unlock();
         launch_flight(s, fl, cls / 1000);
         lk.lock();
+        fl.launched = true;
     }
 }
 
 void free_flight_resources(Flight& fl)
 {
     if (fl.stream) cudaStreamDestroy(fl.stream);
+    if (fl.done) cudaEventDestroy(fl.done);
     if (fl.h_entries) cudaFreeHost(fl.h_entries);
     if (fl.h_items) cudaFreeHost(fl.h_items);
     if (fl.d_entries) cudaFree(fl.d_entries);
@@ -409,6 +438,7 @@ PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSolveServerDes
         fl.high = desc->streams > 1 && (int)i < desc->streams / 2;
         ok = ok && cudaStreamCreateWithPriority(&fl.stream, cudaStreamNonBlocking, fl.high ? prio_high : prio_low) ==
                        cudaSuccess;
+        ok = ok && cudaEventCreateWithFlags(&fl.done, cudaEventDisableTiming) == cudaSuccess;
         ok = ok && cudaMallocHost(&fl.h_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
         ok = ok && cudaMallocHost(&fl.h_items, cap * sizeof(WorkItem)) == cudaSuccess;
         ok = ok && cudaMalloc(&fl.d_entries, desc->maxBatchRequests * sizeof(BatchEntryDev)) == cudaSuccess;
