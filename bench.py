@@ -452,6 +452,45 @@ def config3_profile(args):
     app.close()
 
 
+def config4_profile(args):
+    """Profiling case: config 4 (one spectral timestep, degrees l = 0..--lmax),
+    one persistent uneven-batch launch per step (no graph), K timed steps."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import Batch
+    step = WL.config4(lmax=args.lmax)
+    inp = torch.from_numpy(step.rhs).cuda()
+    outb = torch.zeros_like(inp)
+    keep, entries = [], []
+    for k, (l, N, ns) in enumerate(zip(step.ls, step.Ns, step.nsys)):
+        tj = torch.from_numpy(step.jw_bands[k]).cuda()
+        ta = torch.from_numpy(step.dgbmv[k]).cuda()
+        keep += [tj, ta]
+        off = int(step.rhs_offsets[k])
+        entries.append(dict(M=int(N), nsys=int(ns), bands=tj, dgbmvBands=ta, input=inp.data_ptr() + 8 * off,
+                            output=outb.data_ptr() + 8 * off, inputStride=int(N), outputStride=int(N),
+                            lshift=int(l), scaleS=step.scale_s, scaleC=1.0))
+    desc = dict(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=307)
+    if args.rows:
+        desc["rowsPerThread"] = args.rows
+    batch = Batch(entries, **desc)
+    for _ in range(max(1, args.warmup)):
+        batch.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        batch.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    rows = int((step.Ns * step.nsys).sum())
+    print(json.dumps({"profile_case": "config4", "lmax": args.lmax, "ms_per_step": ms,
+                      "gbs": 2.0 * rows * 16 / (ms * 1e-3) / 1e9, "shape": batch.shape()}), flush=True)
+    batch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,8 +503,10 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3"],
-                    help="profiling case (--profile): the config 2 chain or config 3 (--ncplx real systems)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+                    help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems) or "
+                         "config 4 (degrees 0..--lmax)")
+    ap.add_argument("--lmax", type=int, default=511, help="config 4 profiling case: highest harmonic degree")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1],
                     help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
@@ -485,6 +526,9 @@ def main():
         return
     if args.profile and args.workload == "config3":
         config3_profile(args)
+        return
+    if args.profile and args.workload == "config4":
+        config4_profile(args)
         return
     try:
         if args.impl == "reference":

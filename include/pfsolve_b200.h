@@ -349,7 +349,9 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
 /* Kernel shape a JW or dgbmv plan chose: streaming = 1 when its launches use
  * the TMA-staged streaming kernel wherever their buffers allow it, with
  * rowsPerThread x warpsPerSystem rows per group and groupsPerCTA groups;
- * streaming = 0: the group kernel's shape.  No counterpart in the reference. */
+ * streaming = 0: the group kernel's shape; streaming = 2: long systems
+ * (M > 4096), one thread-block cluster per system, warpsPerSystem warps over
+ * the cluster's CTAs.  No counterpart in the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);
 /* Launches that ran on the streaming kernel since load (all apps). */

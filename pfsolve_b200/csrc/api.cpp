@@ -29,7 +29,8 @@ std::atomic<uint64_t> g_stream_launches{0};
 
 enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3 };
 
-constexpr int64_t kMaxRows = 4096;  // single-upload limit of this build (<= 8 warps x 32 x 16 rows)
+constexpr int64_t kMaxRows = 4096;       // one CTA group per system (<= 8 warps x 32 x 16 rows)
+constexpr int64_t kMaxRowsLong = 16384;  // JW apps: one cluster of up to 8 CTAs x 2048 rows per system
 
 struct AppState {
     AppKind kind;
@@ -47,6 +48,9 @@ struct AppState {
     // buffers allow it; `variant` serves the other launches
     const StreamVariant* stream_v = nullptr;
     int stream_G = 0, stream_max_blocks = 0;
+    // long systems (N > 4096): one cluster of CTAs per system
+    const ClusterVariant* cluster_v = nullptr;
+    int cluster_max = 0;
     int R_req = 0;           // caller's rows per thread (0: choose)
     bool no_stream = false;  // kernelPath 1
     // fused-chain plans made with this JW app, by operator shape
@@ -148,6 +152,27 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
     return false;
 }
 
+// Cluster variant for long real systems: C CTAs of 2048 rows, C the smallest
+// compiled count that covers M (rows per thread 8: M must be a multiple of 8).
+bool choose_cluster(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    s->cluster_v = nullptr;
+    if (s->prec != PREC_F64 || s->no_stream || LIN != LAY_REAL || LOUT != LAY_REAL || SCALE || M % 8 != 0)
+        return false;
+    for (int C : {3, 4, 6, 8}) {
+        if ((int64_t)C * 2048 < M) continue;
+        const ClusterVariant* v = find_cluster_variant(C, s->KL, s->KU, s->sv);
+        if (!v) return false;
+        if (!allow_max_smem(v->func)) return false;
+        const int n = v->max_clusters(v->smem_bytes);
+        if (n < 1) return false;
+        s->cluster_v = v;
+        s->cluster_max = n;
+        return true;
+    }
+    return false;
+}
+
 // Pick the kernel variant and launch shape for M rows: register variants
 // first, then coefficient-table variants (FP64); rows per thread from the
 // caller's choice (s->R) first, then the other compiled choices.
@@ -176,10 +201,12 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
             return PFSOLVE_SUCCESS;
         }
     }
-    // No group-kernel variant fits: a streaming-only plan, whose launches need
-    // buffers the streaming kernel can take.
+    // No group-kernel variant fits: a streaming-only plan (or, for long
+    // systems, a cluster plan), whose launches need buffers those kernels can
+    // take.
     s->variant = nullptr;
     if (choose_stream(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
+    if (M > kMaxRows && choose_cluster(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
     // nothing compiled fits: distinguish "too long" from "not compiled"
     for (int R : {2, 4, 8, 16})
         if ((M + 32 * (int64_t)R - 1) / (32 * (int64_t)R) <= 8) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
@@ -258,7 +285,7 @@ void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator
 // Tensor maps of recent launches (encoding is host work; steady-state
 // launches repeat the same buffers).
 struct MapCacheEntry {
-    const StreamVariant* v;
+    const void* v;  // the stream or cluster variant the maps were encoded for
     JwIO io;
     CUtensorMap in, out;
     bool valid;
@@ -272,17 +299,39 @@ bool same_io(const JwIO& a, const JwIO& b)
            a.out_off == b.out_off && a.out_stride == b.out_stride && a.nsys == b.nsys && a.M == b.M;
 }
 
-const MapCacheEntry* stream_maps(const StreamVariant* v, const JwIO& io)
+const MapCacheEntry* row_maps(const void* key, int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io)
 {
     for (const MapCacheEntry& e : g_map_cache)
-        if (e.valid && e.v == v && same_io(e.io, io)) return &e;
+        if (e.valid && e.v == key && same_io(e.io, io)) return &e;
     MapCacheEntry& e = g_map_cache[g_map_next++ % 8];
     e.valid = false;
-    if (!encode_stream_maps(v, io, &e.in, &e.out)) return nullptr;
-    e.v = v;
+    if (!encode_row_maps(R, LIN, LOUT, IB, IBO, io, &e.in, &e.out)) return nullptr;
+    e.v = key;
     e.io = io;
     e.valid = true;
     return &e;
+}
+
+const MapCacheEntry* stream_maps(const StreamVariant* v, const JwIO& io)
+{
+    return row_maps(v, v->R, v->LIN, v->LOUT, v->IB, v->IBO, io);
+}
+
+// Long systems: the cluster kernel, under the streaming kernel's buffer rules.
+PfSolveResult launch_cluster(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
+{
+    const ClusterVariant* v = s->cluster_v;
+    if (io.accumulate || io.oz0 > 0 || io.oz1 < io.M) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, io);
+    if (!e) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const int clusters = (int)std::max<int64_t>(1, std::min<int64_t>(io.nsys, s->cluster_max));
+    const cudaError_t err = v->launch(clusters, v->smem_bytes, stream, &e->in, &e->out, op, io);
+    note_launch(true);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
 }
 
 // Launch on the streaming variant when the plan has one and this launch's
@@ -303,6 +352,7 @@ bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream
 PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
 {
     if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    if (s->cluster_v) return launch_cluster(s, op, io, stream);
     if (launch_stream(s, op, io, stream)) {
         g_launches.fetch_add(1, std::memory_order_relaxed);
         g_stream_launches.fetch_add(1, std::memory_order_relaxed);
@@ -471,6 +521,13 @@ PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int
 {
     if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
     const AppState* s = static_cast<const AppState*>(app->internal);
+    if (s->cluster_v) {
+        if (streaming) *streaming = 2;
+        if (rowsPerThread) *rowsPerThread = s->cluster_v->R;
+        if (warpsPerSystem) *warpsPerSystem = s->cluster_v->W * s->cluster_v->C;
+        if (groupsPerCTA) *groupsPerCTA = 1;
+        return PFSOLVE_SUCCESS;
+    }
     const bool sm = s->stream_v != nullptr;
     if (streaming) *streaming = sm ? 1 : 0;
     if (rowsPerThread) *rowsPerThread = sm ? s->stream_v->R : s->R;
@@ -530,7 +587,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
         else if (c.numConsecutiveJWIterations > 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (((c.jw_type / 100) % 10) == 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // ALT mode
         else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-        else if (c.M_size > kMaxRows || c.M_size < 1) r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+        else if (c.M_size > kMaxRowsLong || c.M_size < 1) r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
         else {
             JwLayout L;
             if (!jw_layout(c, false, false, 0, 0, L)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;

@@ -50,6 +50,22 @@ const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, i
 // Tensor maps of a launch's input and output rows; false when the buffers'
 // alignment, strides or M do not allow the streaming layout.
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out);
+bool encode_row_maps(int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out);
+
+// Long-system variants: one cluster of C CTAs per system, each CTA a slice of
+// 32*W*R rows (real systems, FP64).
+struct ClusterVariant {
+    int R, W, C, KL, KU, SV;
+    const void* func;
+    size_t smem_bytes;
+    int IB, IBO;
+    // grid: clusters * C CTAs; returns the launch error
+    cudaError_t (*launch)(int clusters, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
+                          const JwOperator& op, const JwIO& io);
+    int (*max_clusters)(size_t smem);  // clusters that fit the device at once (0: none)
+};
+const ClusterVariant* find_cluster_variant(int C, int KL, int KU, int SV);
+unsigned cluster_status_fetch_clear();
 // Status word of the streaming kernels' bounded waits since the last call
 // (0: none timed out); reading it synchronises with the device.
 unsigned stream_status_fetch_clear();

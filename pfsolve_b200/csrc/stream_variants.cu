@@ -77,26 +77,31 @@ bool encode_rows(CUtensorMap* map, const void* base, int64_t inner, int64_t chun
 }
 }  // namespace
 
-bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
+bool encode_row_maps(int R_, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
 {
-    const int64_t R = v->R, M = io.M;
+    const int64_t R = R_, M = io.M;
     if (M % R != 0 || io.nsys < 1) return false;
     const int64_t chunks = M / R;
-    const bool cplx = v->LIN != LAY_REAL;
+    const bool cplx = LIN != LAY_REAL;
     const int64_t sets = cplx ? 2 * io.nsys : io.nsys;
-    if (!encode_rows(in, io.in + io.in_off, R, chunks, sets, io.in_stride * 8, v->IB)) return false;
-    if (v->LOUT == LAY_PACKED)
+    if (!encode_rows(in, io.in + io.in_off, R, chunks, sets, io.in_stride * 8, IB)) return false;
+    if (LOUT == LAY_PACKED)
         return encode_rows(out, reinterpret_cast<const double2*>(io.out) + io.out_off, 2 * R, chunks, io.nsys,
-                           io.out_stride * 16, v->IBO);
-    const int64_t osets = (v->LOUT == LAY_XXII) ? 2 * io.nsys : io.nsys;
-    return encode_rows(out, io.out + io.out_off, R, chunks, osets, io.out_stride * 8, v->IBO);
+                           io.out_stride * 16, IBO);
+    const int64_t osets = (LOUT == LAY_XXII) ? 2 * io.nsys : io.nsys;
+    return encode_rows(out, io.out + io.out_off, R, chunks, osets, io.out_stride * 8, IBO);
+}
+
+bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
+{
+    return encode_row_maps(v->R, v->LIN, v->LOUT, v->IB, v->IBO, io, in, out);
 }
 
 unsigned stream_status_fetch_clear()
 {
-    const unsigned a = stream_status_f64(), b = stream_status_mixed();
-    if (a == ~0u || b == ~0u) return ~0u;
-    return a | b;
+    const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
+    if (a == ~0u || b == ~0u || c == ~0u) return ~0u;
+    return a | b | c;
 }
 
 }  // namespace pfb

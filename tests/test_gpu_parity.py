@@ -125,9 +125,12 @@ def test_unsupported_combinations_return_codes():
         with pytest.raises(capi.PfSolveError) as ei:
             App(buffer=b, outputBuffer=r, M_size=64, size=(64, 1), doublePrecision=1, **fields)
         assert ei.value.code == code
-    with pytest.raises(capi.PfSolveError) as ei:
-        App(buffer=b, outputBuffer=r, M_size=5000, size=(5000, 1), doublePrecision=1, upperBanded=2, jw_type=13)
-    assert ei.value.code == capi.PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH
+    # longer than one cluster of 8 x 2048 rows, or a long system whose length
+    # is not a multiple of the cluster kernel's 8 rows per thread
+    for M in (16392, 5001):
+        with pytest.raises(capi.PfSolveError) as ei:
+            App(buffer=b, outputBuffer=r, M_size=M, size=(M, 1), doublePrecision=1, upperBanded=2, jw_type=13)
+        assert ei.value.code == capi.PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH
 
 
 @pytest.mark.parametrize("KL,KU", [(1, 1), (2, 2), (0, 1), (2, 1), (3, 3), (0, 6)])
