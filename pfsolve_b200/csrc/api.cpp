@@ -62,8 +62,6 @@ struct AppState {
         int stream_G, stream_max_blocks;
     };
     std::vector<ChainPlan> chain_plans;
-    // reference band permutation parameters (reorder_i0 inputs)
-    int64_t perm_r = 1, perm_m = 0, perm_ceil = 0, perm_floor = 0;
     // streams
     uint64_t stream_counter = 0;
     cudaEvent_t* events = nullptr;
@@ -273,11 +271,7 @@ void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator
 {
     memset(&op, 0, sizeof(op));
     op.M = c.M_size;
-    op.perm = 1;
-    op.perm_r = s->perm_r;
-    op.perm_m = s->perm_m;
-    op.perm_ceil = s->perm_ceil;
-    op.perm_floor = s->perm_floor;
+    set_band_order(c.M_size, op);
     op.scaleC = 1.0;
     op.refine_sweeps = s->refine_sweeps;
 }
@@ -602,7 +596,6 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->R_fixed = c.rowsPerThread != 0 && c.rowsPerThread != 32;
                 s->R_req = c.rowsPerThread;
                 s->no_stream = c.kernelPath == 1;
-                reference_band_order(c.M_size, s->perm_r, s->perm_m, s->perm_ceil, s->perm_floor);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
         }
@@ -1026,7 +1019,6 @@ PfSolveResult PfSolveBatchCreate(PfSolveBatch** out, CUdevice device, const PfSo
         BatchEntryDev d;
         memset(&d, 0, sizeof(d));
         AppState tmp;
-        reference_band_order(en.M, tmp.perm_r, tmp.perm_m, tmp.perm_ceil, tmp.perm_floor);
         tmp.refine_sweeps = 1 + desc->mixedPrecisionRefinement;
         fill_operator_common(&tmp, c, d.op);
         d.op.bands = static_cast<const double*>(en.bands);

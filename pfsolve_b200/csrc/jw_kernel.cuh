@@ -89,11 +89,25 @@ __host__ size_t jw_smem_bytes(int W, int G)
            (size_t)G * W * kScratchPerWarp * sizeof(double);
 }
 
+// Storage position of row i in the reference's band order (reorder_i0,
+// pfSolve_Plan_JonesWorland.h:66-142): register-major within each piece of
+// perm_piece rows (the whole system when perm_piece == 0).
 __device__ __forceinline__ int64_t band_pos(const JwOperator& op, int64_t i)
 {
     if (!op.perm) return i;
-    int64_t t = i / op.perm_r, j = i - t * op.perm_r;
-    return t + ((j < op.perm_m) ? j * op.perm_ceil : op.perm_m * op.perm_ceil + (j - op.perm_m) * op.perm_floor);
+    int64_t base = 0, li = i, m = op.perm_m, ce = op.perm_ceil, fl = op.perm_floor;
+    if (op.perm_piece) {
+        const int64_t piece = i / op.perm_piece;
+        base = piece * op.perm_piece;
+        li = i - base;
+        if (base + op.perm_piece > op.M) {
+            m = op.perm_lm;
+            ce = op.perm_lceil;
+            fl = op.perm_lfloor;
+        }
+    }
+    const int64_t t = li / op.perm_r, j = li - t * op.perm_r;
+    return base + t + ((j < m) ? j * ce : m * ce + (j - m) * fl);
 }
 
 __device__ __forceinline__ double band(const JwOperator& op, int64_t off, int64_t i)

@@ -17,7 +17,11 @@ struct JwOperator {
     int64_t off_md, off_mo, off_sl, off_su;  // band offsets in elements (resolved on the host)
     int mvj;                                 // JW matvec kind (MVJ_*)
     int perm;                                // 1: bands in the reference's register-major order
+    // reference band order (reorder_i0): rows per lane r, and for the pieces
+    // of perm_piece rows (0: one piece) the count of lanes with ceil rows (m)
+    // and the ceil / floor row counts; the partial last piece has its own
     int64_t perm_r, perm_m, perm_ceil, perm_floor;
+    int64_t perm_piece, perm_lm, perm_lceil, perm_lfloor;
     const double* dgbmv;  // fused general band matrix (band-major), or nullptr
     int64_t dg_off;
     int dg_lda, dg_ku;

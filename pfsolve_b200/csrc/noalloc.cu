@@ -100,8 +100,7 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
         BatchEntryDev& d = g_entries[e];
         memset(&d, 0, sizeof(d));
         d.op.M = en.M;
-        d.op.perm = 1;
-        reference_band_order(en.M, d.op.perm_r, d.op.perm_m, d.op.perm_ceil, d.op.perm_floor);
+        set_band_order(en.M, d.op);
         d.op.refine_sweeps = 1 + desc->mixedPrecisionRefinement;
         d.op.bands = static_cast<const double*>(en.bands);
         d.op.off_md = L.off_md;

@@ -36,19 +36,31 @@ inline bool allow_max_smem(const void* func)
 // PfSolveStreamingLaunchCount when it ran on the streaming kernel).
 void note_launch(bool streaming);
 
-// Rows per lane of the reference's register-major band order
-// (pfSolve_Plan_JonesWorland.h:311-346 and reorder_i0, :66-142).
-inline void reference_band_order(int64_t M, int64_t& r, int64_t& m, int64_t& ceil_n, int64_t& floor_n)
+// The reference's register-major band order (reorder_i0 with the CUDA
+// backend's defaults, pfSolve_Plan_JonesWorland.h:66-142): systems of up to
+// 4352 rows are one piece; longer ones are split into pieces of Msplit = 256
+// rows, each permuted on its own (the last, partial piece with its own counts).
+inline void set_band_order(int64_t M, JwOperator& op)
 {
-    int64_t warp = 64 * ((M + 1023) / 1024);
-    if (M < 512) warp = 32;
+    const int64_t piece = (M > 4352) ? 256 : 0;
+    const int64_t size1 = piece ? piece : M;
+    int64_t warp = 64 * ((size1 + 1023) / 1024);
+    if (size1 < 512) warp = 32;
     if (warp < 32) warp = 32;
     if (warp % 32) warp = 32 * ((warp + 31) / 32);
-    r = (M + warp - 1) / warp;
+    int64_t r = (size1 + warp - 1) / warp;
     if (r < 1) r = 1;
-    m = M % r;
-    ceil_n = (M + r - 1) / r;
-    floor_n = M / r;
+    op.perm = 1;
+    op.perm_r = r;
+    op.perm_piece = piece;
+    const int64_t full = piece ? piece : M;
+    op.perm_m = full % r;
+    op.perm_ceil = (full + r - 1) / r;
+    op.perm_floor = full / r;
+    const int64_t last = piece ? (M % piece) : 0;
+    op.perm_lm = last % r;
+    op.perm_lceil = (last + r - 1) / r;
+    op.perm_lfloor = last / r;
 }
 
 // JW operator kinds for K = 1 (pfSolve_JonesWorland.h:117-353): which matvec,

@@ -46,7 +46,6 @@ struct ServeOp {
     double* bands_dd;  // {hi, lo} copy (lo = 0), owned
     JwLayout L;
     int KL, KU;
-    int64_t perm_r, perm_m, perm_ceil, perm_floor;
 };
 
 struct Req {
@@ -171,13 +170,9 @@ JwOperator make_operator(const PfSolveServer* s, const ServeOp& o, const PfSolve
     op.off_sl = o.L.off_sl;
     op.off_su = o.L.off_su;
     op.mvj = o.L.mvj;
-    op.perm = 1;
-    op.perm_r = o.perm_r;
-    op.perm_m = o.perm_m;
-    op.perm_ceil = o.perm_ceil;
-    op.perm_floor = o.perm_floor;
     op.scaleC = r.scaleC;
     op.M = o.M;
+    set_band_order(o.M, op);
     op.refine_sweeps = 1 + s->desc.refineSweeps;
     return op;
 }
@@ -479,7 +474,6 @@ PfSolveResult PfSolveServerAddOperator(PfSolveServer* s, int64_t M, const double
             !find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, 3, 0))
             return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     }
-    reference_band_order(M, o.perm_r, o.perm_m, o.perm_ceil, o.perm_floor);
     cudaSetDevice(s->desc.device);
     if (cudaMalloc(&o.bands_dd, 3 * M * 2 * sizeof(double)) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
     if (cudaMemset(o.bands_dd, 0, 3 * M * 2 * sizeof(double)) != cudaSuccess ||

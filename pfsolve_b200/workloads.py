@@ -17,19 +17,32 @@ import numpy as np
 
 
 def reference_band_order(M: int) -> np.ndarray:
-    """perm[i] = storage position of logical row i (single upload, M <= 4352)."""
-    warp = 64 * ((M + 1023) // 1024)
-    if M < 512:
+    """perm[i] = storage position of logical row i in the reference's band
+    order (reorder_i0, CUDA backend): register-major over the whole system up
+    to 4352 rows; beyond, register-major within each piece of 256 rows (the
+    partial last piece with its own counts)."""
+    piece = 256 if M > 4352 else 0
+    size1 = piece if piece else M
+    warp = 64 * ((size1 + 1023) // 1024)
+    if size1 < 512:
         warp = 32
     warp = max(warp, 32)
     if warp % 32:
         warp = 32 * ((warp + 31) // 32)
-    r = max(1, (M + warp - 1) // warp)
+    r = max(1, (size1 + warp - 1) // warp)
     i = np.arange(M, dtype=np.int64)
-    t, j = i // r, i % r
-    m = M % r
-    ceil_n, floor_n = (M + r - 1) // r, M // r
-    return t + np.where(j < m, j * ceil_n, m * ceil_n + (j - m) * floor_n)
+    if piece:
+        base = (i // piece) * piece
+        li = i - base
+        size0 = np.where(base + piece > M, M % piece, piece)
+    else:
+        base = np.zeros_like(i)
+        li = i
+        size0 = np.full_like(i, M)
+    t, j = li // r, li % r
+    m = size0 % r
+    ceil_n, floor_n = (size0 + r - 1) // r, size0 // r
+    return base + t + np.where(j < m, j * ceil_n, m * ceil_n + (j - m) * floor_n)
 
 
 def permute_bands(natural: np.ndarray, M: int) -> np.ndarray:

@@ -44,7 +44,7 @@ def _run(case, bands, rhs, **extra):
 
 
 @pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (1, 11), (1, 12), (0, 10), (0, 11), (0, 13)])
-@pytest.mark.parametrize("M", [4104, 6144, 8192, 12000, 16384])
+@pytest.mark.parametrize("M", [4104, 5000, 6000, 6144, 8192, 12000, 16384])
 def test_cluster_modes_and_sizes(ub, jwt, M):
     rng = np.random.default_rng(9000 + 10 * ub + jwt + M)
     case, bands, rhs = _case(rng, M, 7, ub, jwt)

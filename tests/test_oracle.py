@@ -7,7 +7,8 @@ from oracle import oracle as O
 from pfsolve_b200 import workloads as WL
 
 
-@pytest.mark.parametrize("M", [1, 2, 7, 31, 32, 33, 100, 255, 256, 257, 511, 512, 513, 1000, 1024, 2048, 4352])
+@pytest.mark.parametrize("M", [1, 2, 7, 31, 32, 33, 100, 255, 256, 257, 511, 512, 513, 1000, 1024, 2048, 4352,
+                               4353, 4360, 5000, 6144, 8192, 12000, 16383, 16384])
 def test_band_order_matches_reference_formula(M):
     perm_c = O.permutation(M)
     perm_py = WL.reference_band_order(M)
