@@ -431,7 +431,7 @@ def config3_profile(args):
 
     from pfsolve_b200 import workloads as WL
     from pfsolve_b200.api import App
-    wl = WL.config3(B=args.ncplx)
+    wl = WL.config3(M=args.m, B=args.ncplx)
     M, B = wl.M, wl.nrhs
     tb = torch.from_numpy(wl.jw_bands).cuda()
     x = torch.from_numpy(wl.rhs).cuda()
@@ -447,7 +447,7 @@ def config3_profile(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    print(json.dumps({"profile_case": "config3", "rhs": B, "refine": args.refine, "ms_per_step": ms,
+    print(json.dumps({"profile_case": "config3", "M": M, "rhs": B, "refine": args.refine, "ms_per_step": ms,
                       "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9, "kernel": app.shape()}), flush=True)
     app.close()
 
@@ -507,6 +507,7 @@ def main():
                     help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems) or "
                          "config 4 (degrees 0..--lmax)")
     ap.add_argument("--lmax", type=int, default=511, help="config 4 profiling case: highest harmonic degree")
+    ap.add_argument("--m", type=int, default=512, help="config 3 profiling case: rows per system")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1],
                     help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
