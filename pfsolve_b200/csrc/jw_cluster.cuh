@@ -19,10 +19,14 @@
 //    each CTA composes those of the CTAs before it (forward) or after it
 //    (backward).  The tridiagonal pivots' Moebius scan is composed the same
 //    way in the prologue.
-//  * Completion waits stay bounded: every CTA publishes whether its wait
-//    succeeded before the first cluster barrier of a system, and all CTAs of
-//    the cluster stop together when one did not, so no CTA is left at a
-//    cluster barrier its peers never reach.
+//  * Cluster barriers are mbarrier-based (remote arrivals, a bounded wait),
+//    and a CTA publishes whether the TMA load of a system completed before
+//    the barrier that precedes the system's first shared-memory exchange (the
+//    last barrier of the previous system), so all CTAs of the cluster stop
+//    together when one load did not complete, and one barrier per system
+//    serves both the previous system's scan and the next one's halo.  A
+//    barrier whose peers never arrive ends with a status bit instead of a
+//    hang.
 #pragma once
 #include "jw_stream.cuh"
 
@@ -43,7 +47,7 @@ struct ClCfg {
 template <class C>
 __host__ __device__ constexpr size_t cl_smem_bytes()
 {
-    return C::B::TBL + (size_t)C::W * kScratchPerWarp * sizeof(double) + C::XCHG + 2 * sizeof(uint64_t) + 1024 +
+    return C::B::TBL + (size_t)C::W * kScratchPerWarp * sizeof(double) + C::XCHG + 4 * sizeof(uint64_t) + 1024 +
            2 * C::B::BUF;
 }
 
@@ -77,6 +81,55 @@ __device__ __forceinline__ uint32_t mapa_rank(uint32_t local, uint32_t rank)
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(local), "r"(rank));
     return r;
 }
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t remote_bar)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(remote_bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Barrier over the CTAs of the cluster, built on one mbarrier per CTA (C
+// arrivals per phase): after the CTA's own threads meet, the CTA arrives with
+// release semantics on every CTA's mbarrier, and thread 0 waits -- for about
+// two seconds at most -- for the arrivals of all CTAs.  Returns false when
+// that wait ran out; the caller then stops.  A CTA may arrive for the next
+// barrier before a slower peer's current phase completes; that arrival only
+// lands after every CTA has arrived for the current one, so each phase still
+// completes only once all CTAs reached the barrier, and no phase is skipped.
+template <int C>
+__device__ __forceinline__ bool cl_barrier(uint32_t cbar, uint32_t& phase, volatile int* flag, int nthr)
+{
+    group_bar(1, nthr);
+    // lanes 0..C-1 of warp 0 arrive on one CTA each; the release covers the
+    // CTA's writes ordered before the bar.sync above
+    if (threadIdx.x < C) mbar_arrive_remote(mapa_rank(cbar, threadIdx.x));
+    if (threadIdx.x == 0) {
+        bool ok = mbar_try_wait_cluster(cbar, phase);
+        if (!ok) {
+            const long long t0 = clock64();
+            while (!(ok = mbar_try_wait_cluster(cbar, phase)))
+                if (clock64() - t0 > 4000000000LL) break;
+        }
+        *flag = ok ? 1 : 0;
+    }
+    group_bar(1, nthr);
+    phase ^= 1u;
+    return *flag != 0;
+}
+
+// Status bits of a cluster barrier that ran out, by barrier (kStatusWaitTimeout
+// is also set).
+constexpr unsigned kStatusClusterBarrier = 1u << 8;
+
 __device__ __forceinline__ double ld_cluster_f64(uint32_t addr)
 {
     double v;
@@ -150,7 +203,8 @@ __device__ __forceinline__ void group_affine_scan_map(GroupCtx& g, double A, dou
 // ---- Coefficient table of this CTA's slice (rows crank*S + [0, S)), built by
 // all its threads; the Moebius pivots are scanned across the cluster.
 template <class C>
-__device__ void cl_prologue(const JwOperator& op, double* table, double* scratch, double* xchg, uint32_t crank)
+__device__ bool cl_prologue(const JwOperator& op, double* table, double* scratch, double* xchg, uint32_t crank,
+                            uint32_t cbar, uint32_t& cphase, volatile int* cflag)
 {
     using BC = typename C::B;
     constexpr int R = C::R, U = BC::U, NB = BC::NB, S = C::S;
@@ -192,7 +246,7 @@ __device__ void cl_prologue(const JwOperator& op, double* table, double* scratch
             xchg[C::XM + 2] = nc;
             xchg[C::XM + 3] = nd;
         }
-        cluster_sync();
+        if (!cl_barrier<C::C>(cbar, cphase, cflag, nthr)) return false;
         // preceding CTAs: Q = agg[c-1] * ... * agg[0]
         double qa = 1, qb = 0, qc = 0, qd = 1;
         const uint32_t xm = smem_u32(xchg + C::XM);
@@ -247,6 +301,7 @@ __device__ void cl_prologue(const JwOperator& op, double* table, double* scratch
         if constexpr (BC::FWD) put(BC::P_NL, nl);
         if constexpr (BC::BWD) put(BC::P_NH, nh);
     }
+    return true;
 }
 
 template <class C>
@@ -266,16 +321,25 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
     double* scratch = reinterpret_cast<double*>(smem_raw + BC::TBL);
     double* xchg = scratch + W * kScratchPerWarp;  // 2 parities x XN doubles
     uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(xchg) + C::XCHG);
-    unsigned char* after = reinterpret_cast<unsigned char*>(bars + 2);
+    unsigned char* after = reinterpret_cast<unsigned char*>(bars + 4);
     const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
     unsigned char* buf0 = after + pad;
     unsigned char* buf1 = buf0 + BC::BUF;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t cbar = smem_u32(&bars[2]);
+    volatile int* cflag = reinterpret_cast<volatile int*>(&bars[3]);
+    uint32_t cphase = 0;
 
     if (threadIdx.x < 2) mbar_init(smem_u32(&bars[threadIdx.x]), W);
+    if (threadIdx.x == 2) mbar_init(cbar, C::C);
     mbar_init_fence();
-    cl_prologue<C>(op, table, scratch, xchg, crank);
+    // Every CTA of the cluster has started and initialised its mbarriers
+    // before any CTA arrives on a peer's (the one hardware cluster barrier,
+    // which every CTA reaches).
+    cluster_sync();
+    bool alive = cl_prologue<C>(op, table, scratch, xchg, crank, cbar, cphase, cflag);
     __syncthreads();
+    if (!alive && threadIdx.x == 0) atomicOr(&g_stream_status, kStatusWaitTimeout | kStatusClusterBarrier);
 
     GroupCtx g;
     g.lane = lane;
@@ -335,20 +399,44 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
         bulk_commit();
     };
 
+    if (!alive) sys = nsys;
     if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+    // A failed TMA wait (bits 0) stops every CTA at the same point, and the
+    // final barrier still runs; a cluster barrier that ran out (alive = false)
+    // skips it, since a peer that never arrived will not arrive there either.
+    auto stop = [&](unsigned bits) {
+        if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout | bits);
+        if (bits) alive = false;
+    };
+    // Waits for the TMA load of the k-th system of this cluster and publishes
+    // the outcome for the peers.  It is published before a cluster barrier --
+    // the first one for k = 0, otherwise the last one of system k-1 -- after
+    // which the system's rows are readable by every CTA and all CTAs read the
+    // same outcomes.
+    auto wait_publish = [&](int k) {
+        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+        ok = group_and(g.bar_id, g.nthr, ok);
+        if (t == 0) xchg[(k & 1) * C::XN + C::XOK] = ok ? 1.0 : 0.0;
+    };
+    if (sys < nsys) {
+        wait_publish(0);
+        if (!cl_barrier<C::C>(cbar, cphase, cflag, T)) {
+            stop(kStatusClusterBarrier << 1);
+            sys = nsys;
+        }
+    }
     for (int k = 0; sys < nsys; ++k, sys += step) {
         unsigned char* cur = (k & 1) ? buf1 : buf0;
         unsigned char* nxt = (k & 1) ? buf0 : buf1;
         double* xc = xchg + (k & 1) * C::XN;
-        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
-        ok = group_and(g.bar_id, g.nthr, ok);
-        if (t == 0) xc[C::XOK] = ok ? 1.0 : 0.0;
-        cluster_sync();  // every CTA's slice has landed; statuses published
-        bool all_ok = true;
-        for (uint32_t r = 0; r < C::C; ++r) all_ok = all_ok && ld_cluster_f64(mapa_rank(smem_u32(xc + C::XOK), r)) != 0.0;
-        if (!all_ok) {
-            if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
-            break;
+        const bool more = sys + step < nsys;
+        {
+            bool a = true;
+            for (uint32_t r = 0; r < C::C; ++r) a = a && ld_cluster_f64(mapa_rank(smem_u32(xc + C::XOK), r)) != 0.0;
+            if (!a) {
+                stop(0);
+                break;
+            }
         }
 
         double be[R + KL + KU];
@@ -400,7 +488,7 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
             }
         }
         double (&x)[R + KL + KU] = be;
-        if (sys + step < nsys && lane == 0) {
+        if (more && lane == 0) {
             bulk_wait_read_all();
             issue_load(nxt, (k & 1) ? bar0 : bar1, sys + step);
         }
@@ -418,7 +506,11 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
                 xc[C::XF] = At;
                 xc[C::XF + 1] = Bt;
             }
-            cluster_sync();
+            if (!BC::BWD && more) wait_publish(k + 1);
+            if (!cl_barrier<C::C>(cbar, cphase, cflag, T)) {
+                stop(kStatusClusterBarrier << 2);
+                break;
+            }
             double X = 0.0;  // value entering this CTA's slice
             for (uint32_t r = 0; r < crank; ++r) {
                 const uint32_t ra = mapa_rank(smem_u32(xc + C::XF), r);
@@ -448,7 +540,11 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
                 xc[C::XB] = At;
                 xc[C::XB + 1] = Bt;
             }
-            cluster_sync();
+            if (more) wait_publish(k + 1);
+            if (!cl_barrier<C::C>(cbar, cphase, cflag, T)) {
+                stop(kStatusClusterBarrier << 3);
+                break;
+            }
             double X = 0.0;  // value entering this CTA's slice from above
             for (uint32_t r = C::C - 1; r > crank; --r) {
                 const uint32_t ra = mapa_rank(smem_u32(xc + C::XB), r);
@@ -469,8 +565,11 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
         // In place: the neighbour CTAs read this slice's halo rows before the
         // scans' cluster barriers; without a solve, wait for them here.
         if constexpr (C::SV == SV_NONE) {
-            if constexpr (KL + KU > 0) cluster_sync();
-            else group_bar(g.bar_id, g.nthr);
+            if (more) wait_publish(k + 1);
+            if (!cl_barrier<C::C>(cbar, cphase, cflag, T)) {
+                stop(kStatusClusterBarrier << 4);
+                break;
+            }
         }
         __syncwarp();
 #pragma unroll
@@ -484,7 +583,8 @@ __global__ void __launch_bounds__(C::T) jw_cluster_kernel(const __grid_constant_
         if (lane == 0) issue_store(cur, sys);
     }
     if (lane == 0) bulk_wait_all();
-    cluster_sync();  // no CTA leaves while a peer may still read its shared memory
+    // No CTA leaves while a peer may still read its shared memory.
+    if (alive && !cl_barrier<C::C>(cbar, cphase, cflag, T)) stop(kStatusClusterBarrier << 5);
 }
 
 }  // namespace pfb
