@@ -318,6 +318,168 @@ int pfo_jw_step_d(const pfo_params* p, const double* bands, double* rhs, int nth
 }
 
 /* ------------------------------------------------------------------------- */
+/* K consecutive JW steps in one kernel (numConsecutiveJWIterations = K > 1;
+ * pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:108-374).
+ *
+ *  - Step s works on M_s = M - s rows (upperBanded 1 or 2) or M + s rows
+ *    (upperBanded 0) (:109-115).  The right-hand side is read once with M rows
+ *    (rows beyond stay zero, pfSolve_Registers.h:171-177) and written once with
+ *    M_{K-1} rows (pfSolve_ReadWrite.h:1934-1935 with the final M_size);
+ *    rows in between stay in registers, so a row that leaves the system keeps
+ *    its last value and is not written back.
+ *  - Bands of step s come from buffer s when there are several input buffers
+ *    (pfSolve_Transfers.h:250-265), else from buffer 0, at offsets that depend
+ *    on M_s (:117-207, :269-353), in register-major order for M_s rows with the
+ *    register count of the plan (computed from M + K - 1 for upperBanded 0,
+ *    pfSolve_Plan_JonesWorland.h:276-283, 342-346).  Rows at or beyond M_s
+ *    read md = 1, ld = ud = 0 (pfSolve_ReadWrite.h:1678-1695).
+ *  - The matvec diagonal is applied at the first step (upperBanded 1) or the
+ *    last (upperBanded 0) only (pfSolve_MatVecMul.h:74-75, 98-101); for
+ *    upperBanded 2 the diagonal is reloaded only at steps 0 and K-1
+ *    (pfSolve_ReadWrite.h:1650), so only K = 2 is defined there.  jw_type%10
+ *    == 3 with upperBanded 0/1 multiplies by a diagonal that is not reloaded
+ *    for K > 1 and is rejected.
+ *  - The off-diagonal entry of row M_s - 1 couples to row M_s, which still
+ *    holds a value after a shrinking step; scaleC multiplies solution row 0
+ *    after every solve (pfSolve_TridiagonalSolve.h:1918-1927). */
+static int64_t reorder_r(int64_t i, int64_t M, int64_t r)
+{
+    int64_t t = i / r, j = i % r;
+    int64_t m = M % r, ceil_n = (M + r - 1) / r, floor_n = M / r;
+    return t + ((j < m) ? j * ceil_n : m * ceil_n + (j - m) * floor_n);
+}
+
+int64_t pfo_steps_registers(int64_t M, int upperBanded, int K)
+{
+    int64_t tempM = upperBanded ? M : M + K - 1;
+    int64_t warp = 64 * ((tempM + 1023) / 1024);
+    if (tempM < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    int64_t r = (tempM + warp - 1) / warp;
+    return r < 1 ? 1 : r;
+}
+
+int pfo_jw_steps_layout(const pfo_params* p, int K, int s, pfo_step* st)
+{
+    const int ub = p->upperBanded, jwt = p->jw_type % 10;
+    if (K < 1 || s < 0 || s >= K) return -1;
+    if (ub == 2 && (jwt != 3 || K > 2)) return -1;
+    if (ub != 2 && (jwt == 3 || (jwt != 0 && jwt != 1 && jwt != 2))) return -1;
+    const int rtM = (p->bitmask & PFO_RUNTIME_OFFSETM) != 0;
+    const int rtV = (p->bitmask & PFO_RUNTIME_OFFSETV) != 0;
+    const int64_t oM = p->run_offsetM, oV = p->run_offsetV;
+    const int64_t Ms = ub ? p->M - s : p->M + s;
+    if (Ms < 1) return -1;
+    memset(st, 0, sizeof(*st));
+    st->M = Ms;
+    st->r = pfo_steps_registers(p->M, ub, K);
+    if (ub == 2) {
+        st->mv = PFO_MV_DIAG; st->diag = 1; st->off_md = Ms;
+        st->sv = PFO_SV_TRI; st->off_sl = 0; st->off_su = 2 * Ms;
+        return 0;
+    }
+    if (jwt != 2) {
+        if (ub == 1) {
+            st->mv = PFO_MV_UPPER; st->diag = (s == 0);
+            st->off_md = rtM ? oM + Ms : 0;
+            st->off_mo = rtM ? oM : (s == 0 ? Ms : 0);
+        } else {
+            st->mv = PFO_MV_LOWER; st->diag = (s == K - 1);
+            st->off_md = rtM ? oM : Ms;
+            st->off_mo = rtM ? oM + Ms : 0;
+        }
+    }
+    if (jwt != 1) {
+        if (ub == 1) { st->sv = PFO_SV_LOWER; st->off_sl = rtV ? oV : (s == 0 ? 2 * Ms : Ms); }
+        else { st->sv = PFO_SV_UPPER; st->off_su = rtV ? oV : (s == K - 1 ? 2 * Ms : Ms); }
+    }
+    return 0;
+}
+
+#define DEFINE_STEPS(NAME, T)                                                                           \
+    int NAME(const pfo_params* p, int K, int nbuf, const double* const* bands, double* rhs, int nthreads) \
+    {                                                                                                   \
+        if (K < 2 || K > PFO_MAX_STEPS || (nbuf != 1 && nbuf < K) || !bands) return -1;                \
+        pfo_step st[PFO_MAX_STEPS];                                                                     \
+        for (int s = 0; s < K; s++)                                                                     \
+            if (pfo_jw_steps_layout(p, K, s, &st[s])) return -1;                                       \
+        rhs_layout R;                                                                                   \
+        rhs_resolve(p, &R);                                                                             \
+        const int64_t M0 = p->M, Mout = st[K - 1].M;                                                    \
+        const int64_t total = (M0 > Mout ? M0 : Mout) + 1;                                              \
+        T* co = (T*)calloc((size_t)(4 * K * total), sizeof(T));                                         \
+        if (!co) return -1;                                                                             \
+        for (int s = 0; s < K; s++) {                                                                   \
+            const double* b = bands[nbuf > 1 ? s : 0];                                                  \
+            T* md = co + (4 * s + 0) * total;                                                           \
+            T* mo = co + (4 * s + 1) * total;                                                           \
+            T* sl = co + (4 * s + 2) * total;                                                           \
+            T* su = co + (4 * s + 3) * total;                                                           \
+            for (int64_t i = 0; i < st[s].M; i++) {                                                     \
+                const int64_t k = p->bandsPermuted ? reorder_r(i, st[s].M, st[s].r) : i;                \
+                md[i] = (st[s].mv != PFO_MV_NONE && st[s].diag) ? (T)b[st[s].off_md + k] : (T)1;        \
+                if (st[s].mv == PFO_MV_UPPER || st[s].mv == PFO_MV_LOWER) mo[i] = (T)b[st[s].off_mo + k]; \
+                if (st[s].sv == PFO_SV_LOWER || st[s].sv == PFO_SV_TRI) sl[i] = (T)b[st[s].off_sl + k]; \
+                if (st[s].sv == PFO_SV_UPPER || st[s].sv == PFO_SV_TRI) su[i] = (T)b[st[s].off_su + k]; \
+            }                                                                                           \
+        }                                                                                               \
+        const T sC = (T)R.scaleC;                                                                       \
+        _Pragma("omp parallel num_threads(nthreads > 0 ? nthreads : 1)")                                \
+        {                                                                                               \
+            T* x = (T*)malloc(sizeof(T) * (size_t)total);                                               \
+            T* y = (T*)malloc(sizeof(T) * (size_t)total);                                               \
+            T* w = (T*)malloc(sizeof(T) * (size_t)total);                                               \
+            _Pragma("omp for schedule(static)")                                                         \
+            for (int64_t q = 0; q < p->batch; q++) {                                                    \
+                const int64_t base = R.offS + q * R.oStride;                                            \
+                for (int64_t i = 0; i < total; i++)                                                     \
+                    x[i] = (i < M0 && keep(i, R.iz0, R.iz1, R.rtIZ)) ? (T)rhs[base + i] : (T)0;         \
+                for (int s = 0; s < K; s++) {                                                           \
+                    const int64_t Ms = st[s].M;                                                         \
+                    const T* md = co + (4 * s + 0) * total;                                             \
+                    const T* mo = co + (4 * s + 1) * total;                                             \
+                    const T* sl = co + (4 * s + 2) * total;                                             \
+                    const T* su = co + (4 * s + 3) * total;                                             \
+                    for (int64_t i = 0; i < total; i++) y[i] = x[i];                                    \
+                    if (st[s].mv != PFO_MV_NONE)                                                        \
+                        for (int64_t i = 0; i < Ms; i++) {                                              \
+                            T v = md[i] * x[i];                                                         \
+                            if (st[s].mv == PFO_MV_UPPER) v += mo[i] * x[i + 1];                        \
+                            if (st[s].mv == PFO_MV_LOWER && i > 0) v += mo[i] * x[i - 1];               \
+                            y[i] = v;                                                                   \
+                        }                                                                               \
+                    if (st[s].sv == PFO_SV_LOWER) {                                                     \
+                        for (int64_t i = 1; i < Ms; i++) y[i] = y[i] - sl[i] * y[i - 1];                \
+                    } else if (st[s].sv == PFO_SV_UPPER) {                                              \
+                        for (int64_t i = Ms - 1; i >= 0; i--) y[i] = y[i] - su[i] * y[i + 1];           \
+                    } else if (st[s].sv == PFO_SV_TRI) {                                                \
+                        /* rows 0..Ms: row Ms is an identity row coupled from above */                  \
+                        w[0] = su[0];                                                                   \
+                        for (int64_t i = 1; i <= Ms; i++) {                                             \
+                            const T a = (i < Ms) ? sl[i] : (T)0;                                        \
+                            const T c = (i < Ms) ? su[i] : (T)0;                                        \
+                            const T den = (T)1 - a * w[i - 1];                                          \
+                            w[i] = c / den;                                                             \
+                            y[i] = (y[i] - a * y[i - 1]) / den;                                         \
+                        }                                                                               \
+                        for (int64_t i = Ms - 1; i >= 0; i--) y[i] = y[i] - w[i] * y[i + 1];            \
+                    }                                                                                   \
+                    if (st[s].sv != PFO_SV_NONE) y[0] = y[0] * sC;                                      \
+                    for (int64_t i = 0; i < total; i++) x[i] = y[i];                                    \
+                }                                                                                       \
+                for (int64_t i = 0; i < Mout; i++)                                                      \
+                    if (keep(i, R.oz0, R.oz1, R.rtOZ)) rhs[base + i] = (double)x[i];                    \
+            }                                                                                           \
+            free(x); free(y); free(w);                                                                  \
+        }                                                                                               \
+        free(co);                                                                                       \
+        return 0;                                                                                       \
+    }
+DEFINE_STEPS(pfo_jw_steps_q, q_t)
+DEFINE_STEPS(pfo_jw_steps_d, double)
+
+/* ------------------------------------------------------------------------- */
 /* dgbmv: y_r = sum_j A[offsetM + j*M + c] x_c, c = r + KU - j, 0 <= c < M
  * (pfSolve_MatVecMul.h:389-443).  The plan-time offsetM is honoured here
  * (pfSolve_dgbmv.h:79-87), unlike the JW kernel. */

@@ -93,6 +93,23 @@ int pfo_jw_step_q_f32(const pfo_params* p, const float* bands, float* rhs, int n
  * __float128 and rounded back to {hi, lo}. */
 int pfo_jw_step_q_dd(const pfo_params* p, const double* bands_dd, double* rhs_dd, int nthreads);
 
+/* K consecutive JW steps (numConsecutiveJWIterations = K, 2 <= K <= 8) on
+ * real FP64 systems, in __float128 ("q") or double ("d").  `bands` holds
+ * `nbuf` buffer pointers: one per step (nbuf >= K, the reference's
+ * useMultipleInputBuffers) or a single buffer read by every step (nbuf = 1).
+ * Returns 0, or -1 for a combination the reference leaves undefined.
+ * Follows pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:108-374. */
+#define PFO_MAX_STEPS 8
+typedef struct {
+    int64_t M, r;              /* rows of the step; register count of the band order */
+    int32_t mv, sv, diag;      /* operator kinds; whether the matvec diagonal is applied */
+    int64_t off_md, off_mo, off_sl, off_su;
+} pfo_step;
+int64_t pfo_steps_registers(int64_t M, int upperBanded, int K);
+int pfo_jw_steps_layout(const pfo_params* p, int K, int s, pfo_step* st);
+int pfo_jw_steps_q(const pfo_params* p, int K, int nbuf, const double* const* bands, double* rhs, int nthreads);
+int pfo_jw_steps_d(const pfo_params* p, int K, int nbuf, const double* const* bands, double* rhs, int nthreads);
+
 /* General banded matvec y = A x, in place on rhs, A in band-major storage
  * A[offsetM + j*M + c] (pfSolve_KernelsLevel1/pfSolve_MatVecMul.h:383-446,
  * pfSolve_KernelsLevel2/pfSolve_dgbmv.h:38-112). */

@@ -57,6 +57,13 @@ class _Params(ctypes.Structure):
     ]
 
 
+class _Step(ctypes.Structure):
+    _fields_ = [("M", ctypes.c_int64), ("r", ctypes.c_int64),
+                ("mv", ctypes.c_int32), ("sv", ctypes.c_int32), ("diag", ctypes.c_int32),
+                ("off_md", ctypes.c_int64), ("off_mo", ctypes.c_int64),
+                ("off_sl", ctypes.c_int64), ("off_su", ctypes.c_int64)]
+
+
 @dataclass
 class Case:
     """Plan-time and launch-time values of one PfSolve application.
@@ -175,6 +182,14 @@ def lib():
     L.pfo_rel_errors.restype = None
     L.pfo_rel_errors_dd.argtypes = L.pfo_rel_errors.argtypes
     L.pfo_rel_errors_dd.restype = None
+    for name in ("pfo_jw_steps_q", "pfo_jw_steps_d"):
+        fn = getattr(L, name)
+        fn.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(dp), dp, ctypes.c_int]
+        fn.restype = ctypes.c_int
+    L.pfo_steps_registers.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+    L.pfo_steps_registers.restype = ctypes.c_int64
+    L.pfo_jw_steps_layout.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Step)]
+    L.pfo_jw_steps_layout.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -238,6 +253,35 @@ def jw_step(case: Case, bands: np.ndarray, rhs: np.ndarray, mode: str = "q", nth
     return out
 
 
+def steps_layout(case: Case, K: int, s: int) -> dict:
+    """Rows, band-order register count, operator kinds and band offsets of step
+    ``s`` of a K-step application (raises for undefined combinations)."""
+    st = _Step()
+    if lib().pfo_jw_steps_layout(ctypes.byref(case.to_c()), int(K), int(s), ctypes.byref(st)):
+        raise ValueError("combination not defined by the reference")
+    return {f: getattr(st, f) for f, _ in _Step._fields_}
+
+
+def steps_permutation(M, r):
+    """Register-major band order of M rows with r registers per lane."""
+    i = np.arange(M, dtype=np.int64)
+    t, j = i // r, i % r
+    m, ce, fl = M % r, -(-M // r), M // r
+    return t + np.where(j < m, j * ce, m * ce + (j - m) * fl)
+
+
+def jw_steps(case: Case, K: int, bands, rhs: np.ndarray, mode: str = "q", nthreads: int = 1) -> np.ndarray:
+    """K consecutive JW steps on a copy of ``rhs``; ``bands`` is one buffer read
+    by every step or a list of K per-step buffers."""
+    bufs = [np.ascontiguousarray(b, dtype=np.float64) for b in (bands if isinstance(bands, (list, tuple)) else [bands])]
+    arr = (ctypes.POINTER(ctypes.c_double) * len(bufs))(*[_dptr(b) for b in bufs])
+    out = np.array(rhs, dtype=np.float64, copy=True)
+    fn = lib().pfo_jw_steps_q if mode == "q" else lib().pfo_jw_steps_d
+    if fn(ctypes.byref(case.to_c()), int(K), len(bufs), arr, _dptr(out), nthreads):
+        raise ValueError("combination not defined by the reference")
+    return out
+
+
 def dgbmv(case: Case, A: np.ndarray, rhs: np.ndarray, mode: str = "q", nthreads: int = 1) -> np.ndarray:
     out = np.array(rhs, dtype=np.float64, copy=True)
     a = np.ascontiguousarray(A, dtype=np.float64)
@@ -293,9 +337,10 @@ def reference_available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def write_reference_case(case_dir: str, case: Case, bands: np.ndarray, rhs: np.ndarray, *,
-                         precision: str = "f64", inp: np.ndarray | None = None, iters: int = 0):
-    """Write the files ``pfsolve_ref`` reads for one case."""
+def write_reference_case(case_dir: str, case: Case, bands, rhs: np.ndarray, *,
+                         precision: str = "f64", inp: np.ndarray | None = None, iters: int = 0, K: int = 1):
+    """Write the files ``pfsolve_ref`` reads for one case.  ``bands`` may be a
+    list of per-step buffers (K consecutive steps with one input buffer each)."""
     os.makedirs(case_dir, exist_ok=True)
     kv = {
         "M": case.M, "size0": case.size0, "size1": case.size1 if (case.block) else case.batch,
@@ -318,12 +363,18 @@ def write_reference_case(case_dir: str, case: Case, bands: np.ndarray, rhs: np.n
         "doublePrecision": 1 if precision in ("f64",) else 0,
         "quadDoubleDoublePrecision": 1 if precision == "dd" else 0,
         "iters": iters,
+        "K": K,
+        # K > 1 on one buffer: no multiple-buffer binding (inputs<k> would not exist)
+        "useMultipleInputBuffers": len(bands) if isinstance(bands, (list, tuple)) else (1 if K == 1 else 0),
     }
     with open(os.path.join(case_dir, "params.txt"), "w") as f:
         for k, v in kv.items():
             f.write(f"{k}={v}\n")
     dt = np.float32 if precision == "f32" else np.float64
-    if bands is not None:
+    if isinstance(bands, (list, tuple)):
+        for k, b in enumerate(bands):
+            np.ascontiguousarray(b, dtype=dt).tofile(os.path.join(case_dir, f"bands_{k}.bin"))
+    elif bands is not None:
         np.ascontiguousarray(bands, dtype=dt).tofile(os.path.join(case_dir, "bands.bin"))
     np.ascontiguousarray(rhs, dtype=dt).tofile(os.path.join(case_dir, "rhs.bin"))
     if inp is not None:

@@ -8,7 +8,8 @@
 //
 // Usage: pfsolve_ref <case_dir>
 //   <case_dir>/params.txt   key=value lines (see parse below)
-//   <case_dir>/bands.bin    band buffer (raw, storage precision)
+//   <case_dir>/bands.bin    band buffer (raw, storage precision), or
+//   <case_dir>/bands_<k>.bin one buffer per step when useMultipleInputBuffers > 1
 //   <case_dir>/rhs.bin      output/RHS buffer (raw, storage precision), in place
 //   <case_dir>/in.bin       block kernel only: its input buffer
 // Writes <case_dir>/out.bin (the RHS/output buffer after one launch) and,
@@ -69,7 +70,11 @@ int main(int argc, char** argv)
     cuDeviceGet(&dev, 0);
     cudaFree(0);  // create the primary context through the runtime
 
-    std::vector<char> bands = read_file(dir + "/bands.bin");
+    const int nbuf = (int)I("useMultipleInputBuffers", 1);
+    std::vector<std::vector<char>> step_bands;
+    if (nbuf > 1)
+        for (int k = 0; k < nbuf; k++) step_bands.push_back(read_file(dir + "/bands_" + std::to_string(k) + ".bin"));
+    std::vector<char> bands = nbuf > 1 ? step_bands[0] : read_file(dir + "/bands.bin");
     std::vector<char> rhs = read_file(dir + "/rhs.bin");
     std::vector<char> inb = read_file(dir + "/in.bin");
     // Timing cases may omit rhs.bin: `rhs_bytes` zero-filled device bytes instead.
@@ -127,7 +132,13 @@ int main(int argc, char** argv)
     cfg.disableCaching = 1;  // no kernel cache files are written or read
     cfg.device = &dev;
 
-    void* bufArr[1] = {cfg.block ? d_in : d_bands};
+    void* bufArr[16] = {cfg.block ? d_in : d_bands};
+    if (nbuf > 16) { fprintf(stderr, "at most 16 input buffers\n"); return 2; }
+    for (int k = 1; k < nbuf; k++) {
+        const std::vector<char>& b = step_bands[k];
+        if (b.empty() || cudaMalloc(&bufArr[k], b.size())) { fprintf(stderr, "bands_%d\n", k); return 4; }
+        cudaMemcpy(bufArr[k], b.data(), b.size(), cudaMemcpyHostToDevice);
+    }
     void* outArr[1] = {d_rhs};
     void* tmpArr[1] = {d_tmp};
     uint64_t bufSizeArr[1] = {cfg.block ? inSize : bandsSize};
@@ -186,6 +197,7 @@ int main(int argc, char** argv)
         if (ft) { fprintf(ft, "%.6f\n", ms / (double)iters); fclose(ft); }
     }
     deletePfSolve(&app);
+    for (int k = 1; k < nbuf; k++) cudaFree(bufArr[k]);
     cudaFree(d_bands);
     cudaFree(d_rhs);
     cudaFree(d_in);

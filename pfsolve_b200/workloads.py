@@ -55,6 +55,74 @@ def permute_bands(natural: np.ndarray, M: int) -> np.ndarray:
     return out
 
 
+def steps_registers(M: int, upperBanded: int, K: int) -> int:
+    """Rows per lane of the reference's band order for a K-step application:
+    computed from M + K - 1 rows when the steps grow the system (upperBanded 0),
+    else from M (pfSolve_Plan_JonesWorland.h:276-283, 342-346)."""
+    tm = M if upperBanded else M + K - 1
+    warp = 64 * ((tm + 1023) // 1024)
+    if tm < 512:
+        warp = 32
+    warp = max(warp, 32)
+    if warp % 32:
+        warp = 32 * ((warp + 31) // 32)
+    return max(1, (tm + warp - 1) // warp)
+
+
+def step_rows(M: int, upperBanded: int, s: int) -> int:
+    """Rows of step s: M - s (upperBanded 1, 2) or M + s (upperBanded 0)."""
+    return M - s if upperBanded else M + s
+
+
+def steps_band_order(Ms: int, r: int) -> np.ndarray:
+    """perm[i] for Ms rows with r rows per lane (one piece, Ms <= 4352)."""
+    i = np.arange(Ms, dtype=np.int64)
+    t, j = i // r, i % r
+    m, ce, fl = Ms % r, -(-Ms // r), Ms // r
+    return t + np.where(j < m, j * ce, m * ce + (j - m) * fl)
+
+
+def steps_bands(rng, M: int, upperBanded: int, K: int, per_step: bool = True):
+    """Band buffers of a K-step application, three bands of Ms rows each per
+    step, stored in the step's band order.  upperBanded 2: normalised
+    tridiagonal (ld | md | ud).  upperBanded 0/1: three bands in U(-1/2, 1/2)
+    (every section is read as some band by one of the jw_types).  Row 0 of
+    every band is zero; the last row's entry of the third band stays random
+    (it couples to the row that leaves or enters the system) unless the step
+    fills the reference's registers exactly.  per_step False: one buffer of
+    3 * max(Ms) values read by every step at its own offsets.  Tridiagonal
+    bands need per_step."""
+    r = steps_registers(M, upperBanded, K)
+    Mmax = max(step_rows(M, upperBanded, s) for s in range(K))
+    tm = M if upperBanded else M + K - 1
+    lanes = 32 if tm < 512 else 64 * ((tm + 1023) // 1024)
+    capacity = r * lanes  # rows held in the reference's registers
+
+    def one(Ms):
+        if upperBanded == 2:
+            a, d, c = tridiagonal(rng, Ms)
+            c[-1] = rng.uniform(-0.25, 0.25)
+            nat = tri_bands(a, d, c)
+        else:
+            nat = rng.uniform(-0.5, 0.5, 3 * Ms)
+            nat[0] = nat[Ms] = nat[2 * Ms] = 0.0
+        if Ms == capacity:  # no row below the last: its upper coupling is unused
+            nat[Ms - 1] = nat[2 * Ms - 1] = nat[3 * Ms - 1] = 0.0
+        out = np.empty_like(nat)
+        perm = steps_band_order(Ms, r)
+        for k in range(3):
+            out[k * Ms + perm] = nat[k * Ms:(k + 1) * Ms]
+        return out
+
+    if per_step:
+        return [one(step_rows(M, upperBanded, s)) for s in range(K)]
+    buf = rng.uniform(-0.5, 0.5, 3 * Mmax)
+    for s_ in range(K):  # row 0 of every band any step reads
+        Ms = step_rows(M, upperBanded, s_)
+        buf[[0, Ms, 2 * Ms]] = 0.0
+    return buf
+
+
 def tridiagonal(rng, M, dominance=None):
     """(a, d, c): a_0 = c_{M-1} = 0.  d = |a|+|c|+U(1,2), or dominance*(|a|+|c|)."""
     a = rng.uniform(-1.0, 1.0, M)

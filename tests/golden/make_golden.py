@@ -125,6 +125,62 @@ def block_cases():
     return out
 
 
+def steps_cases():
+    """(name, Case, K, band buffers, rhs) for K consecutive steps
+    (numConsecutiveJWIterations), stored under tests/golden/steps/."""
+    out = []
+    combos = [(1, 10, (2, 3, 5)), (0, 10, (2, 3, 5)), (1, 11, (3,)), (0, 11, (3,)), (1, 12, (3,)), (0, 12, (3,)),
+              (2, 13, (2,))]
+    for ub, jwt, Ks in combos:
+        for K in Ks:
+            for M in (33, 250, 1000):
+                rng = np.random.default_rng(12000 + 1000 * ub + 10 * jwt + K + M)
+                bands = WL.steps_bands(rng, M, ub, K)
+                case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=jwt, cfg_outputBufferStride=M + K + 3)
+                rhs = rng.uniform(-1, 1, case.rhs_len() + K)
+                out.append((f"steps_ub{ub}_t{jwt}_K{K}_M{M}", case, K, bands, rhs))
+    # one buffer read by every step at its own offsets
+    for ub in (0, 1):
+        M, K = 120, 3
+        rng = np.random.default_rng(12500 + ub)
+        buf = WL.steps_bands(rng, M, ub, K, per_step=False)
+        case = O.Case(M=M, batch=2, upperBanded=ub, jw_type=10, cfg_outputBufferStride=M + 8)
+        out.append((f"steps_onebuf_ub{ub}", case, K, [buf], rng.uniform(-1, 1, case.rhs_len() + K)))
+    # launch-time windows, scaleC, stride and solution offset
+    bm = (RT.RUNTIME_OFFSETSOLUTION | RT.RUNTIME_INPUTZEROPAD | RT.RUNTIME_OUTPUTZEROPAD | RT.RUNTIME_SCALEC |
+          RT.RUNTIME_OUTPUTBUFFERSTRIDE)
+    for ub in (0, 1, 2):
+        M, K = 200, (2 if ub == 2 else 4)
+        rng = np.random.default_rng(12600 + ub)
+        case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=13 if ub == 2 else 10, bitmask=bm,
+                      run_offsetSolution=4, run_inputZeropad=(2, 190), run_outputZeropad=(3, 199),
+                      run_scaleC=0.75, run_outputBufferStride=M + K + 9)
+        out.append((f"steps_runtime_ub{ub}", case, K, WL.steps_bands(rng, M, ub, K),
+                    rng.uniform(-1, 1, case.rhs_len() + K + 8)))
+    return out
+
+
+def steps_offset_cases():
+    """Launch-time offsetM / offsetV with K > 1 (the reference's generator
+    was seen to fail on the host for these; kept apart so the others run)."""
+    out = []
+    for ub in (0, 1):
+        M, K = 200, 3
+        rng = np.random.default_rng(12700 + ub)
+        oM, oV = 5, 3 * (M + K) + 2
+        bufs = []
+        for s_ in range(K):
+            Ms = WL.step_rows(M, ub, s_)
+            b = rng.uniform(-0.5, 0.5, oV + M + K + 4)
+            b[oV] = 0.0
+            b[oM + Ms] = b[oM] = 0.0
+            bufs.append(b)
+        case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=10, bitmask=RT.RUNTIME_OFFSETM | RT.RUNTIME_OFFSETV,
+                      run_offsetM=oM, run_offsetV=oV, cfg_outputBufferStride=M + K + 3)
+        out.append((f"steps_offsetMV_ub{ub}", case, K, bufs, rng.uniform(-1, 1, case.rhs_len() + K)))
+    return out
+
+
 REF_BIN_FP128 = os.path.join(ROOT, "oracle", "_ref", "pfsolve_ref_fp128")
 
 
@@ -150,11 +206,14 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--time", action="store_true")
+    ap.add_argument("--only", default="all", choices=["all", "steps"],
+                    help="steps: only the K-step fixtures (and K-step timing with --time)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
     summary = {}
-    for name, case, buf, rhs, prec in jw_cases() + dgbmv_cases() + block_cases():
+    single = jw_cases() + dgbmv_cases() + block_cases() if args.only == "all" else []
+    for name, case, buf, rhs, prec in single:
         try:
             ref = run_case(tmp, name, case, buf, rhs, prec)
             np.savez_compressed(os.path.join(args.out, name + ".npz"), params=json.dumps(asdict(case)),
@@ -163,7 +222,7 @@ def main():
         except Exception as e:  # record and continue: one failing case must not hide the others
             summary[name] = f"error: {e}"
             traceback.print_exc()
-    if args.time:
+    if args.time and args.only == "all":
         timing = {}
         for label, M, B in [("config3_jw_t13_N512_B131072", 512, 131072),
                             ("config2_jw_t13_N1024_B131072real", 1024, 131072),
@@ -186,6 +245,45 @@ def main():
             except Exception as e:
                 timing[label] = dict(error=str(e))
         with open(os.path.join(args.out, "ref_timing.json"), "w") as f:
+            json.dump(timing, f, indent=1)
+        print(json.dumps(timing, indent=1))
+    sdir = os.path.join(args.out, "steps")
+    os.makedirs(sdir, exist_ok=True)
+    for name, case, K, bufs, rhs in steps_cases() + steps_offset_cases():
+        try:
+            d = os.path.join(tmp, name)
+            O.write_reference_case(d, case, list(bufs) if len(bufs) > 1 else bufs[0], rhs, K=K)
+            path, _ = O.run_reference(d)
+            ref = np.fromfile(path, dtype=np.float64)
+            np.savez_compressed(os.path.join(sdir, name + ".npz"), params=json.dumps(asdict(case)), K=K,
+                                nbuf=len(bufs), rhs=rhs, ref_out=ref,
+                                **{f"buffer_{k}": b for k, b in enumerate(bufs)})
+            summary[name] = "ok"
+        except Exception as e:
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
+    if args.time:
+        # K consecutive steps in one reference kernel (upperBanded 1, jw_type 10)
+        timing = {}
+        for K in (1, 2, 4):
+            M, B = 512, 131072
+            rng = np.random.default_rng(5)
+            label = f"steps_ub1_t10_N512_K{K}_B131072"
+            case = O.Case(M=M, batch=B, upperBanded=1, jw_type=10)
+            d = os.path.join(tmp, label)
+            os.makedirs(d, exist_ok=True)
+            bufs = WL.steps_bands(rng, M, 1, K) if K > 1 else [WL.steps_bands(rng, M, 1, 2)[0]]
+            O.write_reference_case(d, case, bufs if K > 1 else bufs[0], np.zeros(1), precision="f64",
+                                   iters=20, K=K)
+            os.remove(os.path.join(d, "rhs.bin"))
+            with open(os.path.join(d, "params.txt"), "a") as f:
+                f.write(f"rhs_bytes={8 * M * B}\n")
+            try:
+                _, ms = O.run_reference(d, timeout=300)
+                timing[label] = dict(ms=ms, rhs_per_s=B / (ms * 1e-3), gbs=2 * 8 * M * B / (ms * 1e-3) / 1e9)
+            except Exception as e:
+                timing[label] = dict(error=str(e))
+        with open(os.path.join(args.out, "ref_timing_steps.json"), "w") as f:
             json.dump(timing, f, indent=1)
         print(json.dumps(timing, indent=1))
     with open(os.path.join(args.out, "summary.json"), "w") as f:
