@@ -452,6 +452,40 @@ def config3_profile(args):
     app.close()
 
 
+def steps_profile(args):
+    """Profiling case: K consecutive JW steps in one launch (upperBanded 1,
+    jw_type 10: bidiagonal matvec + lower bidiagonal solve per step; per-step
+    band buffers), N = --m rows, --ncplx systems, --ksteps K; K = 1 runs the
+    single-step kernel on the same operator.  Prints one JSON line."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App
+    M, B, K = args.m, args.ncplx, args.ksteps
+    rng = np.random.default_rng(5)
+    bands = WL.steps_bands(rng, M, 1, max(K, 2))[:max(K, 1)]
+    tbs = [torch.from_numpy(b).cuda() for b in bands]
+    x = torch.from_numpy(rng.uniform(-1, 1, M * B)).cuda()
+    extra = dict(numConsecutiveJWIterations=K, useMultipleInputBuffers=K) if K > 1 else {}
+    app = App(buffer=tbs if K > 1 else tbs[0], outputBuffer=x, M_size=M, size=(M, B), upperBanded=1, jw_type=10,
+              doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows, **extra)
+    for _ in range(max(1, args.warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    mout = M - K + 1
+    print(json.dumps({"profile_case": "ksteps", "M": M, "rhs": B, "K": K, "ms_per_step": ms,
+                      "gbs": (M + mout) * 8 * B / (ms * 1e-3) / 1e9, "rhs_per_s": B / (ms * 1e-3),
+                      "kernel": app.shape()}), flush=True)
+    app.close()
+
+
 def config4_profile(args):
     """Profiling case: config 4 (one spectral timestep, degrees l = 0..--lmax),
     one persistent uneven-batch launch per step (no graph), K timed steps."""
@@ -503,11 +537,12 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps"],
                     help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems) or "
                          "config 4 (degrees 0..--lmax)")
     ap.add_argument("--lmax", type=int, default=511, help="config 4 profiling case: highest harmonic degree")
-    ap.add_argument("--m", type=int, default=512, help="config 3 profiling case: rows per system")
+    ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
+    ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1],
                     help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
@@ -530,6 +565,9 @@ def main():
         return
     if args.profile and args.workload == "config4":
         config4_profile(args)
+        return
+    if args.profile and args.workload == "ksteps":
+        steps_profile(args)
         return
     try:
         if args.impl == "reference":

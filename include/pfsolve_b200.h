@@ -161,8 +161,11 @@ typedef struct {
     uint64_t disableSetLocale;  /* accepted */
     uint64_t useUint64;         /* accepted; addressing is always 64-bit */
 
-    int numConsecutiveJWIterations; /* K; 1 supported */
-    int useMultipleInputBuffers;    /* bands of step k in buffer[k] */
+    int numConsecutiveJWIterations; /* K consecutive steps in one kernel, 1..8: upperBanded 0/1 with
+                                       jw_type % 10 in {0, 1, 2}; upperBanded 2 with K = 2
+                                       (pfSolve_JonesWorland.h:108-374); FP64 only */
+    int useMultipleInputBuffers;    /* >= K: bands of step k in buffer[k]; 0 or 1: every step reads
+                                       buffer[0] at its own offsets (pfSolve_Transfers.h:250-265) */
 
     /* --- extensions (0 keeps the reference behaviour) --- */
     int mixedPrecisionRefinement; /* 1..3 with doublePrecision: FP32 factor-solve plus this many
@@ -351,7 +354,8 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * rowsPerThread x warpsPerSystem rows per group and groupsPerCTA groups;
  * streaming = 0: the group kernel's shape; streaming = 2: long systems
  * (M > 4096), one thread-block cluster per system, warpsPerSystem warps over
- * the cluster's CTAs.  No counterpart in the reference. */
+ * the cluster's CTAs; streaming = 3: the K-step kernel
+ * (numConsecutiveJWIterations > 1).  No counterpart in the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);
 /* Launches that ran on the streaming kernel since load (all apps). */

@@ -68,7 +68,10 @@ class App:
         self.alive = True
 
     def _vpp(self, t):
-        arr = (ctypes.c_void_p * 1)(_ptr(t))
+        """void** for one buffer, or for a list of buffers (one per step of a
+        K-step application with useMultipleInputBuffers)."""
+        ts = list(t) if isinstance(t, (list, tuple)) else [t]
+        arr = (ctypes.c_void_p * len(ts))(*[_ptr(x) for x in ts])
         self._keep.append(arr)
         return ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
 

@@ -53,6 +53,11 @@ struct AppState {
     int cluster_max = 0;
     int R_req = 0;           // caller's rows per thread (0: choose)
     bool no_stream = false;  // kernelPath 1
+    // K consecutive steps (numConsecutiveJWIterations > 1): one kernel
+    int K = 1;
+    const StepsVariant* steps_v = nullptr;
+    int steps_W = 1, steps_G = 1, steps_max_blocks = 0, steps_nbuf = 1;
+    int64_t steps_r = 1;  // rows per lane of the reference's band order
     // fused-chain plans made with this JW app, by operator shape
     struct ChainPlan {
         int KL, KU, sv, LIN, LOUT, SCALE;
@@ -169,6 +174,80 @@ bool choose_cluster(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         return true;
     }
     return false;
+}
+
+// Rows per lane of the reference's band order for a K-step plan: from M + K - 1
+// rows when the steps grow the system (upperBanded 0), else from M
+// (pfSolve_Plan_JonesWorland.h:276-283, 311-314, 342-346).
+int64_t steps_band_registers(int64_t M, int ub, int K)
+{
+    const int64_t tm = ub ? M : M + K - 1;
+    int64_t warp = 64 * ((tm + 1023) / 1024);
+    if (tm < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    const int64_t r = (tm + warp - 1) / warp;
+    return r < 1 ? 1 : r;
+}
+
+// K-step plan (pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:108-374).  Defined
+// combinations: upperBanded 0/1 with jw_type % 10 in {0, 1, 2}; upperBanded 2
+// with jw_type % 10 == 3 and K == 2 (for K > 2 the reference multiplies the
+// middle steps by a diagonal it never reloads, pfSolve_ReadWrite.h:1650; the
+// same holds for jw_type % 10 == 3 with upperBanded 0/1).
+PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
+{
+    const int K = c.numConsecutiveJWIterations, ub = c.upperBanded, jwt = c.jw_type % 10;
+    if (K > kMaxSteps) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (s->prec != PREC_F64 || c.mixedPrecisionRefinement) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (ub == 2 ? (jwt != 3 || K != 2) : !(jwt == 0 || jwt == 1 || jwt == 2)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (c.useMultipleInputBuffers > 1 && c.useMultipleInputBuffers < K) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    // launch-time band offsets: the reference's plan creation fails (the
+    // process crashes) for K > 1, so there is no behaviour to follow
+    if (c.jw_control_bitmask & (RUNTIME_OFFSETM | RUNTIME_OFFSETV)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const int64_t M = c.M_size, Mmax = ub ? M : M + K - 1, Mout = ub ? M - K + 1 : M + K - 1;
+    if (Mout < 1) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+    if (Mmax > kMaxRows) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+    s->K = K;
+    s->steps_nbuf = c.useMultipleInputBuffers > 1 ? c.useMultipleInputBuffers : 1;
+    s->steps_r = steps_band_registers(M, ub, K);
+    const int MV = jwt != 2;
+    const int KL = (MV && ub == 0) ? 1 : 0, KU = (MV && ub == 1) ? 1 : 0;
+    const int SV = ub == 2 ? SV_TRI : (jwt == 1 ? SV_NONE : (ub == 1 ? SV_LOWER : SV_UPPER));
+    int Rs[3] = {4, 8, 16};
+    int n = 3;
+    if (c.rowsPerThread == 4 || c.rowsPerThread == 8 || c.rowsPerThread == 16) {
+        Rs[0] = c.rowsPerThread;
+        n = 1;
+    }
+    int maxopt = 0;
+    cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
+    for (int i = 0; i < n; ++i) {
+        const int R = Rs[i];
+        const int64_t W = (Mmax + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+        // at most 8 warps per system; 4 rows per thread only for one warp
+        if (W > 8 || (n == 3 && R == 4 && W > 1) || (n == 3 && R == 8 && W > 8)) continue;
+        const StepsVariant* v = find_steps_variant(R, KL, KU, SV, MV);
+        if (!v) continue;
+        const int maxthr = R >= 16 ? 256 : 512;
+        if (32 * W > maxthr) continue;
+        for (int G = std::min(maxthr / (32 * (int)W), 15); G >= 1; --G) {  // named barriers 1..15
+            const size_t smem = v->smem_bytes(K, (int)W, G);
+            if ((int)smem > maxopt) continue;
+            if (smem > 48 * 1024 && !allow_max_smem(v->func)) continue;
+            int blocks = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * (int)W * G, smem) != cudaSuccess ||
+                blocks < 1)
+                continue;
+            s->steps_v = v;
+            s->steps_W = (int)W;
+            s->steps_G = G;
+            s->steps_max_blocks = blocks * s->num_sms;
+            return PFSOLVE_SUCCESS;
+        }
+    }
+    cudaGetLastError();
+    return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // the step tables do not fit shared memory
 }
 
 // Pick the kernel variant and launch shape for M rows: register variants
@@ -369,6 +448,89 @@ PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& i
     return PFSOLVE_SUCCESS;
 }
 
+// Band offsets of step s of a K-step launch (pfSolve_JonesWorland.h:117-207 for
+// the matvec operand, :269-353 for the solve operand, with M_size = M_s).
+void step_layout(const PfSolveConfiguration& c, int s, int K, JwStepDesc& d)
+{
+    const int ub = c.upperBanded, jwt = c.jw_type % 10;
+    const int64_t Ms = ub ? c.M_size - s : c.M_size + s;
+    d.M = Ms;
+    d.off_md = d.off_mo = d.off_sl = d.off_su = 0;
+    d.diag = 0;
+    if (ub == 2) {
+        d.diag = 1;
+        d.off_md = Ms;
+        d.off_sl = 0;
+        d.off_su = 2 * Ms;
+        return;
+    }
+    if (jwt != 2) {
+        if (ub == 1) {
+            d.diag = s == 0;
+            d.off_md = 0;
+            d.off_mo = s == 0 ? Ms : 0;
+        } else {
+            d.diag = s == K - 1;
+            d.off_md = Ms;
+            d.off_mo = 0;
+        }
+    }
+    if (jwt != 1) {
+        if (ub == 1) d.off_sl = s == 0 ? 2 * Ms : Ms;
+        else d.off_su = s == K - 1 ? 2 * Ms : Ms;
+    }
+}
+
+PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* lp, const Resolved& r,
+                           cudaStream_t stream)
+{
+    AppState* s = st(app);
+    const PfSolveConfiguration& c = app->configuration;
+    JwSteps S;
+    memset(&S, 0, sizeof(S));
+    S.K = s->K;
+    S.perm = 1;
+    S.scaleC = r.scaleC;
+    S.M_in = c.M_size;
+    for (int k = 0; k < s->K; ++k) {
+        JwStepDesc& d = S.st[k];
+        void* b = r.bands;
+        if (s->steps_nbuf > 1) {
+            void** arr = (lp && lp->buffer) ? lp->buffer : c.buffer;
+            b = arr ? arr[k] : nullptr;
+        }
+        if (!b) return PFSOLVE_ERROR_EMPTY_buffer;
+        d.bands = static_cast<const double*>(b);
+        step_layout(c, k, s->K, d);
+        d.perm_r = s->steps_r;
+        d.perm_m = d.M % d.perm_r;
+        d.perm_ceil = (d.M + d.perm_r - 1) / d.perm_r;
+        d.perm_floor = d.M / d.perm_r;
+    }
+    S.M_out = S.st[s->K - 1].M;
+    JwIO io;
+    memset(&io, 0, sizeof(io));
+    io.in = static_cast<const double*>(r.rhs);
+    io.out = static_cast<double*>(r.rhs);
+    io.in_off = io.out_off = r.offS;
+    io.in_stride = io.out_stride = r.oS;
+    io.iz0 = r.iz0; io.iz1 = r.iz1; io.oz0 = r.oz0; io.oz1 = r.oz1;
+    io.nsys = r.batch;
+    io.M = std::max(S.M_in, S.M_out);
+    if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    const StepsVariant* v = s->steps_v;
+    const int64_t want = (io.nsys + s->steps_G - 1) / s->steps_G;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->steps_max_blocks));
+    v->launch(dim3((unsigned)grid), dim3(32 * s->steps_W * s->steps_G), v->smem_bytes(s->K, s->steps_W, s->steps_G),
+              stream, S, io, s->steps_W);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
 PfSolveResult append_jw(PfSolveApplication* app, const PfSolveLaunchParams* lp, cudaStream_t stream)
 {
     AppState* s = st(app);
@@ -377,6 +539,7 @@ PfSolveResult append_jw(PfSolveApplication* app, const PfSolveLaunchParams* lp, 
     PfSolveResult res = resolve(app, lp, r);
     if (res != PFSOLVE_SUCCESS) return res;
     if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
+    if (s->K > 1) return append_steps(app, lp, r, stream);
     JwLayout L;
     jw_layout(c, (c.jw_control_bitmask & RUNTIME_OFFSETM) != 0, (c.jw_control_bitmask & RUNTIME_OFFSETV) != 0,
               r.offM, r.offV, L);
@@ -515,6 +678,13 @@ PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int
 {
     if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
     const AppState* s = static_cast<const AppState*>(app->internal);
+    if (s->steps_v) {
+        if (streaming) *streaming = 3;
+        if (rowsPerThread) *rowsPerThread = s->steps_v->R;
+        if (warpsPerSystem) *warpsPerSystem = s->steps_W;
+        if (groupsPerCTA) *groupsPerCTA = s->steps_G;
+        return PFSOLVE_SUCCESS;
+    }
     if (s->cluster_v) {
         if (streaming) *streaming = 2;
         if (rowsPerThread) *rowsPerThread = s->cluster_v->R;
@@ -578,9 +748,12 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
         s->kind = APP_JW;
         if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
-        else if (c.numConsecutiveJWIterations > 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (((c.jw_type / 100) % 10) == 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // ALT mode
         else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.numConsecutiveJWIterations > 1) {
+            s->prec = dd_prec;
+            r = plan_steps(s, c);
+        }
         else if (c.M_size > kMaxRowsLong || c.M_size < 1) r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
         else {
             JwLayout L;

@@ -45,6 +45,30 @@ struct JwIO {
     int accumulate;               // output += result
 };
 
+// K consecutive steps in one kernel (numConsecutiveJWIterations = K).
+constexpr int kMaxSteps = 8;
+
+// One step, resolved on the host: its rows, band buffer and offsets, and the
+// register-major band order of its rows (reorder_i0 for M_s rows with the
+// plan's rows per lane, pfSolve_Plan_JonesWorland.h:66-142, 276-283, 342-346).
+struct JwStepDesc {
+    const double* bands;
+    int64_t M;
+    int64_t off_md, off_mo, off_sl, off_su;
+    int diag;  // the matvec multiplies by the band diagonal (else by 1)
+    int pad;
+    int64_t perm_r, perm_m, perm_ceil, perm_floor;
+};
+
+struct JwSteps {
+    int K;
+    int perm;        // bands in the reference's register-major order
+    double scaleC;   // solution row 0 after every solve
+    int64_t M_in;    // rows read (M_0)
+    int64_t M_out;   // rows written (M_{K-1})
+    JwStepDesc st[kMaxSteps];
+};
+
 // Uneven batches: one descriptor per entry (systems sharing one matrix) and
 // a work list of (entry, system range) items consumed through a counter.
 struct BatchEntryDev {

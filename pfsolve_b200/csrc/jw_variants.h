@@ -70,6 +70,16 @@ unsigned cluster_status_fetch_clear();
 // (0: none timed out); reading it synchronises with the device.
 unsigned stream_status_fetch_clear();
 
+// K consecutive JW steps in one kernel (real FP64 systems; R rows per thread,
+// W warps per system given at launch).  MV: the steps have a matvec.
+struct StepsVariant {
+    int R, KL, KU, SV, MV;
+    const void* func;
+    size_t (*smem_bytes)(int K, int W, int G);
+    void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwSteps& S, const JwIO& io, int W);
+};
+const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV);
+
 // Standalone kernels of the block and generic-bandwidth dgbmv applications.
 struct BlockArgs {
     const double* in;

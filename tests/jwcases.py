@@ -40,6 +40,26 @@ def run_app(case: O.Case, buffer: np.ndarray, out: np.ndarray, **extra):
     return res
 
 
+def run_steps(case: O.Case, K: int, bufs, out: np.ndarray, **extra):
+    """K consecutive steps in one app: ``bufs`` is one band buffer read by every
+    step or a list of K per-step buffers (useMultipleInputBuffers = K).
+    Returns (output buffer after the launch, the plan's shape)."""
+    import torch
+
+    from pfsolve_b200.api import App
+    bl = bufs if isinstance(bufs, (list, tuple)) else [bufs]
+    tbs = [torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).cuda() for b in bl]
+    to = torch.from_numpy(np.array(out, dtype=np.float64, copy=True)).cuda()
+    app = App(buffer=tbs, outputBuffer=to, numConsecutiveJWIterations=K,
+              useMultipleInputBuffers=len(tbs) if len(tbs) > 1 else 0, **case_fields(case, **extra))
+    shape = app.shape()
+    app.append(**launch_fields(case))
+    torch.cuda.synchronize()
+    res = to.cpu().numpy()
+    app.close()
+    return res, shape
+
+
 def rel_err(x, ref, case: O.Case):
     return O.rel_errors(x, ref, case.M, case.batch, case.out_stride, case.offset_solution)
 

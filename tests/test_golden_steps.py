@@ -64,3 +64,13 @@ def test_undefined_step_combinations_rejected():
         case = O.Case(M=64, batch=1, upperBanded=ub, jw_type=jwt)
         with pytest.raises(ValueError):
             O.jw_steps(case, K, WL.steps_bands(rng, 64, ub, K), np.zeros(64 + K))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", FILES, ids=IDS)
+def test_kernel_matches_reference(path):
+    import jwcases as J
+    case, K, bufs, rhs, ref = load(path)
+    got, shape = J.run_steps(case, K, bufs if len(bufs) > 1 else bufs[0], rhs)
+    assert shape["streaming"] == 3, shape
+    assert np.abs(got - ref).max() <= 2e-13 * np.abs(ref).max()
