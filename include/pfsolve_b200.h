@@ -355,7 +355,11 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * streaming = 0: the group kernel's shape; streaming = 2: long systems
  * (M > 4096), one thread-block cluster per system, warpsPerSystem warps over
  * the cluster's CTAs; streaming = 3: the K-step kernel
- * (numConsecutiveJWIterations > 1).  No counterpart in the reference. */
+ * (numConsecutiveJWIterations > 1); streaming = 4: K bidiagonal steps with one
+ * system per lane in one sweep wherever a launch's buffers allow it
+ * (16-byte-aligned rows, stride >= the rows written, full output window;
+ * groupsPerCTA = warps per CTA), else the K-step kernel.  No counterpart in
+ * the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);
 /* Launches that ran on the streaming kernel since load (all apps). */

@@ -58,6 +58,10 @@ struct AppState {
     const StepsVariant* steps_v = nullptr;
     int steps_W = 1, steps_G = 1, steps_max_blocks = 0, steps_nbuf = 1;
     int64_t steps_r = 1;  // rows per lane of the reference's band order
+    // bidiagonal kinds: one system per lane, all steps in one sweep (used when
+    // a launch's buffers allow the TMA boxes), NW warps per CTA at most
+    const SeqStepsVariant* seq_v = nullptr;
+    int seq_NW = 0;
     // fused-chain plans made with this JW app, by operator shape
     struct ChainPlan {
         int KL, KU, sv, LIN, LOUT, SCALE;
@@ -222,6 +226,23 @@ PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
     }
     int maxopt = 0;
     cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
+    if (ub != 2 && c.kernelPath != 1) {
+        const SeqStepsVariant* v = find_seq_steps_variant(ub, MV, SV != SV_NONE, K);
+        const int64_t Mtab = ub ? M : Mout;
+        const int64_t fixed = (int64_t)seq_steps_smem_bytes(K, Mtab, 0);
+        const int64_t per_warp = (int64_t)seq_steps_smem_bytes(K, Mtab, 1) - fixed;
+        int nw = (int)std::min<int64_t>(v ? v->max_threads / 32 : 0, ((int64_t)maxopt - fixed) / per_warp);
+        if (v && nw >= 4 && allow_max_smem(v->func)) {
+            int blocks = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * nw,
+                                                              seq_steps_smem_bytes(K, Mtab, nw)) == cudaSuccess &&
+                blocks >= 1) {
+                s->seq_v = v;
+                s->seq_NW = nw;
+            }
+        }
+        cudaGetLastError();
+    }
     for (int i = 0; i < n; ++i) {
         const int R = Rs[i];
         const int64_t W = (Mmax + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
@@ -247,7 +268,8 @@ PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
         }
     }
     cudaGetLastError();
-    return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // the step tables do not fit shared memory
+    // the step tables do not fit shared memory: a sweep-only plan, else none
+    return s->seq_v ? PFSOLVE_SUCCESS : PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
 }
 
 // Pick the kernel variant and launch shape for M rows: register variants
@@ -518,7 +540,28 @@ PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* l
     io.nsys = r.batch;
     io.M = std::max(S.M_in, S.M_out);
     if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    CUtensorMap tin, tout;
+    if (s->seq_v && io.oz0 <= 0 && io.oz1 >= S.M_out && encode_seq_maps(io, S.M_in, S.M_out, &tin, &tout)) {
+        // 32 systems per warp; warps per CTA so that every SM's warps finish
+        // their blocks in the same number of rounds
+        const int64_t nblk = (io.nsys + 31) / 32;
+        const int64_t cap = (int64_t)s->num_sms * s->seq_NW;
+        const int64_t rounds = (nblk + cap - 1) / cap;
+        const int nw = (int)std::max<int64_t>(1, (nblk + (int64_t)s->num_sms * rounds - 1) / ((int64_t)s->num_sms * rounds));
+        const int64_t grid = std::min<int64_t>(s->num_sms, (nblk + nw - 1) / nw);
+        const int64_t Mtab = c.upperBanded ? S.M_in : S.M_out;
+        s->seq_v->launch(dim3((unsigned)grid), dim3(32 * nw), seq_steps_smem_bytes(S.K, Mtab, nw), stream, &tin, &tout,
+                         S, io);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        g_stream_launches.fetch_add(1, std::memory_order_relaxed);
+        if (cudaPeekAtLastError() != cudaSuccess) {
+            cudaGetLastError();
+            return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+        }
+        return PFSOLVE_SUCCESS;
+    }
     const StepsVariant* v = s->steps_v;
+    if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // sweep-only plan, buffers it cannot take
     const int64_t want = (io.nsys + s->steps_G - 1) / s->steps_G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->steps_max_blocks));
     v->launch(dim3((unsigned)grid), dim3(32 * s->steps_W * s->steps_G), v->smem_bytes(s->K, s->steps_W, s->steps_G),
@@ -678,6 +721,13 @@ PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int
 {
     if (!app || !app->internal) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
     const AppState* s = static_cast<const AppState*>(app->internal);
+    if (s->seq_v) {
+        if (streaming) *streaming = 4;
+        if (rowsPerThread) *rowsPerThread = 0;
+        if (warpsPerSystem) *warpsPerSystem = 0;
+        if (groupsPerCTA) *groupsPerCTA = s->seq_NW;
+        return PFSOLVE_SUCCESS;
+    }
     if (s->steps_v) {
         if (streaming) *streaming = 3;
         if (rowsPerThread) *rowsPerThread = s->steps_v->R;

@@ -1,8 +1,10 @@
-// steps_variants.cu -- instantiations of the K-step JW kernel (jw_steps.cuh):
-// the six defined operator kinds of upperBanded 0/1 (jw_type 10, 11, 12) and
-// the tridiagonal kind of upperBanded 2 (jw_type 13), at 4, 8 and 16 rows per
-// thread.
+// steps_variants.cu -- instantiations of the K-step JW kernels: the partition
+// kernel (jw_steps.cuh) for the six defined operator kinds of upperBanded 0/1
+// (jw_type 10, 11, 12) and the tridiagonal kind of upperBanded 2 (jw_type 13)
+// at 4, 8 and 16 rows per thread; the one-system-per-lane sweep kernel
+// (jw_steps_seq.cuh) for the six bidiagonal kinds with K up to 2, 4 or 8.
 #include "jw_steps.cuh"
+#include "jw_steps_seq.cuh"
 #include "jw_variants.h"
 
 namespace pfb {
@@ -41,5 +43,31 @@ const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV)
         if (v.R == R && v.KL == KL && v.KU == KU && v.SV == SV && v.MV == (MV ? 1 : 0)) return &v;
     return nullptr;
 }
+
+template <int UB, bool MV, bool SV, int KMAX>
+static void seq_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in,
+                          const CUtensorMap* out, const JwSteps& S, const JwIO& io)
+{
+    jw_steps_seq_kernel<UB, MV, SV, KMAX><<<grid, block, smem, st>>>(*in, *out, S, io);
+}
+
+#define PFB_SQ(UB, MV, SV, KM)                                                                          \
+    SeqStepsVariant{UB, MV, SV, KM, SeqThreads<KM>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, KM>, \
+                    &seq_launch_fn<UB, MV, SV, KM>}
+#define PFB_SQ3(UB, MV, SV) PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 4), PFB_SQ(UB, MV, SV, 8)
+
+static const SeqStepsVariant kSeqVariants[] = {
+    PFB_SQ3(1, true, true), PFB_SQ3(1, true, false), PFB_SQ3(1, false, true),
+    PFB_SQ3(0, true, true), PFB_SQ3(0, true, false), PFB_SQ3(0, false, true),
+};
+
+const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K)
+{
+    for (const SeqStepsVariant& v : kSeqVariants)
+        if (v.UB == UB && v.MV == (MV ? 1 : 0) && v.SV == (SV ? 1 : 0) && K <= v.KMAX) return &v;
+    return nullptr;
+}
+
+size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW) { return seq_smem_bytes(K, Mtab, NW); }
 
 }  // namespace pfb

@@ -3,6 +3,8 @@
 // right-hand sides, and the status of the kernels' bounded waits.
 #include <cuda.h>
 
+#include <algorithm>
+
 #include "jw_variants.h"
 
 namespace pfb {
@@ -90,6 +92,27 @@ bool encode_row_maps(int R_, int LIN, int LOUT, int IB, int IBO, const JwIO& io,
                            io.out_stride * 16, IBO);
     const int64_t osets = (LOUT == LAY_XXII) ? 2 * io.nsys : io.nsys;
     return encode_rows(out, io.out + io.out_off, R, chunks, osets, io.out_stride * 8, IBO);
+}
+
+bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* in, CUtensorMap* out)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || io.nsys < 1 || io.nsys > INT32_MAX || M_in < 1 || M_out < 1) return false;
+    if (io.in != io.out || io.in_off != io.out_off || io.in_stride != io.out_stride) return false;
+    const double* base = io.in + io.in_off;
+    const int64_t stride = io.in_stride * 8;
+    if (reinterpret_cast<uintptr_t>(base) % 16 || stride % 16 || io.in_stride < std::max(M_in, M_out)) return false;
+    const cuuint64_t strides[1] = {(cuuint64_t)stride};
+    const cuuint32_t box[2] = {8u, 32u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const cuuint64_t din[2] = {(cuuint64_t)M_in, (cuuint64_t)io.nsys};
+    const cuuint64_t dout[2] = {(cuuint64_t)M_out, (cuuint64_t)io.nsys};
+    return fn(in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), din, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+           fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dout, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out)

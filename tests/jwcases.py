@@ -43,18 +43,21 @@ def run_app(case: O.Case, buffer: np.ndarray, out: np.ndarray, **extra):
 def run_steps(case: O.Case, K: int, bufs, out: np.ndarray, **extra):
     """K consecutive steps in one app: ``bufs`` is one band buffer read by every
     step or a list of K per-step buffers (useMultipleInputBuffers = K).
-    Returns (output buffer after the launch, the plan's shape)."""
+    Returns (output buffer after the launch, the plan's shape with the number
+    of TMA-staged launches it made under "tma_launches")."""
     import torch
 
-    from pfsolve_b200.api import App
+    from pfsolve_b200.api import App, streaming_launch_count
     bl = bufs if isinstance(bufs, (list, tuple)) else [bufs]
     tbs = [torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).cuda() for b in bl]
     to = torch.from_numpy(np.array(out, dtype=np.float64, copy=True)).cuda()
     app = App(buffer=tbs, outputBuffer=to, numConsecutiveJWIterations=K,
               useMultipleInputBuffers=len(tbs) if len(tbs) > 1 else 0, **case_fields(case, **extra))
     shape = app.shape()
+    n0 = streaming_launch_count()
     app.append(**launch_fields(case))
     torch.cuda.synchronize()
+    shape["tma_launches"] = streaming_launch_count() - n0
     res = to.cpu().numpy()
     app.close()
     return res, shape

@@ -27,7 +27,7 @@ def _errs(x, ref, case, Mrows):
 
 def _case(rng, M, B, ub, jwt, K, **kw):
     bands = WL.steps_bands(rng, M, ub, K)
-    kw.setdefault("cfg_outputBufferStride", M + K + 1)
+    kw.setdefault("cfg_outputBufferStride", (M + K + 2) // 2 * 2)  # even: 16-byte-aligned rows
     case = O.Case(M=M, batch=B, upperBanded=ub, jw_type=jwt, **kw)
     rhs = rng.uniform(-1, 1, case.rhs_len() + K + 2)
     return case, bands, rhs
@@ -42,17 +42,21 @@ KINDS = [(1, 10), (1, 11), (1, 12), (0, 10), (0, 11), (0, 12)]
 def test_steps_modes_sizes(ub, jwt, K, M):
     rng = np.random.default_rng(20000 + 100 * ub + jwt + 7 * K + M)
     case, bands, rhs = _case(rng, M, 37, ub, jwt, K)
-    try:
-        x, shape = J.run_steps(case, K, bands, rhs)
-    except capi.PfSolveError as e:
-        # the step tables of long systems may not fit shared memory
-        assert e.code == capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION and M * K > 8000, (M, K)
-        return
-    assert shape["streaming"] == 3
     ref = O.jw_steps(case, K, bands, rhs)
-    assert _errs(x, ref, case, M + K) <= TOL
-    # rows beyond the system slots are untouched
-    assert np.array_equal(x[case.rhs_len() + K:], rhs[case.rhs_len() + K:])
+    for path in (0, 1):  # one system per lane (TMA sweep) / the K-step kernel
+        try:
+            x, shape = J.run_steps(case, K, bands, rhs, kernelPath=path)
+        except capi.PfSolveError as e:
+            # the step tables of long systems may not fit shared memory
+            assert e.code == capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION and M * K > 8000, (M, K, path)
+            continue
+        if path == 0 and shape["streaming"] == 4:
+            assert shape["tma_launches"] == 1
+        else:
+            assert shape["streaming"] == 3 and shape["tma_launches"] == 0
+        assert _errs(x, ref, case, M + K) <= TOL, path
+        # rows beyond the system slots are untouched
+        assert np.array_equal(x[case.rhs_len() + K:], rhs[case.rhs_len() + K:])
 
 
 @pytest.mark.parametrize("M", [100, 1024, 2047])
@@ -69,14 +73,14 @@ def test_steps_long_system_two_steps():
     for ub, jwt in [(1, 10), (0, 10), (2, 13)]:
         M = 4096 if ub else 4095
         case, bands, rhs = _case(rng, M, 9, ub, jwt, 2)
-        x, shape = J.run_steps(case, 2, bands, rhs)
+        x, shape = J.run_steps(case, 2, bands, rhs, kernelPath=1)
         assert shape["streaming"] == 3 and shape["rowsPerThread"] == 16
         assert _errs(x, O.jw_steps(case, 2, bands, rhs), case, M + 1) <= TOL
 
 
 def test_steps_one_buffer_and_windows_and_offsets():
     rng = np.random.default_rng(22000)
-    M, K = 300, 3
+    M, K = 300, 3  # odd offsets: the K-step kernel; even ones: the sweep kernel
     bm = (capi.RUNTIME_OFFSETSOLUTION | capi.RUNTIME_INPUTZEROPAD | capi.RUNTIME_OUTPUTZEROPAD |
           capi.RUNTIME_SCALEC | capi.RUNTIME_OUTPUTBUFFERSTRIDE)
     for ub in (0, 1):
@@ -94,10 +98,26 @@ def test_steps_one_buffer_and_windows_and_offsets():
 
 def test_steps_many_systems():
     rng = np.random.default_rng(23000)
-    for B in (1, 2, 1001, 20000):
-        case, bands, rhs = _case(rng, 512, B, 1, 10, 4)
-        x, _ = J.run_steps(case, 4, bands, rhs)
-        assert _errs(x, O.jw_steps(case, 4, bands, rhs, nthreads=8), case, 512) <= TOL
+    for ub in (0, 1):
+        for B in (1, 2, 33, 1001, 20000):
+            case, bands, rhs = _case(rng, 512, B, ub, 10, 4)
+            x, shape = J.run_steps(case, 4, bands, rhs)
+            assert shape["tma_launches"] == 1
+            assert _errs(x, O.jw_steps(case, 4, bands, rhs, nthreads=8), case, 512 + 3) <= TOL
+
+
+def test_steps_sweep_sizes_and_ks():
+    """Every K up to 8 and sizes around the 8-row boxes, both sweep directions."""
+    rng = np.random.default_rng(23500)
+    for ub in (0, 1):
+        for K in range(2, 9):
+            for M in (9, 15, 16, 17, 63, 257):
+                if M - K + 1 < 1:
+                    continue
+                case, bands, rhs = _case(rng, M, 70, ub, 10, K)
+                x, shape = J.run_steps(case, K, bands, rhs)
+                assert shape["tma_launches"] == 1, (ub, K, M)
+                assert _errs(x, O.jw_steps(case, K, bands, rhs), case, M + K) <= TOL, (ub, K, M)
 
 
 def test_steps_rejected_combinations():
