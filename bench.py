@@ -296,8 +296,9 @@ def extras_arm(args):
     """Other parts of the metric, measured on the same GPU: config 3 (N=512,
     131072 real RHS, weakly dominant) in FP64 and in mixed precision (FP32
     solve + 2 FP64 refinement sweeps) with the mixed result's error against
-    FP64, and config 4 (one spectral timestep, l = 0..511, one persistent
-    launch, captured CUDA graph, autotuned shape)."""
+    FP64, config 4 (one spectral timestep, l = 0..511, one persistent
+    launch, captured CUDA graph, autotuned shape), K = 2 and 4 consecutive
+    steps in one launch, and the config 5 serving loop."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -364,6 +365,10 @@ def extras_arm(args):
                                   "graph": True, "launches_per_step": 1}
     batch.close()
     del inp, outb, keep
+    torch.cuda.empty_cache()
+    # K consecutive steps in one launch (numConsecutiveJWIterations)
+    for K in (2, 4):
+        out[f"ksteps_K{K}_ub1_t10_N512_B131072"] = ksteps_measure(512, 131072, K, steps=10, warmup=3)
     torch.cuda.empty_cache()
     out["config5_serving"] = serving_leg()
     return out
@@ -452,38 +457,46 @@ def config3_profile(args):
     app.close()
 
 
-def steps_profile(args):
-    """Profiling case: K consecutive JW steps in one launch (upperBanded 1,
-    jw_type 10: bidiagonal matvec + lower bidiagonal solve per step; per-step
-    band buffers), N = --m rows, --ncplx systems, --ksteps K; K = 1 runs the
-    single-step kernel on the same operator.  Prints one JSON line."""
+def ksteps_measure(M, B, K, steps=20, warmup=5, rows=0, path=0):
+    """K consecutive JW steps in one launch (upperBanded 1, jw_type 10:
+    bidiagonal matvec + lower bidiagonal solve per step, per-step band
+    buffers), N = M rows, B systems (inputs > L2, no flush); K = 1 runs the
+    single-step kernel on the same operator.  Algorithmic bytes: M rows read
+    and M - K + 1 written per system."""
     import torch
 
     from pfsolve_b200 import workloads as WL
     from pfsolve_b200.api import App
-    M, B, K = args.m, args.ncplx, args.ksteps
     rng = np.random.default_rng(5)
     bands = WL.steps_bands(rng, M, 1, max(K, 2))[:max(K, 1)]
     tbs = [torch.from_numpy(b).cuda() for b in bands]
     x = torch.from_numpy(rng.uniform(-1, 1, M * B)).cuda()
     extra = dict(numConsecutiveJWIterations=K, useMultipleInputBuffers=K) if K > 1 else {}
     app = App(buffer=tbs if K > 1 else tbs[0], outputBuffer=x, M_size=M, size=(M, B), upperBanded=1, jw_type=10,
-              doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows, **extra)
-    for _ in range(max(1, args.warmup)):
+              doublePrecision=1, scaleC=1.0, rowsPerThread=rows, kernelPath=path, **extra)
+    for _ in range(max(1, warmup)):
         app.append()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         app.append()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    mout = M - K + 1
-    print(json.dumps({"profile_case": "ksteps", "M": M, "rhs": B, "K": K, "ms_per_step": ms,
-                      "gbs": (M + mout) * 8 * B / (ms * 1e-3) / 1e9, "rhs_per_s": B / (ms * 1e-3),
-                      "kernel": app.shape()}), flush=True)
+    ms = e0.elapsed_time(e1) / steps
+    shape = app.shape()
     app.close()
+    del x, tbs
+    mout = M - K + 1
+    return {"M": M, "rhs": B, "K": K, "ms": ms, "rhs_per_s": B / (ms * 1e-3),
+            "gbs": (M + mout) * 8 * B / (ms * 1e-3) / 1e9, "kernel": shape}
+
+
+def steps_profile(args):
+    """Profiling case: K steps in one launch (--m rows, --ncplx systems,
+    --ksteps K, --path 1 for the K-step partition kernel).  Prints one JSON line."""
+    r = ksteps_measure(args.m, args.ncplx, args.ksteps, args.steps, args.warmup, args.rows, args.path)
+    print(json.dumps(dict(profile_case="ksteps", ms_per_step=r.pop("ms"), **r)), flush=True)
 
 
 def config4_profile(args):
