@@ -318,6 +318,96 @@ int pfo_jw_step_d(const pfo_params* p, const double* bands, double* rhs, int nth
 }
 
 /* ------------------------------------------------------------------------- */
+/* ALT stride-2 mode (jw_type / 100 % 10 == 1, pfSolve_Plan_JonesWorland.h:265).
+ * The kernel's lanes split in two halves (pfSolve_TridiagonalSolve.h:1319-1330
+ * read, :1475-1486 write, :1622-1644 solve): lane t < T/2 holds the even rows
+ * 2 (t R + i), lane t >= T/2 the odd rows 2 ((t - T/2) R + i) + 1, i < R, with
+ * T lanes and R = ceil(M / T) rows per lane as for any JW plan.  The matvec
+ * couples register i with i + 1 (rows r and r + 2) and each half solves its
+ * own parity, so rows of one parity form an independent system with
+ * neighbours r -+ 2.  Band entries of every register are loaded with all
+ * lanes active (pfSolve_ReadWrite.h:1637-1645, 1705-1711): the entry of row r
+ * sits at position i T + t, and the bands are R T entries apart instead of M
+ * (pfSolve_JonesWorland.h:209-222, 262-271).  scaleC multiplies row 0 only
+ * (lane 0 after the halves are merged again, :1901-1927). */
+static void alt_geometry(int64_t M, int64_t* T, int64_t* R)
+{
+    int64_t warp = 64 * ((M + 1023) / 1024);
+    if (M < 512) warp = 32;
+    if (warp < 32) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    *T = warp;
+    *R = (M + warp - 1) / warp;
+}
+
+int64_t pfo_alt_position(int64_t r, int64_t M)
+{
+    int64_t T, R;
+    alt_geometry(M, &T, &R);
+    const int64_t h = r & 1, e = r >> 1;
+    const int64_t t = h * (T / 2) + e / R, i = e % R;
+    return i * T + t;
+}
+
+int pfo_jw_step_alt_q(const pfo_params* p, const double* bands, double* rhs, int nthreads)
+{
+    if (((p->jw_type / 100) % 10) != 1) return -1;
+    if (p->bitmask & (PFO_RUNTIME_OFFSETM | PFO_RUNTIME_OFFSETV)) return -1;
+    int64_t T, R;
+    alt_geometry(p->M, &T, &R);
+    pfo_params q = *p;
+    q.M = R * T;  /* band offsets: multiples of R T */
+    jw_layout L;
+    if (jw_resolve(&q, &L)) return -1;
+    rhs_layout RL;
+    rhs_resolve(p, &RL);
+    const int64_t M = p->M;
+    q_t* co = (q_t*)calloc((size_t)(4 * (M + 2)), sizeof(q_t));
+    if (!co) return -1;
+    q_t *md = co, *mo = co + (M + 2), *sl = co + 2 * (M + 2), *su = co + 3 * (M + 2);
+    for (int64_t r = 0; r < M; r++) {
+        const int64_t k = pfo_alt_position(r, M);
+        if (L.mv != PFO_MV_NONE) md[r] = (q_t)bands[L.off_md + k];
+        if (L.mv == PFO_MV_UPPER || L.mv == PFO_MV_LOWER) mo[r] = (q_t)bands[L.off_mo + k];
+        if (L.sv == PFO_SV_LOWER || L.sv == PFO_SV_TRI) sl[r] = (q_t)bands[L.off_sl + k];
+        if (L.sv == PFO_SV_UPPER || L.sv == PFO_SV_TRI) su[r] = (q_t)bands[L.off_su + k];
+    }
+    const q_t sC = (q_t)RL.scaleC;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+    {
+        const int64_t Mh = (M + 1) / 2 + 1;
+        q_t* b = (q_t*)malloc(sizeof(q_t) * (size_t)Mh);
+        q_t* g = (q_t*)malloc(sizeof(q_t) * (size_t)Mh);
+        q_t* w = (q_t*)malloc(sizeof(q_t) * (size_t)Mh);
+        q_t* c4 = (q_t*)malloc(sizeof(q_t) * (size_t)(4 * Mh));
+#pragma omp for schedule(static)
+        for (int64_t y = 0; y < p->batch; y++) {
+            const int64_t base = RL.offS + y * RL.oStride;
+            for (int h = 0; h < 2; h++) {
+                const int64_t n = (M - h + 1) / 2;  /* rows of this parity */
+                if (n <= 0) continue;
+                for (int64_t e = 0; e < n; e++) {
+                    const int64_t r = 2 * e + h;
+                    b[e] = keep(r, RL.iz0, RL.iz1, RL.rtIZ) ? (q_t)rhs[base + r] : (q_t)0;
+                    c4[e] = md[r];
+                    c4[Mh + e] = mo[r];
+                    c4[2 * Mh + e] = sl[r];
+                    c4[3 * Mh + e] = su[r];
+                }
+                system_q(L.mv, L.sv, n, c4, c4 + Mh, c4 + 2 * Mh, c4 + 3 * Mh, h == 0 ? sC : (q_t)1, b, g, w);
+                for (int64_t e = 0; e < n; e++) {
+                    const int64_t r = 2 * e + h;
+                    if (keep(r, RL.oz0, RL.oz1, RL.rtOZ)) rhs[base + r] = (double)g[e];
+                }
+            }
+        }
+        free(b); free(g); free(w); free(c4);
+    }
+    free(co);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* K consecutive JW steps in one kernel (numConsecutiveJWIterations = K > 1;
  * pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:108-374).
  *

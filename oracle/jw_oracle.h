@@ -93,6 +93,13 @@ int pfo_jw_step_q_f32(const pfo_params* p, const float* bands, float* rhs, int n
  * __float128 and rounded back to {hi, lo}. */
 int pfo_jw_step_q_dd(const pfo_params* p, const double* bands_dd, double* rhs_dd, int nthreads);
 
+/* ALT stride-2 mode (jw_type / 100 % 10 == 1), K = 1, FP64: the even and the
+ * odd rows form two independent systems with neighbours r -+ 2; bands in the
+ * ALT register layout (pfo_alt_position), R T entries apart.  Returns -1 for
+ * launch-time band offsets (the reference rescales only plan-time ones). */
+int64_t pfo_alt_position(int64_t r, int64_t M);
+int pfo_jw_step_alt_q(const pfo_params* p, const double* bands, double* rhs, int nthreads);
+
 /* K consecutive JW steps (numConsecutiveJWIterations = K, 2 <= K <= 8) on
  * real FP64 systems, in __float128 ("q") or double ("d").  `bands` holds
  * `nbuf` buffer pointers: one per step (nbuf >= K, the reference's

@@ -186,6 +186,10 @@ def lib():
         fn = getattr(L, name)
         fn.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(dp), dp, ctypes.c_int]
         fn.restype = ctypes.c_int
+    L.pfo_alt_position.argtypes = [ctypes.c_int64, ctypes.c_int64]
+    L.pfo_alt_position.restype = ctypes.c_int64
+    L.pfo_jw_step_alt_q.argtypes = [P, dp, dp, ctypes.c_int]
+    L.pfo_jw_step_alt_q.restype = ctypes.c_int
     L.pfo_steps_registers.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int]
     L.pfo_steps_registers.restype = ctypes.c_int64
     L.pfo_jw_steps_layout.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Step)]
@@ -249,6 +253,21 @@ def jw_step(case: Case, bands: np.ndarray, rhs: np.ndarray, mode: str = "q", nth
         fn = {"q": L.pfo_jw_step_q, "d": L.pfo_jw_step_d, "dd": L.pfo_jw_step_q_dd}[mode]
         rc = fn(ctypes.byref(p), _dptr(b), _dptr(out), nthreads)
     if rc:
+        raise ValueError("combination not defined by the reference")
+    return out
+
+
+def alt_positions(M):
+    """Storage position of row r in the ALT band layout (stride-2 mode)."""
+    L = lib()
+    return np.array([L.pfo_alt_position(r, M) for r in range(M)], dtype=np.int64)
+
+
+def jw_step_alt(case: Case, bands: np.ndarray, rhs: np.ndarray, nthreads: int = 1) -> np.ndarray:
+    """One ALT-mode JW step (jw_type / 100 % 10 == 1) on a copy of ``rhs``."""
+    b = np.ascontiguousarray(bands, dtype=np.float64)
+    out = np.array(rhs, dtype=np.float64, copy=True)
+    if lib().pfo_jw_step_alt_q(ctypes.byref(case.to_c()), _dptr(b), _dptr(out), nthreads):
         raise ValueError("combination not defined by the reference")
     return out
 

@@ -53,6 +53,11 @@ struct AppState {
     int cluster_max = 0;
     int R_req = 0;           // caller's rows per thread (0: choose)
     bool no_stream = false;  // kernelPath 1
+    bool no_tbl = false;     // register-coefficient variants only
+    // ALT stride-2 mode: even and odd rows solved as two systems on the group
+    // kernel (lanes x rows of the reference's ALT band layout)
+    bool alt = false;
+    int64_t alt_T = 0, alt_R = 0;
     // K consecutive steps (numConsecutiveJWIterations > 1): one kernel
     int K = 1;
     const StepsVariant* steps_v = nullptr;
@@ -272,6 +277,46 @@ PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
     return s->seq_v ? PFSOLVE_SUCCESS : PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
 }
 
+PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE);
+
+// ALT stride-2 mode (jw_type / 100 % 10 == 1, pfSolve_Plan_JonesWorland.h:265):
+// the even and the odd rows of a system are two independent systems with
+// neighbours r -+ 2 (the reference's lanes split in two halves,
+// pfSolve_TridiagonalSolve.h:1319-1330, 1622-1644), bands in its ALT register
+// layout R T entries apart (pfSolve_JonesWorland.h:209-222, 262-271,
+// pfSolve_ReadWrite.h:1705-1711).  K = 1; plan-time band offsets only (the
+// reference rescales only those); FP64 or FP32 solve + FP64 refinement.
+PfSolveResult plan_alt(AppState* s, const PfSolveConfiguration& c, int dd_prec)
+{
+    if (c.numConsecutiveJWIterations > 1 || dd_prec) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (c.jw_control_bitmask & (RUNTIME_OFFSETM | RUNTIME_OFFSETV)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (c.upperBanded < 0 || c.upperBanded > 2) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const int64_t M = c.M_size;
+    if (M < 2 || (M + 1) / 2 > kMaxRows) return PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
+    JwLayout L;
+    if (!jw_layout(c, false, false, 0, 0, L)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    int64_t warp = 64 * ((M + 1023) / 1024);
+    if (M < 512) warp = 32;
+    if (warp % 32) warp = 32 * ((warp + 31) / 32);
+    s->alt = true;
+    s->alt_T = warp;
+    s->alt_R = (M + warp - 1) / warp;
+    s->mvj = L.mvj;
+    s->sv = L.sv;
+    s->prec = (c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? 1 : 0;
+    s->refine_sweeps = 1 + c.mixedPrecisionRefinement;
+    s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
+    s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
+    const int64_t n0 = (M + 1) / 2;  // rows of the even system
+    s->R = pick_rows_per_thread(n0, c.rowsPerThread);
+    s->R_fixed = c.rowsPerThread != 0 && c.rowsPerThread != 32;
+    s->R_req = c.rowsPerThread;
+    s->no_stream = true;  // group kernel: per-group parity, stride-2 rows
+    s->no_tbl = true;     // the two parities have different coefficients
+    const PfSolveResult r = finish_variant(s, n0, LAY_REAL, LAY_REAL, 0);
+    return (r == PFSOLVE_SUCCESS && !s->variant) ? PFSOLVE_ERROR_UNSUPPORTED_COMBINATION : r;
+}
+
 // Pick the kernel variant and launch shape for M rows: register variants
 // first, then coefficient-table variants (FP64); rows per thread from the
 // caller's choice (s->R) first, then the other compiled choices.
@@ -281,7 +326,7 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
     // The caller's rows per thread first; when the group kernel has no such
     // variant (the choice is then the streaming kernel's), any other.
     for (int pass = 0; pass < 2; ++pass)
-    for (int tbl = 0; tbl <= (s->prec == 0 ? 1 : 0); ++tbl) {
+    for (int tbl = 0; tbl <= (s->prec == 0 && !s->no_tbl ? 1 : 0); ++tbl) {
         for (int oi = 0; oi < 4; ++oi) {
             const int R = order[oi];
             if (oi > 0 && (R == s->R || (s->R_fixed && pass == 0))) continue;
@@ -459,7 +504,9 @@ PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& i
     }
     if (!s->variant) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // streaming-only plan
     const int64_t want = (io.nsys + s->G - 1) / s->G;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->max_blocks));
+    int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->max_blocks));
+    // ALT: a group keeps one parity, so the system step (grid x groups) is even
+    if (io.alt && (grid * s->G) % 2) grid = grid > 1 ? grid - 1 : 2;
     const size_t smem = s->variant->smem_bytes(s->W, s->G);
     s->variant->launch(dim3((unsigned)grid), dim3(32 * s->W * s->G), smem, stream, op, io, s->W);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -584,8 +631,14 @@ PfSolveResult append_jw(PfSolveApplication* app, const PfSolveLaunchParams* lp, 
     if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
     if (s->K > 1) return append_steps(app, lp, r, stream);
     JwLayout L;
-    jw_layout(c, (c.jw_control_bitmask & RUNTIME_OFFSETM) != 0, (c.jw_control_bitmask & RUNTIME_OFFSETV) != 0,
-              r.offM, r.offV, L);
+    if (s->alt) {
+        PfSolveConfiguration ca = c;  // ALT: bands R T entries apart
+        ca.M_size = s->alt_R * s->alt_T;
+        jw_layout(ca, false, false, 0, 0, L);
+    } else {
+        jw_layout(c, (c.jw_control_bitmask & RUNTIME_OFFSETM) != 0, (c.jw_control_bitmask & RUNTIME_OFFSETV) != 0,
+                  r.offM, r.offV, L);
+    }
     JwOperator op;
     fill_operator_common(s, c, op);
     op.bands = static_cast<const double*>(r.bands);
@@ -604,6 +657,13 @@ PfSolveResult append_jw(PfSolveApplication* app, const PfSolveLaunchParams* lp, 
     io.iz0 = r.iz0; io.iz1 = r.iz1; io.oz0 = r.oz0; io.oz1 = r.oz1;
     io.nsys = r.batch;
     io.M = c.M_size;
+    if (s->alt) {
+        op.alt = 1;
+        op.alt_T = s->alt_T;
+        op.alt_R = s->alt_R;
+        io.alt = 1;
+        io.nsys = 2 * r.batch;  // system 2y + h: the parity-h rows of right-hand side y
+    }
     return launch_jw_variant(s, op, io, stream);
 }
 
@@ -798,7 +858,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
         s->kind = APP_JW;
         if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
-        else if (((c.jw_type / 100) % 10) == 1) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // ALT mode
+        else if (((c.jw_type / 100) % 10) == 1) r = plan_alt(s, c, dd_prec);
         else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (c.numConsecutiveJWIterations > 1) {
             s->prec = dd_prec;
@@ -1061,7 +1121,8 @@ extern "C" PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveLa
     if (i < n && st(apps[i])->kind == APP_BLOCK) { bl = apps[i]; blp = lps ? lps[i] : nullptr; i++; }
     if (i != n) pattern = false;
     PfSolveResult r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-    if (pattern && (dg || bl)) {
+    const bool fusable = pattern && !st(jw)->alt && st(jw)->K == 1;  // ALT and K-step plans run alone
+    if (fusable && (dg || bl)) {
         cudaStream_t stream = pick_stream(jw);
         r = append_chain_fused(dg, dlp, jw, jlp, bl, blp, stream);
         if (r == PFSOLVE_SUCCESS) record_stream_event(jw, stream);

@@ -94,6 +94,7 @@ __host__ size_t jw_smem_bytes(int W, int G)
 // perm_piece rows (the whole system when perm_piece == 0).
 __device__ __forceinline__ int64_t band_pos(const JwOperator& op, int64_t i)
 {
+    if (op.alt) return (i % op.alt_R) * op.alt_T + op.alt_h * (op.alt_T >> 1) + i / op.alt_R;
     if (!op.perm) return i;
     int64_t base = 0, li = i, m = op.perm_m, ce = op.perm_ceil, fl = op.perm_floor;
     if (op.perm_piece) {
@@ -462,23 +463,27 @@ __device__ __forceinline__ void issue_segment_load(const JwIO& io, int64_t sys, 
     const int64_t M = io.M;
     auto row_ok = [&](int64_t row) { return row >= 0 && row < M && row >= io.iz0 && row < io.iz1; };
     if constexpr (C::kLIN == LAY_REAL) {
-        const double* base = io.in + io.in_off + sys * io.in_stride;
+        // ALT: row e of system sys is row 2 e + (sys & 1) of row set sys / 2
+        const int64_t h = io.alt ? (sys & 1) : 0, es = io.alt ? 2 : 1;
+        const int64_t Msys = io.alt ? (M - h + 1) >> 1 : M;
+        auto ok_at = [&](int64_t e) { return e >= 0 && e < Msys && row_ok(es * e + h); };
+        const double* base = io.in + io.in_off + (io.alt ? sys >> 1 : sys) * io.in_stride + h;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int q = 32 * k + lane;
             const int64_t row = r0 + q;
-            const bool ok = row_ok(row);
-            cp_async8(buf + swz<R, false>(q), ok ? base + row : io.in, ok);
+            const bool ok = ok_at(row);
+            cp_async8(buf + swz<R, false>(q), ok ? base + es * row : io.in, ok);
         }
         if (KL > 0 && lane < KL) {
             const int64_t row = r0 - KL + lane;
-            const bool ok = row_ok(row);
-            cp_async8(buf + 32 * R + lane, ok ? base + row : io.in, ok);
+            const bool ok = ok_at(row);
+            cp_async8(buf + 32 * R + lane, ok ? base + es * row : io.in, ok);
         }
         if (KU > 0 && lane < KU) {
             const int64_t row = r0 + 32 * R + lane;
-            const bool ok = row_ok(row);
-            cp_async8(buf + 32 * R + KL + lane, ok ? base + row : io.in, ok);
+            const bool ok = ok_at(row);
+            cp_async8(buf + 32 * R + KL + lane, ok ? base + es * row : io.in, ok);
         }
     } else {  // XXII complex: real part row block 2*sys, imaginary 2*sys+1
         const double* re = io.in + io.in_off + (2 * sys) * io.in_stride;
@@ -505,14 +510,16 @@ __device__ __forceinline__ void store_segment(const JwIO& io, int64_t sys, int64
 {
     constexpr int R = C::kR;
     const int64_t M = io.M;
+    const int64_t h = io.alt ? (sys & 1) : 0, es = io.alt ? 2 : 1;
+    const int64_t Msys = io.alt ? (M - h + 1) >> 1 : M;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int q = 32 * k + lane;
         const int64_t row = r0 + q;
-        if (row >= M || row < io.oz0 || row >= io.oz1) continue;
+        if (row >= Msys || es * row + h < io.oz0 || es * row + h >= io.oz1) continue;
         if constexpr (C::kLOUT == LAY_REAL) {
             double v = buf[swz<R, false>(q)];
-            double* p = io.out + io.out_off + sys * io.out_stride + row;
+            double* p = io.out + io.out_off + (io.alt ? sys >> 1 : sys) * io.out_stride + es * row + h;
             if (io.accumulate) v += *p;
             *p = v;
         } else if constexpr (C::kLOUT == LAY_PACKED) {
@@ -719,17 +726,25 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_step_kernel(const JwOperato
     cf.tbl = table;
     cf.T = 32 * W;
     cf.tt = g.wg * 32 + g.lane;
-    if constexpr (C::kTbl) {
-        // every group of the CTA solves with the same matrix: group 0 builds
-        // the shared table once
-        if (grp == 0) jw_prologue<C>(op, g, s, cf, table);
-        __syncthreads();
-    } else {
-        jw_prologue<C>(op, g, s, cf);
-    }
     const int64_t sys0 = (int64_t)blockIdx.x * G + grp;
     const int64_t step = (int64_t)gridDim.x * G;
-    jw_run_systems<C>(op, io, g, cf, buf0, buf1, sys0, step);
+    // ALT: this group's systems all have the parity of sys0 (the launch makes
+    // the system step even); the odd rows' system has no scaleC row
+    JwOperator opg = op;
+    if (op.alt) {
+        opg.alt_h = (int)(sys0 & 1);
+        opg.M = (op.M - opg.alt_h + 1) >> 1;
+        if (opg.alt_h) opg.scaleC = 1.0;
+    }
+    if constexpr (C::kTbl) {
+        // every group of the CTA solves with the same matrix: group 0 builds
+        // the shared table once (not used in ALT mode)
+        if (grp == 0) jw_prologue<C>(opg, g, s, cf, table);
+        __syncthreads();
+    } else {
+        jw_prologue<C>(opg, g, s, cf);
+    }
+    jw_run_systems<C>(opg, io, g, cf, buf0, buf1, sys0, step);
 }
 
 // ---- Uneven batch: one persistent launch over many matrices of different

@@ -30,6 +30,11 @@ struct JwOperator {
     double scaleC;  // multiplies solution row 0 when a solve runs
     int64_t M;
     int refine_sweeps;  // mixed precision: FP32 solves in total (1 + refinements)
+    // ALT stride-2 mode: the rows of parity alt_h form the system (M counts
+    // the full rows); bands in the ALT register layout of alt_T lanes x alt_R
+    // rows (entry of row r = 2 e + h at (e % alt_R) alt_T + h alt_T/2 + e / alt_R)
+    int alt, alt_h;
+    int64_t alt_T, alt_R;
 };
 
 // The data side: systems, layouts, keep-windows.
@@ -43,6 +48,7 @@ struct JwIO {
     int64_t nsys;                 // systems (real, or complex pairs)
     int64_t M;
     int accumulate;               // output += result
+    int alt;                      // ALT mode: system 2y + h is the parity-h rows of row set y
 };
 
 // K consecutive steps in one kernel (numConsecutiveJWIterations = K).

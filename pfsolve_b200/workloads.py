@@ -123,6 +123,60 @@ def steps_bands(rng, M: int, upperBanded: int, K: int, per_step: bool = True):
     return buf
 
 
+def alt_positions(M: int) -> np.ndarray:
+    """pos[r] = storage position of row r in the ALT (stride-2) band layout:
+    T lanes and R = ceil(M / T) rows per lane as for any JW plan; lane t < T/2
+    holds the even rows 2 (t R + i), lane t >= T/2 the odd rows
+    2 ((t - T/2) R + i) + 1, and the entry of register i of lane t sits at
+    i T + t (pfSolve_TridiagonalSolve.h:1319-1330, pfSolve_ReadWrite.h:1705-1711)."""
+    warp = 64 * ((M + 1023) // 1024)
+    if M < 512:
+        warp = 32
+    warp = max(warp, 32)
+    if warp % 32:
+        warp = 32 * ((warp + 31) // 32)
+    R = (M + warp - 1) // warp
+    r = np.arange(M, dtype=np.int64)
+    h, e = r & 1, r >> 1
+    t = h * (warp // 2) + e // R
+    return (e % R) * warp + t
+
+
+def alt_band_span(M: int) -> int:
+    """Entries between consecutive ALT bands (R T, the lanes' register capacity)."""
+    warp = 64 * ((M + 1023) // 1024)
+    if M < 512:
+        warp = 32
+    warp = max(warp, 32)
+    return ((M + warp - 1) // warp) * warp
+
+
+def alt_bands(rng, M: int, upperBanded: int) -> np.ndarray:
+    """Three ALT-layout bands of R T entries each.  Natural rows: upperBanded 2
+    a normalised tridiagonal per parity (ld | md | ud, couplings r -+ 2);
+    otherwise U(-1/2, 1/2).  Couplings that leave a parity's rows (lower bands
+    at rows 0, 1; upper bands at the last two rows) and the padding are zero."""
+    span = alt_band_span(M)
+    pos = alt_positions(M)
+    lower = np.arange(M) < 2
+    upper = np.arange(M) >= M - 2
+    if upperBanded == 2:
+        a = rng.uniform(-1, 1, M)
+        c = rng.uniform(-1, 1, M)
+        a[lower] = 0.0
+        c[upper] = 0.0
+        d = np.abs(a) + np.abs(c) + rng.uniform(1, 2, M)
+        nat = [a / d, 1.0 / d, c / d]
+    else:
+        nat = [rng.uniform(-0.5, 0.5, M) for _ in range(3)]
+        for k in range(3):  # each band is a lower or an upper coupling in some jw_type
+            nat[k][lower | upper] = 0.0
+    out = np.zeros(3 * span)
+    for k in range(3):
+        out[k * span + pos] = nat[k]
+    return out
+
+
 def tridiagonal(rng, M, dominance=None):
     """(a, d, c): a_0 = c_{M-1} = 0.  d = |a|+|c|+U(1,2), or dominance*(|a|+|c|)."""
     a = rng.uniform(-1.0, 1.0, M)

@@ -181,6 +181,31 @@ def steps_offset_cases():
     return out
 
 
+def alt_cases():
+    """(name, Case, bands, rhs, precision) for the ALT stride-2 mode
+    (jw_type / 100 % 10 == 1), stored under tests/golden/alt/."""
+    out = []
+    for ub, jwt in [(2, 113), (1, 110), (1, 111), (1, 112), (1, 113), (0, 110), (0, 111), (0, 112), (0, 113)]:
+        for M in ([20, 33, 100, 256, 511, 512, 1000, 2048] if jwt == 113 or jwt == 110 else [33, 300]):
+            rng = np.random.default_rng(13000 + 1000 * ub + jwt + M)
+            bands = WL.alt_bands(rng, M, ub)
+            case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=jwt)
+            rhs = rng.uniform(-1, 1, case.rhs_len())
+            out.append((f"alt_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
+    # launch-time windows, scaleC, stride and solution offset
+    M = 200
+    bm = (RT.RUNTIME_OFFSETSOLUTION | RT.RUNTIME_INPUTZEROPAD | RT.RUNTIME_OUTPUTZEROPAD | RT.RUNTIME_SCALEC |
+          RT.RUNTIME_OUTPUTBUFFERSTRIDE)
+    for ub, jwt in [(2, 113), (1, 110), (0, 110)]:
+        rng = np.random.default_rng(13500 + ub)
+        case = O.Case(M=M, batch=4, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetSolution=6,
+                      run_inputZeropad=(3, 190), run_outputZeropad=(5, 180), run_scaleC=0.625,
+                      run_outputBufferStride=M + 16)
+        out.append((f"alt_runtime_ub{ub}_t{jwt}", case, WL.alt_bands(rng, M, ub),
+                    rng.uniform(-1, 1, case.rhs_len() + 8), "f64"))
+    return out
+
+
 REF_BIN_FP128 = os.path.join(ROOT, "oracle", "_ref", "pfsolve_ref_fp128")
 
 
@@ -206,8 +231,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--time", action="store_true")
-    ap.add_argument("--only", default="all", choices=["all", "steps"],
-                    help="steps: only the K-step fixtures (and K-step timing with --time)")
+    ap.add_argument("--only", default="all", choices=["all", "steps", "alt"],
+                    help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
@@ -247,9 +272,20 @@ def main():
         with open(os.path.join(args.out, "ref_timing.json"), "w") as f:
             json.dump(timing, f, indent=1)
         print(json.dumps(timing, indent=1))
+    adir = os.path.join(args.out, "alt")
+    os.makedirs(adir, exist_ok=True)
+    for name, case, buf, rhs, prec in (alt_cases() if args.only in ("all", "alt") else []):
+        try:
+            ref = run_case(tmp, name, case, buf, rhs, prec)
+            np.savez_compressed(os.path.join(adir, name + ".npz"), params=json.dumps(asdict(case)),
+                                precision=prec, buffer=buf, rhs=rhs, ref_out=ref)
+            summary[name] = "ok"
+        except Exception as e:
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
     sdir = os.path.join(args.out, "steps")
     os.makedirs(sdir, exist_ok=True)
-    for name, case, K, bufs, rhs in steps_cases() + steps_offset_cases():
+    for name, case, K, bufs, rhs in (steps_cases() + steps_offset_cases() if args.only in ("all", "steps") else []):
         try:
             d = os.path.join(tmp, name)
             O.write_reference_case(d, case, list(bufs) if len(bufs) > 1 else bufs[0], rhs, K=K)
@@ -262,7 +298,7 @@ def main():
         except Exception as e:
             summary[name] = f"error: {e}"
             traceback.print_exc()
-    if args.time:
+    if args.time and args.only in ("all", "steps"):
         # K consecutive steps in one reference kernel (upperBanded 1, jw_type 10)
         timing = {}
         for K in (1, 2, 4):

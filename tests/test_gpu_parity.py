@@ -120,7 +120,11 @@ def test_unsupported_combinations_return_codes():
     r = torch.zeros(64, dtype=torch.float64, device="cuda")
     for fields, code in [(dict(upperBanded=2, jw_type=10), capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION),
                          (dict(upperBanded=2, jw_type=12), capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION),
-                         (dict(upperBanded=2, jw_type=13, numConsecutiveJWIterations=2),
+                         # K > 2 tridiagonal steps: the reference never reloads the middle steps' diagonal
+                         (dict(upperBanded=2, jw_type=13, numConsecutiveJWIterations=3),
+                          capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION),
+                         # ALT mode with launch-time band offsets
+                         (dict(upperBanded=2, jw_type=113, jw_control_bitmask=capi.RUNTIME_OFFSETM),
                           capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION)]:
         with pytest.raises(capi.PfSolveError) as ei:
             App(buffer=b, outputBuffer=r, M_size=64, size=(64, 1), doublePrecision=1, **fields)
