@@ -573,6 +573,17 @@ DEFINE_STEPS(pfo_jw_steps_d, double)
 /* dgbmv: y_r = sum_j A[offsetM + j*M + c] x_c, c = r + KU - j, 0 <= c < M
  * (pfSolve_MatVecMul.h:389-443).  The plan-time offsetM is honoured here
  * (pfSolve_dgbmv.h:79-87), unlike the JW kernel. */
+/* ALT_dgbmv (pfSolve_Plan_dgbmv.h:100, pfSolve_MatVecMul.h:390): band j is
+ * dropped when (j % 2 == 1 - LDA % 2 and KL != 0) or (j % 2 == LDA % 2 and
+ * KU != 0), KL and KU as configured.  With one side only and KU, or KL odd,
+ * this keeps the couplings at even distance; the rule is restated as written. */
+int pfo_dgbmv_band_dropped(const pfo_params* p, int64_t j)
+{
+    if (!p->ALT_dgbmv) return 0;
+    const int64_t par = p->LDA % 2;
+    return ((j % 2) == 1 - par && p->KL) || ((j % 2) == par && p->KU);
+}
+
 #define DEFINE_DGBMV(NAME, T)                                                              \
     int NAME(const pfo_params* p, const double* A, double* rhs, int nthreads)              \
     {                                                                                      \
@@ -593,7 +604,7 @@ DEFINE_STEPS(pfo_jw_steps_d, double)
                     T acc = 0;                                                             \
                     for (int64_t j = 0; j < p->LDA; j++) {                                 \
                         int64_t c = r + p->KU - j;                                         \
-                        if (c < 0 || c >= M) continue;                                     \
+                        if (c < 0 || c >= M || pfo_dgbmv_band_dropped(p, j)) continue;     \
                         acc += (T)A[offM + j * M + c] * x[c];                              \
                     }                                                                      \
                     if (keep(r, R.oz0, R.oz1, R.rtOZ)) rhs[base + r] = (double)acc;        \

@@ -62,6 +62,7 @@ typedef struct {
     /* block kernel */
     int32_t block, lshift;
     int64_t size0, size1;      /* block kernel extents */
+    int32_t ALT_dgbmv;         /* dgbmv: drop alternate bands (stride-2 couplings) */
 } pfo_params;
 
 /* Operator kinds of one JW step after the band offsets are resolved. */
@@ -120,6 +121,8 @@ int pfo_jw_steps_d(const pfo_params* p, int K, int nbuf, const double* const* ba
 /* General banded matvec y = A x, in place on rhs, A in band-major storage
  * A[offsetM + j*M + c] (pfSolve_KernelsLevel1/pfSolve_MatVecMul.h:383-446,
  * pfSolve_KernelsLevel2/pfSolve_dgbmv.h:38-112). */
+/* 1 when ALT_dgbmv drops band j of a dgbmv application. */
+int pfo_dgbmv_band_dropped(const pfo_params* p, int64_t j);
 int pfo_dgbmv_q(const pfo_params* p, const double* A, double* rhs, int nthreads);
 int pfo_dgbmv_d(const pfo_params* p, const double* A, double* rhs, int nthreads);
 

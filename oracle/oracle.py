@@ -54,6 +54,7 @@ class _Params(ctypes.Structure):
         ("LDA", ctypes.c_int32), ("KU", ctypes.c_int32), ("KL", ctypes.c_int32),
         ("block", ctypes.c_int32), ("lshift", ctypes.c_int32),
         ("size0", ctypes.c_int64), ("size1", ctypes.c_int64),
+        ("ALT_dgbmv", ctypes.c_int32),
     ]
 
 
@@ -101,6 +102,7 @@ class Case:
     lshift: int = 0
     size0: int = 0
     size1: int = 0
+    ALT_dgbmv: int = 0
 
     def __post_init__(self):
         if self.cfg_inputBufferStride == 0:
@@ -379,6 +381,7 @@ def write_reference_case(case_dir: str, case: Case, bands, rhs: np.ndarray, *,
         "run_inputBufferStride": case.run_inputBufferStride,
         "run_outputBufferStride": case.run_outputBufferStride,
         "LDA": case.LDA, "KU": case.KU, "KL": case.KL, "block": case.block, "lshift": case.lshift,
+        "ALT_dgbmv": case.ALT_dgbmv,
         "doublePrecision": 1 if precision in ("f64",) else 0,
         "quadDoubleDoublePrecision": 1 if precision == "dd" else 0,
         "iters": iters,

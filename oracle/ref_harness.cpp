@@ -127,6 +127,7 @@ int main(int argc, char** argv)
     cfg.LDA = (int)I("LDA", 0);
     cfg.KU = (int)I("KU", 0);
     cfg.KL = (int)I("KL", 0);
+    cfg.ALT_dgbmv = (int)I("ALT_dgbmv", 0);
     cfg.block = (int)I("block", 0);
     cfg.lshift = (int)I("lshift", 0);
     cfg.disableCaching = 1;  // no kernel cache files are written or read

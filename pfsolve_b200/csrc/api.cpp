@@ -54,6 +54,7 @@ struct AppState {
     int R_req = 0;           // caller's rows per thread (0: choose)
     bool no_stream = false;  // kernelPath 1
     bool no_tbl = false;     // register-coefficient variants only
+    uint64_t dg_skip = 0;    // dgbmv with ALT_dgbmv: bands dropped (bit j: band j)
     // ALT stride-2 mode: even and odd rows solved as two systems on the group
     // kernel (lanes x rows of the reference's ALT band layout)
     bool alt = false;
@@ -684,6 +685,7 @@ PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* l
         op.dg_off = r.offM;
         op.dg_lda = c.LDA;
         op.dg_ku = c.KU;
+        op.dg_skip = s->dg_skip;
         JwIO io;
         memset(&io, 0, sizeof(io));
         io.in = static_cast<const double*>(r.rhs);
@@ -706,6 +708,7 @@ PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* l
     a.stride = r.oS;
     a.lda = c.LDA;
     a.ku = c.KU;
+    a.skip = s->dg_skip;
     a.iz0 = r.iz0; a.iz1 = r.iz1; a.oz0 = r.oz0; a.oz1 = r.oz1;
     launch_dgbmv_generic(a, stream, s->num_sms);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -824,7 +827,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
     if (c.M_size == 0) c.M_size = (int64_t)c.size[0];
     if (c.inputBufferStride[0] == 0) c.inputBufferStride[0] = c.size[0];
     if (c.outputBufferStride[0] == 0) c.outputBufferStride[0] = c.size[0];
-    if (c.halfPrecision || c.ALT_dgbmv) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (c.halfPrecision) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
 
     AppState* s = new (std::nothrow) AppState();
     if (!s) return PFSOLVE_ERROR_MALLOC_FAILED;
@@ -886,7 +889,15 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
         s->kind = APP_DGBMV;
         if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (c.KU < 0 || c.KU >= c.LDA) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
+        else if (c.ALT_dgbmv && (c.LDA > 64 || dd_prec)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else {
+            // ALT_dgbmv (pfSolve_Plan_dgbmv.h:100, pfSolve_MatVecMul.h:390) drops band j
+            // when (j % 2 == 1 - LDA % 2 and KL != 0) or (j % 2 == LDA % 2 and KU != 0),
+            // KL and KU as configured
+            if (c.ALT_dgbmv)
+                for (int j = 0; j < c.LDA; ++j)
+                    if (((j % 2) == 1 - (c.LDA % 2) && c.KL) || ((j % 2) == (c.LDA % 2) && c.KU))
+                        s->dg_skip |= 1ull << j;
             const int kl = c.LDA - 1 - c.KU;
             if (dd_prec && !(kl == 1 && c.KU == 1)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
             else if (kl <= 2 && c.KU <= 2 && c.M_size <= kMaxRows) {
@@ -1026,6 +1037,7 @@ PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchPara
         op.dg_off = rd.offM;
         op.dg_lda = cd.LDA;
         op.dg_ku = cd.KU;
+        op.dg_skip = st(dg)->dg_skip;
         KL += kla;
         KU += cd.KU;
         io.iz0 = rd.iz0;  // the chain reads b through the dgbmv's input window

@@ -330,7 +330,7 @@ __device__ __forceinline__ void jw_row_weights(const JwOperator& op, int64_t i, 
             if (vp == 0.0 || p < 0 || p >= M) continue;
             for (int kk = -kla; kk <= op.dg_ku; ++kk) {
                 const int64_t c = p + kk;
-                if (c < 0 || c >= M) continue;
+                if (c < 0 || c >= M || ((op.dg_skip >> (op.dg_ku - kk)) & 1)) continue;
                 const double a = __ldg(op.dgbmv + op.dg_off + (int64_t)(op.dg_ku - kk) * M + c);
                 const int64_t k = c - i;  // within [-KL, KU] by construction of the plan
 #pragma unroll

@@ -25,6 +25,7 @@ struct JwOperator {
     const double* dgbmv;  // fused general band matrix (band-major), or nullptr
     int64_t dg_off;
     int dg_lda, dg_ku;
+    uint64_t dg_skip;  // ALT_dgbmv: bit j set drops band j of the general band matrix
     int scale_kind, lshift;  // fused block Scale operator (0: none)
     double scale_s;
     double scaleC;  // multiplies solution row 0 when a solve runs

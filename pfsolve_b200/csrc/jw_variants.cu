@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) dgbmv_generic_kernel(const DgbmvArgs a)
             double acc = 0.0;
             for (int j = 0; j < a.lda; ++j) {
                 const int64_t c = r + a.ku - j;
-                if (c < 0 || c >= a.M) continue;
+                if (c < 0 || c >= a.M || (j < 64 && ((a.skip >> j) & 1))) continue;
                 acc = __fma_rn(__ldg(a.A + a.off_A + (int64_t)j * a.M + c), xs[c], acc);
             }
             if (r >= a.oz0 && r < a.oz1) x[r] = acc;

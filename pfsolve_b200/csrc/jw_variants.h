@@ -118,6 +118,7 @@ struct DgbmvArgs {
     int64_t M, nsys, off_A, off_x, stride;
     int lda, ku;
     int64_t iz0, iz1, oz0, oz1;
+    uint64_t skip;  // ALT_dgbmv: bit j set drops band j
 };
 void launch_dgbmv_generic(const DgbmvArgs& a, cudaStream_t st, int num_sms);
 

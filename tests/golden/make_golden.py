@@ -112,6 +112,18 @@ def dgbmv_cases():
     return out
 
 
+def alt_dgbmv_cases():
+    """dgbmv with ALT_dgbmv: alternate bands dropped (stored with the dgbmv
+    fixtures; the rule is restated literally, including its one-sided forms)."""
+    out = []
+    for M, KL, KU in [(64, 0, 2), (100, 0, 4), (64, 2, 0), (65, 3, 0), (80, 2, 2), (50, 1, 3)]:
+        rng = np.random.default_rng(9200 + M + 10 * KL + KU)
+        A = WL.band_major(rng, M, KL, KU)
+        case = O.Case(M=M, batch=2, LDA=KL + KU + 1, KU=KU, KL=KL, jw_type=0, ALT_dgbmv=1)
+        out.append((f"dgbmv_alt_M{M}_kl{KL}_ku{KU}", case, A, rng.uniform(-1, 1, case.rhs_len()), "f64"))
+    return out
+
+
 def block_cases():
     out = []
     N, Y = 40, 3
@@ -237,7 +249,8 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
     summary = {}
-    single = jw_cases() + dgbmv_cases() + block_cases() if args.only == "all" else []
+    single = (jw_cases() + dgbmv_cases() + alt_dgbmv_cases() + block_cases() if args.only == "all" else
+              alt_dgbmv_cases() if args.only == "alt" else [])
     for name, case, buf, rhs, prec in single:
         try:
             ref = run_case(tmp, name, case, buf, rhs, prec)

@@ -13,7 +13,7 @@ def case_fields(case: O.Case, **extra):
              inputZeropad=case.cfg_inputZeropad, outputZeropad=case.cfg_outputZeropad,
              scaleC=case.cfg_scaleC, inputBufferStride=case.cfg_inputBufferStride,
              outputBufferStride=case.cfg_outputBufferStride, LDA=case.LDA, KU=case.KU, KL=case.KL,
-             block=case.block, lshift=case.lshift, doublePrecision=1)
+             block=case.block, lshift=case.lshift, doublePrecision=1, ALT_dgbmv=case.ALT_dgbmv)
     f.update(extra)
     return f
 

@@ -91,6 +91,20 @@ def test_alt_rejected():
             App(buffer=bands, outputBuffer=x, **kw)
 
 
+@pytest.mark.parametrize("KL,KU", [(0, 2), (0, 1), (2, 0), (1, 0), (3, 0), (2, 2), (1, 1), (0, 6), (5, 0)])
+@pytest.mark.parametrize("M", [33, 256, 1000])
+def test_alt_dgbmv(KL, KU, M):
+    """ALT_dgbmv: alternate bands of the general band matrix dropped, on the
+    fused-weight group/streaming kernels (KL, KU <= 2) and the generic one."""
+    rng = np.random.default_rng(35000 + 100 * KL + 10 * KU + M)
+    A = WL.band_major(rng, M, KL, KU)
+    case = O.Case(M=M, batch=11, LDA=KL + KU + 1, KU=KU, KL=KL, jw_type=0, ALT_dgbmv=1)
+    rhs = rng.uniform(-1, 1, case.rhs_len())
+    ref = O.dgbmv(case, A, rhs)
+    x = J.run_app(case, A, rhs)
+    assert np.abs(x - ref).max() <= 1e-13 * max(np.abs(ref).max(), 1e-300)
+
+
 def test_alt_device_status_clean():
     from pfsolve_b200.api import device_status
     assert device_status() == 0
