@@ -69,6 +69,7 @@ unsigned cluster_status_fetch_clear();
 // Status word of the streaming kernels' bounded waits since the last call
 // (0: none timed out); reading it synchronises with the device.
 unsigned stream_status_fetch_clear();
+unsigned steps_status_fetch_clear();  // the K-step sweep kernel's waits
 
 // K consecutive JW steps in one kernel (real FP64 systems; R rows per thread,
 // W warps per system given at launch).  MV: the steps have a matvec.

@@ -6,6 +6,7 @@
 #include "jw_steps.cuh"
 #include "jw_steps_seq.cuh"
 #include "jw_variants.h"
+#include "stream_variant_defs.h"
 
 namespace pfb {
 
@@ -69,5 +70,8 @@ const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K)
 }
 
 size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW) { return seq_smem_bytes(K, Mtab, NW); }
+
+// status of the sweep kernel's bounded waits
+PFB_STREAM_STATUS_ACCESSOR(steps_status_fetch_clear)
 
 }  // namespace pfb

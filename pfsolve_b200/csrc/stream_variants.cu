@@ -123,8 +123,9 @@ bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in,
 unsigned stream_status_fetch_clear()
 {
     const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
-    if (a == ~0u || b == ~0u || c == ~0u) return ~0u;
-    return a | b | c;
+    const unsigned d = steps_status_fetch_clear();
+    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u) return ~0u;
+    return a | b | c | d;
 }
 
 }  // namespace pfb
