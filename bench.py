@@ -362,7 +362,8 @@ def extras_arm(args):
     rows = int((step.Ns * step.nsys).sum())
     out["config4_uneven_step"] = {"complex_rhs_per_s": int(step.nsys.sum()) / (ms * 1e-3), "ms": ms,
                                   "gbs": 2.0 * rows * 16 / (ms * 1e-3) / 1e9, "shape": batch.shape(),
-                                  "graph": True, "launches_per_step": 1}
+                                  "graph": True,
+                                  "launches_per_step": 2 if batch.shape()["rowsPerThread"] == 0 else 1}
     batch.close()
     del inp, outb, keep
     torch.cuda.empty_cache()

@@ -268,7 +268,14 @@ PFSOLVE_API PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveL
  * largest first, and refactor the matrix when the entry changes.  The step is
  * the chain [dgbmv] -> JW -> [block] of the apps with the same fields.
  * Every entry uses plan-time band offsets: JW bands at 0, M, 2M of `bands`
- * (reference register-major order for its own M), dgbmv bands band-major. */
+ * (reference register-major order for its own M), dgbmv bands band-major.
+ * Two kernels: the group kernel (a group of warps per system, rowsPerThread
+ * rows per thread) and the sweep kernel (one complex system per lane, its
+ * rows in sequence, a warp per item of 32 systems).  With rowsPerThread and
+ * systemsPerItem both 0 the sweep kernel runs wherever the batch allows it:
+ * FP64, a bidiagonal (or no) solve, the fused V*A within rows i-1..i+1, block
+ * 7 (XXII in, packed complex out) without accumulation, and every entry's
+ * output 16-byte aligned and disjoint from its input. */
 typedef struct {
     int64_t M;               /* rows of this entry's systems (<= 4096) */
     int64_t nsys;            /* systems (complex ones count once) */
@@ -306,12 +313,14 @@ PFSOLVE_API PfSolveResult PfSolveBatchAppend(PfSolveBatch* batch, cudaStream_t s
 /* Capture the batch's launch into a CUDA graph on `stream` (a non-default
  * stream); later PfSolveBatchAppend calls launch the graph. */
 PFSOLVE_API PfSolveResult PfSolveBatchCaptureGraph(PfSolveBatch* batch, cudaStream_t stream);
-/* Time every compiled rows-per-thread / item-size candidate on the batch's
- * own buffers (`iterations` launches each) and keep the fastest; drops a
+/* Time every compiled rows-per-thread / item-size candidate of the group
+ * kernel, and the sweep kernel where the batch allows it, on the batch's own
+ * buffers (`iterations` launches each) and keep the fastest; drops a
  * captured graph.  Entries must be out of place (input != output). */
 PFSOLVE_API PfSolveResult PfSolveBatchAutotune(PfSolveBatch* batch, cudaStream_t stream, int iterations);
 /* Chosen shape: rows per thread, warps per system, systems per item, work
- * items, and the autotuner's best time (ms, 0 when not tuned). */
+ * items, and the autotuner's best time (ms, 0 when not tuned).  Rows per
+ * thread and warps per system 0: the sweep kernel. */
 PFSOLVE_API PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* batch, int* rowsPerThread, int* warpsPerSystem,
                                                int* systemsPerItem, int* items, double* tunedMs);
 PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);

@@ -1162,6 +1162,12 @@ struct PfSolveBatch {
     int R = 8, W = 1, G = 1, spi = 64;
     int max_blocks = 0;
     const BatchVariant* variant = nullptr;
+    // sweep kernel (one system per lane) in use; nullptr: the group kernel
+    const BatchSeqVariant* seq = nullptr;
+    bool seq_ok = false;  // every entry allows the sweep kernel
+    // the sweep kernel's coefficient rows (written by its pre-pass each launch)
+    double* d_coefs = nullptr;
+    int64_t* d_coef_off = nullptr;
     std::vector<BatchEntryDev> entries;
     std::vector<WorkItem> items;
     BatchEntryDev* d_entries = nullptr;
@@ -1218,6 +1224,64 @@ PfSolveResult batch_build_items(PfSolveBatch* b, int spi)
     return PFSOLVE_SUCCESS;
 }
 
+// The sweep kernel: FP64 bidiagonal (or matvec-only) steps whose V*A stays
+// within rows i-1..i+1, XXII in, packed complex out, no accumulation; every
+// entry's output 16-byte aligned and disjoint from its input (the sweep writes
+// a chunk's results before it has read the later rows of the system).
+bool batch_seq_allowed(const PfSolveBatch* b)
+{
+    if (b->PREC != PREC_F64 || b->KL > 1 || b->KU > 1 || b->SV == SV_TRI || b->LIN != LAY_XXII ||
+        b->LOUT != LAY_PACKED)
+        return false;
+    for (const BatchEntryDev& e : b->entries) {
+        if (e.io.accumulate) return false;
+        const uintptr_t i0 = reinterpret_cast<uintptr_t>(e.io.in + e.io.in_off);
+        const uintptr_t i1 = i0 + (uintptr_t)(2 * e.io.nsys * e.io.in_stride) * 8;
+        const uintptr_t o0 = reinterpret_cast<uintptr_t>(e.io.out) + (uintptr_t)e.io.out_off * 16;
+        const uintptr_t o1 = o0 + (uintptr_t)(e.io.nsys * e.io.out_stride) * 16;
+        if ((o0 & 15) != 0 || (e.io.nsys > 0 && i0 < o1 && o0 < i1)) return false;
+    }
+    return true;
+}
+
+PfSolveResult batch_configure_seq(PfSolveBatch* b, int nbuf)
+{
+    const BatchSeqVariant* v = find_batch_seq_variant(b->SV, nbuf);
+    if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (!b->d_coefs) {
+        // one coefficient table for the plan's lifetime: entry e's rows at coef_off[e]
+        std::vector<int64_t> off(b->entries.size());
+        int64_t rows = 0;
+        for (size_t e = 0; e < b->entries.size(); ++e) {
+            off[e] = rows;
+            rows += batch_seq_rows(b->entries[e].op.M);
+        }
+        if (cudaMalloc(&b->d_coefs, std::max<int64_t>(rows, 1) * 48) != cudaSuccess ||
+            cudaMalloc(&b->d_coef_off, std::max<size_t>(off.size(), 1) * sizeof(int64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
+        }
+        if (!off.empty() &&
+            cudaMemcpy(b->d_coef_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+            return PFSOLVE_ERROR_FAILED_TO_COPY;
+    }
+    const size_t smem = batch_seq_smem(v->NBUF, v->NW);
+    if (!allow_max_smem(v->func)) return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * v->NW, smem) != cudaSuccess ||
+        blocks < 1) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
+    }
+    b->seq = v;
+    b->variant = nullptr;
+    b->R = 0;
+    b->W = 0;
+    b->G = v->NW;
+    b->max_blocks = blocks * b->num_sms;
+    return PFSOLVE_SUCCESS;
+}
+
 PfSolveResult batch_configure(PfSolveBatch* b, int R)
 {
     int64_t W = (b->Mmax + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
@@ -1233,6 +1297,7 @@ PfSolveResult batch_configure(PfSolveBatch* b, int R)
         blocks < 1)
         return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
     b->variant = v;
+    b->seq = nullptr;
     b->R = R;
     b->W = (int)W;
     b->G = G;
@@ -1248,6 +1313,17 @@ PfSolveResult batch_launch(PfSolveBatch* b, cudaStream_t stream)
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
     const int64_t want = (nitems + b->G - 1) / b->G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, b->max_blocks));
+    if (b->seq) {
+        b->seq->coefs((int)b->entries.size(), stream, b->d_entries, b->d_coef_off, b->d_coefs);
+        b->seq->launch(dim3((unsigned)grid), batch_seq_smem(b->seq->NBUF, b->seq->NW), stream, b->d_entries,
+                       b->d_coef_off, b->d_coefs, b->d_items, nitems, b->d_counter);
+        g_launches.fetch_add(2, std::memory_order_relaxed);
+        if (cudaPeekAtLastError() != cudaSuccess) {
+            cudaGetLastError();
+            return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+        }
+        return PFSOLVE_SUCCESS;
+    }
     const size_t smem = b->variant->smem_bytes(b->W, b->G);
     b->variant->launch(dim3((unsigned)grid), dim3(32 * b->W * b->G), smem, stream, b->d_entries, b->d_items, nitems,
                        b->d_counter, b->W);
@@ -1355,6 +1431,16 @@ PfSolveResult PfSolveBatchCreate(PfSolveBatch** out, CUdevice device, const PfSo
                        cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(PFSOLVE_ERROR_FAILED_TO_COPY);
     }
+    b->seq_ok = batch_seq_allowed(b);
+    // default shape: the sweep kernel where the batch allows it (items of one
+    // warp's 32 systems), else the group kernel with 8 (or 4) rows per thread
+    if (b->seq_ok && !desc->rowsPerThread && desc->systemsPerItem <= 0 &&
+        batch_configure_seq(b, 4) == PFSOLVE_SUCCESS) {
+        PfSolveResult r = batch_build_items(b, 32);
+        if (r != PFSOLVE_SUCCESS) return fail(r);
+        *out = b;
+        return PFSOLVE_SUCCESS;
+    }
     int R = desc->rowsPerThread ? desc->rowsPerThread : 8;
     PfSolveResult r = batch_configure(b, R);
     if (r != PFSOLVE_SUCCESS && !desc->rowsPerThread) r = batch_configure(b, 4);
@@ -1377,7 +1463,7 @@ PfSolveResult PfSolveBatchAppend(PfSolveBatch* b, cudaStream_t stream)
     if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
     if (b->graph_exec) {
         if (cudaGraphLaunch(b->graph_exec, stream) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
-        g_launches.fetch_add(1, std::memory_order_relaxed);
+        g_launches.fetch_add(b->seq ? 2 : 1, std::memory_order_relaxed);  // kernels in the graph
         return PFSOLVE_SUCCESS;
     }
     return batch_launch(b, stream);
@@ -1419,19 +1505,34 @@ PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int ite
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double best = 1e300;
-    int bestR = b->R, bestSpi = b->spi;
+    int bestR = b->R, bestSpi = b->spi, bestBuf = b->seq ? b->seq->NBUF : 0;
+    auto time_shape = [&]() -> double {
+        if (batch_launch(b, stream) != PFSOLVE_SUCCESS) return 1e300;  // warm-up
+        cudaEventRecord(e0, stream);
+        for (int it = 0; it < iterations; ++it) batch_launch(b, stream);
+        cudaEventRecord(e1, stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) return 1e300;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / iterations;
+    };
+    // the sweep kernel (rows per thread reported as 0), one warp's 32 systems per item
+    for (int nbuf : {3, 4}) {
+        if (!b->seq_ok || batch_configure_seq(b, nbuf) != PFSOLVE_SUCCESS) continue;
+        if (batch_build_items(b, 32) != PFSOLVE_SUCCESS) continue;
+        const double per = time_shape();
+        if (per < best) {
+            best = per;
+            bestR = 0;
+            bestSpi = 32;
+            bestBuf = nbuf;
+        }
+    }
     for (int R : {4, 8, 16, 2}) {
         if (batch_configure(b, R) != PFSOLVE_SUCCESS) continue;
         for (int spi : {16, 32, 64, 128}) {
             if (batch_build_items(b, spi) != PFSOLVE_SUCCESS) continue;
-            if (batch_launch(b, stream) != PFSOLVE_SUCCESS) continue;  // warm-up
-            cudaEventRecord(e0, stream);
-            for (int it = 0; it < iterations; ++it) batch_launch(b, stream);
-            cudaEventRecord(e1, stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) continue;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            const double per = ms / iterations;
+            const double per = time_shape();
             if (per < best) {
                 best = per;
                 bestR = R;
@@ -1441,7 +1542,7 @@ PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int ite
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    PfSolveResult r = batch_configure(b, bestR);
+    PfSolveResult r = bestR ? batch_configure(b, bestR) : batch_configure_seq(b, bestBuf);
     if (r == PFSOLVE_SUCCESS) r = batch_build_items(b, bestSpi);
     if (r == PFSOLVE_SUCCESS) b->tuned_ms = best;
     return r;
@@ -1465,6 +1566,8 @@ void PfSolveBatchDestroy(PfSolveBatch* b)
     if (b->d_entries) cudaFree(b->d_entries);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_counter) cudaFree(b->d_counter);
+    if (b->d_coefs) cudaFree(b->d_coefs);
+    if (b->d_coef_off) cudaFree(b->d_coef_off);
     delete b;
 }
 

@@ -1,4 +1,5 @@
 // batch_variants.cu -- instantiations of the persistent uneven-batch kernel.
+#include "jw_batch_seq.cuh"
 #include "jw_kernel.cuh"
 #include "jw_variants.h"
 
@@ -48,5 +49,39 @@ const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, i
             return &v;
     return nullptr;
 }
+
+template <int SVK, int NBUF, int NW>
+static void batch_seq_launch_fn(dim3 grid, size_t smem, cudaStream_t st, const BatchEntryDev* entries,
+                                const int64_t* coef_off, const double* coefs, const WorkItem* items, int nitems,
+                                unsigned int* counter)
+{
+    jw_batch_seq_kernel<SVK, NBUF, NW><<<grid, 32 * NW, smem, st>>>(entries, coef_off, coefs, items, nitems, counter);
+}
+template <int SVK>
+static void batch_seq_coef_fn(int nentries, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+                              double* coefs)
+{
+    jw_batch_seq_coef_kernel<SVK><<<nentries, 128, 0, st>>>(entries, coef_off, coefs);
+}
+
+// warps per CTA: as many as the shared memory of one SM holds
+#define PFB_BSV(SVK, NBUF, NW)                                                                               \
+    BatchSeqVariant{SVK, NBUF, NW, (const void*)&jw_batch_seq_kernel<SVK, NBUF, NW>,                        \
+                    &batch_seq_launch_fn<SVK, NBUF, NW>, &batch_seq_coef_fn<SVK>}
+
+static const BatchSeqVariant kBatchSeqVariants[] = {
+    PFB_BSV(SV_UPPER, 3, 16), PFB_BSV(SV_UPPER, 4, 12), PFB_BSV(SV_LOWER, 3, 16),
+    PFB_BSV(SV_LOWER, 4, 12), PFB_BSV(SV_NONE, 3, 16),  PFB_BSV(SV_NONE, 4, 12),
+};
+
+const BatchSeqVariant* find_batch_seq_variant(int SV, int NBUF)
+{
+    for (const BatchSeqVariant& v : kBatchSeqVariants)
+        if (v.SV == SV && v.NBUF == NBUF) return &v;
+    return nullptr;
+}
+
+size_t batch_seq_smem(int NBUF, int NW) { return batch_seq_smem_bytes(NBUF, NW); }
+int64_t batch_seq_rows(int64_t M) { return batch_seq_coef_rows(M); }
 
 }  // namespace pfb

@@ -33,6 +33,24 @@ struct BatchVariant {
 };
 const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC);
 
+// Uneven batches of bidiagonal steps (V*A within rows i-1..i+1, XXII in,
+// packed complex out, FP64): one complex system per lane, each system's rows
+// in one sweep, items of up to 32 systems per warp, NBUF chunks of 8 rows
+// staged per warp, NW warps per CTA.  `coefs` launches the pre-pass that
+// writes every entry's coefficient rows (48 bytes each, batch_seq_rows(M) per
+// entry at row offset coef_off[e]) before the sweep.
+struct BatchSeqVariant {
+    int SV, NBUF, NW;
+    const void* func;
+    void (*launch)(dim3 grid, size_t smem, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+                   const double* coefs, const WorkItem* items, int nitems, unsigned int* counter);
+    void (*coefs)(int nentries, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+                  double* coefs);
+};
+const BatchSeqVariant* find_batch_seq_variant(int SV, int NBUF);
+int64_t batch_seq_rows(int64_t M);        // coefficient rows of an entry of M rows
+size_t batch_seq_smem(int NBUF, int NW);  // dynamic shared memory of NW warps
+
 // Streaming variants (TMA-staged systems, R rows per thread, W warps per
 // system).  IB / IBO: 16-byte units per swizzle row of the input / output
 // layout (the TMA box's inner extent).
