@@ -24,9 +24,18 @@
 // -- units 0..3 hold real rows (0,1) .. (6,7), units 4..7 the imaginary rows --
 // with 16-byte unit u stored at u ^ (s & 7), so that a lane's reads of its own
 // slot and the warp's coalesced copies (8 lanes per system) hit distinct bank
-// groups.  cp.async keeps NBUF chunks in flight per warp (16-byte copies when
-// the rows are 16-byte aligned, else 8-byte copies); bytes beyond the system's
-// M rows are zero-filled.  Row i needs the next sweep row's right-hand side,
+// groups.  cp.async keeps NBUF chunks in flight per warp; bytes beyond the
+// system's M rows are zero-filled.  Three copy layouts:
+//   BS_ALIGNED  input 16-byte aligned, even stride: 16-byte copies.
+//   BS_SHIFTED  input 16-byte aligned, odd stride (odd M, packed): the real
+//               rows are 16-byte aligned, the imaginary rows 8 bytes off, so
+//               a chunk's imaginary units hold rows r0+1 .. r0+8 (descending
+//               sweep) or r0-1 .. r0+6 (ascending) -- still 16-byte copies.
+//               The one row outside comes from the next chunk's buffer; for
+//               the last chunk an extra one-unit chunk (sweep index Q) holds
+//               it.  The row the shifted units read at -1 lies inside the
+//               system's real rows and is never used.
+//   BS_UNALIGNED anything else: 8-byte copies.  Row i needs the next sweep row's right-hand side,
 // so the chunk after the current one has landed before a chunk is processed.
 // A lane reads its slot into registers, computes its 8 rows in registers
 // (no shared-memory stores inside the row loop, so the coefficient loads run
@@ -92,10 +101,11 @@ __global__ void __launch_bounds__(128) jw_batch_seq_coef_kernel(const BatchEntry
     }
 }
 
+enum : int { BS_ALIGNED = 0, BS_SHIFTED = 1, BS_UNALIGNED = 2 };
+
 // Sweep of one work item: systems y0 .. y0+ns-1 of entry `ent`, coefficient
-// rows at `ctab`.  AL16: the rows are 16-byte aligned (16-byte copies), else
-// 8-byte copies.
-template <int SVK, int NBUF, bool AL16>
+// rows at `ctab`, copy layout LAY.
+template <int SVK, int NBUF, int LAY>
 __device__ __forceinline__ void batch_seq_item(const BatchEntryDev* __restrict__ ent, const double* __restrict__ ctab,
                                                int64_t y0, int ns, unsigned char* wbase, int lane)
 {
@@ -113,24 +123,30 @@ __device__ __forceinline__ void batch_seq_item(const BatchEntryDev* __restrict__
     const int Q = (M + 7) >> 3;
 
     // chunk of sweep index k: data into buffer k % NBUF, coefficient rows into
-    // slot k % (NBUF + 1); an empty group past the end
+    // slot k % (NBUF + 1); an empty group past the end (BS_SHIFTED: sweep index
+    // Q is the one-unit chunk of the row beyond the last chunk)
+    constexpr int kVirtUnit = DESC ? 7 : 4;  // BS_SHIFTED: the unit of sweep index Q
     auto issue = [&](int k) {
-        if (k < Q) {
+        if (k < Q || (LAY == BS_SHIFTED && k == Q)) {
             const int r0 = 8 * (DESC ? Q - 1 - k : k);
             const uint32_t dst0 = wbase_u + (uint32_t)((k % NBUF) * kBsDataBytes);
-            if (lane < 24)
+            if (lane < 24 && k < Q)
                 cp_async16_n(wbase_u + NBUF * kBsDataBytes + (k % (NBUF + 1)) * kBsCoefBytes + 16 * lane,
                              ctab + 6 * r0 + 2 * lane, 16);
-            if constexpr (AL16) {
-                const int row = r0 + 2 * (pu & 3);
+            if constexpr (LAY != BS_UNALIGNED) {
+                // imaginary units of BS_SHIFTED start one row up (descending) or down
+                const int shift = (LAY == BS_SHIFTED && pu >= 4) ? (DESC ? 1 : -1) : 0;
+                const int row = r0 + 2 * (pu & 3) + shift;
                 const int nb = (M - row >= 2) ? 16 : (M - row == 1 ? 8 : 0);
                 const double* src = re0 + (int64_t)(2 * ps + (pu >> 2)) * istr + row;
+                const bool want = k < Q || pu == kVirtUnit;
 #pragma unroll
                 for (int t = 0; t < 8; ++t) {
                     const int s = 4 * t + ps;
                     const int bytes = (s < ns) ? nb : 0;
-                    cp_async16_n(dst0 + s * 128 + ((pu ^ (s & 7)) << 4), bytes ? src + (int64_t)(8 * t) * istr : in0,
-                                 bytes);
+                    if (want)
+                        cp_async16_n(dst0 + s * 128 + ((pu ^ (s & 7)) << 4),
+                                     bytes ? src + (int64_t)(8 * t) * istr : in0, bytes);
                 }
             } else {
                 const int part = (lane >> 3) & 1, rr = lane & 7;
@@ -163,28 +179,48 @@ __device__ __forceinline__ void batch_seq_item(const BatchEntryDev* __restrict__
         const unsigned char* cb = wbase + (k % NBUF) * kBsDataBytes + lane * 128;
         const double* tab =
             reinterpret_cast<const double*>(wbase + NBUF * kBsDataBytes + (k % (NBUF + 1)) * kBsCoefBytes);
+        const unsigned char* nb = wbase + ((k + 1) % NBUF) * kBsDataBytes + lane * 128;  // next chunk's slot
+        auto unit = [&](const unsigned char* b, int u) { return *reinterpret_cast<const double2*>(b + ((u ^ sw) << 4)); };
         double br[8], bi[8];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const double2 vr = *reinterpret_cast<const double2*>(cb + ((u ^ sw) << 4));
-            const double2 vi = *reinterpret_cast<const double2*>(cb + (((u + 4) ^ sw) << 4));
+            const double2 vr = unit(cb, u);
             br[2 * u] = vr.x;
             br[2 * u + 1] = vr.y;
-            bi[2 * u] = vi.x;
-            bi[2 * u + 1] = vi.y;
         }
-        // first sweep row of the next chunk
+        // first sweep row of the next chunk (row r0 - 1 descending, r0 + 8 ascending)
         double lr = 0.0, li = 0.0;
-        if (k + 1 < Q) {
-            const unsigned char* nb = wbase + ((k + 1) % NBUF) * kBsDataBytes + lane * 128;
-            if constexpr (DESC) {
-                lr = reinterpret_cast<const double2*>(nb + ((3 ^ sw) << 4))->y;
-                li = reinterpret_cast<const double2*>(nb + ((7 ^ sw) << 4))->y;
-            } else {
-                lr = reinterpret_cast<const double2*>(nb + ((0 ^ sw) << 4))->x;
-                li = reinterpret_cast<const double2*>(nb + ((4 ^ sw) << 4))->x;
+        if constexpr (LAY == BS_SHIFTED) {
+            // imaginary units: rows r0+1 .. r0+8 (descending) or r0-1 .. r0+6 (ascending)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double2 vi = unit(cb, u + 4);
+                if constexpr (DESC) {
+                    bi[2 * u + 1] = vi.x;
+                    if (u < 3) bi[2 * u + 2] = vi.y;
+                } else {
+                    if (u > 0) bi[2 * u - 1] = vi.x;
+                    bi[2 * u] = vi.y;
+                }
             }
+            const double2 n = unit(nb, kVirtUnit);  // rows r0-1, r0 (descending) or r0+7, r0+8
+            if constexpr (DESC) {
+                bi[0] = n.y;
+                if (k + 1 < Q) li = n.x;
+            } else {
+                bi[7] = n.x;
+                li = n.y;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double2 vi = unit(cb, u + 4);
+                bi[2 * u] = vi.x;
+                bi[2 * u + 1] = vi.y;
+            }
+            if (k + 1 < Q) li = DESC ? unit(nb, 7).y : unit(nb, 4).x;
         }
+        if (k + 1 < Q) lr = DESC ? unit(nb, 3).y : unit(nb, 0).x;
         double2 res[8];
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
@@ -257,11 +293,11 @@ __global__ void __launch_bounds__(32 * NW, 1) jw_batch_seq_kernel(const BatchEnt
         const WorkItem wi = items[it];
         const BatchEntryDev* ent = entries + wi.entry;
         const double* ctab = coefs + 6 * coef_off[wi.entry];
-        const bool al16 = ((reinterpret_cast<uintptr_t>(ent->io.in + ent->io.in_off) & 15) == 0) &&
-                          ((ent->io.in_stride & 1) == 0);
+        const bool al16 = (reinterpret_cast<uintptr_t>(ent->io.in + ent->io.in_off) & 15) == 0;
         const int ns = (int)(wi.y1 - wi.y0);
-        if (al16) batch_seq_item<SVK, NBUF, true>(ent, ctab, wi.y0, ns, wbase, lane);
-        else batch_seq_item<SVK, NBUF, false>(ent, ctab, wi.y0, ns, wbase, lane);
+        if (al16 && (ent->io.in_stride & 1) == 0) batch_seq_item<SVK, NBUF, BS_ALIGNED>(ent, ctab, wi.y0, ns, wbase, lane);
+        else if (al16) batch_seq_item<SVK, NBUF, BS_SHIFTED>(ent, ctab, wi.y0, ns, wbase, lane);
+        else batch_seq_item<SVK, NBUF, BS_UNALIGNED>(ent, ctab, wi.y0, ns, wbase, lane);
     }
     cp_async_wait<0>();
 }
