@@ -271,8 +271,11 @@ PFSOLVE_API PfSolveResult PfSolveAppendChain(PfSolveApplication** apps, PfSolveL
  * (reference register-major order for its own M), dgbmv bands band-major.
  * Two kernels: the group kernel (a group of warps per system, rowsPerThread
  * rows per thread) and the sweep kernel (one complex system per lane, its
- * rows in sequence, a warp per item of 32 systems).  With rowsPerThread and
- * systemsPerItem both 0 the sweep kernel runs wherever the batch allows it:
+ * rows in sequence, a warp per item of 32 systems).  sweepRows = 8 or 16
+ * asks for the sweep kernel with that many rows per staged chunk
+ * (PFSOLVE_ERROR_UNSUPPORTED_COMBINATION where the batch does not allow it).
+ * With rowsPerThread, systemsPerItem and sweepRows all 0 the sweep kernel runs
+ * wherever the batch allows it:
  * FP64, a bidiagonal (or no) solve, the fused V*A within rows i-1..i+1, block
  * 7 (XXII in, packed complex out) without accumulation, and every entry's
  * output 16-byte aligned and disjoint from its input. */
@@ -299,6 +302,7 @@ typedef struct {
     int mixedPrecisionRefinement; /* as in PfSolveConfiguration */
     int rowsPerThread;            /* 0: default / autotuned */
     int systemsPerItem;           /* work-queue item size (0: default / autotuned) */
+    int sweepRows;                /* sweep kernel with chunks of 8 or 16 rows (0: default / autotuned) */
 } PfSolveBatchDesc;
 
 typedef struct PfSolveBatch PfSolveBatch;
@@ -323,6 +327,10 @@ PFSOLVE_API PfSolveResult PfSolveBatchAutotune(PfSolveBatch* batch, cudaStream_t
  * thread and warps per system 0: the sweep kernel. */
 PFSOLVE_API PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* batch, int* rowsPerThread, int* warpsPerSystem,
                                                int* systemsPerItem, int* items, double* tunedMs);
+/* The sweep kernel's shape: rows per staged chunk, chunk buffers per warp and
+ * warps per CTA (all 0 when the batch runs the group kernel). */
+PFSOLVE_API PfSolveResult PfSolveBatchGetSweepShape(const PfSolveBatch* batch, int* rowsPerChunk, int* buffers,
+                                                    int* warpsPerCTA);
 PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
 
 /* One uneven batch, as PfSolveBatchCreate + PfSolveBatchAppend +
@@ -335,7 +343,8 @@ PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
  * device array inside the library, sized for PFSOLVE_NOALLOC_MAX_ENTRIES
  * entries and PFSOLVE_NOALLOC_MAX_ITEMS work items (ceil(nsys /
  * systemsPerItem) per entry, systemsPerItem 0 meaning 64); larger calls return
- * PFSOLVE_ERROR_CAPACITY.  The work counter must start at zero: each call
+ * PFSOLVE_ERROR_CAPACITY.  It runs the group kernel only (sweepRows must be
+ * 0).  The work counter must start at zero: each call
  * clears it on `stream` before its launch.  All calls share the array, so two
  * calls whose work overlaps in time (on other streams or from other threads)
  * race; serialise them.  The first call on a device looks up the array's

@@ -188,8 +188,11 @@ class Batch:
         ms = ctypes.c_double()
         check(self._lib.PfSolveBatchGetShape(self.handle, ctypes.byref(r), ctypes.byref(w), ctypes.byref(spi),
                                              ctypes.byref(items), ctypes.byref(ms)), "PfSolveBatchGetShape")
+        ch, nb, nw = (ctypes.c_int() for _ in range(3))
+        check(self._lib.PfSolveBatchGetSweepShape(self.handle, ctypes.byref(ch), ctypes.byref(nb), ctypes.byref(nw)),
+              "PfSolveBatchGetSweepShape")
         return dict(rowsPerThread=r.value, warpsPerSystem=w.value, systemsPerItem=spi.value, items=items.value,
-                    tunedMs=ms.value)
+                    tunedMs=ms.value, sweepRows=ch.value, sweepBuffers=nb.value, sweepWarps=nw.value)
 
     def close(self):
         if getattr(self, "handle", None):

@@ -112,7 +112,7 @@ class PfSolveBatchEntry(ctypes.Structure):
 class PfSolveBatchDesc(ctypes.Structure):
     _fields_ = [("upperBanded", c_int), ("jw_type", c_int), ("LDA", c_int), ("KU", c_int), ("KL", c_int),
                 ("block", c_int), ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int),
-                ("systemsPerItem", c_int)]
+                ("systemsPerItem", c_int), ("sweepRows", c_int)]
 
 
 class PfSolveServerDesc(ctypes.Structure):
@@ -170,6 +170,7 @@ SIGNATURES = {
     "PfSolveBatchCaptureGraph": (c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "PfSolveBatchAutotune": (c_int, [ctypes.c_void_p, ctypes.c_void_p, c_int]),
     "PfSolveBatchGetShape": (c_int, [ctypes.c_void_p] + [ctypes.POINTER(c_int)] * 4 + [ctypes.POINTER(ctypes.c_double)]),
+    "PfSolveBatchGetSweepShape": (c_int, [ctypes.c_void_p] + [ctypes.POINTER(c_int)] * 3),
     "PfSolveBatchDestroy": (None, [ctypes.c_void_p]),
     "PfSolveBatchAppendNoAlloc": (c_int, [c_int, ctypes.POINTER(PfSolveBatchDesc), ctypes.POINTER(PfSolveBatchEntry),
                                           c_int, ctypes.c_void_p]),

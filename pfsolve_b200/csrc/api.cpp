@@ -1165,9 +1165,11 @@ struct PfSolveBatch {
     // sweep kernel (one system per lane) in use; nullptr: the group kernel
     const BatchSeqVariant* seq = nullptr;
     bool seq_ok = false;  // every entry allows the sweep kernel
-    // the sweep kernel's coefficient rows (written by its pre-pass each launch)
+    int seq_shape = 0;    // its compiled shape (rows per chunk, buffers, warps)
+    // the sweep kernel's per-entry tensor maps and coefficient rows (written
+    // by its pre-pass each launch)
     double* d_coefs = nullptr;
-    int64_t* d_coef_off = nullptr;
+    BatchSeqEntry* d_seq = nullptr;
     std::vector<BatchEntryDev> entries;
     std::vector<WorkItem> items;
     BatchEntryDev* d_entries = nullptr;
@@ -1239,33 +1241,36 @@ bool batch_seq_allowed(const PfSolveBatch* b)
         const uintptr_t i1 = i0 + (uintptr_t)(2 * e.io.nsys * e.io.in_stride) * 8;
         const uintptr_t o0 = reinterpret_cast<uintptr_t>(e.io.out) + (uintptr_t)e.io.out_off * 16;
         const uintptr_t o1 = o0 + (uintptr_t)(e.io.nsys * e.io.out_stride) * 16;
-        if ((o0 & 15) != 0 || (e.io.nsys > 0 && i0 < o1 && o0 < i1)) return false;
+        if ((o0 & 15) != 0 || e.io.out_stride < e.io.M || (e.io.nsys > 0 && i0 < o1 && o0 < i1)) return false;
     }
     return true;
 }
 
-PfSolveResult batch_configure_seq(PfSolveBatch* b, int nbuf)
+PfSolveResult batch_configure_seq(PfSolveBatch* b, int shape)
 {
-    const BatchSeqVariant* v = find_batch_seq_variant(b->SV, nbuf);
+    const BatchSeqVariant* v = find_batch_seq_variant(b->SV, shape);
     if (!v) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-    if (!b->d_coefs) {
-        // one coefficient table for the plan's lifetime: entry e's rows at coef_off[e]
-        std::vector<int64_t> off(b->entries.size());
+    if (!b->d_seq) {
+        // per entry: tensor maps and its first coefficient row
+        std::vector<BatchSeqEntry> sq(b->entries.size());
         int64_t rows = 0;
         for (size_t e = 0; e < b->entries.size(); ++e) {
-            off[e] = rows;
+            memset(&sq[e], 0, sizeof(BatchSeqEntry));
+            const JwIO& io = b->entries[e].io;
+            if (io.nsys > 0 && !encode_batch_seq_maps(io, &sq[e])) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            sq[e].coef_off = rows;
             rows += batch_seq_rows(b->entries[e].op.M);
         }
         if (cudaMalloc(&b->d_coefs, std::max<int64_t>(rows, 1) * 48) != cudaSuccess ||
-            cudaMalloc(&b->d_coef_off, std::max<size_t>(off.size(), 1) * sizeof(int64_t)) != cudaSuccess) {
+            cudaMalloc(&b->d_seq, std::max<size_t>(sq.size(), 1) * sizeof(BatchSeqEntry)) != cudaSuccess) {
             cudaGetLastError();
             return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
         }
-        if (!off.empty() &&
-            cudaMemcpy(b->d_coef_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        if (!sq.empty() &&
+            cudaMemcpy(b->d_seq, sq.data(), sq.size() * sizeof(BatchSeqEntry), cudaMemcpyHostToDevice) != cudaSuccess)
             return PFSOLVE_ERROR_FAILED_TO_COPY;
     }
-    const size_t smem = batch_seq_smem(v->NBUF, v->NW);
+    const size_t smem = batch_seq_smem(v);
     if (!allow_max_smem(v->func)) return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * v->NW, smem) != cudaSuccess ||
@@ -1274,6 +1279,7 @@ PfSolveResult batch_configure_seq(PfSolveBatch* b, int nbuf)
         return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
     }
     b->seq = v;
+    b->seq_shape = shape;
     b->variant = nullptr;
     b->R = 0;
     b->W = 0;
@@ -1314,9 +1320,9 @@ PfSolveResult batch_launch(PfSolveBatch* b, cudaStream_t stream)
     const int64_t want = (nitems + b->G - 1) / b->G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, b->max_blocks));
     if (b->seq) {
-        b->seq->coefs((int)b->entries.size(), stream, b->d_entries, b->d_coef_off, b->d_coefs);
-        b->seq->launch(dim3((unsigned)grid), batch_seq_smem(b->seq->NBUF, b->seq->NW), stream, b->d_entries,
-                       b->d_coef_off, b->d_coefs, b->d_items, nitems, b->d_counter);
+        b->seq->coefs((int)b->entries.size(), stream, b->d_entries, b->d_seq, b->d_coefs);
+        b->seq->launch(dim3((unsigned)grid), batch_seq_smem(b->seq), stream, b->d_entries, b->d_seq, b->d_coefs,
+                       b->d_items, nitems, b->d_counter);
         g_launches.fetch_add(2, std::memory_order_relaxed);
         if (cudaPeekAtLastError() != cudaSuccess) {
             cudaGetLastError();
@@ -1432,10 +1438,22 @@ PfSolveResult PfSolveBatchCreate(PfSolveBatch** out, CUdevice device, const PfSo
             return fail(PFSOLVE_ERROR_FAILED_TO_COPY);
     }
     b->seq_ok = batch_seq_allowed(b);
+    if (desc->sweepRows) {
+        // the sweep kernel with the first compiled shape of that chunk depth
+        PfSolveResult r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        for (int shape = 0; b->seq_ok && shape < kBatchSeqShapes && r != PFSOLVE_SUCCESS; ++shape) {
+            const BatchSeqVariant* v = find_batch_seq_variant(b->SV, shape);
+            if (v && v->CH == desc->sweepRows) r = batch_configure_seq(b, shape);
+        }
+        if (r == PFSOLVE_SUCCESS) r = batch_build_items(b, 32);
+        if (r != PFSOLVE_SUCCESS) return fail(r);
+        *out = b;
+        return PFSOLVE_SUCCESS;
+    }
     // default shape: the sweep kernel where the batch allows it (items of one
     // warp's 32 systems), else the group kernel with 8 (or 4) rows per thread
     if (b->seq_ok && !desc->rowsPerThread && desc->systemsPerItem <= 0 &&
-        batch_configure_seq(b, 4) == PFSOLVE_SUCCESS) {
+        batch_configure_seq(b, 0) == PFSOLVE_SUCCESS) {
         PfSolveResult r = batch_build_items(b, 32);
         if (r != PFSOLVE_SUCCESS) return fail(r);
         *out = b;
@@ -1505,7 +1523,7 @@ PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int ite
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double best = 1e300;
-    int bestR = b->R, bestSpi = b->spi, bestBuf = b->seq ? b->seq->NBUF : 0;
+    int bestR = b->R, bestSpi = b->spi, bestShape = b->seq_shape;
     auto time_shape = [&]() -> double {
         if (batch_launch(b, stream) != PFSOLVE_SUCCESS) return 1e300;  // warm-up
         cudaEventRecord(e0, stream);
@@ -1517,15 +1535,15 @@ PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int ite
         return ms / iterations;
     };
     // the sweep kernel (rows per thread reported as 0), one warp's 32 systems per item
-    for (int nbuf : {3, 4}) {
-        if (!b->seq_ok || batch_configure_seq(b, nbuf) != PFSOLVE_SUCCESS) continue;
+    for (int shape = 0; shape < kBatchSeqShapes; ++shape) {
+        if (!b->seq_ok || batch_configure_seq(b, shape) != PFSOLVE_SUCCESS) continue;
         if (batch_build_items(b, 32) != PFSOLVE_SUCCESS) continue;
         const double per = time_shape();
         if (per < best) {
             best = per;
             bestR = 0;
             bestSpi = 32;
-            bestBuf = nbuf;
+            bestShape = shape;
         }
     }
     for (int R : {4, 8, 16, 2}) {
@@ -1542,10 +1560,19 @@ PfSolveResult PfSolveBatchAutotune(PfSolveBatch* b, cudaStream_t stream, int ite
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    PfSolveResult r = bestR ? batch_configure(b, bestR) : batch_configure_seq(b, bestBuf);
+    PfSolveResult r = bestR ? batch_configure(b, bestR) : batch_configure_seq(b, bestShape);
     if (r == PFSOLVE_SUCCESS) r = batch_build_items(b, bestSpi);
     if (r == PFSOLVE_SUCCESS) b->tuned_ms = best;
     return r;
+}
+
+PfSolveResult PfSolveBatchGetSweepShape(const PfSolveBatch* b, int* rowsPerChunk, int* buffers, int* warpsPerCTA)
+{
+    if (!b) return PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
+    if (rowsPerChunk) *rowsPerChunk = b->seq ? b->seq->CH : 0;
+    if (buffers) *buffers = b->seq ? b->seq->NBUF : 0;
+    if (warpsPerCTA) *warpsPerCTA = b->seq ? b->seq->NW : 0;
+    return PFSOLVE_SUCCESS;
 }
 
 PfSolveResult PfSolveBatchGetShape(const PfSolveBatch* b, int* R, int* W, int* spi, int* items, double* ms)
@@ -1567,7 +1594,7 @@ void PfSolveBatchDestroy(PfSolveBatch* b)
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_counter) cudaFree(b->d_counter);
     if (b->d_coefs) cudaFree(b->d_coefs);
-    if (b->d_coef_off) cudaFree(b->d_coef_off);
+    if (b->d_seq) cudaFree(b->d_seq);
     delete b;
 }
 

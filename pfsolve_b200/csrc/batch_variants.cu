@@ -2,6 +2,7 @@
 #include "jw_batch_seq.cuh"
 #include "jw_kernel.cuh"
 #include "jw_variants.h"
+#include "stream_variant_defs.h"
 
 namespace pfb {
 
@@ -50,38 +51,45 @@ const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, i
     return nullptr;
 }
 
-template <int SVK, int NBUF, int NW>
+template <int SVK, int CH, int NBUF, int NW>
 static void batch_seq_launch_fn(dim3 grid, size_t smem, cudaStream_t st, const BatchEntryDev* entries,
-                                const int64_t* coef_off, const double* coefs, const WorkItem* items, int nitems,
+                                const BatchSeqEntry* seq, const double* coefs, const WorkItem* items, int nitems,
                                 unsigned int* counter)
 {
-    jw_batch_seq_kernel<SVK, NBUF, NW><<<grid, 32 * NW, smem, st>>>(entries, coef_off, coefs, items, nitems, counter);
+    jw_batch_seq_kernel<SVK, CH, NBUF, NW><<<grid, 32 * NW, smem, st>>>(entries, seq, coefs, items, nitems, counter);
 }
 template <int SVK>
-static void batch_seq_coef_fn(int nentries, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+static void batch_seq_coef_fn(int nentries, cudaStream_t st, const BatchEntryDev* entries, const BatchSeqEntry* seq,
                               double* coefs)
 {
-    jw_batch_seq_coef_kernel<SVK><<<nentries, 128, 0, st>>>(entries, coef_off, coefs);
+    jw_batch_seq_coef_kernel<SVK><<<nentries, 128, 0, st>>>(entries, seq, coefs);
 }
 
 // warps per CTA: as many as the shared memory of one SM holds
-#define PFB_BSV(SVK, NBUF, NW)                                                                               \
-    BatchSeqVariant{SVK, NBUF, NW, (const void*)&jw_batch_seq_kernel<SVK, NBUF, NW>,                        \
-                    &batch_seq_launch_fn<SVK, NBUF, NW>, &batch_seq_coef_fn<SVK>}
+#define PFB_BSV(SVK, CH, NBUF, NW)                                                                  \
+    BatchSeqVariant{SVK, CH, NBUF, NW, (const void*)&jw_batch_seq_kernel<SVK, CH, NBUF, NW>,       \
+                    &batch_seq_launch_fn<SVK, CH, NBUF, NW>, &batch_seq_coef_fn<SVK>}
+// shapes in order of preference: 16-row chunks first (128-byte rows per system
+// and part: fewer, longer DRAM bursts than 8-row chunks)
+#define PFB_BSV_SHAPES(SVK) PFB_BSV(SVK, 16, 4, 5), PFB_BSV(SVK, 16, 3, 6), PFB_BSV(SVK, 8, 4, 10)
 
 static const BatchSeqVariant kBatchSeqVariants[] = {
-    PFB_BSV(SV_UPPER, 3, 16), PFB_BSV(SV_UPPER, 4, 12), PFB_BSV(SV_LOWER, 3, 16),
-    PFB_BSV(SV_LOWER, 4, 12), PFB_BSV(SV_NONE, 3, 16),  PFB_BSV(SV_NONE, 4, 12),
+    PFB_BSV_SHAPES(SV_UPPER),
+    PFB_BSV_SHAPES(SV_LOWER),
+    PFB_BSV_SHAPES(SV_NONE),
 };
 
-const BatchSeqVariant* find_batch_seq_variant(int SV, int NBUF)
+const BatchSeqVariant* find_batch_seq_variant(int SV, int shape)
 {
+    int n = 0;
     for (const BatchSeqVariant& v : kBatchSeqVariants)
-        if (v.SV == SV && v.NBUF == NBUF) return &v;
+        if (v.SV == SV && n++ == shape) return &v;
     return nullptr;
 }
 
-size_t batch_seq_smem(int NBUF, int NW) { return batch_seq_smem_bytes(NBUF, NW); }
+size_t batch_seq_smem(const BatchSeqVariant* v) { return batch_seq_smem_bytes(v->CH, v->NBUF, v->NW); }
 int64_t batch_seq_rows(int64_t M) { return batch_seq_coef_rows(M); }
+
+PFB_STREAM_STATUS_ACCESSOR(batch_status_fetch_clear)
 
 }  // namespace pfb

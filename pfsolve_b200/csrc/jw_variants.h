@@ -38,18 +38,30 @@ const BatchVariant* find_batch_variant(int R, int KL, int KU, int SV, int LIN, i
 // in one sweep, items of up to 32 systems per warp, NBUF chunks of 8 rows
 // staged per warp, NW warps per CTA.  `coefs` launches the pre-pass that
 // writes every entry's coefficient rows (48 bytes each, batch_seq_rows(M) per
-// entry at row offset coef_off[e]) before the sweep.
+// entry from row coef_off) before the sweep.
+struct alignas(64) BatchSeqEntry {
+    CUtensorMap in[2];  // {2 in_stride, nsys} doubles, boxes 8 x 32 (64-byte swizzle) and 16 x 32 (128-byte)
+    CUtensorMap out;    // {2 M, nsys} doubles at row pitch 16 out_stride bytes, box 16 x 32, 128-byte swizzle
+    int64_t coef_off;   // first coefficient row of the entry
+    int tma_in;         // input 16-byte aligned with in_stride >= M: TMA boxes (else 8-byte cp.async)
+    int pad[13];
+};
+// CH rows per chunk (8 or 16).
 struct BatchSeqVariant {
-    int SV, NBUF, NW;
+    int SV, CH, NBUF, NW;
     const void* func;
-    void (*launch)(dim3 grid, size_t smem, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+    void (*launch)(dim3 grid, size_t smem, cudaStream_t st, const BatchEntryDev* entries, const BatchSeqEntry* seq,
                    const double* coefs, const WorkItem* items, int nitems, unsigned int* counter);
-    void (*coefs)(int nentries, cudaStream_t st, const BatchEntryDev* entries, const int64_t* coef_off,
+    void (*coefs)(int nentries, cudaStream_t st, const BatchEntryDev* entries, const BatchSeqEntry* seq,
                   double* coefs);
 };
-const BatchSeqVariant* find_batch_seq_variant(int SV, int NBUF);
-int64_t batch_seq_rows(int64_t M);        // coefficient rows of an entry of M rows
-size_t batch_seq_smem(int NBUF, int NW);  // dynamic shared memory of NW warps
+const BatchSeqVariant* find_batch_seq_variant(int SV, int shape);  // shape: index into the compiled shapes
+constexpr int kBatchSeqShapes = 3;
+int64_t batch_seq_rows(int64_t M);  // coefficient rows of an entry of M rows
+// Tensor maps of one entry; false when its output cannot take TMA stores.
+bool encode_batch_seq_maps(const JwIO& io, BatchSeqEntry* e);
+unsigned batch_status_fetch_clear();  // the sweep batch kernel's waits
+size_t batch_seq_smem(const BatchSeqVariant* v);  // dynamic shared memory of a launch
 
 // Streaming variants (TMA-staged systems, R rows per thread, W warps per
 // system).  IB / IBO: 16-byte units per swizzle row of the input / output

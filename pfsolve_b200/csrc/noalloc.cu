@@ -66,6 +66,7 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
 {
     if (!desc || nentries < 0 || (nentries > 0 && !entries)) return PFSOLVE_ERROR_INVALID_ARGUMENT;
     if (nentries > kMaxEntries) return PFSOLVE_ERROR_CAPACITY;
+    if (desc->sweepRows) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;  // the group kernel only
     if (desc->mixedPrecisionRefinement < 0 || desc->mixedPrecisionRefinement > 3) return PFSOLVE_ERROR_INVALID_ARGUMENT;
     const int bt = desc->block % 10, sk = desc->block / 100;
     if (!(bt == 0 || bt == 1 || bt == 7) || ((desc->block / 10) % 10 != 0 && (desc->block / 10) % 10 != 2) || sk > 4 ||

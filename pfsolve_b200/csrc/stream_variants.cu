@@ -115,6 +115,38 @@ bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* i
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool encode_batch_seq_maps(const JwIO& io, BatchSeqEntry* e)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || io.nsys < 1 || io.nsys > INT32_MAX || io.M < 1 || io.out_stride < io.M) return false;
+    const cuuint32_t estr[2] = {1u, 1u};
+    // output: packed complex rows, 16 bytes each; the map ends at 2 M doubles
+    double* obase = io.out + 2 * io.out_off;
+    if (reinterpret_cast<uintptr_t>(obase) % 16) return false;
+    const cuuint64_t ostr[1] = {(cuuint64_t)io.out_stride * 16};
+    const cuuint64_t dout[2] = {(cuuint64_t)(2 * io.M), (cuuint64_t)io.nsys};
+    const cuuint32_t bout[2] = {16u, 32u};
+    if (fn(&e->out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, obase, dout, ostr, bout, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    // input: a system's real rows then its imaginary rows, one tensor row
+    e->tma_in = 0;
+    const double* ibase = io.in + io.in_off;
+    if (reinterpret_cast<uintptr_t>(ibase) % 16 == 0 && io.in_stride >= io.M && 2 * io.in_stride <= INT32_MAX) {
+        const cuuint64_t istr[1] = {(cuuint64_t)io.in_stride * 16};
+        const cuuint64_t din[2] = {(cuuint64_t)(2 * io.in_stride), (cuuint64_t)io.nsys};
+        const cuuint32_t b8[2] = {8u, 32u}, b16[2] = {16u, 32u};
+        e->tma_in = fn(&e->in[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(ibase), din, istr, b8, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                    fn(&e->in[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(ibase), din, istr, b16, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    return true;
+}
+
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
 {
     return encode_row_maps(v->R, v->LIN, v->LOUT, v->IB, v->IBO, io, in, out);
@@ -123,9 +155,9 @@ bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in,
 unsigned stream_status_fetch_clear()
 {
     const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
-    const unsigned d = steps_status_fetch_clear();
-    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u) return ~0u;
-    return a | b | c | d;
+    const unsigned d = steps_status_fetch_clear(), e = batch_status_fetch_clear();
+    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u) return ~0u;
+    return a | b | c | d | e;
 }
 
 }  // namespace pfb

@@ -105,25 +105,30 @@ def check(ents, outs, mode, untouched=True):
             assert np.all(g[:, 2 * M:] == SENTINEL), (k, M)
 
 
+@pytest.mark.parametrize("rows", [0, 8, 16])
 @pytest.mark.parametrize("name", list(MODES))
-def test_sweep_matches_oracle(name):
+def test_sweep_matches_oracle(name, rows):
+    """Chunks of 8 and 16 rows (0: the plan's default)."""
     mode = MODES[name]
     rng = np.random.default_rng(11)
     ents = make_entries(rng, mode[2], mode[3], SIZES)
-    outs, shape = run_batch(ents, mode)
+    outs, shape = run_batch(ents, mode, sweepRows=rows)
     assert shape["rowsPerThread"] == 0 and shape["systemsPerItem"] == 32, shape
+    assert shape["sweepRows"] == (rows or 16), shape
     check(ents, outs, mode)
 
 
-@pytest.mark.parametrize("istr_pad,ostr_pad,in_shift", [(1, 3, 0), (2, 1, 1), (0, 0, 1), (3, 2, 1)])
-def test_sweep_strides_and_alignment(istr_pad, ostr_pad, in_shift):
-    """Odd input strides or an input 8 bytes off a 16-byte boundary take the
-    8-byte copies; odd output strides keep 16-byte packed rows."""
+@pytest.mark.parametrize("rows", [8, 16])
+@pytest.mark.parametrize("istr_pad,ostr_pad,in_shift", [(1, 3, 0), (2, 1, 1), (0, 0, 1), (3, 2, 1), (4, 0, 0)])
+def test_sweep_strides_and_alignment(istr_pad, ostr_pad, in_shift, rows):
+    """Odd input strides take the shifted imaginary box, an input 8 bytes off
+    a 16-byte boundary the 8-byte copies; padded strides leave the padding
+    out of the results and untouched in the output."""
     for name in ("ub0_j13_dg3_sphlapla", "ub1_j10_dg2_sphlapl"):
         mode = MODES[name]
         rng = np.random.default_rng(12 + istr_pad)
         ents = make_entries(rng, mode[2], mode[3], SIZES[:10], istr_pad, ostr_pad)
-        outs, shape = run_batch(ents, mode, in_shift=in_shift)
+        outs, shape = run_batch(ents, mode, in_shift=in_shift, sweepRows=rows)
         assert shape["rowsPerThread"] == 0, shape
         check(ents, outs, mode)
 
@@ -179,11 +184,16 @@ def test_sweep_rejects_wide_operators_and_keeps_the_group_kernel():
 
     from pfsolve_b200 import capi
     lib = capi.load()
-    d = capi.PfSolveBatchDesc(upperBanded=0, jw_type=10, LDA=3, KU=1, KL=1, block=307)
     e = (capi.PfSolveBatchEntry * 1)()
     e[0].M, e[0].nsys = 64, 0
     e[0].bands = e[0].dgbmvBands = e[0].input = e[0].output = 16
     e[0].inputStride = e[0].outputStride = 64
     h = ctypes.c_void_p()
+    for rows in (0, 8):
+        d = capi.PfSolveBatchDesc(upperBanded=0, jw_type=10, LDA=3, KU=1, KL=1, block=307, sweepRows=rows)
+        assert lib.PfSolveBatchCreate(ctypes.byref(h), 0, ctypes.byref(d), e, 1) == \
+            capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION
+    # the group kernel's operator with sweepRows asks for what the batch cannot do
+    d = capi.PfSolveBatchDesc(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=301, sweepRows=16)
     assert lib.PfSolveBatchCreate(ctypes.byref(h), 0, ctypes.byref(d), e, 1) == \
         capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION
