@@ -218,6 +218,22 @@ def alt_cases():
     return out
 
 
+def long_cases():
+    """(name, Case, bands, rhs, precision) for long systems, N > 4352: the
+    reference splits them over several kernel launches (multi-upload,
+    pfSolve_InitializeApp.h:1540-1583, reduced systems in its temporary buffer);
+    stored under tests/golden/long/."""
+    out = []
+    for ub, jwt in [(2, 13), (1, 10), (0, 10), (1, 12), (0, 13)]:
+        for M in ([4352, 4360, 5000, 8192, 16384] if (ub, jwt) in [(2, 13), (1, 10)] else [4400, 8192]):
+            rng = np.random.default_rng(17000 + 100 * ub + jwt + M)
+            bands = WL.permute_bands(jw_bands(rng, M, ub), M)
+            case = O.Case(M=M, batch=2, upperBanded=ub, jw_type=jwt)
+            rhs = rng.uniform(-1, 1, case.rhs_len())
+            out.append((f"long_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
+    return out
+
+
 REF_BIN_FP128 = os.path.join(ROOT, "oracle", "_ref", "pfsolve_ref_fp128")
 
 
@@ -243,8 +259,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
     ap.add_argument("--time", action="store_true")
-    ap.add_argument("--only", default="all", choices=["all", "steps", "alt"],
-                    help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode")
+    ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long"],
+                    help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode; "
+                         "long: only long systems (N > 4352, and their timing with --time)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
@@ -333,6 +350,39 @@ def main():
             except Exception as e:
                 timing[label] = dict(error=str(e))
         with open(os.path.join(args.out, "ref_timing_steps.json"), "w") as f:
+            json.dump(timing, f, indent=1)
+        print(json.dumps(timing, indent=1))
+    ldir = os.path.join(args.out, "long")
+    os.makedirs(ldir, exist_ok=True)
+    for name, case, buf, rhs, prec in (long_cases() if args.only in ("all", "long") else []):
+        try:
+            ref = run_case(tmp, name, case, buf, rhs, prec)
+            np.savez_compressed(os.path.join(ldir, name + ".npz"), params=json.dumps(asdict(case)),
+                                precision=prec, buffer=buf, rhs=rhs, ref_out=ref)
+            summary[name] = "ok"
+        except Exception as e:
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
+    if args.time and args.only in ("all", "long"):
+        # long tridiagonal systems, 1 GiB of right-hand sides (jw_type 13)
+        timing = {}
+        for M, B in ((8192, 16384), (16384, 8192)):
+            rng = np.random.default_rng(6)
+            label = f"long_jw_t13_N{M}_B{B}"
+            case = O.Case(M=M, batch=B, upperBanded=2, jw_type=13)
+            d = os.path.join(tmp, label)
+            os.makedirs(d, exist_ok=True)
+            O.write_reference_case(d, case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M), np.zeros(1),
+                                   precision="f64", iters=20)
+            os.remove(os.path.join(d, "rhs.bin"))
+            with open(os.path.join(d, "params.txt"), "a") as f:
+                f.write(f"rhs_bytes={8 * M * B}\n")
+            try:
+                _, ms = O.run_reference(d, timeout=300)
+                timing[label] = dict(ms=ms, rhs_per_s=B / (ms * 1e-3), gbs=2 * 8 * M * B / (ms * 1e-3) / 1e9)
+            except Exception as e:
+                timing[label] = dict(error=str(e))
+        with open(os.path.join(args.out, "ref_timing_long.json"), "w") as f:
             json.dump(timing, f, indent=1)
         print(json.dumps(timing, indent=1))
     with open(os.path.join(args.out, "summary.json"), "w") as f:
