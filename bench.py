@@ -558,8 +558,9 @@ def main():
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
-    ap.add_argument("--path", type=int, default=0, choices=[0, 1],
-                    help="kernelPath: 0 streaming kernel where possible, 1 group kernel only")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2],
+                    help="kernelPath: 0 streaming kernel where possible (long systems: two passes), "
+                         "1 group kernel only, 2 long systems on the cluster kernel")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu = True

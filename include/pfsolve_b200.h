@@ -172,7 +172,8 @@ typedef struct {
                                      FP64 residual refinement sweeps, FP64 storage (0: plain FP64) */
     int rowsPerThread;            /* 0: autotuned; else 2, 4, 8, 16 or 32 (32: streaming kernel only) */
     int kernelPath;               /* 0: streaming kernel wherever a launch allows it, else the group
-                                     kernel; 1: group kernel only */
+                                     kernel (long systems: the two-pass kernel); 1: group kernel only;
+                                     2: long systems on the cluster kernel */
 } PfSolveConfiguration;
 
 /* Launch-time values (pfSolve_Structs.h:383-449). */
@@ -376,8 +377,11 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * (numConsecutiveJWIterations > 1); streaming = 4: K bidiagonal steps with one
  * system per lane in one sweep wherever a launch's buffers allow it
  * (16-byte-aligned rows, stride >= the rows written, full output window;
- * groupsPerCTA = warps per CTA), else the K-step kernel.  No counterpart in
- * the reference. */
+ * groupsPerCTA = warps per CTA), else the K-step kernel; streaming = 5: long
+ * systems (M > 4096) in two passes over slices of 32 x warpsPerSystem x
+ * rowsPerThread rows, groupsPerCTA systems in flight per CTA (no waits
+ * between CTAs; the plan holds a record of 64 bytes per system and slice).
+ * No counterpart in the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);
 /* Launches that ran on the streaming kernel since load (all apps). */

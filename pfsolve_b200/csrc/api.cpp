@@ -48,7 +48,14 @@ struct AppState {
     // buffers allow it; `variant` serves the other launches
     const StreamVariant* stream_v = nullptr;
     int stream_G = 0, stream_max_blocks = 0;
-    // long systems (N > 4096): one cluster of CTAs per system
+    // long systems (N > 4096): two passes over slices (default), or one
+    // cluster of CTAs per system (kernelPath 2)
+    const LongVariant* long_v = nullptr;
+    int long_NS = 0, long_grid = 0;
+    double* long_red = nullptr;  // per (system, slice) records, then per-slice constants
+    int64_t long_batch = 0;      // systems the records hold
+    int64_t plan_batch = 0;      // right-hand sides of the plan (size[1] * size[2])
+    bool cluster_only = false;   // kernelPath 2
     const ClusterVariant* cluster_v = nullptr;
     int cluster_max = 0;
     int R_req = 0;           // caller's rows per thread (0: choose)
@@ -162,6 +169,40 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         }
     }
     cudaGetLastError();
+    return false;
+}
+
+// Two-pass variant for long real systems: the first compiled shape that fits
+// (slices of 1024 rows, 4 systems in flight per CTA), with its per-(system,
+// slice) records allocated for the plan's right-hand sides (rows per thread
+// 8: M must be a multiple of 8).
+bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    s->long_v = nullptr;
+    if (s->prec != PREC_F64 || s->no_stream || s->cluster_only || LIN != LAY_REAL || LOUT != LAY_REAL || SCALE ||
+        M % 8 != 0 || s->plan_batch < 1)
+        return false;
+    for (int shape = 0; shape < kLongShapes; ++shape) {
+        const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
+        if (!v) return false;
+        const int b = v->blocks_per_sm();
+        if (b < 1) continue;
+        const int NS = (int)((M + v->S - 1) / v->S);
+        const int64_t res = (int64_t)b * s->num_sms;
+        // CTAs in whole multiples of NS, at most one CTA's worth of systems each
+        const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
+        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 4) * sizeof(double);
+        if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            s->long_red = nullptr;
+            return false;
+        }
+        s->long_v = v;
+        s->long_NS = NS;
+        s->long_grid = (int)(per_slice * NS);
+        s->long_batch = s->plan_batch;
+        return true;
+    }
     return false;
 }
 
@@ -351,6 +392,7 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
     // take.
     s->variant = nullptr;
     if (choose_stream(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
+    if (M > kMaxRows && choose_long(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
     if (M > kMaxRows && choose_cluster(s, M, LIN, LOUT, SCALE)) return PFSOLVE_SUCCESS;
     // nothing compiled fits: distinguish "too long" from "not compiled"
     for (int R : {2, 4, 8, 16})
@@ -475,6 +517,25 @@ PfSolveResult launch_cluster(AppState* s, const JwOperator& op, const JwIO& io, 
     return PFSOLVE_SUCCESS;
 }
 
+// Long systems: the two-pass kernel, under the streaming kernel's buffer rules.
+PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
+{
+    const LongVariant* v = s->long_v;
+    if (io.accumulate || io.oz0 > 0 || io.oz1 < io.M || io.nsys > s->long_batch)
+        return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, io);
+    if (!e) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    double* cst = s->long_red + (size_t)s->long_batch * s->long_NS * 8;
+    const cudaError_t err = v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, s->long_NS);
+    note_launch(true);
+    g_launches.fetch_add(s->sv != SV_NONE ? 2 : 1, std::memory_order_relaxed);  // the carry kernel and pass 2
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
 // Launch on the streaming variant when the plan has one and this launch's
 // buffers allow it (no accumulation, full output window, TMA-encodable rows).
 bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
@@ -493,6 +554,7 @@ bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream
 PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
 {
     if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    if (s->long_v) return launch_long(s, op, io, stream);
     if (s->cluster_v) return launch_cluster(s, op, io, stream);
     if (launch_stream(s, op, io, stream)) {
         g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -798,6 +860,13 @@ PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int
         if (groupsPerCTA) *groupsPerCTA = s->steps_G;
         return PFSOLVE_SUCCESS;
     }
+    if (s->long_v) {
+        if (streaming) *streaming = 5;
+        if (rowsPerThread) *rowsPerThread = s->long_v->R;
+        if (warpsPerSystem) *warpsPerSystem = s->long_v->W;
+        if (groupsPerCTA) *groupsPerCTA = s->long_v->G;
+        return PFSOLVE_SUCCESS;
+    }
     if (s->cluster_v) {
         if (streaming) *streaming = 2;
         if (rowsPerThread) *rowsPerThread = s->cluster_v->R;
@@ -882,6 +951,8 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->R_fixed = c.rowsPerThread != 0 && c.rowsPerThread != 32;
                 s->R_req = c.rowsPerThread;
                 s->no_stream = c.kernelPath == 1;
+                s->cluster_only = c.kernelPath == 2;
+                s->plan_batch = (int64_t)c.size[1] * (int64_t)(c.size[2] ? c.size[2] : 1);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
         }
@@ -977,6 +1048,7 @@ void deletePfSolve(PfSolveApplication* app)
                 if (s->events[i]) cudaEventDestroy(s->events[i]);
             delete[] s->events;
         }
+        if (s->long_red) cudaFree(s->long_red);
         delete s;
     }
     app->internal = nullptr;

@@ -1,0 +1,474 @@
+// jw_long.cuh -- the JW step for long systems (N > 4096) in two passes, with
+// no waiting between CTAs.
+//
+// Same operator as the streaming and cluster kernels (x = M^{-1} V b,
+// x[0] *= scaleC; real FP64 systems; PfSolve_shaderGen_JonesWorlandMV,
+// pfSolve_CodeGen/pfSolve_KernelsLevel2/pfSolve_JonesWorland.h:38-408).  The
+// reference splits such systems over several launches that keep a reduced
+// system in a temporary buffer (multi-upload,
+// pfSolve_AppManagement/pfSolve_InitializeApp.h:1540-1583); so does this
+// kernel, with the reduction written as affine maps:
+//
+//  * A system is cut into NS slices of S = 32*W*R rows.  A CTA owns one slice
+//    position c and the coefficient table of those rows (built once, in shared
+//    memory), and G groups of W warps each stream a different system's slice c
+//    through it (TMA boxes, as in the streaming kernel).
+//  * Within a slice the solve is the group kernel's: per-thread chunk
+//    recurrences and affine scans across the group.  The value entering the
+//    slice from below (forward) or above (backward) is the only coupling.
+//  * Pass 1 (PASS = 1) solves every slice with both carries zero and writes,
+//    per (system, slice): the forward map's offset Bf (the value leaving the
+//    slice), the backward map's offset Bb0, and the slice's matvec halo input
+//    rows (so pass 2 never reads rows a neighbour slice may already have
+//    overwritten in place).  Every CTA also writes its slice's constants: the
+//    forward and backward multipliers Af, Ab, and Psi, the backward offset for
+//    a unit forward carry and zero input (the backward offset is affine in the
+//    forward carry: Bb = Bb0 + X Psi).
+//  * Between the passes a small kernel (one thread per system) composes the
+//    forward carries X_c = Af_{c-1} X_{c-1} + Bf_{c-1} from slice 0 and the
+//    backward ones from the top slice, Y_c = Ab_{c+1} Y_{c+1} + Bb0_{c+1} +
+//    X_{c+1} Psi_{c+1}, into the records.
+//  * Pass 2 solves its slice again with those carries and writes the result.
+//  Input is read twice and written once; the three launches are ordered on
+//  the stream, so no CTA ever waits for another.  The tridiagonal pivots entering
+//  a slice come from the Moebius product of all rows before it, which every
+//  CTA forms itself in its prologue.
+//  * Completion waits are bounded: a wait that runs out records
+//    kStatusWaitTimeout and the group stops.
+#pragma once
+#include "jw_cluster.cuh"
+
+namespace pfb {
+
+template <int R_, int W_, int G_, int KL_, int KU_, int SV_>
+struct LgCfg {
+    using B = StCfg<R_, W_, KL_, KU_, SV_, LAY_REAL, LAY_REAL, false, PREC_F64>;  // slice layout and table planes
+    static constexpr int R = R_, W = W_, G = G_, T = 32 * W_, S = T * R_, NT = T * G_;
+    static constexpr int KL = KL_, KU = KU_, SV = SV_;
+};
+
+// Per (system, slice) record, in doubles: forward offset and backward offset
+// (pass 1), halo rows below (KL <= 2) and above (KU <= 2) (pass 1), and the
+// carries entering the slice from below and from above (the carry kernel).
+constexpr int kLgRed = 8;
+constexpr int kLgRedBf = 0, kLgRedBb = 1, kLgRedLo = 2, kLgRedHi = 4, kLgRedX = 6, kLgRedY = 7;
+// Per slice constants: Af, Ab, Psi.
+constexpr int kLgConst = 4;
+
+template <class C>
+__host__ __device__ constexpr size_t lg_smem_bytes()
+{
+    return C::B::TBL + (size_t)C::G * C::W * kScratchPerWarp * sizeof(double) + 8 * sizeof(double) +
+           (size_t)C::G * 2 * sizeof(uint64_t) + 1024 + (size_t)C::G * 2 * C::B::BUF;
+}
+
+// ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
+// of the CTA; the pivots entering the slice come from the Moebius product of
+// rows [0, c*S), formed here as well.
+template <class C>
+__device__ void lg_prologue(const JwOperator& op, double* table, double* scratch, double* q4, int c)
+{
+    using BC = typename C::B;
+    constexpr int R = C::R, U = BC::U, NB = BC::NB, S = C::S;
+    const int64_t M = op.M;
+    const int nthr = blockDim.x, tid = threadIdx.x;
+    const int64_t s0 = (int64_t)c * S;  // first row of the slice
+    GroupCtx g;
+    g.lane = tid & 31;
+    g.wg = tid >> 5;
+    g.W = nthr >> 5;
+    g.nthr = nthr;
+    g.bar_id = 1;
+    g.seq = 0;
+    g.scratch = scratch;
+    auto mstep = [&](int64_t i, double& a, double& b, double& cc, double& d) {
+        double ac = 0.0;
+        if (i >= 1 && i < M) ac = band(op, op.off_sl, i) * band(op, op.off_su, i - 1);
+        const double na = a - ac * cc, nb = b - ac * d;
+        cc = a;
+        d = b;
+        a = na;
+        b = nb;
+        renorm2x2(a, b, cc, d);
+    };
+    double dprev = 1.0;
+    const int Rp = (S + nthr - 1) / nthr;
+    const int64_t s = s0 + (int64_t)tid * Rp;
+    if constexpr (C::SV == SV_TRI) {
+        // (1) Q = product over rows [0, s0), spread over the CTA's threads
+        if (s0 > 0) {
+            const int64_t Rq = (s0 + nthr - 1) / nthr;
+            double a = 1, b = 0, cc = 0, d = 1;
+            for (int64_t i = (int64_t)tid * Rq; i < (int64_t)(tid + 1) * Rq && i < s0; ++i) mstep(i, a, b, cc, d);
+            const double pa = a, pb = b, pc = cc, pd = d;
+            group_matrix_scan(g, a, b, cc, d);
+            if (tid == nthr - 1) {
+                double na = pa * a + pb * cc, nb = pa * b + pb * d, nc = pc * a + pd * cc, nd = pc * b + pd * d;
+                renorm2x2(na, nb, nc, nd);
+                q4[0] = na;
+                q4[1] = nb;
+                q4[2] = nc;
+                q4[3] = nd;
+            }
+        } else if (tid == 0) {
+            q4[0] = 1.0;
+            q4[1] = 0.0;
+            q4[2] = 0.0;
+            q4[3] = 1.0;
+        }
+        __syncthreads();
+        const double qa = q4[0], qc = q4[2];  // Q applied to (1, 0)^T
+        // (2) this thread's rows of the slice, after the preceding threads' and Q
+        double a = 1, b = 0, cc = 0, d = 1;
+        for (int j = 0; j < Rp; ++j) {
+            const int64_t i = s + j;
+            if (i < s0 + S) mstep(i, a, b, cc, d);
+        }
+        group_matrix_scan(g, a, b, cc, d);  // product of the slice's preceding chunks
+        const double fa = a * qa + b * qc, fc = cc * qa + d * qc;
+        dprev = (s == 0) ? 1.0 : fa / fc;
+    }
+    for (int j = 0; j < Rp; ++j) {
+        const int64_t li = (int64_t)tid * Rp + j;  // row within the slice
+        if (li >= S) break;
+        const int64_t i = s0 + li;
+        double w[NB];
+        double nl = 0.0, nh = 0.0;
+        if (i < M) {
+            jw_row_weights<C::KL, NB>(op, i, w);
+            double m = 1.0;
+            if constexpr (C::SV == SV_TRI) {
+                const double ai = (i >= 1) ? band(op, op.off_sl, i) : 0.0;
+                const double ci = (i < M - 1) ? band(op, op.off_su, i) : 0.0;
+                const double ac = (i >= 1) ? ai * band(op, op.off_su, i - 1) : 0.0;
+                const double dp = (i == 0) ? 1.0 : 1.0 - ac / dprev;
+                m = 1.0 / dp;
+                dprev = dp;
+                nl = -(ai * m);
+                nh = -(ci * m);
+            } else if constexpr (C::SV == SV_LOWER) {
+                nl = (i >= 1) ? -band(op, op.off_sl, i) : 0.0;
+            } else if constexpr (C::SV == SV_UPPER) {
+                nh = (i < M - 1) ? -band(op, op.off_su, i) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) w[k] *= m;
+        } else {
+#pragma unroll
+            for (int k = 0; k < NB; ++k) w[k] = 0.0;
+        }
+        const int tt = (int)(li / R), jj = (int)(li % R);
+        auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * BC::TP + tt) * 2 + (jj & 1)] = v; };
+#pragma unroll
+        for (int k = 0; k < NB; ++k) put(k, w[k]);
+        if constexpr (BC::FWD) put(BC::P_NL, nl);
+        if constexpr (BC::BWD) put(BC::P_NH, nh);
+    }
+}
+
+// One slice solve of a group: x holds the matvec result on entry and the
+// slice's solution on exit.  Carries: fwd_carry(Atot, Btot) returns the value
+// entering the slice from below given the slice's forward total map;
+// bwd_carry likewise from above.  Both are called by every thread of the group.
+template <class C, class TB, class FC, class BCR>
+__device__ __forceinline__ void lg_solve(GroupCtx& g, const TB& coef, double Af, double Ab, double (&x)[C::R + C::KL + C::KU],
+                                         FC fwd_carry, BCR bwd_carry)
+{
+    using BC = typename C::B;
+    constexpr int R = C::R, U = BC::U;
+    (void)R;
+    if constexpr (BC::FWD) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 c = coef(BC::P_NL, u);
+            if (u > 0) x[2 * u] = __fma_rn(c.x, x[2 * u - 1], x[2 * u]);
+            x[2 * u + 1] = __fma_rn(c.y, x[2 * u], x[2 * u + 1]);
+        }
+        double Ain, Bin, At, Bt;
+        group_affine_scan_map<true>(g, Af, x[C::R - 1], Ain, Bin, At, Bt);
+        const double X = fwd_carry(At, Bt);
+        const double pin = __fma_rn(Ain, X, Bin);
+        double p = 1.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 c = coef(BC::P_NL, u);
+            p = c.x * p;
+            x[2 * u] = __fma_rn(p, pin, x[2 * u]);
+            p = c.y * p;
+            x[2 * u + 1] = __fma_rn(p, pin, x[2 * u + 1]);
+        }
+    }
+    if constexpr (BC::BWD) {
+#pragma unroll
+        for (int u = U - 1; u >= 0; --u) {
+            const double2 c = coef(BC::P_NH, u);
+            if (u < U - 1) x[2 * u + 1] = __fma_rn(c.y, x[2 * u + 2], x[2 * u + 1]);
+            x[2 * u] = __fma_rn(c.x, x[2 * u + 1], x[2 * u]);
+        }
+        double Ain, Bin, At, Bt;
+        group_affine_scan_map<false>(g, Ab, x[0], Ain, Bin, At, Bt);
+        const double Y = bwd_carry(At, Bt);
+        const double q = __fma_rn(Ain, Y, Bin);
+        double p = 1.0;
+#pragma unroll
+        for (int u = U - 1; u >= 0; --u) {
+            const double2 c = coef(BC::P_NH, u);
+            p = c.y * p;
+            x[2 * u + 1] = __fma_rn(p, q, x[2 * u + 1]);
+            p = c.x * p;
+            x[2 * u] = __fma_rn(p, q, x[2 * u]);
+        }
+    }
+}
+
+// Carries of every slice of system blockIdx.x * blockDim.x + threadIdx.x.
+template <bool FWD, bool BWD>
+__global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__ red, const double* __restrict__ cst,
+                                                            const int NS, const int64_t nsys)
+{
+    const int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= nsys) return;
+    double* rs = red + (size_t)y * NS * kLgRed;
+    double X = 0.0;
+    for (int c = 0; c < NS; ++c) {
+        rs[c * kLgRed + kLgRedX] = X;
+        if (FWD) X = __fma_rn(cst[c * kLgConst], X, rs[c * kLgRed + kLgRedBf]);
+    }
+    if (BWD) {
+        double Y = 0.0;
+        for (int c = NS - 1; c >= 0; --c) {
+            rs[c * kLgRed + kLgRedY] = Y;
+            const double Bb = FWD ? __fma_rn(rs[c * kLgRed + kLgRedX], cst[c * kLgConst + 2], rs[c * kLgRed + kLgRedBb])
+                                  : rs[c * kLgRed + kLgRedBb];
+            Y = __fma_rn(cst[c * kLgConst + 1], Y, Bb);
+        }
+    }
+}
+
+// grid: CTAs in multiples of NS (CTA b owns slice b % NS); red: nsys * NS
+// records of kLgRed doubles; cst: NS records of kLgConst doubles.
+template <class C, int PASS>
+__global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ CUtensorMap tm_in,
+                                                       const __grid_constant__ CUtensorMap tm_out,
+                                                       const JwOperator op, const JwIO io, double* __restrict__ red,
+                                                       double* __restrict__ cst, const int NS)
+{
+    using BC = typename C::B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int R = C::R, W = C::W, T = C::T, U = BC::U, KL = C::KL, KU = C::KU, NB = BC::NB;
+    constexpr int IB = BC::IB, H = BC::H, IBO = BC::IBO;
+    constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = warp / W, wg = warp - grp * W;
+    const int t = threadIdx.x - grp * T;  // thread within the group
+    const int c = (int)(blockIdx.x % (unsigned)NS);
+
+    double* table = reinterpret_cast<double*>(smem_raw);
+    double* scratch = reinterpret_cast<double*>(smem_raw + BC::TBL);
+    double* q4 = scratch + C::G * W * kScratchPerWarp;  // 8 doubles
+    uint64_t* bars = reinterpret_cast<uint64_t*>(q4 + 8) + 2 * grp;
+    unsigned char* after = reinterpret_cast<unsigned char*>(reinterpret_cast<uint64_t*>(q4 + 8) + 2 * C::G);
+    const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
+    unsigned char* buf0 = after + pad + (size_t)grp * 2 * BC::BUF;
+    unsigned char* buf1 = buf0 + BC::BUF;
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+
+    if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(q4 + 8) + threadIdx.x), W);
+    mbar_init_fence();
+    lg_prologue<C>(op, table, scratch, q4, c);
+    __syncthreads();
+
+    GroupCtx g;
+    g.lane = lane;
+    g.wg = wg;
+    g.W = W;
+    g.nthr = T;
+    g.bar_id = 1 + grp;
+    g.seq = 0;
+    g.scratch = scratch + (size_t)grp * W * kScratchPerWarp;
+
+    const int64_t s0 = (int64_t)c * C::S;
+    const int64_t s_glob = s0 + (int64_t)t * R;
+    const double2* tb = reinterpret_cast<const double2*>(table) + t;
+    auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * BC::TP]; };
+    double Af = 1.0, Ab = 1.0;  // this thread's chunk multipliers
+    if constexpr (BC::FWD) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 cc = coef(BC::P_NL, u);
+            Af = (u == 0) ? cc.x : cc.x * Af;
+            Af = cc.y * Af;
+        }
+    }
+    if constexpr (BC::BWD) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 cc = coef(BC::P_NH, u);
+            Ab = cc.x * Ab;
+            Ab = cc.y * Ab;
+        }
+    }
+
+    // Slice constants (Af, Ab, Psi): a solve of zero input with a unit
+    // forward carry, by group 0; written to cst by pass 1.
+    if (PASS == 1 && grp == 0) {
+        double x[R + KL + KU];
+#pragma unroll
+        for (int i = 0; i < R + KL + KU; ++i) x[i] = 0.0;
+        double afs = 1.0, abs_ = 1.0, psi = 0.0;
+        lg_solve<C>(g, coef, Af, Ab, x,
+                    [&](double At, double) {
+                        afs = At;
+                        return 1.0;
+                    },
+                    [&](double At, double Bt) {
+                        abs_ = At;
+                        psi = Bt;
+                        return 0.0;
+                    });
+        if (t == 0) {
+            cst[c * kLgConst + 0] = afs;
+            cst[c * kLgConst + 1] = abs_;
+            cst[c * kLgConst + 2] = psi;
+        }
+    }
+
+    const int sw_me = swz_row<BC::SWB>(t), sw_prev = swz_row<BC::SWB>(t - 1), sw_next = swz_row<BC::SWB>(t + 1);
+    const int swo_me = swz_row<BC::SWBO>(t);
+    auto unit_off = [&](int u, int ch, int sw) -> uint32_t {
+        return (uint32_t)((H > 1 ? (u / IB) * T : 0) + ch) * ROWB + (((u % IB) ^ sw) << 4);
+    };
+    const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
+    auto in_row = [&](int64_t y, int64_t row) -> double {  // input row of system y as data (0 outside)
+        if (row < 0 || row >= io.M || row < io.iz0 || row >= io.iz1) return 0.0;
+        return io.in[io.in_off + y * io.in_stride + row];
+    };
+    const int64_t nsys = io.nsys;
+    const int64_t per = (int64_t)(gridDim.x / (unsigned)NS) * C::G;  // systems in flight over the grid
+    int64_t sys = (int64_t)(blockIdx.x / (unsigned)NS) * C::G + grp;
+    const int chunk0 = c * T;
+
+    auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(H * 32 * ROWB));
+#pragma unroll
+        for (int h = 0; h < H; ++h)
+            tma_load_3d(smem_u32(b + (size_t)(h * T + 32 * wg) * ROWB), &tm_in, h * IB * 2, chunk0 + 32 * wg, (int)y,
+                        bar);
+    };
+    auto issue_store = [&](unsigned char* b, int64_t y) {
+#pragma unroll
+        for (int h = 0; h < BC::HO; ++h)
+            tma_store_3d(&tm_out, h * IBO * 2, chunk0 + 32 * wg, (int)y,
+                         smem_u32(b + (size_t)(h * T + 32 * wg) * ROWBO));
+        bulk_commit();
+    };
+
+    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+    for (int k = 0; sys < nsys; ++k, sys += per) {
+        unsigned char* cur = (k & 1) ? buf1 : buf0;
+        unsigned char* nxt = (k & 1) ? buf0 : buf1;
+        const bool more = sys + per < nsys;
+        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+        ok = group_and(g.bar_id, g.nthr, ok);
+        if (!ok) {
+            if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
+            break;
+        }
+        double* rec = red + ((size_t)sys * NS + c) * kLgRed;
+        double be[R + KL + KU];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
+            be[KL + 2 * u] = v.x;
+            be[KL + 2 * u + 1] = v.y;
+        }
+        if constexpr (KL > 0) {
+            double2 pv = make_double2(0.0, 0.0);
+            if (t > 0) {
+                pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
+            } else if (PASS == 1) {
+                pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
+                rec[kLgRedLo] = pv.x;
+                rec[kLgRedLo + 1] = pv.y;
+            } else {
+                pv = make_double2(rec[kLgRedLo], rec[kLgRedLo + 1]);
+            }
+            be[KL - 1] = pv.y;
+            if constexpr (KL > 1) be[0] = pv.x;
+        }
+        if constexpr (KU > 0) {
+            double2 nv = make_double2(0.0, 0.0);
+            if (t < T - 1) {
+                nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
+            } else if (PASS == 1) {
+                nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
+                rec[kLgRedHi] = nv.x;
+                rec[kLgRedHi + 1] = nv.y;
+            } else {
+                nv = make_double2(rec[kLgRedHi], rec[kLgRedHi + 1]);
+            }
+            be[KL + R] = nv.x;
+            if constexpr (KU > 1) be[KL + R + 1] = nv.y;
+        }
+        if (win_partial) {
+#pragma unroll
+            for (int i = 0; i < R + KL + KU; ++i) {
+                const int64_t row = s_glob - KL + i;
+                if (row < io.iz0 || row >= io.iz1) be[i] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            double2 wc[NB];
+#pragma unroll
+            for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int j = 2 * u + e;
+                double acc = (e ? wc[0].y : wc[0].x) * be[j];
+#pragma unroll
+                for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
+                be[j] = acc;
+            }
+        }
+        double (&x)[R + KL + KU] = be;
+        // `nxt` was read in the previous iteration by every warp of the group
+        // (all of them have passed this iteration's group_and since) and, in
+        // pass 2, stored from: once this warp's stores have read it, it takes
+        // the next system
+        if (more && lane == 0) {
+            if (PASS == 2) bulk_wait_read_all();
+            issue_load(nxt, (k & 1) ? bar0 : bar1, sys + per);
+        }
+        if constexpr (PASS == 1) {
+            lg_solve<C>(g, coef, Af, Ab, x,
+                        [&](double, double Bt) {
+                            if (t == T - 1) rec[kLgRedBf] = Bt;
+                            return 0.0;
+                        },
+                        [&](double, double Bt) {
+                            if (t == 0) rec[kLgRedBb] = Bt;
+                            return 0.0;
+                        });
+            continue;
+        } else {
+            // carries of this system's slice, from the carry kernel
+            const double Xc = BC::FWD ? rec[kLgRedX] : 0.0, Yc = BC::BWD ? rec[kLgRedY] : 0.0;
+            lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
+        }
+        if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int h = u / IBO, uu = u % IBO;
+            *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
+                make_double2(x[2 * u], x[2 * u + 1]);
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) issue_store(cur, sys);
+    }
+    if (lane == 0) bulk_wait_all();
+}
+
+}  // namespace pfb

@@ -95,6 +95,21 @@ struct ClusterVariant {
     int (*max_clusters)(size_t smem);  // clusters that fit the device at once (0: none)
 };
 const ClusterVariant* find_cluster_variant(int C, int KL, int KU, int SV);
+
+// Long systems in two passes (no cross-CTA waits): slices of S = 32 W R rows,
+// G systems in flight per CTA; launch = pass 1, the carry kernel (solves
+// only) and pass 2 on the stream.
+// red: nsys * NS records of 8 doubles, cst: NS records of 4 doubles.
+struct LongVariant {
+    int R, W, G, KL, KU, SV, S;
+    int IB, IBO;
+    cudaError_t (*launch)(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
+                          const JwOperator& op, const JwIO& io, double* red, double* cst, int NS);
+    int (*blocks_per_sm)();  // resident CTAs per SM (0: does not fit)
+};
+constexpr int kLongShapes = 3;  // compiled shapes per operator kind, in order of preference
+const LongVariant* find_long_variant(int shape, int KL, int KU, int SV);
+unsigned long_status_fetch_clear();
 unsigned cluster_status_fetch_clear();
 // Status word of the streaming kernels' bounded waits since the last call
 // (0: none timed out); reading it synchronises with the device.

@@ -1,0 +1,65 @@
+// long_variants.cu -- instantiations of the two-pass long-system JW-step
+// kernel (jw_long.cuh), their launch, and the status word of their waits.
+#include <cuda.h>
+
+#include "jw_long.cuh"
+#include "jw_variants.h"
+#include "plan.h"
+#include "stream_variant_defs.h"
+
+namespace pfb {
+
+template <class C>
+static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
+                                const JwOperator& op, const JwIO& io, double* red, double* cst, int NS)
+{
+    const size_t smem = lg_smem_bytes<C>();
+    jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, NS);
+    if (C::B::FWD || C::B::BWD)
+        jw_long_carry_kernel<C::B::FWD, C::B::BWD>
+            <<<(unsigned)((io.nsys + 127) / 128), 128, 0, st>>>(red, cst, NS, io.nsys);
+    jw_long_kernel<C, 2><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, NS);
+    return cudaPeekAtLastError();
+}
+
+// resident CTAs per SM of the two passes (0: does not fit)
+template <class C>
+static int lg_blocks_per_sm()
+{
+    const size_t smem = lg_smem_bytes<C>();
+    int b1 = 0, b2 = 0;
+    const void* f1 = (const void*)&jw_long_kernel<C, 1>;
+    const void* f2 = (const void*)&jw_long_kernel<C, 2>;
+    if (!allow_max_smem(f1) || !allow_max_smem(f2)) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, f1, C::NT, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return b1 < b2 ? b1 : b2;
+}
+
+#define PFB_LG(W, G, KL, KU, SV)                                                                      \
+    LongVariant{8, W, G, KL, KU, SV, LgCfg<8, W, G, KL, KU, SV>::S, LgCfg<8, W, G, KL, KU, SV>::B::IB, \
+                LgCfg<8, W, G, KL, KU, SV>::B::IBO, &lg_launch_fn<LgCfg<8, W, G, KL, KU, SV>>,        \
+                &lg_blocks_per_sm<LgCfg<8, W, G, KL, KU, SV>>}
+// slices of 512, 1024 and 2048 rows (2, 4, 8 warps x 32 threads x 8 rows),
+// 8, 4, 2 systems in flight per CTA
+#define PFB_LGK(KL, KU, SV) PFB_LG(4, 4, KL, KU, SV), PFB_LG(2, 8, KL, KU, SV), PFB_LG(8, 2, KL, KU, SV)
+
+static const LongVariant kLongVariants[] = {
+    PFB_LGK(0, 0, SV_TRI),   PFB_LGK(0, 1, SV_LOWER), PFB_LGK(0, 1, SV_NONE), PFB_LGK(0, 0, SV_LOWER),
+    PFB_LGK(1, 0, SV_UPPER), PFB_LGK(1, 0, SV_NONE),  PFB_LGK(0, 0, SV_UPPER),
+};
+
+const LongVariant* find_long_variant(int shape, int KL, int KU, int SV)
+{
+    int n = 0;
+    for (const LongVariant& v : kLongVariants)
+        if (v.KL == KL && v.KU == KU && v.SV == SV && n++ == shape) return &v;
+    return nullptr;
+}
+
+PFB_STREAM_STATUS_ACCESSOR(long_status_fetch_clear)
+
+}  // namespace pfb

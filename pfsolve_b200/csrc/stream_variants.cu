@@ -155,9 +155,9 @@ bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in,
 unsigned stream_status_fetch_clear()
 {
     const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
-    const unsigned d = steps_status_fetch_clear(), e = batch_status_fetch_clear();
-    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u) return ~0u;
-    return a | b | c | d | e;
+    const unsigned d = steps_status_fetch_clear(), e = batch_status_fetch_clear(), f = long_status_fetch_clear();
+    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u || f == ~0u) return ~0u;
+    return a | b | c | d | e | f;
 }
 
 }  // namespace pfb
