@@ -380,7 +380,8 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * groupsPerCTA = warps per CTA), else the K-step kernel; streaming = 5: long
  * systems (M > 4096) in two passes over slices of 32 x warpsPerSystem x
  * rowsPerThread rows, groupsPerCTA systems in flight per CTA (no waits
- * between CTAs; the plan holds a record of 64 bytes per system and slice).
+ * between CTAs; the plan holds a record of 64 bytes per system and slice and
+ * every slice's coefficient table).
  * No counterpart in the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);

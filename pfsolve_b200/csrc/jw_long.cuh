@@ -16,11 +16,16 @@
 //  * Within a slice the solve is the group kernel's: per-thread chunk
 //    recurrences and affine scans across the group.  The value entering the
 //    slice from below (forward) or above (backward) is the only coupling.
+//  * A table pass (PASS = 0, one CTA per slice) builds every slice's
+//    coefficient table once per launch -- the pivots entering a slice come
+//    from the Moebius product of all rows before it -- and writes it, with the
+//    slice's constants (below), to global memory; the two solve passes copy
+//    their slice's table from there.
 //  * Pass 1 (PASS = 1) solves every slice with both carries zero and writes,
 //    per (system, slice): the forward map's offset Bf (the value leaving the
 //    slice), the backward map's offset Bb0, and the slice's matvec halo input
 //    rows (so pass 2 never reads rows a neighbour slice may already have
-//    overwritten in place).  Every CTA also writes its slice's constants: the
+//    overwritten in place).  The slice constants of the table pass: the
 //    forward and backward multipliers Af, Ab, and Psi, the backward offset for
 //    a unit forward carry and zero input (the backward offset is affine in the
 //    forward carry: Bb = Bb0 + X Psi).
@@ -29,10 +34,8 @@
 //    backward ones from the top slice, Y_c = Ab_{c+1} Y_{c+1} + Bb0_{c+1} +
 //    X_{c+1} Psi_{c+1}, into the records.
 //  * Pass 2 solves its slice again with those carries and writes the result.
-//  Input is read twice and written once; the three launches are ordered on
-//  the stream, so no CTA ever waits for another.  The tridiagonal pivots entering
-//  a slice come from the Moebius product of all rows before it, which every
-//  CTA forms itself in its prologue.
+//  Input is read twice and written once; the four launches are ordered on
+//  the stream, so no CTA ever waits for another.
 //  * Completion waits are bounded: a wait that runs out records
 //    kStatusWaitTimeout and the group stops.
 #pragma once
@@ -50,6 +53,9 @@ struct LgCfg {
 // Per (system, slice) record, in doubles: forward offset and backward offset
 // (pass 1), halo rows below (KL <= 2) and above (KU <= 2) (pass 1), and the
 // carries entering the slice from below and from above (the carry kernel).
+// Stored slice-major, field k of system y in slice c at (c * kLgRed + k) *
+// nsys + y, so that the carry kernel's threads (one per system) read
+// consecutive addresses.
 constexpr int kLgRed = 8;
 constexpr int kLgRedBf = 0, kLgRedBb = 1, kLgRedLo = 2, kLgRedHi = 4, kLgRedX = 6, kLgRedY = 7;
 // Per slice constants: Af, Ab, Psi.
@@ -228,30 +234,32 @@ __global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__
 {
     const int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= nsys) return;
-    double* rs = red + (size_t)y * NS * kLgRed;
+    auto rs = [&](int c, int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + y]; };
     double X = 0.0;
     for (int c = 0; c < NS; ++c) {
-        rs[c * kLgRed + kLgRedX] = X;
-        if (FWD) X = __fma_rn(cst[c * kLgConst], X, rs[c * kLgRed + kLgRedBf]);
+        rs(c, kLgRedX) = X;
+        if (FWD) X = __fma_rn(cst[c * kLgConst], X, rs(c, kLgRedBf));
     }
     if (BWD) {
         double Y = 0.0;
         for (int c = NS - 1; c >= 0; --c) {
-            rs[c * kLgRed + kLgRedY] = Y;
-            const double Bb = FWD ? __fma_rn(rs[c * kLgRed + kLgRedX], cst[c * kLgConst + 2], rs[c * kLgRed + kLgRedBb])
-                                  : rs[c * kLgRed + kLgRedBb];
+            rs(c, kLgRedY) = Y;
+            const double Bb = FWD ? __fma_rn(rs(c, kLgRedX), cst[c * kLgConst + 2], rs(c, kLgRedBb)) : rs(c, kLgRedBb);
             Y = __fma_rn(cst[c * kLgConst + 1], Y, Bb);
         }
     }
 }
 
-// grid: CTAs in multiples of NS (CTA b owns slice b % NS); red: nsys * NS
-// records of kLgRed doubles; cst: NS records of kLgConst doubles.
+// PASS 0: grid NS (CTA c builds slice c's table into tab + c * TBL / 8 and
+// its constants into cst); PASS 1, 2: CTAs in multiples of NS (CTA b owns
+// slice b % NS).  red: io.nsys * NS records of kLgRed doubles; cst: NS
+// records of kLgConst doubles.
 template <class C, int PASS>
 __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ CUtensorMap tm_in,
                                                        const __grid_constant__ CUtensorMap tm_out,
                                                        const JwOperator op, const JwIO io, double* __restrict__ red,
-                                                       double* __restrict__ cst, const int NS)
+                                                       double* __restrict__ cst, double* __restrict__ tab,
+                                                       const int NS)
 {
     using BC = typename C::B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -275,7 +283,14 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
 
     if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(q4 + 8) + threadIdx.x), W);
     mbar_init_fence();
-    lg_prologue<C>(op, table, scratch, q4, c);
+    double* gtab = tab + (size_t)c * (BC::TBL / sizeof(double));
+    if constexpr (PASS == 0) {
+        lg_prologue<C>(op, table, scratch, q4, c);
+    } else {
+        const double2* src = reinterpret_cast<const double2*>(gtab);
+        double2* dst = reinterpret_cast<double2*>(table);
+        for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
+    }
     __syncthreads();
 
     GroupCtx g;
@@ -310,8 +325,13 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     }
 
     // Slice constants (Af, Ab, Psi): a solve of zero input with a unit
-    // forward carry, by group 0; written to cst by pass 1.
-    if (PASS == 1 && grp == 0) {
+    // forward carry, by group 0, and the table itself to global memory.
+    if constexpr (PASS == 0) {
+        double2* dst = reinterpret_cast<double2*>(gtab);
+        const double2* src = reinterpret_cast<const double2*>(table);
+        for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    if (PASS == 0 && grp == 0) {
         double x[R + KL + KU];
 #pragma unroll
         for (int i = 0; i < R + KL + KU; ++i) x[i] = 0.0;
@@ -332,6 +352,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             cst[c * kLgConst + 2] = psi;
         }
     }
+    if constexpr (PASS == 0) return;
 
     const int sw_me = swz_row<BC::SWB>(t), sw_prev = swz_row<BC::SWB>(t - 1), sw_next = swz_row<BC::SWB>(t + 1);
     const int swo_me = swz_row<BC::SWBO>(t);
@@ -374,7 +395,8 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
             break;
         }
-        double* rec = red + ((size_t)sys * NS + c) * kLgRed;
+        // field k of this (system, slice) record
+        auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
         double be[R + KL + KU];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -388,10 +410,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
             } else if (PASS == 1) {
                 pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
-                rec[kLgRedLo] = pv.x;
-                rec[kLgRedLo + 1] = pv.y;
+                rec(kLgRedLo) = pv.x;
+                rec(kLgRedLo + 1) = pv.y;
             } else {
-                pv = make_double2(rec[kLgRedLo], rec[kLgRedLo + 1]);
+                pv = make_double2(rec(kLgRedLo), rec(kLgRedLo + 1));
             }
             be[KL - 1] = pv.y;
             if constexpr (KL > 1) be[0] = pv.x;
@@ -402,10 +424,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
             } else if (PASS == 1) {
                 nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
-                rec[kLgRedHi] = nv.x;
-                rec[kLgRedHi + 1] = nv.y;
+                rec(kLgRedHi) = nv.x;
+                rec(kLgRedHi + 1) = nv.y;
             } else {
-                nv = make_double2(rec[kLgRedHi], rec[kLgRedHi + 1]);
+                nv = make_double2(rec(kLgRedHi), rec(kLgRedHi + 1));
             }
             be[KL + R] = nv.x;
             if constexpr (KU > 1) be[KL + R + 1] = nv.y;
@@ -443,17 +465,17 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         if constexpr (PASS == 1) {
             lg_solve<C>(g, coef, Af, Ab, x,
                         [&](double, double Bt) {
-                            if (t == T - 1) rec[kLgRedBf] = Bt;
+                            if (t == T - 1) rec(kLgRedBf) = Bt;
                             return 0.0;
                         },
                         [&](double, double Bt) {
-                            if (t == 0) rec[kLgRedBb] = Bt;
+                            if (t == 0) rec(kLgRedBb) = Bt;
                             return 0.0;
                         });
             continue;
         } else {
             // carries of this system's slice, from the carry kernel
-            const double Xc = BC::FWD ? rec[kLgRedX] : 0.0, Yc = BC::BWD ? rec[kLgRedY] : 0.0;
+            const double Xc = BC::FWD ? rec(kLgRedX) : 0.0, Yc = BC::BWD ? rec(kLgRedY) : 0.0;
             lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
         }
         if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];

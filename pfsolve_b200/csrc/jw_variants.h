@@ -97,14 +97,16 @@ struct ClusterVariant {
 const ClusterVariant* find_cluster_variant(int C, int KL, int KU, int SV);
 
 // Long systems in two passes (no cross-CTA waits): slices of S = 32 W R rows,
-// G systems in flight per CTA; launch = pass 1, the carry kernel (solves
-// only) and pass 2 on the stream.
-// red: nsys * NS records of 8 doubles, cst: NS records of 4 doubles.
+// G systems in flight per CTA; launch = the table pass, pass 1, the carry
+// kernel (solves only) and pass 2 on the stream.
+// red: nsys * NS records of 8 doubles, cst: NS records of 4 doubles, tab: NS
+// slice tables of tbl_bytes.
 struct LongVariant {
     int R, W, G, KL, KU, SV, S;
     int IB, IBO;
+    size_t tbl_bytes;
     cudaError_t (*launch)(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
-                          const JwOperator& op, const JwIO& io, double* red, double* cst, int NS);
+                          const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS);
     int (*blocks_per_sm)();  // resident CTAs per SM (0: does not fit)
 };
 constexpr int kLongShapes = 3;  // compiled shapes per operator kind, in order of preference

@@ -11,14 +11,15 @@ namespace pfb {
 
 template <class C>
 static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
-                                const JwOperator& op, const JwIO& io, double* red, double* cst, int NS)
+                                const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS)
 {
     const size_t smem = lg_smem_bytes<C>();
-    jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, NS);
+    jw_long_kernel<C, 0><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
+    jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
     if (C::B::FWD || C::B::BWD)
         jw_long_carry_kernel<C::B::FWD, C::B::BWD>
             <<<(unsigned)((io.nsys + 127) / 128), 128, 0, st>>>(red, cst, NS, io.nsys);
-    jw_long_kernel<C, 2><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, NS);
+    jw_long_kernel<C, 2><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
     return cudaPeekAtLastError();
 }
 
@@ -28,9 +29,10 @@ static int lg_blocks_per_sm()
 {
     const size_t smem = lg_smem_bytes<C>();
     int b1 = 0, b2 = 0;
+    const void* f0 = (const void*)&jw_long_kernel<C, 0>;
     const void* f1 = (const void*)&jw_long_kernel<C, 1>;
     const void* f2 = (const void*)&jw_long_kernel<C, 2>;
-    if (!allow_max_smem(f1) || !allow_max_smem(f2)) return 0;
+    if (!allow_max_smem(f0) || !allow_max_smem(f1) || !allow_max_smem(f2)) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, f1, C::NT, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess) {
         cudaGetLastError();
@@ -41,8 +43,8 @@ static int lg_blocks_per_sm()
 
 #define PFB_LG(W, G, KL, KU, SV)                                                                      \
     LongVariant{8, W, G, KL, KU, SV, LgCfg<8, W, G, KL, KU, SV>::S, LgCfg<8, W, G, KL, KU, SV>::B::IB, \
-                LgCfg<8, W, G, KL, KU, SV>::B::IBO, &lg_launch_fn<LgCfg<8, W, G, KL, KU, SV>>,        \
-                &lg_blocks_per_sm<LgCfg<8, W, G, KL, KU, SV>>}
+                LgCfg<8, W, G, KL, KU, SV>::B::IBO, LgCfg<8, W, G, KL, KU, SV>::B::TBL,               \
+                &lg_launch_fn<LgCfg<8, W, G, KL, KU, SV>>, &lg_blocks_per_sm<LgCfg<8, W, G, KL, KU, SV>>}
 // slices of 512, 1024 and 2048 rows (2, 4, 8 warps x 32 threads x 8 rows),
 // 8, 4, 2 systems in flight per CTA
 #define PFB_LGK(KL, KU, SV) PFB_LG(4, 4, KL, KU, SV), PFB_LG(2, 8, KL, KU, SV), PFB_LG(8, 2, KL, KU, SV)
