@@ -173,9 +173,9 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 }
 
 // Two-pass variant for long real systems: the first compiled shape that fits
-// (slices of 1024 rows, 4 systems in flight per CTA), with its per-(system,
-// slice) records allocated for the plan's right-hand sides (rows per thread
-// 8: M must be a multiple of 8).
+// and whose rows per thread divide M (16, else 8: M must be a multiple of 8),
+// with its per-(system, slice) records allocated for the plan's right-hand
+// sides.
 bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {
     s->long_v = nullptr;
@@ -185,6 +185,7 @@ bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
     for (int shape = 0; shape < kLongShapes; ++shape) {
         const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
         if (!v) return false;
+        if (M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
         const int b = v->blocks_per_sm();
         if (b < 1) continue;
         const int NS = (int)((M + v->S - 1) / v->S);

@@ -41,13 +41,14 @@ static int lg_blocks_per_sm()
     return b1 < b2 ? b1 : b2;
 }
 
-#define PFB_LG(W, G, KL, KU, SV)                                                                      \
-    LongVariant{8, W, G, KL, KU, SV, LgCfg<8, W, G, KL, KU, SV>::S, LgCfg<8, W, G, KL, KU, SV>::B::IB, \
-                LgCfg<8, W, G, KL, KU, SV>::B::IBO, LgCfg<8, W, G, KL, KU, SV>::B::TBL,               \
-                &lg_launch_fn<LgCfg<8, W, G, KL, KU, SV>>, &lg_blocks_per_sm<LgCfg<8, W, G, KL, KU, SV>>}
-// slices of 512, 1024 and 2048 rows (2, 4, 8 warps x 32 threads x 8 rows),
-// 8, 4, 2 systems in flight per CTA
-#define PFB_LGK(KL, KU, SV) PFB_LG(4, 4, KL, KU, SV), PFB_LG(2, 8, KL, KU, SV), PFB_LG(8, 2, KL, KU, SV)
+#define PFB_LG(R, W, G, KL, KU, SV)                                                                    \
+    LongVariant{R, W, G, KL, KU, SV, LgCfg<R, W, G, KL, KU, SV>::S, LgCfg<R, W, G, KL, KU, SV>::B::IB,     \
+                LgCfg<R, W, G, KL, KU, SV>::B::IBO, LgCfg<R, W, G, KL, KU, SV>::B::TBL,                    \
+                &lg_launch_fn<LgCfg<R, W, G, KL, KU, SV>>, &lg_blocks_per_sm<LgCfg<R, W, G, KL, KU, SV>>}
+// (rows per thread, warps per slice, systems in flight per CTA): slices of
+// 1024 rows with 16 rows per thread (the scans' cost spread over more rows),
+// then 1024 and 512 rows with 8 rows per thread
+#define PFB_LGK(KL, KU, SV) PFB_LG(16, 2, 8, KL, KU, SV), PFB_LG(8, 4, 4, KL, KU, SV), PFB_LG(16, 4, 2, KL, KU, SV)
 
 static const LongVariant kLongVariants[] = {
     PFB_LGK(0, 0, SV_TRI),   PFB_LGK(0, 1, SV_LOWER), PFB_LGK(0, 1, SV_NONE), PFB_LGK(0, 0, SV_LOWER),
