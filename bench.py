@@ -298,7 +298,8 @@ def extras_arm(args):
     solve + 2 FP64 refinement sweeps) with the mixed result's error against
     FP64, config 4 (one spectral timestep, l = 0..511, one persistent
     launch, captured CUDA graph, autotuned shape), K = 2 and 4 consecutive
-    steps in one launch, and the config 5 serving loop."""
+    steps in one launch, a long system (N = 16384) and the config 5 serving
+    loop."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -370,6 +371,9 @@ def extras_arm(args):
     # K consecutive steps in one launch (numConsecutiveJWIterations)
     for K in (2, 4):
         out[f"ksteps_K{K}_ub1_t10_N512_B131072"] = ksteps_measure(512, 131072, K, steps=10, warmup=3)
+    torch.cuda.empty_cache()
+    # long systems, beyond one CTA group (the reference's multi-upload range)
+    out["long_t13_N16384_B8192"] = long_measure(16384, 8192)
     torch.cuda.empty_cache()
     out["config5_serving"] = serving_leg()
     return out
@@ -456,6 +460,37 @@ def config3_profile(args):
     print(json.dumps({"profile_case": "config3", "M": M, "rhs": B, "refine": args.refine, "ms_per_step": ms,
                       "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9, "kernel": app.shape()}), flush=True)
     app.close()
+
+
+def long_measure(M, B, steps=10, warmup=3, path=0):
+    """A long tridiagonal system (config 3's coefficients at N = M rows), B
+    real right-hand sides in place, FP64: the two-pass long-system kernel
+    (path 2: the cluster kernel).  Algorithmic bytes: M rows read and written
+    per system."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App
+    wl = WL.config3(M=M, B=B)
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    x = torch.from_numpy(wl.rhs).cuda()
+    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
+              scaleC=1.0, kernelPath=path)
+    for _ in range(max(1, warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    shape = app.shape()
+    app.close()
+    del x, tb
+    return {"M": M, "rhs": B, "ms": ms, "rhs_per_s": B / (ms * 1e-3), "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9,
+            "kernel": shape}
 
 
 def ksteps_measure(M, B, K, steps=20, warmup=5, rows=0, path=0):

@@ -192,7 +192,7 @@ bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         const int64_t res = (int64_t)b * s->num_sms;
         // CTAs in whole multiples of NS, at most one CTA's worth of systems each
         const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
-        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 4) * sizeof(double) + (size_t)NS * v->tbl_bytes;
+        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) + (size_t)NS * v->tbl_bytes;
         if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
             cudaGetLastError();
             s->long_red = nullptr;
@@ -527,12 +527,12 @@ PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cud
     const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, io);
     if (!e) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     double* cst = s->long_red + (size_t)s->long_batch * s->long_NS * 8;
-    double* tab = cst + (size_t)s->long_NS * 4;
+    double* tab = cst + (size_t)s->long_NS * 8;
     const cudaError_t err =
         v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, tab, s->long_NS);
     note_launch(true);
-    // the table pass, the carry kernel (solves only) and pass 2
-    g_launches.fetch_add(s->sv != SV_NONE ? 3 : 2, std::memory_order_relaxed);
+    // the table passes, the carry kernel (solves only) and pass 2
+    g_launches.fetch_add((s->sv != SV_NONE ? 3 : 2) + (s->sv == SV_TRI ? 1 : 0), std::memory_order_relaxed);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;

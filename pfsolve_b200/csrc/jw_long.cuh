@@ -16,11 +16,13 @@
 //  * Within a slice the solve is the group kernel's: per-thread chunk
 //    recurrences and affine scans across the group.  The value entering the
 //    slice from below (forward) or above (backward) is the only coupling.
-//  * A table pass (PASS = 0, one CTA per slice) builds every slice's
-//    coefficient table once per launch -- the pivots entering a slice come
-//    from the Moebius product of all rows before it -- and writes it, with the
-//    slice's constants (below), to global memory; the two solve passes copy
-//    their slice's table from there.
+//  * Two table passes, one CTA per slice, build every slice's coefficient
+//    table once per launch: the first (PASS = 3, tridiagonal solves only)
+//    writes the Moebius product of each slice's pivot recurrence, the second
+//    (PASS = 0) composes those of the slices below it -- the pivot entering
+//    the slice -- builds the table and writes it, with the slice's constants
+//    (below), to global memory; the two solve passes copy their slice's
+//    table from there.
 //  * Pass 1 (PASS = 1) solves every slice with both carries zero and writes,
 //    per (system, slice): the forward map's offset Bf (the value leaving the
 //    slice), the backward map's offset Bb0, and the slice's matvec halo input
@@ -58,8 +60,10 @@ struct LgCfg {
 // consecutive addresses.
 constexpr int kLgRed = 8;
 constexpr int kLgRedBf = 0, kLgRedBb = 1, kLgRedLo = 2, kLgRedHi = 4, kLgRedX = 6, kLgRedY = 7;
-// Per slice constants: Af, Ab, Psi.
-constexpr int kLgConst = 4;
+// Per slice constants: Af, Ab, Psi, then the Moebius product of the slice's
+// rows (tridiagonal pivots; 4 doubles at kLgConstMob).
+constexpr int kLgConst = 8;
+constexpr int kLgConstMob = 4;
 
 template <class C>
 __host__ __device__ constexpr size_t lg_smem_bytes()
@@ -69,10 +73,12 @@ __host__ __device__ constexpr size_t lg_smem_bytes()
 }
 
 // ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
-// of the CTA; the pivots entering the slice come from the Moebius product of
-// rows [0, c*S), formed here as well.
-template <class C>
-__device__ void lg_prologue(const JwOperator& op, double* table, double* scratch, double* q4, int c)
+// of the CTA; the pivots entering the slice come from the Moebius products
+// of the slices below it (cst, written by the PASS = 3 launch).  With
+// AGG_ONLY the CTA instead writes its own slice's product there.
+template <class C, bool AGG_ONLY = false>
+__device__ void lg_prologue(const JwOperator& op, double* table, double* scratch, double* q4, int c,
+                            double* __restrict__ cst)
 {
     using BC = typename C::B;
     constexpr int R = C::R, U = BC::U, NB = BC::NB, S = C::S;
@@ -101,36 +107,42 @@ __device__ void lg_prologue(const JwOperator& op, double* table, double* scratch
     const int Rp = (S + nthr - 1) / nthr;
     const int64_t s = s0 + (int64_t)tid * Rp;
     if constexpr (C::SV == SV_TRI) {
-        // (1) Q = product over rows [0, s0), spread over the CTA's threads
-        if (s0 > 0) {
-            const int64_t Rq = (s0 + nthr - 1) / nthr;
-            double a = 1, b = 0, cc = 0, d = 1;
-            for (int64_t i = (int64_t)tid * Rq; i < (int64_t)(tid + 1) * Rq && i < s0; ++i) mstep(i, a, b, cc, d);
-            const double pa = a, pb = b, pc = cc, pd = d;
-            group_matrix_scan(g, a, b, cc, d);
-            if (tid == nthr - 1) {
-                double na = pa * a + pb * cc, nb = pa * b + pb * d, nc = pc * a + pd * cc, nd = pc * b + pd * d;
-                renorm2x2(na, nb, nc, nd);
-                q4[0] = na;
-                q4[1] = nb;
-                q4[2] = nc;
-                q4[3] = nd;
-            }
-        } else if (tid == 0) {
-            q4[0] = 1.0;
-            q4[1] = 0.0;
-            q4[2] = 0.0;
-            q4[3] = 1.0;
-        }
-        __syncthreads();
-        const double qa = q4[0], qc = q4[2];  // Q applied to (1, 0)^T
-        // (2) this thread's rows of the slice, after the preceding threads' and Q
+        // this thread's rows of the slice, then the product of the slice's
+        // preceding chunks
         double a = 1, b = 0, cc = 0, d = 1;
         for (int j = 0; j < Rp; ++j) {
             const int64_t i = s + j;
             if (i < s0 + S) mstep(i, a, b, cc, d);
         }
-        group_matrix_scan(g, a, b, cc, d);  // product of the slice's preceding chunks
+        const double pa = a, pb = b, pc = cc, pd = d;
+        group_matrix_scan(g, a, b, cc, d);
+        if constexpr (AGG_ONLY) {
+            // the slice's product = last thread's own * its preceding
+            if (tid == nthr - 1) {
+                double na = pa * a + pb * cc, nb = pa * b + pb * d, nc = pc * a + pd * cc, nd = pc * b + pd * d;
+                renorm2x2(na, nb, nc, nd);
+                double* o = cst + c * kLgConst + kLgConstMob;
+                o[0] = na;
+                o[1] = nb;
+                o[2] = nc;
+                o[3] = nd;
+            }
+            return;
+        }
+        // Q = product of the slices below: agg[c-1] * ... * agg[0]
+        double qa = 1, qb = 0, qc = 0, qd = 1;
+        for (int r = 0; r < c; ++r) {
+            const double* o = cst + r * kLgConst + kLgConstMob;
+            double na = o[0] * qa + o[1] * qc, nb = o[0] * qb + o[1] * qd, nc = o[2] * qa + o[3] * qc,
+                   nd = o[2] * qb + o[3] * qd;
+            renorm2x2(na, nb, nc, nd);
+            qa = na;
+            qb = nb;
+            qc = nc;
+            qd = nd;
+        }
+        (void)q4;
+        // full prefix = (slice prefix) * Q; incoming vector = prefix * (1, 0)^T
         const double fa = a * qa + b * qc, fc = cc * qa + d * qc;
         dprev = (s == 0) ? 1.0 : fa / fc;
     }
@@ -250,8 +262,9 @@ __global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__
     }
 }
 
-// PASS 0: grid NS (CTA c builds slice c's table into tab + c * TBL / 8 and
-// its constants into cst); PASS 1, 2: CTAs in multiples of NS (CTA b owns
+// PASS 3: grid NS (CTA c writes slice c's pivot product into cst, tridiagonal
+// only); PASS 0: grid NS (CTA c builds slice c's table into tab + c * TBL / 8
+// and its constants into cst); PASS 1, 2: CTAs in multiples of NS (CTA b owns
 // slice b % NS).  red: io.nsys * NS records of kLgRed doubles; cst: NS
 // records of kLgConst doubles.
 template <class C, int PASS>
@@ -284,8 +297,11 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(q4 + 8) + threadIdx.x), W);
     mbar_init_fence();
     double* gtab = tab + (size_t)c * (BC::TBL / sizeof(double));
-    if constexpr (PASS == 0) {
-        lg_prologue<C>(op, table, scratch, q4, c);
+    if constexpr (PASS == 3) {
+        lg_prologue<C, true>(op, table, scratch, q4, c, cst);
+        return;
+    } else if constexpr (PASS == 0) {
+        lg_prologue<C>(op, table, scratch, q4, c, cst);
     } else {
         const double2* src = reinterpret_cast<const double2*>(gtab);
         double2* dst = reinterpret_cast<double2*>(table);

@@ -97,10 +97,10 @@ struct ClusterVariant {
 const ClusterVariant* find_cluster_variant(int C, int KL, int KU, int SV);
 
 // Long systems in two passes (no cross-CTA waits): slices of S = 32 W R rows,
-// G systems in flight per CTA; launch = the table pass, pass 1, the carry
-// kernel (solves only) and pass 2 on the stream.
-// red: nsys * NS records of 8 doubles, cst: NS records of 4 doubles, tab: NS
-// slice tables of tbl_bytes.
+// G systems in flight per CTA; launch = the table passes (two for a
+// tridiagonal solve), pass 1, the carry kernel (solves only) and pass 2 on the
+// stream.  red: nsys * NS records of 8 doubles, cst: NS records of 8 doubles,
+// tab: NS slice tables of tbl_bytes.
 struct LongVariant {
     int R, W, G, KL, KU, SV, S;
     int IB, IBO;

@@ -14,6 +14,7 @@ static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in
                                 const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS)
 {
     const size_t smem = lg_smem_bytes<C>();
+    if (C::SV == SV_TRI) jw_long_kernel<C, 3><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
     jw_long_kernel<C, 0><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
     jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
     if (C::B::FWD || C::B::BWD)
@@ -29,6 +30,8 @@ static int lg_blocks_per_sm()
 {
     const size_t smem = lg_smem_bytes<C>();
     int b1 = 0, b2 = 0;
+    const void* f3 = (const void*)&jw_long_kernel<C, 3>;
+    if (!allow_max_smem(f3)) return 0;
     const void* f0 = (const void*)&jw_long_kernel<C, 0>;
     const void* f1 = (const void*)&jw_long_kernel<C, 1>;
     const void* f2 = (const void*)&jw_long_kernel<C, 2>;
