@@ -192,7 +192,9 @@ bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         const int64_t res = (int64_t)b * s->num_sms;
         // CTAs in whole multiples of NS, at most one CTA's worth of systems each
         const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
-        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) + (size_t)NS * v->tbl_bytes;
+        // records, slice constants, slice tables, PASS 1 weights (16 bytes per row)
+        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) +
+                             (size_t)NS * v->tbl_bytes + (size_t)NS * v->S * 16;
         if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
             cudaGetLastError();
             s->long_red = nullptr;

@@ -23,10 +23,15 @@
 //    the slice -- builds the table and writes it, with the slice's constants
 //    (below), to global memory; the two solve passes copy their slice's
 //    table from there.
-//  * Pass 1 (PASS = 1) solves every slice with both carries zero and writes,
-//    per (system, slice): the forward map's offset Bf (the value leaving the
-//    slice), the backward map's offset Bb0, and the slice's matvec halo input
-//    rows (so pass 2 never reads rows a neighbour slice may already have
+//  * Pass 1 (PASS = 1) needs, per (system, slice), only the slice's offsets
+//    with both carries zero: the forward offset Bf (the value leaving the
+//    slice) and the backward offset Bb0.  Both are linear in the matvec result
+//    g of the slice's rows -- Bf = sum alpha_k g_k, Bb0 = sum beta_k g_k with
+//    alpha_k the product of the forward solve band over rows k+1.., gamma_i
+//    that of the backward band over rows ..i-1 and beta_k = gamma_k +
+//    nl_{k+1} beta_{k+1} -- so pass 1 is the matvec and two reductions, with
+//    alpha and beta formed once per launch by the table pass.  It writes them
+//    and the slice's matvec halo input rows (so pass 2 never reads rows a neighbour slice may already have
 //    overwritten in place).  The slice constants of the table pass: the
 //    forward and backward multipliers Af, Ab, and Psi, the backward offset for
 //    a unit forward carry and zero input (the backward offset is affine in the
@@ -65,11 +70,13 @@ constexpr int kLgRedBf = 0, kLgRedBb = 1, kLgRedLo = 2, kLgRedHi = 4, kLgRedX = 
 constexpr int kLgConst = 8;
 constexpr int kLgConstMob = 4;
 
+// Shared memory: table | scratch | 8 doubles | mbarriers | (align 1024) |
+// buffers | the slice's PASS 1 weights (alpha, beta per row, S * 16 bytes).
 template <class C>
 __host__ __device__ constexpr size_t lg_smem_bytes()
 {
     return C::B::TBL + (size_t)C::G * C::W * kScratchPerWarp * sizeof(double) + 8 * sizeof(double) +
-           (size_t)C::G * 2 * sizeof(uint64_t) + 1024 + (size_t)C::G * 2 * C::B::BUF;
+           (size_t)C::G * 2 * sizeof(uint64_t) + 1024 + (size_t)C::G * 2 * C::B::BUF + (size_t)C::S * 16;
 }
 
 // ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
@@ -292,6 +299,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
     unsigned char* buf0 = after + pad + (size_t)grp * 2 * BC::BUF;
     unsigned char* buf1 = buf0 + BC::BUF;
+    // PASS 1 weights: row tt * R + jj at [jj * T + tt] (consecutive threads,
+    // consecutive entries)
+    double2* ab_s = reinterpret_cast<double2*>(after + pad + (size_t)C::G * 2 * BC::BUF);
+    double2* ab_g = reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)c * C::S;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
 
     if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(q4 + 8) + threadIdx.x), W);
@@ -306,6 +317,8 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         const double2* src = reinterpret_cast<const double2*>(gtab);
         double2* dst = reinterpret_cast<double2*>(table);
         for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
+        if constexpr (PASS == 1)
+            for (int i = threadIdx.x; i < C::S; i += blockDim.x) ab_s[i] = ab_g[i];
     }
     __syncthreads();
 
@@ -368,7 +381,60 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             cst[c * kLgConst + 2] = psi;
         }
     }
-    if constexpr (PASS == 0) return;
+    if constexpr (PASS == 0) {
+        // PASS 1 weights of the slice, by group 0 (thread t: rows tR .. tR+R-1):
+        // gamma by a forward product scan, alpha by a backward product scan,
+        // beta by a backward affine scan of beta_k = gamma_k + nl_{k+1} beta_{k+1}
+        if (grp == 0) {
+            double nlv[R], nhv[R];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 l2 = BC::FWD ? coef(BC::P_NL, u) : make_double2(0.0, 0.0);
+                const double2 h2 = BC::BWD ? coef(BC::P_NH, u) : make_double2(1.0, 1.0);
+                nlv[2 * u] = l2.x;
+                nlv[2 * u + 1] = l2.y;
+                nhv[2 * u] = h2.x;
+                nhv[2 * u + 1] = h2.y;
+            }
+            double Ain, Bin, At, Bt;
+            double P = 1.0;
+#pragma unroll
+            for (int j = 0; j < R; ++j) P *= nhv[j];
+            group_affine_scan_map<true>(g, P, 0.0, Ain, Bin, At, Bt);
+            double gam[R];
+            double cur = Ain;  // product of the preceding chunks' bands
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                gam[j] = cur;
+                cur *= nhv[j];
+            }
+            P = 1.0;
+#pragma unroll
+            for (int j = 0; j < R; ++j) P *= nlv[j];
+            double Aa, Ba, At2, Bt2;
+            group_affine_scan_map<false>(g, P, 0.0, Aa, Ba, At2, Bt2);  // Aa: product of the later chunks' bands
+            // nl of the next chunk's first row (0 past the slice)
+            const double nl_after = (BC::FWD && t + 1 < T) ? tb[(BC::P_NL * U) * BC::TP + 1].x : 0.0;
+            double A = 1.0, Bl = 0.0;  // this chunk's beta map, entering value = beta of row (t+1)R
+#pragma unroll
+            for (int k = R - 1; k >= 0; --k) {
+                const double nn = (k == R - 1) ? nl_after : nlv[k + 1];
+                Bl = __fma_rn(nn, Bl, gam[k]);
+                A *= nn;
+            }
+            double Ab2, Bb2, At3, Bt3;
+            group_affine_scan_map<false>(g, A, Bl, Ab2, Bb2, At3, Bt3);
+            double beta = Bb2, alpha = Aa;  // entering this chunk from above (slice input 0)
+#pragma unroll
+            for (int k = R - 1; k >= 0; --k) {
+                const double nn = (k == R - 1) ? nl_after : nlv[k + 1];
+                beta = __fma_rn(nn, beta, gam[k]);
+                if (k < R - 1) alpha *= nlv[k + 1];
+                ab_g[k * T + t] = make_double2(BC::FWD ? alpha : 0.0, BC::BWD ? beta : 0.0);
+            }
+        }
+        return;
+    }
 
     const int sw_me = swz_row<BC::SWB>(t), sw_prev = swz_row<BC::SWB>(t - 1), sw_next = swz_row<BC::SWB>(t + 1);
     const int swo_me = swz_row<BC::SWBO>(t);
@@ -479,15 +545,41 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             issue_load(nxt, (k & 1) ? bar0 : bar1, sys + per);
         }
         if constexpr (PASS == 1) {
-            lg_solve<C>(g, coef, Af, Ab, x,
-                        [&](double, double Bt) {
-                            if (t == T - 1) rec(kLgRedBf) = Bt;
-                            return 0.0;
-                        },
-                        [&](double, double Bt) {
-                            if (t == 0) rec(kLgRedBb) = Bt;
-                            return 0.0;
-                        });
+            if constexpr (BC::FWD || BC::BWD) {
+                // Bf = sum alpha g, Bb0 = sum beta g over the slice
+                double sa = 0.0, sb = 0.0;
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const double2 w = ab_s[j * T + t];
+                    sa = __fma_rn(w.x, x[j], sa);
+                    sb = __fma_rn(w.y, x[j], sb);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sa += __shfl_xor_sync(FULL, sa, o);
+                    sb += __shfl_xor_sync(FULL, sb, o);
+                }
+                if (W > 1) {
+                    double* my = g.warp_area(wg) + 16;
+                    if (lane == 0) {
+                        my[0] = sa;
+                        my[1] = sb;
+                    }
+                    group_bar(g.bar_id, g.nthr);
+                    if (t == 0) {
+                        sa = 0.0;
+                        sb = 0.0;
+                        for (int w = 0; w < W; ++w) {
+                            sa += g.warp_area(w)[16];
+                            sb += g.warp_area(w)[17];
+                        }
+                    }
+                }
+                if (t == 0) {
+                    if constexpr (BC::FWD) rec(kLgRedBf) = sa;
+                    if constexpr (BC::BWD) rec(kLgRedBb) = sb;
+                }
+            }
             continue;
         } else {
             // carries of this system's slice, from the carry kernel
