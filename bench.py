@@ -216,39 +216,55 @@ def gpu_arm(args, rank, world):
             print(json.dumps({"profile_case": True, "ncplx": nc, "ms_per_step": ms_max, "gbs": achieved,
                               "gpu_launches": int(launches), "kernel": jw.shape()}), flush=True)
         return
-    # Double-buffered on three streams: the H2D of step k+1 (PCIe up) overlaps
-    # the D2H of step k (PCIe down); each step still copies its whole input
-    # in and its whole result out inside the timed region.
+    # Double-buffered on three streams, in chunks: each step's systems are cut
+    # into CH chunks, each copied in (PCIe up), solved and copied out (PCIe
+    # down) on its own, so the two directions overlap chunk by chunk and the
+    # pipeline fills and drains in a chunk rather than a whole step.  Every
+    # step still copies its whole input in and its whole result out inside
+    # the timed region.
+    CH = 8 if nc % 8 == 0 else 1
+    ncc = nc // CH  # complex systems per chunk
     host_in = torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True)
     host_in.copy_(rhs.cpu())
     host_out = [torch.empty(2 * M * nc, dtype=torch.float64, pin_memory=True) for _ in range(2)]
     dev_in = [rhs, torch.empty_like(rhs)]
     dev_out = [out, torch.empty_like(out)]
     s_up, s_comp, s_down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
-    jw_e = App(device=local, stream=s_comp.cuda_stream, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * nc),
+    dg_e = App(device=local, stream=s_comp.cuda_stream, buffer=tA, outputBuffer=rhs, M_size=M, size=(M, 2 * ncc),
+               LDA=5, KU=2, KL=2, doublePrecision=1)
+    jw_e = App(device=local, stream=s_comp.cuda_stream, buffer=tb, outputBuffer=rhs, M_size=M, size=(M, 2 * ncc),
                upperBanded=2, jw_type=13, doublePrecision=1, scaleC=1.0, rowsPerThread=args.rows,
                kernelPath=args.path)
-    apps_e = [dg, jw_e, bl]
-    lps_e = [[dg.launch_params(outputBuffer=dev_in[b]), jw_e.launch_params(outputBuffer=dev_in[b]),
-              bl.launch_params(buffer=dev_in[b], outputBuffer=dev_out[b])] for b in range(2)]
-    ev_up = [torch.cuda.Event() for _ in range(2)]
-    ev_comp = [torch.cuda.Event() for _ in range(2)]
-    ev_down = [torch.cuda.Event() for _ in range(2)]
+    bl_e = App(device=local, stream=s_comp.cuda_stream, buffer=rhs, outputBuffer=out, M_size=M, size=(M, ncc),
+               block=7, doublePrecision=1)
+    apps_e = [dg_e, jw_e, bl_e]
+    span = 2 * M * ncc  # doubles of one chunk, in and out
+
+    def piece(t, c):
+        return t[c * span:(c + 1) * span]
+
+    lps_e = [[[dg_e.launch_params(outputBuffer=piece(dev_in[b], c)), jw_e.launch_params(outputBuffer=piece(dev_in[b], c)),
+               bl_e.launch_params(buffer=piece(dev_in[b], c), outputBuffer=piece(dev_out[b], c))] for c in range(CH)]
+             for b in range(2)]
+    ev_up = [[torch.cuda.Event() for _ in range(CH)] for _ in range(2)]
+    ev_comp = [[torch.cuda.Event() for _ in range(CH)] for _ in range(2)]
+    ev_down = [[torch.cuda.Event() for _ in range(CH)] for _ in range(2)]
 
     def e2e_step(k):
         b = k & 1
-        s_up.wait_event(ev_comp[b])  # the kernel of step k-2 has read dev_in[b]
-        with torch.cuda.stream(s_up):
-            dev_in[b].copy_(host_in, non_blocking=True)
-        ev_up[b].record(s_up)
-        s_comp.wait_event(ev_up[b])
-        s_comp.wait_event(ev_down[b])  # the D2H of step k-2 has read dev_out[b]
-        append_chain(apps_e, lps_e[b])
-        ev_comp[b].record(s_comp)
-        s_down.wait_event(ev_comp[b])
-        with torch.cuda.stream(s_down):
-            host_out[b].copy_(dev_out[b], non_blocking=True)
-        ev_down[b].record(s_down)
+        for c in range(CH):
+            s_up.wait_event(ev_comp[b][c])  # the solve of step k-2 has read this chunk of dev_in[b]
+            with torch.cuda.stream(s_up):
+                piece(dev_in[b], c).copy_(piece(host_in, c), non_blocking=True)
+            ev_up[b][c].record(s_up)
+            s_comp.wait_event(ev_up[b][c])
+            s_comp.wait_event(ev_down[b][c])  # the D2H of step k-2 has read this chunk of dev_out[b]
+            append_chain(apps_e, lps_e[b][c])
+            ev_comp[b][c].record(s_comp)
+            s_down.wait_event(ev_comp[b][c])
+            with torch.cuda.stream(s_down):
+                piece(host_out[b], c).copy_(piece(dev_out[b], c), non_blocking=True)
+            ev_down[b][c].record(s_down)
 
     e_steps = max(4, min(args.steps, 10))
     for k in range(2):
@@ -264,7 +280,8 @@ def gpu_arm(args, rank, world):
     torch.cuda.synchronize()
     e2e_ms = t0.elapsed_time(t1) / e_steps
     e2e_value = replicas.job_throughput(nc, replicas.max_over_ranks(e2e_ms, dev), world)
-    jw_e.close()
+    for a in apps_e:
+        a.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -284,8 +301,9 @@ def gpu_arm(args, rank, world):
                              "bytes_per_launch": bytes_alg},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * M * nc * 8,
                         "d2h_bytes_per_step": 2 * M * nc * 8, "steps": e_steps, "ms_per_step": e2e_ms,
-                        "pipeline": "pinned host buffers; H2D, kernel and D2H on three streams, double-buffered: "
-                                    "step k+1's upload overlaps step k's download"},
+                        "pipeline": f"pinned host buffers; H2D, fused kernel and D2H on three streams, "
+                                    f"double-buffered, {CH} chunks per step: each chunk's upload overlaps the "
+                                    f"previous chunks' downloads", "chunks_per_step": CH},
                 "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
         if not args.no_extras and world == 1:
             line["extras"] = extras_arm(args)
