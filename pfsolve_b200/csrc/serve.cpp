@@ -15,8 +15,8 @@
 // With `streams` batches in flight, requests that arrive while others run are
 // admitted as soon as a stream and bytes free up, and their kernels overlap on
 // the device.  Mixed-precision batches prefer high-priority streams;
-// double-double batches (one launch per request) use only the low-priority
-// ones and take at most kDdBatch requests.
+// double-double requests run one per flight (one launch each) on the
+// low-priority ones.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -322,10 +322,11 @@ int free_flight(PfSolveServer* s, int cls)
     return -1;
 }
 
-// Double-double requests run one launch each, sequentially on their stream,
-// a few per batch and only on the low-priority streams, so that short
-// mixed-precision batches are never queued behind them.
-constexpr int kDdBatch = 4;
+// Double-double requests run one launch each, one request per flight and
+// only on the low-priority streams: short mixed-precision batches are never
+// queued behind them, and a short double-double request never waits for a
+// long one batched with it (a flight completes as a whole).
+constexpr int kDdBatch = 1;
 
 // The request that opens the next batch: the first queued request whose class
 // has a free stream; nullptr when none has (or its bytes do not fit yet:
