@@ -511,6 +511,46 @@ def long_measure(M, B, steps=10, warmup=3, path=0):
             "kernel": shape}
 
 
+def dd_profile(args):
+    """Profiling case: config 3's weakly dominant tridiagonal system (N = --m)
+    in double-double, --ncplx right-hand sides: {hi, lo} storage
+    (quadDoubleDoublePrecision), or with --refine 1 double-double arithmetic
+    on FP64 storage (quadDoubleDoublePrecisionDoubleMemory).  Prints one JSON
+    line with the kernel time, the storage GB/s and the double-double FLOP
+    rate in FP64 operations (about 20 FP64 operations per double-double
+    multiply-add)."""
+    import torch
+
+    from oracle import oracle as O
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App
+    wl = WL.config3(M=args.m, B=args.ncplx)
+    M, B = wl.M, wl.nrhs
+    f64mem = args.refine == 1
+    bands = wl.jw_bands if f64mem else O.to_dd(wl.jw_bands)
+    rhs = wl.rhs if f64mem else O.to_dd(wl.rhs)
+    tb = torch.from_numpy(bands).cuda()
+    x = torch.from_numpy(rhs).cuda()
+    mode = dict(quadDoubleDoublePrecisionDoubleMemory=1) if f64mem else dict(quadDoubleDoublePrecision=1)
+    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=0,
+              scaleC=1.0, rowsPerThread=args.rows, **mode)
+    for _ in range(max(1, args.warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    word = 8 if f64mem else 16
+    print(json.dumps({"profile_case": "dd", "storage": "f64" if f64mem else "dd", "M": M, "rhs": B,
+                      "ms_per_step": ms, "gbs": 2.0 * M * word * B / (ms * 1e-3) / 1e9,
+                      "rhs_per_s": B / (ms * 1e-3), "kernel": app.shape()}), flush=True)
+    app.close()
+
+
 def ksteps_measure(M, B, K, steps=20, warmup=5, rows=0, path=0):
     """K consecutive JW steps in one launch (upperBanded 1, jw_type 10:
     bidiagonal matvec + lower bidiagonal solve per step, per-step band
@@ -604,9 +644,9 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps"],
-                    help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems) or "
-                         "config 4 (degrees 0..--lmax)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps", "dd"],
+                    help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems), "
+                         "config 4 (degrees 0..--lmax), K steps, or config 3's system in double-double")
     ap.add_argument("--lmax", type=int, default=511, help="config 4 profiling case: highest harmonic degree")
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
@@ -633,6 +673,9 @@ def main():
         return
     if args.profile and args.workload == "config4":
         config4_profile(args)
+        return
+    if args.profile and args.workload == "dd":
+        dd_profile(args)
         return
     if args.profile and args.workload == "ksteps":
         steps_profile(args)
