@@ -2,9 +2,9 @@
 
 Runs ``oracle/_ref/pfsolve_ref`` (the unmodified PfSolve library, compiled from
 its sources by ``make -C oracle ref``) on seeded inputs and stores inputs plus
-the reference's outputs as ``tests/golden/<case>.npz``.  Needs a CUDA GPU; run
-it as ``python tests/golden/make_golden.py --out gpurun_out/golden`` and copy the
-fixtures into ``tests/golden/``.  ``--time`` also times the reference's JW
+the reference's outputs as ``<out>/<case>.npz``.  Needs a CUDA GPU; run it as
+``python tests/golden/make_golden.py --out <dir>`` and copy the fixtures into
+``tests/golden/``.  ``--time`` also times the reference's JW
 kernel on the full-size configurations and writes ``ref_timing.json``.
 """
 from __future__ import annotations
@@ -257,7 +257,7 @@ def run_case(tmp, name, case, buf, rhs, prec):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--time", action="store_true")
     ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long"],
                     help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode; "
