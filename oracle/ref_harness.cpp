@@ -24,6 +24,23 @@
 #include <string>
 #include <vector>
 
+#include <csignal>
+#include <execinfo.h>
+#include <unistd.h>
+
+// Host crash report: the phase the harness was in and the return addresses
+// (offsets into this binary, for addr2line), written to stderr.
+static const char* volatile g_phase = "setup";
+
+static void on_crash(int sig)
+{
+    void* frames[48];
+    int n = backtrace(frames, 48);
+    dprintf(2, "signal %d in phase %s\n", sig, g_phase);
+    backtrace_symbols_fd(frames, n, 2);
+    _exit(128 + sig);
+}
+
 static std::map<std::string, std::string> read_params(const std::string& path)
 {
     std::map<std::string, std::string> kv;
@@ -60,6 +77,8 @@ int main(int argc, char** argv)
 {
     if (argc < 2) { fprintf(stderr, "usage: %s <case_dir>\n", argv[0]); return 2; }
     std::string dir = argv[1];
+    signal(SIGSEGV, on_crash);
+    signal(SIGABRT, on_crash);
     auto kv = read_params(dir + "/params.txt");
     auto I = [&](const char* k, long long d) { return kv.count(k) ? atoll(kv[k].c_str()) : d; };
     auto D = [&](const char* k, double d) { return kv.count(k) ? atof(kv[k].c_str()) : d; };
@@ -131,6 +150,10 @@ int main(int argc, char** argv)
     cfg.block = (int)I("block", 0);
     cfg.lshift = (int)I("lshift", 0);
     cfg.disableCaching = 1;  // no kernel cache files are written or read
+    // code-generation buffers (0 keeps the reference's defaults: 4 000 000 and
+    // 5 000 chars); its double-double kernels need a larger intermediate buffer
+    cfg.maxCodeLength = I("maxCodeLength", 0);
+    cfg.maxTempLength = I("maxTempLength", 0);
     cfg.device = &dev;
 
     void* bufArr[16] = {cfg.block ? d_in : d_bands};
@@ -151,6 +174,7 @@ int main(int argc, char** argv)
     cfg.outputBufferSize = outSizeArr;
     cfg.kernelSize = outSizeArr;
 
+    g_phase = "initializePfSolve";
     PfSolveResult r = initializePfSolve(&app, cfg);
     if (r != PFSOLVE_SUCCESS) { fprintf(stderr, "initializePfSolve: %d\n", (int)r); return 10; }
 
@@ -169,8 +193,10 @@ int main(int argc, char** argv)
     lp.inputBufferStride = I("run_inputBufferStride", cfg.size[0]);
     lp.outputBufferStride = I("run_outputBufferStride", cfg.size[0]);
 
+    g_phase = "PfSolveAppend";
     r = PfSolveAppend(&app, 0, &lp);
     if (r != PFSOLVE_SUCCESS) { fprintf(stderr, "PfSolveAppend: %d\n", (int)r); return 11; }
+    g_phase = "after launch";
     cudaError_t ce = cudaDeviceSynchronize();
     if (ce != cudaSuccess) { fprintf(stderr, "sync: %s\n", cudaGetErrorString(ce)); return 12; }
     if (!rhs.empty()) {

@@ -237,6 +237,60 @@ def long_cases():
 REF_BIN_FP128 = os.path.join(ROOT, "oracle", "_ref", "pfsolve_ref_fp128")
 
 
+# The reference's double-double code generation stops with SIGSEGV inside
+# initializePfSolve whenever it moves a double-double constant into a
+# register: the constant is declared with the double-double type but only its
+# plain value is set (pfSolve_ReadWrite.h:1567-1568, moved at :1682 and
+# :1692; the same in pfSolve_TridiagonalSolve.h, e.g. :1048), so
+# PfCopyContainer (pfSolve_MathUtils.h:51-55) follows its unallocated
+# {hi, lo} parts.  The sequential-Thomas generation, taken only for M <= 32
+# with one step (pfSolve_Plan_JonesWorland.h:306), avoids those moves for the
+# bidiagonal kinds; those cases are the fixtures.  DD_CRASHING lists the
+# kinds and sizes seen to crash, kept to re-run the evidence (--only dd-crash).
+DD_PINNED = [(1, 10, 16), (1, 10, 32), (0, 13, 32)]
+DD_CRASHING = [(2, 13, 16), (2, 13, 32), (2, 13, 64), (2, 13, 256), (2, 13, 1000), (1, 10, 100), (1, 10, 512),
+               (0, 10, 32), (0, 10, 100), (0, 10, 512), (0, 13, 300)]
+
+
+def dd_cases(which=DD_PINNED):
+    """(name, Case, bands, rhs, precision) in double-double storage ({hi, lo}
+    pairs, non-zero lo parts), stored under tests/golden/dd/."""
+    out = []
+    for ub, jwt, M in which:
+        rng = np.random.default_rng(18000 + 100 * ub + jwt + M)
+        bands = WL.permute_bands(jw_bands(rng, M, ub), M)
+        case = O.Case(M=M, batch=2, upperBanded=ub, jw_type=jwt)
+        rhs = rng.uniform(-1, 1, case.rhs_len())
+        bdd = O.to_dd(bands)
+        bdd[1::2] = bands * rng.uniform(-1, 1, bands.shape) * 2.0 ** -60
+        rdd = O.to_dd(rhs)
+        rdd[1::2] = rhs * rng.uniform(-1, 1, rhs.shape) * 2.0 ** -60
+        out.append((f"dd_ub{ub}_t{jwt}_M{M}", case, bdd, rdd, "dd"))
+    return out
+
+
+def run_dd_case(tmp, name, case, buf, rhs):
+    """The reference's double-double JW app (default build first, then the
+    PfSolve_use_FP128 build).  Its code-generation buffers are raised above
+    the defaults (maxTempLength, maxCodeLength); that does not change the
+    crash described above.  A crash report carries the harness phase and the
+    return addresses, for addr2line on the same binary."""
+    import subprocess
+    d = os.path.join(tmp, name)
+    O.write_reference_case(d, case, buf, rhs, precision="dd")
+    with open(os.path.join(d, "params.txt"), "a") as f:
+        f.write(f"maxTempLength={1 << 20}\nmaxCodeLength={1 << 27}\n")
+    errs = []
+    for binary in (O.REF_BIN, REF_BIN_FP128):
+        if not os.path.exists(binary):
+            continue
+        r = subprocess.run([binary, d], capture_output=True, text=True, timeout=300)
+        if r.returncode == 0:
+            return np.fromfile(os.path.join(d, "out.bin"), dtype=np.float64), os.path.basename(binary)
+        errs.append(f"{os.path.basename(binary)} rc={r.returncode}: {r.stderr.strip()[-4000:]}")
+    raise RuntimeError("; ".join(errs))
+
+
 def run_case(tmp, name, case, buf, rhs, prec):
     d = os.path.join(tmp, name)
     if prec == "dd" and os.path.exists(REF_BIN_FP128):
@@ -259,9 +313,10 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--time", action="store_true")
-    ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long"],
+    ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long", "dd", "dd-crash"],
                     help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode; "
-                         "long: only long systems (N > 4352, and their timing with --time)")
+                         "long: only long systems (N > 4352, and their timing with --time); dd: only the double-double "
+                         "fixtures; dd-crash: the double-double cases the reference crashes on (no fixtures)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
@@ -385,6 +440,18 @@ def main():
         with open(os.path.join(args.out, "ref_timing_long.json"), "w") as f:
             json.dump(timing, f, indent=1)
         print(json.dumps(timing, indent=1))
+    ddir = os.path.join(args.out, "dd")
+    os.makedirs(ddir, exist_ok=True)
+    dd_set = {"all": DD_PINNED, "dd": DD_PINNED, "dd-crash": DD_CRASHING}.get(args.only, [])
+    for name, case, buf, rhs, prec in dd_cases(dd_set):
+        try:
+            ref, binary = run_dd_case(tmp, name, case, buf, rhs)
+            np.savez_compressed(os.path.join(ddir, name + ".npz"), params=json.dumps(asdict(case)),
+                                precision=prec, buffer=buf, rhs=rhs, ref_out=ref, binary=binary)
+            summary[name] = "ok"
+        except Exception as e:
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
     with open(os.path.join(args.out, "summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
     bad = [k for k, v in summary.items() if v != "ok"]
