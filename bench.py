@@ -392,6 +392,8 @@ def extras_arm(args):
     torch.cuda.empty_cache()
     # long systems, beyond one CTA group (the reference's multi-upload range)
     out["long_t13_N16384_B8192"] = long_measure(16384, 8192)
+    out["alt_t113_N1024_B131072"] = alt_measure(1024, 131072)
+    out["alt_t113_N1024_B131072_group"] = alt_measure(1024, 131072, path=1)
     torch.cuda.empty_cache()
     out["config5_serving"] = serving_leg()
     return out
@@ -493,6 +495,38 @@ def long_measure(M, B, steps=10, warmup=3, path=0):
     tb = torch.from_numpy(wl.jw_bands).cuda()
     x = torch.from_numpy(wl.rhs).cuda()
     app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
+              scaleC=1.0, kernelPath=path)
+    for _ in range(max(1, warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    shape = app.shape()
+    app.close()
+    del x, tb
+    return {"M": M, "rhs": B, "ms": ms, "rhs_per_s": B / (ms * 1e-3), "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9,
+            "kernel": shape}
+
+
+def alt_measure(M, B, steps=10, warmup=3, path=0):
+    """ALT stride-2 mode (jw_type 113: the even and the odd rows of each row
+    set are two tridiagonal systems), M rows per row set, B real row sets in
+    place, FP64: the streaming kernel (path 1: the group kernel).  Algorithmic
+    bytes: M rows read and written per row set."""
+    import numpy as np
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App
+    rng = np.random.default_rng(4242)
+    tb = torch.from_numpy(WL.alt_bands(rng, M, 2)).cuda()
+    x = torch.from_numpy(rng.uniform(-1, 1, M * B)).cuda()
+    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=113, doublePrecision=1,
               scaleC=1.0, kernelPath=path)
     for _ in range(max(1, warmup)):
         app.append()
@@ -644,9 +678,10 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps", "dd"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps", "dd", "alt"],
                     help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems), "
-                         "config 4 (degrees 0..--lmax), K steps, or config 3's system in double-double")
+                         "config 4 (degrees 0..--lmax), K steps, config 3's system in double-double, or ALT mode "
+                         "(--m rows per row set, --ncplx row sets)")
     ap.add_argument("--lmax", type=int, default=511, help="config 4 profiling case: highest harmonic degree")
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
@@ -679,6 +714,10 @@ def main():
         return
     if args.profile and args.workload == "ksteps":
         steps_profile(args)
+        return
+    if args.profile and args.workload == "alt":
+        print(json.dumps(alt_measure(args.m, args.ncplx, steps=args.steps, warmup=args.warmup, path=args.path)),
+              flush=True)
         return
     try:
         if args.impl == "reference":

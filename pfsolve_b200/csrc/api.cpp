@@ -126,8 +126,9 @@ int pick_rows_per_thread(int64_t M, int requested)
 
 // Streaming variant for M rows: rows per thread R (the caller's choice, else
 // the compiled R whose groups leave the fewest idle rows, 16 first), W warps
-// per system, and the most groups per CTA that fit shared memory.
-bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+// per system, and the most groups per CTA that fit shared memory.  ALT: M
+// counts the rows of a row set (both systems).
+bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool alt = false)
 {
     s->stream_v = nullptr;
     if ((s->prec != PREC_F64 && s->prec != PREC_MIXED) || s->no_stream) return false;
@@ -151,7 +152,7 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         }
     for (int i = 0; i < n; ++i) {
         const StreamVariant* v =
-            find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec);
+            find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, alt);
         if (!v) continue;
         const int T = 32 * v->W;
         for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
@@ -359,7 +360,13 @@ PfSolveResult plan_alt(AppState* s, const PfSolveConfiguration& c, int dd_prec)
     s->no_stream = true;  // group kernel: per-group parity, stride-2 rows
     s->no_tbl = true;     // the two parities have different coefficients
     const PfSolveResult r = finish_variant(s, n0, LAY_REAL, LAY_REAL, 0);
-    return (r == PFSOLVE_SUCCESS && !s->variant) ? PFSOLVE_ERROR_UNSUPPORTED_COMBINATION : r;
+    if (r != PFSOLVE_SUCCESS || !s->variant) return r == PFSOLVE_SUCCESS ? PFSOLVE_ERROR_UNSUPPORTED_COMBINATION : r;
+    // FP64: the streaming kernel stages whole row sets and solves their two
+    // systems together; the group kernel above takes the launches it cannot
+    // (partial output windows, unaligned rows) and kernelPath 1.
+    s->no_stream = c.kernelPath == 1;
+    if (s->prec == PREC_F64) choose_stream(s, M, LAY_REAL, LAY_REAL, 0, true);
+    return PFSOLVE_SUCCESS;
 }
 
 // Pick the kernel variant and launch shape for M rows: register variants
@@ -548,12 +555,15 @@ bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream
 {
     const StreamVariant* v = s->stream_v;
     if (!v || io.accumulate || io.oz0 > 0 || io.oz1 < io.M) return false;
-    const MapCacheEntry* e = stream_maps(v, io);
+    // ALT: the launch counts systems (two per row set); the kernel, row sets
+    JwIO rs = io;
+    if (v->ALT) rs.nsys = io.nsys / 2;
+    const MapCacheEntry* e = stream_maps(v, rs);
     if (!e) return false;
-    const int64_t want = (io.nsys + s->stream_G - 1) / s->stream_G;
+    const int64_t want = (rs.nsys + s->stream_G - 1) / s->stream_G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->stream_max_blocks));
     v->launch(dim3((unsigned)grid), dim3(32 * v->W * s->stream_G), v->smem_bytes(s->stream_G), stream, &e->in, &e->out,
-              op, io);
+              op, rs);
     return true;
 }
 

@@ -32,10 +32,19 @@ namespace pfb {
 constexpr unsigned kStatusWaitTimeout = 1u;
 static __device__ unsigned int g_stream_status;
 
-template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_, int PREC_ = PREC_F64>
+template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_, int PREC_ = PREC_F64,
+          int ALT_ = 0>
 struct StCfg {
     static constexpr int R = R_, W = W_, KL = KL_, KU = KU_, SV = SV_, LIN = LIN_, LOUT = LOUT_;
     static constexpr bool SCALE = SCALE_;
+    // ALT stride-2 mode (pfSolve_TridiagonalSolve.h:1319-1330, 1622-1644): the
+    // even rows and the odd rows of a staged row set are two systems.  A
+    // 16-byte unit holds rows 2u and 2u + 1, one row of each system with the
+    // same index in it, and a row's neighbours in its system are S = 2 rows
+    // away; the staged halo is S KL rows before and S KU rows after a chunk.
+    static constexpr bool ALT = ALT_ != 0;
+    static constexpr int S = ALT ? 2 : 1;
+    static constexpr int KLP = S * KL_, KUP = S * KU_;
     static constexpr bool CPLX = (LIN != LAY_REAL);
     using V = typename std::conditional<CPLX, double2, double>::type;
     using VF = typename Lower<V>::type;
@@ -81,11 +90,12 @@ struct StCfg {
     // solve vector); the launch bound leaves the compiler room for them:
     // 512 threads cap at 128 registers, 384 at 170, 256 at 255.  Complex
     // variants stay at 256 (measured faster than 384 on the config 2 chain).
-    static constexpr int kDataRegs = (R + KL + KU) * (CPLX ? 4 : 2) * (MIXED ? 3 : 1);
+    static constexpr int kDataRegs = (R + KLP + KUP) * (CPLX ? 4 : 2) * (MIXED ? 3 : 1);
     static constexpr int kMaxThreads =
         (kDataRegs >= 96 || (CPLX && kDataRegs >= 64)) ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
-    static_assert(KL <= 2 && KU <= 2, "halo of at most two rows");
+    static_assert(KLP <= 2 && KUP <= 2, "halo of at most two rows");
+    static_assert(!ALT || (!CPLX && !MIXED && !SCALE), "ALT: real FP64 systems without a Scale epilogue");
     static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");
     static_assert(W == 1 || kSameRows, "multi-warp groups need matching input/output rows");
 };
@@ -184,22 +194,14 @@ __device__ __forceinline__ int swz_row(int t)
 // [((p*U + j/2)*T + tt)*2 + (j&1)]: thread tt reads rows 2u, 2u+1 of a plane
 // as one 16-byte word, lanes on consecutive words.
 template <class C>
-__device__ void st_prologue(const JwOperator& op, double* table, double* scratch_all)
+__device__ void st_prologue_system(const JwOperator& op, int h, double* table, GroupCtx& g)
 {
     constexpr int R = C::R, T = C::T, U = C::U, NB = C::NB;
     const int64_t M = op.M;
-    const int rows = T * R;
+    const int rows = T * R / C::S;
     const int nthr = blockDim.x, tid = threadIdx.x;
     const int Rp = (rows + nthr - 1) / nthr;
     const int64_t s = (int64_t)tid * Rp;
-    GroupCtx g;
-    g.lane = tid & 31;
-    g.wg = tid >> 5;
-    g.W = nthr >> 5;
-    g.nthr = nthr;
-    g.bar_id = 1;
-    g.seq = 0;
-    g.scratch = scratch_all;
     double dprev = 1.0;
     if constexpr (C::SV == SV_TRI) {
         // Moebius product of this thread's rows, then the CTA-wide scan gives
@@ -253,7 +255,8 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
 #pragma unroll
             for (int k = 0; k < NB; ++k) w[k] = 0.0;
         }
-        const int tt = (int)(i / R), jj = (int)(i % R);
+        const int64_t si = C::S * i + h;  // staged row
+        const int tt = (int)(si / R), jj = (int)(si % R);
         auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 2 + (jj & 1)] = v; };
         auto put32 = [&](int p, int k, double v) {
             reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 4 + k + (jj & 1)] = (float)v;
@@ -277,6 +280,33 @@ __device__ void st_prologue(const JwOperator& op, double* table, double* scratch
     }
 }
 
+// Coefficient table of the staged system(s), built by all threads of the CTA.
+// ALT: system h is the parity-h rows, with its own row count and band
+// positions (the group kernel's per-parity operator, jw_step_kernel).
+template <class C>
+__device__ void st_prologue(const JwOperator& op, double* table, double* scratch_all)
+{
+    GroupCtx g;
+    g.lane = threadIdx.x & 31;
+    g.wg = threadIdx.x >> 5;
+    g.W = blockDim.x >> 5;
+    g.nthr = blockDim.x;
+    g.bar_id = 1;
+    g.seq = 0;
+    g.scratch = scratch_all;
+    if constexpr (!C::ALT) {
+        st_prologue_system<C>(op, 0, table, g);
+    } else {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            JwOperator oph = op;
+            oph.alt_h = h;
+            oph.M = (op.M - h + 1) >> 1;
+            st_prologue_system<C>(oph, h, table, g);
+        }
+    }
+}
+
 // ---- The kernel.
 template <class C>
 __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_constant__ CUtensorMap tm_in,
@@ -286,7 +316,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using V = typename C::V;
     using O = VOps<V>;
-    constexpr int R = C::R, W = C::W, T = C::T, U = C::U, KL = C::KL, KU = C::KU, NB = C::NB;
+    constexpr int R = C::R, W = C::W, T = C::T, U = C::U, NB = C::NB, S = C::S;
+    constexpr int KL = C::KLP, KU = C::KUP;  // staged halo rows (S times the band halo)
     constexpr int IB = C::IB, H = C::H, IBO = C::IBO, HO = C::HO;
     const int G = blockDim.x / T;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -354,22 +385,34 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
     // Scan multipliers: products of -l and -h over this thread's chunk (in the
     // precision of the solve that uses them).
-    double Af = 1.0, Ab = 1.0;
+    // ALT: one multiplier per system, Af / Ab for the even rows and Af1 / Ab1
+    // for the odd rows.
+    double Af = 1.0, Ab = 1.0, Af1 = 1.0, Ab1 = 1.0;
     float Af32 = 1.0f, Ab32 = 1.0f;
     if constexpr (C::FWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const double2 c = coef(C::P_NL, u);
-            Af = (u == 0) ? c.x : c.x * Af;
-            Af = c.y * Af;
+            if constexpr (C::ALT) {
+                Af = c.x * Af;
+                Af1 = c.y * Af1;
+            } else {
+                Af = (u == 0) ? c.x : c.x * Af;
+                Af = c.y * Af;
+            }
         }
     }
     if constexpr (C::BWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const double2 c = coef(C::P_NH, u);
-            Ab = c.x * Ab;
-            Ab = c.y * Ab;
+            if constexpr (C::ALT) {
+                Ab = c.x * Ab;
+                Ab1 = c.y * Ab1;
+            } else {
+                Ab = c.x * Ab;
+                Ab = c.y * Ab;
+            }
         }
     }
     if constexpr (C::FWD && C::MIXED) {
@@ -501,7 +544,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 const int j = 2 * u + e;
                 V acc = O::mul(e ? wc[0].y : wc[0].x, be[j]);
 #pragma unroll
-                for (int q = 1; q < NB; ++q) acc = O::fma(e ? wc[q].y : wc[q].x, be[j + q], acc);
+                for (int q = 1; q < NB; ++q) acc = O::fma(e ? wc[q].y : wc[q].x, be[j + S * q], acc);
                 be[j] = acc;
             }
         }
@@ -594,7 +637,27 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
             }
         }
-        if constexpr (C::FWD && !C::MIXED) {
+        if constexpr (C::FWD && !C::MIXED && C::ALT) {
+            // the same per system: z_j = x_j - l_j z_{j-2}, one scan each
+#pragma unroll
+            for (int u = 1; u < U; ++u) {
+                const double2 c = coef(C::P_NL, u);
+                x[2 * u] = O::fma(c.x, x[2 * u - 2], x[2 * u]);
+                x[2 * u + 1] = O::fma(c.y, x[2 * u - 1], x[2 * u + 1]);
+            }
+            const V pin0 = group_affine_scan<V, double, true>(g, Af, x[R - 2]);
+            const V pin1 = group_affine_scan<V, double, true>(g, Af1, x[R - 1]);
+            double p0 = 1.0, p1 = 1.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 c = coef(C::P_NL, u);
+                p0 = c.x * p0;
+                x[2 * u] = O::fma(p0, pin0, x[2 * u]);
+                p1 = c.y * p1;
+                x[2 * u + 1] = O::fma(p1, pin1, x[2 * u + 1]);
+            }
+        }
+        if constexpr (C::FWD && !C::MIXED && !C::ALT) {
             // z_j = x_j - l_j z_{j-1} within the chunk, then add the coupling
             // from the preceding chunks scaled by prod_{k<=j}(-l_k)
 #pragma unroll
@@ -614,7 +677,26 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 x[2 * u + 1] = O::fma(p, pin, x[2 * u + 1]);
             }
         }
-        if constexpr (C::BWD && !C::MIXED) {
+        if constexpr (C::BWD && !C::MIXED && C::ALT) {
+#pragma unroll
+            for (int u = U - 2; u >= 0; --u) {
+                const double2 c = coef(C::P_NH, u);
+                x[2 * u + 1] = O::fma(c.y, x[2 * u + 3], x[2 * u + 1]);
+                x[2 * u] = O::fma(c.x, x[2 * u + 2], x[2 * u]);
+            }
+            const V q0 = group_affine_scan<V, double, false>(g, Ab, x[0]);
+            const V q1 = group_affine_scan<V, double, false>(g, Ab1, x[1]);
+            double p0 = 1.0, p1 = 1.0;
+#pragma unroll
+            for (int u = U - 1; u >= 0; --u) {
+                const double2 c = coef(C::P_NH, u);
+                p1 = c.y * p1;
+                x[2 * u + 1] = O::fma(p1, q1, x[2 * u + 1]);
+                p0 = c.x * p0;
+                x[2 * u] = O::fma(p0, q0, x[2 * u]);
+            }
+        }
+        if constexpr (C::BWD && !C::MIXED && !C::ALT) {
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
                 const double2 c = coef(C::P_NH, u);

@@ -74,9 +74,10 @@ struct StreamVariant {
     int IB, IBO;
     void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
                    const JwOperator& op, const JwIO& io);
+    int ALT = 0;  // ALT stride-2 mode: one staged row set holds two systems (its even and odd rows)
 };
 const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE,
-                                        int PREC);
+                                        int PREC, int ALT = 0);
 // Tensor maps of a launch's input and output rows; false when the buffers'
 // alignment, strides or M do not allow the streaming layout.
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out);

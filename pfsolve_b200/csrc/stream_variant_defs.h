@@ -30,6 +30,20 @@ inline void st_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, co
                   StCfg<R, W, KL, KU, SV, LIN, LOUT, SC, P>::IB, StCfg<R, W, KL, KU, SV, LIN, LOUT, SC, P>::IBO, \
                   &st_launch_fn<StCfg<R, W, KL, KU, SV, LIN, LOUT, SC, P>>}
 #define PFB_SV(R, W, KL, KU, SV, LIN, LOUT, SC) PFB_SVP(R, W, KL, KU, SV, LIN, LOUT, SC, PREC_F64)
+// ALT stride-2 mode: real FP64 row sets, each holding two systems
+#define PFB_SVA(R, W, KL, KU, SV)                                                                              \
+    StreamVariant{R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64,                                      \
+                  StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>::kMaxThreads,                \
+                  (const void*)&jw_stream_kernel<StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>>, \
+                  &st_smem_fn<StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>>,                 \
+                  StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>::IB,                          \
+                  StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>::IBO,                         \
+                  &st_launch_fn<StCfg<R, W, KL, KU, SV, LAY_REAL, LAY_REAL, false, PREC_F64, 1>>, 1}
+// 8, 16 and 32 rows per thread, 1, 2 and 4 warps per row set (M <= 4096)
+#define PFB_SALT(KL, KU, SV)                                                                                  \
+    PFB_SVA(8, 1, KL, KU, SV), PFB_SVA(8, 2, KL, KU, SV), PFB_SVA(8, 4, KL, KU, SV), PFB_SVA(16, 1, KL, KU, SV), \
+        PFB_SVA(16, 2, KL, KU, SV), PFB_SVA(16, 4, KL, KU, SV), PFB_SVA(32, 1, KL, KU, SV),                    \
+        PFB_SVA(32, 2, KL, KU, SV), PFB_SVA(32, 4, KL, KU, SV)
 // real systems: 8 rows per thread (M <= 256, 512, 1024), 16 (M <= 512, 1024,
 // 2048) and 32 (M <= 1024, 2048, 4096)
 #define PFB_SREALP(KL, KU, SV, P)                                                                        \

@@ -11,18 +11,21 @@ namespace pfb {
 
 const StreamVariant* stream_variants_f64(int* count);
 const StreamVariant* stream_variants_mixed(int* count);
+const StreamVariant* stream_variants_alt(int* count);
 unsigned stream_status_f64();
 unsigned stream_status_mixed();
+unsigned stream_status_alt();
 
-const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC)
+const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC,
+                                         int ALT)
 {
-    for (auto part : {stream_variants_f64, stream_variants_mixed}) {
+    for (auto part : {stream_variants_f64, stream_variants_mixed, stream_variants_alt}) {
         int n = 0;
         const StreamVariant* vs = part(&n);
         for (int i = 0; i < n; ++i) {
             const StreamVariant& v = vs[i];
             if (v.R == R && v.W == W && v.KL == KL && v.KU == KU && v.SV == SV && v.LIN == LIN && v.LOUT == LOUT &&
-                v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC)
+                v.SCALE == (SCALE ? 1 : 0) && v.PREC == PREC && v.ALT == (ALT ? 1 : 0))
                 return &v;
         }
     }
@@ -156,8 +159,9 @@ unsigned stream_status_fetch_clear()
 {
     const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
     const unsigned d = steps_status_fetch_clear(), e = batch_status_fetch_clear(), f = long_status_fetch_clear();
-    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u || f == ~0u) return ~0u;
-    return a | b | c | d | e | f;
+    const unsigned g = stream_status_alt();
+    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u || f == ~0u || g == ~0u) return ~0u;
+    return a | b | c | d | e | f | g;
 }
 
 }  // namespace pfb

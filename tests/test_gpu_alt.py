@@ -1,6 +1,8 @@
 """GPU parity of ALT stride-2 mode (jw_type / 100 % 10 == 1) through the C
-ABI: the group kernel with one parity per group against the oracle's ALT
-restatement (pinned on the reference's ALT outputs, tests/test_golden_alt.py).
+ABI: the streaming kernel (FP64, whole row sets staged by TMA, both parities
+solved together) and the group kernel with one parity per group, against the
+oracle's ALT restatement (pinned on the reference's ALT outputs,
+tests/test_golden_alt.py).
 FP64 to 1e-13 relative L2 per system; mixed precision to 1e-12 after two
 refinement sweeps."""
 import numpy as np
@@ -33,6 +35,47 @@ def test_alt_modes_sizes(ub, jwt, M):
     rhs = rng.uniform(-1, 1, case.rhs_len())
     x = J.run_app(case, bands, rhs)
     assert _errs(x, O.jw_step_alt(case, bands, rhs), case) <= 1e-13
+
+
+@pytest.mark.parametrize("ub,jwt", KINDS)
+@pytest.mark.parametrize("M", [64, 512, 1000, 2048, 4096])
+def test_alt_streaming_kernel(ub, jwt, M):
+    """FP64 ALT on the streaming kernel (a row set staged by TMA, its even and
+    odd systems solved together): one streaming launch, against the oracle
+    and against the group kernel (kernelPath 1)."""
+    from pfsolve_b200.api import streaming_launch_count
+    rng = np.random.default_rng(36000 + 10 * ub + jwt + M)
+    bands = WL.alt_bands(rng, M, ub)
+    case = O.Case(M=M, batch=301, upperBanded=ub, jw_type=jwt)
+    rhs = rng.uniform(-1, 1, case.rhs_len())
+    n0 = streaming_launch_count()
+    x = J.run_app(case, bands, rhs)
+    assert streaming_launch_count() == n0 + 1
+    assert _errs(x, O.jw_step_alt(case, bands, rhs, nthreads=8), case) <= 1e-13
+    xg = J.run_app(case, bands, rhs, kernelPath=1)
+    assert streaming_launch_count() == n0 + 1
+    assert np.abs(x - xg).max() <= 1e-13 * np.abs(xg).max()
+
+
+@pytest.mark.parametrize("off", [3, 4])
+def test_alt_streaming_input_window_scaleC(off):
+    """Launch-time input window, scaleC and solution offset on the streaming
+    ALT kernel (offset 4: 16-byte-aligned row sets, streamed; offset 3: the
+    group kernel takes the launch)."""
+    from pfsolve_b200.api import streaming_launch_count
+    rng = np.random.default_rng(37000 + off)
+    M = 320
+    bm = capi.RUNTIME_OFFSETSOLUTION | capi.RUNTIME_INPUTZEROPAD | capi.RUNTIME_SCALEC
+    for ub, jwt in [(2, 113), (1, 110), (0, 110), (1, 111), (0, 112)]:
+        case = O.Case(M=M, batch=9, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetSolution=off,
+                      run_inputZeropad=(3, 290), run_scaleC=0.5)
+        bands = WL.alt_bands(rng, M, ub)
+        rhs = rng.uniform(-1, 1, case.rhs_len() + 8)
+        n0 = streaming_launch_count()
+        x = J.run_app(case, bands, rhs)
+        assert streaming_launch_count() == n0 + (1 if off == 4 else 0)
+        ref = O.jw_step_alt(case, bands, rhs)
+        assert np.abs(x - ref).max() <= 1e-13 * np.abs(ref).max(), (ub, jwt)
 
 
 def test_alt_windows_offsets_scaleC():
