@@ -243,6 +243,61 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
     return O::fma(Ae, win, Be);
 }
 
+// Two independent affine scans at once, elementwise in .x and .y (the two
+// ALT systems of a staged row set): one shuffle chain and one group barrier
+// instead of two.  Same slots as group_affine_scan (a double2 multiplier and
+// a double2 value fill the 4 doubles of a slot).
+template <bool FORWARD>
+__device__ __forceinline__ double2 group_affine_scan2(GroupCtx& g, double2 A, double2 B)
+{
+    using O = VOps<double2>;
+    auto fma2 = [](double2 a, double2 v, double2 w) {
+        return make_double2(__fma_rn(a.x, v.x, w.x), __fma_rn(a.y, v.y, w.y));
+    };
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double2 Ap = FORWARD ? O::shfl_up(A, d) : O::shfl_down(A, d);
+        const double2 Bp = FORWARD ? O::shfl_up(B, d) : O::shfl_down(B, d);
+        const bool take = FORWARD ? (g.lane >= d) : (g.lane + d < 32);
+        if (take) {
+            B = fma2(A, Bp, B);
+            A = make_double2(A.x * Ap.x, A.y * Ap.y);
+        }
+    }
+    double2 Ae = FORWARD ? O::shfl_up(A, 1) : O::shfl_down(A, 1);
+    double2 Be = FORWARD ? O::shfl_up(B, 1) : O::shfl_down(B, 1);
+    const bool first = FORWARD ? (g.lane == 0) : (g.lane == 31);
+    if (first) {
+        Ae = make_double2(1.0, 1.0);
+        Be = O::zero();
+    }
+    double2 win = O::zero();
+    if (g.W > 1) {
+        const int slot = (FORWARD ? 0 : 8) + 4 * (g.seq & 1);
+        const bool agg = FORWARD ? (g.lane == 31) : (g.lane == 0);
+        if (agg) {
+            double* my = g.warp_area(g.wg) + slot;
+            store_v<double2>(my, A);
+            store_v<double2>(my + 2, B);
+        }
+        __syncwarp();
+        group_bar(g.bar_id, g.nthr);
+        if (FORWARD) {
+            for (int w = 0; w < g.wg; ++w) {
+                const double* o = g.warp_area(w) + slot;
+                win = fma2(load_v<double2>(o), win, load_v<double2>(o + 2));
+            }
+        } else {
+            for (int w = g.W - 1; w > g.wg; --w) {
+                const double* o = g.warp_area(w) + slot;
+                win = fma2(load_v<double2>(o), win, load_v<double2>(o + 2));
+            }
+        }
+        g.seq++;
+    }
+    return fma2(Ae, win, Be);
+}
+
 // Values of the rows around this thread's chunk: x[s-1] (prev) and x[s+R]
 // (next); zero outside the system.
 template <class V>

@@ -638,15 +638,16 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             }
         }
         if constexpr (C::FWD && !C::MIXED && C::ALT) {
-            // the same per system: z_j = x_j - l_j z_{j-2}, one scan each
+            // the same per system: z_j = x_j - l_j z_{j-2}; both systems' chunk
+            // couplings in one paired scan
 #pragma unroll
             for (int u = 1; u < U; ++u) {
                 const double2 c = coef(C::P_NL, u);
                 x[2 * u] = O::fma(c.x, x[2 * u - 2], x[2 * u]);
                 x[2 * u + 1] = O::fma(c.y, x[2 * u - 1], x[2 * u + 1]);
             }
-            const V pin0 = group_affine_scan<V, double, true>(g, Af, x[R - 2]);
-            const V pin1 = group_affine_scan<V, double, true>(g, Af1, x[R - 1]);
+            const double2 pin = group_affine_scan2<true>(g, make_double2(Af, Af1), make_double2(x[R - 2], x[R - 1]));
+            const V pin0 = pin.x, pin1 = pin.y;
             double p0 = 1.0, p1 = 1.0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -684,8 +685,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 x[2 * u + 1] = O::fma(c.y, x[2 * u + 3], x[2 * u + 1]);
                 x[2 * u] = O::fma(c.x, x[2 * u + 2], x[2 * u]);
             }
-            const V q0 = group_affine_scan<V, double, false>(g, Ab, x[0]);
-            const V q1 = group_affine_scan<V, double, false>(g, Ab1, x[1]);
+            const double2 q = group_affine_scan2<false>(g, make_double2(Ab, Ab1), make_double2(x[0], x[1]));
+            const V q0 = q.x, q1 = q.y;
             double p0 = 1.0, p1 = 1.0;
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
