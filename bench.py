@@ -98,24 +98,26 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sample(target_s=12.0, threads=None):
-    """Time the reference's CPU verification path (port) on a bounded sample of
-    the workload; returns (complex RHS/s, cores, sample description)."""
+def cpu_reference_sample(target_s=12.0, threads=None, mode="d"):
+    """Time the reference's CPU verification path (port: banded matvec plus
+    sequential Thomas per RHS, in double, or in __float128 with mode "q") on a
+    bounded sample of the workload; returns (complex RHS/s, cores, sample
+    description)."""
     from oracle import oracle as O
     from pfsolve_b200 import workloads as WL
     threads = threads or os.cpu_count() or 1
-    probe = 64
+    probe = 64 if mode == "d" else 8
     wl = WL.config2(B=probe)
     M = wl.M
 
     def run(ncplx, rhs):
         c1 = O.Case(M=M, batch=2 * ncplx, LDA=5, KU=2, KL=2, jw_type=0)
-        y = O.dgbmv(c1, wl.dgbmv, rhs, mode="d", nthreads=threads)
+        y = O.dgbmv(c1, wl.dgbmv, rhs, mode=mode, nthreads=threads)
         c2 = O.Case(M=M, batch=2 * ncplx, upperBanded=2, jw_type=13)
-        O.jw_step(c2, wl.jw_bands, y, mode="d", nthreads=threads)
+        O.jw_step(c2, wl.jw_bands, y, mode=mode, nthreads=threads)
 
     t0 = time.perf_counter()
-    run(probe, wl.rhs)
+    run(probe, wl.rhs[:2 * M * probe])
     t = time.perf_counter() - t0
     n = int(min(N_CPLX, max(probe, probe * target_s / max(t, 1e-6))))
     rng = np.random.default_rng(1)
@@ -123,7 +125,19 @@ def cpu_reference_sample(target_s=12.0, threads=None):
     t0 = time.perf_counter()
     run(n, rhs)
     t = time.perf_counter() - t0
-    return n / t, threads, f"{n} of {N_CPLX} complex RHS (N=1024), double, {threads} OpenMP threads, {t:.1f} s"
+    kind = "double" if mode == "d" else "__float128"
+    return n / t, threads, f"{n} of {N_CPLX} complex RHS (N=1024), {kind}, {threads} OpenMP threads, {t:.1f} s"
+
+
+def cpu_reference_variants(target_s=3.0):
+    """The same CPU path single-threaded (as the reference's test drivers run
+    it) and in __float128 on all host cores: short bounded samples, reported
+    beside the main CPU baseline."""
+    out = []
+    for threads, mode in ((1, "d"), (None, "q")):
+        v, cores, desc = cpu_reference_sample(target_s=target_s, threads=threads, mode=mode)
+        out.append({"value": v, "unit": UNIT, "cores": cores, "sample": desc})
+    return out
 
 
 def reference_arm(args, rank, world):
@@ -286,7 +300,8 @@ def gpu_arm(args, rank, world):
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, cores, desc = cpu_reference_sample(target_s=12.0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc,
+               "variants": cpu_reference_variants()}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
