@@ -243,6 +243,79 @@ __device__ __forceinline__ V group_affine_scan(GroupCtx& g, S A, V B)
     return O::fma(Ae, win, Be);
 }
 
+// The multipliers of an affine scan whose per-thread multipliers A are the
+// same for every system (products of a coefficient table that all systems
+// share): each lane's multiplier at each shuffle level, the multiplier of its
+// exclusive result and its warp's aggregate, formed once so that a system's
+// scan (group_affine_scan_pre) shuffles only its values.
+template <class S>
+struct ScanMul {
+    S lev[5];
+    S Ae;
+    S Aw;
+};
+
+template <class S, bool FORWARD>
+__device__ __forceinline__ ScanMul<S> scan_multipliers(const GroupCtx& g, S A)
+{
+    ScanMul<S> m;
+    int i = 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1, ++i) {
+        m.lev[i] = A;
+        const S Ap = FORWARD ? shfl_up_s<S>(A, d) : shfl_down_s<S>(A, d);
+        const bool take = FORWARD ? (g.lane >= d) : (g.lane + d < 32);
+        if (take) A = A * Ap;
+    }
+    m.Aw = A;
+    const S Ae = FORWARD ? shfl_up_s<S>(A, 1) : shfl_down_s<S>(A, 1);
+    const bool first = FORWARD ? (g.lane == 0) : (g.lane == 31);
+    m.Ae = first ? S(1) : Ae;
+    return m;
+}
+
+// group_affine_scan with the multipliers formed by scan_multipliers.
+template <class V, class S, bool FORWARD>
+__device__ __forceinline__ V group_affine_scan_pre(GroupCtx& g, const ScanMul<S>& m, V B)
+{
+    using O = VOps<V>;
+    int i = 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1, ++i) {
+        const V Bp = FORWARD ? O::shfl_up(B, d) : O::shfl_down(B, d);
+        const bool take = FORWARD ? (g.lane >= d) : (g.lane + d < 32);
+        if (take) B = O::fma(m.lev[i], Bp, B);
+    }
+    V Be = FORWARD ? O::shfl_up(B, 1) : O::shfl_down(B, 1);
+    const bool first = FORWARD ? (g.lane == 0) : (g.lane == 31);
+    if (first) Be = O::zero();
+    V win = O::zero();
+    if (g.W > 1) {
+        const int slot = (FORWARD ? 0 : 8) + 4 * (g.seq & 1);
+        const bool agg = FORWARD ? (g.lane == 31) : (g.lane == 0);
+        if (agg) {
+            double* my = g.warp_area(g.wg) + slot;
+            store_v<S>(my, m.Aw);
+            store_v<V>(my + 2, B);
+        }
+        __syncwarp();
+        group_bar(g.bar_id, g.nthr);
+        if (FORWARD) {
+            for (int w = 0; w < g.wg; ++w) {
+                const double* o = g.warp_area(w) + slot;
+                win = O::fma(load_v<S>(o), win, load_v<V>(o + 2));
+            }
+        } else {
+            for (int w = g.W - 1; w > g.wg; --w) {
+                const double* o = g.warp_area(w) + slot;
+                win = O::fma(load_v<S>(o), win, load_v<V>(o + 2));
+            }
+        }
+        g.seq++;
+    }
+    return O::fma(m.Ae, win, Be);
+}
+
 // Two independent affine scans at once, elementwise in .x and .y (the two
 // ALT systems of a staged row set): one shuffle chain and one group barrier
 // instead of two.  Same slots as group_affine_scan (a double2 multiplier and

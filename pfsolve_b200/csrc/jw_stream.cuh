@@ -432,6 +432,18 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         }
     }
 
+    // Complex and mixed variants of up to 16 rows per thread under a
+    // 256-thread launch bound: each lane's scan multipliers formed once (all
+    // systems share them).  The others, with fewer registers to spare, keep
+    // the plain scan.
+    constexpr bool kPre = (C::CPLX || C::MIXED) && !C::ALT && R <= 16 && C::kMaxThreads <= 256;
+    ScanMul<double> mf{}, mb{};
+    ScanMul<float> mf32{}, mb32{};
+    if constexpr (kPre && C::FWD && !C::MIXED) mf = scan_multipliers<double, true>(g, Af);
+    if constexpr (kPre && C::BWD && !C::MIXED) mb = scan_multipliers<double, false>(g, Ab);
+    if constexpr (kPre && C::FWD && C::MIXED) mf32 = scan_multipliers<float, true>(g, Af32);
+    if constexpr (kPre && C::BWD && C::MIXED) mb32 = scan_multipliers<float, false>(g, Ab32);
+
     // Shared-memory byte offsets of 16-byte unit uu (< IB) of swizzle row h of
     // plane p for chunk c: plane_row(p, h) * T * IB*16 + c * IB*16 + (uu ^ swz(c))*16.
     constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
@@ -604,7 +616,9 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                         if (u > 0) d[2 * u] = OF::fma(f.z, d[2 * u - 1], d[2 * u]);
                         d[2 * u + 1] = OF::fma(f.w, d[2 * u], d[2 * u + 1]);
                     }
-                    const VF pin = group_affine_scan<VF, float, true>(g, Af32, d[R - 1]);
+                    VF pin;
+                    if constexpr (kPre) pin = group_affine_scan_pre<VF, float, true>(g, mf32, d[R - 1]);
+                    else pin = group_affine_scan<VF, float, true>(g, Af32, d[R - 1]);
                     float p = 1.0f;
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
@@ -622,7 +636,9 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                         if (u < U - 1) d[2 * u + 1] = OF::fma(f.y, d[2 * u + 2], d[2 * u + 1]);
                         d[2 * u] = OF::fma(f.x, d[2 * u + 1], d[2 * u]);
                     }
-                    const VF q = group_affine_scan<VF, float, false>(g, Ab32, d[0]);
+                    VF q;
+                    if constexpr (kPre) q = group_affine_scan_pre<VF, float, false>(g, mb32, d[0]);
+                    else q = group_affine_scan<VF, float, false>(g, Ab32, d[0]);
                     float p = 1.0f;
 #pragma unroll
                     for (int u = U - 1; u >= 0; --u) {
@@ -667,7 +683,9 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 if (u > 0) x[2 * u] = O::fma(c.x, x[2 * u - 1], x[2 * u]);
                 x[2 * u + 1] = O::fma(c.y, x[2 * u], x[2 * u + 1]);
             }
-            const V pin = group_affine_scan<V, double, true>(g, Af, x[R - 1]);
+            V pin;
+            if constexpr (kPre) pin = group_affine_scan_pre<V, double, true>(g, mf, x[R - 1]);
+            else pin = group_affine_scan<V, double, true>(g, Af, x[R - 1]);
             double p = 1.0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -704,7 +722,9 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 if (u < U - 1) x[2 * u + 1] = O::fma(c.y, x[2 * u + 2], x[2 * u + 1]);
                 x[2 * u] = O::fma(c.x, x[2 * u + 1], x[2 * u]);
             }
-            const V q = group_affine_scan<V, double, false>(g, Ab, x[0]);
+            V q;
+            if constexpr (kPre) q = group_affine_scan_pre<V, double, false>(g, mb, x[0]);
+            else q = group_affine_scan<V, double, false>(g, Ab, x[0]);
             double p = 1.0;
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
