@@ -6,6 +6,10 @@ the reference's outputs as ``<out>/<case>.npz``.  Needs a CUDA GPU; run it as
 ``python tests/golden/make_golden.py --out <dir>`` and copy the fixtures into
 ``tests/golden/``.  ``--time`` also times the reference's JW
 kernel on the full-size configurations and writes ``ref_timing.json``.
+Subsets (``--only``): K-step fixtures, ALT mode, long systems (into
+``<out>/long/``), double-double (into ``<out>/dd/``, copied to
+``tests/golden/dd/``), and ``dd-crash``, which re-runs the double-double cases
+the reference's code generation crashes on and stores no fixtures.
 """
 from __future__ import annotations
 
