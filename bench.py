@@ -140,6 +140,34 @@ def cpu_reference_variants(target_s=3.0):
     return out
 
 
+def spread_sample(nsys, ngroups, n=64, seed=7):
+    """Systems their group solves first, second and last (group y mod
+    ngroups takes system y at its (y div ngroups)-th turn), plus others."""
+    rng = np.random.default_rng(seed)
+    g = rng.choice(min(ngroups, nsys), n // 4, replace=False)
+    parts = [g, g + ngroups, g + ngroups * ((nsys - 1 - g) // ngroups), rng.choice(nsys, n // 4, replace=False)]
+    return np.unique(np.concatenate(parts) % nsys)
+
+
+def parity_check(snap_in, snap_out, dgbmv, bands, M, ys):
+    """Checker for the timed output: the sampled systems' XXII inputs through
+    the __float128 oracle chain (dgbmv -> JW step -> block 7), against the
+    packed results the GPU wrote in its last timed step."""
+    from oracle import oracle as O
+    n = len(ys)
+    th = os.cpu_count() or 1
+    y = O.dgbmv(O.Case(M=M, batch=2 * n, LDA=5, KU=2, KL=2, jw_type=0), dgbmv, snap_in.ravel(), nthreads=th)
+    x = O.jw_step(O.Case(M=M, batch=2 * n, upperBanded=2, jw_type=13), bands, y, "q", nthreads=th)
+    ref = O.block(O.Case(M=M, batch=n, block=7, jw_type=0), x, np.zeros(2 * M * n)).reshape(n, -1)
+    got = snap_out.reshape(n, -1)
+    rel = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    return {"max_rel_err": float(rel.max()), "systems_checked": int(n), "tolerance": 1e-13,
+            "ok": bool(rel.max() <= 1e-13),
+            "oracle": "__float128 chain (dgbmv -> JW step -> block 7) on the host",
+            "sample": "systems solved first, second and last by their group, plus random ones, "
+                      "from the output of the last timed step"}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -169,7 +197,7 @@ def gpu_arm(args, rank, world):
 
     from pfsolve_b200 import replicas
     from pfsolve_b200 import workloads as WL
-    from pfsolve_b200.api import App, append_chain, launch_count
+    from pfsolve_b200.api import App, append_chain, last_launch, launch_count
 
     nc = args.ncplx
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -213,6 +241,13 @@ def gpu_arm(args, rank, world):
     launches = launch_count() - n0
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
+    # the kernel instance that ran, and a spread sample of the last timed
+    # step's output (checked against the oracle in the CPU leg below)
+    kinfo = last_launch()
+    ys = spread_sample(nc, max(1, kinfo["gridCTAs"] * kinfo["groupsPerCTA"]))
+    ys_t = torch.from_numpy(ys).to(dev)
+    snap_out = out.view(nc, M, 2)[ys_t].cpu().numpy()
+    snap_in = rhs.view(nc, 2, M)[ys_t].cpu().numpy()
     ms_max = replicas.max_over_ranks(ms, dev)
     value = replicas.job_throughput(nc, ms_max, world)
     bytes_alg = 2.0 * M * 16 * nc + (5 + 3) * M * 8
@@ -298,7 +333,9 @@ def gpu_arm(args, rank, world):
         a.close()
 
     cpu = None
+    parity = None
     if rank == 0 and not args.no_cpu:
+        parity = parity_check(snap_in, snap_out, tA.cpu().numpy(), tb.cpu().numpy(), M, ys)
         v, cores, desc = cpu_reference_sample(target_s=12.0)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc,
                "variants": cpu_reference_variants()}
@@ -310,6 +347,7 @@ def gpu_arm(args, rank, world):
                 "config": {"workload": "config2: N=1024, 65536 complex RHS per GPU, XXII in -> packed out, "
                                        "dgbmv(5) + tridiagonal JW step (jw_type 13) fused, one kernel per step",
                            "rhs_per_gpu": nc, "l2": "inputs 2 GiB > L2, no flush", "kernel": jw.shape(),
+                           "kernel_instance": kinfo,
                            "parallelism": f"replicas x{world} (independent RHS shards, no collective)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
@@ -319,7 +357,7 @@ def gpu_arm(args, rank, world):
                         "pipeline": f"pinned host buffers; H2D, fused kernel and D2H on three streams, "
                                     f"double-buffered, {CH} chunks per step: each chunk's upload overlaps the "
                                     f"previous chunks' downloads", "chunks_per_step": CH},
-                "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu}
+                "gpu_launches": int(launches), "clocks": clocks, "cpu_baseline": cpu, "parity": parity}
         if not args.no_extras and world == 1:
             line["extras"] = extras_arm(args)
         print(json.dumps(line), flush=True)
@@ -367,6 +405,7 @@ def extras_arm(args):
     out["config3_mixed_vs_fp64_rel_l2_max"] = float(d.max().item())
     out["config3_mixed_speedup"] = out["config3_fp64"]["ms"] / out["config3_mixed"]["ms"]
     del res, base
+    out["config1_latency"] = config1_measure()
     step = WL.config4()
     dev = torch.device("cuda")
     inp = torch.from_numpy(step.rhs).to(dev)
@@ -411,7 +450,52 @@ def extras_arm(args):
     out["alt_t113_N1024_B131072_group"] = alt_measure(1024, 131072, path=1)
     torch.cuda.empty_cache()
     out["config5_serving"] = serving_leg()
+    # each HBM-bound entry's fraction of the measured HBM peak
+    peak, kind = peaks()
+    for v in out.values():
+        if isinstance(v, dict) and "gbs" in v and "note" not in v:
+            v["hbm_frac"] = v["gbs"] / peak
+            v["hbm_peak_kind"] = kind
     return out
+
+
+def config1_measure(steps=200, warmup=20):
+    """Config 1 (the test-1 form: N = 256, 512 real RHS, a 3-band dgbmv
+    fused ahead of the upper-bidiagonal JW step, jw_type 13, upperBanded 0),
+    and the JW step alone as the reference times it: per-step latency of
+    back-to-back launches on one stream (CUDA events over `steps` launches
+    after `warmup`; 2.1 MB of right-hand sides, L2-resident)."""
+    import torch
+
+    from pfsolve_b200 import workloads as WL
+    from pfsolve_b200.api import App, append_chain
+    wl = WL.config1()
+    M, B = wl.M, wl.nrhs
+    tA = torch.from_numpy(wl.dgbmv).cuda()
+    tb = torch.from_numpy(wl.jw_bands).cuda()
+    tr = torch.from_numpy(wl.rhs.copy()).cuda()
+    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1)
+    jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1,
+             scaleC=1.0)
+    lps = [dg.launch_params(), jw.launch_params()]
+    res = {}
+    for name, fn in (("fused_chain", lambda: append_chain([dg, jw], lps)), ("jw_only", lambda: jw.append(lps[1]))):
+        for _ in range(warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[name] = {"ms": ms, "rhs_per_s": B / (ms * 1e-3), "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9}
+    dg.close()
+    jw.close()
+    res["reference_jw_ms"] = 0.0042  # its own JW kernel on the same pool, same method (20 launches)
+    res["note"] = "L2-resident (2.1 MB): latency of back-to-back launches, not an HBM roofline"
+    return res
 
 
 def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):

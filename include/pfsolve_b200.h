@@ -73,6 +73,10 @@ typedef struct CUstream_st* cudaStream_t;
 #define JWT_DIAGONAL_MATVECMUL 3
 #define JWT_USE_PARALLEL_THOMAS 10
 
+/* Result codes: every code of pfSolve_Structs.h:450-543, same names and
+ * numbers (most name backend steps this library never takes; they are kept
+ * so that callers' switch statements and getPfSolveErrorString cover them),
+ * plus four extension codes. */
 typedef enum PfSolveResult {
     PFSOLVE_SUCCESS = 0,
     PFSOLVE_ERROR_MALLOC_FAILED = 1,
@@ -83,22 +87,89 @@ typedef enum PfSolveResult {
     PFSOLVE_ERROR_MATH_FAILED = 6,
     PFSOLVE_ERROR_INVALID_PHYSICAL_DEVICE = 1001,
     PFSOLVE_ERROR_INVALID_DEVICE = 1002,
+    PFSOLVE_ERROR_INVALID_QUEUE = 1003,
+    PFSOLVE_ERROR_INVALID_COMMAND_POOL = 1004,
+    PFSOLVE_ERROR_INVALID_FENCE = 1005,
+    PFSOLVE_ERROR_ONLY_FORWARD_FFT_INITIALIZED = 1006,
+    PFSOLVE_ERROR_ONLY_INVERSE_FFT_INITIALIZED = 1007,
     PFSOLVE_ERROR_INVALID_CONTEXT = 1008,
+    PFSOLVE_ERROR_INVALID_PLATFORM = 1009,
+    PFSOLVE_ERROR_ENABLED_saveApplicationToString = 1010,
+    PFSOLVE_ERROR_EMPTY_FILE = 1011,
     PFSOLVE_ERROR_EMPTY_FFTdim = 2001,
     PFSOLVE_ERROR_EMPTY_size = 2002,
     PFSOLVE_ERROR_EMPTY_bufferSize = 2003,
     PFSOLVE_ERROR_EMPTY_buffer = 2004,
+    PFSOLVE_ERROR_EMPTY_tempBufferSize = 2005,
+    PFSOLVE_ERROR_EMPTY_tempBuffer = 2006,
+    PFSOLVE_ERROR_EMPTY_inputBufferSize = 2007,
+    PFSOLVE_ERROR_EMPTY_inputBuffer = 2008,
     PFSOLVE_ERROR_EMPTY_outputBufferSize = 2009,
     PFSOLVE_ERROR_EMPTY_outputBuffer = 2010,
+    PFSOLVE_ERROR_EMPTY_kernelSize = 2011,
     PFSOLVE_ERROR_EMPTY_kernel = 2012,
+    PFSOLVE_ERROR_EMPTY_applicationString = 2013,
+    PFSOLVE_ERROR_EMPTY_useCustomBluesteinPaddingPattern_arrays = 2014,
     PFSOLVE_ERROR_UNSUPPORTED_RADIX = 3001,
     PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH = 3002,
+    PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_R2C = 3003,
+    PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_DCT = 3004,
+    PFSOLVE_ERROR_UNSUPPORTED_FFT_OMIT = 3005,
     PFSOLVE_ERROR_FAILED_TO_ALLOCATE = 4001,
+    PFSOLVE_ERROR_FAILED_TO_MAP_MEMORY = 4002,
+    PFSOLVE_ERROR_FAILED_TO_ALLOCATE_COMMAND_BUFFERS = 4003,
+    PFSOLVE_ERROR_FAILED_TO_BEGIN_COMMAND_BUFFER = 4004,
+    PFSOLVE_ERROR_FAILED_TO_END_COMMAND_BUFFER = 4005,
+    PFSOLVE_ERROR_FAILED_TO_SUBMIT_QUEUE = 4006,
+    PFSOLVE_ERROR_FAILED_TO_WAIT_FOR_FENCES = 4007,
+    PFSOLVE_ERROR_FAILED_TO_RESET_FENCES = 4008,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_POOL = 4009,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_SET_LAYOUT = 4010,
+    PFSOLVE_ERROR_FAILED_TO_ALLOCATE_DESCRIPTOR_SETS = 4011,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE_LAYOUT = 4012,
+    PFSOLVE_ERROR_FAILED_SHADER_PREPROCESS = 4013,
+    PFSOLVE_ERROR_FAILED_SHADER_PARSE = 4014,
+    PFSOLVE_ERROR_FAILED_SHADER_LINK = 4015,
+    PFSOLVE_ERROR_FAILED_SPIRV_GENERATE = 4016,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_SHADER_MODULE = 4017,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_INSTANCE = 4018,
+    PFSOLVE_ERROR_FAILED_TO_SETUP_DEBUG_MESSENGER = 4019,
+    PFSOLVE_ERROR_FAILED_TO_FIND_PHYSICAL_DEVICE = 4020,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_DEVICE = 4021,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_FENCE = 4022,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_POOL = 4023,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_BUFFER = 4024,
+    PFSOLVE_ERROR_FAILED_TO_ALLOCATE_MEMORY = 4025,
+    PFSOLVE_ERROR_FAILED_TO_BIND_BUFFER_MEMORY = 4026,
+    PFSOLVE_ERROR_FAILED_TO_FIND_MEMORY = 4027,
     PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE = 4028,
     PFSOLVE_ERROR_FAILED_TO_COPY = 4029,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_PROGRAM = 4030,
+    PFSOLVE_ERROR_FAILED_TO_COMPILE_PROGRAM = 4031,
+    PFSOLVE_ERROR_FAILED_TO_GET_CODE_SIZE = 4032,
+    PFSOLVE_ERROR_FAILED_TO_GET_CODE = 4033,
+    PFSOLVE_ERROR_FAILED_TO_DESTROY_PROGRAM = 4034,
+    PFSOLVE_ERROR_FAILED_TO_LOAD_MODULE = 4035,
+    PFSOLVE_ERROR_FAILED_TO_GET_FUNCTION = 4036,
+    PFSOLVE_ERROR_FAILED_TO_SET_DYNAMIC_SHARED_MEMORY = 4037,
+    PFSOLVE_ERROR_FAILED_TO_MODULE_GET_GLOBAL = 4038,
     PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL = 4039,
     PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD = 4040,
+    PFSOLVE_ERROR_FAILED_TO_ADD_NAME_EXPRESSION = 4041,
+    PFSOLVE_ERROR_FAILED_TO_INITIALIZE = 4042,
+    PFSOLVE_ERROR_FAILED_TO_SET_DEVICE_ID = 4043,
+    PFSOLVE_ERROR_FAILED_TO_GET_DEVICE = 4044,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_CONTEXT = 4045,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE = 4046,
+    PFSOLVE_ERROR_FAILED_TO_SET_KERNEL_ARG = 4047,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_QUEUE = 4048,
+    PFSOLVE_ERROR_FAILED_TO_RELEASE_COMMAND_QUEUE = 4049,
+    PFSOLVE_ERROR_FAILED_TO_ENUMERATE_DEVICES = 4050,
     PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE = 4051,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_EVENT = 4052,
+    PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_LIST = 4053,
+    PFSOLVE_ERROR_FAILED_TO_DESTROY_COMMAND_LIST = 4054,
+    PFSOLVE_ERROR_FAILED_TO_SUBMIT_BARRIER = 4055,
     /* extension codes (no counterpart in the reference) */
     PFSOLVE_ERROR_UNSUPPORTED_COMBINATION = 5001, /* parameter combination the reference leaves undefined */
     PFSOLVE_ERROR_INVALID_ARGUMENT = 5002,        /* NULL pointer, negative size, misaligned buffer */
@@ -132,7 +203,8 @@ typedef struct {
     int LDA;              /* > 0 selects the dgbmv application: LDA = KL + KU + 1 bands */
     int KU;
     int KL;
-    int ALT_dgbmv;        /* not supported: must be 0 */
+    int ALT_dgbmv;        /* dgbmv: drop alternate bands by the reference's rule (pfSolve_Plan_dgbmv.h:100,
+                             pfSolve_MatVecMul.h:390); LDA <= 64, not with double-double */
     uint64_t Msplit[3];   /* multi-upload split (accepted, single upload used for M <= 4352) */
 
     int64_t jw_control_bitmask; /* RUNTIME_* bits */
@@ -217,7 +289,13 @@ PFSOLVE_API PfSolveResult PfSolveSync(PfSolveApplication* app);
 /* Release the plan's host and device state (never the user's buffers). */
 PFSOLVE_API void deletePfSolve(PfSolveApplication* app);
 
+/* Name of a result code, as the reference's helper of the same name
+ * (pfSolve_Structs/pfSolve_Structs.h:545): every code declared above has its
+ * own name; other values give "PFSOLVE_ERROR_UNKNOWN". */
 PFSOLVE_API const char* getPfSolveErrorString(PfSolveResult result);
+/* The reference's version value (pfSolve.h:101-103): its source writes it as
+ * the literal 00102 ("X.XX.XX format"), which C reads as octal, so the value
+ * is 66. */
 PFSOLVE_API int PfSolveGetVersion(void);
 
 /* ---- App library (kernel reuse cache), pfSolve_AppCollectionManager.hpp ---- */
@@ -336,7 +414,8 @@ PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
 
 /* One uneven batch, as PfSolveBatchCreate + PfSolveBatchAppend +
  * PfSolveBatchDestroy, that allocates nothing: no cudaMalloc, no cudaFree,
- * no host heap.  For callers that must not reach the device allocator during
+ * no host heap (the work list is sorted in place in fixed host arrays).
+ * For callers that must not reach the device allocator during
  * their time loop -- code whose device memory is all owned by its own pool,
  * or which cannot afford the implicit device synchronisation and the failure
  * modes of cudaMalloc.  No counterpart in the reference.
@@ -350,8 +429,13 @@ PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
  * calls whose work overlaps in time (on other streams or from other threads)
  * race; serialise them.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress); make that call before any stream
- * capture on the device.  Results equal PfSolveBatchAppend's for the same
- * descriptor, rows per thread and systems per item. */
+ * capture on the device.  The descriptors reach the device by
+ * cudaMemcpyAsync from the library's fixed host arrays, which are ordinary
+ * (pageable) memory: the call returns once the driver has staged them, so it
+ * may block the host for that copy (never for the device's queued work).
+ * The caller's current device is the same on return as on entry.  Results
+ * equal PfSolveBatchAppend's for the same descriptor, rows per thread and
+ * systems per item. */
 #define PFSOLVE_NOALLOC_MAX_ENTRIES 1024
 #define PFSOLVE_NOALLOC_MAX_ITEMS 16384
 PFSOLVE_API PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolveBatchDesc* desc,
@@ -388,6 +472,39 @@ PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* st
 /* Launches that ran on the streaming kernel since load (all apps). */
 PFSOLVE_API uint64_t PfSolveStreamingLaunchCount(void);
 
+/* The kernel instance of the most recent launch this library enqueued from
+ * the calling thread (PfSolveAppend, PfSolveAppendChain), so that a caller
+ * or a test can tell which compiled kernel ran.  No counterpart in the
+ * reference. */
+enum {
+    PFSOLVE_KERNEL_NONE = 0,      /* no launch yet on this thread */
+    PFSOLVE_KERNEL_GROUP = 1,     /* jw_step_kernel: a group of warps per system, cp.async staging */
+    PFSOLVE_KERNEL_STREAMING = 2, /* jw_stream_kernel: whole systems staged by TMA */
+    PFSOLVE_KERNEL_LONG = 3,      /* jw_long_kernel: long systems in two passes over slices */
+    PFSOLVE_KERNEL_CLUSTER = 4,   /* jw_cluster_kernel: one thread-block cluster per long system */
+    PFSOLVE_KERNEL_STEPS = 5,     /* jw_steps_kernel: K consecutive steps */
+    PFSOLVE_KERNEL_STEPS_SWEEP = 6, /* jw_steps_seq_kernel: K bidiagonal steps, one system per lane */
+    PFSOLVE_KERNEL_DGBMV = 7,     /* dgbmv_generic_kernel: band matrices wider than two bands a side */
+    PFSOLVE_KERNEL_BLOCK = 8      /* block_kernel */
+};
+typedef struct {
+    int kernel;         /* PFSOLVE_KERNEL_* */
+    int rowsPerThread;  /* 0 where the kernel has no such parameter */
+    int warpsPerSystem;
+    int groupsPerCTA;
+    int bandsBelow;     /* KL of the fused matvec weights (JW matvec and dgbmv together) */
+    int bandsAbove;     /* KU */
+    int solve;          /* 0 none, 1 unit lower, 2 unit upper, 3 unit tridiagonal */
+    int layoutIn;       /* 0 real rows, 1 complex XXII (real rows, then imaginary rows), 2 packed complex */
+    int layoutOut;
+    int scale;          /* a fused Scale operator (block 1xx..4xx) */
+    int precision;      /* 0 FP64, 1 FP32 solve + FP64 refinement, 2 double-double storage, 3 double-double on
+                           FP64 storage, 4 FP32, 5 FP64 arithmetic on FP32 storage */
+    int alt;            /* ALT stride-2 mode */
+    int64_t gridCTAs;   /* CTAs of the (last) kernel of the launch */
+} PfSolveLaunchInfo;
+PFSOLVE_API PfSolveResult PfSolveGetLastLaunch(PfSolveLaunchInfo* info);
+
 /* ---- Serving engine.  No counterpart in the reference (whose callers drive
  * one application at a time): JW-step requests of mixed size and precision are
  * queued, admitted while the bytes of the requests on the device stay within
@@ -415,6 +532,12 @@ typedef struct {
     void* output;        /* device; may equal input */
     int64_t stride;      /* values between consecutive systems (0: M) */
     double scaleC;       /* multiplies solution row 0 */
+    cudaStream_t stream; /* the caller's stream that writes `input` (NULL: the legacy default stream).  The
+                            server's streams do not synchronise with the caller's, so Submit records an event
+                            on this stream and the request's kernel waits for it: work the caller enqueued on
+                            it before Submit (writing the input, clearing the output) comes first. */
+    int inputReady;      /* 1: skip that wait -- the caller guarantees that nothing still pending on the
+                            device writes `input` or `output` (e.g. it synchronised) */
 } PfSolveRequest;
 
 typedef struct {
@@ -431,8 +554,10 @@ PFSOLVE_API PfSolveResult PfSolveServerCreate(PfSolveServer** server, const PfSo
  * PfSolveConfiguration.  A double-double copy is made on the device. */
 PFSOLVE_API PfSolveResult PfSolveServerAddOperator(PfSolveServer* server, int64_t M, const double* bands,
                                                    int upperBanded, int jw_type, int* opId);
-/* Queue a request; returns at once.  PFSOLVE_ERROR_CAPACITY when the request
- * alone exceeds the HBM budget. */
+/* Queue a request; returns at once (after recording the ordering event on
+ * request->stream unless inputReady).  PFSOLVE_ERROR_CAPACITY when the
+ * request alone exceeds the HBM budget.  The output is complete, and visible
+ * to any later work of the caller, once PfSolveServerWait returns. */
 PFSOLVE_API PfSolveResult PfSolveServerSubmit(PfSolveServer* server, const PfSolveRequest* request,
                                               uint64_t* ticket);
 /* Block until the request is done; its latency (ms) when latencyMs != NULL.

@@ -125,6 +125,13 @@ def streaming_launch_count() -> int:
     return int(capi.load().PfSolveStreamingLaunchCount())
 
 
+def last_launch() -> dict:
+    """The kernel instance of this thread's most recent launch (``PfSolveGetLastLaunch``)."""
+    info = capi.PfSolveLaunchInfo()
+    check(capi.load().PfSolveGetLastLaunch(ctypes.byref(info)), "PfSolveGetLastLaunch")
+    return {k: getattr(info, k) for k, _ in info._fields_}
+
+
 def device_status() -> int:
     """``PfSolveGetDeviceStatus``: 0, or PFSOLVE_ERROR_DEVICE_FAULT after a bounded wait ran out."""
     return int(capi.load().PfSolveGetDeviceStatus())

@@ -122,7 +122,19 @@ class PfSolveServerDesc(ctypes.Structure):
 
 class PfSolveRequest(ctypes.Structure):
     _fields_ = [("op", c_int), ("precision", c_int), ("nrhs", i64), ("input", ctypes.c_void_p),
-                ("output", ctypes.c_void_p), ("stride", i64), ("scaleC", ctypes.c_double)]
+                ("output", ctypes.c_void_p), ("stride", i64), ("scaleC", ctypes.c_double),
+                ("stream", ctypes.c_void_p), ("inputReady", c_int)]
+
+
+class PfSolveLaunchInfo(ctypes.Structure):
+    _fields_ = [("kernel", c_int), ("rowsPerThread", c_int), ("warpsPerSystem", c_int), ("groupsPerCTA", c_int),
+                ("bandsBelow", c_int), ("bandsAbove", c_int), ("solve", c_int), ("layoutIn", c_int),
+                ("layoutOut", c_int), ("scale", c_int), ("precision", c_int), ("alt", c_int), ("gridCTAs", i64)]
+
+
+PFSOLVE_KERNEL_NONE, PFSOLVE_KERNEL_GROUP, PFSOLVE_KERNEL_STREAMING, PFSOLVE_KERNEL_LONG = 0, 1, 2, 3
+PFSOLVE_KERNEL_CLUSTER, PFSOLVE_KERNEL_STEPS, PFSOLVE_KERNEL_STEPS_SWEEP = 4, 5, 6
+PFSOLVE_KERNEL_DGBMV, PFSOLVE_KERNEL_BLOCK = 7, 8
 
 
 class PfSolveServerStats(ctypes.Structure):
@@ -157,6 +169,7 @@ SIGNATURES = {
     "PfSolveGetDeviceStatus": (c_int, []),
     "PfSolveGetShape": (c_int, [_APP_P] + [ctypes.POINTER(c_int)] * 4),
     "PfSolveStreamingLaunchCount": (u64, []),
+    "PfSolveGetLastLaunch": (c_int, [ctypes.POINTER(PfSolveLaunchInfo)]),
     "PfSolveServerCreate": (c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(PfSolveServerDesc)]),
     "PfSolveServerAddOperator": (c_int, [ctypes.c_void_p, i64, ctypes.c_void_p, c_int, c_int,
                                          ctypes.POINTER(c_int)]),

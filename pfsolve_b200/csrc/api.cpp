@@ -91,6 +91,29 @@ struct AppState {
 
 AppState* st(PfSolveApplication* app) { return static_cast<AppState*>(app->internal); }
 
+// The kernel instance of the calling thread's most recent launch
+// (PfSolveGetLastLaunch).
+thread_local PfSolveLaunchInfo g_last_launch;
+
+void record_launch(int kernel, int R, int W, int G, int KL, int KU, int sv, int lin, int lout, int scale, int prec,
+                   int alt, int64_t grid)
+{
+    PfSolveLaunchInfo& i = g_last_launch;
+    i.kernel = kernel;
+    i.rowsPerThread = R;
+    i.warpsPerSystem = W;
+    i.groupsPerCTA = G;
+    i.bandsBelow = KL;
+    i.bandsAbove = KU;
+    i.solve = sv;
+    i.layoutIn = lin;
+    i.layoutOut = lout;
+    i.scale = scale;
+    i.precision = prec;
+    i.alt = alt;
+    i.gridCTAs = grid;
+}
+
 }  // namespace
 
 void pfb::note_launch(bool streaming)
@@ -520,6 +543,8 @@ PfSolveResult launch_cluster(AppState* s, const JwOperator& op, const JwIO& io, 
     const int clusters = (int)std::max<int64_t>(1, std::min<int64_t>(io.nsys, s->cluster_max));
     const cudaError_t err = v->launch(clusters, v->smem_bytes, stream, &e->in, &e->out, op, io);
     note_launch(true);
+    record_launch(PFSOLVE_KERNEL_CLUSTER, v->R, v->W * v->C, 1, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0, PREC_F64,
+                  0, (int64_t)clusters * v->C);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
@@ -540,6 +565,8 @@ PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cud
     const cudaError_t err =
         v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, tab, s->long_NS);
     note_launch(true);
+    record_launch(PFSOLVE_KERNEL_LONG, v->R, v->W, v->G, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0, PREC_F64, 0,
+                  s->long_grid);
     // the table passes, the carry kernel (solves only) and pass 2
     g_launches.fetch_add((s->sv != SV_NONE ? 3 : 2) + (s->sv == SV_TRI ? 1 : 0), std::memory_order_relaxed);
     if (err != cudaSuccess) {
@@ -564,6 +591,8 @@ bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->stream_max_blocks));
     v->launch(dim3((unsigned)grid), dim3(32 * v->W * s->stream_G), v->smem_bytes(s->stream_G), stream, &e->in, &e->out,
               op, rs);
+    record_launch(PFSOLVE_KERNEL_STREAMING, v->R, v->W, s->stream_G, v->KL, v->KU, v->SV, v->LIN, v->LOUT, v->SCALE,
+                  v->PREC, v->ALT, grid);
     return true;
 }
 
@@ -589,6 +618,11 @@ PfSolveResult launch_jw_variant(AppState* s, const JwOperator& op, const JwIO& i
     const size_t smem = s->variant->smem_bytes(s->W, s->G);
     s->variant->launch(dim3((unsigned)grid), dim3(32 * s->W * s->G), smem, stream, op, io, s->W);
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    {
+        const JwVariant* v = s->variant;
+        record_launch(PFSOLVE_KERNEL_GROUP, v->R, s->W, s->G, v->KL, v->KU, v->SV, v->LIN, v->LOUT, v->SCALE, v->PREC,
+                      io.alt, grid);
+    }
     if (cudaPeekAtLastError() != cudaSuccess) {
         cudaGetLastError();
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
@@ -679,6 +713,9 @@ PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* l
         s->seq_v->launch(dim3((unsigned)grid), dim3(32 * nw), seq_steps_smem_bytes(S.K, Mtab, nw), stream, &tin, &tout,
                          S, io);
         g_launches.fetch_add(1, std::memory_order_relaxed);
+        record_launch(PFSOLVE_KERNEL_STEPS_SWEEP, 0, 0, nw, c.upperBanded == 0 ? 1 : 0, c.upperBanded == 1 ? 1 : 0,
+                      s->seq_v->SV ? (c.upperBanded ? SV_LOWER : SV_UPPER) : SV_NONE, LAY_REAL, LAY_REAL, 0,
+                      PREC_F64, 0, grid);
         g_stream_launches.fetch_add(1, std::memory_order_relaxed);
         if (cudaPeekAtLastError() != cudaSuccess) {
             cudaGetLastError();
@@ -693,6 +730,8 @@ PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* l
     v->launch(dim3((unsigned)grid), dim3(32 * s->steps_W * s->steps_G), v->smem_bytes(s->K, s->steps_W, s->steps_G),
               stream, S, io, s->steps_W);
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    record_launch(PFSOLVE_KERNEL_STEPS, v->R, s->steps_W, s->steps_G, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0,
+                  PREC_F64, 0, grid);
     if (cudaPeekAtLastError() != cudaSuccess) {
         cudaGetLastError();
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
@@ -790,6 +829,7 @@ PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* l
     a.iz0 = r.iz0; a.iz1 = r.iz1; a.oz0 = r.oz0; a.oz1 = r.oz1;
     launch_dgbmv_generic(a, stream, s->num_sms);
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    record_launch(PFSOLVE_KERNEL_DGBMV, 0, 0, 0, c.LDA - 1 - c.KU, c.KU, SV_NONE, LAY_REAL, LAY_REAL, 0, s->prec, 0, 0);
     if (cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL; }
     return PFSOLVE_SUCCESS;
 }
@@ -820,6 +860,7 @@ PfSolveResult append_block(PfSolveApplication* app, const PfSolveLaunchParams* l
     a.skip_read = (a.scale_kind == 1) && !(c.jw_control_bitmask & RUNTIME_SCALEC) && c.scaleC == 0.0;
     launch_block(a, stream, s->num_sms);
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    record_launch(PFSOLVE_KERNEL_BLOCK, 0, 0, 0, 0, 0, SV_NONE, 0, 0, a.scale_kind != 0, s->prec, 0, 0);
     if (cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL; }
     return PFSOLVE_SUCCESS;
 }
@@ -830,32 +871,127 @@ extern "C" {
 
 const char* getPfSolveErrorString(PfSolveResult result)
 {
-    switch (result) {
-    case PFSOLVE_SUCCESS: return "PFSOLVE_SUCCESS";
-    case PFSOLVE_ERROR_MALLOC_FAILED: return "PFSOLVE_ERROR_MALLOC_FAILED";
-    case PFSOLVE_ERROR_PLAN_NOT_INITIALIZED: return "PFSOLVE_ERROR_PLAN_NOT_INITIALIZED";
-    case PFSOLVE_ERROR_INVALID_DEVICE: return "PFSOLVE_ERROR_INVALID_DEVICE";
-    case PFSOLVE_ERROR_EMPTY_FFTdim: return "PFSOLVE_ERROR_EMPTY_FFTdim";
-    case PFSOLVE_ERROR_EMPTY_size: return "PFSOLVE_ERROR_EMPTY_size";
-    case PFSOLVE_ERROR_EMPTY_buffer: return "PFSOLVE_ERROR_EMPTY_buffer";
-    case PFSOLVE_ERROR_EMPTY_outputBuffer: return "PFSOLVE_ERROR_EMPTY_outputBuffer";
-    case PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH: return "PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH";
-    case PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE: return "PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE";
-    case PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL: return "PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL";
-    case PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE: return "PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE";
-    case PFSOLVE_ERROR_UNSUPPORTED_COMBINATION: return "PFSOLVE_ERROR_UNSUPPORTED_COMBINATION";
-    case PFSOLVE_ERROR_INVALID_ARGUMENT: return "PFSOLVE_ERROR_INVALID_ARGUMENT";
-    case PFSOLVE_ERROR_CAPACITY: return "PFSOLVE_ERROR_CAPACITY";
-    case PFSOLVE_ERROR_DEVICE_FAULT: return "PFSOLVE_ERROR_DEVICE_FAULT";
-    default: return "PFSOLVE_ERROR_UNKNOWN";
-    }
+    // every code of the header's PfSolveResult, each with its own name
+    static const struct {
+        PfSolveResult code;
+        const char* name;
+    } kNames[] = {
+        {PFSOLVE_SUCCESS, "PFSOLVE_SUCCESS"},
+        {PFSOLVE_ERROR_MALLOC_FAILED, "PFSOLVE_ERROR_MALLOC_FAILED"},
+        {PFSOLVE_ERROR_INSUFFICIENT_CODE_BUFFER, "PFSOLVE_ERROR_INSUFFICIENT_CODE_BUFFER"},
+        {PFSOLVE_ERROR_INSUFFICIENT_TEMP_BUFFER, "PFSOLVE_ERROR_INSUFFICIENT_TEMP_BUFFER"},
+        {PFSOLVE_ERROR_PLAN_NOT_INITIALIZED, "PFSOLVE_ERROR_PLAN_NOT_INITIALIZED"},
+        {PFSOLVE_ERROR_NULL_TEMP_PASSED, "PFSOLVE_ERROR_NULL_TEMP_PASSED"},
+        {PFSOLVE_ERROR_MATH_FAILED, "PFSOLVE_ERROR_MATH_FAILED"},
+        {PFSOLVE_ERROR_INVALID_PHYSICAL_DEVICE, "PFSOLVE_ERROR_INVALID_PHYSICAL_DEVICE"},
+        {PFSOLVE_ERROR_INVALID_DEVICE, "PFSOLVE_ERROR_INVALID_DEVICE"},
+        {PFSOLVE_ERROR_INVALID_QUEUE, "PFSOLVE_ERROR_INVALID_QUEUE"},
+        {PFSOLVE_ERROR_INVALID_COMMAND_POOL, "PFSOLVE_ERROR_INVALID_COMMAND_POOL"},
+        {PFSOLVE_ERROR_INVALID_FENCE, "PFSOLVE_ERROR_INVALID_FENCE"},
+        {PFSOLVE_ERROR_ONLY_FORWARD_FFT_INITIALIZED, "PFSOLVE_ERROR_ONLY_FORWARD_FFT_INITIALIZED"},
+        {PFSOLVE_ERROR_ONLY_INVERSE_FFT_INITIALIZED, "PFSOLVE_ERROR_ONLY_INVERSE_FFT_INITIALIZED"},
+        {PFSOLVE_ERROR_INVALID_CONTEXT, "PFSOLVE_ERROR_INVALID_CONTEXT"},
+        {PFSOLVE_ERROR_INVALID_PLATFORM, "PFSOLVE_ERROR_INVALID_PLATFORM"},
+        {PFSOLVE_ERROR_ENABLED_saveApplicationToString, "PFSOLVE_ERROR_ENABLED_saveApplicationToString"},
+        {PFSOLVE_ERROR_EMPTY_FILE, "PFSOLVE_ERROR_EMPTY_FILE"},
+        {PFSOLVE_ERROR_EMPTY_FFTdim, "PFSOLVE_ERROR_EMPTY_FFTdim"},
+        {PFSOLVE_ERROR_EMPTY_size, "PFSOLVE_ERROR_EMPTY_size"},
+        {PFSOLVE_ERROR_EMPTY_bufferSize, "PFSOLVE_ERROR_EMPTY_bufferSize"},
+        {PFSOLVE_ERROR_EMPTY_buffer, "PFSOLVE_ERROR_EMPTY_buffer"},
+        {PFSOLVE_ERROR_EMPTY_tempBufferSize, "PFSOLVE_ERROR_EMPTY_tempBufferSize"},
+        {PFSOLVE_ERROR_EMPTY_tempBuffer, "PFSOLVE_ERROR_EMPTY_tempBuffer"},
+        {PFSOLVE_ERROR_EMPTY_inputBufferSize, "PFSOLVE_ERROR_EMPTY_inputBufferSize"},
+        {PFSOLVE_ERROR_EMPTY_inputBuffer, "PFSOLVE_ERROR_EMPTY_inputBuffer"},
+        {PFSOLVE_ERROR_EMPTY_outputBufferSize, "PFSOLVE_ERROR_EMPTY_outputBufferSize"},
+        {PFSOLVE_ERROR_EMPTY_outputBuffer, "PFSOLVE_ERROR_EMPTY_outputBuffer"},
+        {PFSOLVE_ERROR_EMPTY_kernelSize, "PFSOLVE_ERROR_EMPTY_kernelSize"},
+        {PFSOLVE_ERROR_EMPTY_kernel, "PFSOLVE_ERROR_EMPTY_kernel"},
+        {PFSOLVE_ERROR_EMPTY_applicationString, "PFSOLVE_ERROR_EMPTY_applicationString"},
+        {PFSOLVE_ERROR_EMPTY_useCustomBluesteinPaddingPattern_arrays, "PFSOLVE_ERROR_EMPTY_useCustomBluesteinPaddingPattern_arrays"},
+        {PFSOLVE_ERROR_UNSUPPORTED_RADIX, "PFSOLVE_ERROR_UNSUPPORTED_RADIX"},
+        {PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH, "PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH"},
+        {PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_R2C, "PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_R2C"},
+        {PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_DCT, "PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_DCT"},
+        {PFSOLVE_ERROR_UNSUPPORTED_FFT_OMIT, "PFSOLVE_ERROR_UNSUPPORTED_FFT_OMIT"},
+        {PFSOLVE_ERROR_FAILED_TO_ALLOCATE, "PFSOLVE_ERROR_FAILED_TO_ALLOCATE"},
+        {PFSOLVE_ERROR_FAILED_TO_MAP_MEMORY, "PFSOLVE_ERROR_FAILED_TO_MAP_MEMORY"},
+        {PFSOLVE_ERROR_FAILED_TO_ALLOCATE_COMMAND_BUFFERS, "PFSOLVE_ERROR_FAILED_TO_ALLOCATE_COMMAND_BUFFERS"},
+        {PFSOLVE_ERROR_FAILED_TO_BEGIN_COMMAND_BUFFER, "PFSOLVE_ERROR_FAILED_TO_BEGIN_COMMAND_BUFFER"},
+        {PFSOLVE_ERROR_FAILED_TO_END_COMMAND_BUFFER, "PFSOLVE_ERROR_FAILED_TO_END_COMMAND_BUFFER"},
+        {PFSOLVE_ERROR_FAILED_TO_SUBMIT_QUEUE, "PFSOLVE_ERROR_FAILED_TO_SUBMIT_QUEUE"},
+        {PFSOLVE_ERROR_FAILED_TO_WAIT_FOR_FENCES, "PFSOLVE_ERROR_FAILED_TO_WAIT_FOR_FENCES"},
+        {PFSOLVE_ERROR_FAILED_TO_RESET_FENCES, "PFSOLVE_ERROR_FAILED_TO_RESET_FENCES"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_POOL, "PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_POOL"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_SET_LAYOUT, "PFSOLVE_ERROR_FAILED_TO_CREATE_DESCRIPTOR_SET_LAYOUT"},
+        {PFSOLVE_ERROR_FAILED_TO_ALLOCATE_DESCRIPTOR_SETS, "PFSOLVE_ERROR_FAILED_TO_ALLOCATE_DESCRIPTOR_SETS"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE_LAYOUT, "PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE_LAYOUT"},
+        {PFSOLVE_ERROR_FAILED_SHADER_PREPROCESS, "PFSOLVE_ERROR_FAILED_SHADER_PREPROCESS"},
+        {PFSOLVE_ERROR_FAILED_SHADER_PARSE, "PFSOLVE_ERROR_FAILED_SHADER_PARSE"},
+        {PFSOLVE_ERROR_FAILED_SHADER_LINK, "PFSOLVE_ERROR_FAILED_SHADER_LINK"},
+        {PFSOLVE_ERROR_FAILED_SPIRV_GENERATE, "PFSOLVE_ERROR_FAILED_SPIRV_GENERATE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_SHADER_MODULE, "PFSOLVE_ERROR_FAILED_TO_CREATE_SHADER_MODULE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_INSTANCE, "PFSOLVE_ERROR_FAILED_TO_CREATE_INSTANCE"},
+        {PFSOLVE_ERROR_FAILED_TO_SETUP_DEBUG_MESSENGER, "PFSOLVE_ERROR_FAILED_TO_SETUP_DEBUG_MESSENGER"},
+        {PFSOLVE_ERROR_FAILED_TO_FIND_PHYSICAL_DEVICE, "PFSOLVE_ERROR_FAILED_TO_FIND_PHYSICAL_DEVICE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_DEVICE, "PFSOLVE_ERROR_FAILED_TO_CREATE_DEVICE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_FENCE, "PFSOLVE_ERROR_FAILED_TO_CREATE_FENCE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_POOL, "PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_POOL"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_BUFFER, "PFSOLVE_ERROR_FAILED_TO_CREATE_BUFFER"},
+        {PFSOLVE_ERROR_FAILED_TO_ALLOCATE_MEMORY, "PFSOLVE_ERROR_FAILED_TO_ALLOCATE_MEMORY"},
+        {PFSOLVE_ERROR_FAILED_TO_BIND_BUFFER_MEMORY, "PFSOLVE_ERROR_FAILED_TO_BIND_BUFFER_MEMORY"},
+        {PFSOLVE_ERROR_FAILED_TO_FIND_MEMORY, "PFSOLVE_ERROR_FAILED_TO_FIND_MEMORY"},
+        {PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE, "PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE"},
+        {PFSOLVE_ERROR_FAILED_TO_COPY, "PFSOLVE_ERROR_FAILED_TO_COPY"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_PROGRAM, "PFSOLVE_ERROR_FAILED_TO_CREATE_PROGRAM"},
+        {PFSOLVE_ERROR_FAILED_TO_COMPILE_PROGRAM, "PFSOLVE_ERROR_FAILED_TO_COMPILE_PROGRAM"},
+        {PFSOLVE_ERROR_FAILED_TO_GET_CODE_SIZE, "PFSOLVE_ERROR_FAILED_TO_GET_CODE_SIZE"},
+        {PFSOLVE_ERROR_FAILED_TO_GET_CODE, "PFSOLVE_ERROR_FAILED_TO_GET_CODE"},
+        {PFSOLVE_ERROR_FAILED_TO_DESTROY_PROGRAM, "PFSOLVE_ERROR_FAILED_TO_DESTROY_PROGRAM"},
+        {PFSOLVE_ERROR_FAILED_TO_LOAD_MODULE, "PFSOLVE_ERROR_FAILED_TO_LOAD_MODULE"},
+        {PFSOLVE_ERROR_FAILED_TO_GET_FUNCTION, "PFSOLVE_ERROR_FAILED_TO_GET_FUNCTION"},
+        {PFSOLVE_ERROR_FAILED_TO_SET_DYNAMIC_SHARED_MEMORY, "PFSOLVE_ERROR_FAILED_TO_SET_DYNAMIC_SHARED_MEMORY"},
+        {PFSOLVE_ERROR_FAILED_TO_MODULE_GET_GLOBAL, "PFSOLVE_ERROR_FAILED_TO_MODULE_GET_GLOBAL"},
+        {PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL, "PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL"},
+        {PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD, "PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD"},
+        {PFSOLVE_ERROR_FAILED_TO_ADD_NAME_EXPRESSION, "PFSOLVE_ERROR_FAILED_TO_ADD_NAME_EXPRESSION"},
+        {PFSOLVE_ERROR_FAILED_TO_INITIALIZE, "PFSOLVE_ERROR_FAILED_TO_INITIALIZE"},
+        {PFSOLVE_ERROR_FAILED_TO_SET_DEVICE_ID, "PFSOLVE_ERROR_FAILED_TO_SET_DEVICE_ID"},
+        {PFSOLVE_ERROR_FAILED_TO_GET_DEVICE, "PFSOLVE_ERROR_FAILED_TO_GET_DEVICE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_CONTEXT, "PFSOLVE_ERROR_FAILED_TO_CREATE_CONTEXT"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE, "PFSOLVE_ERROR_FAILED_TO_CREATE_PIPELINE"},
+        {PFSOLVE_ERROR_FAILED_TO_SET_KERNEL_ARG, "PFSOLVE_ERROR_FAILED_TO_SET_KERNEL_ARG"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_QUEUE, "PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_QUEUE"},
+        {PFSOLVE_ERROR_FAILED_TO_RELEASE_COMMAND_QUEUE, "PFSOLVE_ERROR_FAILED_TO_RELEASE_COMMAND_QUEUE"},
+        {PFSOLVE_ERROR_FAILED_TO_ENUMERATE_DEVICES, "PFSOLVE_ERROR_FAILED_TO_ENUMERATE_DEVICES"},
+        {PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE, "PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_EVENT, "PFSOLVE_ERROR_FAILED_TO_CREATE_EVENT"},
+        {PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_LIST, "PFSOLVE_ERROR_FAILED_TO_CREATE_COMMAND_LIST"},
+        {PFSOLVE_ERROR_FAILED_TO_DESTROY_COMMAND_LIST, "PFSOLVE_ERROR_FAILED_TO_DESTROY_COMMAND_LIST"},
+        {PFSOLVE_ERROR_FAILED_TO_SUBMIT_BARRIER, "PFSOLVE_ERROR_FAILED_TO_SUBMIT_BARRIER"},
+        {PFSOLVE_ERROR_UNSUPPORTED_COMBINATION, "PFSOLVE_ERROR_UNSUPPORTED_COMBINATION"},
+        {PFSOLVE_ERROR_INVALID_ARGUMENT, "PFSOLVE_ERROR_INVALID_ARGUMENT"},
+        {PFSOLVE_ERROR_CAPACITY, "PFSOLVE_ERROR_CAPACITY"},
+        {PFSOLVE_ERROR_DEVICE_FAULT, "PFSOLVE_ERROR_DEVICE_FAULT"},
+    };
+    for (const auto& e : kNames)
+        if (e.code == result) return e.name;
+    return "PFSOLVE_ERROR_UNKNOWN";
 }
 
-int PfSolveGetVersion(void) { return 102; }
+// The reference's version function returns the literal 00102 (pfSolve.h:101-103),
+// an octal literal whose value is 66.
+int PfSolveGetVersion(void) { return 66; }
 
 uint64_t PfSolveLaunchCount(void) { return g_launches.load(); }
 
 uint64_t PfSolveStreamingLaunchCount(void) { return g_stream_launches.load(); }
+
+PfSolveResult PfSolveGetLastLaunch(PfSolveLaunchInfo* info)
+{
+    if (!info) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    *info = g_last_launch;
+    return PFSOLVE_SUCCESS;
+}
 
 PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread, int* warpsPerSystem,
                               int* groupsPerCTA)

@@ -8,7 +8,10 @@
 // kMaxItems work items per call.  The work counter must start at zero: every
 // call clears it with cudaMemsetAsync on its stream before the launch.  All
 // calls share the one scratch array, so calls whose work overlaps in time
-// (other streams, other host threads) race on it.
+// (other streams, other host threads) race on it.  The host staging arrays
+// are pageable: cudaMemcpyAsync stages them before it returns, so the next
+// call may rewrite them at once.  The caller's current device is restored on
+// every return.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -56,6 +59,32 @@ PfSolveResult scratch_address(int device, unsigned char** out)
     }
     *out = g_scratch_ptr[device];
     return PFSOLVE_SUCCESS;
+}
+
+// Restores the calling thread's current device when the call returns.
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard()
+    {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            cudaGetLastError();
+            saved = -1;
+        }
+    }
+    ~DeviceGuard()
+    {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
+
+// Work items largest first; ties by (entry, first system), so the order is
+// the same on every call.  std::sort sorts in place: no temporary buffer.
+bool item_before(const WorkItem& x, const WorkItem& y)
+{
+    const int64_t a = g_entries[x.entry].op.M * (x.y1 - x.y0), b = g_entries[y.entry].op.M * (y.y1 - y.y0);
+    if (a != b) return a > b;
+    if (x.entry != y.entry) return x.entry < y.entry;
+    return x.y0 < y.y0;
 }
 
 }  // namespace
@@ -142,11 +171,10 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
             w.y0 = y0;
             w.y1 = std::min<int64_t>(entries[e].nsys, y0 + spi);
         }
-    std::stable_sort(g_items, g_items + nitems, [](const WorkItem& x, const WorkItem& y) {
-        return g_entries[x.entry].op.M * (x.y1 - x.y0) > g_entries[y.entry].op.M * (y.y1 - y.y0);
-    });
+    std::sort(g_items, g_items + nitems, item_before);
     if (nitems == 0) return PFSOLVE_SUCCESS;
 
+    DeviceGuard keep_device;
     if (cudaSetDevice(device) != cudaSuccess) return PFSOLVE_ERROR_INVALID_DEVICE;
     int num_sms = 0;
     if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
@@ -154,6 +182,10 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
     unsigned char* scratch = nullptr;
     PfSolveResult res = scratch_address(device, &scratch);
     if (res != PFSOLVE_SUCCESS) return res;
+
+    int maxopt = 0;
+    if (cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+        return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;
 
     // launch shape: as PfSolveBatchCreate (rows per thread 8, else 4)
     const BatchVariant* v = nullptr;
@@ -167,7 +199,15 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
         if (!cand) continue;
         const int g = std::max(1, 8 / (int)w);
         const size_t smem = cand->smem_bytes((int)w, g);
-        if (smem > 48 * 1024 && !allow_max_smem(cand->func)) continue;
+        // the shared-memory opt-in, set directly to the device's maximum as
+        // the plan path sets it (idempotent; the plan path's cache of
+        // opted-in kernels is a std::set, which would allocate)
+        if (smem > 48 * 1024 &&
+            (smem > (size_t)maxopt ||
+             cudaFuncSetAttribute(cand->func, cudaFuncAttributeMaxDynamicSharedMemorySize, maxopt) != cudaSuccess)) {
+            cudaGetLastError();
+            continue;
+        }
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, cand->func, 32 * (int)w * g, smem) != cudaSuccess || b < 1)
             continue;

@@ -9,6 +9,12 @@
 //     uneven-batch launch over all requests of the batch (jw_batch_kernel),
 //     descriptors copied from pinned staging on the same stream;
 //   * double-double: one JW-step launch per request (jw_dd_kernel).
+// Ordering with the caller: the server's streams are non-blocking, so they do
+// not follow the caller's (legacy default or other) stream.  Submit records an
+// event on the request's `stream` (unless the caller marks the input ready)
+// and the flight waits for it before the request's kernel: whatever the
+// caller enqueued before Submit (writing the input, clearing the output)
+// happens first.
 // An event is recorded behind every batch; the worker polls the events of
 // the batches in flight (at least every 20 us while any is), stamps the
 // requests' completion time, releases their bytes and wakes the waiters.
@@ -55,6 +61,7 @@ struct Req {
     uint64_t bytes;
     int cls;  // batch class: precision class and operator kind (one kernel per batch)
     PfSolveResult status = PFSOLVE_SUCCESS;
+    cudaEvent_t ready = nullptr;  // recorded on the caller's stream at submit (nullptr: input ready)
     Clock::time_point t_submit, t_dispatch, t_done;
     bool done = false;
 };
@@ -96,6 +103,7 @@ struct PfSolveServer {
     std::deque<Req*> pending;
     std::unordered_map<uint64_t, Req*> reqs;
     std::vector<Flight> flights;
+    std::vector<cudaEvent_t> ready_pool;  // ordering events not in use (guarded by mu)
     uint64_t next_id = 1;
     uint64_t inflight_bytes = 0, peak_inflight = 0;
     uint64_t submitted = 0, completed = 0, batches = 0, rhs = 0;
@@ -230,9 +238,27 @@ bool reap_flights(PfSolveServer* s)
 }
 
 // Enqueue the batch of flight `fl` (mixed: one uneven-batch launch; dd: one
-// launch per request), then its completion callback.
+// launch per request), then its completion event.  First the flight's
+// stream waits for each request's ordering event; a wait captures the
+// event's state when it is enqueued, so the events go back to the pool
+// right after.
 void launch_flight(PfSolveServer* s, Flight& fl, int cls)
 {
+    for (Req* r : fl.reqs) {
+        if (!r->ready) continue;
+        if (cudaStreamWaitEvent(fl.stream, r->ready, 0) != cudaSuccess) {
+            cudaGetLastError();
+            r->status = PFSOLVE_ERROR_FAILED_TO_SYNCHRONIZE;
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (Req* r : fl.reqs)
+            if (r->ready) {
+                s->ready_pool.push_back(r->ready);
+                r->ready = nullptr;
+            }
+    }
     if (cls == 0) {
         int64_t Mmax = 0, S = 0;
         for (Req* r : fl.reqs) {
@@ -505,9 +531,40 @@ PfSolveResult PfSolveServerSubmit(PfSolveServer* s, const PfSolveRequest* r, uin
     if (r->precision < PFSOLVE_SERVE_MIXED || r->precision > PFSOLVE_SERVE_DD_FP64MEM) return PFSOLVE_ERROR_INVALID_ARGUMENT;
     Req* q = new (std::nothrow) Req();
     if (!q) return PFSOLVE_ERROR_MALLOC_FAILED;
+    if (!r->inputReady) {
+        // the ordering event, recorded on the caller's stream on the server's
+        // device (the caller's current device is restored)
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (!s->ready_pool.empty()) {
+                q->ready = s->ready_pool.back();
+                s->ready_pool.pop_back();
+            }
+        }
+        int saved = -1;
+        if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+        bool ok = cudaSetDevice(s->desc.device) == cudaSuccess;
+        if (ok && !q->ready) ok = cudaEventCreateWithFlags(&q->ready, cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaEventRecord(q->ready, r->stream) == cudaSuccess;
+        if (saved >= 0 && saved != s->desc.device) cudaSetDevice(saved);
+        if (!ok) {
+            cudaGetLastError();
+            if (q->ready) {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->ready_pool.push_back(q->ready);
+            }
+            delete q;
+            return PFSOLVE_ERROR_FAILED_TO_EVENT_RECORD;
+        }
+    }
+    // a rejected request returns its ordering event to the pool
+    auto reject = [&](Req* q_) {
+        if (q_->ready) s->ready_pool.push_back(q_->ready);
+        delete q_;
+    };
     std::unique_lock<std::mutex> lk(s->mu);
     if (r->op < 0 || r->op >= (int)s->ops.size()) {
-        delete q;
+        reject(q);
         return PFSOLVE_ERROR_INVALID_ARGUMENT;
     }
     q->r = *r;
@@ -515,13 +572,13 @@ PfSolveResult PfSolveServerSubmit(PfSolveServer* s, const PfSolveRequest* r, uin
     q->M = o.M;
     q->cls = (r->precision == PFSOLVE_SERVE_MIXED ? 0 : 1000) + 100 * o.KL + 10 * o.KU + o.L.sv;
     if (r->stride && r->stride < q->M) {
-        delete q;
+        reject(q);
         return PFSOLVE_ERROR_INVALID_ARGUMENT;
     }
     const uint64_t elem = (r->precision == PFSOLVE_SERVE_DD) ? 16 : 8;
     q->bytes = (uint64_t)r->nrhs * (uint64_t)q->M * elem * (r->input == r->output ? 1 : 2);
     if (q->bytes > s->desc.hbmBudgetBytes) {
-        delete q;
+        reject(q);
         return PFSOLVE_ERROR_CAPACITY;
     }
     q->id = s->next_id++;
@@ -593,7 +650,11 @@ void PfSolveServerDestroy(PfSolveServer* s)
     for (Flight& fl : s->flights) free_flight_resources(fl);
     for (ServeOp& o : s->ops)
         if (o.bands_dd) cudaFree(o.bands_dd);
-    for (auto& kv : s->reqs) delete kv.second;
+    for (auto& kv : s->reqs) {
+        if (kv.second->ready) cudaEventDestroy(kv.second->ready);
+        delete kv.second;
+    }
+    for (cudaEvent_t e : s->ready_pool) cudaEventDestroy(e);
     delete s;
 }
 

@@ -26,7 +26,8 @@ def declared_functions():
 def test_library_builds_and_loads():
     assert os.path.exists(capi.LIB_PATH), "run make -C pfsolve_b200"
     lib = capi.load()
-    assert lib.PfSolveGetVersion() == 102
+    # the reference returns the literal 00102 (pfSolve.h:101-103): octal, value 66
+    assert lib.PfSolveGetVersion() == 0o102 == 66
 
 
 def test_every_declared_symbol_is_exported():
@@ -48,9 +49,10 @@ int main(void) {
          sizeof(PfSolveConfiguration), sizeof(PfSolveLaunchParams), sizeof(PfSolveApplication),
          sizeof(PfSolve_MapKey_JonesWorland), sizeof(PfSolve_MapKey_dgbmv), sizeof(PfSolve_MapKey_block),
          sizeof(PfSolveBatchEntry), sizeof(PfSolveBatchDesc));
-  printf("sdesc %zu\nsreq %zu\nsstat %zu\n", sizeof(PfSolveServerDesc), sizeof(PfSolveRequest),
-         sizeof(PfSolveServerStats));
-  F(PfSolveRequest, nrhs) F(PfSolveRequest, scaleC) F(PfSolveServerDesc, hbmBudgetBytes)
+  printf("sdesc %zu\nsreq %zu\nsstat %zu\nlinfo %zu\n", sizeof(PfSolveServerDesc), sizeof(PfSolveRequest),
+         sizeof(PfSolveServerStats), sizeof(PfSolveLaunchInfo));
+  F(PfSolveRequest, nrhs) F(PfSolveRequest, scaleC) F(PfSolveRequest, stream) F(PfSolveRequest, inputReady)
+  F(PfSolveLaunchInfo, precision) F(PfSolveLaunchInfo, gridCTAs) F(PfSolveServerDesc, hbmBudgetBytes)
   F(PfSolveServerStats, p50Ms) F(PfSolveServerStats, p99DeviceMs) F(PfSolveConfiguration, kernelPath)
   F(PfSolveConfiguration, jw_type) F(PfSolveConfiguration, jw_control_bitmask)
   F(PfSolveConfiguration, scaleC) F(PfSolveConfiguration, doublePrecision)
@@ -81,6 +83,7 @@ def test_ctypes_layout_matches_c(tmp_path):
     assert int(out["sdesc"]) == ctypes.sizeof(capi.PfSolveServerDesc)
     assert int(out["sreq"]) == ctypes.sizeof(capi.PfSolveRequest)
     assert int(out["sstat"]) == ctypes.sizeof(capi.PfSolveServerStats)
+    assert int(out["linfo"]) == ctypes.sizeof(capi.PfSolveLaunchInfo)
     for key, val in out.items():
         if "." in key:
             T, f = key.split(".")
@@ -118,10 +121,27 @@ def test_validation_errors_before_device_use():
     assert lib.PfSolveAppend(ctypes.byref(capi.PfSolveApplication()), 0, None) == 4
 
 
+def header_result_codes():
+    """(name, value) of every PfSolveResult code the header declares."""
+    text = open(os.path.join(ROOT, "include", "pfsolve_b200.h")).read()
+    body = text[text.index("typedef enum PfSolveResult {"):text.index("} PfSolveResult;")]
+    return [(m.group(1), int(m.group(2))) for m in re.finditer(r"(PFSOLVE_\w+)\s*=\s*(\d+)", body)]
+
+
 def test_error_strings():
+    """Every declared code has its own name (as the reference's
+    getPfSolveErrorString, pfSolve_Structs.h:545 onward); the 92 reference
+    codes keep their numbers."""
     lib = capi.load()
+    codes = header_result_codes()
+    assert len(codes) == 96 and len({v for _, v in codes}) == 96
+    for name, value in codes:
+        assert lib.getPfSolveErrorString(value) == name.encode(), (name, value)
     assert lib.getPfSolveErrorString(0) == b"PFSOLVE_SUCCESS"
+    assert lib.getPfSolveErrorString(4029) == b"PFSOLVE_ERROR_FAILED_TO_COPY"
+    assert lib.getPfSolveErrorString(4055) == b"PFSOLVE_ERROR_FAILED_TO_SUBMIT_BARRIER"
     assert lib.getPfSolveErrorString(5001) == b"PFSOLVE_ERROR_UNSUPPORTED_COMBINATION"
+    assert lib.getPfSolveErrorString(12345) == b"PFSOLVE_ERROR_UNKNOWN"
 
 
 def test_app_library_keys_order_and_lookup():
@@ -163,9 +183,9 @@ def test_server_argument_checks_before_device_use():
 
 
 def test_integration_example_compiles_and_links(tmp_path):
-    """The C caller in INTEGRATION.md builds against the header and links the library."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    code = text.split("```c\n", 1)[1].split("```", 1)[0]
+    """The C caller quoted in the integration guide (tests/abi_example.c)
+    builds against the header and links the library."""
+    code = open(os.path.join(ROOT, "tests", "abi_example.c")).read()
     src = tmp_path / "jw_step.c"
     src.write_text(code + "\nint main(void) { return 0; }\n")
     cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"

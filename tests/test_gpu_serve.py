@@ -69,6 +69,9 @@ def test_each_request_matches_oracle_alone_and_in_mix():
         srv.wait(t)
         alone.append(r["out"].cpu().numpy().copy())
         r["out"].zero_()
+    # the clears are done before the mix starts (each request also waits for
+    # the default stream's work queued before its submit)
+    torch.cuda.synchronize()
     # in the mix: all submitted back to back, batched and overlapped
     tickets = [srv.submit(r["op"], r["spec"].precision, r["spec"].nrhs, r["inp"], r["out"]) for r in reqs]
     for t in tickets:
@@ -94,6 +97,40 @@ def test_each_request_matches_oracle_alone_and_in_mix():
             bad.append((i, sp, e_alone, e_mix, d))
     srv.close()
     assert not bad, bad
+
+
+@pytest.mark.parametrize("precision", [MIXED, DD])
+def test_submit_waits_for_pending_default_stream_write(precision):
+    """A request submitted while the caller's default-stream write of its input
+    (and clear of its output) is still queued behind a long kernel reads the
+    written input: the request's kernel waits for the event Submit records on
+    the caller's stream.  Checked against the __float128 oracle."""
+    import torch
+
+    from pfsolve_b200.serving import Server
+    M, nrhs = 256, 64
+    srv = Server(streams=2, max_batch_requests=4)
+    bands = WL.serve_operator_bands(np.random.default_rng(M), M)
+    tb = torch.from_numpy(bands).cuda()
+    op = srv.add_operator(M, tb)
+    rng = np.random.default_rng(17)
+    rhs = rng.uniform(-1, 1, M * nrhs)
+    if precision == DD:
+        rhs = O.to_dd(rhs)
+    src = torch.from_numpy(rhs).cuda()
+    inp = torch.full_like(src, 1e30)   # a stale input the request must not see
+    out = torch.full_like(src, 7.0)
+    torch.cuda.synchronize()
+    torch.cuda._sleep(200_000_000)     # ~0.1 s of GPU spinning on the default stream (bounded by its cycle count)
+    inp.copy_(src)                     # queued behind it
+    out.zero_()
+    t = srv.submit(op, precision, nrhs, inp, out)   # stream None: the legacy default stream
+    srv.wait(t)
+    got = out.cpu().numpy()
+    srv.close()
+    r = dict(spec=WL.ServeRequestSpec(M, nrhs, precision), bands=bands, rhs=rhs)
+    e = _oracle_err(r, got)
+    assert e <= (1e-27 if precision == DD else 1e-12), e
 
 
 def test_admission_by_hbm_budget():

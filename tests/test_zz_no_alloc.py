@@ -4,17 +4,34 @@ PfSolveBatchAppend on the same descriptor, through the C ABI.
 
 Both run the same kernel with the same rows per thread and systems per item,
 so every system agrees to 1e-13 relative L2 (observed: identical); checked on
-two calls in a row.  Capacity errors need no device work."""
+two calls in a row.  A sample of degrees is also checked against the
+__float128 oracle chain (dgbmv -> JW step -> block 307) at 1e-13, so that the
+two paths cannot agree on a wrong answer.  After a warm-up call, further calls
+leave the device's free memory unchanged, launch exactly one kernel each and
+leave the caller's current device as it was.  Capacity errors need no device
+work."""
 import ctypes
 
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from pfsolve_b200 import capi
 from pfsolve_b200 import workloads as WL
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-13
+
+
+def _oracle_degree(step, k):
+    """The degree-k systems of an uneven step by the __float128 oracle chain."""
+    l, N, ns = int(step.ls[k]), int(step.Ns[k]), int(step.nsys[k])
+    off = int(step.rhs_offsets[k])
+    rhs = step.rhs[off:off + 2 * N * ns]
+    y = O.dgbmv(O.Case(M=N, batch=2 * ns, LDA=3, KU=1, KL=1, jw_type=0), step.dgbmv[k], rhs)
+    x = O.jw_step(O.Case(M=N, batch=2 * ns, upperBanded=0, jw_type=13), step.jw_bands[k], y, "q")
+    cb = O.Case(M=N, batch=ns, block=307, lshift=l, jw_type=0, bitmask=O.RUNTIME_SCALEC, run_scaleC=step.scale_s)
+    return O.block(cb, x, np.zeros(2 * N * ns))
 
 
 def _entry_array(entries):
@@ -57,6 +74,13 @@ def test_noalloc_matches_batch_append_twice():
     b.close()
     desc = capi.PfSolveBatchDesc(**shape)
     arr = _entry_array(ents)
+    # the oracle on a sample of degrees (first, middle, last) of the reference path
+    for k in (0, len(step.ls) // 2, len(step.ls) - 1):
+        N, ns = int(step.Ns[k]), int(step.nsys[k])
+        off = int(step.rhs_offsets[k])
+        o = _oracle_degree(step, k).reshape(ns, 2 * N)
+        r = ref[off:off + 2 * N * ns].reshape(ns, 2 * N)
+        assert (np.linalg.norm(r - o, axis=1) / np.linalg.norm(o, axis=1)).max() <= TOL, k
     for call in range(2):
         out.zero_()
         torch.cuda.synchronize()
@@ -71,6 +95,47 @@ def test_noalloc_matches_batch_append_twice():
             r = ref[off:off + 2 * N * ns].reshape(ns, 2 * N)
             worst = max(worst, float((np.linalg.norm(g - r, axis=1) / np.linalg.norm(r, axis=1)).max()))
         assert worst <= TOL, (call, worst)
+
+
+def test_noalloc_allocates_nothing_and_keeps_the_device():
+    """After a warm-up call (which loads the kernel and looks up the array's
+    address), calls change neither the device's free memory nor the caller's
+    current device, and each launches exactly one kernel."""
+    import torch
+
+    lib = capi.load()
+    step = WL.config4(lmax=31, Nmax=128, seed=9)
+    inp = torch.from_numpy(step.rhs).cuda()
+    out = torch.zeros_like(inp)
+    keep, ents = [], []
+    for k, (l, N, ns) in enumerate(zip(step.ls, step.Ns, step.nsys)):
+        tj = torch.from_numpy(step.jw_bands[k]).cuda()
+        ta = torch.from_numpy(step.dgbmv[k]).cuda()
+        keep += [tj, ta]
+        off = 8 * int(step.rhs_offsets[k])
+        ents.append(dict(M=int(N), nsys=int(ns), bands=tj.data_ptr(), dgbmvBands=ta.data_ptr(), lshift=int(l),
+                         scaleS=step.scale_s, input=inp.data_ptr() + off, output=out.data_ptr() + off))
+    desc = capi.PfSolveBatchDesc(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=307)
+    arr = _entry_array(ents)
+    assert lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(desc), arr, len(ents), None) == capi.PFSOLVE_SUCCESS
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    dev0 = torch.cuda.current_device()
+    for _ in range(5):
+        n0 = lib.PfSolveLaunchCount()
+        assert lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(desc), arr, len(ents), None) == capi.PFSOLVE_SUCCESS
+        assert lib.PfSolveLaunchCount() == n0 + 1
+        assert torch.cuda.current_device() == dev0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    # the result of the last call against the oracle on one degree
+    k = len(step.ls) - 1
+    N, ns = int(step.Ns[k]), int(step.nsys[k])
+    off = int(step.rhs_offsets[k])
+    o = _oracle_degree(step, k).reshape(ns, 2 * N)
+    g = out.cpu().numpy()[off:off + 2 * N * ns].reshape(ns, 2 * N)
+    assert (np.linalg.norm(g - o, axis=1) / np.linalg.norm(o, axis=1)).max() <= TOL
 
 
 def test_noalloc_capacity_and_argument_errors():
