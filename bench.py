@@ -404,7 +404,34 @@ def extras_arm(args):
     d = (res["mixed"] - res["fp64"]).view(B, M).norm(dim=1) / res["fp64"].view(B, M).norm(dim=1)
     out["config3_mixed_vs_fp64_rel_l2_max"] = float(d.max().item())
     out["config3_mixed_speedup"] = out["config3_fp64"]["ms"] / out["config3_mixed"]["ms"]
-    del res, base
+    # the same system and right-hand sides on FP32 storage (8-byte rows: 4 bytes
+    # in, 4 out): the reference's default precision (FP32 arithmetic) and
+    # doublePrecisionFloatMemory (FP64 arithmetic); error against the FP64 result
+    tb32 = tb.float()
+    base32 = base.float()
+    bytes32 = 2.0 * M * 4 * B + 3 * M * 4
+    for name, dpfm in (("f32", 0), ("f32mem", 1)):
+        x = base32.clone()
+        app = App(buffer=tb32, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=0,
+                  doublePrecisionFloatMemory=dpfm, scaleC=1.0)
+        app.append()
+        torch.cuda.synchronize()
+        err = ((x.double() - res["fp64"]).view(B, M).norm(dim=1) / res["fp64"].view(B, M).norm(dim=1)).max().item()
+        for _ in range(3):
+            app.append()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            app.append()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[f"config3_{name}"] = {"rhs_per_s": B / (ms * 1e-3), "ms": ms, "gbs": bytes32 / (ms * 1e-3) / 1e9,
+                                  "rel_l2_vs_fp64_max": err, "kernel": app.shape(),
+                                  "speedup_vs_fp64": out["config3_fp64"]["ms"] / ms}
+        app.close()
+        del x
+    del res, base, base32, tb32
     out["config1_latency"] = config1_measure()
     step = WL.config4()
     dev = torch.device("cuda")
@@ -446,6 +473,8 @@ def extras_arm(args):
     torch.cuda.empty_cache()
     # long systems, beyond one CTA group (the reference's multi-upload range)
     out["long_t13_N16384_B8192"] = long_measure(16384, 8192)
+    out["long_t13_N16384_B8192_two_pass"] = long_measure(16384, 8192, path=3)
+    out["long_t13_N65536_B2048"] = long_measure(65536, 2048)
     out["alt_t113_N1024_B131072"] = alt_measure(1024, 131072)
     out["alt_t113_N1024_B131072_group"] = alt_measure(1024, 131072, path=1)
     torch.cuda.empty_cache()
@@ -583,9 +612,9 @@ def config3_profile(args):
 
 def long_measure(M, B, steps=10, warmup=3, path=0):
     """A long tridiagonal system (config 3's coefficients at N = M rows), B
-    real right-hand sides in place, FP64: the two-pass long-system kernel
-    (path 2: the cluster kernel).  Algorithmic bytes: M rows read and written
-    per system."""
+    real right-hand sides in place, FP64: the single-pass long-system kernel
+    (path 3: the two-pass form; path 2: the cluster kernel).  Algorithmic
+    bytes: M rows read and written per system."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -785,9 +814,9 @@ def main():
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
-    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2],
-                    help="kernelPath: 0 streaming kernel where possible (long systems: two passes), "
-                         "1 group kernel only, 2 long systems on the cluster kernel")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="kernelPath: 0 streaming kernel where possible (long systems: single pass), "
+                         "1 group kernel only, 2 long systems on the cluster kernel, 3 long systems in two passes")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu = True

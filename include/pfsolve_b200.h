@@ -216,6 +216,12 @@ typedef struct {
     int64_t outputZeropad[2];
     double scaleC;
 
+    /* Precision, in the reference's order (pfSolve_InitAPIParameters.h:148-245):
+     * quadDoubleDoublePrecision, quadDoubleDoublePrecisionDoubleMemory, doublePrecision,
+     * doublePrecisionFloatMemory; none of them: FP32 storage and arithmetic (the reference's
+     * default).  The FP32-storage precisions cover the JW application with M <= 4096 and K = 1
+     * (no ALT mode, no mixedPrecisionRefinement), dgbmv, block and fused chains; buffers then
+     * hold FP32 values, and offsets and strides count FP32 elements. */
     uint64_t doublePrecision;                       /* FP64 storage and arithmetic */
     uint64_t quadDoubleDoublePrecision;             /* double-double storage and arithmetic */
     uint64_t quadDoubleDoublePrecisionDoubleMemory; /* double-double arithmetic, FP64 storage */
@@ -244,8 +250,9 @@ typedef struct {
                                      FP64 residual refinement sweeps, FP64 storage (0: plain FP64) */
     int rowsPerThread;            /* 0: autotuned; else 2, 4, 8, 16 or 32 (32: streaming kernel only) */
     int kernelPath;               /* 0: streaming kernel wherever a launch allows it, else the group
-                                     kernel (long systems: the two-pass kernel); 1: group kernel only;
-                                     2: long systems on the cluster kernel */
+                                     kernel (long systems: the single pass); 1: group kernel only;
+                                     2: long systems on the cluster kernel (M <= 16384); 3: long systems
+                                     in two passes (no waits between CTAs) */
 } PfSolveConfiguration;
 
 /* Launch-time values (pfSolve_Structs.h:383-449). */
@@ -462,10 +469,12 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * system per lane in one sweep wherever a launch's buffers allow it
  * (16-byte-aligned rows, stride >= the rows written, full output window;
  * groupsPerCTA = warps per CTA), else the K-step kernel; streaming = 5: long
- * systems (M > 4096) in two passes over slices of 32 x warpsPerSystem x
- * rowsPerThread rows, groupsPerCTA systems in flight per CTA (no waits
- * between CTAs; the plan holds a record of 64 bytes per system and slice and
- * every slice's coefficient table).
+ * systems (M > 4096) over slices of 32 x warpsPerSystem x rowsPerThread rows,
+ * groupsPerCTA systems in flight per CTA: a single cooperative pass whose
+ * CTAs wait (bounded) for the other slices of each system, or (kernelPath 3)
+ * two passes with no waits between CTAs; the plan holds a record of 64 bytes
+ * and a 4-byte flag per system and slice, and every slice's coefficient
+ * table.
  * No counterpart in the reference. */
 PFSOLVE_API PfSolveResult PfSolveGetShape(const PfSolveApplication* app, int* streaming, int* rowsPerThread,
                                           int* warpsPerSystem, int* groupsPerCTA);

@@ -383,6 +383,7 @@ def write_reference_case(case_dir: str, case: Case, bands, rhs: np.ndarray, *,
         "LDA": case.LDA, "KU": case.KU, "KL": case.KL, "block": case.block, "lshift": case.lshift,
         "ALT_dgbmv": case.ALT_dgbmv,
         "doublePrecision": 1 if precision in ("f64",) else 0,
+        "doublePrecisionFloatMemory": 1 if precision == "f32mem" else 0,
         "quadDoubleDoublePrecision": 1 if precision == "dd" else 0,
         "iters": iters,
         "K": K,
@@ -392,7 +393,7 @@ def write_reference_case(case_dir: str, case: Case, bands, rhs: np.ndarray, *,
     with open(os.path.join(case_dir, "params.txt"), "w") as f:
         for k, v in kv.items():
             f.write(f"{k}={v}\n")
-    dt = np.float32 if precision == "f32" else np.float64
+    dt = np.float32 if precision in ("f32", "f32mem") else np.float64
     if isinstance(bands, (list, tuple)):
         for k, b in enumerate(bands):
             np.ascontiguousarray(b, dtype=dt).tofile(os.path.join(case_dir, f"bands_{k}.bin"))

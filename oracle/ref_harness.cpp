@@ -127,6 +127,7 @@ int main(int argc, char** argv)
     cfg.doublePrecision = I("doublePrecision", 1);
     cfg.quadDoubleDoublePrecision = I("quadDoubleDoublePrecision", 0);
     cfg.quadDoubleDoublePrecisionDoubleMemory = I("quadDoubleDoublePrecisionDoubleMemory", 0);
+    cfg.doublePrecisionFloatMemory = I("doublePrecisionFloatMemory", 0);
     cfg.isOutputFormatted = 1;
     cfg.jw_type = (int)I("jw_type", 0);
     cfg.upperBanded = (int)I("upperBanded", 0);

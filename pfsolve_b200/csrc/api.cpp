@@ -30,7 +30,7 @@ std::atomic<uint64_t> g_stream_launches{0};
 enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3 };
 
 constexpr int64_t kMaxRows = 4096;       // one CTA group per system (<= 8 warps x 32 x 16 rows)
-constexpr int64_t kMaxRowsLong = 16384;  // JW apps: one cluster of up to 8 CTAs x 2048 rows per system
+constexpr int64_t kMaxRowsLong = 65536;  // JW apps: up to 64 slices of 1024 rows per system (single pass)
 
 struct AppState {
     AppKind kind;
@@ -39,7 +39,7 @@ struct AppState {
     // JW / dgbmv plan
     int R = 0, W = 1, G = 1;
     int mvj = MVJ_NONE, sv = SV_NONE, KL = 0, KU = 0;
-    int prec = 0;           // 0: FP64, 1: FP32 solve + FP64 refinement
+    int prec = 0;           // PREC_*: FP64, FP32 solve + FP64 refinement, dd, FP32, FP64 on FP32 storage
     bool R_fixed = false;   // rows per thread requested by the caller
     int refine_sweeps = 1;  // FP32 solves per system in the mixed mode
     const JwVariant* variant = nullptr;
@@ -53,6 +53,9 @@ struct AppState {
     const LongVariant* long_v = nullptr;
     int long_NS = 0, long_grid = 0;
     double* long_red = nullptr;  // per (system, slice) records, then per-slice constants
+    unsigned* long_flags = nullptr;  // single pass: per (system, slice) publication flags
+    unsigned long_epoch = 0;         // single pass: flag value of the latest launch
+    bool long_single = true;         // single pass (else pass 1, carries, pass 2: kernelPath 3)
     int64_t long_batch = 0;      // systems the records hold
     int64_t plan_batch = 0;      // right-hand sides of the plan (size[1] * size[2])
     bool cluster_only = false;   // kernelPath 2
@@ -154,7 +157,7 @@ int pick_rows_per_thread(int64_t M, int requested)
 bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool alt = false)
 {
     s->stream_v = nullptr;
-    if ((s->prec != PREC_F64 && s->prec != PREC_MIXED) || s->no_stream) return false;
+    if ((s->prec != PREC_F64 && s->prec != PREC_MIXED && !prec_f32_storage(s->prec)) || s->no_stream) return false;
     int cand[3][2];
     int n = 0;
     const int prefs[3] = {16, 32, 8};
@@ -196,31 +199,42 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
     return false;
 }
 
-// Two-pass variant for long real systems: the first compiled shape that fits
-// and whose rows per thread divide M (16, else 8: M must be a multiple of 8),
-// with its per-(system, slice) records allocated for the plan's right-hand
-// sides.
+// Long-system variant for real systems: the first compiled shape that fits
+// and, for two passes, whose rows per thread divide M (16, else 8: M a
+// multiple of 8); the single pass takes any M (its last partial chunk moves
+// outside the TMA boxes).  The per-(system, slice) records are allocated for
+// the plan's right-hand sides.
 bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {
     s->long_v = nullptr;
     if (s->prec != PREC_F64 || s->no_stream || s->cluster_only || LIN != LAY_REAL || LOUT != LAY_REAL || SCALE ||
-        M % 8 != 0 || s->plan_batch < 1)
+        (!s->long_single && M % 8 != 0) || s->plan_batch < 1)
         return false;
     for (int shape = 0; shape < kLongShapes; ++shape) {
         const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
         if (!v) return false;
-        if (M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
+        if (!s->long_single && M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
         const int b = v->blocks_per_sm();
         if (b < 1) continue;
         const int NS = (int)((M + v->S - 1) / v->S);
         const int64_t res = (int64_t)b * s->num_sms;
         // CTAs in whole multiples of NS, at most one CTA's worth of systems each
         const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
-        // records, slice constants, slice tables, PASS 1 weights (16 bytes per row)
+        if (s->long_single && NS > kLongMaxSlices) continue;
+        // records, slice constants, slice tables, PASS 1 weights (16 bytes per
+        // row), then the single pass's flags (4 bytes per system and slice)
+        const size_t fbytes = (size_t)s->plan_batch * NS * sizeof(unsigned);
         const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) +
-                             (size_t)NS * v->tbl_bytes + (size_t)NS * v->S * 16;
+                             (size_t)NS * v->tbl_bytes + (size_t)NS * v->S * 16 + fbytes;
         if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
             cudaGetLastError();
+            s->long_red = nullptr;
+            return false;
+        }
+        s->long_flags = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(s->long_red) + bytes - fbytes);
+        if (cudaMemset(s->long_flags, 0, fbytes) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(s->long_red);
             s->long_red = nullptr;
             return false;
         }
@@ -355,9 +369,9 @@ PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCAL
 // layout R T entries apart (pfSolve_JonesWorland.h:209-222, 262-271,
 // pfSolve_ReadWrite.h:1705-1711).  K = 1; plan-time band offsets only (the
 // reference rescales only those); FP64 or FP32 solve + FP64 refinement.
-PfSolveResult plan_alt(AppState* s, const PfSolveConfiguration& c, int dd_prec)
+PfSolveResult plan_alt(AppState* s, const PfSolveConfiguration& c, int base_prec)
 {
-    if (c.numConsecutiveJWIterations > 1 || dd_prec) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (c.numConsecutiveJWIterations > 1 || base_prec != PREC_F64) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     if (c.jw_control_bitmask & (RUNTIME_OFFSETM | RUNTIME_OFFSETV)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     if (c.upperBanded < 0 || c.upperBanded > 2) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     const int64_t M = c.M_size;
@@ -496,6 +510,7 @@ void fill_operator_common(AppState* s, const PfSolveConfiguration& c, JwOperator
     set_band_order(c.M_size, op);
     op.scaleC = 1.0;
     op.refine_sweeps = s->refine_sweeps;
+    op.bands32 = prec_f32_storage(s->prec) ? 1 : 0;
 }
 
 // Tensor maps of recent launches (encoding is host work; steady-state
@@ -515,13 +530,13 @@ bool same_io(const JwIO& a, const JwIO& b)
            a.out_off == b.out_off && a.out_stride == b.out_stride && a.nsys == b.nsys && a.M == b.M;
 }
 
-const MapCacheEntry* row_maps(const void* key, int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io)
+const MapCacheEntry* row_maps(const void* key, int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io, int es = 8)
 {
     for (const MapCacheEntry& e : g_map_cache)
         if (e.valid && e.v == key && same_io(e.io, io)) return &e;
     MapCacheEntry& e = g_map_cache[g_map_next++ % 8];
     e.valid = false;
-    if (!encode_row_maps(R, LIN, LOUT, IB, IBO, io, &e.in, &e.out)) return nullptr;
+    if (!encode_row_maps(R, LIN, LOUT, IB, IBO, io, &e.in, &e.out, es)) return nullptr;
     e.v = key;
     e.io = io;
     e.valid = true;
@@ -530,7 +545,7 @@ const MapCacheEntry* row_maps(const void* key, int R, int LIN, int LOUT, int IB,
 
 const MapCacheEntry* stream_maps(const StreamVariant* v, const JwIO& io)
 {
-    return row_maps(v, v->R, v->LIN, v->LOUT, v->IB, v->IBO, io);
+    return row_maps(v, v->R, v->LIN, v->LOUT, v->IB, v->IBO, io, prec_f32_storage(v->PREC) ? 4 : 8);
 }
 
 // Long systems: the cluster kernel, under the streaming kernel's buffer rules.
@@ -558,17 +573,21 @@ PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cud
     const LongVariant* v = s->long_v;
     if (io.accumulate || io.oz0 > 0 || io.oz1 < io.M || io.nsys > s->long_batch)
         return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-    const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, io);
+    JwIO mio = io;  // the maps cover the whole chunks of R rows
+    mio.M = (io.M / v->R) * v->R;
+    const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, mio);
     if (!e) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     double* cst = s->long_red + (size_t)s->long_batch * s->long_NS * 8;
     double* tab = cst + (size_t)s->long_NS * 8;
-    const cudaError_t err =
-        v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, tab, s->long_NS);
+    if (++s->long_epoch == 0) s->long_epoch = 1;  // 0 is the flags' initial value
+    const cudaError_t err = v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, tab,
+                                      s->long_NS, s->long_flags, s->long_epoch, s->long_single);
     note_launch(true);
     record_launch(PFSOLVE_KERNEL_LONG, v->R, v->W, v->G, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0, PREC_F64, 0,
                   s->long_grid);
-    // the table passes, the carry kernel (solves only) and pass 2
-    g_launches.fetch_add((s->sv != SV_NONE ? 3 : 2) + (s->sv == SV_TRI ? 1 : 0), std::memory_order_relaxed);
+    // the table passes, and for two passes the carry kernel (solves only) and pass 2
+    g_launches.fetch_add((s->long_single ? 1 : (s->sv != SV_NONE ? 3 : 2)) + (s->sv == SV_TRI ? 1 : 0),
+                         std::memory_order_relaxed);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
@@ -814,8 +833,9 @@ PfSolveResult append_dgbmv(PfSolveApplication* app, const PfSolveLaunchParams* l
         io.M = c.M_size;
         return launch_jw_variant(s, op, io, stream);
     }
-    if (s->prec) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    if (s->prec && !prec_f32_storage(s->prec)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     DgbmvArgs a;
+    a.f32 = prec_f32_storage(s->prec) ? 1 : 0;
     a.A = static_cast<const double*>(r.bands);
     a.x = static_cast<double*>(r.rhs);
     a.M = c.M_size;
@@ -843,6 +863,7 @@ PfSolveResult append_block(PfSolveApplication* app, const PfSolveLaunchParams* l
     if (res != PFSOLVE_SUCCESS) return res;
     if (!r.bands) return PFSOLVE_ERROR_EMPTY_buffer;
     BlockArgs a;
+    a.f32 = prec_f32_storage(s->prec) ? 1 : 0;
     a.in = static_cast<const double*>(r.bands);
     a.out = static_cast<double*>(r.rhs);
     a.size0 = (int64_t)c.size[0];
@@ -1070,22 +1091,29 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
             }
         }
     }
-    // Precision: FP64 (doublePrecision, optionally with FP32-solve refinement),
-    // double-double storage (quadDoubleDoublePrecision) or double-double
-    // arithmetic on FP64 storage (quadDoubleDoublePrecisionDoubleMemory).
+    // Precision, in the reference's order (pfSolve_InitAPIParameters.h:148-245,
+    // pfSolve_Plan_JonesWorland.h:244-264): double-double storage
+    // (quadDoubleDoublePrecision) or arithmetic on FP64 storage
+    // (quadDoubleDoublePrecisionDoubleMemory); FP64 (doublePrecision,
+    // optionally with the FP32-solve refinement extension); FP64 arithmetic on
+    // FP32 storage (doublePrecisionFloatMemory); else FP32 storage and
+    // arithmetic, the reference's default.
     const bool ddmem = c.quadDoubleDoublePrecision != 0;
     const bool ddf64 = !ddmem && c.quadDoubleDoublePrecisionDoubleMemory != 0;
-    const bool fp64 = (c.doublePrecision && !ddmem && !ddf64 && !c.doublePrecisionFloatMemory) || ddmem || ddf64;
     const int dd_prec = ddmem ? 2 : (ddf64 ? 3 : 0);
+    const int base_prec = dd_prec                        ? dd_prec
+                          : c.doublePrecision            ? PREC_F64
+                          : c.doublePrecisionFloatMemory ? PREC_F64_F32MEM
+                                                         : PREC_F32;
     PfSolveResult r = PFSOLVE_SUCCESS;
     if (c.jw_type >= 10) {
         s->kind = APP_JW;
-        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-        else if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
-        else if (((c.jw_type / 100) % 10) == 1) r = plan_alt(s, c, dd_prec);
+        if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
+        else if (c.mixedPrecisionRefinement && base_prec != PREC_F64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (((c.jw_type / 100) % 10) == 1) r = plan_alt(s, c, base_prec);
         else if (c.upperBanded < 0 || c.upperBanded > 2) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (c.numConsecutiveJWIterations > 1) {
-            s->prec = dd_prec;
+            s->prec = base_prec;
             r = plan_steps(s, c);
         }
         else if (c.M_size > kMaxRowsLong || c.M_size < 1) r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH;
@@ -1095,7 +1123,9 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
             else {
                 s->mvj = L.mvj;
                 s->sv = L.sv;
-                s->prec = dd_prec ? dd_prec : ((c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? 1 : 0);
+                s->prec = base_prec != PREC_F64 ? base_prec
+                                                : ((c.mixedPrecisionRefinement > 0 && L.sv != SV_NONE) ? PREC_MIXED
+                                                                                                       : PREC_F64);
                 s->refine_sweeps = 1 + c.mixedPrecisionRefinement;
                 s->KL = (L.mvj == MVJ_LOWER) ? 1 : 0;
                 s->KU = (L.mvj == MVJ_UPPER) ? 1 : 0;
@@ -1104,14 +1134,15 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->R_req = c.rowsPerThread;
                 s->no_stream = c.kernelPath == 1;
                 s->cluster_only = c.kernelPath == 2;
+                s->long_single = c.kernelPath != 3;
                 s->plan_batch = (int64_t)c.size[1] * (int64_t)(c.size[2] ? c.size[2] : 1);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
         }
     } else if (c.LDA > 0) {
         s->kind = APP_DGBMV;
-        if (!fp64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
-        else if (c.KU < 0 || c.KU >= c.LDA) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
+        s->prec = base_prec;
+        if (c.KU < 0 || c.KU >= c.LDA) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
         else if (c.ALT_dgbmv && (c.LDA > 64 || dd_prec)) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else {
             // ALT_dgbmv (pfSolve_Plan_dgbmv.h:100, pfSolve_MatVecMul.h:390) drops band j
@@ -1128,7 +1159,6 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->KU = c.KU;
                 s->sv = SV_NONE;
                 s->mvj = MVJ_NONE;
-                s->prec = dd_prec;
                 s->R = pick_rows_per_thread(c.M_size, c.rowsPerThread);
                 if (s->R < 4) s->R = 4;
                 s->R_req = c.rowsPerThread;
@@ -1140,7 +1170,8 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
     } else if (c.block > 0) {
         s->kind = APP_BLOCK;
         const int bt = c.block % 10, acc = (c.block / 10) % 10, sk = c.block / 100;
-        if (!fp64 || dd_prec) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        s->prec = base_prec;
+        if (dd_prec) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (bt < 1 || bt > 7 || (acc != 0 && acc != 2) || sk > 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
         else if (acc == 2 && bt == 4) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     } else {
@@ -1248,6 +1279,12 @@ PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchPara
     io.out_stride = rj.oS;
     io.nsys = rj.batch;
     int LIN = LAY_REAL, LOUT = LAY_REAL, SCALE = 0;
+    // with FP32 storage anywhere along the chain, one precision for all of it
+    auto same_storage = [&](PfSolveApplication* a) {
+        const int pa = st(a)->prec;
+        return !(prec_f32_storage(pa) || prec_f32_storage(sj->prec)) || pa == sj->prec;
+    };
+    if ((dg && !same_storage(dg)) || (bl && !same_storage(bl))) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     if (dg) {
         const PfSolveConfiguration& cd = dg->configuration;
         Resolved rd;

@@ -97,6 +97,31 @@ __device__ __forceinline__ double2 to_f64(float2 v) { return make_double2((doubl
 template <class V> struct Lower;
 template <> struct Lower<double> { using type = float; };
 template <> struct Lower<double2> { using type = float2; };
+template <> struct Lower<float> { using type = float; };
+template <> struct Lower<float2> { using type = float2; };
+
+// Two-component vector of a scalar type (complex values: re, im).
+template <class S> struct Vec2Of;
+template <> struct Vec2Of<double> { using type = double2; };
+template <> struct Vec2Of<float> { using type = float2; };
+
+// Value conversions between storage and arithmetic types (FP32 <-> FP64,
+// real or complex; round to nearest when narrowing).
+__device__ __forceinline__ void cvt(double& d, double s) { d = s; }
+__device__ __forceinline__ void cvt(double& d, float s) { d = (double)s; }
+__device__ __forceinline__ void cvt(float& d, double s) { d = __double2float_rn(s); }
+__device__ __forceinline__ void cvt(float& d, float s) { d = s; }
+__device__ __forceinline__ void cvt(double2& d, double2 s) { d = s; }
+__device__ __forceinline__ void cvt(double2& d, float2 s) { d = make_double2((double)s.x, (double)s.y); }
+__device__ __forceinline__ void cvt(float2& d, double2 s) { d = make_float2(__double2float_rn(s.x), __double2float_rn(s.y)); }
+__device__ __forceinline__ void cvt(float2& d, float2 s) { d = s; }
+template <class D, class S>
+__device__ __forceinline__ D conv(S s)
+{
+    D d;
+    cvt(d, s);
+    return d;
+}
 
 template <int R> struct Log2 { static constexpr int v = (R <= 1) ? 0 : 1 + Log2<R / 2>::v; };
 template <> struct Log2<1> { static constexpr int v = 0; };
@@ -126,6 +151,19 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     int src = valid ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid)
+{
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int src = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
+}
+// One element of 4 or 8 bytes (an FP32 or FP64 value).
+template <class T>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, bool valid)
+{
+    if constexpr (sizeof(T) == 4) cp_async4(smem, gmem, valid);
+    else cp_async8(smem, gmem, valid);
 }
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid)
 {

@@ -34,6 +34,10 @@
 //  * PREC_MIXED: FP64 storage, the solve factors rounded to FP32 and applied
 //    in FP32; the residual r = V*A*b - M*x and the correction accumulation run
 //    in FP64 (iterative refinement, all on chip: b is never re-read).
+//  * PREC_F32 / PREC_F64_F32MEM: FP32 storage (right-hand sides and bands),
+//    FP32 or FP64 arithmetic (the reference's precision 0 and its
+//    doublePrecisionFloatMemory).  The coefficients are still formed in FP64
+//    from the FP32 bands, then held in the arithmetic type.
 #pragma once
 #include <type_traits>
 
@@ -47,7 +51,12 @@ struct JwCfg {
     static constexpr int kR = R, kKL = KL, kKU = KU, kSV = SV, kLIN = LIN, kLOUT = LOUT, kPrec = PREC;
     static constexpr bool kScale = SCALE;
     static constexpr bool kCplx = (LIN != LAY_REAL);
-    using V = typename std::conditional<kCplx, double2, double>::type;
+    static constexpr bool kF32Mem = prec_f32_storage(PREC);  // FP32 storage
+    static constexpr bool kF32 = (PREC == PREC_F32);          // FP32 arithmetic
+    using MS = typename std::conditional<kF32, float, double>::type;  // arithmetic scalar
+    using T = typename std::conditional<kF32Mem, float, double>::type;  // storage scalar
+    using V = typename std::conditional<kCplx, typename Vec2Of<MS>::type, MS>::type;
+    using TS = typename std::conditional<kCplx, typename Vec2Of<T>::type, T>::type;  // staged element
     using VF = typename Lower<V>::type;
     static constexpr int NB = KL + KU + 1;
     static constexpr int SEG = 32 * R + KL + KU;  // elements per warp buffer
@@ -58,7 +67,7 @@ struct JwCfg {
     static constexpr int NBW = kBwd ? R : 1;
     // Coefficients in a CTA-shared table: planes w[0..NB), l, h, sc, each
     // [R][T] doubles (T threads per group) -- lane-contiguous, conflict-free.
-    static constexpr bool kTbl = TBL && !kMixed;
+    static constexpr bool kTbl = TBL && !kMixed && PREC == PREC_F64;
     static constexpr int P_L = NB, P_H = NB + (kFwd ? 1 : 0), P_SC = P_H + (kBwd ? 1 : 0);
     static constexpr int NPLANES = P_SC + (SCALE ? 1 : 0);
     // Register-resident coefficients need up to 255 registers: 256-thread
@@ -73,7 +82,7 @@ constexpr int kScratchPerWarp = 32;  // doubles
 template <class C>
 __host__ __device__ constexpr size_t jw_smem_per_warp()
 {
-    return ((2 * (size_t)C::SEG * sizeof(typename C::V)) + 15) / 16 * 16;
+    return ((2 * (size_t)C::SEG * sizeof(typename C::TS)) + 15) / 16 * 16;
 }
 
 template <class C>
@@ -111,9 +120,15 @@ __device__ __forceinline__ int64_t band_pos(const JwOperator& op, int64_t i)
     return base + t + ((j < m) ? j * ce : m * ce + (j - m) * fl);
 }
 
+// Band entry at element index idx: FP64, or FP32 widened (bands32).
+__device__ __forceinline__ double band_at(const JwOperator& op, const double* base, int64_t idx)
+{
+    return op.bands32 ? (double)__ldg(reinterpret_cast<const float*>(base) + idx) : __ldg(base + idx);
+}
+
 __device__ __forceinline__ double band(const JwOperator& op, int64_t off, int64_t i)
 {
-    return __ldg(op.bands + off + band_pos(op, i));
+    return band_at(op, op.bands, off + band_pos(op, i));
 }
 
 // Per-row Scale factor, runtime-scaleC form (pfSolve_RegistersScaleC.h:27-201).
@@ -138,20 +153,21 @@ __device__ __forceinline__ double scale_factor(int kind, int64_t x, int L, doubl
 // the recurrences (-l and -h) are formed on the fly by the solve.
 template <class C>
 struct JwCoef {
-    using S = typename std::conditional<C::kMixed, float, double>::type;
+    using S = typename std::conditional<C::kMixed || C::kF32, float, double>::type;
+    using WT = typename C::MS;  // matvec weights and Scale factors: the arithmetic type
     static constexpr int RR = C::kTbl ? 1 : C::kR;
-    double w_[C::NB][RR];
+    WT w_[C::NB][RR];
     S m_[C::kMixed ? C::kR : 1];
     S l_[C::kTbl ? 1 : C::NF];
     S h_[C::kTbl ? 1 : C::NBW];
     double al_[C::kMixed ? C::NF : 1];   // M's sub-diagonal (residual)
     double cu_[C::kMixed ? C::NBW : 1];  // M's super-diagonal (residual)
-    double sc_[(C::kScale && !C::kTbl) ? C::kR : 1];
+    WT sc_[(C::kScale && !C::kTbl) ? C::kR : 1];
     const double* tbl;  // table mode: plane p, row j of thread tt at tbl[(p*R + j)*T + tt]
     int T, tt;
 
     __device__ __forceinline__ double t_(int p, int j) const { return tbl[(p * C::kR + j) * T + tt]; }
-    __device__ __forceinline__ double w(int k, int j) const
+    __device__ __forceinline__ WT w(int k, int j) const
     {
         if constexpr (C::kTbl) return t_(k, j);
         else return w_[k][j];
@@ -166,7 +182,7 @@ struct JwCoef {
         if constexpr (C::kTbl) return t_(C::P_H, j);
         else return h_[j];
     }
-    __device__ __forceinline__ double sc(int j) const
+    __device__ __forceinline__ WT sc(int j) const
     {
         if constexpr (C::kTbl) return t_(C::P_SC, j);
         else return sc_[j];
@@ -459,7 +475,7 @@ __device__ __forceinline__ void jw_row_weights(const JwOperator& op, int64_t i, 
             for (int kk = -kla; kk <= op.dg_ku; ++kk) {
                 const int64_t c = p + kk;
                 if (c < 0 || c >= M || ((op.dg_skip >> (op.dg_ku - kk)) & 1)) continue;
-                const double a = __ldg(op.dgbmv + op.dg_off + (int64_t)(op.dg_ku - kk) * M + c);
+                const double a = band_at(op, op.dgbmv, op.dg_off + (int64_t)(op.dg_ku - kk) * M + c);
                 const int64_t k = c - i;  // within [-KL, KU] by construction of the plan
 #pragma unroll
                 for (int q = 0; q < NB; ++q)
@@ -585,42 +601,44 @@ __device__ __forceinline__ void jw_prologue(const JwOperator& op, GroupCtx& g, i
 // ---- Global <-> shared movement of one warp segment.
 template <class C>
 __device__ __forceinline__ void issue_segment_load(const JwIO& io, int64_t sys, int64_t r0, int lane,
-                                                   typename C::V* buf)
+                                                   typename C::TS* buf)
 {
+    using T = typename C::T;
     constexpr int R = C::kR, KL = C::kKL, KU = C::kKU;
     const int64_t M = io.M;
+    const T* in = reinterpret_cast<const T*>(io.in);
     auto row_ok = [&](int64_t row) { return row >= 0 && row < M && row >= io.iz0 && row < io.iz1; };
     if constexpr (C::kLIN == LAY_REAL) {
         // ALT: row e of system sys is row 2 e + (sys & 1) of row set sys / 2
         const int64_t h = io.alt ? (sys & 1) : 0, es = io.alt ? 2 : 1;
         const int64_t Msys = io.alt ? (M - h + 1) >> 1 : M;
         auto ok_at = [&](int64_t e) { return e >= 0 && e < Msys && row_ok(es * e + h); };
-        const double* base = io.in + io.in_off + (io.alt ? sys >> 1 : sys) * io.in_stride + h;
+        const T* base = in + io.in_off + (io.alt ? sys >> 1 : sys) * io.in_stride + h;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int q = 32 * k + lane;
             const int64_t row = r0 + q;
             const bool ok = ok_at(row);
-            cp_async8(buf + swz<R, false>(q), ok ? base + es * row : io.in, ok);
+            cp_async_elem<T>(buf + swz<R, false>(q), ok ? base + es * row : in, ok);
         }
         if (KL > 0 && lane < KL) {
             const int64_t row = r0 - KL + lane;
             const bool ok = ok_at(row);
-            cp_async8(buf + 32 * R + lane, ok ? base + es * row : io.in, ok);
+            cp_async_elem<T>(buf + 32 * R + lane, ok ? base + es * row : in, ok);
         }
         if (KU > 0 && lane < KU) {
             const int64_t row = r0 + 32 * R + lane;
             const bool ok = ok_at(row);
-            cp_async8(buf + 32 * R + KL + lane, ok ? base + es * row : io.in, ok);
+            cp_async_elem<T>(buf + 32 * R + KL + lane, ok ? base + es * row : in, ok);
         }
     } else {  // XXII complex: real part row block 2*sys, imaginary 2*sys+1
-        const double* re = io.in + io.in_off + (2 * sys) * io.in_stride;
-        const double* im = re + io.in_stride;
+        const T* re = in + io.in_off + (2 * sys) * io.in_stride;
+        const T* im = re + io.in_stride;
         auto put = [&](int slot, int64_t row) {
             const bool ok = row_ok(row);
-            double* dst = reinterpret_cast<double*>(buf + slot);
-            cp_async8(dst, ok ? re + row : io.in, ok);
-            cp_async8(dst + 1, ok ? im + row : io.in, ok);
+            T* dst = reinterpret_cast<T*>(buf + slot);
+            cp_async_elem<T>(dst, ok ? re + row : in, ok);
+            cp_async_elem<T>(dst + 1, ok ? im + row : in, ok);
         };
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -634,9 +652,12 @@ __device__ __forceinline__ void issue_segment_load(const JwIO& io, int64_t sys, 
 
 template <class C>
 __device__ __forceinline__ void store_segment(const JwIO& io, int64_t sys, int64_t r0, int lane,
-                                              const typename C::V* buf)
+                                              const typename C::TS* buf)
 {
+    using T = typename C::T;
+    using T2 = typename Vec2Of<T>::type;
     constexpr int R = C::kR;
+    T* out = reinterpret_cast<T*>(io.out);
     const int64_t M = io.M;
     const int64_t h = io.alt ? (sys & 1) : 0, es = io.alt ? 2 : 1;
     const int64_t Msys = io.alt ? (M - h + 1) >> 1 : M;
@@ -646,23 +667,23 @@ __device__ __forceinline__ void store_segment(const JwIO& io, int64_t sys, int64
         const int64_t row = r0 + q;
         if (row >= Msys || es * row + h < io.oz0 || es * row + h >= io.oz1) continue;
         if constexpr (C::kLOUT == LAY_REAL) {
-            double v = buf[swz<R, false>(q)];
-            double* p = io.out + io.out_off + (io.alt ? sys >> 1 : sys) * io.out_stride + es * row + h;
+            T v = buf[swz<R, false>(q)];
+            T* p = out + io.out_off + (io.alt ? sys >> 1 : sys) * io.out_stride + es * row + h;
             if (io.accumulate) v += *p;
             *p = v;
         } else if constexpr (C::kLOUT == LAY_PACKED) {
-            double2 v = buf[swz<R, true>(q)];
-            double2* p = reinterpret_cast<double2*>(io.out) + io.out_off + sys * io.out_stride + row;
+            T2 v = buf[swz<R, true>(q)];
+            T2* p = reinterpret_cast<T2*>(io.out) + io.out_off + sys * io.out_stride + row;
             if (io.accumulate) {
-                const double2 o = *p;
+                const T2 o = *p;
                 v.x += o.x;
                 v.y += o.y;
             }
             *p = v;
         } else {  // XXII complex output
-            double2 v = buf[swz<R, true>(q)];
-            double* pr = io.out + io.out_off + (2 * sys) * io.out_stride + row;
-            double* pi = pr + io.out_stride;
+            T2 v = buf[swz<R, true>(q)];
+            T* pr = out + io.out_off + (2 * sys) * io.out_stride + row;
+            T* pi = pr + io.out_stride;
             if (io.accumulate) {
                 v.x += *pr;
                 v.y += *pi;
@@ -762,10 +783,11 @@ __device__ __forceinline__ void mixed_solve(GroupCtx& g, const JwCoef<C>& cf, in
 // ---- Process systems sys0, sys0+step, ... with the group's coefficients.
 template <class C>
 __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO& io, GroupCtx& g,
-                                               const JwCoef<C>& cf, typename C::V* buf0, typename C::V* buf1,
+                                               const JwCoef<C>& cf, typename C::TS* buf0, typename C::TS* buf1,
                                                int64_t sys0, int64_t step)
 {
     using V = typename C::V;
+    using TS = typename C::TS;
     using O = VOps<V>;
     constexpr int R = C::kR, KL = C::kKL, KU = C::kKU;
     constexpr bool CPLX = C::kCplx;
@@ -776,8 +798,8 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
     cp_async_commit();
     int it = 0;
     for (int64_t sys = sys0; sys < io.nsys; sys += step, ++it) {
-        V* cur = (it & 1) ? buf1 : buf0;
-        V* nxt = (it & 1) ? buf0 : buf1;
+        TS* cur = (it & 1) ? buf1 : buf0;
+        TS* nxt = (it & 1) ? buf0 : buf1;
         if (sys + step < io.nsys) issue_segment_load<C>(io, sys + step, r0, g.lane, nxt);
         cp_async_commit();
         cp_async_wait<1>();
@@ -797,7 +819,7 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
             if (q < 0) slot = 32 * R + (q + KL);
             else if (q >= 32 * R) slot = 32 * R + KL + (q - 32 * R);
             else slot = swz<R, CPLX>(q);
-            be[j] = cur[slot];
+            be[j] = conv<V>(cur[slot]);
         }
         V x[R];
 #pragma unroll
@@ -810,7 +832,8 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
         if constexpr (C::kMixed) {
             mixed_solve<C>(g, cf, op.refine_sweeps, x);
         } else if constexpr (C::kSV != SV_NONE) {
-            chunk_solve<R, C::kSV, V, double>(g, [&](int j) { return cf.l(j); }, [&](int j) { return cf.h(j); }, x);
+            chunk_solve<R, C::kSV, V, typename JwCoef<C>::S>(g, [&](int j) { return cf.l(j); },
+                                                             [&](int j) { return cf.h(j); }, x);
         }
         if (C::kSV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
         if constexpr (C::kScale) {
@@ -819,7 +842,7 @@ __device__ __forceinline__ void jw_run_systems(const JwOperator& op, const JwIO&
         }
         __syncwarp();  // every lane has read `cur`
 #pragma unroll
-        for (int j = 0; j < R; ++j) cur[swz<R, CPLX>(g.lane * R + j)] = x[j];
+        for (int j = 0; j < R; ++j) cur[swz<R, CPLX>(g.lane * R + j)] = conv<TS>(x[j]);
         __syncwarp();
         store_segment<C>(io, sys, r0, g.lane, cur);
         __syncwarp();  // `cur` is the target of the load issued next iteration
@@ -831,7 +854,7 @@ template <class C>
 __global__ void __launch_bounds__(C::kMaxThreads) jw_step_kernel(const JwOperator op, const JwIO io, const int W)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using V = typename C::V;
+    using TS = typename C::TS;
     const int warp = threadIdx.x >> 5;
     const int G = blockDim.x / (32 * W);
     const int grp = warp / W;
@@ -845,8 +868,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_step_kernel(const JwOperato
     constexpr size_t per_warp = jw_smem_per_warp<C>();
     double* table = reinterpret_cast<double*>(smem_raw);
     unsigned char* data = smem_raw + jw_table_bytes<C>(W);
-    V* buf0 = reinterpret_cast<V*>(data + (size_t)warp * per_warp);
-    V* buf1 = buf0 + C::SEG;
+    TS* buf0 = reinterpret_cast<TS*>(data + (size_t)warp * per_warp);
+    TS* buf1 = buf0 + C::SEG;
     g.scratch = reinterpret_cast<double*>(data + (size_t)G * W * per_warp) + (size_t)grp * W * kScratchPerWarp;
 
     const int64_t s = (int64_t)(g.wg * 32 + g.lane) * C::kR;
@@ -886,7 +909,7 @@ __global__ void __launch_bounds__(256) jw_batch_kernel(const BatchEntryDev* __re
                                                       unsigned int* __restrict__ counter, const int W)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using V = typename C::V;
+    using TS = typename C::TS;
     const int warp = threadIdx.x >> 5;
     const int G = blockDim.x / (32 * W);
     const int grp = warp / W;
@@ -898,8 +921,8 @@ __global__ void __launch_bounds__(256) jw_batch_kernel(const BatchEntryDev* __re
     g.bar_id = 1 + grp;
     g.seq = 0;
     constexpr size_t per_warp = jw_smem_per_warp<C>();
-    V* buf0 = reinterpret_cast<V*>(smem_raw + (size_t)warp * per_warp);
-    V* buf1 = buf0 + C::SEG;
+    TS* buf0 = reinterpret_cast<TS*>(smem_raw + (size_t)warp * per_warp);
+    TS* buf1 = buf0 + C::SEG;
     double* scratch_all = reinterpret_cast<double*>(smem_raw + (size_t)G * W * per_warp);
     g.scratch = scratch_all + (size_t)grp * W * kScratchPerWarp;
     int* slots = reinterpret_cast<int*>(scratch_all + (size_t)G * W * kScratchPerWarp) + 2 * grp;

@@ -43,6 +43,20 @@
 //  * Pass 2 solves its slice again with those carries and writes the result.
 //  Input is read twice and written once; the four launches are ordered on
 //  the stream, so no CTA ever waits for another.
+//  * The single-pass form (PASS = 4, the default) reads the input once: after
+//    the two table passes, one cooperative launch (every CTA resident) solves
+//    each slice with zero carries, publishes the slice's offsets (Bf, Bb0)
+//    with a release flag, waits for the other slices of the same system
+//    (acquire loads of their flags, bounded), composes the carries entering
+//    its slice from the published offsets and the slice constants, and adds
+//    their responses: x = x0 + X psi + Y G, with psi (a unit forward carry,
+//    zero input) and G (a unit backward carry) per row, built once per CTA.
+//    All slices of a system are handled by the same group index of the CTAs
+//    of one column (CTA b: slice b % NS, column b / NS), which take the
+//    systems in the same order, so every wait is on groups that are resident
+//    and about to publish.  A slice reads its matvec halo rows from global
+//    memory before publishing, and no slice of a system stores before all of
+//    them have published: in place is safe.
 //  * Completion waits are bounded: a wait that runs out records
 //    kStatusWaitTimeout and the group stops.
 #pragma once
@@ -69,14 +83,33 @@ constexpr int kLgRedBf = 0, kLgRedBb = 1, kLgRedLo = 2, kLgRedHi = 4, kLgRedX = 
 // rows (tridiagonal pivots; 4 doubles at kLgConstMob).
 constexpr int kLgConst = 8;
 constexpr int kLgConstMob = 4;
+// Slices per system the single-pass form composes (two rounds of a warp).
+constexpr int kLgMaxSlices = 64;
+// Cross-CTA waits of the single-pass form give up after this many cycles
+// (about 0.5 s at the B200's clock).
+constexpr long long kLgWaitCycles = 1000000000LL;
 
-// Shared memory: table | scratch | 8 doubles | mbarriers | (align 1024) |
-// buffers | the slice's PASS 1 weights (alpha, beta per row, S * 16 bytes).
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Shared memory: table | scratch | 8 doubles | slice constants (Af, Ab, Psi
+// of up to kLgMaxSlices slices, 4 doubles each) | mbarriers | (align 1024) |
+// buffers | per row of the slice, 16 bytes: the PASS 1 weights (alpha, beta),
+// or in the single pass the carry responses (psi, G).
 template <class C>
 __host__ __device__ constexpr size_t lg_smem_bytes()
 {
     return C::B::TBL + (size_t)C::G * C::W * kScratchPerWarp * sizeof(double) + 8 * sizeof(double) +
-           (size_t)C::G * 2 * sizeof(uint64_t) + 1024 + (size_t)C::G * 2 * C::B::BUF + (size_t)C::S * 16;
+           (size_t)kLgMaxSlices * 4 * sizeof(double) + (size_t)C::G * 2 * sizeof(uint64_t) + 1024 +
+           (size_t)C::G * 2 * C::B::BUF + (size_t)C::S * 16;
 }
 
 // ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
@@ -271,15 +304,18 @@ __global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__
 
 // PASS 3: grid NS (CTA c writes slice c's pivot product into cst, tridiagonal
 // only); PASS 0: grid NS (CTA c builds slice c's table into tab + c * TBL / 8
-// and its constants into cst); PASS 1, 2: CTAs in multiples of NS (CTA b owns
-// slice b % NS).  red: io.nsys * NS records of kLgRed doubles; cst: NS
-// records of kLgConst doubles.
+// and its constants into cst); PASS 1, 2 and 4 (the single pass, a
+// cooperative launch): CTAs in multiples of NS (CTA b owns slice b % NS).
+// red: io.nsys * NS records of kLgRed doubles; cst: NS records of kLgConst
+// doubles; flags (single pass): io.nsys * NS words, slice-major, set to
+// `epoch` when a (system, slice) record is published.
 template <class C, int PASS>
 __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ CUtensorMap tm_in,
                                                        const __grid_constant__ CUtensorMap tm_out,
                                                        const JwOperator op, const JwIO io, double* __restrict__ red,
                                                        double* __restrict__ cst, double* __restrict__ tab,
-                                                       const int NS)
+                                                       const int NS, unsigned* __restrict__ flags,
+                                                       const unsigned epoch)
 {
     using BC = typename C::B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -294,8 +330,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     double* table = reinterpret_cast<double*>(smem_raw);
     double* scratch = reinterpret_cast<double*>(smem_raw + BC::TBL);
     double* q4 = scratch + C::G * W * kScratchPerWarp;  // 8 doubles
-    uint64_t* bars = reinterpret_cast<uint64_t*>(q4 + 8) + 2 * grp;
-    unsigned char* after = reinterpret_cast<unsigned char*>(reinterpret_cast<uint64_t*>(q4 + 8) + 2 * C::G);
+    double* cst_s = q4 + 8;                              // slice constants (single pass)
+    uint64_t* bars_all = reinterpret_cast<uint64_t*>(cst_s + kLgMaxSlices * 4);
+    uint64_t* bars = bars_all + 2 * grp;
+    unsigned char* after = reinterpret_cast<unsigned char*>(bars_all + 2 * C::G);
     const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
     unsigned char* buf0 = after + pad + (size_t)grp * 2 * BC::BUF;
     unsigned char* buf1 = buf0 + BC::BUF;
@@ -305,7 +343,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     double2* ab_g = reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)c * C::S;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
 
-    if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(reinterpret_cast<uint64_t*>(q4 + 8) + threadIdx.x), W);
+    if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(bars_all + threadIdx.x), W);
     mbar_init_fence();
     double* gtab = tab + (size_t)c * (BC::TBL / sizeof(double));
     if constexpr (PASS == 3) {
@@ -319,6 +357,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
         if constexpr (PASS == 1)
             for (int i = threadIdx.x; i < C::S; i += blockDim.x) ab_s[i] = ab_g[i];
+        if constexpr (PASS == 4)
+            for (int i = threadIdx.x; i < NS; i += blockDim.x) {
+                cst_s[4 * i] = cst[i * kLgConst];          // Af
+                cst_s[4 * i + 1] = cst[i * kLgConst + 1];  // Ab
+                cst_s[4 * i + 2] = cst[i * kLgConst + 2];  // Psi
+            }
     }
     __syncthreads();
 
@@ -353,6 +397,23 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         }
     }
 
+    // Single pass: the responses of the slice's rows to a unit forward carry
+    // (psi) and to a unit backward carry (G), by group 0: zero-input solves.
+    if constexpr (PASS == 4) {
+        if (grp == 0) {
+            double xp[R + KL + KU], xg[R + KL + KU];
+#pragma unroll
+            for (int i = 0; i < R + KL + KU; ++i) {
+                xp[i] = 0.0;
+                xg[i] = 0.0;
+            }
+            lg_solve<C>(g, coef, Af, Ab, xp, [&](double, double) { return 1.0; }, [&](double, double) { return 0.0; });
+            lg_solve<C>(g, coef, Af, Ab, xg, [&](double, double) { return 0.0; }, [&](double, double) { return 1.0; });
+#pragma unroll
+            for (int j = 0; j < R; ++j) ab_s[j * T + t] = make_double2(xp[j], xg[j]);
+        }
+        __syncthreads();
+    }
     // Slice constants (Af, Ab, Psi): a solve of zero input with a unit
     // forward carry, by group 0, and the table itself to global memory.
     if constexpr (PASS == 0) {
@@ -442,6 +503,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         return (uint32_t)((H > 1 ? (u / IB) * T : 0) + ch) * ROWB + (((u % IB) ^ sw) << 4);
     };
     const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
+    // Single pass, M not a multiple of R: the tensor maps hold the first
+    // Mfull rows; the thread whose chunk starts at Mfull (the tail chunk,
+    // outside the maps: zero-filled by the loads, dropped by the stores)
+    // moves its rows between global memory and its staged units itself.
+    const int64_t Mfull = (io.M / R) * R;
+    const bool tail_thread = PASS == 4 && Mfull < io.M && s_glob == Mfull;
     auto in_row = [&](int64_t y, int64_t row) -> double {  // input row of system y as data (0 outside)
         if (row < 0 || row >= io.M || row < io.iz0 || row >= io.iz1) return 0.0;
         return io.in[io.in_off + y * io.in_stride + row];
@@ -477,6 +544,18 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
             break;
         }
+        if (PASS == 4 && Mfull < io.M && s0 + C::S > Mfull) {  // the slice holding the tail chunk
+            if (tail_thread) {
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const int64_t row = Mfull + j;
+                    const double v = (row < io.M) ? io.in[io.in_off + sys * io.in_stride + row] : 0.0;
+                    reinterpret_cast<double*>(cur + unit_off(j >> 1, t, sw_me))[j & 1] = v;
+                }
+            }
+            if (W > 1) group_bar(g.bar_id, g.nthr);
+            else __syncwarp();
+        }
         // field k of this (system, slice) record
         auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
         double be[R + KL + KU];
@@ -490,6 +569,8 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             double2 pv = make_double2(0.0, 0.0);
             if (t > 0) {
                 pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
+            } else if (PASS == 4) {
+                pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
             } else if (PASS == 1) {
                 pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
                 rec(kLgRedLo) = pv.x;
@@ -504,6 +585,8 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             double2 nv = make_double2(0.0, 0.0);
             if (t < T - 1) {
                 nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
+            } else if (PASS == 4) {
+                nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
             } else if (PASS == 1) {
                 nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
                 rec(kLgRedHi) = nv.x;
@@ -541,7 +624,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         // pass 2, stored from: once this warp's stores have read it, it takes
         // the next system
         if (more && lane == 0) {
-            if (PASS == 2) bulk_wait_read_all();
+            if (PASS == 2 || PASS == 4) bulk_wait_read_all();
             issue_load(nxt, (k & 1) ? bar0 : bar1, sys + per);
         }
         if constexpr (PASS == 1) {
@@ -581,12 +664,146 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 }
             }
             continue;
+        } else if constexpr (PASS == 4) {
+            // the slice with zero carries; its offsets Bf (forward total) and
+            // Bb0 (backward total)
+            double Bf = 0.0, Bb0 = 0.0;
+            if constexpr (BC::FWD || BC::BWD)
+                lg_solve<C>(g, coef, Af, Ab, x,
+                            [&](double, double Bt) {
+                                Bf = Bt;
+                                return 0.0;
+                            },
+                            [&](double, double Bt) {
+                                Bb0 = Bt;
+                                return 0.0;
+                            });
+            // Slices couple through the carries (a solve) or through the
+            // matvec halo rows read in place (a matvec alone): publish, then
+            // wait for every slice of this system (bounded).
+            if constexpr (BC::FWD || BC::BWD || KL > 0 || KU > 0) {
+                if (t == 0) {
+                    rec(kLgRedBf) = Bf;
+                    rec(kLgRedBb) = Bb0;
+                    st_release_u32(flags + (size_t)c * nsys + sys, epoch);
+                }
+                bool ok2 = true;
+                double Xin = 0.0, Yin = 0.0;
+                if (wg == 0) {
+                    const long long t0 = clock64();
+                    for (int cc = lane; cc < NS && ok2; cc += 32)
+                        while (ld_acquire_u32(flags + (size_t)cc * nsys + sys) != epoch) {
+                            if (clock64() - t0 > kLgWaitCycles) {
+                                ok2 = false;
+                                break;
+                            }
+                            __nanosleep(32);
+                        }
+                    ok2 = __all_sync(FULL, ok2) != 0;
+                    if (ok2 && (BC::FWD || BC::BWD)) {
+                        // carries entering slice c: X from below (affine maps
+                        // (Af, Bf) composed upwards), Y from above (maps
+                        // (Ab, Bb0 + X Psi) composed downwards); lanes hold
+                        // slices, in rounds of 32
+                        double Xr[kLgMaxSlices / 32];
+                        double carry = 0.0;
+#pragma unroll
+                        for (int r = 0; r < kLgMaxSlices / 32; ++r) {
+                            if (32 * r >= NS) break;  // no slices left (NS is uniform)
+                            const int cc = 32 * r + lane;
+                            const bool v = cc < NS;
+                            double A = v ? cst_s[4 * cc] : 1.0;
+                            double B = v ? __ldcg(&red[((size_t)cc * kLgRed + kLgRedBf) * nsys + sys]) : 0.0;
+                            if (!BC::FWD) {
+                                A = 1.0;
+                                B = 0.0;
+                            }
+#pragma unroll
+                            for (int d = 1; d < 32; d <<= 1) {  // inclusive scan of the maps
+                                const double Ap = __shfl_up_sync(FULL, A, d), Bp = __shfl_up_sync(FULL, B, d);
+                                if (lane >= d) {
+                                    B = __fma_rn(A, Bp, B);
+                                    A = A * Ap;
+                                }
+                            }
+                            const double incl = __fma_rn(A, carry, B);  // value leaving slice cc
+                            double ex = __shfl_up_sync(FULL, incl, 1);
+                            if (lane == 0) ex = carry;
+                            Xr[r] = ex;  // value entering slice cc
+                            if (cc == c) Xin = ex;
+                            carry = __shfl_sync(FULL, incl, 31);
+                        }
+                        if constexpr (BC::BWD) {
+                            carry = 0.0;
+#pragma unroll
+                            for (int r = kLgMaxSlices / 32 - 1; r >= 0; --r) {
+                                if (32 * r >= NS) continue;  // identity maps above the top slice
+                                const int cc = 32 * r + lane;
+                                const bool v = cc < NS;
+                                double A = v ? cst_s[4 * cc + 1] : 1.0;
+                                double B = v ? __fma_rn(Xr[r], cst_s[4 * cc + 2],
+                                                        __ldcg(&red[((size_t)cc * kLgRed + kLgRedBb) * nsys + sys]))
+                                             : 0.0;
+#pragma unroll
+                                for (int d = 1; d < 32; d <<= 1) {  // inclusive scan from the top
+                                    const double Ap = __shfl_down_sync(FULL, A, d), Bp = __shfl_down_sync(FULL, B, d);
+                                    if (lane + d < 32) {
+                                        B = __fma_rn(A, Bp, B);
+                                        A = A * Ap;
+                                    }
+                                }
+                                const double incl = __fma_rn(A, carry, B);  // value leaving slice cc downwards
+                                double ex = __shfl_down_sync(FULL, incl, 1);
+                                if (lane == 31) ex = carry;
+                                if (cc == c) Yin = ex;
+                                carry = __shfl_sync(FULL, incl, 0);
+                            }
+                        }
+                        // the lane of slice c holds its carries: to the group
+                        const int owner = c & 31;
+                        Xin = __shfl_sync(FULL, Xin, owner);
+                        Yin = __shfl_sync(FULL, Yin, owner);
+                        if (lane == 0) {
+                            g.warp_area(0)[16] = Xin;
+                            g.warp_area(0)[17] = Yin;
+                        }
+                    }
+                }
+                if (W > 1) {
+                    ok2 = group_and(g.bar_id, g.nthr, ok2);
+                    if (wg != 0) {
+                        Xin = g.warp_area(0)[16];
+                        Yin = g.warp_area(0)[17];
+                    }
+                    group_bar(g.bar_id, g.nthr);  // slot read by all before the next system rewrites it
+                }
+                if (!ok2) {
+                    if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
+                    // the next system's load, if issued, completes before the CTA exits
+                    if (more && lane == 0) mbar_wait_bounded((k & 1) ? bar0 : bar1, (uint32_t)(((k + 1) >> 1) & 1));
+                    break;
+                }
+                if constexpr (BC::FWD || BC::BWD) {
+#pragma unroll
+                    for (int j = 0; j < R; ++j) {
+                        const double2 pg = ab_s[j * T + t];
+                        x[j] = __fma_rn(Xin, pg.x, __fma_rn(Yin, pg.y, x[j]));
+                    }
+                }
+            }
         } else {
             // carries of this system's slice, from the carry kernel
             const double Xc = BC::FWD ? rec(kLgRedX) : 0.0, Yc = BC::BWD ? rec(kLgRedY) : 0.0;
             lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
         }
         if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
+        if (tail_thread) {  // the tail rows (the TMA store drops the tail chunk)
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const int64_t row = Mfull + j;
+                if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
+            }
+        }
         __syncwarp();
 #pragma unroll
         for (int u = 0; u < U; ++u) {

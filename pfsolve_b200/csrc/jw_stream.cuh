@@ -22,6 +22,12 @@
 //    group kernel (warp shuffles, then shared memory across warps).
 //  * Completion waits are bounded: a wait that exceeds its limit records
 //    kStatusWaitTimeout in the device status word and the CTA stops.
+//  * Storage is FP64 or FP32 (PREC_F32, PREC_F64_F32MEM); a 16-byte unit of a
+//    staged plane holds 2 or 4 rows.  The staging buffer is warp-major: the
+//    boxes of warp w's 32 chunks (every plane and swizzle row) come before
+//    warp w+1's, for the input and for the output layout, so each warp's
+//    input and output bytes coincide and the warp's own bulk-copy waits order
+//    its next load after its last store.
 #pragma once
 #include <cuda.h>
 
@@ -46,15 +52,22 @@ struct StCfg {
     static constexpr int S = ALT ? 2 : 1;
     static constexpr int KLP = S * KL_, KUP = S * KU_;
     static constexpr bool CPLX = (LIN != LAY_REAL);
-    using V = typename std::conditional<CPLX, double2, double>::type;
+    static constexpr bool F32MEM = prec_f32_storage(PREC_);  // FP32 storage
+    static constexpr bool F32 = (PREC_ == PREC_F32);          // FP32 arithmetic
+    using Sto = typename std::conditional<F32MEM, float, double>::type;  // storage scalar
+    using MS = typename std::conditional<F32, float, double>::type;     // arithmetic scalar
+    using CT = MS;                                                       // coefficient table scalar
+    using CT2 = typename Vec2Of<CT>::type;                              // one table entry: a row pair
+    static constexpr int ES = (int)sizeof(Sto);
+    using V = typename std::conditional<CPLX, typename Vec2Of<MS>::type, MS>::type;
     using VF = typename Lower<V>::type;
     static constexpr int T = 32 * W;  // chunks (threads) per group
     static constexpr int NB = KL + KU + 1;
     static constexpr bool FWD = (SV == SV_LOWER || SV == SV_TRI);
     static constexpr bool BWD = (SV == SV_UPPER || SV == SV_TRI);
     static constexpr bool MIXED = (PREC_ == PREC_MIXED) && (SV != SV_NONE);
-    // Coefficient table planes, each 16 bytes per (row pair, thread).
-    // FP64: NB weights (scaled by the LU pivots), -l, -h, Scale factor.
+    // Coefficient table planes, each one CT2 per (row pair, thread).
+    // FP64 / FP32: NB weights (scaled by the LU pivots), -l, -h, Scale factor.
     // Mixed: NB weights (unscaled), the solve's sub- and super-diagonal in FP64
     // (residual), FP32 packs {m, m', -l, -l'} and {-h, -h', 0, 0}, Scale factor.
     static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0);  // FP64 path
@@ -62,42 +75,50 @@ struct StCfg {
     static constexpr int P_F1 = P_CU + (BWD ? 1 : 0), P_F2 = P_F1 + 1;
     static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0);
     static constexpr int NPL = P_SC + (SCALE ? 1 : 0);
-    // Input: NPIN planes of 8-byte rows; a chunk holds U 16-byte units per
-    // plane, stored as H swizzle rows of IB units (TMA box inner extent).
-    static constexpr int NPIN = CPLX ? 2 : 1;
+    // Table: U row pairs per chunk.
     static constexpr int U = R / 2;
-    static constexpr int IB = U < 8 ? U : 8;
-    static constexpr int H = U / IB;
+    // Input: NPIN planes of ES-byte rows; a 16-byte unit holds EPU rows, a
+    // chunk UD units per plane, stored as H swizzle rows of IB units (TMA box
+    // inner extent).
+    static constexpr int NPIN = CPLX ? 2 : 1;
+    static constexpr int EPU = 16 / ES;
+    static constexpr int UD = R / EPU;
+    static constexpr int IB = UD < 8 ? UD : 8;
+    static constexpr int H = UD / IB;
     static constexpr int SWB = Log2<IB>::v;
-    // Output: packed complex (16-byte rows) or planes of 8-byte rows.
+    // Output: packed complex (2 ES-byte rows) or planes of ES-byte rows; a
+    // 16-byte unit holds EPUO rows.
     static constexpr bool OPK = (LOUT == LAY_PACKED);
     static constexpr int NPOUT = OPK ? 1 : (LOUT == LAY_XXII ? 2 : 1);
-    static constexpr int UO = OPK ? R : R / 2;
+    static constexpr int EPUO = OPK ? 8 / ES : EPU;
+    static constexpr int UO = R / EPUO;
     static constexpr int IBO = UO < 8 ? UO : 8;
     static constexpr int HO = UO / IBO;
     static constexpr int SWBO = Log2<IBO>::v;
-    static constexpr size_t BUF = (size_t)T * R * (CPLX ? 16 : 8);  // bytes of one system
+    static constexpr size_t BUF = (size_t)T * R * ES * (CPLX ? 2 : 1);  // bytes of one system
     // Table rows of T 16-byte units, padded by one unit: the prologue's
     // writes (consecutive threads on consecutive row pairs of one chunk) then
     // fall on different banks; the loop's reads (consecutive threads on
     // consecutive units of one row) are conflict-free either way.
     static constexpr int TP = (W <= 2) ? T + 1 : T;  // 4-warp groups: no room to spare at N = 4096
-    static constexpr size_t TBL = (size_t)NPL * U * TP * 16;
-    // A warp's input and output bytes coincide when both layouts have the same
-    // swizzle rows; otherwise a warp's staging overlaps its neighbours' input.
-    static constexpr bool kSameRows = (IB == IBO) && (NPIN * H == NPOUT * HO);
+    static constexpr size_t TBL = (size_t)NPL * U * TP * sizeof(CT2);
+    // Bytes per chunk of the input and of the output layout (equal: a system
+    // is staged in place); with the warp-major layout, warp w's input and
+    // output bytes are then the same range.
+    static constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
+    static_assert(NPIN * H * ROWB == NPOUT * HO * ROWBO, "in-place staging");
     // Registers held by the right-hand-side data (mixed: x, g and the FP32
     // solve vector); the launch bound leaves the compiler room for them:
     // 512 threads cap at 128 registers, 384 at 170, 256 at 255.  Complex
     // variants stay at 256 (measured faster than 384 on the config 2 chain).
-    static constexpr int kDataRegs = (R + KLP + KUP) * (CPLX ? 4 : 2) * (MIXED ? 3 : 1);
+    static constexpr int kDataRegs = (R + KLP + KUP) * (CPLX ? 2 : 1) * (F32 ? 1 : 2) * (MIXED ? 3 : 1);
     static constexpr int kMaxThreads =
         (kDataRegs >= 96 || (CPLX && kDataRegs >= 64)) ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
     static_assert(KLP <= 2 && KUP <= 2, "halo of at most two rows");
-    static_assert(!ALT || (!CPLX && !MIXED && !SCALE), "ALT: real FP64 systems without a Scale epilogue");
+    static_assert(!ALT || (!CPLX && !MIXED && !SCALE && !F32MEM), "ALT: real FP64 systems without a Scale epilogue");
+    static_assert(!MIXED || !F32MEM, "mixed precision: FP64 storage");
     static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");
-    static_assert(W == 1 || kSameRows, "multi-warp groups need matching input/output rows");
 };
 
 template <class C>
@@ -194,7 +215,7 @@ __device__ __forceinline__ int swz_row(int t)
 // [((p*U + j/2)*T + tt)*2 + (j&1)]: thread tt reads rows 2u, 2u+1 of a plane
 // as one 16-byte word, lanes on consecutive words.
 template <class C>
-__device__ void st_prologue_system(const JwOperator& op, int h, double* table, GroupCtx& g)
+__device__ void st_prologue_system(const JwOperator& op, int h, typename C::CT* table, GroupCtx& g)
 {
     constexpr int R = C::R, T = C::T, U = C::U, NB = C::NB;
     const int64_t M = op.M;
@@ -257,7 +278,9 @@ __device__ void st_prologue_system(const JwOperator& op, int h, double* table, G
         }
         const int64_t si = C::S * i + h;  // staged row
         const int tt = (int)(si / R), jj = (int)(si % R);
-        auto put = [&](int p, double v) { table[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 2 + (jj & 1)] = v; };
+        auto put = [&](int p, double v) {
+            table[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 2 + (jj & 1)] = (typename C::CT)v;
+        };
         auto put32 = [&](int p, int k, double v) {
             reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 4 + k + (jj & 1)] = (float)v;
         };
@@ -284,7 +307,7 @@ __device__ void st_prologue_system(const JwOperator& op, int h, double* table, G
 // ALT: system h is the parity-h rows, with its own row count and band
 // positions (the group kernel's per-parity operator, jw_step_kernel).
 template <class C>
-__device__ void st_prologue(const JwOperator& op, double* table, double* scratch_all)
+__device__ void st_prologue(const JwOperator& op, typename C::CT* table, double* scratch_all)
 {
     GroupCtx g;
     g.lane = threadIdx.x & 31;
@@ -316,14 +339,18 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using V = typename C::V;
     using O = VOps<V>;
+    using MS = typename C::MS;
+    using CT = typename C::CT;
+    using CT2 = typename C::CT2;
     constexpr int R = C::R, W = C::W, T = C::T, U = C::U, NB = C::NB, S = C::S;
+    constexpr int EPU = C::EPU, UD = C::UD, UO = C::UO, ES = C::ES;
     constexpr int KL = C::KLP, KU = C::KUP;  // staged halo rows (S times the band halo)
     constexpr int IB = C::IB, H = C::H, IBO = C::IBO, HO = C::HO;
     const int G = blockDim.x / T;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = warp / W, wg = warp - grp * W;
 
-    double* table = reinterpret_cast<double*>(smem_raw);
+    CT* table = reinterpret_cast<CT*>(smem_raw);
     double* scratch_all = reinterpret_cast<double*>(smem_raw + C::TBL);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::TBL + (size_t)G * W * kScratchPerWarp * sizeof(double));
     unsigned char* after = reinterpret_cast<unsigned char*>(bars + 2 * G);
@@ -348,8 +375,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
     const int t = wg * 32 + lane;
     const int64_t s = (int64_t)t * R;
-    const double2* tb = reinterpret_cast<const double2*>(table) + t;  // pair (p, u) at tb[(p*U + u)*T]
-    auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * C::TP]; };
+    const CT2* tb = reinterpret_cast<const CT2*>(table) + t;  // pair (p, u) at tb[(p*U + u)*TP]
+    auto coef = [&](int p, int u) -> CT2 { return tb[(p * U + u) * C::TP]; };
 
     auto coef4 = [&](int p, int u) -> float4 { return reinterpret_cast<const float4*>(tb)[(p * U + u) * C::TP]; };
     // Mixed precision, real systems of up to 16 rows per thread: the FP32 solve
@@ -387,12 +414,12 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     // precision of the solve that uses them).
     // ALT: one multiplier per system, Af / Ab for the even rows and Af1 / Ab1
     // for the odd rows.
-    double Af = 1.0, Ab = 1.0, Af1 = 1.0, Ab1 = 1.0;
+    CT Af = 1, Ab = 1, Af1 = 1, Ab1 = 1;
     float Af32 = 1.0f, Ab32 = 1.0f;
     if constexpr (C::FWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const double2 c = coef(C::P_NL, u);
+            const CT2 c = coef(C::P_NL, u);
             if constexpr (C::ALT) {
                 Af = c.x * Af;
                 Af1 = c.y * Af1;
@@ -405,7 +432,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     if constexpr (C::BWD && !C::MIXED) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const double2 c = coef(C::P_NH, u);
+            const CT2 c = coef(C::P_NH, u);
             if constexpr (C::ALT) {
                 Ab = c.x * Ab;
                 Ab1 = c.y * Ab1;
@@ -437,22 +464,47 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     // systems share them).  The others, with fewer registers to spare, keep
     // the plain scan.
     constexpr bool kPre = (C::CPLX || C::MIXED) && !C::ALT && R <= 16 && C::kMaxThreads <= 256;
-    ScanMul<double> mf{}, mb{};
+    ScanMul<CT> mf{}, mb{};
     ScanMul<float> mf32{}, mb32{};
-    if constexpr (kPre && C::FWD && !C::MIXED) mf = scan_multipliers<double, true>(g, Af);
-    if constexpr (kPre && C::BWD && !C::MIXED) mb = scan_multipliers<double, false>(g, Ab);
+    if constexpr (kPre && C::FWD && !C::MIXED) mf = scan_multipliers<CT, true>(g, Af);
+    if constexpr (kPre && C::BWD && !C::MIXED) mb = scan_multipliers<CT, false>(g, Ab);
     if constexpr (kPre && C::FWD && C::MIXED) mf32 = scan_multipliers<float, true>(g, Af32);
     if constexpr (kPre && C::BWD && C::MIXED) mb32 = scan_multipliers<float, false>(g, Ab32);
 
-    // Shared-memory byte offsets of 16-byte unit uu (< IB) of swizzle row h of
-    // plane p for chunk c: plane_row(p, h) * T * IB*16 + c * IB*16 + (uu ^ swz(c))*16.
-    constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
+    // Shared-memory byte offset of swizzle row h of plane p of chunk c, in the
+    // warp-major staging layout (the boxes of warp c/32, then the next
+    // warp's); unit uu (< IB) of that row is at + ((uu ^ swz(c)) << 4).
+    constexpr int ROWB = C::ROWB, ROWBO = C::ROWBO;
+    auto in_row = [&](int p, int h, int c) -> size_t {
+        return ((size_t)(((c >> 5) * C::NPIN + p) * H + h) * 32 + (c & 31)) * ROWB;
+    };
+    auto out_row = [&](int p, int h, int c) -> size_t {
+        return ((size_t)(((c >> 5) * C::NPOUT + p) * HO + h) * 32 + (c & 31)) * ROWBO;
+    };
     const int sw_me = swz_row<C::SWB>(t), sw_prev = swz_row<C::SWB>(t - 1), sw_next = swz_row<C::SWB>(t + 1);
     const int swo_me = swz_row<C::SWBO>(t);
     const bool has_prev = t > 0, has_next = t < T - 1;
-    auto unit_at = [&](const unsigned char* b, int p, int u, int c, int sw) -> double2 {
-        const int h = u / IB, uu = u % IB;
-        return *reinterpret_cast<const double2*>(b + (size_t)((p * H + h) * T + c) * ROWB + ((uu ^ sw) << 4));
+    // rows EPU u .. EPU u + EPU - 1 of plane p of chunk c, in the arithmetic type
+    auto unit_rows = [&](const unsigned char* b, int p, int u, int c, int sw, MS (&v)[EPU]) {
+        const unsigned char* a = b + in_row(p, u / IB, c) + (((u % IB) ^ sw) << 4);
+        if constexpr (ES == 8) {
+            const double2 d = *reinterpret_cast<const double2*>(a);
+            v[0] = (MS)d.x;
+            v[1] = (MS)d.y;
+        } else {
+            const float4 f = *reinterpret_cast<const float4*>(a);
+            v[0] = (MS)f.x;
+            v[1] = (MS)f.y;
+            v[2] = (MS)f.z;
+            v[3] = (MS)f.w;
+        }
+    };
+    // the 16 bytes at `a` from EPU (or, packed complex, 16 / ES) values
+    auto put_unit = [&](unsigned char* a, const MS* v) {
+        if constexpr (ES == 8) *reinterpret_cast<double2*>(a) = make_double2((double)v[0], (double)v[1]);
+        else
+            *reinterpret_cast<float4*>(a) =
+                make_float4(conv<float>(v[0]), conv<float>(v[1]), conv<float>(v[2]), conv<float>(v[3]));
     };
 
     const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
@@ -461,13 +513,14 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     int64_t sys = (int64_t)blockIdx.x * G + grp;
 
     // lane 0 of each warp: load / store this warp's 32 chunks of one system
+    // (TMA x coordinates in storage elements: 16 / ES per 16-byte unit)
     auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
         mbar_arrive_expect_tx(bar, (uint32_t)(C::NPIN * H * 32 * ROWB));
 #pragma unroll
         for (int p = 0; p < C::NPIN; ++p)
 #pragma unroll
             for (int h = 0; h < H; ++h)
-                tma_load_3d(smem_u32(b + (size_t)((p * H + h) * T + 32 * wg) * ROWB), &tm_in, h * IB * 2, 32 * wg,
+                tma_load_3d(smem_u32(b + in_row(p, h, 32 * wg)), &tm_in, h * IB * (16 / ES), 32 * wg,
                             (int)(C::CPLX ? 2 * y + p : y), bar);
     };
     auto issue_store = [&](unsigned char* b, int64_t y) {
@@ -475,8 +528,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         for (int p = 0; p < C::NPOUT; ++p)
 #pragma unroll
             for (int h = 0; h < HO; ++h)
-                tma_store_3d(&tm_out, h * IBO * 2, 32 * wg, (int)(C::NPOUT == 2 ? 2 * y + p : y),
-                             smem_u32(b + (size_t)((p * HO + h) * T + 32 * wg) * ROWBO));
+                tma_store_3d(&tm_out, h * IBO * (16 / ES), 32 * wg, (int)(C::NPOUT == 2 ? 2 * y + p : y),
+                             smem_u32(b + out_row(p, h, 32 * wg)));
         bulk_commit();
     };
 
@@ -493,46 +546,45 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
         // rows s-KL .. s+R+KU-1 of this system
         V be[R + KL + KU];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
+        // row e of 16-byte unit u of chunk c (both planes when complex)
+        auto rows_of = [&](int u, int c, int sw, V (&v)[EPU]) {
+            MS re[EPU];
+            unit_rows(cur, 0, u, c, sw, re);
             if constexpr (C::CPLX) {
-                const double2 re = unit_at(cur, 0, u, t, sw_me), im = unit_at(cur, 1, u, t, sw_me);
-                be[KL + 2 * u] = make_double2(re.x, im.x);
-                be[KL + 2 * u + 1] = make_double2(re.y, im.y);
+                MS im[EPU];
+                unit_rows(cur, 1, u, c, sw, im);
+#pragma unroll
+                for (int e = 0; e < EPU; ++e) v[e] = V{re[e], im[e]};
             } else {
-                const double2 v = unit_at(cur, 0, u, t, sw_me);
-                be[KL + 2 * u] = v.x;
-                be[KL + 2 * u + 1] = v.y;
+#pragma unroll
+                for (int e = 0; e < EPU; ++e) v[e] = re[e];
             }
+        };
+#pragma unroll
+        for (int u = 0; u < UD; ++u) {
+            V v[EPU];
+            rows_of(u, t, sw_me, v);
+#pragma unroll
+            for (int e = 0; e < EPU; ++e) be[KL + EPU * u + e] = v[e];
         }
         if constexpr (KL > 0) {
             V pv[2] = {O::zero(), O::zero()};
-            if (has_prev) {
-                if constexpr (C::CPLX) {
-                    const double2 re = unit_at(cur, 0, U - 1, t - 1, sw_prev), im = unit_at(cur, 1, U - 1, t - 1, sw_prev);
-                    pv[0] = make_double2(re.x, im.x);
-                    pv[1] = make_double2(re.y, im.y);
-                } else {
-                    const double2 v = unit_at(cur, 0, U - 1, t - 1, sw_prev);
-                    pv[0] = v.x;
-                    pv[1] = v.y;
-                }
+            if (has_prev) {  // the last two rows of the chunk before
+                V v[EPU];
+                rows_of(UD - 1, t - 1, sw_prev, v);
+                pv[0] = v[EPU - 2];
+                pv[1] = v[EPU - 1];
             }
             be[KL - 1] = pv[1];
             if constexpr (KL > 1) be[0] = pv[0];
         }
         if constexpr (KU > 0) {
             V nv[2] = {O::zero(), O::zero()};
-            if (has_next) {
-                if constexpr (C::CPLX) {
-                    const double2 re = unit_at(cur, 0, 0, t + 1, sw_next), im = unit_at(cur, 1, 0, t + 1, sw_next);
-                    nv[0] = make_double2(re.x, im.x);
-                    nv[1] = make_double2(re.y, im.y);
-                } else {
-                    const double2 v = unit_at(cur, 0, 0, t + 1, sw_next);
-                    nv[0] = v.x;
-                    nv[1] = v.y;
-                }
+            if (has_next) {  // the first two rows of the chunk after
+                V v[EPU];
+                rows_of(0, t + 1, sw_next, v);
+                nv[0] = v[0];
+                nv[1] = v[1];
             }
             be[KL + R] = nv[0];
             if constexpr (KU > 1) be[KL + R + 1] = nv[1];
@@ -548,7 +600,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         // x = (V A b) scaled by the LU pivots, in place over be[0 .. R)
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            double2 wc[NB];
+            CT2 wc[NB];
 #pragma unroll
             for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
 #pragma unroll
@@ -658,16 +710,16 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             // couplings in one paired scan
 #pragma unroll
             for (int u = 1; u < U; ++u) {
-                const double2 c = coef(C::P_NL, u);
+                const CT2 c = coef(C::P_NL, u);
                 x[2 * u] = O::fma(c.x, x[2 * u - 2], x[2 * u]);
                 x[2 * u + 1] = O::fma(c.y, x[2 * u - 1], x[2 * u + 1]);
             }
             const double2 pin = group_affine_scan2<true>(g, make_double2(Af, Af1), make_double2(x[R - 2], x[R - 1]));
             const V pin0 = pin.x, pin1 = pin.y;
-            double p0 = 1.0, p1 = 1.0;
+            CT p0 = 1, p1 = 1;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double2 c = coef(C::P_NL, u);
+                const CT2 c = coef(C::P_NL, u);
                 p0 = c.x * p0;
                 x[2 * u] = O::fma(p0, pin0, x[2 * u]);
                 p1 = c.y * p1;
@@ -679,17 +731,17 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             // from the preceding chunks scaled by prod_{k<=j}(-l_k)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double2 c = coef(C::P_NL, u);
+                const CT2 c = coef(C::P_NL, u);
                 if (u > 0) x[2 * u] = O::fma(c.x, x[2 * u - 1], x[2 * u]);
                 x[2 * u + 1] = O::fma(c.y, x[2 * u], x[2 * u + 1]);
             }
             V pin;
-            if constexpr (kPre) pin = group_affine_scan_pre<V, double, true>(g, mf, x[R - 1]);
-            else pin = group_affine_scan<V, double, true>(g, Af, x[R - 1]);
-            double p = 1.0;
+            if constexpr (kPre) pin = group_affine_scan_pre<V, CT, true>(g, mf, x[R - 1]);
+            else pin = group_affine_scan<V, CT, true>(g, Af, x[R - 1]);
+            CT p = 1;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double2 c = coef(C::P_NL, u);
+                const CT2 c = coef(C::P_NL, u);
                 p = c.x * p;
                 x[2 * u] = O::fma(p, pin, x[2 * u]);
                 p = c.y * p;
@@ -699,16 +751,16 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         if constexpr (C::BWD && !C::MIXED && C::ALT) {
 #pragma unroll
             for (int u = U - 2; u >= 0; --u) {
-                const double2 c = coef(C::P_NH, u);
+                const CT2 c = coef(C::P_NH, u);
                 x[2 * u + 1] = O::fma(c.y, x[2 * u + 3], x[2 * u + 1]);
                 x[2 * u] = O::fma(c.x, x[2 * u + 2], x[2 * u]);
             }
             const double2 q = group_affine_scan2<false>(g, make_double2(Ab, Ab1), make_double2(x[0], x[1]));
             const V q0 = q.x, q1 = q.y;
-            double p0 = 1.0, p1 = 1.0;
+            CT p0 = 1, p1 = 1;
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
-                const double2 c = coef(C::P_NH, u);
+                const CT2 c = coef(C::P_NH, u);
                 p1 = c.y * p1;
                 x[2 * u + 1] = O::fma(p1, q1, x[2 * u + 1]);
                 p0 = c.x * p0;
@@ -718,17 +770,17 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         if constexpr (C::BWD && !C::MIXED && !C::ALT) {
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
-                const double2 c = coef(C::P_NH, u);
+                const CT2 c = coef(C::P_NH, u);
                 if (u < U - 1) x[2 * u + 1] = O::fma(c.y, x[2 * u + 2], x[2 * u + 1]);
                 x[2 * u] = O::fma(c.x, x[2 * u + 1], x[2 * u]);
             }
             V q;
-            if constexpr (kPre) q = group_affine_scan_pre<V, double, false>(g, mb, x[0]);
-            else q = group_affine_scan<V, double, false>(g, Ab, x[0]);
-            double p = 1.0;
+            if constexpr (kPre) q = group_affine_scan_pre<V, CT, false>(g, mb, x[0]);
+            else q = group_affine_scan<V, CT, false>(g, Ab, x[0]);
+            CT p = 1;
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
-                const double2 c = coef(C::P_NH, u);
+                const CT2 c = coef(C::P_NH, u);
                 p = c.y * p;
                 x[2 * u + 1] = O::fma(p, q, x[2 * u + 1]);
                 p = c.x * p;
@@ -739,7 +791,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         if constexpr (C::SCALE) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const double2 c = coef(C::P_SC, u);
+                const CT2 c = coef(C::P_SC, u);
                 x[2 * u] = O::mul(c.x, x[2 * u]);
                 x[2 * u + 1] = O::mul(c.y, x[2 * u + 1]);
             }
@@ -751,24 +803,33 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             if (W > 1) group_bar(g.bar_id, g.nthr);
         }
         __syncwarp();
+        // output unit uo holds EPUO rows (packed complex: re, im of each)
+        auto out_unit = [&](int p, int uo) -> unsigned char* {
+            return cur + out_row(p, uo / IBO, t) + (((uo % IBO) ^ swo_me) << 4);
+        };
         if constexpr (C::OPK) {
 #pragma unroll
-            for (int j = 0; j < R; ++j) {
-                const int h = j / IBO, uu = j % IBO;
-                *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) = x[j];
+            for (int uo = 0; uo < UO; ++uo) {
+                MS v[4];
+#pragma unroll
+                for (int e = 0; e < C::EPUO; ++e) {
+                    v[2 * e] = x[C::EPUO * uo + e].x;
+                    v[2 * e + 1] = x[C::EPUO * uo + e].y;
+                }
+                put_unit(out_unit(0, uo), v);
             }
         } else {
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int h = u / IBO, uu = u % IBO;
-                if constexpr (C::CPLX) {
-                    *reinterpret_cast<double2*>(cur + (size_t)((0 * HO + h) * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
-                        make_double2(x[2 * u].x, x[2 * u + 1].x);
-                    *reinterpret_cast<double2*>(cur + (size_t)((1 * HO + h) * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
-                        make_double2(x[2 * u].y, x[2 * u + 1].y);
-                } else {
-                    *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
-                        make_double2(x[2 * u], x[2 * u + 1]);
+            for (int uo = 0; uo < UO; ++uo) {
+#pragma unroll
+                for (int p = 0; p < C::NPOUT; ++p) {
+                    MS v[4];
+#pragma unroll
+                    for (int e = 0; e < EPU; ++e) {
+                        if constexpr (C::CPLX) v[e] = p ? x[EPU * uo + e].y : x[EPU * uo + e].x;
+                        else v[e] = x[EPU * uo + e];
+                    }
+                    put_unit(out_unit(p, uo), v);
                 }
             }
         }

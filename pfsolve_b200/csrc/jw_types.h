@@ -8,12 +8,17 @@ enum : int { SV_NONE = 0, SV_LOWER = 1, SV_UPPER = 2, SV_TRI = 3 };
 enum : int { LAY_REAL = 0, LAY_XXII = 1, LAY_PACKED = 2 };
 enum : int { MVJ_NONE = 0, MVJ_DIAG = 1, MVJ_UPPER = 2, MVJ_LOWER = 3 };
 // Arithmetic of a kernel variant: FP64; FP32 solve + FP64 refinement;
-// double-double on double-double storage; double-double on FP64 storage.
-enum : int { PREC_F64 = 0, PREC_MIXED = 1, PREC_DD = 2, PREC_DD_F64MEM = 3 };
+// double-double on double-double storage; double-double on FP64 storage;
+// FP32 on FP32 storage (the reference's default precision); FP64 on FP32
+// storage (its doublePrecisionFloatMemory).
+enum : int { PREC_F64 = 0, PREC_MIXED = 1, PREC_DD = 2, PREC_DD_F64MEM = 3, PREC_F32 = 4, PREC_F64_F32MEM = 5 };
+
+// Precisions whose buffers (bands, dgbmv matrix, right-hand sides) hold FP32 values.
+constexpr bool prec_f32_storage(int prec) { return prec == PREC_F32 || prec == PREC_F64_F32MEM; }
 
 // The matrix side of a JW step: where the bands live and how to read them.
 struct JwOperator {
-    const double* bands;  // JW band buffer (FP64)
+    const double* bands;  // JW band buffer (FP64, or FP32 values when bands32)
     int64_t off_md, off_mo, off_sl, off_su;  // band offsets in elements (resolved on the host)
     int mvj;                                 // JW matvec kind (MVJ_*)
     int perm;                                // 1: bands in the reference's register-major order
@@ -36,14 +41,15 @@ struct JwOperator {
     // rows (entry of row r = 2 e + h at (e % alt_R) alt_T + h alt_T/2 + e / alt_R)
     int alt, alt_h;
     int64_t alt_T, alt_R;
+    int bands32;  // bands and the dgbmv matrix hold FP32 values (FP32-storage precisions)
 };
 
 // The data side: systems, layouts, keep-windows.
 struct JwIO {
-    const double* in;
+    const double* in;             // FP64 values, or FP32 values for the FP32-storage precisions
     double* out;
-    int64_t in_off, in_stride;    // elements (see LAY_*)
-    int64_t out_off, out_stride;  // elements of the output type (double or double2)
+    int64_t in_off, in_stride;    // elements of the storage type (see LAY_*)
+    int64_t out_off, out_stride;  // elements of the output type (real or complex, of the storage type)
     int64_t iz0, iz1;             // rows read as data: [iz0, iz1); others read as 0
     int64_t oz0, oz1;             // rows written: [oz0, oz1)
     int64_t nsys;                 // systems (real, or complex pairs)

@@ -56,6 +56,28 @@ inline void dd_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, co
 #define PFB_R2(KL, KU, SV, LIN, LOUT, SC) PFB_V(4, KL, KU, SV, LIN, LOUT, SC), PFB_V(8, KL, KU, SV, LIN, LOUT, SC)
 #define PFB_M2(KL, KU, SV, LIN, LOUT, SC) \
     PFB_VP(4, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED), PFB_VP(8, KL, KU, SV, LIN, LOUT, SC, PREC_MIXED)
+// the same rows-per-thread choices in a given precision (the FP32-storage ones)
+#define PFB_R4P(KL, KU, SV, LIN, LOUT, SC, P)                                                                \
+    PFB_VP(2, KL, KU, SV, LIN, LOUT, SC, P), PFB_VP(4, KL, KU, SV, LIN, LOUT, SC, P),                          \
+        PFB_VP(8, KL, KU, SV, LIN, LOUT, SC, P), PFB_VP(16, KL, KU, SV, LIN, LOUT, SC, P)
+#define PFB_R2P(KL, KU, SV, LIN, LOUT, SC, P) PFB_VP(4, KL, KU, SV, LIN, LOUT, SC, P), PFB_VP(8, KL, KU, SV, LIN, LOUT, SC, P)
+// every application kind of the FP32-storage precisions: the JW application
+// on real systems, the dgbmv application with KL, KU <= 2, and the fused
+// chains the FP64 tables hold
+#define PFB_F32_KINDS(P)                                                                                      \
+    PFB_R4P(0, 0, SV_TRI, LAY_REAL, LAY_REAL, false, P), PFB_R4P(0, 1, SV_LOWER, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R4P(0, 1, SV_NONE, LAY_REAL, LAY_REAL, false, P), PFB_R4P(0, 0, SV_LOWER, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R4P(1, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, P), PFB_R4P(1, 0, SV_NONE, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R4P(0, 0, SV_UPPER, LAY_REAL, LAY_REAL, false, P), PFB_R2P(1, 1, SV_NONE, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R2P(2, 2, SV_NONE, LAY_REAL, LAY_REAL, false, P), PFB_R2P(0, 2, SV_NONE, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R2P(2, 0, SV_NONE, LAY_REAL, LAY_REAL, false, P), PFB_R2P(1, 2, SV_NONE, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R2P(2, 1, SV_NONE, LAY_REAL, LAY_REAL, false, P), PFB_R2P(0, 0, SV_NONE, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R2P(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, false, P), PFB_R2P(1, 1, SV_LOWER, LAY_REAL, LAY_REAL, false, P), \
+        PFB_R2P(1, 1, SV_TRI, LAY_REAL, LAY_REAL, false, P), PFB_R2P(2, 2, SV_TRI, LAY_REAL, LAY_REAL, false, P),   \
+        PFB_R2P(0, 0, SV_TRI, LAY_REAL, LAY_REAL, true, P), PFB_R2P(1, 1, SV_UPPER, LAY_REAL, LAY_REAL, true, P),   \
+        PFB_R2P(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, false, P), PFB_R2P(2, 2, SV_TRI, LAY_XXII, LAY_PACKED, true, P), \
+        PFB_R2P(0, 0, SV_TRI, LAY_XXII, LAY_PACKED, false, P), PFB_R2P(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, true, P), \
+        PFB_R2P(1, 1, SV_UPPER, LAY_XXII, LAY_PACKED, false, P), PFB_R2P(0, 0, SV_UPPER, LAY_XXII, LAY_PACKED, true, P)
 
 
 }  // namespace pfb

@@ -12,10 +12,13 @@ const JwVariant* jw_variants_real(int* count);
 const JwVariant* jw_variants_chain(int* count);
 const JwVariant* jw_variants_mixed(int* count);
 const JwVariant* jw_variants_dd(int* count);
+const JwVariant* jw_variants_f32(int* count);
+const JwVariant* jw_variants_f32mem(int* count);
 
 namespace {
 using PartFn = const JwVariant* (*)(int*);
-const PartFn kParts[] = {jw_variants_real, jw_variants_chain, jw_variants_mixed, jw_variants_dd};
+const PartFn kParts[] = {jw_variants_real, jw_variants_chain, jw_variants_mixed, jw_variants_dd, jw_variants_f32,
+                         jw_variants_f32mem};
 }  // namespace
 
 const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC, int TBL)
@@ -38,8 +41,14 @@ const JwVariant* find_jw_variant(int R, int KL, int KU, int SV, int LIN, int LOU
 // (PfSolve/pfSolve_CodeGen/pfSolve_KernelsLevel2/pfSolve_block.h:37-115).
 // HBM-bound elementwise work: a grid-stride loop over rows y with the threads
 // of a block striding x, so reads and writes of each row are coalesced.
+// T: the storage type (FP64, or FP32 for the FP32-storage precisions); values
+// are widened to FP64 in registers and rounded once on store.
+template <class T>
 __global__ void __launch_bounds__(256) block_kernel(const BlockArgs a)
 {
+    using T2 = typename Vec2Of<T>::type;
+    const T* in = reinterpret_cast<const T*>(a.in);
+    T* out = reinterpret_cast<T*>(a.out);
     const int bt = a.layout;
     for (int64_t y = blockIdx.x; y < a.size1; y += gridDim.x) {
         const int64_t ii = a.in_off + y * a.in_stride;
@@ -49,16 +58,16 @@ __global__ void __launch_bounds__(256) block_kernel(const BlockArgs a)
             if (!a.skip_read) {
                 if (x >= a.iz0 && x < a.iz1) {
                     switch (bt) {
-                    case 1: vr = a.in[ii + x]; break;
+                    case 1: vr = in[ii + x]; break;
                     case 2: case 3: case 4: {
-                        const double2 v = reinterpret_cast<const double2*>(a.in)[ii + x];
+                        const T2 v = reinterpret_cast<const T2*>(in)[ii + x];
                         vr = v.x;
                         vi = v.y;
                         break;
                     }
-                    case 5: vr = a.in[ii + x]; break;
-                    case 6: vi = a.in[ii + x]; break;
-                    default: vr = a.in[2 * ii + x]; vi = a.in[2 * ii + x + a.in_stride]; break;
+                    case 5: vr = in[ii + x]; break;
+                    case 6: vi = in[ii + x]; break;
+                    default: vr = in[2 * ii + x]; vi = in[2 * ii + x + a.in_stride]; break;
                     }
                 }
                 if (a.scale_kind) {
@@ -70,27 +79,27 @@ __global__ void __launch_bounds__(256) block_kernel(const BlockArgs a)
             if (x < a.oz0 || x >= a.oz1) continue;
             switch (bt) {
             case 1: case 2: {
-                double* p = a.out + oi + x;
-                *p = a.accumulate ? vr + *p : vr;
+                T* p = out + oi + x;
+                *p = (T)(a.accumulate ? vr + (double)*p : vr);
                 break;
             }
             case 3: {
-                double* p = a.out + oi + x;
-                *p = a.accumulate ? vi + *p : vi;
+                T* p = out + oi + x;
+                *p = (T)(a.accumulate ? vi + (double)*p : vi);
                 break;
             }
             case 4:
-                a.out[2 * oi + x] = vr;
-                a.out[2 * oi + x + a.out_stride] = vi;
+                out[2 * oi + x] = (T)vr;
+                out[2 * oi + x + a.out_stride] = (T)vi;
                 break;
             default: {
-                double2* p = reinterpret_cast<double2*>(a.out) + oi + x;
+                T2* p = reinterpret_cast<T2*>(out) + oi + x;
                 if (a.accumulate) {
-                    const double2 o = *p;
+                    const T2 o = *p;
                     vr += o.x;
                     vi += o.y;
                 }
-                *p = make_double2(vr, vi);
+                *p = T2{(T)vr, (T)vi};
                 break;
             }
             }
@@ -104,29 +113,33 @@ void launch_block(const BlockArgs& a, cudaStream_t st, int num_sms)
     const int64_t cap = (int64_t)num_sms * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    block_kernel<<<(unsigned)blocks, 256, 0, st>>>(a);
+    if (a.f32) block_kernel<float><<<(unsigned)blocks, 256, 0, st>>>(a);
+    else block_kernel<double><<<(unsigned)blocks, 256, 0, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------
 // dgbmv with any bandwidth (pfSolve_KernelsLevel1/pfSolve_MatVecMul.h:383-446):
 // one block per system, the system staged in shared memory (zero outside the
 // input keep-window), y_r = sum_j A[off + j*M + c] x_c, c = r + ku - j.
+// T: the storage type of A and x; the sums run in FP64.
+template <class T>
 __global__ void __launch_bounds__(256) dgbmv_generic_kernel(const DgbmvArgs a)
 {
     extern __shared__ double xs[];
+    const T* A = reinterpret_cast<const T*>(a.A);
     for (int64_t sys = blockIdx.x; sys < a.nsys; sys += gridDim.x) {
-        double* x = a.x + a.off_x + sys * a.stride;
+        T* x = reinterpret_cast<T*>(a.x) + a.off_x + sys * a.stride;
         for (int64_t r = threadIdx.x; r < a.M; r += blockDim.x)
-            xs[r] = (r >= a.iz0 && r < a.iz1) ? x[r] : 0.0;
+            xs[r] = (r >= a.iz0 && r < a.iz1) ? (double)x[r] : 0.0;
         __syncthreads();
         for (int64_t r = threadIdx.x; r < a.M; r += blockDim.x) {
             double acc = 0.0;
             for (int j = 0; j < a.lda; ++j) {
                 const int64_t c = r + a.ku - j;
                 if (c < 0 || c >= a.M || (j < 64 && ((a.skip >> j) & 1))) continue;
-                acc = __fma_rn(__ldg(a.A + a.off_A + (int64_t)j * a.M + c), xs[c], acc);
+                acc = __fma_rn((double)__ldg(A + a.off_A + (int64_t)j * a.M + c), xs[c], acc);
             }
-            if (r >= a.oz0 && r < a.oz1) x[r] = acc;
+            if (r >= a.oz0 && r < a.oz1) x[r] = (T)acc;
         }
         __syncthreads();
     }
@@ -139,9 +152,13 @@ void launch_dgbmv_generic(const DgbmvArgs& a, cudaStream_t st, int num_sms)
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     const size_t smem = (size_t)a.M * sizeof(double);
-    if (smem > 48 * 1024)
-        allow_max_smem((const void*)dgbmv_generic_kernel);
-    dgbmv_generic_kernel<<<(unsigned)blocks, 256, smem, st>>>(a);
+    if (a.f32) {
+        if (smem > 48 * 1024) allow_max_smem((const void*)dgbmv_generic_kernel<float>);
+        dgbmv_generic_kernel<float><<<(unsigned)blocks, 256, smem, st>>>(a);
+    } else {
+        if (smem > 48 * 1024) allow_max_smem((const void*)dgbmv_generic_kernel<double>);
+        dgbmv_generic_kernel<double><<<(unsigned)blocks, 256, smem, st>>>(a);
+    }
 }
 
 }  // namespace pfb

@@ -81,7 +81,9 @@ const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, i
 // Tensor maps of a launch's input and output rows; false when the buffers'
 // alignment, strides or M do not allow the streaming layout.
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out);
-bool encode_row_maps(int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out);
+// es: bytes per stored value (8: FP64, 4: FP32).
+bool encode_row_maps(int R, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out,
+                     int es = 8);
 
 // Long-system variants: one cluster of C CTAs per system, each CTA a slice of
 // 32*W*R rows (real systems, FP64).
@@ -97,19 +99,24 @@ struct ClusterVariant {
 };
 const ClusterVariant* find_cluster_variant(int C, int KL, int KU, int SV);
 
-// Long systems in two passes (no cross-CTA waits): slices of S = 32 W R rows,
-// G systems in flight per CTA; launch = the table passes (two for a
-// tridiagonal solve), pass 1, the carry kernel (solves only) and pass 2 on the
-// stream.  red: nsys * NS records of 8 doubles, cst: NS records of 8 doubles,
-// tab: NS slice tables of tbl_bytes.
+// Long systems over slices of S = 32 W R rows, G systems in flight per CTA;
+// launch = the table passes (two for a tridiagonal solve), then the single
+// pass (`single`: one cooperative launch whose CTAs wait for the other slices
+// of each system, up to kLgMaxSlices slices) or pass 1, the carry kernel
+// (solves only) and pass 2 on the stream.  red: nsys * NS records of 8
+// doubles, cst: NS records of 8 doubles, tab: NS slice tables of tbl_bytes,
+// flags: nsys * NS words (single pass; zero before the first launch),
+// epoch: the launch's flag value (never 0, never repeated while flags live).
 struct LongVariant {
     int R, W, G, KL, KU, SV, S;
     int IB, IBO;
     size_t tbl_bytes;
     cudaError_t (*launch)(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
-                          const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS);
+                          const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS,
+                          unsigned* flags, unsigned epoch, bool single);
     int (*blocks_per_sm)();  // resident CTAs per SM (0: does not fit)
 };
+constexpr int kLongMaxSlices = 64;  // slices per system of the single pass
 constexpr int kLongShapes = 3;  // compiled shapes per operator kind, in order of preference
 const LongVariant* find_long_variant(int shape, int KL, int KU, int SV);
 unsigned long_status_fetch_clear();
@@ -158,6 +165,7 @@ struct BlockArgs {
     int scale_kind, lshift;
     double s;
     int skip_read;
+    int f32;  // FP32 storage (in and out hold FP32 values)
 };
 void launch_block(const BlockArgs& a, cudaStream_t st, int num_sms);
 
@@ -168,6 +176,7 @@ struct DgbmvArgs {
     int lda, ku;
     int64_t iz0, iz1, oz0, oz1;
     uint64_t skip;  // ALT_dgbmv: bit j set drops band j
+    int f32;        // FP32 storage (A and x hold FP32 values)
 };
 void launch_dgbmv_generic(const DgbmvArgs& a, cudaStream_t st, int num_sms);
 

@@ -9,18 +9,36 @@
 
 namespace pfb {
 
+// The table passes, then either the single pass (a cooperative launch: every
+// CTA resident, as its cross-CTA waits need) or pass 1, the carry kernel and
+// pass 2.
 template <class C>
 static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
-                                const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS)
+                                const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS,
+                                unsigned* flags, unsigned epoch, bool single)
 {
     const size_t smem = lg_smem_bytes<C>();
-    if (C::SV == SV_TRI) jw_long_kernel<C, 3><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
-    jw_long_kernel<C, 0><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
-    jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
+    if (C::SV == SV_TRI)
+        jw_long_kernel<C, 3><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS, flags, epoch);
+    jw_long_kernel<C, 0><<<NS, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS, flags, epoch);
+    if (single) {
+        if (NS > kLgMaxSlices) return cudaErrorInvalidValue;
+        CUtensorMap tin = *in, tout = *out;
+        JwOperator o = op;
+        JwIO i = io;
+        int ns = NS;
+        unsigned ep = epoch;
+        void* args[] = {&tin, &tout, &o, &i, &red, &cst, &tab, &ns, &flags, &ep};
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void*)&jw_long_kernel<C, 4>, dim3((unsigned)grid),
+                                                          dim3(C::NT), args, smem, st);
+        if (e != cudaSuccess) return e;
+        return cudaPeekAtLastError();
+    }
+    jw_long_kernel<C, 1><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS, flags, epoch);
     if (C::B::FWD || C::B::BWD)
         jw_long_carry_kernel<C::B::FWD, C::B::BWD>
             <<<(unsigned)((io.nsys + 127) / 128), 128, 0, st>>>(red, cst, NS, io.nsys);
-    jw_long_kernel<C, 2><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS);
+    jw_long_kernel<C, 2><<<grid, C::NT, smem, st>>>(*in, *out, op, io, red, cst, tab, NS, flags, epoch);
     return cudaPeekAtLastError();
 }
 
@@ -35,13 +53,17 @@ static int lg_blocks_per_sm()
     const void* f0 = (const void*)&jw_long_kernel<C, 0>;
     const void* f1 = (const void*)&jw_long_kernel<C, 1>;
     const void* f2 = (const void*)&jw_long_kernel<C, 2>;
-    if (!allow_max_smem(f0) || !allow_max_smem(f1) || !allow_max_smem(f2)) return 0;
+    const void* f4 = (const void*)&jw_long_kernel<C, 4>;
+    if (!allow_max_smem(f0) || !allow_max_smem(f1) || !allow_max_smem(f2) || !allow_max_smem(f4)) return 0;
+    int b4 = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, f1, C::NT, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, f4, C::NT, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    return b1 < b2 ? b1 : b2;
+    const int b = b1 < b2 ? b1 : b2;
+    return b < b4 ? b : b4;
 }
 
 #define PFB_LG(R, W, G, KL, KU, SV)                                                                    \

@@ -12,14 +12,19 @@ namespace pfb {
 const StreamVariant* stream_variants_f64(int* count);
 const StreamVariant* stream_variants_mixed(int* count);
 const StreamVariant* stream_variants_alt(int* count);
+const StreamVariant* stream_variants_f32(int* count);
+const StreamVariant* stream_variants_f32mem(int* count);
 unsigned stream_status_f64();
 unsigned stream_status_mixed();
 unsigned stream_status_alt();
+unsigned stream_status_f32();
+unsigned stream_status_f32mem();
 
 const StreamVariant* find_stream_variant(int R, int W, int KL, int KU, int SV, int LIN, int LOUT, int SCALE, int PREC,
                                          int ALT)
 {
-    for (auto part : {stream_variants_f64, stream_variants_mixed, stream_variants_alt}) {
+    for (auto part : {stream_variants_f64, stream_variants_mixed, stream_variants_alt, stream_variants_f32,
+                      stream_variants_f32mem}) {
         int n = 0;
         const StreamVariant* vs = part(&n);
         for (int i = 0; i < n; ++i) {
@@ -62,39 +67,44 @@ CUtensorMapSwizzle swizzle_for(int units)
     }
 }
 
-// 3-D view of a set of rows: {row in chunk (inner, `inner` doubles), chunk
-// (`chunks`, `inner` doubles apart), row set (`sets`, `set_stride` bytes apart)};
-// box {box_units * 2 doubles, 32 chunks, 1 set}.
+// 3-D view of a set of rows of `es`-byte elements (FP64 or FP32): {row in
+// chunk (inner, `inner` elements), chunk (`chunks`, `inner` elements apart),
+// row set (`sets`, `set_stride` bytes apart)}; box {box_units 16-byte units,
+// 32 chunks, 1 set}.
 bool encode_rows(CUtensorMap* map, const void* base, int64_t inner, int64_t chunks, int64_t sets, int64_t set_stride,
-                 int box_units)
+                 int box_units, int es)
 {
     EncodeTiledFn fn = encode_fn();
-    if (!fn) return false;
-    if (reinterpret_cast<uintptr_t>(base) % 16 || set_stride % 16 || set_stride <= 0 || sets < 1 || sets > INT32_MAX)
+    if (!fn || (es != 4 && es != 8)) return false;
+    if (reinterpret_cast<uintptr_t>(base) % 16 || set_stride % 16 || set_stride <= 0 || sets < 1 || sets > INT32_MAX ||
+        (inner * es) % 16)
         return false;
     const cuuint64_t dims[3] = {(cuuint64_t)inner, (cuuint64_t)chunks, (cuuint64_t)sets};
-    const cuuint64_t strides[2] = {(cuuint64_t)(inner * 8), (cuuint64_t)set_stride};
-    const cuuint32_t box[3] = {(cuuint32_t)(box_units * 2), 32u, 1u};
+    const cuuint64_t strides[2] = {(cuuint64_t)(inner * es), (cuuint64_t)set_stride};
+    const cuuint32_t box[3] = {(cuuint32_t)(box_units * (16 / es)), 32u, 1u};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
-    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(base), dims, strides, box, estr,
+    return fn(map, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+              const_cast<void*>(base), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(box_units), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 }  // namespace
 
-bool encode_row_maps(int R_, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
+bool encode_row_maps(int R_, int LIN, int LOUT, int IB, int IBO, const JwIO& io, CUtensorMap* in, CUtensorMap* out,
+                     int es)
 {
     const int64_t R = R_, M = io.M;
     if (M % R != 0 || io.nsys < 1) return false;
     const int64_t chunks = M / R;
     const bool cplx = LIN != LAY_REAL;
     const int64_t sets = cplx ? 2 * io.nsys : io.nsys;
-    if (!encode_rows(in, io.in + io.in_off, R, chunks, sets, io.in_stride * 8, IB)) return false;
-    if (LOUT == LAY_PACKED)
-        return encode_rows(out, reinterpret_cast<const double2*>(io.out) + io.out_off, 2 * R, chunks, io.nsys,
-                           io.out_stride * 16, IBO);
+    const char* in0 = reinterpret_cast<const char*>(io.in) + io.in_off * es;
+    char* out0 = reinterpret_cast<char*>(io.out);
+    if (!encode_rows(in, in0, R, chunks, sets, io.in_stride * es, IB, es)) return false;
+    if (LOUT == LAY_PACKED)  // complex elements of 2 es bytes: 2 R storage elements per chunk
+        return encode_rows(out, out0 + io.out_off * 2 * es, 2 * R, chunks, io.nsys, io.out_stride * 2 * es, IBO, es);
     const int64_t osets = (LOUT == LAY_XXII) ? 2 * io.nsys : io.nsys;
-    return encode_rows(out, io.out + io.out_off, R, chunks, osets, io.out_stride * 8, IBO);
+    return encode_rows(out, out0 + io.out_off * es, R, chunks, osets, io.out_stride * es, IBO, es);
 }
 
 bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* in, CUtensorMap* out)
@@ -152,16 +162,17 @@ bool encode_batch_seq_maps(const JwIO& io, BatchSeqEntry* e)
 
 bool encode_stream_maps(const StreamVariant* v, const JwIO& io, CUtensorMap* in, CUtensorMap* out)
 {
-    return encode_row_maps(v->R, v->LIN, v->LOUT, v->IB, v->IBO, io, in, out);
+    return encode_row_maps(v->R, v->LIN, v->LOUT, v->IB, v->IBO, io, in, out, prec_f32_storage(v->PREC) ? 4 : 8);
 }
 
 unsigned stream_status_fetch_clear()
 {
     const unsigned a = stream_status_f64(), b = stream_status_mixed(), c = cluster_status_fetch_clear();
     const unsigned d = steps_status_fetch_clear(), e = batch_status_fetch_clear(), f = long_status_fetch_clear();
-    const unsigned g = stream_status_alt();
-    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u || f == ~0u || g == ~0u) return ~0u;
-    return a | b | c | d | e | f | g;
+    const unsigned g = stream_status_alt(), h = stream_status_f32(), i = stream_status_f32mem();
+    if (a == ~0u || b == ~0u || c == ~0u || d == ~0u || e == ~0u || f == ~0u || g == ~0u || h == ~0u || i == ~0u)
+        return ~0u;
+    return a | b | c | d | e | f | g | h | i;
 }
 
 }  // namespace pfb

@@ -8,8 +8,10 @@ the reference's outputs as ``<out>/<case>.npz``.  Needs a CUDA GPU; run it as
 kernel on the full-size configurations and writes ``ref_timing.json``.
 Subsets (``--only``): K-step fixtures, ALT mode, long systems (into
 ``<out>/long/``), double-double (into ``<out>/dd/``, copied to
-``tests/golden/dd/``), and ``dd-crash``, which re-runs the double-double cases
-the reference's code generation crashes on and stores no fixtures.
+``tests/golden/dd/``), ``dd-crash``, which re-runs the double-double cases
+the reference's code generation crashes on and stores no fixtures, and
+``f32``: the FP32-storage precisions (into ``<out>/f32/``, copied to
+``tests/golden/f32/``).
 """
 from __future__ import annotations
 
@@ -103,6 +105,48 @@ def jw_cases():
     case = O.Case(M=M, batch=3, upperBanded=2, jw_type=13)
     out.append(("jw_f32_M256", case, WL.permute_bands(WL.tri_bands(*WL.tridiagonal(rng, M)), M),
                 rng.uniform(-1, 1, case.rhs_len()), "f32"))
+    return out
+
+
+def f32_cases():
+    """(name, Case, buffer, rhs, precision) on FP32 storage: the reference's
+    default precision ("f32": FP32 arithmetic) and doublePrecisionFloatMemory
+    ("f32mem": FP64 arithmetic), for every JW mode, launch-time values, the
+    dgbmv application and the block layouts.  Inputs are FP32 values."""
+    out = []
+    f = np.float32
+    for prec in ("f32", "f32mem"):
+        for ub, jwt in [(2, 13), (1, 10), (1, 11), (1, 12), (1, 13), (0, 10), (0, 11), (0, 12), (0, 13)]:
+            for M in ([33, 256, 1000] if (ub, jwt) in [(2, 13), (1, 10), (0, 10)] else [100]):
+                rng = np.random.default_rng(15000 + 100 * ub + jwt + M)
+                bands = WL.permute_bands(jw_bands(rng, M, ub), M).astype(f)
+                case = O.Case(M=M, batch=3, upperBanded=ub, jw_type=jwt)
+                out.append((f"{prec}_jw_ub{ub}_t{jwt}_M{M}", case, bands,
+                            rng.uniform(-1, 1, case.rhs_len()).astype(f), prec))
+        M = 200
+        bm = (RT.RUNTIME_OFFSETSOLUTION | RT.RUNTIME_INPUTZEROPAD | RT.RUNTIME_OUTPUTZEROPAD | RT.RUNTIME_SCALEC |
+              RT.RUNTIME_OUTPUTBUFFERSTRIDE)
+        for ub, jwt in [(2, 13), (1, 10), (0, 13)]:
+            rng = np.random.default_rng(15500 + ub)
+            case = O.Case(M=M, batch=4, upperBanded=ub, jw_type=jwt, bitmask=bm, run_offsetSolution=5,
+                          run_inputZeropad=(3, 190), run_outputZeropad=(5, 180), run_scaleC=0.625,
+                          run_outputBufferStride=M + 131)
+            out.append((f"{prec}_jw_runtime_ub{ub}_t{jwt}", case, WL.permute_bands(jw_bands(rng, M, ub), M).astype(f),
+                        rng.uniform(-1, 1, case.rhs_len() + 8).astype(f), prec))
+        for M, KL, KU in [(128, 2, 2), (64, 3, 1)]:
+            rng = np.random.default_rng(15700 + M + KL)
+            case = O.Case(M=M, batch=2, LDA=KL + KU + 1, KU=KU, KL=KL, jw_type=0)
+            out.append((f"{prec}_dgbmv_M{M}_kl{KL}_ku{KU}", case, WL.band_major(rng, M, KL, KU).astype(f),
+                        rng.uniform(-1, 1, case.rhs_len()).astype(f), prec))
+        N, Y = 40, 3
+        for block in (1, 4, 7, 27, 301):
+            rng = np.random.default_rng(15900 + block)
+            bt = block % 10
+            nin = (2 if bt in (2, 3, 4, 7) else 1) * N * Y
+            nout = (2 if bt in (4, 5, 6, 7) else 1) * N * Y
+            case = O.Case(M=N, batch=Y, block=block, lshift=2, jw_type=0, bitmask=RT.RUNTIME_SCALEC, run_scaleC=0.5)
+            out.append((f"{prec}_block_{block}", case, rng.standard_normal(nin).astype(f),
+                        rng.standard_normal(nout).astype(f), prec))
     return out
 
 
@@ -235,6 +279,12 @@ def long_cases():
             case = O.Case(M=M, batch=2, upperBanded=ub, jw_type=jwt)
             rhs = rng.uniform(-1, 1, case.rhs_len())
             out.append((f"long_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
+    # beyond one cluster of 8 x 2048 rows: up to 64 slices of 1024 rows
+    for M in (20000, 32768, 65536):
+        rng = np.random.default_rng(17500 + M)
+        bands = WL.permute_bands(jw_bands(rng, M, 2), M)
+        case = O.Case(M=M, batch=2, upperBanded=2, jw_type=13)
+        out.append((f"long_ub2_t13_M{M}", case, bands, rng.uniform(-1, 1, case.rhs_len()), "f64"))
     return out
 
 
@@ -309,7 +359,7 @@ def run_case(tmp, name, case, buf, rhs, prec):
     else:
         O.write_reference_case(d, case, buf, rhs, precision=prec)
     path, _ = O.run_reference(d)
-    dt = np.float32 if prec == "f32" else np.float64
+    dt = np.float32 if prec in ("f32", "f32mem") else np.float64
     return np.fromfile(path, dtype=dt)
 
 
@@ -317,10 +367,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "golden_out"))
     ap.add_argument("--time", action="store_true")
-    ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long", "dd", "dd-crash"],
+    ap.add_argument("--only", default="all", choices=["all", "steps", "alt", "long", "dd", "dd-crash", "f32"],
                     help="steps: only the K-step fixtures (and K-step timing with --time); alt: only ALT mode; "
                          "long: only long systems (N > 4352, and their timing with --time); dd: only the double-double "
-                         "fixtures; dd-crash: the double-double cases the reference crashes on (no fixtures)")
+                         "fixtures; dd-crash: the double-double cases the reference crashes on (no fixtures); "
+                         "f32: the FP32-storage precisions")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     tmp = os.path.join(args.out, "_cases")
@@ -444,6 +495,17 @@ def main():
         with open(os.path.join(args.out, "ref_timing_long.json"), "w") as f:
             json.dump(timing, f, indent=1)
         print(json.dumps(timing, indent=1))
+    fdir = os.path.join(args.out, "f32")
+    os.makedirs(fdir, exist_ok=True)
+    for name, case, buf, rhs, prec in (f32_cases() if args.only in ("all", "f32") else []):
+        try:
+            ref = run_case(tmp, name, case, buf, rhs, prec)
+            np.savez_compressed(os.path.join(fdir, name + ".npz"), params=json.dumps(asdict(case)),
+                                precision=prec, buffer=buf, rhs=rhs, ref_out=ref)
+            summary[name] = "ok"
+        except Exception as e:
+            summary[name] = f"error: {e}"
+            traceback.print_exc()
     ddir = os.path.join(args.out, "dd")
     os.makedirs(ddir, exist_ok=True)
     dd_set = {"all": DD_PINNED, "dd": DD_PINNED, "dd-crash": DD_CRASHING}.get(args.only, [])

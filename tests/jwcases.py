@@ -40,6 +40,34 @@ def run_app(case: O.Case, buffer: np.ndarray, out: np.ndarray, **extra):
     return res
 
 
+def precision_fields(prec: str) -> dict:
+    """PfSolveConfiguration precision fields: "f64", "f32" (FP32 storage and
+    arithmetic, the reference's default) or "f32mem" (FP64 arithmetic on FP32
+    storage, doublePrecisionFloatMemory)."""
+    if prec == "f64":
+        return dict(doublePrecision=1)
+    return dict(doublePrecision=0, doublePrecisionFloatMemory=1 if prec == "f32mem" else 0)
+
+
+def run_app_prec(case: O.Case, buffer: np.ndarray, out: np.ndarray, prec: str, **extra):
+    """run_app in a given precision; FP32-storage precisions take and return
+    float32 buffers."""
+    import torch
+
+    from pfsolve_b200.api import App
+    dt = np.float64 if prec == "f64" else np.float32
+    tb = torch.from_numpy(np.ascontiguousarray(buffer, dtype=dt)).cuda()
+    to = torch.from_numpy(np.array(out, dtype=dt, copy=True)).cuda()
+    fields = case_fields(case, **extra)
+    fields.update(precision_fields(prec))
+    app = App(buffer=tb, outputBuffer=to, **fields)
+    app.append(**launch_fields(case))
+    torch.cuda.synchronize()
+    res = to.cpu().numpy()
+    app.close()
+    return res
+
+
 def run_steps(case: O.Case, K: int, bufs, out: np.ndarray, **extra):
     """K consecutive steps in one app: ``bufs`` is one band buffer read by every
     step or a list of K per-step buffers (useMultipleInputBuffers = K).

@@ -98,3 +98,16 @@ def test_kernels_match_reference(path):
     case, prec, buf, rhs, ref = load(path)
     got = J.run_app(case, buf, rhs)
     assert np.abs(got - ref).max() <= 2e-13 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+def test_f32_kernel_matches_reference_default_precision():
+    """jw_f32_M256: the reference's default precision (FP32 storage and
+    arithmetic) run by the FP32 kernels: within 2e-5 of the reference's FP32
+    output (two FP32 solves that order their operations differently)."""
+    path = os.path.join(HERE, "golden", "jw_f32_M256.npz")
+    case, prec, buf, rhs, ref = load(path)
+    assert prec == "f32"
+    got = J.run_app_prec(case, buf, rhs, "f32").astype(np.float64)
+    ref = ref.astype(np.float64)
+    assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max()

@@ -1,12 +1,15 @@
 """GPU parity of the long-system JW kernels, through the C ABI.
 
-Systems of 4 096 < N <= 16 384 rows run on the two-pass kernel (slices, no
-waits between CTAs; the default, PfSolveGetShape streaming = 5) or, with
-kernelPath 2, on one thread-block cluster of 3, 4, 6 or 8 CTAs per system
-(streaming = 2).  Every case checks that the plan chose the kernel asked for,
-that the launch ran on it, and that every system matches the __float128
-oracle to 1e-13 relative L2 (the FP64 tolerance of the other kernels).  The
-app works in place, so the two-pass kernel's halo records are exercised."""
+Systems of 4 096 < N <= 65 536 rows run over slices of 1 024 rows
+(PfSolveGetShape streaming = 5): by default in a single pass, one
+cooperative launch whose CTAs wait (bounded) for the other slices of each
+system; with kernelPath 3 in two passes with no waits between CTAs.  With
+kernelPath 2, systems of up to 16 384 rows run on one thread-block cluster of
+3, 4, 6 or 8 CTAs per system (streaming = 2).  Every case checks that the
+plan chose the kernel asked for, that the launch ran on it, and that every
+system matches the __float128 oracle to 1e-13 relative L2 (the FP64
+tolerance of the other kernels).  The app works in place, so the halo rows
+of neighbouring slices are exercised."""
 import numpy as np
 import pytest
 
@@ -45,13 +48,15 @@ def _run(case, bands, rhs, **extra):
     return x, shape, n
 
 
-PATHS = {0: 5, 2: 2}  # kernelPath -> PfSolveGetShape streaming
+PATHS = {0: 5, 3: 5, 2: 2}  # kernelPath -> PfSolveGetShape streaming
 
 
 @pytest.mark.parametrize("path", list(PATHS))
 @pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (1, 11), (1, 12), (0, 10), (0, 11), (0, 13)])
-@pytest.mark.parametrize("M", [4104, 4360, 5000, 6000, 6144, 8192, 12000, 16384])
+@pytest.mark.parametrize("M", [4104, 4360, 5000, 6000, 6144, 8192, 12000, 16384, 20000, 40000, 65536])
 def test_long_modes_and_sizes(ub, jwt, M, path):
+    if path == 2 and M > 16384:
+        pytest.skip("the cluster kernel holds one system on 8 CTAs of 2048 rows at most")
     rng = np.random.default_rng(9000 + 10 * ub + jwt + M)
     case, bands, rhs = _case(rng, M, 7, ub, jwt)
     x, shape, n = _run(case, bands, rhs, kernelPath=path)
@@ -64,9 +69,12 @@ def test_long_modes_and_sizes(ub, jwt, M, path):
 @pytest.mark.parametrize("path", list(PATHS))
 def test_long_many_systems_and_windows(path):
     rng = np.random.default_rng(77)
-    M = 8192
-    for B, kw in [(301, {}), (65, dict(bitmask=capi.RUNTIME_INPUTZEROPAD, run_inputZeropad=(5, 8000))),
-                  (2000, {}), (40, dict(bitmask=capi.RUNTIME_INPUTZEROPAD, run_inputZeropad=(1030, 3100)))]:
+    for M, B, kw in [(8192, 301, {}), (8192, 65, dict(bitmask=capi.RUNTIME_INPUTZEROPAD, run_inputZeropad=(5, 8000))),
+                     (8192, 2000, {}),
+                     (8192, 40, dict(bitmask=capi.RUNTIME_INPUTZEROPAD, run_inputZeropad=(1030, 3100))),
+                     (65536, 150, {})]:
+        if path == 2 and M > 16384:
+            continue
         case, bands, rhs = _case(rng, M, B, 2, 13, **kw)
         x, shape, n = _run(case, bands, rhs, kernelPath=path)
         assert n == 1
@@ -83,6 +91,50 @@ def test_long_rejects_buffers_it_cannot_take(path):
     with pytest.raises(capi.PfSolveError) as ei:
         _run(case, bands, rhs, kernelPath=path)
     assert ei.value.code == capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION
+
+
+@pytest.mark.parametrize("M", [4097, 5001, 12345, 30001])
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (0, 13)])
+def test_single_pass_any_length(M, ub, jwt):
+    """Lengths that are not a multiple of the rows per thread: the last,
+    partial chunk moves between global memory and its staged rows outside
+    the TMA boxes (single pass only)."""
+    rng = np.random.default_rng(M + 10 * ub + jwt)
+    case, bands, rhs = _case(rng, M, 37, ub, jwt)
+    x, shape, n = _run(case, bands, rhs)
+    assert shape["streaming"] == 5 and n == 1, shape
+    e, emax = J.rel_err(x, O.jw_step(case, bands, rhs, "q"), case)
+    assert e <= TOL, (e, emax)
+
+
+def test_single_pass_is_the_default_and_repeats():
+    """The default plan runs the single pass (one long-kernel launch after the
+    table passes: three launches in all for a tridiagonal solve); repeated
+    launches of one plan (new flag epochs each time) give the same result."""
+    import torch
+
+    from pfsolve_b200.api import App, last_launch, launch_count
+    rng = np.random.default_rng(5)
+    M, B = 16384, 600
+    case, bands, rhs = _case(rng, M, B, 2, 13)
+    tb = torch.from_numpy(bands).cuda()
+    base = torch.from_numpy(rhs).cuda()
+    x = base.clone()
+    app = App(buffer=tb, outputBuffer=x, **J.case_fields(case))
+    n0 = launch_count()
+    app.append()
+    torch.cuda.synchronize()
+    assert launch_count() - n0 == 3
+    assert last_launch()["kernel"] == capi.PFSOLVE_KERNEL_LONG
+    first = x.cpu().numpy()
+    for _ in range(3):
+        x.copy_(base)
+        app.append()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(x.cpu().numpy(), first)
+    e, _ = J.rel_err(first, O.jw_step(case, bands, rhs, "q"), case)
+    assert e <= TOL
+    app.close()
 
 
 def test_cluster_device_status_clean():
