@@ -576,12 +576,21 @@ PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cud
     JwIO mio = io;  // the maps cover the whole chunks of R rows
     mio.M = (io.M / v->R) * v->R;
     const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, mio);
-    if (!e) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    // Rows no tensor map can describe (stride or offset not a multiple of 16
+    // bytes): the single pass moves them with plain loads and stores.
+    static const CUtensorMap kNoMap = {};
+    JwIO lio = io;
+    if (!e) {
+        if (!s->long_single) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        lio.plain = 1;
+    }
+    const CUtensorMap* tin = e ? &e->in : &kNoMap;
+    const CUtensorMap* tout = e ? &e->out : &kNoMap;
     double* cst = s->long_red + (size_t)s->long_batch * s->long_NS * 8;
     double* tab = cst + (size_t)s->long_NS * 8;
     if (++s->long_epoch == 0) s->long_epoch = 1;  // 0 is the flags' initial value
-    const cudaError_t err = v->launch(s->long_grid, stream, &e->in, &e->out, op, io, s->long_red, cst, tab,
-                                      s->long_NS, s->long_flags, s->long_epoch, s->long_single);
+    const cudaError_t err = v->launch(s->long_grid, stream, tin, tout, op, lio, s->long_red, cst, tab, s->long_NS,
+                                      s->long_flags, s->long_epoch, s->long_single);
     note_launch(true);
     record_launch(PFSOLVE_KERNEL_LONG, v->R, v->W, v->G, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0, PREC_F64, 0,
                   s->long_grid);

@@ -508,7 +508,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     // outside the maps: zero-filled by the loads, dropped by the stores)
     // moves its rows between global memory and its staged units itself.
     const int64_t Mfull = (io.M / R) * R;
-    const bool tail_thread = PASS == 4 && Mfull < io.M && s_glob == Mfull;
+    // Single pass on rows no tensor map can describe (a stride or offset
+    // that is not a multiple of 16 bytes, e.g. an odd M at stride M): every
+    // thread reads its rows and halo rows from global memory and writes its
+    // results with plain stores; no staging, no TMA.
+    const bool plain = PASS == 4 && io.plain != 0;
+    const bool tail_thread = PASS == 4 && !plain && Mfull < io.M && s_glob == Mfull;
     auto in_row = [&](int64_t y, int64_t row) -> double {  // input row of system y as data (0 outside)
         if (row < 0 || row >= io.M || row < io.iz0 || row >= io.iz1) return 0.0;
         return io.in[io.in_off + y * io.in_stride + row];
@@ -533,12 +538,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         bulk_commit();
     };
 
-    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+    if (!plain && sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
     for (int k = 0; sys < nsys; ++k, sys += per) {
         unsigned char* cur = (k & 1) ? buf1 : buf0;
         unsigned char* nxt = (k & 1) ? buf0 : buf1;
-        const bool more = sys + per < nsys;
-        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+        const bool more = !plain && sys + per < nsys;
+        bool ok = plain || mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
         ok = group_and(g.bar_id, g.nthr, ok);
         if (!ok) {
             if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
@@ -559,13 +564,18 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         // field k of this (system, slice) record
         auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
         double be[R + KL + KU];
+        if (plain) {
+#pragma unroll
+            for (int i = 0; i < R + KL + KU; ++i) be[i] = in_row(sys, s_glob - KL + i);
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
+            if (plain) break;
             const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
             be[KL + 2 * u] = v.x;
             be[KL + 2 * u + 1] = v.y;
         }
-        if constexpr (KL > 0) {
+        if constexpr (KL > 0) if (!plain) {
             double2 pv = make_double2(0.0, 0.0);
             if (t > 0) {
                 pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
@@ -581,7 +591,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             be[KL - 1] = pv.y;
             if constexpr (KL > 1) be[0] = pv.x;
         }
-        if constexpr (KU > 0) {
+        if constexpr (KU > 0) if (!plain) {
             double2 nv = make_double2(0.0, 0.0);
             if (t < T - 1) {
                 nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
@@ -797,6 +807,14 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
         }
         if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
+        if (plain) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const int64_t row = s_glob + j;
+                if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
+            }
+            continue;
+        }
         if (tail_thread) {  // the tail rows (the TMA store drops the tail chunk)
 #pragma unroll
             for (int j = 0; j < R; ++j) {

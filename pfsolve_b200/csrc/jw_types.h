@@ -56,6 +56,7 @@ struct JwIO {
     int64_t M;
     int accumulate;               // output += result
     int alt;                      // ALT mode: system 2y + h is the parity-h rows of row set y
+    int plain;                    // long-system single pass: rows not 16-byte aligned, moved by plain loads/stores
 };
 
 // K consecutive steps in one kernel (numConsecutiveJWIterations = K).

@@ -82,15 +82,35 @@ def test_long_many_systems_and_windows(path):
         assert e <= TOL
 
 
-@pytest.mark.parametrize("path", list(PATHS))
+@pytest.mark.parametrize("path", [3, 2])
 def test_long_rejects_buffers_it_cannot_take(path):
-    """No group-kernel fallback exists beyond 4096 rows: a misaligned launch
-    returns UNSUPPORTED_COMBINATION instead of running."""
+    """The two-pass and cluster forms have no fallback for rows a TMA tensor
+    map cannot describe: a misaligned launch returns UNSUPPORTED_COMBINATION
+    instead of running."""
     rng = np.random.default_rng(3)
     case, bands, rhs = _case(rng, 6144, 3, 2, 13, bitmask=capi.RUNTIME_OFFSETSOLUTION, run_offsetSolution=1)
     with pytest.raises(capi.PfSolveError) as ei:
         _run(case, bands, rhs, kernelPath=path)
     assert ei.value.code == capi.PFSOLVE_ERROR_UNSUPPORTED_COMBINATION
+
+
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (0, 13), (1, 11)])
+@pytest.mark.parametrize("M,kw", [(6144, dict(bitmask=capi.RUNTIME_OFFSETSOLUTION, run_offsetSolution=1)),
+                                  (5000, dict(cfg_outputBufferStride=5003)),
+                                  (9001, dict(bitmask=capi.RUNTIME_INPUTZEROPAD | capi.RUNTIME_OFFSETSOLUTION,
+                                              run_inputZeropad=(7, 8990), run_offsetSolution=3))])
+def test_single_pass_unaligned_rows(ub, jwt, M, kw):
+    """Rows that are not 16-byte aligned (odd offsets and strides): the single
+    pass moves them with plain loads and stores and still matches the oracle;
+    rows outside the systems keep their values."""
+    rng = np.random.default_rng(M + ub + jwt)
+    case, bands, rhs = _case(rng, M, 21, ub, jwt, **kw)
+    x, shape, n = _run(case, bands, rhs)
+    assert shape["streaming"] == 5 and n == 1
+    e, emax = J.rel_err(x, O.jw_step(case, bands, rhs, "q"), case)
+    assert e <= TOL, (e, emax)
+    off = case.offset_solution
+    np.testing.assert_array_equal(x[:off], rhs[:off])
 
 
 @pytest.mark.parametrize("M", [4097, 5001, 12345, 30001])
