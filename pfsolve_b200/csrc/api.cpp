@@ -214,7 +214,7 @@ bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
         const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
         if (!v) return false;
         if (!s->long_single && M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
-        const int b = v->blocks_per_sm();
+        const int b = v->blocks_per_sm(s->long_single);
         if (b < 1) continue;
         const int NS = (int)((M + v->S - 1) / v->S);
         const int64_t res = (int64_t)b * s->num_sms;

@@ -100,16 +100,23 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
     return v;
 }
 
+// Staging buffers per group: two (a system in flight ahead of the one being
+// solved), three in the single pass (its phase B trails phase A by a system).
+template <int PASS>
+struct LgBufs {
+    static constexpr int v = PASS == 4 ? 3 : 2;
+};
+
 // Shared memory: table | scratch | 8 doubles | slice constants (Af, Ab, Psi
 // of up to kLgMaxSlices slices, 4 doubles each) | mbarriers | (align 1024) |
 // buffers | per row of the slice, 16 bytes: the PASS 1 weights (alpha, beta),
 // or in the single pass the carry responses (psi, G).
-template <class C>
+template <class C, int NBUF = 2>
 __host__ __device__ constexpr size_t lg_smem_bytes()
 {
     return C::B::TBL + (size_t)C::G * C::W * kScratchPerWarp * sizeof(double) + 8 * sizeof(double) +
-           (size_t)kLgMaxSlices * 4 * sizeof(double) + (size_t)C::G * 2 * sizeof(uint64_t) + 1024 +
-           (size_t)C::G * 2 * C::B::BUF + (size_t)C::S * 16;
+           (size_t)kLgMaxSlices * 4 * sizeof(double) + (size_t)C::G * NBUF * sizeof(uint64_t) + 1024 +
+           (size_t)C::G * NBUF * C::B::BUF + (size_t)C::S * 16;
 }
 
 // ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
@@ -302,6 +309,74 @@ __global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__
     }
 }
 
+
+// Carries entering slice c of system y in the single pass (called by the 32
+// lanes of one warp once every slice of y has published): X from below, the
+// maps (Af, Bf) of the slices composed upwards; Y from above, the maps
+// (Ab, Bb0 + X Psi) composed downwards.  Lanes hold slices, in rounds of 32.
+// Returns the carries on every lane.
+template <bool FWD, bool BWD>
+__device__ __forceinline__ void lg_compose(int lane, int c, int NS, int64_t nsys, int64_t y,
+                                           const double* __restrict__ red, const double* cst_s, double& Xin,
+                                           double& Yin)
+{
+    double Xr[kLgMaxSlices / 32];
+    double carry = 0.0;
+    Xin = 0.0;
+    Yin = 0.0;
+#pragma unroll
+    for (int r = 0; r < kLgMaxSlices / 32; ++r) {
+        Xr[r] = 0.0;
+        if (32 * r >= NS) break;  // no slices left (NS is uniform)
+        const int cc = 32 * r + lane;
+        const bool v = cc < NS && FWD;
+        double A = v ? cst_s[4 * cc] : 1.0;
+        double B = v ? __ldcg(&red[((size_t)cc * kLgRed + kLgRedBf) * nsys + y]) : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {  // inclusive scan of the maps
+            const double Ap = __shfl_up_sync(FULL, A, d), Bp = __shfl_up_sync(FULL, B, d);
+            if (lane >= d) {
+                B = __fma_rn(A, Bp, B);
+                A = A * Ap;
+            }
+        }
+        const double incl = __fma_rn(A, carry, B);  // value leaving slice cc
+        double ex = __shfl_up_sync(FULL, incl, 1);
+        if (lane == 0) ex = carry;
+        Xr[r] = ex;  // value entering slice cc
+        if (cc == c) Xin = ex;
+        carry = __shfl_sync(FULL, incl, 31);
+    }
+    if constexpr (BWD) {
+        carry = 0.0;
+#pragma unroll
+        for (int r = kLgMaxSlices / 32 - 1; r >= 0; --r) {
+            if (32 * r >= NS) continue;  // identity maps above the top slice
+            const int cc = 32 * r + lane;
+            const bool v = cc < NS;
+            double A = v ? cst_s[4 * cc + 1] : 1.0;
+            double B = v ? __fma_rn(Xr[r], cst_s[4 * cc + 2], __ldcg(&red[((size_t)cc * kLgRed + kLgRedBb) * nsys + y]))
+                         : 0.0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {  // inclusive scan from the top
+                const double Ap = __shfl_down_sync(FULL, A, d), Bp = __shfl_down_sync(FULL, B, d);
+                if (lane + d < 32) {
+                    B = __fma_rn(A, Bp, B);
+                    A = A * Ap;
+                }
+            }
+            const double incl = __fma_rn(A, carry, B);  // value leaving slice cc downwards
+            double ex = __shfl_down_sync(FULL, incl, 1);
+            if (lane == 31) ex = carry;
+            if (cc == c) Yin = ex;
+            carry = __shfl_sync(FULL, incl, 0);
+        }
+    }
+    const int owner = c & 31;  // the lane of slice c holds its carries
+    Xin = __shfl_sync(FULL, Xin, owner);
+    Yin = __shfl_sync(FULL, Yin, owner);
+}
+
 // PASS 3: grid NS (CTA c writes slice c's pivot product into cst, tridiagonal
 // only); PASS 0: grid NS (CTA c builds slice c's table into tab + c * TBL / 8
 // and its constants into cst); PASS 1, 2 and 4 (the single pass, a
@@ -332,18 +407,19 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     double* q4 = scratch + C::G * W * kScratchPerWarp;  // 8 doubles
     double* cst_s = q4 + 8;                              // slice constants (single pass)
     uint64_t* bars_all = reinterpret_cast<uint64_t*>(cst_s + kLgMaxSlices * 4);
-    uint64_t* bars = bars_all + 2 * grp;
-    unsigned char* after = reinterpret_cast<unsigned char*>(bars_all + 2 * C::G);
+    uint64_t* bars = bars_all + LgBufs<PASS>::v * grp;
+    constexpr int NBUF = LgBufs<PASS>::v;
+    unsigned char* after = reinterpret_cast<unsigned char*>(bars_all + NBUF * C::G);
     const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
-    unsigned char* buf0 = after + pad + (size_t)grp * 2 * BC::BUF;
+    unsigned char* buf0 = after + pad + (size_t)grp * NBUF * BC::BUF;
     unsigned char* buf1 = buf0 + BC::BUF;
     // PASS 1 weights: row tt * R + jj at [jj * T + tt] (consecutive threads,
     // consecutive entries)
-    double2* ab_s = reinterpret_cast<double2*>(after + pad + (size_t)C::G * 2 * BC::BUF);
+    double2* ab_s = reinterpret_cast<double2*>(after + pad + (size_t)C::G * NBUF * BC::BUF);
     double2* ab_g = reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)c * C::S;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
 
-    if (threadIdx.x < 2 * C::G) mbar_init(smem_u32(bars_all + threadIdx.x), W);
+    if (threadIdx.x < NBUF * C::G) mbar_init(smem_u32(bars_all + threadIdx.x), W);
     mbar_init_fence();
     double* gtab = tab + (size_t)c * (BC::TBL / sizeof(double));
     if constexpr (PASS == 3) {
@@ -538,49 +614,235 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         bulk_commit();
     };
 
-    if (!plain && sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+
+    if constexpr (PASS == 4) {
+        // Pipelined single pass.  Iteration k prefetches system k+1, runs
+        // phase A of system k (the slice solved with zero carries, its
+        // offsets published, the result x0 staged in place of the input) and
+        // phase B of system k-1 (once every slice of it has published: the
+        // carries composed, their responses added, the result stored).  The
+        // wait for a system's flags therefore trails its publication by a
+        // whole system of work.  Three buffers per group: A's, B's and the
+        // prefetch's, which reuses the buffer stored from two iterations ago.
+        const int64_t sys0 = sys;
+        const int64_t nk = sys0 < nsys ? (nsys - sys0 + per - 1) / per : 0;  // this group's systems
+        auto bufp = [&](int64_t k) -> unsigned char* { return buf0 + (size_t)(k % 3) * BC::BUF; };
+        auto barp = [&](int64_t k) -> uint32_t { return smem_u32(&bars[k % 3]); };
+        auto parity = [&](int64_t k) -> uint32_t { return (uint32_t)((k / 3) & 1); };
+        auto sys_of = [&](int64_t k) -> int64_t { return sys0 + k * per; };
+        auto recf = [&](int64_t y, int f) -> double& { return red[((size_t)c * kLgRed + f) * nsys + y]; };
+        auto stage_off = [&](int u) -> uint32_t { return unit_off(u, t, sw_me); };  // this thread's units
+        constexpr bool COUPLED = BC::FWD || BC::BWD || KL > 0 || KU > 0;
+        const bool tail_slice = !plain && Mfull < io.M && s0 + C::S > Mfull;
+        if (!plain && nk > 0 && lane == 0) issue_load(bufp(0), barp(0), sys_of(0));
+        for (int64_t k = 0; k <= nk; ++k) {
+            const bool prefetch = !plain && k + 1 < nk;
+            if (prefetch && lane == 0) {
+                bulk_wait_read_all();  // the store from this buffer (system k-2) has read it
+                issue_load(bufp(k + 1), barp(k + 1), sys_of(k + 1));
+            }
+            bool ok = true;
+            if (k < nk) {
+                // ---- phase A of system k
+                const int64_t y = sys_of(k);
+                unsigned char* cur = bufp(k);
+                ok = plain || mbar_wait_bounded(barp(k), parity(k));
+                ok = group_and(g.bar_id, g.nthr, ok);
+                if (ok) {
+                    if (tail_slice) {  // the partial last chunk, outside the TMA boxes
+                        if (tail_thread) {
+#pragma unroll
+                            for (int j = 0; j < R; ++j) {
+                                const int64_t row = Mfull + j;
+                                const double v = (row < io.M) ? io.in[io.in_off + y * io.in_stride + row] : 0.0;
+                                reinterpret_cast<double*>(cur + stage_off(j >> 1))[j & 1] = v;
+                            }
+                        }
+                        if (W > 1) group_bar(g.bar_id, g.nthr);
+                        else __syncwarp();
+                    }
+                    double x[R + KL + KU];
+                    if (plain) {
+#pragma unroll
+                        for (int i = 0; i < R + KL + KU; ++i) x[i] = in_row(y, s_glob - KL + i);
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            const double2 v = *reinterpret_cast<const double2*>(cur + stage_off(u));
+                            x[KL + 2 * u] = v.x;
+                            x[KL + 2 * u + 1] = v.y;
+                        }
+                        if constexpr (KL > 0) {
+                            double2 pv;
+                            if (t > 0) pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
+                            else pv = make_double2(in_row(y, s0 - 2), in_row(y, s0 - 1));
+                            x[KL - 1] = pv.y;
+                            if constexpr (KL > 1) x[0] = pv.x;
+                        }
+                        if constexpr (KU > 0) {
+                            double2 nv;
+                            if (t < T - 1) nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
+                            else nv = make_double2(in_row(y, s0 + C::S), in_row(y, s0 + C::S + 1));
+                            x[KL + R] = nv.x;
+                            if constexpr (KU > 1) x[KL + R + 1] = nv.y;
+                        }
+                        if (win_partial) {
+#pragma unroll
+                            for (int i = 0; i < R + KL + KU; ++i) {
+                                const int64_t row = s_glob - KL + i;
+                                if (row < io.iz0 || row >= io.iz1) x[i] = 0.0;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        double2 wc[NB];
+#pragma unroll
+                        for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int j = 2 * u + e;
+                            double acc = (e ? wc[0].y : wc[0].x) * x[j];
+#pragma unroll
+                            for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, x[j + q], acc);
+                            x[j] = acc;
+                        }
+                    }
+                    double Bf = 0.0, Bb0 = 0.0;
+                    if constexpr (BC::FWD || BC::BWD)
+                        lg_solve<C>(g, coef, Af, Ab, x,
+                                    [&](double, double Bt) {
+                                        Bf = Bt;
+                                        return 0.0;
+                                    },
+                                    [&](double, double Bt) {
+                                        Bb0 = Bt;
+                                        return 0.0;
+                                    });
+                    if constexpr (COUPLED) {
+                        if (t == 0) {
+                            recf(y, kLgRedBf) = Bf;
+                            recf(y, kLgRedBb) = Bb0;
+                            st_release_u32(flags + (size_t)c * nsys + y, epoch);
+                        }
+                    }
+                    // every thread has read its rows (the solve's scans are
+                    // group barriers; without a solve, wait): stage x0
+                    if constexpr (!(BC::FWD || BC::BWD)) {
+                        if (W > 1) group_bar(g.bar_id, g.nthr);
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        *reinterpret_cast<double2*>(cur + stage_off(u)) = make_double2(x[2 * u], x[2 * u + 1]);
+                }
+            }
+            if (ok && k >= 1) {
+                // ---- phase B of system k-1
+                const int64_t y = sys_of(k - 1);
+                unsigned char* cur = bufp(k - 1);
+                double Xin = 0.0, Yin = 0.0;
+                if constexpr (COUPLED) {
+                    bool ok2 = true;
+                    if (wg == 0) {
+                        const long long t0 = clock64();
+                        for (int cc = lane; cc < NS && ok2; cc += 32)
+                            while (ld_acquire_u32(flags + (size_t)cc * nsys + y) != epoch) {
+                                if (clock64() - t0 > kLgWaitCycles) {
+                                    ok2 = false;
+                                    break;
+                                }
+                                __nanosleep(32);
+                            }
+                        ok2 = __all_sync(FULL, ok2) != 0;
+                        if (ok2 && (BC::FWD || BC::BWD)) {
+                            lg_compose<BC::FWD, BC::BWD>(lane, c, NS, nsys, y, red, cst_s, Xin, Yin);
+                            if (lane == 0) {
+                                g.warp_area(0)[16] = Xin;
+                                g.warp_area(0)[17] = Yin;
+                            }
+                        }
+                    }
+                    if (W > 1) {
+                        ok2 = group_and(g.bar_id, g.nthr, ok2);
+                        if (wg != 0) {
+                            Xin = g.warp_area(0)[16];
+                            Yin = g.warp_area(0)[17];
+                        }
+                        group_bar(g.bar_id, g.nthr);  // the slot is read before the next system rewrites it
+                    }
+                    ok = ok2;
+                }
+                if (ok) {
+                    double x[R];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const double2 v = *reinterpret_cast<const double2*>(cur + stage_off(u));
+                        x[2 * u] = v.x;
+                        x[2 * u + 1] = v.y;
+                    }
+                    if constexpr (BC::FWD || BC::BWD) {
+#pragma unroll
+                        for (int j = 0; j < R; ++j) {
+                            const double2 pg = ab_s[j * T + t];
+                            x[j] = __fma_rn(Xin, pg.x, __fma_rn(Yin, pg.y, x[j]));
+                        }
+                    }
+                    if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
+                    if (plain || tail_thread) {  // plain stores (the TMA store drops the tail chunk)
+                        const int64_t r0 = plain ? s_glob : Mfull;
+#pragma unroll
+                        for (int j = 0; j < R; ++j) {
+                            const int64_t row = r0 + j;
+                            if (row < io.M && row >= io.oz0 && row < io.oz1)
+                                io.out[io.out_off + y * io.out_stride + row] = x[j];
+                        }
+                    }
+                    if (!plain) {
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            *reinterpret_cast<double2*>(cur + stage_off(u)) = make_double2(x[2 * u], x[2 * u + 1]);
+                        fence_proxy_async();
+                        __syncwarp();
+                        if (lane == 0) issue_store(cur, y);
+                    }
+                }
+            }
+            if (!ok) {
+                if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
+                // the prefetched load completes before the CTA exits
+                if (prefetch && lane == 0) mbar_wait_bounded(barp(k + 1), parity(k + 1));
+                break;
+            }
+        }
+        if (lane == 0) bulk_wait_all();
+        return;
+    }
+
+    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
     for (int k = 0; sys < nsys; ++k, sys += per) {
         unsigned char* cur = (k & 1) ? buf1 : buf0;
         unsigned char* nxt = (k & 1) ? buf0 : buf1;
-        const bool more = !plain && sys + per < nsys;
-        bool ok = plain || mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+        const bool more = sys + per < nsys;
+        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
         ok = group_and(g.bar_id, g.nthr, ok);
         if (!ok) {
             if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
             break;
         }
-        if (PASS == 4 && Mfull < io.M && s0 + C::S > Mfull) {  // the slice holding the tail chunk
-            if (tail_thread) {
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    const int64_t row = Mfull + j;
-                    const double v = (row < io.M) ? io.in[io.in_off + sys * io.in_stride + row] : 0.0;
-                    reinterpret_cast<double*>(cur + unit_off(j >> 1, t, sw_me))[j & 1] = v;
-                }
-            }
-            if (W > 1) group_bar(g.bar_id, g.nthr);
-            else __syncwarp();
-        }
         // field k of this (system, slice) record
         auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
         double be[R + KL + KU];
-        if (plain) {
-#pragma unroll
-            for (int i = 0; i < R + KL + KU; ++i) be[i] = in_row(sys, s_glob - KL + i);
-        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (plain) break;
             const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
             be[KL + 2 * u] = v.x;
             be[KL + 2 * u + 1] = v.y;
         }
-        if constexpr (KL > 0) if (!plain) {
+        if constexpr (KL > 0) {
             double2 pv = make_double2(0.0, 0.0);
             if (t > 0) {
                 pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
-            } else if (PASS == 4) {
-                pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
             } else if (PASS == 1) {
                 pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
                 rec(kLgRedLo) = pv.x;
@@ -591,12 +853,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             be[KL - 1] = pv.y;
             if constexpr (KL > 1) be[0] = pv.x;
         }
-        if constexpr (KU > 0) if (!plain) {
+        if constexpr (KU > 0) {
             double2 nv = make_double2(0.0, 0.0);
             if (t < T - 1) {
                 nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
-            } else if (PASS == 4) {
-                nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
             } else if (PASS == 1) {
                 nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
                 rec(kLgRedHi) = nv.x;
@@ -634,7 +894,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         // pass 2, stored from: once this warp's stores have read it, it takes
         // the next system
         if (more && lane == 0) {
-            if (PASS == 2 || PASS == 4) bulk_wait_read_all();
+            if (PASS == 2) bulk_wait_read_all();
             issue_load(nxt, (k & 1) ? bar0 : bar1, sys + per);
         }
         if constexpr (PASS == 1) {
@@ -674,154 +934,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 }
             }
             continue;
-        } else if constexpr (PASS == 4) {
-            // the slice with zero carries; its offsets Bf (forward total) and
-            // Bb0 (backward total)
-            double Bf = 0.0, Bb0 = 0.0;
-            if constexpr (BC::FWD || BC::BWD)
-                lg_solve<C>(g, coef, Af, Ab, x,
-                            [&](double, double Bt) {
-                                Bf = Bt;
-                                return 0.0;
-                            },
-                            [&](double, double Bt) {
-                                Bb0 = Bt;
-                                return 0.0;
-                            });
-            // Slices couple through the carries (a solve) or through the
-            // matvec halo rows read in place (a matvec alone): publish, then
-            // wait for every slice of this system (bounded).
-            if constexpr (BC::FWD || BC::BWD || KL > 0 || KU > 0) {
-                if (t == 0) {
-                    rec(kLgRedBf) = Bf;
-                    rec(kLgRedBb) = Bb0;
-                    st_release_u32(flags + (size_t)c * nsys + sys, epoch);
-                }
-                bool ok2 = true;
-                double Xin = 0.0, Yin = 0.0;
-                if (wg == 0) {
-                    const long long t0 = clock64();
-                    for (int cc = lane; cc < NS && ok2; cc += 32)
-                        while (ld_acquire_u32(flags + (size_t)cc * nsys + sys) != epoch) {
-                            if (clock64() - t0 > kLgWaitCycles) {
-                                ok2 = false;
-                                break;
-                            }
-                            __nanosleep(32);
-                        }
-                    ok2 = __all_sync(FULL, ok2) != 0;
-                    if (ok2 && (BC::FWD || BC::BWD)) {
-                        // carries entering slice c: X from below (affine maps
-                        // (Af, Bf) composed upwards), Y from above (maps
-                        // (Ab, Bb0 + X Psi) composed downwards); lanes hold
-                        // slices, in rounds of 32
-                        double Xr[kLgMaxSlices / 32];
-                        double carry = 0.0;
-#pragma unroll
-                        for (int r = 0; r < kLgMaxSlices / 32; ++r) {
-                            if (32 * r >= NS) break;  // no slices left (NS is uniform)
-                            const int cc = 32 * r + lane;
-                            const bool v = cc < NS;
-                            double A = v ? cst_s[4 * cc] : 1.0;
-                            double B = v ? __ldcg(&red[((size_t)cc * kLgRed + kLgRedBf) * nsys + sys]) : 0.0;
-                            if (!BC::FWD) {
-                                A = 1.0;
-                                B = 0.0;
-                            }
-#pragma unroll
-                            for (int d = 1; d < 32; d <<= 1) {  // inclusive scan of the maps
-                                const double Ap = __shfl_up_sync(FULL, A, d), Bp = __shfl_up_sync(FULL, B, d);
-                                if (lane >= d) {
-                                    B = __fma_rn(A, Bp, B);
-                                    A = A * Ap;
-                                }
-                            }
-                            const double incl = __fma_rn(A, carry, B);  // value leaving slice cc
-                            double ex = __shfl_up_sync(FULL, incl, 1);
-                            if (lane == 0) ex = carry;
-                            Xr[r] = ex;  // value entering slice cc
-                            if (cc == c) Xin = ex;
-                            carry = __shfl_sync(FULL, incl, 31);
-                        }
-                        if constexpr (BC::BWD) {
-                            carry = 0.0;
-#pragma unroll
-                            for (int r = kLgMaxSlices / 32 - 1; r >= 0; --r) {
-                                if (32 * r >= NS) continue;  // identity maps above the top slice
-                                const int cc = 32 * r + lane;
-                                const bool v = cc < NS;
-                                double A = v ? cst_s[4 * cc + 1] : 1.0;
-                                double B = v ? __fma_rn(Xr[r], cst_s[4 * cc + 2],
-                                                        __ldcg(&red[((size_t)cc * kLgRed + kLgRedBb) * nsys + sys]))
-                                             : 0.0;
-#pragma unroll
-                                for (int d = 1; d < 32; d <<= 1) {  // inclusive scan from the top
-                                    const double Ap = __shfl_down_sync(FULL, A, d), Bp = __shfl_down_sync(FULL, B, d);
-                                    if (lane + d < 32) {
-                                        B = __fma_rn(A, Bp, B);
-                                        A = A * Ap;
-                                    }
-                                }
-                                const double incl = __fma_rn(A, carry, B);  // value leaving slice cc downwards
-                                double ex = __shfl_down_sync(FULL, incl, 1);
-                                if (lane == 31) ex = carry;
-                                if (cc == c) Yin = ex;
-                                carry = __shfl_sync(FULL, incl, 0);
-                            }
-                        }
-                        // the lane of slice c holds its carries: to the group
-                        const int owner = c & 31;
-                        Xin = __shfl_sync(FULL, Xin, owner);
-                        Yin = __shfl_sync(FULL, Yin, owner);
-                        if (lane == 0) {
-                            g.warp_area(0)[16] = Xin;
-                            g.warp_area(0)[17] = Yin;
-                        }
-                    }
-                }
-                if (W > 1) {
-                    ok2 = group_and(g.bar_id, g.nthr, ok2);
-                    if (wg != 0) {
-                        Xin = g.warp_area(0)[16];
-                        Yin = g.warp_area(0)[17];
-                    }
-                    group_bar(g.bar_id, g.nthr);  // slot read by all before the next system rewrites it
-                }
-                if (!ok2) {
-                    if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
-                    // the next system's load, if issued, completes before the CTA exits
-                    if (more && lane == 0) mbar_wait_bounded((k & 1) ? bar0 : bar1, (uint32_t)(((k + 1) >> 1) & 1));
-                    break;
-                }
-                if constexpr (BC::FWD || BC::BWD) {
-#pragma unroll
-                    for (int j = 0; j < R; ++j) {
-                        const double2 pg = ab_s[j * T + t];
-                        x[j] = __fma_rn(Xin, pg.x, __fma_rn(Yin, pg.y, x[j]));
-                    }
-                }
-            }
         } else {
             // carries of this system's slice, from the carry kernel
             const double Xc = BC::FWD ? rec(kLgRedX) : 0.0, Yc = BC::BWD ? rec(kLgRedY) : 0.0;
             lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
         }
         if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
-        if (plain) {
-#pragma unroll
-            for (int j = 0; j < R; ++j) {
-                const int64_t row = s_glob + j;
-                if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
-            }
-            continue;
-        }
-        if (tail_thread) {  // the tail rows (the TMA store drops the tail chunk)
-#pragma unroll
-            for (int j = 0; j < R; ++j) {
-                const int64_t row = Mfull + j;
-                if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
-            }
-        }
         __syncwarp();
 #pragma unroll
         for (int u = 0; u < U; ++u) {

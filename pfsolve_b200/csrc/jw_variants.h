@@ -114,10 +114,10 @@ struct LongVariant {
     cudaError_t (*launch)(int grid, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
                           const JwOperator& op, const JwIO& io, double* red, double* cst, double* tab, int NS,
                           unsigned* flags, unsigned epoch, bool single);
-    int (*blocks_per_sm)();  // resident CTAs per SM (0: does not fit)
+    int (*blocks_per_sm)(bool single);  // resident CTAs per SM of the single pass or the two (0: does not fit)
 };
 constexpr int kLongMaxSlices = 64;  // slices per system of the single pass
-constexpr int kLongShapes = 3;  // compiled shapes per operator kind, in order of preference
+constexpr int kLongShapes = 4;  // compiled shapes per operator kind, in order of preference
 const LongVariant* find_long_variant(int shape, int KL, int KU, int SV);
 unsigned long_status_fetch_clear();
 unsigned cluster_status_fetch_clear();

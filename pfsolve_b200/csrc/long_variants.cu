@@ -30,7 +30,7 @@ static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in
         unsigned ep = epoch;
         void* args[] = {&tin, &tout, &o, &i, &red, &cst, &tab, &ns, &flags, &ep};
         const cudaError_t e = cudaLaunchCooperativeKernel((const void*)&jw_long_kernel<C, 4>, dim3((unsigned)grid),
-                                                          dim3(C::NT), args, smem, st);
+                                                          dim3(C::NT), args, lg_smem_bytes<C, 3>(), st);
         if (e != cudaSuccess) return e;
         return cudaPeekAtLastError();
     }
@@ -42,28 +42,37 @@ static cudaError_t lg_launch_fn(int grid, cudaStream_t st, const CUtensorMap* in
     return cudaPeekAtLastError();
 }
 
-// resident CTAs per SM of the two passes (0: does not fit)
+// resident CTAs per SM of the single pass (single) or of the two passes
+// (0: does not fit)
 template <class C>
-static int lg_blocks_per_sm()
+static int lg_blocks_per_sm(bool single)
 {
-    const size_t smem = lg_smem_bytes<C>();
-    int b1 = 0, b2 = 0;
     const void* f3 = (const void*)&jw_long_kernel<C, 3>;
-    if (!allow_max_smem(f3)) return 0;
     const void* f0 = (const void*)&jw_long_kernel<C, 0>;
+    if (!allow_max_smem(f3) || !allow_max_smem(f0)) return 0;
+    int b1 = 0, b2 = 0;
+    if (single) {
+        const void* f4 = (const void*)&jw_long_kernel<C, 4>;
+        int maxopt = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (lg_smem_bytes<C, 3>() > (size_t)maxopt || !allow_max_smem(f4)) return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, f4, C::NT, lg_smem_bytes<C, 3>()) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return b1;
+    }
+    const size_t smem = lg_smem_bytes<C>();
     const void* f1 = (const void*)&jw_long_kernel<C, 1>;
     const void* f2 = (const void*)&jw_long_kernel<C, 2>;
-    const void* f4 = (const void*)&jw_long_kernel<C, 4>;
-    if (!allow_max_smem(f0) || !allow_max_smem(f1) || !allow_max_smem(f2) || !allow_max_smem(f4)) return 0;
-    int b4 = 0;
+    if (!allow_max_smem(f1) || !allow_max_smem(f2)) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, f1, C::NT, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, f4, C::NT, smem) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, f2, C::NT, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    const int b = b1 < b2 ? b1 : b2;
-    return b < b4 ? b : b4;
+    return b1 < b2 ? b1 : b2;
 }
 
 #define PFB_LG(R, W, G, KL, KU, SV)                                                                    \
@@ -71,9 +80,12 @@ static int lg_blocks_per_sm()
                 LgCfg<R, W, G, KL, KU, SV>::B::IBO, LgCfg<R, W, G, KL, KU, SV>::B::TBL,                    \
                 &lg_launch_fn<LgCfg<R, W, G, KL, KU, SV>>, &lg_blocks_per_sm<LgCfg<R, W, G, KL, KU, SV>>}
 // (rows per thread, warps per slice, systems in flight per CTA): slices of
-// 1024 rows with 16 rows per thread (the scans' cost spread over more rows),
-// then 1024 and 512 rows with 8 rows per thread
-#define PFB_LGK(KL, KU, SV) PFB_LG(16, 2, 8, KL, KU, SV), PFB_LG(8, 4, 4, KL, KU, SV), PFB_LG(16, 4, 2, KL, KU, SV)
+// 1024 rows with 16 rows per thread (the scans' cost spread over more rows;
+// 8 groups for two passes, 7 for the single pass's three buffers a group),
+// then 1024 and 2048 rows with 8 and 16 rows per thread
+#define PFB_LGK(KL, KU, SV)                                                                                 \
+    PFB_LG(16, 2, 8, KL, KU, SV), PFB_LG(16, 2, 7, KL, KU, SV), PFB_LG(8, 4, 4, KL, KU, SV),                 \
+        PFB_LG(16, 4, 2, KL, KU, SV)
 
 static const LongVariant kLongVariants[] = {
     PFB_LGK(0, 0, SV_TRI),   PFB_LGK(0, 1, SV_LOWER), PFB_LGK(0, 1, SV_NONE), PFB_LGK(0, 0, SV_LOWER),
