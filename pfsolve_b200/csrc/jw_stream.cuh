@@ -359,8 +359,47 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     unsigned char* buf1 = buf0 + C::BUF;
     const uint32_t bar0 = smem_u32(&bars[2 * grp]), bar1 = smem_u32(&bars[2 * grp + 1]);
 
+    // Shared-memory byte offset of swizzle row h of plane p of chunk c, in the
+    // warp-major staging layout (the boxes of warp c/32, then the next
+    // warp's); unit uu (< IB) of that row is at + ((uu ^ swz(c)) << 4).
+    constexpr int ROWB = C::ROWB, ROWBO = C::ROWBO;
+    auto in_row = [&](int p, int h, int c) -> size_t {
+        return ((size_t)(((c >> 5) * C::NPIN + p) * H + h) * 32 + (c & 31)) * ROWB;
+    };
+    auto out_row = [&](int p, int h, int c) -> size_t {
+        return ((size_t)(((c >> 5) * C::NPOUT + p) * HO + h) * 32 + (c & 31)) * ROWBO;
+    };
+    const int64_t nsys = io.nsys;
+    const int64_t step = (int64_t)gridDim.x * G;
+    int64_t sys = (int64_t)blockIdx.x * G + grp;
+
+    // lane 0 of each warp: load / store this warp's 32 chunks of one system
+    // (TMA x coordinates in storage elements: 16 / ES per 16-byte unit)
+    auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
+        mbar_arrive_expect_tx(bar, (uint32_t)(C::NPIN * H * 32 * ROWB));
+#pragma unroll
+        for (int p = 0; p < C::NPIN; ++p)
+#pragma unroll
+            for (int h = 0; h < H; ++h)
+                tma_load_3d(smem_u32(b + in_row(p, h, 32 * wg)), &tm_in, h * IB * (16 / ES), 32 * wg,
+                            (int)(C::CPLX ? 2 * y + p : y), bar);
+    };
+    auto issue_store = [&](unsigned char* b, int64_t y) {
+#pragma unroll
+        for (int p = 0; p < C::NPOUT; ++p)
+#pragma unroll
+            for (int h = 0; h < HO; ++h)
+                tma_store_3d(&tm_out, h * IBO * (16 / ES), 32 * wg, (int)(C::NPOUT == 2 ? 2 * y + p : y),
+                             smem_u32(b + out_row(p, h, 32 * wg)));
+        bulk_commit();
+    };
+
     if ((int)threadIdx.x < 2 * G) mbar_init(smem_u32(&bars[threadIdx.x]), W);
     mbar_init_fence();
+    __syncthreads();  // the barriers are initialised before any copy can complete on them
+    // The first system's copy does not depend on the coefficient table: it is
+    // in flight while the prologue reads the bands.
+    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
     st_prologue<C>(op, table, scratch_all);
     __syncthreads();
 
@@ -471,16 +510,6 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     if constexpr (kPre && C::FWD && C::MIXED) mf32 = scan_multipliers<float, true>(g, Af32);
     if constexpr (kPre && C::BWD && C::MIXED) mb32 = scan_multipliers<float, false>(g, Ab32);
 
-    // Shared-memory byte offset of swizzle row h of plane p of chunk c, in the
-    // warp-major staging layout (the boxes of warp c/32, then the next
-    // warp's); unit uu (< IB) of that row is at + ((uu ^ swz(c)) << 4).
-    constexpr int ROWB = C::ROWB, ROWBO = C::ROWBO;
-    auto in_row = [&](int p, int h, int c) -> size_t {
-        return ((size_t)(((c >> 5) * C::NPIN + p) * H + h) * 32 + (c & 31)) * ROWB;
-    };
-    auto out_row = [&](int p, int h, int c) -> size_t {
-        return ((size_t)(((c >> 5) * C::NPOUT + p) * HO + h) * 32 + (c & 31)) * ROWBO;
-    };
     const int sw_me = swz_row<C::SWB>(t), sw_prev = swz_row<C::SWB>(t - 1), sw_next = swz_row<C::SWB>(t + 1);
     const int swo_me = swz_row<C::SWBO>(t);
     const bool has_prev = t > 0, has_next = t < T - 1;
@@ -508,32 +537,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     };
 
     const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
-    const int64_t nsys = io.nsys;
-    const int64_t step = (int64_t)gridDim.x * G;
-    int64_t sys = (int64_t)blockIdx.x * G + grp;
 
-    // lane 0 of each warp: load / store this warp's 32 chunks of one system
-    // (TMA x coordinates in storage elements: 16 / ES per 16-byte unit)
-    auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
-        mbar_arrive_expect_tx(bar, (uint32_t)(C::NPIN * H * 32 * ROWB));
-#pragma unroll
-        for (int p = 0; p < C::NPIN; ++p)
-#pragma unroll
-            for (int h = 0; h < H; ++h)
-                tma_load_3d(smem_u32(b + in_row(p, h, 32 * wg)), &tm_in, h * IB * (16 / ES), 32 * wg,
-                            (int)(C::CPLX ? 2 * y + p : y), bar);
-    };
-    auto issue_store = [&](unsigned char* b, int64_t y) {
-#pragma unroll
-        for (int p = 0; p < C::NPOUT; ++p)
-#pragma unroll
-            for (int h = 0; h < HO; ++h)
-                tma_store_3d(&tm_out, h * IBO * (16 / ES), 32 * wg, (int)(C::NPOUT == 2 ? 2 * y + p : y),
-                             smem_u32(b + out_row(p, h, 32 * wg)));
-        bulk_commit();
-    };
-
-    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
     for (int k = 0; sys < nsys; ++k, sys += step) {
         unsigned char* cur = (k & 1) ? buf1 : buf0;
         unsigned char* nxt = (k & 1) ? buf0 : buf1;
