@@ -440,6 +440,9 @@ PFSOLVE_API void PfSolveBatchDestroy(PfSolveBatch* batch);
  * cudaMemcpyAsync from the library's fixed host arrays, which are ordinary
  * (pageable) memory: the call returns once the driver has staged them, so it
  * may block the host for that copy (never for the device's queued work).
+ * The next call rewrites those host arrays, so a call on a stream that is
+ * being captured returns PFSOLVE_ERROR_INVALID_ARGUMENT and enqueues nothing;
+ * do not issue it under stream capture.
  * The caller's current device is the same on return as on entry.  Results
  * equal PfSolveBatchAppend's for the same descriptor, rows per thread and
  * systems per item. */

@@ -107,11 +107,12 @@ struct StCfg {
     // output bytes are then the same range.
     static constexpr int ROWB = IB * 16, ROWBO = IBO * 16;
     static_assert(NPIN * H * ROWB == NPOUT * HO * ROWBO, "in-place staging");
-    // Registers held by the right-hand-side data (mixed: x, g and the FP32
-    // solve vector); the launch bound leaves the compiler room for them:
+    // Registers held by the right-hand-side data (mixed: x and the FP32
+    // correction; g waits in shared memory); the launch bound leaves the compiler room for them:
     // 512 threads cap at 128 registers, 384 at 170, 256 at 255.  Complex
     // variants stay at 256 (measured faster than 384 on the config 2 chain).
-    static constexpr int kDataRegs = (R + KLP + KUP) * (CPLX ? 2 : 1) * (F32 ? 1 : 2) * (MIXED ? 3 : 1);
+    static constexpr int kDataRegs =
+        (R + KLP + KUP) * (CPLX ? 2 : 1) * (F32 ? 1 : 2) + (MIXED ? R * (CPLX ? 2 : 1) : 0);
     static constexpr int kMaxThreads =
         (kDataRegs >= 96 || (CPLX && kDataRegs >= 64)) ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
@@ -419,19 +420,21 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
     auto coef4 = [&](int p, int u) -> float4 { return reinterpret_cast<const float4*>(tb)[(p * U + u) * C::TP]; };
     // Mixed precision, real systems of up to 16 rows per thread: the FP32 solve
-    // factors stay in registers for the whole kernel (every refinement sweep
-    // reuses them).
+    // factors {m, -l} stay in registers for the whole kernel (every refinement
+    // sweep reuses them); {-h} too for up to 8 rows per thread (at 16, the
+    // 128-register bound of a 512-thread CTA leaves no room for them).
     constexpr bool kHoist = C::MIXED && !C::CPLX && U <= 8;
+    constexpr bool kHoist2 = kHoist && U <= 4;
     float4 hf1[kHoist ? U : 1];
-    float2 hf2[kHoist ? U : 1];
+    float2 hf2[kHoist2 ? U : 1];
     if constexpr (kHoist) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             hf1[u] = coef4(C::P_F1, u);
-            if constexpr (C::BWD) {
+            if constexpr (kHoist2 && C::BWD) {
                 const float4 f = coef4(C::P_F2, u);
                 hf2[u] = make_float2(f.x, f.y);
-            } else {
+            } else if constexpr (kHoist2) {
                 hf2[u] = make_float2(0.0f, 0.0f);
             }
         }
@@ -441,7 +444,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         else return coef4(C::P_F1, u);
     };
     auto F2 = [&](int u) -> float2 {
-        if constexpr (kHoist) {
+        if constexpr (kHoist2) {
             return hf2[u];
         } else {
             const float4 f = coef4(C::P_F2, u);
@@ -498,11 +501,12 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         }
     }
 
-    // Complex and mixed variants of up to 16 rows per thread under a
-    // 256-thread launch bound: each lane's scan multipliers formed once (all
-    // systems share them).  The others, with fewer registers to spare, keep
-    // the plain scan.
-    constexpr bool kPre = (C::CPLX || C::MIXED) && !C::ALT && R <= 16 && C::kMaxThreads <= 256;
+    // Complex variants of up to 16 rows per thread under a 256-thread launch
+    // bound, and mixed variants of up to 8: each lane's scan multipliers
+    // formed once (all systems share them).  The others, with fewer registers
+    // to spare, keep the plain scan.
+    constexpr bool kPre =
+        !C::ALT && ((C::CPLX && R <= 16 && C::kMaxThreads <= 256) || (C::MIXED && !C::CPLX && R <= 8));
     ScanMul<CT> mf{}, mb{};
     ScanMul<float> mf32{}, mb32{};
     if constexpr (kPre && C::FWD && !C::MIXED) mf = scan_multipliers<CT, true>(g, Af);
@@ -627,14 +631,27 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
         if constexpr (C::MIXED) {
             // x = M^{-1} g: FP32 solves of the residual, accumulated in FP64
-            // (one initial solve, refine_sweeps - 1 refinements).
+            // (one initial solve, refine_sweeps - 1 refinements).  g = V A b
+            // stays in shared memory in place of b (this thread's own rows),
+            // so the registers hold only x and the FP32 correction.
             using VF = typename C::VF;
             using OF = VOps<VF>;
-            V gv[R];
+            if constexpr (KL + KU > 0) {  // the neighbours' halo reads of b come first
+                if (W == 1) __syncwarp();
+                else group_bar(g.bar_id, g.nthr);
+            }
 #pragma unroll
-            for (int j = 0; j < R; ++j) {
-                gv[j] = x[j];
-                x[j] = O::zero();
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int p = 0; p < C::NPIN; ++p) {
+                    MS v[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        if constexpr (C::CPLX) v[e] = p ? x[2 * u + e].y : x[2 * u + e].x;
+                        else v[e] = x[2 * u + e];
+                    }
+                    put_unit(cur + in_row(p, u / IB, t) + (((u % IB) ^ sw_me) << 4), v);
+                }
             }
             for (int it = 0; it < op.refine_sweeps; ++it) {
                 VF d[R];
@@ -642,8 +659,8 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 #pragma unroll
                     for (int u = 0; u < U; ++u) {
                         const float4 f = F1(u);
-                        d[2 * u] = OF::mul(f.x, to_f32(gv[2 * u]));
-                        d[2 * u + 1] = OF::mul(f.y, to_f32(gv[2 * u + 1]));
+                        d[2 * u] = OF::mul(f.x, to_f32(x[2 * u]));
+                        d[2 * u + 1] = OF::mul(f.y, to_f32(x[2 * u + 1]));
                     }
                 } else {
                     // r = g - M x in FP64 (M: unit diagonal, sub al, super cu)
@@ -655,13 +672,15 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                         double2 al = make_double2(0.0, 0.0), cu = make_double2(0.0, 0.0);
                         if constexpr (C::FWD) al = coef(C::P_AL, u);
                         if constexpr (C::BWD) cu = coef(C::P_CU, u);
+                        V gu[2];
+                        rows_of(u, t, sw_me, gu);
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
                             const int j = 2 * u + e;
                             V mx = x[j];
                             if constexpr (C::FWD) mx = O::fma(e ? al.y : al.x, j > 0 ? x[j - 1] : prev, mx);
                             if constexpr (C::BWD) mx = O::fma(e ? cu.y : cu.x, j < R - 1 ? x[j + 1] : next, mx);
-                            d[j] = OF::mul(e ? f.y : f.x, to_f32(O::fma(-1.0, mx, gv[j])));
+                            d[j] = OF::mul(e ? f.y : f.x, to_f32(O::fma(-1.0, mx, gu[e])));
                         }
                     }
                 }
@@ -705,8 +724,13 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                         d[2 * u] = OF::fma(p, q, d[2 * u]);
                     }
                 }
+                if (it == 0) {
 #pragma unroll
-                for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
+                    for (int j = 0; j < R; ++j) x[j] = to_f64(d[j]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < R; ++j) x[j] = O::add(x[j], to_f64(d[j]));
+                }
             }
         }
         if constexpr (C::FWD && !C::MIXED && C::ALT) {

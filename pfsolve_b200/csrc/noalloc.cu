@@ -10,7 +10,9 @@
 // calls share the one scratch array, so calls whose work overlaps in time
 // (other streams, other host threads) race on it.  The host staging arrays
 // are pageable: cudaMemcpyAsync stages them before it returns, so the next
-// call may rewrite them at once.  The caller's current device is restored on
+// call may rewrite them at once.  Because the next call rewrites them, a call
+// on a stream that is being captured is refused (PFSOLVE_ERROR_INVALID_ARGUMENT)
+// before it enqueues anything.  The caller's current device is restored on
 // every return.
 #include <cuda_runtime.h>
 
@@ -176,6 +178,19 @@ extern "C" PfSolveResult PfSolveBatchAppendNoAlloc(CUdevice device, const PfSolv
 
     DeviceGuard keep_device;
     if (cudaSetDevice(device) != cudaSuccess) return PFSOLVE_ERROR_INVALID_DEVICE;
+    // The descriptors are copied from g_entries / g_items, which the next call
+    // rewrites: a captured copy would replay whatever the latest call left
+    // there.  A stream under capture (or one whose capture state cannot be
+    // read, e.g. the legacy stream while another stream captures globally)
+    // is refused before anything is enqueued.
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            return PFSOLVE_ERROR_INVALID_ARGUMENT;
+        }
+        if (cs != cudaStreamCaptureStatusNone) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    }
     int num_sms = 0;
     if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return PFSOLVE_ERROR_FAILED_TO_GET_ATTRIBUTE;

@@ -153,3 +153,51 @@ def test_noalloc_capacity_and_argument_errors():
     d1 = capi.PfSolveBatchDesc(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=307, systemsPerItem=1)
     assert lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(d1), big, 1, None) == capi.PFSOLVE_ERROR_CAPACITY
     assert lib.PfSolveBatchAppendNoAlloc(0, None, big, 1, None) == capi.PFSOLVE_ERROR_INVALID_ARGUMENT
+
+
+def test_noalloc_refused_under_stream_capture():
+    """The descriptors are copied from host arrays that the next call
+    rewrites, so a call on a stream under capture must enqueue nothing and
+    return PFSOLVE_ERROR_INVALID_ARGUMENT; the same call outside the capture
+    still runs."""
+    import torch
+
+    lib = capi.load()
+    step = WL.config4(lmax=15, Nmax=64, seed=11)
+    inp = torch.from_numpy(step.rhs).cuda()
+    out = torch.zeros_like(inp)
+    keep, ents = [], []
+    for k, (l, N, ns) in enumerate(zip(step.ls, step.Ns, step.nsys)):
+        tj = torch.from_numpy(step.jw_bands[k]).cuda()
+        ta = torch.from_numpy(step.dgbmv[k]).cuda()
+        keep += [tj, ta]
+        off = 8 * int(step.rhs_offsets[k])
+        ents.append(dict(M=int(N), nsys=int(ns), bands=tj.data_ptr(), dgbmvBands=ta.data_ptr(), lshift=int(l),
+                         scaleS=step.scale_s, input=inp.data_ptr() + off, output=out.data_ptr() + off))
+    desc = capi.PfSolveBatchDesc(upperBanded=0, jw_type=13, LDA=3, KU=1, KL=1, block=307)
+    arr = _entry_array(ents)
+    s = torch.cuda.Stream()
+    # set-up (the array's address) outside any capture
+    assert lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(desc), arr, len(ents),
+                                         ctypes.c_void_p(s.cuda_stream)) == capi.PFSOLVE_SUCCESS
+    s.synchronize()
+    g = torch.cuda.CUDAGraph()
+    marker = torch.zeros(1, device="cuda")
+    n0 = lib.PfSolveLaunchCount()
+    with torch.cuda.graph(g, stream=s):
+        marker.add_(1.0)
+        rc = lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(desc), arr, len(ents), ctypes.c_void_p(s.cuda_stream))
+    assert rc == capi.PFSOLVE_ERROR_INVALID_ARGUMENT, rc
+    assert lib.PfSolveLaunchCount() == n0
+    del g
+    out.zero_()
+    torch.cuda.synchronize()
+    assert lib.PfSolveBatchAppendNoAlloc(0, ctypes.byref(desc), arr, len(ents),
+                                         ctypes.c_void_p(s.cuda_stream)) == capi.PFSOLVE_SUCCESS
+    s.synchronize()
+    k = len(step.ls) - 1
+    N, ns = int(step.Ns[k]), int(step.nsys[k])
+    off = int(step.rhs_offsets[k])
+    o = _oracle_degree(step, k).reshape(ns, 2 * N)
+    got = out.cpu().numpy()[off:off + 2 * N * ns].reshape(ns, 2 * N)
+    assert (np.linalg.norm(got - o, axis=1) / np.linalg.norm(o, axis=1)).max() <= TOL
