@@ -473,8 +473,9 @@ def extras_arm(args):
     torch.cuda.empty_cache()
     # long systems, beyond one CTA group (the reference's multi-upload range)
     out["long_t13_N16384_B8192"] = long_measure(16384, 8192)
-    out["long_t13_N16384_B8192_two_pass"] = long_measure(16384, 8192, path=3)
+    out["long_t13_N16384_B8192_single_pass"] = long_measure(16384, 8192, path=4)
     out["long_t13_N65536_B2048"] = long_measure(65536, 2048)
+    out["long_t13_N20000_B6553"] = long_measure(20000, 6553)
     out["alt_t113_N1024_B131072"] = alt_measure(1024, 131072)
     out["alt_t113_N1024_B131072_group"] = alt_measure(1024, 131072, path=1)
     torch.cuda.empty_cache()
@@ -493,7 +494,10 @@ def config1_measure(steps=200, warmup=20):
     fused ahead of the upper-bidiagonal JW step, jw_type 13, upperBanded 0),
     and the JW step alone as the reference times it: per-step latency of
     back-to-back launches on one stream (CUDA events over `steps` launches
-    after `warmup`; 2.1 MB of right-hand sides, L2-resident)."""
+    after `warmup`; 2.1 MB of right-hand sides, L2-resident).  Each is timed
+    twice: called from Python through the C ABI one launch at a time (host
+    overhead included), and as `steps` launches captured once in a CUDA graph
+    and replayed (device time per launch)."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -503,27 +507,48 @@ def config1_measure(steps=200, warmup=20):
     tA = torch.from_numpy(wl.dgbmv).cuda()
     tb = torch.from_numpy(wl.jw_bands).cuda()
     tr = torch.from_numpy(wl.rhs.copy()).cuda()
-    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1)
+    st = torch.cuda.Stream()
+    dg = App(buffer=tA, outputBuffer=tr, M_size=M, size=(M, B), LDA=3, KU=1, KL=1, doublePrecision=1,
+             stream=st.cuda_stream)
     jw = App(buffer=tb, outputBuffer=tr, M_size=M, size=(M, B), upperBanded=0, jw_type=13, doublePrecision=1,
-             scaleC=1.0)
+             scaleC=1.0, stream=st.cuda_stream)
     lps = [dg.launch_params(), jw.launch_params()]
     res = {}
     for name, fn in (("fused_chain", lambda: append_chain([dg, jw], lps)), ("jw_only", lambda: jw.append(lps[1]))):
-        for _ in range(warmup):
-            fn()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(steps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            for _ in range(warmup):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st.synchronize()
+            e0.record(st)
+            for _ in range(steps):
+                fn()
+            e1.record(st)
+        st.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        res[name] = {"ms": ms, "rhs_per_s": B / (ms * 1e-3), "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9}
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            for _ in range(steps):
+                fn()
+        with torch.cuda.stream(st):  # a graph replays on the current stream
+            for _ in range(3):
+                g.replay()
+            st.synchronize()
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record(st)
+            for _ in range(5):
+                g.replay()
+            g1.record(st)
+        st.synchronize()
+        gms = g0.elapsed_time(g1) / (5 * steps)
+        del g
+        res[name] = {"ms": ms, "rhs_per_s": B / (ms * 1e-3), "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9,
+                     "graph_ms": gms, "graph_rhs_per_s": B / (gms * 1e-3)}
     dg.close()
     jw.close()
-    res["reference_jw_ms"] = 0.0042  # its own JW kernel on the same pool, same method (20 launches)
-    res["note"] = "L2-resident (2.1 MB): latency of back-to-back launches, not an HBM roofline"
+    res["reference_jw_ms"] = 0.0042  # its own JW kernel on the same pool: 20 launches from C++, no graph
+    res["note"] = ("L2-resident (2.1 MB): latency of back-to-back launches, not an HBM roofline; ms from Python "
+                   "calls (host overhead included), graph_ms from a replayed CUDA graph of the same launches")
     return res
 
 
@@ -612,9 +637,9 @@ def config3_profile(args):
 
 def long_measure(M, B, steps=10, warmup=3, path=0):
     """A long tridiagonal system (config 3's coefficients at N = M rows), B
-    real right-hand sides in place, FP64: the single-pass long-system kernel
-    (path 3: the two-pass form; path 2: the cluster kernel).  Algorithmic
-    bytes: M rows read and written per system."""
+    real right-hand sides in place, FP64: the plan's default long-system
+    kernel (path 3: two passes only; 4: the single pass only; 2: the cluster
+    kernel).  Algorithmic bytes: M rows read and written per system."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -814,9 +839,10 @@ def main():
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
-    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="kernelPath: 0 streaming kernel where possible (long systems: single pass), "
-                         "1 group kernel only, 2 long systems on the cluster kernel, 3 long systems in two passes")
+    ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="kernelPath: 0 streaming kernel where possible (long systems: two passes where N is a "
+                         "multiple of 8, else the single pass), 1 group kernel only, 2 long systems on the cluster "
+                         "kernel, 3 long systems in two passes only, 4 long systems in the single pass only")
     args = ap.parse_args()
     if args.profile:
         args.no_cpu = True

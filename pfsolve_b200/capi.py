@@ -73,6 +73,7 @@ class PfSolveConfiguration(ctypes.Structure):
         ("disableSetLocale", u64), ("useUint64", u64),
         ("numConsecutiveJWIterations", c_int), ("useMultipleInputBuffers", c_int),
         ("mixedPrecisionRefinement", c_int), ("rowsPerThread", c_int), ("kernelPath", c_int),
+        ("stagingBuffers", c_int),
     ]
 
 

@@ -48,6 +48,8 @@ struct AppState {
     // buffers allow it; `variant` serves the other launches
     const StreamVariant* stream_v = nullptr;
     int stream_G = 0, stream_max_blocks = 0;
+    int stream_nbuf = 2;  // staging buffers per group
+    int nbuf_req = 0;     // caller's staging buffers per group (0: choose)
     // long systems (N > 4096): two passes over slices (default), or one
     // cluster of CTAs per system (kernelPath 2)
     const LongVariant* long_v = nullptr;
@@ -55,7 +57,10 @@ struct AppState {
     double* long_red = nullptr;  // per (system, slice) records, then per-slice constants
     unsigned* long_flags = nullptr;  // single pass: per (system, slice) publication flags
     unsigned long_epoch = 0;         // single pass: flag value of the latest launch
-    bool long_single = true;         // single pass (else pass 1, carries, pass 2: kernelPath 3)
+    bool long_single = false;        // the plan's form: single pass, else pass 1, carries, pass 2
+    int long_mode = 0;               // kernelPath: 0 two passes where M allows (else single), 3 two, 4 single
+    const LongVariant* long_v_fb = nullptr;  // single-pass fallback for rows no tensor map describes
+    int long_grid_fb = 0;
     int64_t long_batch = 0;      // systems the records hold
     int64_t plan_batch = 0;      // right-hand sides of the plan (size[1] * size[2])
     bool cluster_only = false;   // kernelPath 2
@@ -84,7 +89,7 @@ struct AppState {
         const JwVariant* variant;
         int R, W, G, max_blocks;
         const StreamVariant* stream_v;
-        int stream_G, stream_max_blocks;
+        int stream_G, stream_max_blocks, stream_nbuf;
     };
     std::vector<ChainPlan> chain_plans;
     // streams
@@ -181,16 +186,25 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
             find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, alt);
         if (!v) continue;
         const int T = 32 * v->W;
+        // Most groups first, two staging buffers per group (a caller's
+        // request: the most groups that fit with it).  Measured at N = 512
+        // (131 072 systems): 3 or 4 buffers per group were no faster for FP64
+        // or the mixed mode and at most 4 % faster for FP32 storage, and
+        // where they cost groups (the config-2 chain) much slower.
+        auto fits = [&](int G, int nb, int* blocks) {
+            const size_t smem = v->smem_bytes(G, nb);
+            if (smem > 227 * 1024 || !allow_max_smem(v->func)) return false;
+            return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, v->func, T * G, smem) == cudaSuccess &&
+                   *blocks >= 1;
+        };
+        const bool req = s->nbuf_req >= 2 && s->nbuf_req <= kStMaxBuffers;
         for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
-            const size_t smem = v->smem_bytes(G);
-            if (smem > 227 * 1024) continue;
-            if (!allow_max_smem(v->func)) continue;
             int blocks = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, T * G, smem) != cudaSuccess ||
-                blocks < 1)
-                continue;
+            const int nb = req ? s->nbuf_req : 2;
+            if (!fits(G, nb, &blocks)) continue;
             s->stream_v = v;
             s->stream_G = G;
+            s->stream_nbuf = nb;
             s->stream_max_blocks = blocks * s->num_sms;
             return true;
         }
@@ -200,51 +214,86 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
 }
 
 // Long-system variant for real systems: the first compiled shape that fits
-// and, for two passes, whose rows per thread divide M (16, else 8: M a
-// multiple of 8); the single pass takes any M (its last partial chunk moves
-// outside the TMA boxes).  The per-(system, slice) records are allocated for
-// the plan's right-hand sides.
-bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+// the given form and, for two passes, whose rows per thread divide M (16,
+// else 8: M a multiple of 8); the single pass takes any M (its last partial
+// chunk moves outside the TMA boxes).
+const LongVariant* pick_long(AppState* s, int64_t M, bool single, int* NS_out, int* grid_out,
+                             const LongVariant* like = nullptr)
 {
-    s->long_v = nullptr;
-    if (s->prec != PREC_F64 || s->no_stream || s->cluster_only || LIN != LAY_REAL || LOUT != LAY_REAL || SCALE ||
-        (!s->long_single && M % 8 != 0) || s->plan_batch < 1)
-        return false;
+    if (!single && M % 8 != 0) return nullptr;
     for (int shape = 0; shape < kLongShapes; ++shape) {
         const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
-        if (!v) return false;
-        if (!s->long_single && M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
-        const int b = v->blocks_per_sm(s->long_single);
+        if (!v) return nullptr;
+        if (!single && M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
+        // a fallback shares the plan's records and tables: same slices
+        if (like && (v->R != like->R || v->W != like->W || v->S != like->S || v->tbl_bytes != like->tbl_bytes))
+            continue;
+        const int b = v->blocks_per_sm(single);
         if (b < 1) continue;
         const int NS = (int)((M + v->S - 1) / v->S);
+        if (single && NS > kLongMaxSlices) continue;
         const int64_t res = (int64_t)b * s->num_sms;
         // CTAs in whole multiples of NS, at most one CTA's worth of systems each
         const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
-        if (s->long_single && NS > kLongMaxSlices) continue;
-        // records, slice constants, slice tables, PASS 1 weights (16 bytes per
-        // row), then the single pass's flags (4 bytes per system and slice)
-        const size_t fbytes = (size_t)s->plan_batch * NS * sizeof(unsigned);
-        const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) +
-                             (size_t)NS * v->tbl_bytes + (size_t)NS * v->S * 16 + fbytes;
-        if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            s->long_red = nullptr;
-            return false;
-        }
-        s->long_flags = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(s->long_red) + bytes - fbytes);
-        if (cudaMemset(s->long_flags, 0, fbytes) != cudaSuccess) {
-            cudaGetLastError();
-            cudaFree(s->long_red);
-            s->long_red = nullptr;
-            return false;
-        }
-        s->long_v = v;
-        s->long_NS = NS;
-        s->long_grid = (int)(per_slice * NS);
-        s->long_batch = s->plan_batch;
-        return true;
+        *NS_out = NS;
+        *grid_out = (int)(per_slice * NS);
+        return v;
     }
-    return false;
+    return nullptr;
+}
+
+// Long systems (M > 4096, real FP64).  kernelPath 0: two passes where M is a
+// multiple of 8 (measured faster than the single pass at every length), with
+// a single-pass fallback for launches whose rows no tensor map can describe;
+// else the single pass.  kernelPath 3: two passes only; 4: the single pass
+// only.  The per-(system, slice) records are allocated for the plan's
+// right-hand sides.
+bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
+{
+    s->long_v = nullptr;
+    s->long_v_fb = nullptr;
+    if (s->prec != PREC_F64 || s->no_stream || s->cluster_only || LIN != LAY_REAL || LOUT != LAY_REAL || SCALE ||
+        s->plan_batch < 1)
+        return false;
+    int NS = 0, grid = 0, NSf = 0, gridf = 0;
+    const LongVariant* v = nullptr;
+    const LongVariant* fb = nullptr;
+    if (s->long_mode != 4) v = pick_long(s, M, false, &NS, &grid);
+    if (v && s->long_mode == 0) {
+        fb = pick_long(s, M, true, &NSf, &gridf, v);
+        if (!fb || NSf != NS) v = fb = nullptr;  // no fallback of the same slices: the single pass alone
+    }
+    bool single = false;
+    if (!v && s->long_mode != 3) {
+        v = pick_long(s, M, true, &NS, &grid);
+        single = true;
+    }
+    if (!v) return false;
+    // records, slice constants, slice tables, PASS 1 weights (16 bytes per
+    // row), then the single pass's flags (4 bytes per system and slice)
+    const size_t fbytes = (size_t)s->plan_batch * NS * sizeof(unsigned);
+    const size_t bytes = ((size_t)s->plan_batch * NS * 8 + (size_t)NS * 8) * sizeof(double) +
+                         (size_t)NS * v->tbl_bytes + (size_t)NS * v->S * 16 + fbytes;
+    if (cudaMalloc(&s->long_red, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        s->long_red = nullptr;
+        return false;
+    }
+    s->long_flags = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(s->long_red) + bytes - fbytes);
+    if (cudaMemset(s->long_flags, 0, fbytes) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(s->long_red);
+        s->long_red = nullptr;
+        return false;
+    }
+    s->long_v = v;
+    s->long_single = single;
+    s->long_NS = NS;
+    s->long_grid = grid;
+    s->long_v_fb = fb;
+    s->long_grid_fb = gridf;
+    s->long_batch = s->plan_batch;
+    return true;
 }
 
 // Cluster variant for long real systems: C CTAs of 2048 rows, C the smallest
@@ -571,17 +620,25 @@ PfSolveResult launch_cluster(AppState* s, const JwOperator& op, const JwIO& io, 
 PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cudaStream_t stream)
 {
     const LongVariant* v = s->long_v;
+    bool single = s->long_single;
+    int grid = s->long_grid;
     if (io.accumulate || io.oz0 > 0 || io.oz1 < io.M || io.nsys > s->long_batch)
         return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     JwIO mio = io;  // the maps cover the whole chunks of R rows
     mio.M = (io.M / v->R) * v->R;
     const MapCacheEntry* e = row_maps(v, v->R, LAY_REAL, LAY_REAL, v->IB, v->IBO, mio);
     // Rows no tensor map can describe (stride or offset not a multiple of 16
-    // bytes): the single pass moves them with plain loads and stores.
+    // bytes): the single pass moves them with plain loads and stores (a
+    // two-pass plan's fallback, when it has one, shares its records).
     static const CUtensorMap kNoMap = {};
     JwIO lio = io;
     if (!e) {
-        if (!s->long_single) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        if (!single) {
+            if (!s->long_v_fb) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+            v = s->long_v_fb;
+            grid = s->long_grid_fb;
+            single = true;
+        }
         lio.plain = 1;
     }
     const CUtensorMap* tin = e ? &e->in : &kNoMap;
@@ -589,13 +646,13 @@ PfSolveResult launch_long(AppState* s, const JwOperator& op, const JwIO& io, cud
     double* cst = s->long_red + (size_t)s->long_batch * s->long_NS * 8;
     double* tab = cst + (size_t)s->long_NS * 8;
     if (++s->long_epoch == 0) s->long_epoch = 1;  // 0 is the flags' initial value
-    const cudaError_t err = v->launch(s->long_grid, stream, tin, tout, op, lio, s->long_red, cst, tab, s->long_NS,
-                                      s->long_flags, s->long_epoch, s->long_single);
+    const cudaError_t err = v->launch(grid, stream, tin, tout, op, lio, s->long_red, cst, tab, s->long_NS,
+                                      s->long_flags, s->long_epoch, single);
     note_launch(true);
     record_launch(PFSOLVE_KERNEL_LONG, v->R, v->W, v->G, v->KL, v->KU, v->SV, LAY_REAL, LAY_REAL, 0, PREC_F64, 0,
-                  s->long_grid);
+                  grid);
     // the table passes, and for two passes the carry kernel (solves only) and pass 2
-    g_launches.fetch_add((s->long_single ? 1 : (s->sv != SV_NONE ? 3 : 2)) + (s->sv == SV_TRI ? 1 : 0),
+    g_launches.fetch_add((single ? 1 : (s->sv != SV_NONE ? 3 : 2)) + (s->sv == SV_TRI ? 1 : 0),
                          std::memory_order_relaxed);
     if (err != cudaSuccess) {
         cudaGetLastError();
@@ -617,8 +674,9 @@ bool launch_stream(AppState* s, const JwOperator& op, const JwIO& io, cudaStream
     if (!e) return false;
     const int64_t want = (rs.nsys + s->stream_G - 1) / s->stream_G;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, s->stream_max_blocks));
-    v->launch(dim3((unsigned)grid), dim3(32 * v->W * s->stream_G), v->smem_bytes(s->stream_G), stream, &e->in, &e->out,
-              op, rs);
+    rs.nbuf = s->stream_nbuf;
+    v->launch(dim3((unsigned)grid), dim3(32 * v->W * s->stream_G), v->smem_bytes(s->stream_G, s->stream_nbuf), stream,
+              &e->in, &e->out, op, rs);
     record_launch(PFSOLVE_KERNEL_STREAMING, v->R, v->W, s->stream_G, v->KL, v->KU, v->SV, v->LIN, v->LOUT, v->SCALE,
                   v->PREC, v->ALT, grid);
     return true;
@@ -1084,6 +1142,11 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
     if (!s) return PFSOLVE_ERROR_MALLOC_FAILED;
     app->internal = s;
     s->device = *c.device;
+    if (c.stagingBuffers != 0 && (c.stagingBuffers < 2 || c.stagingBuffers > kStMaxBuffers)) {
+        deletePfSolve(app);
+        return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    }
+    s->nbuf_req = c.stagingBuffers;
     if (cudaSetDevice(s->device) != cudaSuccess) { deletePfSolve(app); return PFSOLVE_ERROR_INVALID_DEVICE; }
     if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device) != cudaSuccess) {
         deletePfSolve(app);
@@ -1143,7 +1206,7 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                 s->R_req = c.rowsPerThread;
                 s->no_stream = c.kernelPath == 1;
                 s->cluster_only = c.kernelPath == 2;
-                s->long_single = c.kernelPath != 3;
+                s->long_mode = c.kernelPath;
                 s->plan_batch = (int64_t)c.size[1] * (int64_t)(c.size[2] ? c.size[2] : 1);
                 r = finish_variant(s, c.M_size, LAY_REAL, LAY_REAL, 0);
             }
@@ -1364,6 +1427,7 @@ PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchPara
         t.stream_v = cp.stream_v;
         t.stream_G = cp.stream_G;
         t.stream_max_blocks = cp.stream_max_blocks;
+        t.stream_nbuf = cp.stream_nbuf;
         return launch_jw_variant(&t, op, io, stream);
     }
     AppState t;
@@ -1379,9 +1443,11 @@ PfSolveResult append_chain_fused(PfSolveApplication* dg, const PfSolveLaunchPara
     t.R_fixed = cj.rowsPerThread != 0 && cj.rowsPerThread != 32;
     t.R_req = cj.rowsPerThread;
     t.no_stream = cj.kernelPath == 1;
+    t.nbuf_req = cj.stagingBuffers;
     if (finish_variant(&t, M, LIN, LOUT, SCALE) != PFSOLVE_SUCCESS) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     sj->chain_plans.push_back(AppState::ChainPlan{KL, KU, L.sv, LIN, LOUT, SCALE, t.variant, t.R, t.W, t.G,
-                                                  t.max_blocks, t.stream_v, t.stream_G, t.stream_max_blocks});
+                                                  t.max_blocks, t.stream_v, t.stream_G, t.stream_max_blocks,
+                                                  t.stream_nbuf});
     return launch_jw_variant(&t, op, io, stream);
 }
 

@@ -89,7 +89,7 @@ template <class S> __device__ __forceinline__ S shfl_down_s(S v, int d) { return
 template <> __device__ __forceinline__ dd shfl_up_s<dd>(dd v, int d) { return VOps<dd>::shfl_up(v, d); }
 template <> __device__ __forceinline__ dd shfl_down_s<dd>(dd v, int d) { return VOps<dd>::shfl_down(v, d); }
 
-// FP64 <-> FP32 value conversions (round to nearest).
+// FP64 <-> FP32 value conversions (round to nearest when narrowing).
 __device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v); }
 __device__ __forceinline__ float2 to_f32(double2 v) { return make_float2(__double2float_rn(v.x), __double2float_rn(v.y)); }
 __device__ __forceinline__ double to_f64(float v) { return (double)v; }

@@ -29,10 +29,10 @@ constexpr int kSeqChunk = 8;                     // rows per box
 constexpr int kSeqBufBytes = kSeqChunk * 32 * 8;  // 2 KB
 constexpr int kSeqBufs = 4;
 // threads per CTA: 24 warps (85 registers a thread) for K <= 4, 16 warps
-// (128 registers) for the 8-step variants
-template <int KMAX>
+// (128 registers) for 5 to 8 steps
+template <int K>
 struct SeqThreads {
-    static constexpr int v = KMAX > 4 ? 512 : 768;
+    static constexpr int v = K > 4 ? 512 : 768;
 };
 
 // Shared table: per step s and row i the pair {o, q} (matvec off-diagonal,
@@ -63,14 +63,16 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
 }
 
 // UB: 1 ascending sweep (upper matvec, lower solve), 0 descending.
-// KMAX: compiled bound of K (the step loop is unrolled to it).
-template <int UB, bool MV, bool SV, int KMAX>
-__global__ void __launch_bounds__(SeqThreads<KMAX>::v) jw_steps_seq_kernel(const __grid_constant__ CUtensorMap tm_in,
-                                                                         const __grid_constant__ CUtensorMap tm_out,
-                                                                         const __grid_constant__ JwSteps S, const JwIO io)
+// K: the number of steps (compiled per K, so the step loop unrolls exactly
+// and the step that applies the matvec diagonal -- the first for UB 1, the
+// last for UB 0 -- is known at compile time).
+template <int UB, bool MV, bool SV, int K>
+__global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __grid_constant__ CUtensorMap tm_in,
+                                                                      const __grid_constant__ CUtensorMap tm_out,
+                                                                      const __grid_constant__ JwSteps S, const JwIO io)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int K = S.K;
+    constexpr int KMAX = K;
     const int NW = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int M0 = (int)S.M_in, Mout = (int)S.M_out;
@@ -84,9 +86,8 @@ __global__ void __launch_bounds__(SeqThreads<KMAX>::v) jw_steps_seq_kernel(const
                      warp * kSeqBufs;
 
     // ---- coefficient table (rows at or beyond a step's M_s are never read)
-    int dstep = -1;  // the step that applies the matvec diagonal
-    for (int s = 0; s < K; ++s)
-        if (MV && S.st[s].diag) dstep = s;
+    // the step that applies the matvec diagonal (JwStepDesc.diag)
+    constexpr int dstep = MV ? (UB ? 0 : K - 1) : -1;
     for (int e = threadIdx.x; e < K * Mtab; e += blockDim.x) {
         const int s = e / Mtab, i = e - s * Mtab;
         const JwStepDesc& d = S.st[s];
@@ -238,8 +239,11 @@ __global__ void __launch_bounds__(SeqThreads<KMAX>::v) jw_steps_seq_kernel(const
                             const double2 c = lds2(ta[s] + (UB ? 16 * o : -16 * o));
                             double y = xa[s];
                             if (MV && s == dstep) y *= lds(td + (UB ? 8 * o : -8 * o));
-                            if (MV) y = __fma_rn(c.x, v, y);
-                            const double z = SV ? __fma_rn(-c.y, zp[s], y) : y;
+                            // z = (y - q z_prev) + o v: the part that does not
+                            // depend on the step before is formed first, so
+                            // the chain through the K steps is one FMA a step
+                            if (SV) y = __fma_rn(-c.y, zp[s], y);
+                            const double z = MV ? __fma_rn(c.x, v, y) : y;
                             zp[s] = z;
                             xa[s] = v;
                             v = z;
@@ -282,8 +286,8 @@ __global__ void __launch_bounds__(SeqThreads<KMAX>::v) jw_steps_seq_kernel(const
                         const double2 c = lds2(tabA_u + (uint32_t)((s * Mtab + i) * 16));
                         double y = xa[s];
                         if (MV && s == dstep) y *= lds(tabD_u + (uint32_t)(i * 8));
-                        if (MV) y = __fma_rn(c.x, v, y);
-                        z = SV ? __fma_rn(-c.y, zp[s], y) : y;
+                        if (SV) y = __fma_rn(-c.y, zp[s], y);
+                        z = MV ? __fma_rn(c.x, v, y) : y;
                     } else {
                         z = xa[s];
                     }

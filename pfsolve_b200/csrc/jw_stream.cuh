@@ -122,17 +122,18 @@ struct StCfg {
     static_assert(CPLX ? (LOUT != LAY_REAL) : (LOUT == LAY_REAL), "layout pair");
 };
 
+// NB: staging buffers per group (2..kStMaxBuffers).
 template <class C>
-__host__ __device__ constexpr size_t st_fixed_bytes(int G)
+__host__ __device__ constexpr size_t st_fixed_bytes(int G, int NB)
 {
-    return C::TBL + (size_t)G * C::W * kScratchPerWarp * sizeof(double) + (size_t)G * 2 * sizeof(uint64_t);
+    return C::TBL + (size_t)G * C::W * kScratchPerWarp * sizeof(double) + (size_t)G * NB * sizeof(uint64_t);
 }
 
 // Dynamic shared memory: table | scratch | mbarriers | (align 1024) | buffers.
 template <class C>
-__host__ __device__ constexpr size_t st_smem_bytes(int G)
+__host__ __device__ constexpr size_t st_smem_bytes(int G, int NB)
 {
-    return st_fixed_bytes<C>(G) + 1024 + (size_t)G * 2 * C::BUF;
+    return st_fixed_bytes<C>(G, NB) + 1024 + (size_t)G * NB * C::BUF;
 }
 
 // ---- TMA, mbarrier and bulk-group primitives (PTX).
@@ -354,11 +355,14 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     CT* table = reinterpret_cast<CT*>(smem_raw);
     double* scratch_all = reinterpret_cast<double*>(smem_raw + C::TBL);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::TBL + (size_t)G * W * kScratchPerWarp * sizeof(double));
-    unsigned char* after = reinterpret_cast<unsigned char*>(bars + 2 * G);
+    // NBUF staging buffers per group, used in turn: system k of the group in
+    // buffer k mod NBUF, its load issued NBUF - 1 systems ahead.
+    const int NBUF = (io.nbuf >= 2 && io.nbuf <= kStMaxBuffers) ? io.nbuf : 2;
+    unsigned char* after = reinterpret_cast<unsigned char*>(bars + NBUF * G);
     const uint32_t pad = (1024u - (smem_u32(after) & 1023u)) & 1023u;
-    unsigned char* buf0 = after + pad + (size_t)(2 * grp) * C::BUF;
-    unsigned char* buf1 = buf0 + C::BUF;
-    const uint32_t bar0 = smem_u32(&bars[2 * grp]), bar1 = smem_u32(&bars[2 * grp + 1]);
+    unsigned char* buf_base = after + pad + (size_t)(NBUF * grp) * C::BUF;
+    auto buf_at = [&](int b) -> unsigned char* { return buf_base + (size_t)b * C::BUF; };
+    auto bar_at = [&](int b) -> uint32_t { return smem_u32(&bars[NBUF * grp + b]); };
 
     // Shared-memory byte offset of swizzle row h of plane p of chunk c, in the
     // warp-major staging layout (the boxes of warp c/32, then the next
@@ -395,12 +399,13 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         bulk_commit();
     };
 
-    if ((int)threadIdx.x < 2 * G) mbar_init(smem_u32(&bars[threadIdx.x]), W);
+    if ((int)threadIdx.x < NBUF * G) mbar_init(smem_u32(&bars[threadIdx.x]), W);
     mbar_init_fence();
     __syncthreads();  // the barriers are initialised before any copy can complete on them
     // The first system's copy does not depend on the coefficient table: it is
     // in flight while the prologue reads the bands.
-    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
+    if (lane == 0)
+        for (int j = 0; j < NBUF - 1 && sys + j * step < nsys; ++j) issue_load(buf_at(j), bar_at(j), sys + j * step);
     st_prologue<C>(op, table, scratch_all);
     __syncthreads();
 
@@ -526,10 +531,10 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             v[1] = (MS)d.y;
         } else {
             const float4 f = *reinterpret_cast<const float4*>(a);
-            v[0] = (MS)f.x;
-            v[1] = (MS)f.y;
-            v[2] = (MS)f.z;
-            v[3] = (MS)f.w;
+            v[0] = conv<MS>(f.x);
+            v[1] = conv<MS>(f.y);
+            v[2] = conv<MS>(f.z);
+            v[3] = conv<MS>(f.w);
         }
     };
     // the 16 bytes at `a` from EPU (or, packed complex, 16 / ES) values
@@ -542,10 +547,11 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
 
     const bool win_partial = io.iz0 > 0 || io.iz1 < io.M;
 
-    for (int k = 0; sys < nsys; ++k, sys += step) {
-        unsigned char* cur = (k & 1) ? buf1 : buf0;
-        unsigned char* nxt = (k & 1) ? buf0 : buf1;
-        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
+    int bi = 0;        // buffer of this system
+    uint32_t par = 0;  // phase parity of its barrier
+    for (; sys < nsys; sys += step) {
+        unsigned char* cur = buf_at(bi);
+        bool ok = mbar_wait_bounded(bar_at(bi), par);
         ok = (W == 1) ? (__all_sync(FULL, ok) != 0) : group_and(g.bar_id, g.nthr, ok);
         if (!ok) {
             if (threadIdx.x == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
@@ -622,11 +628,13 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         }
         V (&x)[R + KL + KU] = be;
 
-        // The next system's load goes into the other buffer once this warp's
-        // stores from it have been read out of shared memory.
-        if (sys + step < nsys && lane == 0) {
+        // The load NBUF - 1 systems ahead goes into the buffer of the system
+        // before this one, once this warp's stores from it have been read out
+        // of shared memory.
+        if (sys + (NBUF - 1) * step < nsys && lane == 0) {
+            const int pb = (bi == 0) ? NBUF - 1 : bi - 1;
             bulk_wait_read_all();
-            issue_load(nxt, (k & 1) ? bar0 : bar1, sys + step);
+            issue_load(buf_at(pb), bar_at(pb), sys + (NBUF - 1) * step);
         }
 
         if constexpr (C::MIXED) {
@@ -864,6 +872,10 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) issue_store(cur, sys);
+        if (++bi == NBUF) {
+            bi = 0;
+            par ^= 1u;
+        }
     }
     if (lane == 0) bulk_wait_all();
 }

@@ -45,6 +45,9 @@ struct JwOperator {
 };
 
 // The data side: systems, layouts, keep-windows.
+// Streaming kernel: at most this many TMA staging buffers per group.
+constexpr int kStMaxBuffers = 4;
+
 struct JwIO {
     const double* in;             // FP64 values, or FP32 values for the FP32-storage precisions
     double* out;
@@ -57,6 +60,7 @@ struct JwIO {
     int accumulate;               // output += result
     int alt;                      // ALT mode: system 2y + h is the parity-h rows of row set y
     int plain;                    // long-system single pass: rows not 16-byte aligned, moved by plain loads/stores
+    int nbuf;                     // streaming kernel: staging buffers per group (2..4; 0: 2)
 };
 
 // K consecutive steps in one kernel (numConsecutiveJWIterations = K).

@@ -70,7 +70,7 @@ struct StreamVariant {
     int R, W, KL, KU, SV, LIN, LOUT, SCALE, PREC;
     int max_threads;
     const void* func;
-    size_t (*smem_bytes)(int G);
+    size_t (*smem_bytes)(int G, int NB);  // G groups of NB staging buffers
     int IB, IBO;
     void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
                    const JwOperator& op, const JwIO& io);
@@ -137,7 +137,7 @@ struct StepsVariant {
 const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV);
 
 // K bidiagonal steps, one system per lane, all steps in one sweep (UB 1:
-// ascending rows, 0: descending), K <= KMAX; systems staged by TMA boxes of
+// ascending rows, 0: descending), compiled for K = KMAX steps; systems staged by TMA boxes of
 // 8 rows x 32 systems.
 struct SeqStepsVariant {
     int UB, MV, SV, KMAX;

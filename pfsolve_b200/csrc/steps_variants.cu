@@ -45,17 +45,20 @@ const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV)
     return nullptr;
 }
 
-template <int UB, bool MV, bool SV, int KMAX>
+template <int UB, bool MV, bool SV, int K>
 static void seq_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in,
                           const CUtensorMap* out, const JwSteps& S, const JwIO& io)
 {
-    jw_steps_seq_kernel<UB, MV, SV, KMAX><<<grid, block, smem, st>>>(*in, *out, S, io);
+    jw_steps_seq_kernel<UB, MV, SV, K><<<grid, block, smem, st>>>(*in, *out, S, io);
 }
 
-#define PFB_SQ(UB, MV, SV, KM)                                                                          \
-    SeqStepsVariant{UB, MV, SV, KM, SeqThreads<KM>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, KM>, \
-                    &seq_launch_fn<UB, MV, SV, KM>}
-#define PFB_SQ3(UB, MV, SV) PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 4), PFB_SQ(UB, MV, SV, 8)
+#define PFB_SQ(UB, MV, SV, K)                                                                         \
+    SeqStepsVariant{UB, MV, SV, K, SeqThreads<K>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, K>, \
+                    &seq_launch_fn<UB, MV, SV, K>}
+// one instance per step count, 2..8
+#define PFB_SQ3(UB, MV, SV)                                                                               \
+    PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 3), PFB_SQ(UB, MV, SV, 4), PFB_SQ(UB, MV, SV, 5),            \
+        PFB_SQ(UB, MV, SV, 6), PFB_SQ(UB, MV, SV, 7), PFB_SQ(UB, MV, SV, 8)
 
 static const SeqStepsVariant kSeqVariants[] = {
     PFB_SQ3(1, true, true), PFB_SQ3(1, true, false), PFB_SQ3(1, false, true),
@@ -65,7 +68,7 @@ static const SeqStepsVariant kSeqVariants[] = {
 const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K)
 {
     for (const SeqStepsVariant& v : kSeqVariants)
-        if (v.UB == UB && v.MV == (MV ? 1 : 0) && v.SV == (SV ? 1 : 0) && K <= v.KMAX) return &v;
+        if (v.UB == UB && v.MV == (MV ? 1 : 0) && v.SV == (SV ? 1 : 0) && K == v.KMAX) return &v;
     return nullptr;
 }
 

@@ -11,9 +11,9 @@
 namespace pfb {
 
 template <class C>
-inline size_t st_smem_fn(int G)
+inline size_t st_smem_fn(int G, int NB)
 {
-    return st_smem_bytes<C>(G);
+    return st_smem_bytes<C>(G, NB);
 }
 
 template <class C>

@@ -6,8 +6,10 @@ tests/golden/make_golden.py --only long).
 CPU: the oracle reproduces the tridiagonal fixtures (N = 4352 .. 16384) and the
 single-launch bidiagonal one at N = 4352 (pins it); the reference's bidiagonal
 multi-upload outputs are recorded as a defect (below).
-GPU: the long-system kernels (the single pass, the default; the two-pass
-form, kernelPath 3; the cluster kernel, kernelPath 2, up to 16 384 rows)
+GPU: the long-system kernels (the default plan: two passes where N is a
+multiple of 8, else the single pass; two passes alone, kernelPath 3; the
+single pass alone, kernelPath 4; the cluster kernel, kernelPath 2, up to
+16 384 rows)
 reproduce the fixtures through the C ABI, and match the oracle where the
 reference's output is defective.
 Tolerances as for the single-step fixtures: 2e-15 (oracle), 2e-13 (kernels
@@ -62,7 +64,7 @@ def test_oracle_against_reference(path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel_path", [0, 3, 2], ids=["single_pass", "two_pass", "cluster"])
+@pytest.mark.parametrize("kernel_path", [0, 3, 4, 2], ids=["default", "two_pass", "single_pass", "cluster"])
 @pytest.mark.parametrize("path", FILES, ids=IDS)
 def test_kernel_against_reference(path, kernel_path):
     import jwcases as J

@@ -1,9 +1,12 @@
 """GPU parity of the long-system JW kernels, through the C ABI.
 
 Systems of 4 096 < N <= 65 536 rows run over slices of 1 024 rows
-(PfSolveGetShape streaming = 5): by default in a single pass, one
+(PfSolveGetShape streaming = 5): by default in two passes with no waits
+between CTAs where N is a multiple of 8 (launches whose rows no tensor map
+can describe fall back to the single pass), else in a single pass, one
 cooperative launch whose CTAs wait (bounded) for the other slices of each
-system; with kernelPath 3 in two passes with no waits between CTAs.  With
+system; kernelPath 3 asks for two passes only, kernelPath 4 for the single
+pass only.  With
 kernelPath 2, systems of up to 16 384 rows run on one thread-block cluster of
 3, 4, 6 or 8 CTAs per system (streaming = 2).  Every case checks that the
 plan chose the kernel asked for, that the launch ran on it, and that every
@@ -48,7 +51,7 @@ def _run(case, bands, rhs, **extra):
     return x, shape, n
 
 
-PATHS = {0: 5, 3: 5, 2: 2}  # kernelPath -> PfSolveGetShape streaming
+PATHS = {0: 5, 3: 5, 4: 5, 2: 2}  # kernelPath -> PfSolveGetShape streaming
 
 
 @pytest.mark.parametrize("path", list(PATHS))
@@ -84,9 +87,9 @@ def test_long_many_systems_and_windows(path):
 
 @pytest.mark.parametrize("path", [3, 2])
 def test_long_rejects_buffers_it_cannot_take(path):
-    """The two-pass and cluster forms have no fallback for rows a TMA tensor
-    map cannot describe: a misaligned launch returns UNSUPPORTED_COMBINATION
-    instead of running."""
+    """The two-pass form asked for alone (kernelPath 3) and the cluster form
+    have no fallback for rows a TMA tensor map cannot describe: a misaligned
+    launch returns UNSUPPORTED_COMBINATION instead of running."""
     rng = np.random.default_rng(3)
     case, bands, rhs = _case(rng, 6144, 3, 2, 13, bitmask=capi.RUNTIME_OFFSETSOLUTION, run_offsetSolution=1)
     with pytest.raises(capi.PfSolveError) as ei:
@@ -127,24 +130,28 @@ def test_single_pass_any_length(M, ub, jwt):
     assert e <= TOL, (e, emax)
 
 
-def test_single_pass_is_the_default_and_repeats():
-    """The default plan runs the single pass (one long-kernel launch after the
-    table passes: three launches in all for a tridiagonal solve); repeated
-    launches of one plan (new flag epochs each time) give the same result."""
+@pytest.mark.parametrize("M,path,launches", [(16384, 0, 5), (16384, 4, 3), (12345, 0, 3)])
+def test_long_default_forms_and_repeats(M, path, launches):
+    """The default plan runs two passes where N is a multiple of 8 (pivot
+    products, tables, pass 1, carries, pass 2: five launches for a
+    tridiagonal solve) and the single pass otherwise (tables and one
+    cooperative launch: three); kernelPath 4 asks for the single pass.
+    Repeated launches of one plan (new flag epochs each time) give the same
+    result."""
     import torch
 
     from pfsolve_b200.api import App, last_launch, launch_count
     rng = np.random.default_rng(5)
-    M, B = 16384, 600
+    B = 600
     case, bands, rhs = _case(rng, M, B, 2, 13)
     tb = torch.from_numpy(bands).cuda()
     base = torch.from_numpy(rhs).cuda()
     x = base.clone()
-    app = App(buffer=tb, outputBuffer=x, **J.case_fields(case))
+    app = App(buffer=tb, outputBuffer=x, **J.case_fields(case, kernelPath=path))
     n0 = launch_count()
     app.append()
     torch.cuda.synchronize()
-    assert launch_count() - n0 == 3
+    assert launch_count() - n0 == launches
     assert last_launch()["kernel"] == capi.PFSOLVE_KERNEL_LONG
     first = x.cpu().numpy()
     for _ in range(3):
