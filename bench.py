@@ -608,8 +608,9 @@ def serving_leg(rate=20000.0, duration_s=1.5, pool=256, warm=2000):
 
 def config3_profile(args):
     """Profiling case: config 3 (N = 512 real tridiagonal, weakly dominant),
-    `--ncplx` systems, FP64 or mixed precision (`--refine`), K timed steps;
-    prints one JSON line with the kernel time."""
+    `--ncplx` systems, FP64 or mixed precision (`--refine`), or FP32 storage
+    (`--prec f32` / `f32mem`), K timed steps; prints one JSON line with the
+    kernel time."""
     import torch
 
     from pfsolve_b200 import workloads as WL
@@ -618,8 +619,13 @@ def config3_profile(args):
     M, B = wl.M, wl.nrhs
     tb = torch.from_numpy(wl.jw_bands).cuda()
     x = torch.from_numpy(wl.rhs).cuda()
-    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, doublePrecision=1,
-              scaleC=1.0, mixedPrecisionRefinement=args.refine, rowsPerThread=args.rows, kernelPath=args.path)
+    prec = dict(doublePrecision=1)
+    es = 8
+    if args.prec != "f64":  # FP32 storage: FP32 arithmetic, or FP64 arithmetic (doublePrecisionFloatMemory)
+        tb, x, es = tb.float(), x.float(), 4
+        prec = dict(doublePrecision=0, doublePrecisionFloatMemory=1 if args.prec == "f32mem" else 0)
+    app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, scaleC=1.0,
+              mixedPrecisionRefinement=args.refine, rowsPerThread=args.rows, kernelPath=args.path, **prec)
     for _ in range(max(1, args.warmup)):
         app.append()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -630,8 +636,9 @@ def config3_profile(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    print(json.dumps({"profile_case": "config3", "M": M, "rhs": B, "refine": args.refine, "ms_per_step": ms,
-                      "gbs": 2.0 * M * 8 * B / (ms * 1e-3) / 1e9, "kernel": app.shape()}), flush=True)
+    print(json.dumps({"profile_case": "config3", "M": M, "rhs": B, "refine": args.refine, "prec": args.prec,
+                      "ms_per_step": ms, "gbs": 2.0 * M * es * B / (ms * 1e-3) / 1e9, "kernel": app.shape()}),
+          flush=True)
     app.close()
 
 
@@ -708,14 +715,16 @@ def dd_profile(args):
     multiply-add)."""
     import torch
 
-    from oracle import oracle as O
     from pfsolve_b200 import workloads as WL
     from pfsolve_b200.api import App
+
+    def to_dd(a):  # FP64 values -> double-double {hi, lo = 0} pairs
+        return np.stack([a, np.zeros_like(a)], -1).ravel()
     wl = WL.config3(M=args.m, B=args.ncplx)
     M, B = wl.M, wl.nrhs
     f64mem = args.refine == 1
-    bands = wl.jw_bands if f64mem else O.to_dd(wl.jw_bands)
-    rhs = wl.rhs if f64mem else O.to_dd(wl.rhs)
+    bands = wl.jw_bands if f64mem else to_dd(wl.jw_bands)
+    rhs = wl.rhs if f64mem else to_dd(wl.rhs)
     tb = torch.from_numpy(bands).cuda()
     x = torch.from_numpy(rhs).cuda()
     mode = dict(quadDoubleDoublePrecisionDoubleMemory=1) if f64mem else dict(quadDoubleDoublePrecision=1)
@@ -839,6 +848,8 @@ def main():
     ap.add_argument("--m", type=int, default=512, help="config 3 / K-step profiling case: rows per system")
     ap.add_argument("--ksteps", type=int, default=4, help="K-step profiling case: consecutive steps")
     ap.add_argument("--refine", type=int, default=0, help="config 3 profiling case: mixed-precision sweeps (0: FP64)")
+    ap.add_argument("--prec", default="f64", choices=["f64", "f32", "f32mem"],
+                    help="config 3 profiling case: FP64 storage, or FP32 storage with FP32 or FP64 arithmetic")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="kernelPath: 0 streaming kernel where possible (long systems: two passes where N is a "
                          "multiple of 8, else the single pass), 1 group kernel only, 2 long systems on the cluster "
