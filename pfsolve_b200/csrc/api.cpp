@@ -460,6 +460,29 @@ PfSolveResult plan_alt(AppState* s, const PfSolveConfiguration& c, int base_prec
 // caller's choice (s->R) first, then the other compiled choices.
 PfSolveResult finish_variant(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {
+    // Double-double: the table form first (16 rows per thread where a system
+    // fits one warp, else 8), then the register form (the caller's rows per
+    // thread: those, in either form).
+    if ((s->prec == PREC_DD || s->prec == PREC_DD_F64MEM) && !s->no_tbl && LIN == LAY_REAL && LOUT == LAY_REAL &&
+        !SCALE) {
+        const int cand[3][2] = {{16, 1}, {8, 1}, {4, 1}};
+        for (const auto& rc : cand) {
+            const int R = rc[0];
+            if (s->R_req && R != s->R_req) continue;
+            const int64_t W = (M + 32 * (int64_t)R - 1) / (32 * (int64_t)R);
+            if (W < 1 || W > 4 || (R == 16 && W > 1 && !s->R_req)) continue;
+            const JwVariant* v = find_jw_variant(R, s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, 1);
+            if (!v || 32 * W > v->max_threads) continue;
+            int G = 0, maxb = 0;
+            if (!choose_groups(v, (int)W, s->num_sms, G, maxb)) continue;
+            s->variant = v;
+            s->R = R;
+            s->W = (int)W;
+            s->G = G;
+            s->max_blocks = maxb;
+            return PFSOLVE_SUCCESS;
+        }
+    }
     const int order[4] = {s->R, 8, 4, 16};
     // The caller's rows per thread first; when the group kernel has no such
     // variant (the choice is then the streaming kernel's), any other.

@@ -45,9 +45,22 @@ inline void dd_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, co
     JwVariant{R, KL, KU, SV, LAY_REAL, LAY_REAL, 0, (MEM) ? 2 : 3, 0, 256,                              \
               (const void*)&jw_dd_kernel<DdCfg<R, KL, KU, SV, MEM>>, &dd_smem_fn<DdCfg<R, KL, KU, SV, MEM>>, \
               &dd_launch_fn<DdCfg<R, KL, KU, SV, MEM>>}
-#define PFB_DD(KL, KU, SV) \
-    PFB_DDV(4, KL, KU, SV, true), PFB_DDV(8, KL, KU, SV, true), PFB_DDV(4, KL, KU, SV, false), \
-        PFB_DDV(8, KL, KU, SV, false)
+template <class C>
+inline void dd_tbl_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const JwOperator& op,
+                             const JwIO& io, int W)
+{
+    jw_dd_tbl_kernel<C><<<grid, block, smem, st>>>(op, io, W);
+}
+// table form (TBL = 1): coefficients, chunk products and scan multipliers in
+// shared memory
+#define PFB_DDT(R, KL, KU, SV, MEM)                                                                               \
+    JwVariant{R, KL, KU, SV, LAY_REAL, LAY_REAL, 0, (MEM) ? 2 : 3, 1, 256,                                        \
+              (const void*)&jw_dd_tbl_kernel<DdCfg<R, KL, KU, SV, MEM, true>>,                                      \
+              &dd_smem_fn<DdCfg<R, KL, KU, SV, MEM, true>>, &dd_tbl_launch_fn<DdCfg<R, KL, KU, SV, MEM, true>>}
+#define PFB_DD(KL, KU, SV)                                                                                 \
+    PFB_DDV(4, KL, KU, SV, true), PFB_DDV(8, KL, KU, SV, true), PFB_DDV(4, KL, KU, SV, false),               \
+        PFB_DDV(8, KL, KU, SV, false), PFB_DDT(8, KL, KU, SV, true), PFB_DDT(16, KL, KU, SV, true),          \
+        PFB_DDT(8, KL, KU, SV, false), PFB_DDT(16, KL, KU, SV, false)
 
 // Rows-per-thread choices for the single-application (drop-in) variants.
 #define PFB_R4(KL, KU, SV, LIN, LOUT, SC) \

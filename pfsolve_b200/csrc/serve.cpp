@@ -129,6 +129,23 @@ void serve_rows(int64_t Mmax, int& R, int& W)
     W = p;
 }
 
+// Double-double kernel for systems of M rows: the register form at 4 rows
+// per thread up to 128 rows, else the table form (coefficients built once per
+// CTA in shared memory), 16 rows per thread up to 512 rows (one warp), else 8.
+const JwVariant* serve_dd_variant(int64_t M, int KL, int KU, int sv, int prec, int& W)
+{
+    int R = 4, tbl = 0;
+    if (M > 128) {
+        R = (M <= 512) ? 16 : 8;
+        tbl = 1;
+    }
+    W = (int)((M + 32 * R - 1) / (32 * R));
+    int p = 1;
+    while (p < W) p <<= 1;
+    W = p;
+    return find_jw_variant(R, KL, KU, sv, LAY_REAL, LAY_REAL, 0, prec, tbl);
+}
+
 bool batch_shape(PfSolveServer* s, const BatchVariant* v, int W, Shape& out)
 {
     std::lock_guard<std::mutex> lk(s->shape_mu);
@@ -310,10 +327,9 @@ void launch_flight(PfSolveServer* s, Flight& fl, int cls)
     } else {
         for (Req* r : fl.reqs) {
             const ServeOp& o = s->ops[r->r.op];
-            int R, W;
-            serve_rows(o.M, R, W);
+            int W;
             const int prec = (r->r.precision == PFSOLVE_SERVE_DD) ? 2 : 3;
-            const JwVariant* v = find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, prec, 0);
+            const JwVariant* v = serve_dd_variant(o.M, o.KL, o.KU, o.L.sv, prec, W);
             Shape sh;
             if (!v || !jw_shape(s, v, W, sh)) {
                 r->status = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
@@ -496,10 +512,12 @@ PfSolveResult PfSolveServerAddOperator(PfSolveServer* s, int64_t M, const double
     o.KL = (o.L.mvj == MVJ_LOWER) ? 1 : 0;
     o.KU = (o.L.mvj == MVJ_UPPER) ? 1 : 0;
     for (int R : {4, 8}) {
-        if (!find_batch_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED) ||
-            !find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, 2, 0) ||
-            !find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, 3, 0))
+        if (!find_batch_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED))
             return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+    }
+    for (int prec : {PREC_DD, PREC_DD_F64MEM}) {
+        int W;
+        if (!serve_dd_variant(M, o.KL, o.KU, o.L.sv, prec, W)) return PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
     }
     cudaSetDevice(s->desc.device);
     if (cudaMalloc(&o.bands_dd, 3 * M * 2 * sizeof(double)) != cudaSuccess) return PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
@@ -515,10 +533,15 @@ PfSolveResult PfSolveServerAddOperator(PfSolveServer* s, int64_t M, const double
         for (int W = 1; W <= (R == 4 ? 1 : 4); W *= 2) {  // the shapes serve_rows picks for M <= 1024
             Shape sh;
             batch_shape(s, find_batch_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, PREC_MIXED), W, sh);
-            for (int prec : {PREC_DD, PREC_DD_F64MEM})
-                jw_shape(s, find_jw_variant(R, o.KL, o.KU, o.L.sv, LAY_REAL, LAY_REAL, 0, prec, 0), W, sh);
         }
     }
+    for (int64_t Mr : {(int64_t)64, (int64_t)256, (int64_t)768, (int64_t)1024})  // every dd variant and W
+        for (int prec : {PREC_DD, PREC_DD_F64MEM}) {
+            int W;
+            Shape sh;
+            const JwVariant* v = serve_dd_variant(Mr, o.KL, o.KU, o.L.sv, prec, W);
+            if (v) jw_shape(s, v, W, sh);
+        }
     std::lock_guard<std::mutex> lk(s->mu);
     s->ops.push_back(o);
     *opId = (int)s->ops.size() - 1;

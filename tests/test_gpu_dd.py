@@ -46,3 +46,38 @@ def test_dd_double_memory_config3():
     ref = O.jw_step(case, wl.jw_bands, wl.rhs, "q")
     e, _ = O.rel_errors(got, ref, case.M, case.batch, case.M)
     assert e <= 2e-16, e
+
+
+@pytest.mark.parametrize("rows", [0, 4, 8, 16])
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (0, 13), (1, 11)])
+@pytest.mark.parametrize("M", [200, 512, 1000])
+def test_dd_table_and_register_forms(ub, jwt, M, rows):
+    """Both forms of the double-double kernel on many systems per group (so
+    every group swaps its staging buffers several times): the table form
+    (coefficients, chunk products and scan multipliers built once per CTA in
+    shared memory; the default, 16 rows per thread for systems of up to 512
+    rows, else 8) and the register form (rowsPerThread 4), against the
+    __float128 oracle at 1e-27 relative L2 per system."""
+    from pfsolve_b200.api import App
+    import torch
+    rng = np.random.default_rng(4000 + 10 * ub + jwt + M + rows)
+    bands = WL.permute_bands(J.random_bands(rng, M, ub), M)
+    case = O.Case(M=M, batch=700, upperBanded=ub, jw_type=jwt)
+    rhs = rng.uniform(-1, 1, case.rhs_len())
+    bdd = O.to_dd(bands)
+    bdd[1::2] = bands * rng.uniform(-1, 1, bands.shape) * 2.0 ** -60
+    rdd = O.to_dd(rhs)
+    rdd[1::2] = rhs * rng.uniform(-1, 1, rhs.shape) * 2.0 ** -60
+    tb = torch.from_numpy(bdd).cuda()
+    to = torch.from_numpy(rdd.copy()).cuda()
+    app = App(buffer=tb, outputBuffer=to,
+              **J.case_fields(case, doublePrecision=0, quadDoubleDoublePrecision=1, rowsPerThread=rows))
+    want = rows if rows else (16 if M <= 512 else 8)
+    assert app.shape()["rowsPerThread"] == want, app.shape()
+    app.append(**J.launch_fields(case))
+    torch.cuda.synchronize()
+    got = to.cpu().numpy()
+    app.close()
+    ref = O.jw_step(case, bdd, rdd, "dd")
+    e, _ = O.rel_errors_dd(got, ref, case.M, case.batch, case.out_stride, case.offset_solution)
+    assert e <= 1e-27, e
