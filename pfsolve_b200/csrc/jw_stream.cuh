@@ -35,6 +35,12 @@
 
 namespace pfb {
 
+// Component e (0..3, a compile-time index after unrolling) of a float4.
+__device__ __forceinline__ float f4_at(const float4& v, int e)
+{
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
 constexpr unsigned kStatusWaitTimeout = 1u;
 static __device__ unsigned int g_stream_status;
 
@@ -70,11 +76,19 @@ struct StCfg {
     // FP64 / FP32: NB weights (scaled by the LU pivots), -l, -h, Scale factor.
     // Mixed: NB weights (unscaled), the solve's sub- and super-diagonal in FP64
     // (residual), FP32 packs {m, m', -l, -l'} and {-h, -h', 0, 0}, Scale factor.
-    static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0);  // FP64 path
+    // FP32 arithmetic, 16 or 32 rows per thread (QUAD): one float4 per (row
+    // quad, thread), and two more planes, the products of -l over the chunk's
+    // rows up to each row and of -h from each row on, so that a system's
+    // coupling terms cost one FMA a row.  (At 8 rows per thread the extra
+    // table loads measured slower than forming the products per system.)
+    static constexpr bool QUAD = F32 && R >= 16;
+    static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0);  // FP64 / FP32 path
     static constexpr int P_AL = NB, P_CU = NB + (FWD ? 1 : 0);  // mixed path
     static constexpr int P_F1 = P_CU + (BWD ? 1 : 0), P_F2 = P_F1 + 1;
-    static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0);
+    static constexpr int P_PL = P_NH + (BWD ? 1 : 0), P_PH = P_PL + ((QUAD && FWD) ? 1 : 0);  // QUAD
+    static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : (QUAD ? P_PH + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0));
     static constexpr int NPL = P_SC + (SCALE ? 1 : 0);
+    static constexpr int U4 = R / 4;  // QUAD: row quads per chunk
     // Table: U row pairs per chunk.
     static constexpr int U = R / 2;
     // Input: NPIN planes of ES-byte rows; a 16-byte unit holds EPU rows, a
@@ -116,6 +130,7 @@ struct StCfg {
     static constexpr int kMaxThreads =
         (kDataRegs >= 96 || (CPLX && kDataRegs >= 64)) ? 256 : (kDataRegs >= 64 ? 384 : 512);
     static_assert(R % 2 == 0 && R >= 4 && R <= 32, "rows per thread");
+    static_assert(!QUAD || R % 4 == 0, "FP32: whole row quads per chunk");
     static_assert(KLP <= 2 && KUP <= 2, "halo of at most two rows");
     static_assert(!ALT || (!CPLX && !MIXED && !SCALE && !F32MEM), "ALT: real FP64 systems without a Scale epilogue");
     static_assert(!MIXED || !F32MEM, "mixed precision: FP64 storage");
@@ -283,6 +298,18 @@ __device__ void st_prologue_system(const JwOperator& op, int h, typename C::CT* 
         auto put = [&](int p, double v) {
             table[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 2 + (jj & 1)] = (typename C::CT)v;
         };
+        if constexpr (C::QUAD) {  // float4 per (row quad, thread)
+            const int q4 = jj >> 2, e4 = jj & 3;
+            auto putq = [&](int p, double v) {
+                reinterpret_cast<float*>(table)[(((size_t)p * C::U4 + q4) * C::TP + tt) * 4 + e4] = (float)v;
+            };
+#pragma unroll
+            for (int k = 0; k < NB; ++k) putq(k, w[k]);
+            if constexpr (C::FWD) putq(C::P_NL, nl);
+            if constexpr (C::BWD) putq(C::P_NH, nh);
+            if constexpr (C::SCALE) putq(C::P_SC, sc);
+            continue;
+        }
         auto put32 = [&](int p, int k, double v) {
             reinterpret_cast<float*>(table)[(((size_t)p * U + (jj >> 1)) * C::TP + tt) * 4 + k + (jj & 1)] = (float)v;
         };
@@ -321,6 +348,31 @@ __device__ void st_prologue(const JwOperator& op, typename C::CT* table, double*
     g.scratch = scratch_all;
     if constexpr (!C::ALT) {
         st_prologue_system<C>(op, 0, table, g);
+        if constexpr (C::QUAD && (C::FWD || C::BWD)) {
+            // one thread per chunk: the products of -l up to each row and of
+            // -h from each row on, in the order the solve used to form them
+            __syncthreads();
+            float* tf = reinterpret_cast<float*>(table);
+            auto at = [&](int p, int j, int tt) -> float& {
+                return tf[(((size_t)p * C::U4 + (j >> 2)) * C::TP + tt) * 4 + (j & 3)];
+            };
+            for (int tt = threadIdx.x; tt < C::T; tt += blockDim.x) {
+                if constexpr (C::FWD) {
+                    float pr = 1.0f;
+                    for (int j = 0; j < C::R; ++j) {
+                        pr = at(C::P_NL, j, tt) * pr;
+                        at(C::P_PL, j, tt) = pr;
+                    }
+                }
+                if constexpr (C::BWD) {
+                    float pr = 1.0f;
+                    for (int j = C::R - 1; j >= 0; --j) {
+                        pr = at(C::P_NH, j, tt) * pr;
+                        at(C::P_PH, j, tt) = pr;
+                    }
+                }
+            }
+        }
     } else {
 #pragma unroll 1
         for (int h = 0; h < 2; ++h) {
@@ -463,7 +515,15 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
     // for the odd rows.
     CT Af = 1, Ab = 1, Af1 = 1, Ab1 = 1;
     float Af32 = 1.0f, Ab32 = 1.0f;
-    if constexpr (C::FWD && !C::MIXED) {
+    // QUAD: row quad q of plane p as a float4
+    auto coefq = [&](int p, int q) -> float4 {
+        return reinterpret_cast<const float4*>(table)[((size_t)p * C::U4 + q) * C::TP + t];
+    };
+    if constexpr (C::QUAD) {
+        if constexpr (C::FWD) Af = (CT)coefq(C::P_PL, C::U4 - 1).w;
+        if constexpr (C::BWD) Ab = (CT)coefq(C::P_PH, 0).x;
+    }
+    if constexpr (C::FWD && !C::MIXED && !C::QUAD) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const CT2 c = coef(C::P_NL, u);
@@ -476,7 +536,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             }
         }
     }
-    if constexpr (C::BWD && !C::MIXED) {
+    if constexpr (C::BWD && !C::MIXED && !C::QUAD) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const CT2 c = coef(C::P_NH, u);
@@ -612,18 +672,35 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         }
 
         // x = (V A b) scaled by the LU pivots, in place over be[0 .. R)
+        if constexpr (C::QUAD) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            CT2 wc[NB];
+            for (int q4 = 0; q4 < C::U4; ++q4) {
+                float4 wc[NB];
 #pragma unroll
-            for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+                for (int q = 0; q < NB; ++q) wc[q] = coefq(q, q4);
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int j = 2 * u + e;
-                V acc = O::mul(e ? wc[0].y : wc[0].x, be[j]);
+                for (int e = 0; e < 4; ++e) {
+                    const int j = 4 * q4 + e;
+                    V acc = O::mul(f4_at(wc[0], e), be[j]);
 #pragma unroll
-                for (int q = 1; q < NB; ++q) acc = O::fma(e ? wc[q].y : wc[q].x, be[j + S * q], acc);
-                be[j] = acc;
+                    for (int q = 1; q < NB; ++q) acc = O::fma(f4_at(wc[q], e), be[j + S * q], acc);
+                    be[j] = acc;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                CT2 wc[NB];
+#pragma unroll
+                for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int j = 2 * u + e;
+                    V acc = O::mul(e ? wc[0].y : wc[0].x, be[j]);
+#pragma unroll
+                    for (int q = 1; q < NB; ++q) acc = O::fma(e ? wc[q].y : wc[q].x, be[j + S * q], acc);
+                    be[j] = acc;
+                }
             }
         }
         V (&x)[R + KL + KU] = be;
@@ -762,7 +839,29 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 x[2 * u + 1] = O::fma(p1, pin1, x[2 * u + 1]);
             }
         }
-        if constexpr (C::FWD && !C::MIXED && !C::ALT) {
+        if constexpr (C::FWD && C::QUAD) {
+            // z_j = x_j - l_j z_{j-1} within the chunk, then the coupling from
+            // the preceding chunks times the stored product of -l up to row j
+#pragma unroll
+            for (int q4 = 0; q4 < C::U4; ++q4) {
+                const float4 c = coefq(C::P_NL, q4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int j = 4 * q4 + e;
+                    if (j > 0) x[j] = O::fma(f4_at(c, e), x[j - 1], x[j]);
+                }
+            }
+            V pin;
+            if constexpr (kPre) pin = group_affine_scan_pre<V, CT, true>(g, mf, x[R - 1]);
+            else pin = group_affine_scan<V, CT, true>(g, Af, x[R - 1]);
+#pragma unroll
+            for (int q4 = 0; q4 < C::U4; ++q4) {
+                const float4 pl = coefq(C::P_PL, q4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) x[4 * q4 + e] = O::fma(f4_at(pl, e), pin, x[4 * q4 + e]);
+            }
+        }
+        if constexpr (C::FWD && !C::MIXED && !C::ALT && !C::QUAD) {
             // z_j = x_j - l_j z_{j-1} within the chunk, then add the coupling
             // from the preceding chunks scaled by prod_{k<=j}(-l_k)
 #pragma unroll
@@ -803,7 +902,27 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
                 x[2 * u] = O::fma(p0, q0, x[2 * u]);
             }
         }
-        if constexpr (C::BWD && !C::MIXED && !C::ALT) {
+        if constexpr (C::BWD && C::QUAD) {
+#pragma unroll
+            for (int q4 = C::U4 - 1; q4 >= 0; --q4) {
+                const float4 c = coefq(C::P_NH, q4);
+#pragma unroll
+                for (int e = 3; e >= 0; --e) {
+                    const int j = 4 * q4 + e;
+                    if (j < R - 1) x[j] = O::fma(f4_at(c, e), x[j + 1], x[j]);
+                }
+            }
+            V q;
+            if constexpr (kPre) q = group_affine_scan_pre<V, CT, false>(g, mb, x[0]);
+            else q = group_affine_scan<V, CT, false>(g, Ab, x[0]);
+#pragma unroll
+            for (int q4 = 0; q4 < C::U4; ++q4) {
+                const float4 ph = coefq(C::P_PH, q4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) x[4 * q4 + e] = O::fma(f4_at(ph, e), q, x[4 * q4 + e]);
+            }
+        }
+        if constexpr (C::BWD && !C::MIXED && !C::ALT && !C::QUAD) {
 #pragma unroll
             for (int u = U - 1; u >= 0; --u) {
                 const CT2 c = coef(C::P_NH, u);
@@ -824,7 +943,15 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             }
         }
         if (C::SV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
-        if constexpr (C::SCALE) {
+        if constexpr (C::SCALE && C::QUAD) {
+#pragma unroll
+            for (int q4 = 0; q4 < C::U4; ++q4) {
+                const float4 c = coefq(C::P_SC, q4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) x[4 * q4 + e] = O::mul(f4_at(c, e), x[4 * q4 + e]);
+            }
+        }
+        if constexpr (C::SCALE && !C::QUAD) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const CT2 c = coef(C::P_SC, u);
