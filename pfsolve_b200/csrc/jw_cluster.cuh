@@ -34,7 +34,7 @@ namespace pfb {
 
 template <int R_, int W_, int C_, int KL_, int KU_, int SV_>
 struct ClCfg {
-    using B = StCfg<R_, W_, KL_, KU_, SV_, LAY_REAL, LAY_REAL, false, PREC_F64>;  // slice layout and table planes
+    using B = StCfg<R_, W_, KL_, KU_, SV_, LAY_REAL, LAY_REAL, false, PREC_F64, 0, 0>;  // slice layout and table planes
     static constexpr int C = C_;
     static constexpr int R = R_, W = W_, T = 32 * W_, S = T * R_;
     static constexpr int KL = KL_, KU = KU_, SV = SV_;

@@ -66,7 +66,7 @@ namespace pfb {
 
 template <int R_, int W_, int G_, int KL_, int KU_, int SV_>
 struct LgCfg {
-    using B = StCfg<R_, W_, KL_, KU_, SV_, LAY_REAL, LAY_REAL, false, PREC_F64>;  // slice layout and table planes
+    using B = StCfg<R_, W_, KL_, KU_, SV_, LAY_REAL, LAY_REAL, false, PREC_F64, 0, 0>;  // slice layout and table planes
     static constexpr int R = R_, W = W_, G = G_, T = 32 * W_, S = T * R_, NT = T * G_;
     static constexpr int KL = KL_, KU = KU_, SV = SV_;
 };

@@ -44,8 +44,10 @@ __device__ __forceinline__ float f4_at(const float4& v, int e)
 constexpr unsigned kStatusWaitTimeout = 1u;
 static __device__ unsigned int g_stream_status;
 
+// PRODS_: 0 leaves out the chunk-product planes (the long-system kernels use
+// this layout for their slice tables and form their products themselves).
 template <int R_, int W_, int KL_, int KU_, int SV_, int LIN_, int LOUT_, bool SCALE_, int PREC_ = PREC_F64,
-          int ALT_ = 0>
+          int ALT_ = 0, int PRODS_ = 1>
 struct StCfg {
     static constexpr int R = R_, W = W_, KL = KL_, KU = KU_, SV = SV_, LIN = LIN_, LOUT = LOUT_;
     static constexpr bool SCALE = SCALE_;
@@ -81,12 +83,18 @@ struct StCfg {
     // rows up to each row and of -h from each row on, so that a system's
     // coupling terms cost one FMA a row.  (At 8 rows per thread the extra
     // table loads measured slower than forming the products per system.)
-    static constexpr bool QUAD = F32 && R >= 16;
+    static constexpr bool QUAD = F32 && R >= 16 && PRODS_;
+    // FP64 storage and arithmetic, 16 or 32 rows per thread (PROD): the same
+    // two planes of chunk products, as row pairs (measured: config 3, N = 512,
+    // 0.197 -> 0.179 ms; on FP32 storage with FP64 arithmetic it measured
+    // slower at N = 512, so those variants keep the per-system products).
+    static constexpr bool PROD = PREC_ == PREC_F64 && !ALT_ && R >= 16 && PRODS_;
+    static constexpr bool PRODS = QUAD || PROD;
     static constexpr int P_NL = NB, P_NH = NB + (FWD ? 1 : 0);  // FP64 / FP32 path
     static constexpr int P_AL = NB, P_CU = NB + (FWD ? 1 : 0);  // mixed path
     static constexpr int P_F1 = P_CU + (BWD ? 1 : 0), P_F2 = P_F1 + 1;
-    static constexpr int P_PL = P_NH + (BWD ? 1 : 0), P_PH = P_PL + ((QUAD && FWD) ? 1 : 0);  // QUAD
-    static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : (QUAD ? P_PH + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0));
+    static constexpr int P_PL = P_NH + (BWD ? 1 : 0), P_PH = P_PL + ((PRODS && FWD) ? 1 : 0);  // QUAD / PROD
+    static constexpr int P_SC = MIXED ? P_F2 + (BWD ? 1 : 0) : (PRODS ? P_PH + (BWD ? 1 : 0) : P_NH + (BWD ? 1 : 0));
     static constexpr int NPL = P_SC + (SCALE ? 1 : 0);
     static constexpr int U4 = R / 4;  // QUAD: row quads per chunk
     // Table: U row pairs per chunk.
@@ -348,6 +356,30 @@ __device__ void st_prologue(const JwOperator& op, typename C::CT* table, double*
     g.scratch = scratch_all;
     if constexpr (!C::ALT) {
         st_prologue_system<C>(op, 0, table, g);
+        if constexpr (C::PROD && (C::FWD || C::BWD)) {
+            // one thread per chunk: the products of -l up to each row and of
+            // -h from each row on, in the order the solve used to form them
+            __syncthreads();
+            auto at = [&](int p, int j, int tt) -> double& {
+                return table[(((size_t)p * C::U + (j >> 1)) * C::TP + tt) * 2 + (j & 1)];
+            };
+            for (int tt = threadIdx.x; tt < C::T; tt += blockDim.x) {
+                if constexpr (C::FWD) {
+                    double pr = 1.0;
+                    for (int j = 0; j < C::R; ++j) {
+                        pr = at(C::P_NL, j, tt) * pr;
+                        at(C::P_PL, j, tt) = pr;
+                    }
+                }
+                if constexpr (C::BWD) {
+                    double pr = 1.0;
+                    for (int j = C::R - 1; j >= 0; --j) {
+                        pr = at(C::P_NH, j, tt) * pr;
+                        at(C::P_PH, j, tt) = pr;
+                    }
+                }
+            }
+        }
         if constexpr (C::QUAD && (C::FWD || C::BWD)) {
             // one thread per chunk: the products of -l up to each row and of
             // -h from each row on, in the order the solve used to form them
@@ -523,7 +555,11 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
         if constexpr (C::FWD) Af = (CT)coefq(C::P_PL, C::U4 - 1).w;
         if constexpr (C::BWD) Ab = (CT)coefq(C::P_PH, 0).x;
     }
-    if constexpr (C::FWD && !C::MIXED && !C::QUAD) {
+    if constexpr (C::PROD) {
+        if constexpr (C::FWD) Af = coef(C::P_PL, U - 1).y;
+        if constexpr (C::BWD) Ab = coef(C::P_PH, 0).x;
+    }
+    if constexpr (C::FWD && !C::MIXED && !C::QUAD && !C::PROD) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const CT2 c = coef(C::P_NL, u);
@@ -536,7 +572,7 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             }
         }
     }
-    if constexpr (C::BWD && !C::MIXED && !C::QUAD) {
+    if constexpr (C::BWD && !C::MIXED && !C::QUAD && !C::PROD) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const CT2 c = coef(C::P_NH, u);
@@ -873,14 +909,23 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             V pin;
             if constexpr (kPre) pin = group_affine_scan_pre<V, CT, true>(g, mf, x[R - 1]);
             else pin = group_affine_scan<V, CT, true>(g, Af, x[R - 1]);
-            CT p = 1;
+            if constexpr (C::PROD) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const CT2 c = coef(C::P_NL, u);
-                p = c.x * p;
-                x[2 * u] = O::fma(p, pin, x[2 * u]);
-                p = c.y * p;
-                x[2 * u + 1] = O::fma(p, pin, x[2 * u + 1]);
+                for (int u = 0; u < U; ++u) {
+                    const CT2 pl = coef(C::P_PL, u);
+                    x[2 * u] = O::fma(pl.x, pin, x[2 * u]);
+                    x[2 * u + 1] = O::fma(pl.y, pin, x[2 * u + 1]);
+                }
+            } else {
+                CT p = 1;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const CT2 c = coef(C::P_NL, u);
+                    p = c.x * p;
+                    x[2 * u] = O::fma(p, pin, x[2 * u]);
+                    p = c.y * p;
+                    x[2 * u + 1] = O::fma(p, pin, x[2 * u + 1]);
+                }
             }
         }
         if constexpr (C::BWD && !C::MIXED && C::ALT) {
@@ -932,14 +977,23 @@ __global__ void __launch_bounds__(C::kMaxThreads) jw_stream_kernel(const __grid_
             V q;
             if constexpr (kPre) q = group_affine_scan_pre<V, CT, false>(g, mb, x[0]);
             else q = group_affine_scan<V, CT, false>(g, Ab, x[0]);
-            CT p = 1;
+            if constexpr (C::PROD) {
 #pragma unroll
-            for (int u = U - 1; u >= 0; --u) {
-                const CT2 c = coef(C::P_NH, u);
-                p = c.y * p;
-                x[2 * u + 1] = O::fma(p, q, x[2 * u + 1]);
-                p = c.x * p;
-                x[2 * u] = O::fma(p, q, x[2 * u]);
+                for (int u = 0; u < U; ++u) {
+                    const CT2 ph = coef(C::P_PH, u);
+                    x[2 * u] = O::fma(ph.x, q, x[2 * u]);
+                    x[2 * u + 1] = O::fma(ph.y, q, x[2 * u + 1]);
+                }
+            } else {
+                CT p = 1;
+#pragma unroll
+                for (int u = U - 1; u >= 0; --u) {
+                    const CT2 c = coef(C::P_NH, u);
+                    p = c.y * p;
+                    x[2 * u + 1] = O::fma(p, q, x[2 * u + 1]);
+                    p = c.x * p;
+                    x[2 * u] = O::fma(p, q, x[2 * u]);
+                }
             }
         }
         if (C::SV != SV_NONE && s == 0) x[0] = O::mul(op.scaleC, x[0]);
