@@ -254,9 +254,9 @@ def gpu_arm(args, rank, world):
     achieved = bytes_alg / (ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
     # DRAM bytes (read + write) of one full-size launch of this kernel, from a
-    # single-pass ncu capture of this command (dram__bytes_read.sum +
-    # dram__bytes_write.sum = 1.07 + 1.02 GB); the output tail still in L2 at
-    # kernel end makes it slightly below the algorithmic bytes.
+    # single-pass ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) at
+    # 32768 systems scaled to 65536 (reads in proportion: 1.074 GB; writes the
+    # same less the output tail still in L2 at kernel end: ~1.02 GB).
     traffic = 2.09e9 if (nc == N_CPLX and jw.shape()["streaming"] == 1) else None
 
     # ---- e2e through the C ABI with host buffers (pinned), copies inside the timed region
