@@ -476,6 +476,9 @@ def extras_arm(args):
     out["long_t13_N16384_B8192_single_pass"] = long_measure(16384, 8192, path=4)
     out["long_t13_N65536_B2048"] = long_measure(65536, 2048)
     out["long_t13_N20000_B6553"] = long_measure(20000, 6553)
+    out["dct2_N512_B131072"] = dct_measure(512, 131072, 2)
+    out["dct3_N512_B131072"] = dct_measure(512, 131072, 3)
+    out["dct2_N4096_B16384"] = dct_measure(4096, 16384, 2)
     out["alt_t113_N1024_B131072"] = alt_measure(1024, 131072)
     out["alt_t113_N1024_B131072_group"] = alt_measure(1024, 131072, path=1)
     torch.cuda.empty_cache()
@@ -673,6 +676,32 @@ def long_measure(M, B, steps=10, warmup=3, path=0):
             "kernel": shape}
 
 
+def dct_measure(N, B, dct_type=2, steps=10, warmup=3):
+    """The DCT step (performDCT 2 or 3): B rows of N points, FP64, out of
+    place; algorithmic bytes: each row read once and written once."""
+    import torch
+
+    from pfsolve_b200.api import App
+    rng = np.random.default_rng(5)
+    x = torch.from_numpy(rng.standard_normal(N * B)).cuda()
+    y = torch.empty_like(x)
+    app = App(buffer=x, outputBuffer=y, FFTdim=1, size=(N, B), performDCT=dct_type, doublePrecision=1)
+    for _ in range(max(1, warmup)):
+        app.append()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        app.append()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    app.close()
+    del x, y
+    return {"N": N, "rows": B, "type": dct_type, "ms": ms, "rows_per_s": B / (ms * 1e-3),
+            "gbs": 2.0 * N * 8 * B / (ms * 1e-3) / 1e9}
+
+
 def alt_measure(M, B, steps=10, warmup=3, path=0):
     """ALT stride-2 mode (jw_type 113: the even and the odd rows of each row
     set are two tridiagonal systems), M rows per row set, B real row sets in
@@ -840,7 +869,8 @@ def main():
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "ksteps", "dd", "alt"],
+    ap.add_argument("--workload", default="config2",
+                    choices=["config2", "config3", "config4", "ksteps", "dd", "alt", "dct"],
                     help="profiling case (--profile): the config 2 chain, config 3 (--ncplx real systems), "
                          "config 4 (degrees 0..--lmax), K steps, config 3's system in double-double, or ALT mode "
                          "(--m rows per row set, --ncplx row sets)")
@@ -879,6 +909,10 @@ def main():
         return
     if args.profile and args.workload == "ksteps":
         steps_profile(args)
+        return
+    if args.profile and args.workload == "dct":
+        print(json.dumps(dict(profile_case="dct", **dct_measure(args.m, args.ncplx, 2 if args.refine == 0 else 3,
+                                                                 steps=args.steps, warmup=args.warmup))), flush=True)
         return
     if args.profile and args.workload == "alt":
         print(json.dumps(alt_measure(args.m, args.ncplx, steps=args.steps, warmup=args.warmup, path=args.path)),

@@ -206,6 +206,12 @@ typedef struct {
     int ALT_dgbmv;        /* dgbmv: drop alternate bands by the reference's rule (pfSolve_Plan_dgbmv.h:100,
                              pfSolve_MatVecMul.h:390); LDA <= 64, not with double-double */
     uint64_t Msplit[3];   /* multi-upload split (accepted, single upload used for M <= 4352) */
+    uint64_t performDCT;  /* 2 or 3 selects the DCT application (pfSolve_Structs.h:272): the radial DCT
+                             step that feeds the JW chain, DCT-II or DCT-III (FFTW's unnormalized
+                             REDFT10 / REDFT01) of size[1]*size[2] rows of size[0] = 2^p points,
+                             8 <= size[0] <= 4096, FP64 (doublePrecision); rows are read from buffer at
+                             inputBufferStride[0] and written to outputBuffer (or in place to buffer
+                             when outputBuffer is NULL) at outputBufferStride[0] (0: size[0]) */
 
     int64_t jw_control_bitmask; /* RUNTIME_* bits */
     int64_t M_size;
@@ -504,7 +510,8 @@ enum {
     PFSOLVE_KERNEL_STEPS = 5,     /* jw_steps_kernel: K consecutive steps */
     PFSOLVE_KERNEL_STEPS_SWEEP = 6, /* jw_steps_seq_kernel: K bidiagonal steps, one system per lane */
     PFSOLVE_KERNEL_DGBMV = 7,     /* dgbmv_generic_kernel: band matrices wider than two bands a side */
-    PFSOLVE_KERNEL_BLOCK = 8      /* block_kernel */
+    PFSOLVE_KERNEL_BLOCK = 8,     /* block_kernel */
+    PFSOLVE_KERNEL_DCT = 9        /* dct_kernel: the DCT step (performDCT 2 or 3) */
 };
 typedef struct {
     int kernel;         /* PFSOLVE_KERNEL_* */

@@ -754,3 +754,33 @@ void pfo_rel_errors_dd(const double* a, const double* ref, int64_t M, int64_t ba
     *rel_l2_max = worst;
     *rel_max = (rmax > 0) ? dmax / rmax : dmax;
 }
+
+/* ---- DCT step (see jw_oracle.h). */
+int pfo_dct_q(int type, int64_t N, int64_t nsys, const double* in, int64_t in_stride, double* out,
+              int64_t out_stride, int nthreads)
+{
+    if ((type != 2 && type != 3) || N < 1) return -1;
+    /* c[j] = cos(pi j / (2N)), j in [0, 4N) */
+    q_t* c = (q_t*)malloc(sizeof(q_t) * 4 * N);
+    if (!c) return -1;
+    const q_t pi = M_PIq;
+    for (int64_t j = 0; j < 4 * N; j++) c[j] = cosq(pi * (q_t)j / (q_t)(2 * N));
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static)
+    for (int64_t y = 0; y < nsys; y++) {
+        const double* x = in + y * in_stride;
+        double* X = out + y * out_stride;
+        for (int64_t k = 0; k < N; k++) {
+            q_t acc = 0;
+            if (type == 2) {
+                for (int64_t n = 0; n < N; n++) acc += (q_t)x[n] * c[(k * (2 * n + 1)) % (4 * N)];
+                acc *= 2;
+            } else {
+                for (int64_t n = 1; n < N; n++) acc += (q_t)x[n] * c[(n * (2 * k + 1)) % (4 * N)];
+                acc = 2 * acc + (q_t)x[0];
+            }
+            X[k] = (double)acc;
+        }
+    }
+    free(c);
+    return 0;
+}

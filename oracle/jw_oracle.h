@@ -145,6 +145,19 @@ void pfo_rel_errors(const double* a, const double* ref, int64_t M, int64_t batch
 void pfo_rel_errors_dd(const double* a, const double* ref, int64_t M, int64_t batch, int64_t stride,
                        int64_t offset, double* rel_l2_max, double* rel_max);
 
+/* The radial DCT step that feeds the JW chain, batched over rows of N points:
+ * type 2 (REDFT10) or 3 (REDFT01) in FFTW's unnormalized definitions,
+ *   type 2: X_k = 2 sum_{n=0}^{N-1} x_n cos(pi k (2n+1) / (2N)),
+ *   type 3: X_k = x_0 + 2 sum_{n=1}^{N-1} x_n cos(pi n (2k+1) / (2N)),
+ * so that type 3 applied to type 2 is 2N times the identity.  PfSolve carries
+ * the selector (PfSolveConfiguration.performDCT, pfSolve_Structs.h:272) from the
+ * VkFFT it grew out of; the transform itself is VkFFT's, which follows FFTW's
+ * definitions.  Direct O(N^2) sums in __float128, the angles reduced exactly
+ * modulo 4N.  Row y is read at in + y*in_stride and written at out +
+ * y*out_stride (out of place).  Returns 0, or -1 for a type other than 2, 3. */
+int pfo_dct_q(int type, int64_t N, int64_t nsys, const double* in, int64_t in_stride, double* out,
+              int64_t out_stride, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -196,6 +196,9 @@ def lib():
     L.pfo_steps_registers.restype = ctypes.c_int64
     L.pfo_jw_steps_layout.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Step)]
     L.pfo_jw_steps_layout.restype = ctypes.c_int
+    L.pfo_dct_q.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, dp, ctypes.c_int64, dp, ctypes.c_int64,
+                            ctypes.c_int]
+    L.pfo_dct_q.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -414,3 +417,17 @@ def run_reference(case_dir: str, timeout: float = 120.0):
     if os.path.exists(tp):
         t = float(open(tp).read().strip())
     return os.path.join(case_dir, "out.bin"), t
+
+
+def dct(dct_type: int, x: np.ndarray, N: int, nsys: int, in_stride: int = 0, out_stride: int = 0,
+        nthreads: int = 4) -> np.ndarray:
+    """The DCT step (type 2 or 3, FFTW's unnormalized REDFT10 / REDFT01) of
+    nsys rows of N points, in __float128 (pfo_dct_q); rows at in_stride
+    (default N), results packed at out_stride (default N)."""
+    in_stride = in_stride or N
+    out_stride = out_stride or N
+    xi = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(max(1, (nsys - 1) * out_stride + N))
+    if lib().pfo_dct_q(int(dct_type), N, nsys, _dptr(xi), in_stride, _dptr(out), out_stride, nthreads) != 0:
+        raise ValueError("DCT type must be 2 or 3")
+    return out

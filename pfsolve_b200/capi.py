@@ -41,6 +41,7 @@ PFSOLVE_ERROR_INVALID_DEVICE = 1002
 PFSOLVE_ERROR_EMPTY_FFTdim = 2001
 PFSOLVE_ERROR_EMPTY_size = 2002
 PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH = 3002
+PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_DCT = 3004
 PFSOLVE_ERROR_UNSUPPORTED_COMBINATION = 5001
 PFSOLVE_ERROR_INVALID_ARGUMENT = 5002
 PFSOLVE_ERROR_CAPACITY = 5003
@@ -60,7 +61,7 @@ class PfSolveConfiguration(ctypes.Structure):
         ("buffer", vpp), ("outputBuffer", vpp), ("kernel", vpp),
         ("upperBanded", c_int), ("jw_type", c_int), ("block", c_int), ("lshift", c_int),
         ("LDA", c_int), ("KU", c_int), ("KL", c_int), ("ALT_dgbmv", c_int),
-        ("Msplit", u64 * 3),
+        ("Msplit", u64 * 3), ("performDCT", u64),
         ("jw_control_bitmask", i64), ("M_size", i64), ("offsetM", i64), ("offsetV", i64),
         ("offsetSolution", i64), ("inputZeropad", i64 * 2), ("outputZeropad", i64 * 2),
         ("scaleC", ctypes.c_double),
@@ -135,7 +136,7 @@ class PfSolveLaunchInfo(ctypes.Structure):
 
 PFSOLVE_KERNEL_NONE, PFSOLVE_KERNEL_GROUP, PFSOLVE_KERNEL_STREAMING, PFSOLVE_KERNEL_LONG = 0, 1, 2, 3
 PFSOLVE_KERNEL_CLUSTER, PFSOLVE_KERNEL_STEPS, PFSOLVE_KERNEL_STEPS_SWEEP = 4, 5, 6
-PFSOLVE_KERNEL_DGBMV, PFSOLVE_KERNEL_BLOCK = 7, 8
+PFSOLVE_KERNEL_DGBMV, PFSOLVE_KERNEL_BLOCK, PFSOLVE_KERNEL_DCT = 7, 8, 9
 
 
 class PfSolveServerStats(ctypes.Structure):

@@ -27,7 +27,7 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 std::atomic<uint64_t> g_stream_launches{0};
 
-enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3 };
+enum AppKind { APP_JW = 1, APP_DGBMV = 2, APP_BLOCK = 3, APP_DCT = 4 };
 
 constexpr int64_t kMaxRows = 4096;       // one CTA group per system (<= 8 warps x 32 x 16 rows)
 constexpr int64_t kMaxRowsLong = 65536;  // JW apps: up to 64 slices of 1024 rows per system (single pass)
@@ -57,6 +57,8 @@ struct AppState {
     double* long_red = nullptr;  // per (system, slice) records, then per-slice constants
     unsigned* long_flags = nullptr;  // single pass: per (system, slice) publication flags
     unsigned long_epoch = 0;         // single pass: flag value of the latest launch
+    double2* dct_tables = nullptr;   // DCT step: twiddles, then pre/post factors (2N values)
+    int dct_logn = 0;
     bool long_single = false;        // the plan's form: single pass, else pass 1, carries, pass 2
     int long_mode = 0;               // kernelPath: 0 two passes where M allows (else single), 3 two, 4 single
     const LongVariant* long_v_fb = nullptr;  // single-pass fallback for rows no tensor map describes
@@ -976,6 +978,51 @@ PfSolveResult append_block(PfSolveApplication* app, const PfSolveLaunchParams* l
     return PFSOLVE_SUCCESS;
 }
 
+// The DCT step: rows from `buffer` (launch-time buffer first) at the input
+// stride, results to `outputBuffer`, or in place when there is none.  Runtime
+// input / output strides and offsets follow the same RUNTIME_* bits as the
+// other applications (offsetM: input rows, offsetSolution: output rows).
+PfSolveResult append_dct(PfSolveApplication* app, const PfSolveLaunchParams* lp, cudaStream_t stream)
+{
+    AppState* s = st(app);
+    PfSolveConfiguration& c = app->configuration;
+    const int64_t bm = c.jw_control_bitmask;
+    if (lp && lp->batchSize > 0) c.size[1] = lp->batchSize;  // persists, as in the reference
+    void* in = (lp && lp->buffer) ? lp->buffer[0] : (c.buffer ? c.buffer[0] : nullptr);
+    void* out = (lp && lp->outputBuffer) ? lp->outputBuffer[0] : (c.outputBuffer ? c.outputBuffer[0] : nullptr);
+    if (!in) return PFSOLVE_ERROR_EMPTY_buffer;
+    if (!out) out = in;
+    auto pick = [&](int64_t bit, int64_t cfgv, uint64_t runv) -> int64_t {
+        return (bm & bit) ? (lp ? (int64_t)runv : 0) : cfgv;
+    };
+    const int64_t N = (int64_t)c.size[0];
+    DctIO io;
+    io.in = static_cast<const double*>(in);
+    io.out = static_cast<double*>(out);
+    io.in_off = pick(RUNTIME_OFFSETM, c.offsetM, lp ? lp->offsetM : 0);
+    io.out_off = pick(RUNTIME_OFFSETSOLUTION, c.offsetSolution, lp ? lp->offsetSolution : 0);
+    io.in_stride = pick(RUNTIME_INPUTBUFFERSTRIDE, (int64_t)c.inputBufferStride[0], lp ? lp->inputBufferStride : 0);
+    io.out_stride =
+        pick(RUNTIME_OUTPUTBUFFERSTRIDE, (int64_t)c.outputBufferStride[0], lp ? lp->outputBufferStride : 0);
+    if (io.in_stride == 0) io.in_stride = N;
+    if (io.out_stride == 0) io.out_stride = N;
+    if (io.in_stride < N || io.out_stride < N || io.in_off < 0 || io.out_off < 0) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    io.nsys = (int64_t)c.size[1] * (int64_t)(c.size[2] ? c.size[2] : 1);
+    if (io.nsys <= 0) return PFSOLVE_SUCCESS;
+    // in place needs each row's input and output at the same place
+    if (out == in && (io.in_off != io.out_off || io.in_stride != io.out_stride)) return PFSOLVE_ERROR_INVALID_ARGUMENT;
+    const double2* tw = s->dct_tables;
+    const double2* pt = s->dct_tables + N;
+    const cudaError_t e = dct_launch(s->dct_logn, (int)c.performDCT, io, tw, pt, s->num_sms, stream);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    record_launch(PFSOLVE_KERNEL_DCT, 0, 0, 0, 0, 0, SV_NONE, 0, 0, 0, PREC_F64, 0, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return PFSOLVE_ERROR_FAILED_TO_LAUNCH_KERNEL;
+    }
+    return PFSOLVE_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1201,7 +1248,25 @@ PfSolveResult initializePfSolve(PfSolveApplication* app, PfSolveConfiguration cf
                           : c.doublePrecisionFloatMemory ? PREC_F64_F32MEM
                                                          : PREC_F32;
     PfSolveResult r = PFSOLVE_SUCCESS;
-    if (c.jw_type >= 10) {
+    if (c.performDCT) {
+        // the DCT step: rows of N = 2^p points, FP64
+        s->kind = APP_DCT;
+        const int64_t N = (int64_t)c.size[0];
+        int logn = 0;
+        while ((int64_t)1 << logn < N) ++logn;
+        if (c.performDCT != 2 && c.performDCT != 3) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (c.FFTdim != 1 || N < 8 || N > 4096 || ((int64_t)1 << logn) != N)
+            r = PFSOLVE_ERROR_UNSUPPORTED_FFT_LENGTH_DCT;
+        else if (base_prec != PREC_F64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
+        else if (dct_tables(N, &s->dct_tables) != cudaSuccess) {
+            cudaGetLastError();
+            s->dct_tables = nullptr;
+            r = PFSOLVE_ERROR_FAILED_TO_ALLOCATE;
+        } else {
+            s->dct_logn = logn;
+            s->prec = PREC_F64;
+        }
+    } else if (c.jw_type >= 10) {
         s->kind = APP_JW;
         if (c.mixedPrecisionRefinement < 0 || c.mixedPrecisionRefinement > 3) r = PFSOLVE_ERROR_INVALID_ARGUMENT;
         else if (c.mixedPrecisionRefinement && base_prec != PREC_F64) r = PFSOLVE_ERROR_UNSUPPORTED_COMBINATION;
@@ -1290,6 +1355,7 @@ PfSolveResult PfSolveAppend(PfSolveApplication* app, int inverse, PfSolveLaunchP
     case APP_JW: r = append_jw(app, launchParams, stream); break;
     case APP_DGBMV: r = append_dgbmv(app, launchParams, stream); break;
     case APP_BLOCK: r = append_block(app, launchParams, stream); break;
+    case APP_DCT: r = append_dct(app, launchParams, stream); break;
     default: r = PFSOLVE_ERROR_PLAN_NOT_INITIALIZED;
     }
     if (r == PFSOLVE_SUCCESS) record_stream_event(app, stream);
@@ -1327,6 +1393,7 @@ void deletePfSolve(PfSolveApplication* app)
             delete[] s->events;
         }
         if (s->long_red) cudaFree(s->long_red);
+        if (s->dct_tables) cudaFree(s->dct_tables);
         delete s;
     }
     app->internal = nullptr;

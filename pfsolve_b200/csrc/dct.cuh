@@ -1,0 +1,235 @@
+// dct.cuh -- the radial DCT step that feeds the JW chain: batched real DCT-II
+// and DCT-III of rows of N = 2^p points (8 <= N <= 4096), FP64.
+//
+// Definitions (FFTW's unnormalized REDFT10 / REDFT01, which the VkFFT that
+// PfSolve carries performDCT from follows; pfSolve_Structs.h:272):
+//   type 2: X_k = 2 sum_{n} x_n cos(pi k (2n+1) / (2N))
+//   type 3: x_k = X_0 + 2 sum_{n>=1} X_n cos(pi n (2k+1) / (2N))
+// Both run as one complex N-point FFT per row (Makhoul, IEEE TASSP 28 (1980)):
+//   type 2: v = (x_0, x_2, ..., x_{N-2}, x_{N-1}, ..., x_3, x_1), V = FFT(v),
+//           X_k = 2 Re(e^{-i pi k/2N} V_k);
+//   type 3: z_k = e^{-i pi k/2N} (X_k + i X_{N-k}) (X_N = 0), Z = FFT(z),
+//           x_{2n} = Re Z_n, x_{2n+1} = Re Z_{N-1-n}
+// (type 3 is the inverse transform of the conjugate sequence; the real part
+// of the conjugate is that of Z).
+//
+// The FFT is Stockham's self-sorting form in shared memory, in place (each
+// stage reads, synchronises, writes): radix-8 stages, then one radix-4 or
+// radix-2 stage when log2 N is not a multiple of 3; every thread does one
+// radix-8 butterfly per stage (N/8 threads per row), and a CTA holds as many
+// rows as 256 threads cover.  Each thread loads the next row's inputs into
+// registers while the current row is transformed.  Twiddles e^{-2 pi i j/N} and the
+// pre/post factors (cos, sin)(pi k/2N) come from tables the plan computes once
+// in long double on the host.  Rows are read and written with coalesced
+// global accesses; a row is fully staged before its result is written, so
+// the transform may run in place.  The step is bound by HBM bandwidth at
+// large batches (16 bytes moved per point, in and out).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "jw_types.h"
+
+namespace pfb {
+
+template <int LOGN>
+struct DctShape {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int TPS = N >= 8 ? N / 8 : 1;    // threads per row
+    static constexpr int NT = TPS > 256 ? TPS : 256;  // threads per CTA
+    static constexpr int SPC = NT / TPS;              // rows per CTA round
+    static constexpr int L8 = LOGN / 3;               // radix-8 stages
+    static constexpr int REM = LOGN % 3;              // then one radix-2 (1) or radix-4 (2) stage
+    static constexpr int NP = N + N / 8;  // the buffer, one 16-byte pad after every 8 values
+    // one buffer of N complex values per row, then the twiddles (N values)
+    static constexpr size_t SMEM = ((size_t)SPC * NP + N) * 16;
+};
+
+__device__ __forceinline__ double2 dct_cmul(double2 a, double2 b)
+{
+    return make_double2(__fma_rn(a.x, b.x, -a.y * b.y), __fma_rn(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 dct_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 dct_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// times -i
+__device__ __forceinline__ double2 dct_mi(double2 a) { return make_double2(a.y, -a.x); }
+
+template <int R>
+__device__ __forceinline__ void dct_dft(double2 (&a)[R]);
+
+template <>
+__device__ __forceinline__ void dct_dft<2>(double2 (&a)[2])
+{
+    const double2 t = a[0];
+    a[0] = dct_add(t, a[1]);
+    a[1] = dct_sub(t, a[1]);
+}
+
+template <>
+__device__ __forceinline__ void dct_dft<4>(double2 (&a)[4])
+{
+    const double2 t0 = dct_add(a[0], a[2]), t1 = dct_sub(a[0], a[2]);
+    const double2 t2 = dct_add(a[1], a[3]), t3 = dct_mi(dct_sub(a[1], a[3]));
+    a[0] = dct_add(t0, t2);
+    a[1] = dct_add(t1, t3);
+    a[2] = dct_sub(t0, t2);
+    a[3] = dct_sub(t1, t3);
+}
+
+// Radix 8 by one decimation-in-frequency step into two radix-4 transforms:
+// the first gives the even outputs, the second (after the e^{-2 pi i r/8}
+// twiddles) the odd ones.
+template <>
+__device__ __forceinline__ void dct_dft<8>(double2 (&a)[8])
+{
+    constexpr double h = 0.70710678118654752440;  // sqrt(2)/2
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const double2 t = a[r];
+        a[r] = dct_add(t, a[r + 4]);
+        a[r + 4] = dct_sub(t, a[r + 4]);
+    }
+    a[5] = make_double2(h * (a[5].x + a[5].y), h * (a[5].y - a[5].x));    // e^{-i pi/4}
+    a[6] = dct_mi(a[6]);                                                  // e^{-i pi/2}
+    a[7] = make_double2(h * (a[7].y - a[7].x), -h * (a[7].x + a[7].y));   // e^{-3 i pi/4}
+    double2 f[4] = {a[0], a[1], a[2], a[3]}, g[4] = {a[4], a[5], a[6], a[7]};
+    dct_dft<4>(f);
+    dct_dft<4>(g);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        a[2 * m] = f[m];
+        a[2 * m + 1] = g[m];
+    }
+}
+
+// Position of value i in a row's buffer: one 16-byte pad after every 8 values,
+// so that a first-stage butterfly's 8 consecutive outputs (thread b writes
+// 8b .. 8b+7) fall on different banks from its neighbours'.
+__device__ __forceinline__ int dct_pad(int i) { return i + (i >> 3); }
+
+// One Stockham stage of radix R over N points with Ns points already
+// transformed per sub-sequence, in place: butterfly b reads buf[b + r N/R],
+// twiddles by e^{-2 pi i r k/(Ns R)} (k = b mod Ns), and, once every thread
+// of the row has read (`sync`), writes buf[(b - k) R + k + r Ns].
+template <int R, int N, int TPS, class SY>
+__device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const double2* tw, SY sync)
+{
+    constexpr int NBF = N / R, NB = NBF / TPS;
+    double2 a[NB][R];
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[i][r] = buf[dct_pad(j + i * TPS + r * NBF)];
+    sync();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const int b = j + i * TPS;
+        const int k = b & (Ns - 1);
+        if (Ns > 1) {
+            // w^r for r = 1 .. R-1 from w = e^{-2 pi i k/(Ns R)} (one table
+            // value, then products: the error grows by about an ulp a factor)
+            double2 wr[R];
+            wr[1] = tw[k * (N / (Ns * R))];
+#pragma unroll
+            for (int r = 2; r < R; ++r) wr[r] = dct_cmul(wr[r / 2], wr[r - r / 2]);
+#pragma unroll
+            for (int r = 1; r < R; ++r) a[i][r] = dct_cmul(a[i][r], wr[r]);
+        }
+        dct_dft<R>(a[i]);
+        const int base = (b - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[dct_pad(base + r * Ns)] = a[i][r];
+    }
+    sync();
+}
+
+// tw[j] = e^{-2 pi i j/N} (j < N); pt[k] = (cos, sin)(pi k/(2N)) (k < N).
+// One buffer of N complex values per row; each thread keeps the next row's
+// N/TPS input values in registers, loaded while the current row is
+// transformed.
+template <int LOGN, int TYPE>
+__global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 ? 3 : 1) dct_kernel(const DctIO io, const double2* __restrict__ tw,
+                                                                 const double2* __restrict__ pt)
+{
+    using S = DctShape<LOGN>;
+    constexpr int N = S::N, TPS = S::TPS, PER = N / TPS;
+    extern __shared__ __align__(16) double2 dct_smem[];
+    const int s = threadIdx.x / TPS, j = threadIdx.x - s * TPS;
+    double2* buf = dct_smem + (size_t)s * S::NP;
+    double2* tws = dct_smem + (size_t)S::SPC * S::NP;  // the twiddles, shared by the CTA's rows
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+    __syncthreads();
+    // Makhoul's order: input point e sits at position perm(e) of the sequence
+    auto perm = [](int e) { return (e & 1) ? N - 1 - (e >> 1) : (e >> 1); };
+    // The threads of one row synchronise among themselves only: a warp (rows
+    // of up to 256 points share warps, and keep in step), else a named
+    // barrier per row (ids 1..SPC).
+    auto sync = [&]() {
+        if constexpr (TPS <= 32) __syncwarp();
+        else asm volatile("bar.sync %0, %1;\n" ::"r"(1 + s), "r"(TPS) : "memory");
+    };
+    const int64_t stride_rows = (int64_t)gridDim.x * S::SPC;
+    double pre[PER];
+    auto fetch = [&](int64_t y) {
+        const bool live = y < io.nsys;
+        const double* x = io.in + io.in_off + (live ? y : 0) * io.in_stride;
+#pragma unroll
+        for (int i = 0; i < PER; ++i) pre[i] = live ? x[j + i * TPS] : 0.0;
+    };
+    int64_t y = (int64_t)blockIdx.x * S::SPC + s;
+    fetch(y);
+    for (int64_t base = (int64_t)blockIdx.x * S::SPC; base < io.nsys; base += stride_rows, y += stride_rows) {
+        const bool live = y < io.nsys;
+        if constexpr (TYPE == 2) {
+#pragma unroll
+            for (int i = 0; i < PER; ++i) buf[dct_pad(perm(j + i * TPS))] = make_double2(pre[i], 0.0);
+        } else {
+#pragma unroll
+            for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)].x = pre[i];
+            sync();
+            double Xr[PER];
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int k = j + i * TPS;
+                Xr[i] = (k == 0) ? 0.0 : buf[dct_pad(N - k)].x;
+            }
+            sync();
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int k = j + i * TPS;
+                const double Xk = pre[i];
+                const double2 c = __ldg(&pt[k]);
+                // e^{-i t} (Xk + i Xr) = (Xk cos t + Xr sin t) + i (Xr cos t - Xk sin t)
+                buf[dct_pad(k)] = make_double2(__fma_rn(Xk, c.x, Xr[i] * c.y), __fma_rn(Xr[i], c.x, -(Xk * c.y)));
+            }
+        }
+        sync();
+        fetch(y + stride_rows);  // in flight while this row is transformed
+        int Ns = 1;
+#pragma unroll 1
+        for (int st = 0; st < S::L8; ++st) {
+            dct_stage<8, N, TPS>(buf, Ns, j, tws, sync);
+            Ns *= 8;
+        }
+        if constexpr (S::REM == 1) dct_stage<2, N, TPS>(buf, Ns, j, tws, sync);
+        else if constexpr (S::REM == 2) dct_stage<4, N, TPS>(buf, Ns, j, tws, sync);
+        if (live) {
+            double* o = io.out + io.out_off + y * io.out_stride;
+            if constexpr (TYPE == 2) {
+#pragma unroll
+                for (int i = 0; i < PER; ++i) {
+                    const int k = j + i * TPS;
+                    const double2 Z = buf[dct_pad(k)];
+                    const double2 c = __ldg(&pt[k]);
+                    o[k] = 2.0 * __fma_rn(Z.x, c.x, Z.y * c.y);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < PER; ++i) o[j + i * TPS] = buf[dct_pad(perm(j + i * TPS))].x;
+            }
+        }
+        sync();  // the buffer takes the next round's row
+    }
+}
+
+}  // namespace pfb

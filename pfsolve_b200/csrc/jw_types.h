@@ -45,6 +45,15 @@ struct JwOperator {
 };
 
 // The data side: systems, layouts, keep-windows.
+// The DCT step (dct.cuh): rows of N points, in and out (possibly the same).
+struct DctIO {
+    const double* in;
+    double* out;
+    int64_t in_off, in_stride;    // elements
+    int64_t out_off, out_stride;  // elements
+    int64_t nsys;
+};
+
 // Streaming kernel: at most this many TMA staging buffers per group.
 constexpr int kStMaxBuffers = 4;
 

@@ -119,6 +119,13 @@ struct LongVariant {
 constexpr int kLongMaxSlices = 64;  // slices per system of the single pass
 constexpr int kLongShapes = 4;  // compiled shapes per operator kind, in order of preference
 const LongVariant* find_long_variant(int shape, int KL, int KU, int SV);
+
+// The DCT step (dct.cu): type 2 or 3 of rows of 2^logn points (3 <= logn <=
+// 12), with the plan's tables from dct_tables (twiddles, then the pre/post
+// factors; 2N values of 16 bytes, one cudaMalloc).
+cudaError_t dct_launch(int logn, int type, const DctIO& io, const double2* tw, const double2* pt, int num_sms,
+                       cudaStream_t st);
+cudaError_t dct_tables(int64_t N, double2** tables);
 unsigned long_status_fetch_clear();
 unsigned cluster_status_fetch_clear();
 // Status word of the streaming kernels' bounded waits since the last call
