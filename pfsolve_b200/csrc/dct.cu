@@ -36,7 +36,7 @@ cudaError_t dct_launch_t(const DctIO& io, const double2* tw, const double2* pt, 
         }
         blocks = blocks_of[dev];
     }
-    const int64_t want = (io.nsys + S::SPC - 1) / S::SPC;
+    const int64_t want = ((io.nsys + 1) / 2 + S::SPC - 1) / S::SPC;  // row pairs per CTA round: SPC
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)blocks * num_sms));
     dct_kernel<LOGN, TYPE><<<(unsigned)grid, S::NT, S::SMEM, st>>>(io, tw, pt);
     return cudaPeekAtLastError();

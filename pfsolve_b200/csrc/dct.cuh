@@ -5,7 +5,7 @@
 // PfSolve carries performDCT from follows; pfSolve_Structs.h:272):
 //   type 2: X_k = 2 sum_{n} x_n cos(pi k (2n+1) / (2N))
 //   type 3: x_k = X_0 + 2 sum_{n>=1} X_n cos(pi n (2k+1) / (2N))
-// Both run as one complex N-point FFT per row (Makhoul, IEEE TASSP 28 (1980)):
+// Both run through a complex N-point FFT (Makhoul, IEEE TASSP 28 (1980)):
 //   type 2: v = (x_0, x_2, ..., x_{N-2}, x_{N-1}, ..., x_3, x_1), V = FFT(v),
 //           X_k = 2 Re(e^{-i pi k/2N} V_k);
 //   type 3: z_k = e^{-i pi k/2N} (X_k + i X_{N-k}) (X_N = 0), Z = FFT(z),
@@ -17,8 +17,9 @@
 // stage reads, synchronises, writes): radix-8 stages, then one radix-4 or
 // radix-2 stage when log2 N is not a multiple of 3; every thread does one
 // radix-8 butterfly per stage (N/8 threads per row), and a CTA holds as many
-// rows as 256 threads cover.  Each thread loads the next row's inputs into
-// registers while the current row is transformed.  Twiddles e^{-2 pi i j/N} and the
+// row pairs as 256 threads cover: one FFT transforms two rows (see the
+// kernel).  Each thread loads the next pair's inputs into registers while the
+// current pair is transformed.  Twiddles e^{-2 pi i j/N} and the
 // pre/post factors (cos, sin)(pi k/2N) come from tables the plan computes once
 // in long double on the host.  Rows are read and written with coalesced
 // global accesses; a row is fully staged before its result is written, so
@@ -37,11 +38,11 @@ struct DctShape {
     static constexpr int N = 1 << LOGN;
     static constexpr int TPS = N >= 8 ? N / 8 : 1;    // threads per row
     static constexpr int NT = TPS > 256 ? TPS : 256;  // threads per CTA
-    static constexpr int SPC = NT / TPS;              // rows per CTA round
+    static constexpr int SPC = NT / TPS;              // row pairs per CTA round
     static constexpr int L8 = LOGN / 3;               // radix-8 stages
     static constexpr int REM = LOGN % 3;              // then one radix-2 (1) or radix-4 (2) stage
     static constexpr int NP = N + N / 8;  // the buffer, one 16-byte pad after every 8 values
-    // one buffer of N complex values per row, then the twiddles (N values)
+    // one buffer of N complex values per row pair, then the twiddles (N values)
     static constexpr size_t SMEM = ((size_t)SPC * NP + N) * 16;
 };
 
@@ -144,67 +145,82 @@ __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const dou
 }
 
 // tw[j] = e^{-2 pi i j/N} (j < N); pt[k] = (cos, sin)(pi k/(2N)) (k < N).
-// One buffer of N complex values per row; each thread keeps the next row's
-// N/TPS input values in registers, loaded while the current row is
+//
+// Two rows share one complex FFT (a "pair"; rows 2u and 2u + 1):
+//   type 2: c = v1 + i v2 (both rows in Makhoul's order), Z = FFT(c); with
+//           Zr = Z_{N-k} (Z_0 for k = 0) the rows' transforms are
+//           X1_k = (Re Z + Re Zr) cos t + (Im Z - Im Zr) sin t,
+//           X2_k = (Im Z + Im Zr) cos t - (Re Z - Re Zr) sin t   (t = pi k/2N);
+//   type 3: each row's z_k = e^{-i t}(X_k + i X_{N-k}) is conjugate-symmetric
+//           (z_{N-k} = conj z_k), so FFT(z) is real: c = z1 + i z2 gives
+//           Re FFT(c) = FFT(z1) and Im FFT(c) = FFT(z2).
+// One buffer of N complex values per pair; each thread keeps the next pair's
+// 2 N/TPS input values in registers, loaded while the current pair is
 // transformed.
 template <int LOGN, int TYPE>
-__global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 ? 3 : 1) dct_kernel(const DctIO io, const double2* __restrict__ tw,
-                                                                 const double2* __restrict__ pt)
+__global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 ? 2 : 1)
+    dct_kernel(const DctIO io, const double2* __restrict__ tw, const double2* __restrict__ pt)
 {
     using S = DctShape<LOGN>;
     constexpr int N = S::N, TPS = S::TPS, PER = N / TPS;
     extern __shared__ __align__(16) double2 dct_smem[];
     const int s = threadIdx.x / TPS, j = threadIdx.x - s * TPS;
     double2* buf = dct_smem + (size_t)s * S::NP;
-    double2* tws = dct_smem + (size_t)S::SPC * S::NP;  // the twiddles, shared by the CTA's rows
+    double2* tws = dct_smem + (size_t)S::SPC * S::NP;  // the twiddles, shared by the CTA's pairs
     for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
     __syncthreads();
     // Makhoul's order: input point e sits at position perm(e) of the sequence
     auto perm = [](int e) { return (e & 1) ? N - 1 - (e >> 1) : (e >> 1); };
-    // The threads of one row synchronise among themselves only: a warp (rows
-    // of up to 256 points share warps, and keep in step), else a named
-    // barrier per row (ids 1..SPC).
+    // The threads of one pair synchronise among themselves only: a warp
+    // (pairs of up to 256 points share warps, and keep in step), else a named
+    // barrier per pair (ids 1..SPC).
     auto sync = [&]() {
         if constexpr (TPS <= 32) __syncwarp();
         else asm volatile("bar.sync %0, %1;\n" ::"r"(1 + s), "r"(TPS) : "memory");
     };
-    const int64_t stride_rows = (int64_t)gridDim.x * S::SPC;
-    double pre[PER];
-    auto fetch = [&](int64_t y) {
-        const bool live = y < io.nsys;
-        const double* x = io.in + io.in_off + (live ? y : 0) * io.in_stride;
+    const int64_t npairs = (io.nsys + 1) / 2;
+    const int64_t stride_units = (int64_t)gridDim.x * S::SPC;
+    double p1[PER], p2[PER];
+    auto fetch = [&](int64_t u) {
+        const int64_t y1 = 2 * u, y2 = 2 * u + 1;
+        const bool l1 = y1 < io.nsys, l2 = y2 < io.nsys;
+        const double* x1 = io.in + io.in_off + (l1 ? y1 : 0) * io.in_stride;
+        const double* x2 = io.in + io.in_off + (l2 ? y2 : 0) * io.in_stride;
 #pragma unroll
-        for (int i = 0; i < PER; ++i) pre[i] = live ? x[j + i * TPS] : 0.0;
+        for (int i = 0; i < PER; ++i) {
+            p1[i] = l1 ? x1[j + i * TPS] : 0.0;
+            p2[i] = l2 ? x2[j + i * TPS] : 0.0;
+        }
     };
-    int64_t y = (int64_t)blockIdx.x * S::SPC + s;
-    fetch(y);
-    for (int64_t base = (int64_t)blockIdx.x * S::SPC; base < io.nsys; base += stride_rows, y += stride_rows) {
-        const bool live = y < io.nsys;
+    int64_t u = (int64_t)blockIdx.x * S::SPC + s;
+    fetch(u);
+    for (int64_t base = (int64_t)blockIdx.x * S::SPC; base < npairs; base += stride_units, u += stride_units) {
         if constexpr (TYPE == 2) {
 #pragma unroll
-            for (int i = 0; i < PER; ++i) buf[dct_pad(perm(j + i * TPS))] = make_double2(pre[i], 0.0);
+            for (int i = 0; i < PER; ++i) buf[dct_pad(perm(j + i * TPS))] = make_double2(p1[i], p2[i]);
         } else {
 #pragma unroll
-            for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)].x = pre[i];
+            for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)] = make_double2(p1[i], p2[i]);
             sync();
-            double Xr[PER];
+            double2 Xr[PER];
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int k = j + i * TPS;
-                Xr[i] = (k == 0) ? 0.0 : buf[dct_pad(N - k)].x;
+                Xr[i] = (k == 0) ? make_double2(0.0, 0.0) : buf[dct_pad(N - k)];
             }
             sync();
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int k = j + i * TPS;
-                const double Xk = pre[i];
                 const double2 c = __ldg(&pt[k]);
-                // e^{-i t} (Xk + i Xr) = (Xk cos t + Xr sin t) + i (Xr cos t - Xk sin t)
-                buf[dct_pad(k)] = make_double2(__fma_rn(Xk, c.x, Xr[i] * c.y), __fma_rn(Xr[i], c.x, -(Xk * c.y)));
+                // z_k = e^{-i t} (X_k + i X_{N-k}) = (X_k cos t + X_{N-k} sin t) + i (X_{N-k} cos t - X_k sin t)
+                const double z1r = __fma_rn(p1[i], c.x, Xr[i].x * c.y), z1i = __fma_rn(Xr[i].x, c.x, -(p1[i] * c.y));
+                const double z2r = __fma_rn(p2[i], c.x, Xr[i].y * c.y), z2i = __fma_rn(Xr[i].y, c.x, -(p2[i] * c.y));
+                buf[dct_pad(k)] = make_double2(z1r - z2i, z1i + z2r);  // z1 + i z2
             }
         }
         sync();
-        fetch(y + stride_rows);  // in flight while this row is transformed
+        fetch(u + stride_units);  // in flight while this pair is transformed
         int Ns = 1;
 #pragma unroll 1
         for (int st = 0; st < S::L8; ++st) {
@@ -213,22 +229,28 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
         }
         if constexpr (S::REM == 1) dct_stage<2, N, TPS>(buf, Ns, j, tws, sync);
         else if constexpr (S::REM == 2) dct_stage<4, N, TPS>(buf, Ns, j, tws, sync);
-        if (live) {
-            double* o = io.out + io.out_off + y * io.out_stride;
-            if constexpr (TYPE == 2) {
+        const int64_t y1 = 2 * u, y2 = 2 * u + 1;
+        const bool l1 = y1 < io.nsys, l2 = y2 < io.nsys;
+        double* o1 = io.out + io.out_off + (l1 ? y1 : 0) * io.out_stride;
+        double* o2 = io.out + io.out_off + (l2 ? y2 : 0) * io.out_stride;
+        if constexpr (TYPE == 2) {
 #pragma unroll
-                for (int i = 0; i < PER; ++i) {
-                    const int k = j + i * TPS;
-                    const double2 Z = buf[dct_pad(k)];
-                    const double2 c = __ldg(&pt[k]);
-                    o[k] = 2.0 * __fma_rn(Z.x, c.x, Z.y * c.y);
-                }
-            } else {
+            for (int i = 0; i < PER; ++i) {
+                const int k = j + i * TPS;
+                const double2 Z = buf[dct_pad(k)], Zr = buf[dct_pad((N - k) & (N - 1))];
+                const double2 c = __ldg(&pt[k]);
+                if (l1) o1[k] = __fma_rn(Z.x + Zr.x, c.x, (Z.y - Zr.y) * c.y);
+                if (l2) o2[k] = __fma_rn(Z.y + Zr.y, c.x, -((Z.x - Zr.x) * c.y));
+            }
+        } else {
 #pragma unroll
-                for (int i = 0; i < PER; ++i) o[j + i * TPS] = buf[dct_pad(perm(j + i * TPS))].x;
+            for (int i = 0; i < PER; ++i) {
+                const double2 Z = buf[dct_pad(perm(j + i * TPS))];
+                if (l1) o1[j + i * TPS] = Z.x;
+                if (l2) o2[j + i * TPS] = Z.y;
             }
         }
-        sync();  // the buffer takes the next round's row
+        sync();  // the buffer takes the next round's pair
     }
 }
 
