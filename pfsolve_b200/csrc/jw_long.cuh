@@ -634,9 +634,31 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         auto stage_off = [&](int u) -> uint32_t { return unit_off(u, t, sw_me); };  // this thread's units
         constexpr bool COUPLED = BC::FWD || BC::BWD || KL > 0 || KU > 0;
         const bool tail_slice = !plain && Mfull < io.M && s0 + C::S > Mfull;
+        // the halo rows of the first and last threads, loaded a system ahead
+        // beside the TMA load (they are used, and so read, before the slice
+        // publishes that system: no neighbour has stored it yet)
+        auto halo = [&](int64_t kk, double (&h)[4]) {
+            if (kk >= nk) return;
+            const int64_t y = sys_of(kk);
+            if constexpr (KL > 0) {
+                if (t == 0) {
+                    h[0] = in_row(y, s0 - 2);
+                    h[1] = in_row(y, s0 - 1);
+                }
+            }
+            if constexpr (KU > 0) {
+                if (t == T - 1) {
+                    h[2] = in_row(y, s0 + C::S);
+                    h[3] = in_row(y, s0 + C::S + 1);
+                }
+            }
+        };
+        double hc[4] = {0.0, 0.0, 0.0, 0.0}, hn[4] = {0.0, 0.0, 0.0, 0.0};
+        if (!plain) halo(0, hc);
         if (!plain && nk > 0 && lane == 0) issue_load(bufp(0), barp(0), sys_of(0));
         for (int64_t k = 0; k <= nk; ++k) {
             const bool prefetch = !plain && k + 1 < nk;
+            if (prefetch) halo(k + 1, hn);
             if (prefetch && lane == 0) {
                 bulk_wait_read_all();  // the store from this buffer (system k-2) has read it
                 issue_load(bufp(k + 1), barp(k + 1), sys_of(k + 1));
@@ -675,14 +697,14 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                         if constexpr (KL > 0) {
                             double2 pv;
                             if (t > 0) pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
-                            else pv = make_double2(in_row(y, s0 - 2), in_row(y, s0 - 1));
+                            else pv = make_double2(hc[0], hc[1]);
                             x[KL - 1] = pv.y;
                             if constexpr (KL > 1) x[0] = pv.x;
                         }
                         if constexpr (KU > 0) {
                             double2 nv;
                             if (t < T - 1) nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
-                            else nv = make_double2(in_row(y, s0 + C::S), in_row(y, s0 + C::S + 1));
+                            else nv = make_double2(hc[2], hc[3]);
                             x[KL + R] = nv.x;
                             if constexpr (KU > 1) x[KL + R + 1] = nv.y;
                         }
@@ -814,16 +836,49 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 if (prefetch && lane == 0) mbar_wait_bounded(barp(k + 1), parity(k + 1));
                 break;
             }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) hc[i] = hn[i];
         }
         if (lane == 0) bulk_wait_all();
         return;
     }
 
+    // The per-system scalars a pass reads from global memory -- the halo rows
+    // (the input in pass 1, the records in pass 2) and pass 2's carries -- are
+    // loaded a system ahead, beside the next system's TMA load, so that their
+    // latency is not in the solve's path.
+    struct Scal {
+        double lo0, lo1, hi0, hi1, X, Y;
+    };
+    auto fetch = [&](int64_t y) -> Scal {
+        Scal r{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (y >= nsys) return r;
+        auto rv = [&](int k) -> double { return red[((size_t)c * kLgRed + k) * nsys + y]; };
+        if constexpr (KL > 0) {
+            if (t == 0) {
+                r.lo0 = PASS == 1 ? in_row(y, s0 - 2) : rv(kLgRedLo);
+                r.lo1 = PASS == 1 ? in_row(y, s0 - 1) : rv(kLgRedLo + 1);
+            }
+        }
+        if constexpr (KU > 0) {
+            if (t == T - 1) {
+                r.hi0 = PASS == 1 ? in_row(y, s0 + C::S) : rv(kLgRedHi);
+                r.hi1 = PASS == 1 ? in_row(y, s0 + C::S + 1) : rv(kLgRedHi + 1);
+            }
+        }
+        if constexpr (PASS == 2) {
+            if constexpr (BC::FWD) r.X = rv(kLgRedX);
+            if constexpr (BC::BWD) r.Y = rv(kLgRedY);
+        }
+        return r;
+    };
+    Scal sc = fetch(sys), scn;
     if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
-    for (int k = 0; sys < nsys; ++k, sys += per) {
+    for (int k = 0; sys < nsys; ++k, sys += per, sc = scn) {
         unsigned char* cur = (k & 1) ? buf1 : buf0;
         unsigned char* nxt = (k & 1) ? buf0 : buf1;
         const bool more = sys + per < nsys;
+        scn = fetch(sys + per);
         bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
         ok = group_and(g.bar_id, g.nthr, ok);
         if (!ok) {
@@ -843,12 +898,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             double2 pv = make_double2(0.0, 0.0);
             if (t > 0) {
                 pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
-            } else if (PASS == 1) {
-                pv = make_double2(in_row(sys, s0 - 2), in_row(sys, s0 - 1));
-                rec(kLgRedLo) = pv.x;
-                rec(kLgRedLo + 1) = pv.y;
             } else {
-                pv = make_double2(rec(kLgRedLo), rec(kLgRedLo + 1));
+                pv = make_double2(sc.lo0, sc.lo1);
+                if (PASS == 1) {
+                    rec(kLgRedLo) = pv.x;
+                    rec(kLgRedLo + 1) = pv.y;
+                }
             }
             be[KL - 1] = pv.y;
             if constexpr (KL > 1) be[0] = pv.x;
@@ -857,12 +912,12 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             double2 nv = make_double2(0.0, 0.0);
             if (t < T - 1) {
                 nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
-            } else if (PASS == 1) {
-                nv = make_double2(in_row(sys, s0 + C::S), in_row(sys, s0 + C::S + 1));
-                rec(kLgRedHi) = nv.x;
-                rec(kLgRedHi + 1) = nv.y;
             } else {
-                nv = make_double2(rec(kLgRedHi), rec(kLgRedHi + 1));
+                nv = make_double2(sc.hi0, sc.hi1);
+                if (PASS == 1) {
+                    rec(kLgRedHi) = nv.x;
+                    rec(kLgRedHi + 1) = nv.y;
+                }
             }
             be[KL + R] = nv.x;
             if constexpr (KU > 1) be[KL + R + 1] = nv.y;
@@ -936,7 +991,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             continue;
         } else {
             // carries of this system's slice, from the carry kernel
-            const double Xc = BC::FWD ? rec(kLgRedX) : 0.0, Yc = BC::BWD ? rec(kLgRedY) : 0.0;
+            const double Xc = sc.X, Yc = sc.Y;
             lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
         }
         if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];

@@ -44,7 +44,6 @@ struct JwOperator {
     int bands32;  // bands and the dgbmv matrix hold FP32 values (FP32-storage precisions)
 };
 
-// The data side: systems, layouts, keep-windows.
 // The DCT step (dct.cuh): rows of N points, in and out (possibly the same).
 struct DctIO {
     const double* in;
@@ -57,6 +56,7 @@ struct DctIO {
 // Streaming kernel: at most this many TMA staging buffers per group.
 constexpr int kStMaxBuffers = 4;
 
+// The data side: systems, layouts, keep-windows.
 struct JwIO {
     const double* in;             // FP64 values, or FP32 values for the FP32-storage precisions
     double* out;
