@@ -235,10 +235,18 @@ const LongVariant* pick_long(AppState* s, int64_t M, bool single, int* NS_out, i
         const int NS = (int)((M + v->S - 1) / v->S);
         if (single && NS > kLongMaxSlices) continue;
         const int64_t res = (int64_t)b * s->num_sms;
-        // CTAs in whole multiples of NS, at most one CTA's worth of systems each
-        const int64_t per_slice = std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
         *NS_out = NS;
-        *grid_out = (int)(per_slice * NS);
+        if (single) {
+            // CTAs in whole multiples of NS, at most one CTA's worth of systems each
+            const int64_t per_slice =
+                std::max<int64_t>(1, std::min<int64_t>(res / NS, (s->plan_batch + v->G - 1) / v->G));
+            *grid_out = (int)(per_slice * NS);
+        } else {
+            // the solve passes split the (slice, system) items evenly over
+            // every resident CTA, at least a group's worth each
+            const int64_t items = (int64_t)NS * s->plan_batch;
+            *grid_out = (int)std::max<int64_t>(1, std::min<int64_t>(res, (items + v->G - 1) / v->G));
+        }
         return v;
     }
     return nullptr;

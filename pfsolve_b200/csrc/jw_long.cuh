@@ -9,10 +9,11 @@
 // pfSolve_AppManagement/pfSolve_InitializeApp.h:1540-1583); so does this
 // kernel, with the reduction written as affine maps:
 //
-//  * A system is cut into NS slices of S = 32*W*R rows.  A CTA owns one slice
-//    position c and the coefficient table of those rows (built once, in shared
-//    memory), and G groups of W warps each stream a different system's slice c
-//    through it (TMA boxes, as in the streaming kernel).
+//  * A system is cut into NS slices of S = 32*W*R rows.  In the solve passes a
+//    CTA takes an even share of the (slice, system) items in slice-major
+//    order -- one slice or a few, whose coefficient tables it loads into
+//    shared memory in turn -- and G groups of W warps each stream a different
+//    system's slice through the table (TMA boxes, as in the streaming kernel).
 //  * Within a slice the solve is the group kernel's: per-thread chunk
 //    recurrences and affine scans across the group.  The value entering the
 //    slice from below (forward) or above (backward) is the only coupling.
@@ -176,17 +177,27 @@ __device__ void lg_prologue(const JwOperator& op, double* table, double* scratch
             }
             return;
         }
-        // Q = product of the slices below: agg[c-1] * ... * agg[0]
+        // Q = product of the slices below: agg[c-1] * ... * agg[0], the
+        // products loaded in blocks of 8 ahead of their chain
         double qa = 1, qb = 0, qc = 0, qd = 1;
-        for (int r = 0; r < c; ++r) {
-            const double* o = cst + r * kLgConst + kLgConstMob;
-            double na = o[0] * qa + o[1] * qc, nb = o[0] * qb + o[1] * qd, nc = o[2] * qa + o[3] * qc,
-                   nd = o[2] * qb + o[3] * qd;
-            renorm2x2(na, nb, nc, nd);
-            qa = na;
-            qb = nb;
-            qc = nc;
-            qd = nd;
+        for (int r0 = 0; r0 < c; r0 += 8) {
+            double4 m[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const double* o = cst + (r0 + q) * kLgConst + kLgConstMob;
+                m[q] = (r0 + q < c) ? make_double4(o[0], o[1], o[2], o[3]) : make_double4(1.0, 0.0, 0.0, 1.0);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if (r0 + q >= c) break;
+                double na = m[q].x * qa + m[q].y * qc, nb = m[q].x * qb + m[q].y * qd, nc = m[q].z * qa + m[q].w * qc,
+                       nd = m[q].z * qb + m[q].w * qd;
+                renorm2x2(na, nb, nc, nd);
+                qa = na;
+                qb = nb;
+                qc = nc;
+                qd = nd;
+            }
         }
         (void)q4;
         // full prefix = (slice prefix) * Q; incoming vector = prefix * (1, 0)^T
@@ -294,17 +305,45 @@ __global__ void __launch_bounds__(128) jw_long_carry_kernel(double* __restrict__
     const int64_t y = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= nsys) return;
     auto rs = [&](int c, int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + y]; };
+    // slices in blocks of B, each block's loads issued together ahead of its
+    // dependent chain of FMAs
+    constexpr int B = 8;
     double X = 0.0;
-    for (int c = 0; c < NS; ++c) {
-        rs(c, kLgRedX) = X;
-        if (FWD) X = __fma_rn(cst[c * kLgConst], X, rs(c, kLgRedBf));
+    for (int c0 = 0; c0 < NS; c0 += B) {
+        double bf[B], af[B];
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            const bool v = FWD && c0 + q < NS;
+            bf[q] = v ? rs(c0 + q, kLgRedBf) : 0.0;
+            af[q] = v ? cst[(c0 + q) * kLgConst] : 1.0;
+        }
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+            if (c0 + q >= NS) break;
+            rs(c0 + q, kLgRedX) = X;
+            if (FWD) X = __fma_rn(af[q], X, bf[q]);
+        }
     }
     if (BWD) {
         double Y = 0.0;
-        for (int c = NS - 1; c >= 0; --c) {
-            rs(c, kLgRedY) = Y;
-            const double Bb = FWD ? __fma_rn(rs(c, kLgRedX), cst[c * kLgConst + 2], rs(c, kLgRedBb)) : rs(c, kLgRedBb);
-            Y = __fma_rn(cst[c * kLgConst + 1], Y, Bb);
+        for (int c0 = ((NS - 1) / B) * B; c0 >= 0; c0 -= B) {
+            double bb[B], ab[B];
+#pragma unroll
+            for (int q = 0; q < B; ++q) {
+                const int c = c0 + q;
+                bb[q] = 0.0;
+                ab[q] = 1.0;
+                if (c < NS) {
+                    bb[q] = FWD ? __fma_rn(rs(c, kLgRedX), cst[c * kLgConst + 2], rs(c, kLgRedBb)) : rs(c, kLgRedBb);
+                    ab[q] = cst[c * kLgConst + 1];
+                }
+            }
+#pragma unroll
+            for (int q = B - 1; q >= 0; --q) {
+                if (c0 + q >= NS) continue;
+                rs(c0 + q, kLgRedY) = Y;
+                Y = __fma_rn(ab[q], Y, bb[q]);
+            }
         }
     }
 }
@@ -400,7 +439,20 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = warp / W, wg = warp - grp * W;
     const int t = threadIdx.x - grp * T;  // thread within the group
-    const int c = (int)(blockIdx.x % (unsigned)NS);
+    // Passes 1 and 2 take a range of the slice-major list of (slice, system)
+    // items -- CTA b: [b L, (b+1) L), L = ceil(NS nsys / grid) -- so that every
+    // CTA of the grid has work whatever NS; a range spans one slice or a few,
+    // and the CTA loads each one's table in turn.  The other passes: CTA b
+    // owns slice b % NS.
+    int64_t it_beg = 0, it_end = 0;
+    int c = (int)(blockIdx.x % (unsigned)NS);
+    if constexpr (PASS == 1 || PASS == 2) {
+        const int64_t total = (int64_t)NS * io.nsys;
+        const int64_t L = (total + gridDim.x - 1) / gridDim.x;
+        it_beg = (int64_t)blockIdx.x * L < total ? (int64_t)blockIdx.x * L : total;
+        it_end = it_beg + L < total ? it_beg + L : total;
+        c = it_beg < it_end ? (int)(it_beg / io.nsys) : 0;
+    }
 
     double* table = reinterpret_cast<double*>(smem_raw);
     double* scratch = reinterpret_cast<double*>(smem_raw + BC::TBL);
@@ -416,23 +468,32 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     // PASS 1 weights: row tt * R + jj at [jj * T + tt] (consecutive threads,
     // consecutive entries)
     double2* ab_s = reinterpret_cast<double2*>(after + pad + (size_t)C::G * NBUF * BC::BUF);
-    double2* ab_g = reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)c * C::S;
+    auto ab_g_of = [&](int cc) -> double2* {
+        return reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)cc * C::S;
+    };
+    double2* ab_g = ab_g_of(c);
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
 
     if (threadIdx.x < NBUF * C::G) mbar_init(smem_u32(bars_all + threadIdx.x), W);
     mbar_init_fence();
     double* gtab = tab + (size_t)c * (BC::TBL / sizeof(double));
+    // the solve passes' copy of slice c's table (and pass 1's weights)
+    auto load_slice = [&]() {
+        const double2* src = reinterpret_cast<const double2*>(tab + (size_t)c * (BC::TBL / sizeof(double)));
+        double2* dst = reinterpret_cast<double2*>(table);
+        for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
+        if constexpr (PASS == 1) {
+            const double2* w = ab_g_of(c);
+            for (int i = threadIdx.x; i < C::S; i += blockDim.x) ab_s[i] = w[i];
+        }
+    };
     if constexpr (PASS == 3) {
         lg_prologue<C, true>(op, table, scratch, q4, c, cst);
         return;
     } else if constexpr (PASS == 0) {
         lg_prologue<C>(op, table, scratch, q4, c, cst);
     } else {
-        const double2* src = reinterpret_cast<const double2*>(gtab);
-        double2* dst = reinterpret_cast<double2*>(table);
-        for (int i = threadIdx.x; i < (int)(BC::TBL / 16); i += blockDim.x) dst[i] = src[i];
-        if constexpr (PASS == 1)
-            for (int i = threadIdx.x; i < C::S; i += blockDim.x) ab_s[i] = ab_g[i];
+        load_slice();
         if constexpr (PASS == 4)
             for (int i = threadIdx.x; i < NS; i += blockDim.x) {
                 cst_s[4 * i] = cst[i * kLgConst];          // Af
@@ -451,27 +512,32 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     g.seq = 0;
     g.scratch = scratch + (size_t)grp * W * kScratchPerWarp;
 
-    const int64_t s0 = (int64_t)c * C::S;
-    const int64_t s_glob = s0 + (int64_t)t * R;
+    int64_t s0 = (int64_t)c * C::S;
+    int64_t s_glob = s0 + (int64_t)t * R;
     const double2* tb = reinterpret_cast<const double2*>(table) + t;
     auto coef = [&](int p, int u) -> double2 { return tb[(p * U + u) * BC::TP]; };
     double Af = 1.0, Ab = 1.0;  // this thread's chunk multipliers
-    if constexpr (BC::FWD) {
+    auto chunk_mults = [&]() {
+        Af = 1.0;
+        Ab = 1.0;
+        if constexpr (BC::FWD) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const double2 cc = coef(BC::P_NL, u);
-            Af = (u == 0) ? cc.x : cc.x * Af;
-            Af = cc.y * Af;
+            for (int u = 0; u < U; ++u) {
+                const double2 cc = coef(BC::P_NL, u);
+                Af = (u == 0) ? cc.x : cc.x * Af;
+                Af = cc.y * Af;
+            }
         }
-    }
-    if constexpr (BC::BWD) {
+        if constexpr (BC::BWD) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const double2 cc = coef(BC::P_NH, u);
-            Ab = cc.x * Ab;
-            Ab = cc.y * Ab;
+            for (int u = 0; u < U; ++u) {
+                const double2 cc = coef(BC::P_NH, u);
+                Ab = cc.x * Ab;
+                Ab = cc.y * Ab;
+            }
         }
-    }
+    };
+    chunk_mults();
 
     // Single pass: the responses of the slice's rows to a unit forward carry
     // (psi) and to a unit backward carry (G), by group 0: zero-input solves.
@@ -595,9 +661,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         return io.in[io.in_off + y * io.in_stride + row];
     };
     const int64_t nsys = io.nsys;
-    const int64_t per = (int64_t)(gridDim.x / (unsigned)NS) * C::G;  // systems in flight over the grid
+    // systems in flight over the grid (passes 1 and 2: over the CTA's range)
+    const int64_t per = (PASS == 1 || PASS == 2) ? (int64_t)C::G : (int64_t)(gridDim.x / (unsigned)NS) * C::G;
     int64_t sys = (int64_t)(blockIdx.x / (unsigned)NS) * C::G + grp;
-    const int chunk0 = c * T;
+    int chunk0 = c * T;
 
     auto issue_load = [&](unsigned char* b, uint32_t bar, int64_t y) {
         mbar_arrive_expect_tx(bar, (uint32_t)(H * 32 * ROWB));
@@ -850,9 +917,10 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     struct Scal {
         double lo0, lo1, hi0, hi1, X, Y;
     };
+    int64_t ylim = 0;  // end of the current segment's systems
     auto fetch = [&](int64_t y) -> Scal {
         Scal r{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (y >= nsys) return r;
+        if (y >= ylim) return r;
         auto rv = [&](int k) -> double { return red[((size_t)c * kLgRed + k) * nsys + y]; };
         if constexpr (KL > 0) {
             if (t == 0) {
@@ -872,139 +940,166 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         }
         return r;
     };
-    Scal sc = fetch(sys), scn;
-    if (sys < nsys && lane == 0) issue_load(buf0, bar0, sys);
-    for (int k = 0; sys < nsys; ++k, sys += per, sc = scn) {
-        unsigned char* cur = (k & 1) ? buf1 : buf0;
-        unsigned char* nxt = (k & 1) ? buf0 : buf1;
-        const bool more = sys + per < nsys;
-        scn = fetch(sys + per);
-        bool ok = mbar_wait_bounded((k & 1) ? bar1 : bar0, (uint32_t)((k >> 1) & 1));
-        ok = group_and(g.bar_id, g.nthr, ok);
-        if (!ok) {
-            if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
-            break;
+    // The CTA's range in segments of one slice each; at a slice change every
+    // group has finished with the old table (no load of this CTA is in
+    // flight then: the last item of a segment prefetches nothing).
+    int kk = 0;  // items this group has run: its buffer and barrier phase
+    bool stop = false;
+    for (int64_t seg = it_beg; seg < it_end;) {
+        const int cs = (int)(seg / nsys);
+        const int64_t seg_end = it_end < (int64_t)(cs + 1) * nsys ? it_end : (int64_t)(cs + 1) * nsys;
+        if (cs != c) {
+            __syncthreads();
+            c = cs;
+            s0 = (int64_t)c * C::S;
+            s_glob = s0 + (int64_t)t * R;
+            chunk0 = c * T;
+            load_slice();
+            __syncthreads();
+            chunk_mults();
         }
-        // field k of this (system, slice) record
-        auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
-        double be[R + KL + KU];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
-            be[KL + 2 * u] = v.x;
-            be[KL + 2 * u + 1] = v.y;
+        sys = seg - (int64_t)cs * nsys + grp;
+        ylim = seg_end - (int64_t)cs * nsys;
+        seg = seg_end;
+        if (stop) continue;
+        Scal sc = fetch(sys), scn;
+        if (sys < ylim && lane == 0) {
+            if (PASS == 2) bulk_wait_read_all();  // the store from this buffer (two items ago) has read it
+            issue_load((kk & 1) ? buf1 : buf0, (kk & 1) ? bar1 : bar0, sys);
         }
-        if constexpr (KL > 0) {
-            double2 pv = make_double2(0.0, 0.0);
-            if (t > 0) {
-                pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
-            } else {
-                pv = make_double2(sc.lo0, sc.lo1);
-                if (PASS == 1) {
-                    rec(kLgRedLo) = pv.x;
-                    rec(kLgRedLo + 1) = pv.y;
-                }
+        for (; sys < ylim; ++kk, sys += per, sc = scn) {
+            unsigned char* cur = (kk & 1) ? buf1 : buf0;
+            unsigned char* nxt = (kk & 1) ? buf0 : buf1;
+            const bool more = sys + per < ylim;
+            scn = fetch(sys + per);
+            bool ok = mbar_wait_bounded((kk & 1) ? bar1 : bar0, (uint32_t)((kk >> 1) & 1));
+            ok = group_and(g.bar_id, g.nthr, ok);
+            if (!ok) {
+                if (t == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);
+                stop = true;
+                break;
             }
-            be[KL - 1] = pv.y;
-            if constexpr (KL > 1) be[0] = pv.x;
-        }
-        if constexpr (KU > 0) {
-            double2 nv = make_double2(0.0, 0.0);
-            if (t < T - 1) {
-                nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
-            } else {
-                nv = make_double2(sc.hi0, sc.hi1);
-                if (PASS == 1) {
-                    rec(kLgRedHi) = nv.x;
-                    rec(kLgRedHi + 1) = nv.y;
-                }
+            // field k of this (system, slice) record
+            auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
+            double be[R + KL + KU];
+    #pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
+                be[KL + 2 * u] = v.x;
+                be[KL + 2 * u + 1] = v.y;
             }
-            be[KL + R] = nv.x;
-            if constexpr (KU > 1) be[KL + R + 1] = nv.y;
-        }
-        if (win_partial) {
-#pragma unroll
-            for (int i = 0; i < R + KL + KU; ++i) {
-                const int64_t row = s_glob - KL + i;
-                if (row < io.iz0 || row >= io.iz1) be[i] = 0.0;
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            double2 wc[NB];
-#pragma unroll
-            for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int j = 2 * u + e;
-                double acc = (e ? wc[0].y : wc[0].x) * be[j];
-#pragma unroll
-                for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
-                be[j] = acc;
-            }
-        }
-        double (&x)[R + KL + KU] = be;
-        // `nxt` was read in the previous iteration by every warp of the group
-        // (all of them have passed this iteration's group_and since) and, in
-        // pass 2, stored from: once this warp's stores have read it, it takes
-        // the next system
-        if (more && lane == 0) {
-            if (PASS == 2) bulk_wait_read_all();
-            issue_load(nxt, (k & 1) ? bar0 : bar1, sys + per);
-        }
-        if constexpr (PASS == 1) {
-            if constexpr (BC::FWD || BC::BWD) {
-                // Bf = sum alpha g, Bb0 = sum beta g over the slice
-                double sa = 0.0, sb = 0.0;
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    const double2 w = ab_s[j * T + t];
-                    sa = __fma_rn(w.x, x[j], sa);
-                    sb = __fma_rn(w.y, x[j], sb);
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    sa += __shfl_xor_sync(FULL, sa, o);
-                    sb += __shfl_xor_sync(FULL, sb, o);
-                }
-                if (W > 1) {
-                    double* my = g.warp_area(wg) + 16;
-                    if (lane == 0) {
-                        my[0] = sa;
-                        my[1] = sb;
+            if constexpr (KL > 0) {
+                double2 pv = make_double2(0.0, 0.0);
+                if (t > 0) {
+                    pv = *reinterpret_cast<const double2*>(cur + unit_off(U - 1, t - 1, sw_prev));
+                } else {
+                    pv = make_double2(sc.lo0, sc.lo1);
+                    if (PASS == 1) {
+                        rec(kLgRedLo) = pv.x;
+                        rec(kLgRedLo + 1) = pv.y;
                     }
-                    group_bar(g.bar_id, g.nthr);
-                    if (t == 0) {
-                        sa = 0.0;
-                        sb = 0.0;
-                        for (int w = 0; w < W; ++w) {
-                            sa += g.warp_area(w)[16];
-                            sb += g.warp_area(w)[17];
+                }
+                be[KL - 1] = pv.y;
+                if constexpr (KL > 1) be[0] = pv.x;
+            }
+            if constexpr (KU > 0) {
+                double2 nv = make_double2(0.0, 0.0);
+                if (t < T - 1) {
+                    nv = *reinterpret_cast<const double2*>(cur + unit_off(0, t + 1, sw_next));
+                } else {
+                    nv = make_double2(sc.hi0, sc.hi1);
+                    if (PASS == 1) {
+                        rec(kLgRedHi) = nv.x;
+                        rec(kLgRedHi + 1) = nv.y;
+                    }
+                }
+                be[KL + R] = nv.x;
+                if constexpr (KU > 1) be[KL + R + 1] = nv.y;
+            }
+            if (win_partial) {
+    #pragma unroll
+                for (int i = 0; i < R + KL + KU; ++i) {
+                    const int64_t row = s_glob - KL + i;
+                    if (row < io.iz0 || row >= io.iz1) be[i] = 0.0;
+                }
+            }
+    #pragma unroll
+            for (int u = 0; u < U; ++u) {
+                double2 wc[NB];
+    #pragma unroll
+                for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+    #pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int j = 2 * u + e;
+                    double acc = (e ? wc[0].y : wc[0].x) * be[j];
+    #pragma unroll
+                    for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
+                    be[j] = acc;
+                }
+            }
+            double (&x)[R + KL + KU] = be;
+            // `nxt` was read in the previous iteration by every warp of the group
+            // (all of them have passed this iteration's group_and since) and, in
+            // pass 2, stored from: once this warp's stores have read it, it takes
+            // the next system
+            if (more && lane == 0) {
+                if (PASS == 2) bulk_wait_read_all();
+                issue_load(nxt, (kk & 1) ? bar0 : bar1, sys + per);
+            }
+            if constexpr (PASS == 1) {
+                if constexpr (BC::FWD || BC::BWD) {
+                    // Bf = sum alpha g, Bb0 = sum beta g over the slice
+                    double sa = 0.0, sb = 0.0;
+    #pragma unroll
+                    for (int j = 0; j < R; ++j) {
+                        const double2 w = ab_s[j * T + t];
+                        sa = __fma_rn(w.x, x[j], sa);
+                        sb = __fma_rn(w.y, x[j], sb);
+                    }
+    #pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        sa += __shfl_xor_sync(FULL, sa, o);
+                        sb += __shfl_xor_sync(FULL, sb, o);
+                    }
+                    if (W > 1) {
+                        double* my = g.warp_area(wg) + 16;
+                        if (lane == 0) {
+                            my[0] = sa;
+                            my[1] = sb;
+                        }
+                        group_bar(g.bar_id, g.nthr);
+                        if (t == 0) {
+                            sa = 0.0;
+                            sb = 0.0;
+                            for (int w = 0; w < W; ++w) {
+                                sa += g.warp_area(w)[16];
+                                sb += g.warp_area(w)[17];
+                            }
                         }
                     }
+                    if (t == 0) {
+                        if constexpr (BC::FWD) rec(kLgRedBf) = sa;
+                        if constexpr (BC::BWD) rec(kLgRedBb) = sb;
+                    }
                 }
-                if (t == 0) {
-                    if constexpr (BC::FWD) rec(kLgRedBf) = sa;
-                    if constexpr (BC::BWD) rec(kLgRedBb) = sb;
-                }
+                continue;
+            } else {
+                // carries of this system's slice, from the carry kernel
+                const double Xc = sc.X, Yc = sc.Y;
+                lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
             }
-            continue;
-        } else {
-            // carries of this system's slice, from the carry kernel
-            const double Xc = sc.X, Yc = sc.Y;
-            lg_solve<C>(g, coef, Af, Ab, x, [&](double, double) { return Xc; }, [&](double, double) { return Yc; });
+            if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
+            __syncwarp();
+    #pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int h = u / IBO, uu = u % IBO;
+                *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
+                    make_double2(x[2 * u], x[2 * u + 1]);
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) issue_store(cur, sys);
         }
-        if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
-        __syncwarp();
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int h = u / IBO, uu = u % IBO;
-            *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
-                make_double2(x[2 * u], x[2 * u + 1]);
-        }
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) issue_store(cur, sys);
     }
     if (lane == 0) bulk_wait_all();
 }
