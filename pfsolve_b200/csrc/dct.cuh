@@ -42,8 +42,9 @@ struct DctShape {
     static constexpr int L8 = LOGN / 3;               // radix-8 stages
     static constexpr int REM = LOGN % 3;              // then one radix-2 (1) or radix-4 (2) stage
     static constexpr int NP = N + N / 8;  // the buffer, one 16-byte pad after every 8 values
-    // one buffer of N complex values per row pair, then the twiddles (N values)
-    static constexpr size_t SMEM = ((size_t)SPC * NP + N) * 16;
+    static constexpr int NTW = N + N / 8 + N / 64 + 1;  // the twiddles, padded (dct_twpad)
+    // one buffer of N complex values per row pair, then the twiddles
+    static constexpr size_t SMEM = ((size_t)SPC * NP + NTW) * 16;
 };
 
 __device__ __forceinline__ double2 dct_cmul(double2 a, double2 b)
@@ -107,12 +108,23 @@ __device__ __forceinline__ void dct_dft<8>(double2 (&a)[8])
 // so that a first-stage butterfly's 8 consecutive outputs (thread b writes
 // 8b .. 8b+7) fall on different banks from its neighbours'.
 __device__ __forceinline__ int dct_pad(int i) { return i + (i >> 3); }
+// Position of twiddle i in the CTA's table: a stage reads it at a stride of
+// N/(Ns R) (1 to 64), and with one pad after every 8 and another after every
+// 64 values, the 8 threads of a 16-byte access phase land on 8 different
+// bank groups at each of those strides.
+__device__ __forceinline__ int dct_twpad(int i) { return i + (i >> 3) + (i >> 6); }
 
 // One Stockham stage of radix R over N points with Ns points already
 // transformed per sub-sequence, in place: butterfly b reads buf[b + r N/R],
 // twiddles by e^{-2 pi i r k/(Ns R)} (k = b mod Ns), and, once every thread
-// of the row has read (`sync`), writes buf[(b - k) R + k + r Ns].
-template <int R, int N, int TPS, class SY>
+// of the row has read (`sync`), writes buf[(b - k) R + k + r Ns].  With
+// MAKHOUL_IN the buffer holds the rows in their natural order and the stage
+// reads sequence point p from Makhoul's position of it (2p for p < N/2,
+// 2N - 1 - 2p above); with MAKHOUL_OUT the stage writes point q there, so
+// the result leaves in the natural order.  Either way the reordering costs no
+// pass of its own, and both halves touch 8 different bank groups per access
+// phase.
+template <int R, int N, int TPS, bool MAKHOUL_IN = false, bool MAKHOUL_OUT = false, class SY>
 __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const double2* tw, SY sync)
 {
     constexpr int NBF = N / R, NB = NBF / TPS;
@@ -120,7 +132,10 @@ __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const dou
 #pragma unroll
     for (int i = 0; i < NB; ++i)
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[i][r] = buf[dct_pad(j + i * TPS + r * NBF)];
+        for (int r = 0; r < R; ++r) {
+            const int p = j + i * TPS + r * NBF;
+            a[i][r] = buf[dct_pad(MAKHOUL_IN ? (p < N / 2 ? 2 * p : 2 * N - 1 - 2 * p) : p)];
+        }
     sync();
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
@@ -130,7 +145,7 @@ __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const dou
             // w^r for r = 1 .. R-1 from w = e^{-2 pi i k/(Ns R)} (one table
             // value, then products: the error grows by about an ulp a factor)
             double2 wr[R];
-            wr[1] = tw[k * (N / (Ns * R))];
+            wr[1] = tw[dct_twpad(k * (N / (Ns * R)))];
 #pragma unroll
             for (int r = 2; r < R; ++r) wr[r] = dct_cmul(wr[r / 2], wr[r - r / 2]);
 #pragma unroll
@@ -139,7 +154,10 @@ __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const dou
         dct_dft<R>(a[i]);
         const int base = (b - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[dct_pad(base + r * Ns)] = a[i][r];
+        for (int r = 0; r < R; ++r) {
+            const int q = base + r * Ns;
+            buf[dct_pad(MAKHOUL_OUT ? (q < N / 2 ? 2 * q : 2 * N - 1 - 2 * q) : q)] = a[i][r];
+        }
     }
     sync();
 }
@@ -167,10 +185,8 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
     const int s = threadIdx.x / TPS, j = threadIdx.x - s * TPS;
     double2* buf = dct_smem + (size_t)s * S::NP;
     double2* tws = dct_smem + (size_t)S::SPC * S::NP;  // the twiddles, shared by the CTA's pairs
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = __ldg(&tw[i]);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[dct_twpad(i)] = __ldg(&tw[i]);
     __syncthreads();
-    // Makhoul's order: input point e sits at position perm(e) of the sequence
-    auto perm = [](int e) { return (e & 1) ? N - 1 - (e >> 1) : (e >> 1); };
     // The threads of one pair synchronise among themselves only: a warp
     // (pairs of up to 256 points share warps, and keep in step), else a named
     // barrier per pair (ids 1..SPC).
@@ -196,8 +212,9 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
     fetch(u);
     for (int64_t base = (int64_t)blockIdx.x * S::SPC; base < npairs; base += stride_units, u += stride_units) {
         if constexpr (TYPE == 2) {
+            // natural order; the first stage reads it in Makhoul's
 #pragma unroll
-            for (int i = 0; i < PER; ++i) buf[dct_pad(perm(j + i * TPS))] = make_double2(p1[i], p2[i]);
+            for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)] = make_double2(p1[i], p2[i]);
         } else {
 #pragma unroll
             for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)] = make_double2(p1[i], p2[i]);
@@ -221,14 +238,22 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
         }
         sync();
         fetch(u + stride_units);  // in flight while this pair is transformed
-        int Ns = 1;
+        // The stages: the first reads type 2's rows in Makhoul's order, the
+        // last writes type 3's results in the rows' order.
+        constexpr bool OUT8 = TYPE == 3 && S::REM == 0;  // the last radix-8 stage is the last
+        dct_stage<8, N, TPS, TYPE == 2, OUT8 && S::L8 == 1>(buf, 1, j, tws, sync);
+        int Ns = 8;
 #pragma unroll 1
-        for (int st = 0; st < S::L8; ++st) {
+        for (int st = 1; st < S::L8 - 1; ++st) {
             dct_stage<8, N, TPS>(buf, Ns, j, tws, sync);
             Ns *= 8;
         }
-        if constexpr (S::REM == 1) dct_stage<2, N, TPS>(buf, Ns, j, tws, sync);
-        else if constexpr (S::REM == 2) dct_stage<4, N, TPS>(buf, Ns, j, tws, sync);
+        if constexpr (S::L8 >= 2) {
+            dct_stage<8, N, TPS, false, OUT8>(buf, Ns, j, tws, sync);
+            Ns *= 8;
+        }
+        if constexpr (S::REM == 1) dct_stage<2, N, TPS, false, TYPE == 3>(buf, Ns, j, tws, sync);
+        else if constexpr (S::REM == 2) dct_stage<4, N, TPS, false, TYPE == 3>(buf, Ns, j, tws, sync);
         const int64_t y1 = 2 * u, y2 = 2 * u + 1;
         const bool l1 = y1 < io.nsys, l2 = y2 < io.nsys;
         double* o1 = io.out + io.out_off + (l1 ? y1 : 0) * io.out_stride;
@@ -245,7 +270,7 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
         } else {
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
-                const double2 Z = buf[dct_pad(perm(j + i * TPS))];
+                const double2 Z = buf[dct_pad(j + i * TPS)];  // in the rows' order (the last stage)
                 if (l1) o1[j + i * TPS] = Z.x;
                 if (l2) o2[j + i * TPS] = Z.y;
             }
