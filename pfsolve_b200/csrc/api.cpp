@@ -346,6 +346,12 @@ int64_t steps_band_registers(int64_t M, int ub, int K)
 // with jw_type % 10 == 3 and K == 2 (for K > 2 the reference multiplies the
 // middle steps by a diagonal it never reloads, pfSolve_ReadWrite.h:1650; the
 // same holds for jw_type % 10 == 3 with upperBanded 0/1).
+// Rows per TMA box of the K-step sweep kernel: 16 (128 bytes of each system
+// per box) up to 4 steps, where the step tables leave shared memory for 11 or
+// 12 warps of them; 8 above, where 16-row boxes would leave 9 to 10 (measured
+// at N = 512, 131 072 RHS: K = 2 and 4 4-7 % faster with 16, K = 8 16 % slower).
+static int seq_chunk_rows(int K) { return K <= 4 ? 16 : 8; }
+
 PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
 {
     const int K = c.numConsecutiveJWIterations, ub = c.upperBanded, jwt = c.jw_type % 10;
@@ -374,21 +380,25 @@ PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
     int maxopt = 0;
     cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
     if (ub != 2 && c.kernelPath != 1) {
-        const SeqStepsVariant* v = find_seq_steps_variant(ub, MV, SV != SV_NONE, K);
         const int64_t Mtab = ub ? M : Mout;
-        const int64_t fixed = (int64_t)seq_steps_smem_bytes(K, Mtab, 0);
-        const int64_t per_warp = (int64_t)seq_steps_smem_bytes(K, Mtab, 1) - fixed;
-        int nw = (int)std::min<int64_t>(v ? v->max_threads / 32 : 0, ((int64_t)maxopt - fixed) / per_warp);
-        if (v && nw >= 4 && allow_max_smem(v->func)) {
-            int blocks = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * nw,
-                                                              seq_steps_smem_bytes(K, Mtab, nw)) == cudaSuccess &&
-                blocks >= 1) {
-                s->seq_v = v;
-                s->seq_NW = nw;
+        for (int CH : {seq_chunk_rows(K), 8}) {
+            const SeqStepsVariant* v = find_seq_steps_variant(ub, MV, SV != SV_NONE, K, CH);
+            const int64_t fixed = (int64_t)seq_steps_smem_bytes(K, Mtab, 0, CH);
+            const int64_t per_warp = (int64_t)seq_steps_smem_bytes(K, Mtab, 1, CH) - fixed;
+            int nw = (int)std::min<int64_t>(v ? v->max_threads / 32 : 0, ((int64_t)maxopt - fixed) / per_warp);
+            if (v && nw >= 4 && allow_max_smem(v->func)) {
+                int blocks = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, v->func, 32 * nw,
+                                                                  seq_steps_smem_bytes(K, Mtab, nw, CH)) ==
+                        cudaSuccess &&
+                    blocks >= 1) {
+                    s->seq_v = v;
+                    s->seq_NW = nw;
+                    break;
+                }
             }
+            cudaGetLastError();
         }
-        cudaGetLastError();
     }
     for (int i = 0; i < n; ++i) {
         const int R = Rs[i];
@@ -820,7 +830,8 @@ PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* l
     io.M = std::max(S.M_in, S.M_out);
     if (io.nsys <= 0) return PFSOLVE_SUCCESS;
     CUtensorMap tin, tout;
-    if (s->seq_v && io.oz0 <= 0 && io.oz1 >= S.M_out && encode_seq_maps(io, S.M_in, S.M_out, &tin, &tout)) {
+    if (s->seq_v && io.oz0 <= 0 && io.oz1 >= S.M_out &&
+        encode_seq_maps(io, S.M_in, S.M_out, s->seq_v->CH, &tin, &tout)) {
         // 32 systems per warp; warps per CTA so that every SM's warps finish
         // their blocks in the same number of rounds
         const int64_t nblk = (io.nsys + 31) / 32;
@@ -829,7 +840,8 @@ PfSolveResult append_steps(PfSolveApplication* app, const PfSolveLaunchParams* l
         const int nw = (int)std::max<int64_t>(1, (nblk + (int64_t)s->num_sms * rounds - 1) / ((int64_t)s->num_sms * rounds));
         const int64_t grid = std::min<int64_t>(s->num_sms, (nblk + nw - 1) / nw);
         const int64_t Mtab = c.upperBanded ? S.M_in : S.M_out;
-        s->seq_v->launch(dim3((unsigned)grid), dim3(32 * nw), seq_steps_smem_bytes(S.K, Mtab, nw), stream, &tin, &tout,
+        s->seq_v->launch(dim3((unsigned)grid), dim3(32 * nw), seq_steps_smem_bytes(S.K, Mtab, nw, s->seq_v->CH), stream,
+                         &tin, &tout,
                          S, io);
         g_launches.fetch_add(1, std::memory_order_relaxed);
         record_launch(PFSOLVE_KERNEL_STEPS_SWEEP, 0, 0, nw, c.upperBanded == 0 ? 1 : 0, c.upperBanded == 1 ? 1 : 0,

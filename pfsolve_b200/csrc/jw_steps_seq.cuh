@@ -16,23 +16,25 @@
 // all lanes at the same address (broadcast).
 //
 // Staging: a warp owns 32 consecutive systems; their rows move in boxes of
-// 8 rows x 32 systems (2 KB, 64-byte swizzle: a lane's 8-byte reads of one row
-// hit 8 distinct bank groups) through four buffers per warp -- two chunks
-// ahead in flight, one being consumed, one receiving results (in place) before
-// its TMA store.  Boxes beyond the system (or below row 0) read as zeros.
+// CH = 8 or 16 rows x 32 systems (2 or 4 KB; 64- or 128-byte swizzle, so that
+// a lane's 8-byte reads of one row hit 8 distinct bank groups) through four
+// buffers per warp -- two chunks ahead in flight, one being consumed, one
+// receiving results (in place) before its TMA store.  Boxes beyond the system
+// (or below row 0) read as zeros.  16-row boxes read 128 bytes of each system
+// per DRAM burst instead of 64, with fewer warps per SM.
 #pragma once
 #include "jw_stream.cuh"
 
 namespace pfb {
 
-constexpr int kSeqChunk = 8;                     // rows per box
-constexpr int kSeqBufBytes = kSeqChunk * 32 * 8;  // 2 KB
 constexpr int kSeqBufs = 4;
-// threads per CTA: 24 warps (85 registers a thread) for K <= 4, 16 warps
-// (128 registers) for 5 to 8 steps
-template <int K>
+__host__ __device__ constexpr int seq_buf_bytes(int CH) { return CH * 32 * 8; }
+// threads per CTA: 24 warps (85 registers a thread) for K <= 4 with 8-row
+// boxes, else 16 warps (128 registers; 16-row boxes leave shared memory for
+// about 12 warps anyway)
+template <int K, int CH>
 struct SeqThreads {
-    static constexpr int v = K > 4 ? 512 : 768;
+    static constexpr int v = (K > 4 || CH > 8) ? 512 : 768;
 };
 
 // Shared table: per step s and row i the pair {o, q} (matvec off-diagonal,
@@ -42,9 +44,9 @@ __host__ __device__ constexpr size_t seq_table_bytes(int K, int64_t Mtab)
 {
     return ((size_t)K * Mtab * 16 + (size_t)Mtab * 8 + 1023) / 1024 * 1024;
 }
-__host__ __device__ constexpr size_t seq_smem_bytes(int K, int64_t Mtab, int NW)
+__host__ __device__ constexpr size_t seq_smem_bytes(int K, int64_t Mtab, int NW, int CH)
 {
-    return 1024 + seq_table_bytes(K, Mtab) + (size_t)NW * kSeqBufs * kSeqBufBytes + (size_t)NW * kSeqBufs * 8;
+    return 1024 + seq_table_bytes(K, Mtab) + (size_t)NW * kSeqBufs * seq_buf_bytes(CH) + (size_t)NW * kSeqBufs * 8;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
@@ -65,13 +67,17 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
 // UB: 1 ascending sweep (upper matvec, lower solve), 0 descending.
 // K: the number of steps (compiled per K, so the step loop unrolls exactly
 // and the step that applies the matvec diagonal -- the first for UB 1, the
-// last for UB 0 -- is known at compile time).
-template <int UB, bool MV, bool SV, int K>
-__global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __grid_constant__ CUtensorMap tm_in,
+// last for UB 0 -- is known at compile time).  CH: rows per box (8 or 16).
+template <int UB, bool MV, bool SV, int K, int CH>
+__global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(const __grid_constant__ CUtensorMap tm_in,
                                                                       const __grid_constant__ CUtensorMap tm_out,
                                                                       const __grid_constant__ JwSteps S, const JwIO io)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int kSeqChunk = CH, kSeqBufBytes = seq_buf_bytes(CH);
+    constexpr int CM = CH - 1;                  // row within a chunk: & CM
+    constexpr int CS = CH == 16 ? 4 : 3;        // chunk of a sweep position: >> CS
+    constexpr int ROWB = CH * 8;                // bytes of a system's row in a box
     constexpr int KMAX = K;
     const int NW = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -124,7 +130,7 @@ __global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __
     auto chunk_row0 = [&](int k) -> int { return UB ? k * kSeqChunk : (cT - k) * kSeqChunk; };
     const int lo = io.iz0 > 0 ? (int)io.iz0 : 0;          // rows read as data: [lo, hi)
     const int hi = io.iz1 < M0 ? (int)io.iz1 : M0;
-    const int sw = (lane >> 1) & 3;
+    const int sw = CH == 16 ? (lane & 7) : ((lane >> 1) & 3);
     const double sC = S.scaleC;
     int Ms[KMAX];
 #pragma unroll
@@ -145,8 +151,10 @@ __global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __
         return v;
     };
     auto sts = [](uint32_t a, double v) { asm volatile("st.shared.f64 [%0], %1;\n" ::"r"(a), "d"(v) : "memory"); };
-    // byte offset of box row rb (0..7) of this lane's system in a buffer
-    auto lane_off = [&](int rb) -> uint32_t { return (uint32_t)(lane * 64 + ((((rb >> 1) ^ sw)) << 4) + ((rb & 1) << 3)); };
+    // byte offset of box row rb (0 .. CH-1) of this lane's system in a buffer
+    auto lane_off = [&](int rb) -> uint32_t {
+        return (uint32_t)(lane * ROWB + ((((rb >> 1) ^ sw)) << 4) + ((rb & 1) << 3));
+    };
     auto buf_of = [&](int k) -> uint32_t { return bufs_u + ((seq + (uint32_t)k) & 3) * kSeqBufBytes; };
     auto issue = [&](int k, int sys0) {
         const uint32_t b = (seq + (uint32_t)k) & 3;
@@ -207,20 +215,20 @@ __global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __
             const uint32_t cbuf = buf_of(k), pbuf = buf_of(k - 1);
             // steady chunk: every step active on rows 1 <= i < M_s, all input
             // rows inside the keep-window, every result row written
-            const bool steady = UB ? (p0 >= K + 1 && p0 + 7 < M0 && rb >= lo && rb + 8 <= hi)
-                                   : (p0 >= K + 1 && p0 + 7 <= R0 && p0 >= R0 - M0 + 2 && p0 >= R0 - Mout + K + 1 &&
-                                      rb >= lo && rb + 8 <= hi);
+            const bool steady = UB ? (p0 >= K + 1 && p0 + CM < M0 && rb >= lo && rb + CH <= hi)
+                                   : (p0 >= K + 1 && p0 + CM <= R0 && p0 >= R0 - M0 + 2 && p0 >= R0 - Mout + K + 1 &&
+                                      rb >= lo && rb + CH <= hi);
             if (steady) {
                 double vin[kSeqChunk];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const double2 w2 = lds2(cbuf + lane * 64 + ((u ^ sw) << 4));
+                for (int u = 0; u < CH / 2; ++u) {
+                    const double2 w2 = lds2(cbuf + lane * ROWB + ((u ^ sw) << 4));
                     if (UB) {
                         vin[2 * u] = w2.x;
                         vin[2 * u + 1] = w2.y;
                     } else {
-                        vin[7 - 2 * u] = w2.x;
-                        vin[6 - 2 * u] = w2.y;
+                        vin[CM - 2 * u] = w2.x;
+                        vin[CM - 1 - 2 * u] = w2.y;
                     }
                 }
                 // table row of step s at o = 0 (ascending: p0 - 1 - s;
@@ -250,8 +258,8 @@ __global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __
                         }
                     }
                     const int oo = o - K;  // result position relative to this chunk
-                    const int qo = oo & 7;
-                    sts((oo >= 0 ? cbuf : pbuf) + lane_off(UB ? qo : 7 - qo), v);
+                    const int qo = oo & CM;
+                    sts((oo >= 0 ? cbuf : pbuf) + lane_off(UB ? qo : CM - qo), v);
                     if (o == K - 1) store_chunk(k - 1, sys0);
                 }
                 continue;
@@ -298,7 +306,7 @@ __global__ void __launch_bounds__(SeqThreads<K>::v) jw_steps_seq_kernel(const __
                 if (!out) continue;
                 // v: result of the last step at sweep position q = p - K
                 const int q = p - K;
-                const int qk = q >> 3, qo = q & 7;
+                const int qk = q >> CS, qo = q & CM;
                 const int qrb = UB ? qo : kSeqChunk - 1 - qo;
                 const int orow = chunk_row0(qk) + qrb;
                 if (orow >= 0 && orow < Mout) sts(buf_of(qk) + lane_off(qrb), v);

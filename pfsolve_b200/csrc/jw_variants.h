@@ -147,18 +147,18 @@ const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV);
 // ascending rows, 0: descending), compiled for K = KMAX steps; systems staged by TMA boxes of
 // 8 rows x 32 systems.
 struct SeqStepsVariant {
-    int UB, MV, SV, KMAX;
+    int UB, MV, SV, KMAX, CH;  // CH: rows per TMA box (8 or 16)
     int max_threads;
     const void* func;
     void (*launch)(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in, const CUtensorMap* out,
                    const JwSteps& S, const JwIO& io);
 };
-const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K);
-size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW);
+const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K, int CH);
+size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW, int CH);
 // 2-D tensor maps {rows, systems} of a K-step launch's right-hand sides: M_in
-// rows read, M_out rows written, boxes of 8 rows x 32 systems; false when the
-// buffers' alignment or stride does not allow them.
-bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* in, CUtensorMap* out);
+// rows read, M_out rows written, boxes of CH (8 or 16) rows x 32 systems;
+// false when the buffers' alignment or stride does not allow them.
+bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, int CH, CUtensorMap* in, CUtensorMap* out);
 
 // Standalone kernels of the block and generic-bandwidth dgbmv applications.
 struct BlockArgs {

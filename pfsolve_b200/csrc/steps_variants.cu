@@ -45,34 +45,36 @@ const StepsVariant* find_steps_variant(int R, int KL, int KU, int SV, int MV)
     return nullptr;
 }
 
-template <int UB, bool MV, bool SV, int K>
+template <int UB, bool MV, bool SV, int K, int CH>
 static void seq_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const CUtensorMap* in,
                           const CUtensorMap* out, const JwSteps& S, const JwIO& io)
 {
-    jw_steps_seq_kernel<UB, MV, SV, K><<<grid, block, smem, st>>>(*in, *out, S, io);
+    jw_steps_seq_kernel<UB, MV, SV, K, CH><<<grid, block, smem, st>>>(*in, *out, S, io);
 }
 
-#define PFB_SQ(UB, MV, SV, K)                                                                         \
-    SeqStepsVariant{UB, MV, SV, K, SeqThreads<K>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, K>, \
-                    &seq_launch_fn<UB, MV, SV, K>}
-// one instance per step count, 2..8
+#define PFB_SQC(UB, MV, SV, K, CH)                                                                            \
+    SeqStepsVariant{UB, MV, SV, K, CH, SeqThreads<K, CH>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, K, CH>, \
+                    &seq_launch_fn<UB, MV, SV, K, CH>}
+#define PFB_SQ(UB, MV, SV, K) PFB_SQC(UB, MV, SV, K, 8), PFB_SQC(UB, MV, SV, K, 16)
+// one instance per step count, 2..8: 16-row boxes up to 4 steps (the default
+// there), 8-row boxes at every count
 #define PFB_SQ3(UB, MV, SV)                                                                               \
-    PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 3), PFB_SQ(UB, MV, SV, 4), PFB_SQ(UB, MV, SV, 5),            \
-        PFB_SQ(UB, MV, SV, 6), PFB_SQ(UB, MV, SV, 7), PFB_SQ(UB, MV, SV, 8)
+    PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 3), PFB_SQ(UB, MV, SV, 4), PFB_SQC(UB, MV, SV, 5, 8),        \
+        PFB_SQC(UB, MV, SV, 6, 8), PFB_SQC(UB, MV, SV, 7, 8), PFB_SQC(UB, MV, SV, 8, 8)
 
 static const SeqStepsVariant kSeqVariants[] = {
     PFB_SQ3(1, true, true), PFB_SQ3(1, true, false), PFB_SQ3(1, false, true),
     PFB_SQ3(0, true, true), PFB_SQ3(0, true, false), PFB_SQ3(0, false, true),
 };
 
-const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K)
+const SeqStepsVariant* find_seq_steps_variant(int UB, int MV, int SV, int K, int CH)
 {
     for (const SeqStepsVariant& v : kSeqVariants)
-        if (v.UB == UB && v.MV == (MV ? 1 : 0) && v.SV == (SV ? 1 : 0) && K == v.KMAX) return &v;
+        if (v.UB == UB && v.MV == (MV ? 1 : 0) && v.SV == (SV ? 1 : 0) && K == v.KMAX && CH == v.CH) return &v;
     return nullptr;
 }
 
-size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW) { return seq_smem_bytes(K, Mtab, NW); }
+size_t seq_steps_smem_bytes(int K, int64_t Mtab, int NW, int CH) { return seq_smem_bytes(K, Mtab, NW, CH); }
 
 // status of the sweep kernel's bounded waits
 PFB_STREAM_STATUS_ACCESSOR(steps_status_fetch_clear)

@@ -107,7 +107,7 @@ bool encode_row_maps(int R_, int LIN, int LOUT, int IB, int IBO, const JwIO& io,
     return encode_rows(out, out0 + io.out_off * es, R, chunks, osets, io.out_stride * es, IBO, es);
 }
 
-bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* in, CUtensorMap* out)
+bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, int CH, CUtensorMap* in, CUtensorMap* out)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn || io.nsys < 1 || io.nsys > INT32_MAX || M_in < 1 || M_out < 1) return false;
@@ -116,15 +116,17 @@ bool encode_seq_maps(const JwIO& io, int64_t M_in, int64_t M_out, CUtensorMap* i
     const int64_t stride = io.in_stride * 8;
     if (reinterpret_cast<uintptr_t>(base) % 16 || stride % 16 || io.in_stride < std::max(M_in, M_out)) return false;
     const cuuint64_t strides[1] = {(cuuint64_t)stride};
-    const cuuint32_t box[2] = {8u, 32u};
+    if (CH != 8 && CH != 16) return false;
+    const cuuint32_t box[2] = {(cuuint32_t)CH, 32u};
     const cuuint32_t estr[2] = {1u, 1u};
     const cuuint64_t din[2] = {(cuuint64_t)M_in, (cuuint64_t)io.nsys};
     const cuuint64_t dout[2] = {(cuuint64_t)M_out, (cuuint64_t)io.nsys};
+    const CUtensorMapSwizzle swz = CH == 16 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
     return fn(in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), din, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
            fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dout, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 

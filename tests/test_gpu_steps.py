@@ -107,11 +107,12 @@ def test_steps_many_systems():
 
 
 def test_steps_sweep_sizes_and_ks():
-    """Every K up to 8 and sizes around the 8-row boxes, both sweep directions."""
+    """Every K up to 8 and sizes around the boxes (16 rows up to K = 4, 8
+    above), both sweep directions."""
     rng = np.random.default_rng(23500)
     for ub in (0, 1):
         for K in range(2, 9):
-            for M in (9, 15, 16, 17, 63, 257):
+            for M in (9, 15, 16, 17, 31, 32, 33, 63, 257):
                 if M - K + 1 < 1:
                     continue
                 case, bands, rhs = _case(rng, M, 70, ub, 10, K)
