@@ -628,7 +628,8 @@ def config3_profile(args):
         tb, x, es = tb.float(), x.float(), 4
         prec = dict(doublePrecision=0, doublePrecisionFloatMemory=1 if args.prec == "f32mem" else 0)
     app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=13, scaleC=1.0,
-              mixedPrecisionRefinement=args.refine, rowsPerThread=args.rows, kernelPath=args.path, **prec)
+              mixedPrecisionRefinement=args.refine, rowsPerThread=args.rows, kernelPath=args.path,
+              stagingBuffers=args.staging, **prec)
     for _ in range(max(1, args.warmup)):
         app.append()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -867,6 +868,8 @@ def main():
     ap.add_argument("--ncplx", type=int, default=N_CPLX, help="complex RHS per GPU (profiling cases only)")
     ap.add_argument("--profile", action="store_true", help="kernel steps only: no e2e leg, no CPU baseline")
     ap.add_argument("--rows", type=int, default=0, help="rows per thread (0: the plan's default)")
+    ap.add_argument("--staging", type=int, default=0,
+                    help="config 3 profiling case: TMA staging buffers per group (stagingBuffers; 0: default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the config 3 / config 4 measurements")
     ap.add_argument("--serve", action="store_true", help="only the serving leg (config 5); prints its JSON")
     ap.add_argument("--workload", default="config2",

@@ -120,11 +120,13 @@ __device__ __forceinline__ int dct_twpad(int i) { return i + (i >> 3) + (i >> 6)
 // of the row has read (`sync`), writes buf[(b - k) R + k + r Ns].  With
 // MAKHOUL_IN the buffer holds the rows in their natural order and the stage
 // reads sequence point p from Makhoul's position of it (2p for p < N/2,
-// 2N - 1 - 2p above); with MAKHOUL_OUT the stage writes point q there, so
-// the result leaves in the natural order.  Either way the reordering costs no
+// 2N - 1 - 2p above); with OUT = 1 the stage writes point q there, so the
+// result leaves in the natural order.  Either way the reordering costs no
 // pass of its own, and both halves touch 8 different bank groups per access
-// phase.
-template <int R, int N, int TPS, bool MAKHOUL_IN = false, bool MAKHOUL_OUT = false, class SY>
+// phase.  OUT = 2 writes the natural order without the pads: type 2's last
+// stage, so that the post-processing's reads of Z_k and Z_{N-k} (ascending
+// and descending runs of 8) each touch 8 different bank groups.
+template <int R, int N, int TPS, bool MAKHOUL_IN = false, int OUT = 0, class SY>
 __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const double2* tw, SY sync)
 {
     constexpr int NBF = N / R, NB = NBF / TPS;
@@ -156,7 +158,8 @@ __device__ __forceinline__ void dct_stage(double2* buf, int Ns, int j, const dou
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int q = base + r * Ns;
-            buf[dct_pad(MAKHOUL_OUT ? (q < N / 2 ? 2 * q : 2 * N - 1 - 2 * q) : q)] = a[i][r];
+            if constexpr (OUT == 2) buf[q] = a[i][r];
+            else buf[dct_pad(OUT == 1 ? (q < N / 2 ? 2 * q : 2 * N - 1 - 2 * q) : q)] = a[i][r];
         }
     }
     sync();
@@ -239,9 +242,11 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
         sync();
         fetch(u + stride_units);  // in flight while this pair is transformed
         // The stages: the first reads type 2's rows in Makhoul's order, the
-        // last writes type 3's results in the rows' order.
-        constexpr bool OUT8 = TYPE == 3 && S::REM == 0;  // the last radix-8 stage is the last
-        dct_stage<8, N, TPS, TYPE == 2, OUT8 && S::L8 == 1>(buf, 1, j, tws, sync);
+        // last writes type 3's results in the rows' order and type 2's
+        // without the pads.
+        constexpr int LAST = TYPE == 3 ? 1 : 2;
+        constexpr int OUT8 = S::REM == 0 ? LAST : 0;  // the last radix-8 stage is the last
+        dct_stage<8, N, TPS, TYPE == 2, S::L8 == 1 ? OUT8 : 0>(buf, 1, j, tws, sync);
         int Ns = 8;
 #pragma unroll 1
         for (int st = 1; st < S::L8 - 1; ++st) {
@@ -252,8 +257,8 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
             dct_stage<8, N, TPS, false, OUT8>(buf, Ns, j, tws, sync);
             Ns *= 8;
         }
-        if constexpr (S::REM == 1) dct_stage<2, N, TPS, false, TYPE == 3>(buf, Ns, j, tws, sync);
-        else if constexpr (S::REM == 2) dct_stage<4, N, TPS, false, TYPE == 3>(buf, Ns, j, tws, sync);
+        if constexpr (S::REM == 1) dct_stage<2, N, TPS, false, LAST>(buf, Ns, j, tws, sync);
+        else if constexpr (S::REM == 2) dct_stage<4, N, TPS, false, LAST>(buf, Ns, j, tws, sync);
         const int64_t y1 = 2 * u, y2 = 2 * u + 1;
         const bool l1 = y1 < io.nsys, l2 = y2 < io.nsys;
         double* o1 = io.out + io.out_off + (l1 ? y1 : 0) * io.out_stride;
@@ -262,7 +267,7 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int k = j + i * TPS;
-                const double2 Z = buf[dct_pad(k)], Zr = buf[dct_pad((N - k) & (N - 1))];
+                const double2 Z = buf[k], Zr = buf[(N - k) & (N - 1)];  // unpadded (the last stage)
                 const double2 c = __ldg(&pt[k]);
                 if (l1) o1[k] = __fma_rn(Z.x + Zr.x, c.x, (Z.y - Zr.y) * c.y);
                 if (l2) o2[k] = __fma_rn(Z.y + Zr.y, c.x, -((Z.x - Zr.x) * c.y));
