@@ -219,14 +219,16 @@ __global__ void __launch_bounds__(DctShape<LOGN>::NT, DctShape<LOGN>::NT <= 256 
 #pragma unroll
             for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)] = make_double2(p1[i], p2[i]);
         } else {
+            // unpadded here, so that the descending reads of X_{N-k} touch 8
+            // different bank groups per access phase
 #pragma unroll
-            for (int i = 0; i < PER; ++i) buf[dct_pad(j + i * TPS)] = make_double2(p1[i], p2[i]);
+            for (int i = 0; i < PER; ++i) buf[j + i * TPS] = make_double2(p1[i], p2[i]);
             sync();
             double2 Xr[PER];
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int k = j + i * TPS;
-                Xr[i] = (k == 0) ? make_double2(0.0, 0.0) : buf[dct_pad(N - k)];
+                Xr[i] = (k == 0) ? make_double2(0.0, 0.0) : buf[N - k];
             }
             sync();
 #pragma unroll
