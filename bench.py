@@ -884,8 +884,8 @@ def main():
     ap.add_argument("--prec", default="f64", choices=["f64", "f32", "f32mem"],
                     help="config 3 profiling case: FP64 storage, or FP32 storage with FP32 or FP64 arithmetic")
     ap.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3, 4],
-                    help="kernelPath: 0 streaming kernel where possible (long systems: two passes where N is a "
-                         "multiple of 8, else the single pass), 1 group kernel only, 2 long systems on the cluster "
+                    help="kernelPath: 0 streaming kernel where possible (long systems: two passes, the single "
+                         "pass for unaligned rows), 1 group kernel only, 2 long systems on the cluster "
                          "kernel, 3 long systems in two passes only, 4 long systems in the single pass only")
     args = ap.parse_args()
     if args.profile:

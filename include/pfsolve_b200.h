@@ -256,9 +256,9 @@ typedef struct {
                                      FP64 residual refinement sweeps, FP64 storage (0: plain FP64) */
     int rowsPerThread;            /* 0: autotuned; else 2, 4, 8, 16 or 32 (32: streaming kernel only) */
     int kernelPath;               /* 0: streaming kernel wherever a launch allows it, else the group
-                                     kernel (long systems: two passes where M is a multiple of 8, with
-                                     the single pass for launches whose rows are not 16-byte aligned;
-                                     else the single pass); 1: group kernel only; 2: long systems on the
+                                     kernel (long systems: two passes, with the single pass for
+                                     launches whose rows are not 16-byte aligned); 1: group kernel
+                                     only; 2: long systems on the
                                      cluster kernel (M <= 16384); 3: long systems in two passes only (no
                                      waits between CTAs); 4: long systems in the single pass only */
     int stagingBuffers;           /* streaming kernel: TMA staging buffers per group of warps, 2..4, so
@@ -485,10 +485,11 @@ PFSOLVE_API PfSolveResult PfSolveGetDeviceStatus(void);
  * groupsPerCTA = warps per CTA), else the K-step kernel; streaming = 5: long
  * systems (M > 4096) over slices of 32 x warpsPerSystem x rowsPerThread rows,
  * groupsPerCTA systems in flight per CTA: two passes with no waits between
- * CTAs (the default where M is a multiple of 8, and kernelPath 3), or a
- * single cooperative pass whose CTAs wait (bounded) for the other slices of
- * each system (other M, kernelPath 4, and a two-pass plan's launches whose
- * rows are not 16-byte aligned); the plan holds a record of 64 bytes
+ * CTAs (the default, and kernelPath 3), or a single cooperative pass whose
+ * CTAs wait (bounded) for the other slices of each system (kernelPath 4, and
+ * a two-pass plan's launches whose rows are not 16-byte aligned); a last
+ * partial chunk of rowsPerThread rows moves by plain loads and stores; the
+ * plan holds a record of 64 bytes
  * and a 4-byte flag per system and slice, and every slice's coefficient
  * table.
  * No counterpart in the reference. */

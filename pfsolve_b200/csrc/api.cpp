@@ -216,17 +216,16 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
 }
 
 // Long-system variant for real systems: the first compiled shape that fits
-// the given form and, for two passes, whose rows per thread divide M (16,
-// else 8: M a multiple of 8); the single pass takes any M (its last partial
-// chunk moves outside the TMA boxes).
+// the given form.  Both forms take any M: a last partial chunk of R rows moves
+// outside the TMA boxes, by its thread's plain loads and stores (measured at
+// M = 4 104: 16 rows per thread with a partial chunk, 0.816 ms, against 8 rows
+// per thread and whole chunks, 0.884 ms).
 const LongVariant* pick_long(AppState* s, int64_t M, bool single, int* NS_out, int* grid_out,
                              const LongVariant* like = nullptr)
 {
-    if (!single && M % 8 != 0) return nullptr;
     for (int shape = 0; shape < kLongShapes; ++shape) {
         const LongVariant* v = find_long_variant(shape, s->KL, s->KU, s->sv);
         if (!v) return nullptr;
-        if (!single && M % v->R != 0) continue;  // whole chunks of R rows (the TMA boxes)
         // a fallback shares the plan's records and tables: same slices
         if (like && (v->R != like->R || v->W != like->W || v->S != like->S || v->tbl_bytes != like->tbl_bytes))
             continue;
@@ -252,11 +251,10 @@ const LongVariant* pick_long(AppState* s, int64_t M, bool single, int* NS_out, i
     return nullptr;
 }
 
-// Long systems (M > 4096, real FP64).  kernelPath 0: two passes where M is a
-// multiple of 8 (measured faster than the single pass at every length), with
-// a single-pass fallback for launches whose rows no tensor map can describe;
-// else the single pass.  kernelPath 3: two passes only; 4: the single pass
-// only.  The per-(system, slice) records are allocated for the plan's
+// Long systems (M > 4096, real FP64).  kernelPath 0: two passes (measured
+// faster than the single pass at every length), with a single-pass fallback
+// for launches whose rows no tensor map can describe.  kernelPath 3: two
+// passes only; 4: the single pass only.  The per-(system, slice) records are allocated for the plan's
 // right-hand sides.
 bool choose_long(AppState* s, int64_t M, int LIN, int LOUT, int SCALE)
 {

@@ -981,6 +981,24 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             }
             // field k of this (system, slice) record
             auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
+            // M not a multiple of R: the tensor maps hold the first Mfull
+            // rows, and the thread whose chunk starts at Mfull moves its rows
+            // between global memory and its staged units itself (stored
+            // below with plain stores); its neighbours read its first unit
+            // as their halo, after the group barrier
+            const bool tail_thr = Mfull < io.M && s_glob == Mfull;
+            if (Mfull < io.M && s0 + C::S > Mfull) {
+                if (tail_thr) {
+    #pragma unroll
+                    for (int j = 0; j < R; ++j) {
+                        const int64_t row = Mfull + j;
+                        const double v = (row < io.M) ? io.in[io.in_off + sys * io.in_stride + row] : 0.0;
+                        reinterpret_cast<double*>(cur + unit_off(j >> 1, t, sw_me))[j & 1] = v;
+                    }
+                }
+                if (W > 1) group_bar(g.bar_id, g.nthr);
+                else __syncwarp();
+            }
             double be[R + KL + KU];
     #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -1095,6 +1113,13 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 const int h = u / IBO, uu = u % IBO;
                 *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
                     make_double2(x[2 * u], x[2 * u + 1]);
+            }
+            if (tail_thr) {  // plain stores (the TMA store drops the tail chunk)
+    #pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    const int64_t row = Mfull + j;
+                    if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
+                }
             }
             fence_proxy_async();
             __syncwarp();

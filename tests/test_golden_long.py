@@ -6,8 +6,8 @@ tests/golden/make_golden.py --only long).
 CPU: the oracle reproduces the tridiagonal fixtures (N = 4352 .. 16384) and the
 single-launch bidiagonal one at N = 4352 (pins it); the reference's bidiagonal
 multi-upload outputs are recorded as a defect (below).
-GPU: the long-system kernels (the default plan: two passes where N is a
-multiple of 8, else the single pass; two passes alone, kernelPath 3; the
+GPU: the long-system kernels (the default plan: two passes, the single pass
+for rows no tensor map can describe; two passes alone, kernelPath 3; the
 single pass alone, kernelPath 4; the cluster kernel, kernelPath 2, up to
 16 384 rows)
 reproduce the fixtures through the C ABI, and match the oracle where the

@@ -2,11 +2,10 @@
 
 Systems of 4 096 < N <= 65 536 rows run over slices of 1 024 rows
 (PfSolveGetShape streaming = 5): by default in two passes with no waits
-between CTAs where N is a multiple of 8 (launches whose rows no tensor map
-can describe fall back to the single pass), else in a single pass, one
-cooperative launch whose CTAs wait (bounded) for the other slices of each
-system; kernelPath 3 asks for two passes only, kernelPath 4 for the single
-pass only.  With
+between CTAs at any N (launches whose rows no tensor map can describe fall
+back to the single pass, one cooperative launch whose CTAs wait (bounded)
+for the other slices of each system); kernelPath 3 asks for two passes
+only, kernelPath 4 for the single pass only.  With
 kernelPath 2, systems of up to 16 384 rows run on one thread-block cluster of
 3, 4, 6 or 8 CTAs per system (streaming = 2).  Every case checks that the
 plan chose the kernel asked for, that the launch ran on it, and that every
@@ -119,9 +118,9 @@ def test_single_pass_unaligned_rows(ub, jwt, M, kw):
 @pytest.mark.parametrize("M", [4097, 5001, 12345, 30001])
 @pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (0, 13)])
 def test_single_pass_any_length(M, ub, jwt):
-    """Lengths that are not a multiple of the rows per thread: the last,
-    partial chunk moves between global memory and its staged rows outside
-    the TMA boxes (single pass only)."""
+    """Odd lengths at the packed stride M: rows no tensor map can describe,
+    so the default plan's launch falls back to the single pass, which moves
+    every row with plain loads and stores."""
     rng = np.random.default_rng(M + 10 * ub + jwt)
     case, bands, rhs = _case(rng, M, 37, ub, jwt)
     x, shape, n = _run(case, bands, rhs)
@@ -130,12 +129,47 @@ def test_single_pass_any_length(M, ub, jwt):
     assert e <= TOL, (e, emax)
 
 
+@pytest.mark.parametrize("path", [0, 3, 4])
+@pytest.mark.parametrize("ub,jwt", [(2, 13), (1, 10), (0, 13), (1, 11)])
+@pytest.mark.parametrize("M", [4104, 4097, 5001, 12345, 30001])
+def test_two_passes_any_length(M, ub, jwt, path):
+    """Lengths that are not a multiple of the 16 rows per thread, with even
+    strides (rows 16-byte aligned): two passes (pivot products for a
+    tridiagonal solve, tables, pass 1, carries unless there is no solve,
+    pass 2; kernelPath 0 and 3) or the single pass (tables and one
+    cooperative launch; kernelPath 4), the last partial chunk moved by its
+    thread with plain loads and stores; in place, against the oracle, with
+    the rows between the systems left as they were."""
+    import torch
+
+    from pfsolve_b200.api import App, launch_count
+    rng = np.random.default_rng(M + 7 * ub + jwt)
+    stride = M + (M & 1) + 2
+    case, bands, rhs = _case(rng, M, 37, ub, jwt, cfg_outputBufferStride=stride)
+    tb = torch.from_numpy(np.ascontiguousarray(bands)).cuda()
+    x = torch.from_numpy(np.array(rhs, copy=True)).cuda()
+    app = App(buffer=tb, outputBuffer=x, **J.case_fields(case, kernelPath=path))
+    n0 = launch_count()
+    app.append(**J.launch_fields(case))
+    torch.cuda.synchronize()
+    solve = not (ub == 1 and jwt == 11)
+    assert launch_count() - n0 == (1 if ub == 2 else 0) + (2 if path == 4 else (4 if solve else 3))
+    got = x.cpu().numpy()
+    app.close()
+    e, emax = J.rel_err(got, O.jw_step(case, bands, rhs, "q"), case)
+    assert e <= TOL, (e, emax)
+    gaps = np.concatenate([got[y * stride + M:(y + 1) * stride] for y in range(37)])
+    ref_gaps = np.concatenate([rhs[y * stride + M:(y + 1) * stride] for y in range(37)])
+    np.testing.assert_array_equal(gaps, ref_gaps)
+
+
 @pytest.mark.parametrize("M,path,launches", [(16384, 0, 5), (16384, 4, 3), (12345, 0, 3)])
 def test_long_default_forms_and_repeats(M, path, launches):
-    """The default plan runs two passes where N is a multiple of 8 (pivot
-    products, tables, pass 1, carries, pass 2: five launches for a
-    tridiagonal solve) and the single pass otherwise (tables and one
-    cooperative launch: three); kernelPath 4 asks for the single pass.
+    """The default plan runs two passes (pivot products, tables, pass 1,
+    carries, pass 2: five launches for a tridiagonal solve), and the single
+    pass (tables and one cooperative launch: three) for launches whose rows
+    no tensor map can describe (M = 12 345 at a stride of M); kernelPath 4
+    asks for the single pass.
     Repeated launches of one plan (new flag epochs each time) give the same
     result."""
     import torch
