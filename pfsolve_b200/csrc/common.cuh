@@ -171,6 +171,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool va
     int src = valid ? 16 : 0;
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src) : "memory");
 }
+// 16 bytes of shared memory from the first `nbytes` (0, 4, 8, 12 or 16)
+// bytes at gmem, the rest zero-filled; no byte beyond them is read.
+__device__ __forceinline__ void cp_async16n(void* smem, const void* gmem, int nbytes)
+{
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(nbytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }

@@ -111,13 +111,15 @@ struct LgBufs {
 // Shared memory: table | scratch | 8 doubles | slice constants (Af, Ab, Psi
 // of up to kLgMaxSlices slices, 4 doubles each) | mbarriers | (align 1024) |
 // buffers | per row of the slice, 16 bytes: the PASS 1 weights (alpha, beta),
-// or in the single pass the carry responses (psi, G).
+// or in the single pass the carry responses (psi, G) | in the solve passes,
+// two slots of R doubles per group for a last partial chunk.
 template <class C, int NBUF = 2>
 __host__ __device__ constexpr size_t lg_smem_bytes()
 {
     return C::B::TBL + (size_t)C::G * C::W * kScratchPerWarp * sizeof(double) + 8 * sizeof(double) +
            (size_t)kLgMaxSlices * 4 * sizeof(double) + (size_t)C::G * NBUF * sizeof(uint64_t) + 1024 +
-           (size_t)C::G * NBUF * C::B::BUF + (size_t)C::S * 16;
+           (size_t)C::G * NBUF * C::B::BUF + (size_t)C::S * 16 +
+           (NBUF == 2 ? (size_t)C::G * 2 * C::R * sizeof(double) : 0);  // the solve passes' tail slots
 }
 
 // ---- Coefficient table of slice c (rows c*S + [0, S)), built by all threads
@@ -468,6 +470,8 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
     // PASS 1 weights: row tt * R + jj at [jj * T + tt] (consecutive threads,
     // consecutive entries)
     double2* ab_s = reinterpret_cast<double2*>(after + pad + (size_t)C::G * NBUF * BC::BUF);
+    // solve passes: this group's two slots for a last partial chunk of R rows
+    double* tail_s = reinterpret_cast<double*>(ab_s + C::S) + (size_t)grp * 2 * R;
     auto ab_g_of = [&](int cc) -> double2* {
         return reinterpret_cast<double2*>(tab + (size_t)NS * (BC::TBL / sizeof(double))) + (size_t)cc * C::S;
     };
@@ -962,7 +966,26 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
         ylim = seg_end - (int64_t)cs * nsys;
         seg = seg_end;
         if (stop) continue;
+        // M not a multiple of R: the tensor maps hold the first Mfull rows,
+        // and the thread whose chunk starts at Mfull (in this segment's
+        // slice, if at all) copies its rows of each system into a slot of its
+        // own by cp.async, beside the system's TMA load, stages them after the
+        // load's wait, and stores its results with plain stores
+        const bool tail_thr = Mfull < io.M && s_glob == Mfull;
+        const bool tail_slice = Mfull < io.M && s0 + C::S > Mfull;
+        auto tail_copy = [&](int slot, int64_t y) {
+            const double* src = io.in + io.in_off + y * io.in_stride + Mfull;
+            double* dst = tail_s + slot * R;
+            const int64_t have = io.M - Mfull;  // rows present, 1 .. R-1
+#pragma unroll
+            for (int j = 0; j < R; j += 2) {
+                const int64_t nb = have - j <= 0 ? 0 : (have - j >= 2 ? 16 : 8);
+                cp_async16n(dst + j, nb ? src + j : src, (int)nb);
+            }
+            cp_async_commit();
+        };
         Scal sc = fetch(sys), scn;
+        if (sys < ylim && tail_thr) tail_copy(kk & 1, sys);
         if (sys < ylim && lane == 0) {
             if (PASS == 2) bulk_wait_read_all();  // the store from this buffer (two items ago) has read it
             issue_load((kk & 1) ? buf1 : buf0, (kk & 1) ? bar1 : bar0, sys);
@@ -981,20 +1004,17 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             }
             // field k of this (system, slice) record
             auto rec = [&](int k) -> double& { return red[((size_t)c * kLgRed + k) * nsys + sys]; };
-            // M not a multiple of R: the tensor maps hold the first Mfull
-            // rows, and the thread whose chunk starts at Mfull moves its rows
-            // between global memory and its staged units itself (stored
-            // below with plain stores); its neighbours read its first unit
-            // as their halo, after the group barrier
-            const bool tail_thr = Mfull < io.M && s_glob == Mfull;
-            if (Mfull < io.M && s0 + C::S > Mfull) {
+            // the partial chunk's rows into the staged units (the TMA filled
+            // them with zeros); its neighbours read its first unit as their
+            // halo, after the group barrier
+            if (tail_slice) {
                 if (tail_thr) {
+                    cp_async_wait<0>();
+                    const double* src = tail_s + (kk & 1) * R;
     #pragma unroll
-                    for (int j = 0; j < R; ++j) {
-                        const int64_t row = Mfull + j;
-                        const double v = (row < io.M) ? io.in[io.in_off + sys * io.in_stride + row] : 0.0;
-                        reinterpret_cast<double*>(cur + unit_off(j >> 1, t, sw_me))[j & 1] = v;
-                    }
+                    for (int u = 0; u < U; ++u)
+                        *reinterpret_cast<double2*>(cur + unit_off(u, t, sw_me)) =
+                            *reinterpret_cast<const double2*>(src + 2 * u);
                 }
                 if (W > 1) group_bar(g.bar_id, g.nthr);
                 else __syncwarp();
@@ -1060,6 +1080,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             // (all of them have passed this iteration's group_and since) and, in
             // pass 2, stored from: once this warp's stores have read it, it takes
             // the next system
+            if (more && tail_thr) tail_copy((kk + 1) & 1, sys + per);
             if (more && lane == 0) {
                 if (PASS == 2) bulk_wait_read_all();
                 issue_load(nxt, (kk & 1) ? bar0 : bar1, sys + per);
@@ -1126,6 +1147,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             if (lane == 0) issue_store(cur, sys);
         }
     }
+    cp_async_wait<0>();  // a partial chunk's copy of an item a wait gave up on
     if (lane == 0) bulk_wait_all();
 }
 
