@@ -80,7 +80,17 @@ __device__ __forceinline__ dd operator/(dd a, dd b)
 
 __device__ __forceinline__ bool dd_is_zero(dd a) { return a.hi == 0.0; }
 
-// a*v + w
-__device__ __forceinline__ dd dd_fma(dd a, dd v, dd w) { return a * v + w; }
+// a*v + w: the product's two terms (two_prod and the cross terms) go into
+// the accurate addition as they are, without the quick_two_sum that would
+// renormalise them first -- the addition's two_sum steps are exact for any
+// pair of doubles, and the result is renormalised at its end.  Three FP64
+// operations fewer than a * v + w.
+__device__ __forceinline__ dd dd_fma(dd a, dd v, dd w)
+{
+    dd p = two_prod(a.hi, v.hi);
+    p.lo = __fma_rn(a.hi, v.lo, p.lo);
+    p.lo = __fma_rn(a.lo, v.hi, p.lo);
+    return p + w;
+}
 
 }  // namespace pfb
