@@ -84,8 +84,8 @@ __device__ __forceinline__ void group_matrix_scan_dd(GroupCtx& g, dd& a, dd& b, 
     for (int s = 1; s < 32; s <<= 1) {
         const dd pa = O::shfl_up(a, s), pb = O::shfl_up(b, s), pc = O::shfl_up(c, s), pd = O::shfl_up(d, s);
         if (g.lane >= s) {
-            const dd na = a * pa + b * pc, nb = a * pb + b * pd;
-            const dd nc = c * pa + d * pc, nd = c * pb + d * pd;
+            const dd na = dd_fma(a, pa, b * pc), nb = dd_fma(a, pb, b * pd);
+            const dd nc = dd_fma(c, pa, d * pc), nd = dd_fma(c, pb, d * pd);
             a = na; b = nb; c = nc; d = nd;
             renorm2x2_dd(a, b, c, d);
         }
@@ -104,17 +104,17 @@ __device__ __forceinline__ void group_matrix_scan_dd(GroupCtx& g, dd& a, dd& b, 
         for (int w = 0; w < g.wg; ++w) {
             const double* o = g.warp_area(w) + 16;
             const dd oa = load_v<dd>(o), ob = load_v<dd>(o + 2), oc = load_v<dd>(o + 4), od = load_v<dd>(o + 6);
-            const dd na = oa * wa + ob * wc, nb = oa * wb + ob * wd;
-            const dd nc = oc * wa + od * wc, nd = oc * wb + od * wd;
+            const dd na = dd_fma(oa, wa, ob * wc), nb = dd_fma(oa, wb, ob * wd);
+            const dd nc = dd_fma(oc, wa, od * wc), nd = dd_fma(oc, wb, od * wd);
             wa = na; wb = nb; wc = nc; wd = nd;
             renorm2x2_dd(wa, wb, wc, wd);
         }
         group_bar(g.bar_id, g.nthr);
     }
-    a = ea * wa + eb * wc;
-    b = ea * wb + eb * wd;
-    c = ec * wa + ed * wc;
-    d = ec * wb + ed * wd;
+    a = dd_fma(ea, wa, eb * wc);
+    b = dd_fma(ea, wb, eb * wd);
+    c = dd_fma(ec, wa, ed * wc);
+    d = dd_fma(ec, wb, ed * wd);
 }
 
 template <class C>
