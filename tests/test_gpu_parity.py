@@ -129,10 +129,8 @@ def test_unsupported_combinations_return_codes():
         with pytest.raises(capi.PfSolveError) as ei:
             App(buffer=b, outputBuffer=r, M_size=64, size=(64, 1), doublePrecision=1, **fields)
         assert ei.value.code == code
-    # longer than 64 slices of 1024 rows; a long system whose length is not a
-    # multiple of 8 rows in the two-pass form (kernelPath 3; the single pass
-    # takes it)
-    for M, path in ((65544, 0), (5001, 3)):
+    # longer than 64 slices of 1024 rows, in either long-system form
+    for M, path in ((65544, 0), (65544, 3)):
         with pytest.raises(capi.PfSolveError) as ei:
             App(buffer=b, outputBuffer=r, M_size=M, size=(M, 1), doublePrecision=1, upperBanded=2, jw_type=13,
                 kernelPath=path)
