@@ -1011,7 +1011,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 if (tail_thr) {
                     cp_async_wait<0>();
                     const double* src = tail_s + (kk & 1) * R;
-    #pragma unroll
+#pragma unroll
                     for (int u = 0; u < U; ++u)
                         *reinterpret_cast<double2*>(cur + unit_off(u, t, sw_me)) =
                             *reinterpret_cast<const double2*>(src + 2 * u);
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 else __syncwarp();
             }
             double be[R + KL + KU];
-    #pragma unroll
+#pragma unroll
             for (int u = 0; u < U; ++u) {
                 const double2 v = *reinterpret_cast<const double2*>(cur + unit_off(u, t, sw_me));
                 be[KL + 2 * u] = v.x;
@@ -1055,22 +1055,22 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 if constexpr (KU > 1) be[KL + R + 1] = nv.y;
             }
             if (win_partial) {
-    #pragma unroll
+#pragma unroll
                 for (int i = 0; i < R + KL + KU; ++i) {
                     const int64_t row = s_glob - KL + i;
                     if (row < io.iz0 || row >= io.iz1) be[i] = 0.0;
                 }
             }
-    #pragma unroll
+#pragma unroll
             for (int u = 0; u < U; ++u) {
                 double2 wc[NB];
-    #pragma unroll
+#pragma unroll
                 for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
-    #pragma unroll
+#pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     const int j = 2 * u + e;
                     double acc = (e ? wc[0].y : wc[0].x) * be[j];
-    #pragma unroll
+#pragma unroll
                     for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
                     be[j] = acc;
                 }
@@ -1089,13 +1089,13 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 if constexpr (BC::FWD || BC::BWD) {
                     // Bf = sum alpha g, Bb0 = sum beta g over the slice
                     double sa = 0.0, sb = 0.0;
-    #pragma unroll
+#pragma unroll
                     for (int j = 0; j < R; ++j) {
                         const double2 w = ab_s[j * T + t];
                         sa = __fma_rn(w.x, x[j], sa);
                         sb = __fma_rn(w.y, x[j], sb);
                     }
-    #pragma unroll
+#pragma unroll
                     for (int o = 16; o > 0; o >>= 1) {
                         sa += __shfl_xor_sync(FULL, sa, o);
                         sb += __shfl_xor_sync(FULL, sb, o);
@@ -1129,14 +1129,14 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
             }
             if (C::SV != SV_NONE && s_glob == 0) x[0] = op.scaleC * x[0];
             __syncwarp();
-    #pragma unroll
+#pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int h = u / IBO, uu = u % IBO;
                 *reinterpret_cast<double2*>(cur + (size_t)(h * T + t) * ROWBO + ((uu ^ swo_me) << 4)) =
                     make_double2(x[2 * u], x[2 * u + 1]);
             }
             if (tail_thr) {  // plain stores (the TMA store drops the tail chunk)
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < R; ++j) {
                     const int64_t row = Mfull + j;
                     if (row < io.M && row >= io.oz0 && row < io.oz1) io.out[io.out_off + sys * io.out_stride + row] = x[j];
