@@ -345,10 +345,11 @@ int64_t steps_band_registers(int64_t M, int ub, int K)
 // middle steps by a diagonal it never reloads, pfSolve_ReadWrite.h:1650; the
 // same holds for jw_type % 10 == 3 with upperBanded 0/1).
 // Rows per TMA box of the K-step sweep kernel: 16 (128 bytes of each system
-// per box) up to 4 steps, where the step tables leave shared memory for 11 or
-// 12 warps of them; 8 above, where 16-row boxes would leave 9 to 10 (measured
-// at N = 512, 131 072 RHS: K = 2 and 4 4-7 % faster with 16, K = 8 16 % slower).
-static int seq_chunk_rows(int K) { return K <= 4 ? 16 : 8; }
+// per box) up to 6 steps, 8 above, where the step tables leave room for too
+// few warps of 16-row buffers (measured at N = 512, 131 072 RHS with 16-row
+// boxes against 8: K = 2, 4 4-7 % faster; K = 5, 6 (three buffers a warp)
+// 4 % faster; K = 8 9 % slower).
+static int seq_chunk_rows(int K) { return K <= 6 ? 16 : 8; }
 
 PfSolveResult plan_steps(AppState* s, const PfSolveConfiguration& c)
 {

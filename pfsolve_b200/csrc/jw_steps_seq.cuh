@@ -27,7 +27,10 @@
 
 namespace pfb {
 
-constexpr int kSeqBufs = 4;
+// Buffers per warp: four (two chunks ahead in flight); three for 16-row
+// boxes above four steps (one chunk of 4 KB ahead), so that 14-15 warps fit
+// beside the larger step tables instead of 9-10.
+__host__ __device__ constexpr int seq_nbufs(int K, int CH) { return (CH == 16 && K > 4) ? 3 : 4; }
 __host__ __device__ constexpr int seq_buf_bytes(int CH) { return CH * 32 * 8; }
 // threads per CTA: 24 warps (85 registers a thread) for K <= 4 with 8-row
 // boxes, else 16 warps (128 registers; 16-row boxes leave shared memory for
@@ -46,7 +49,8 @@ __host__ __device__ constexpr size_t seq_table_bytes(int K, int64_t Mtab)
 }
 __host__ __device__ constexpr size_t seq_smem_bytes(int K, int64_t Mtab, int NW, int CH)
 {
-    return 1024 + seq_table_bytes(K, Mtab) + (size_t)NW * kSeqBufs * seq_buf_bytes(CH) + (size_t)NW * kSeqBufs * 8;
+    return 1024 + seq_table_bytes(K, Mtab) + (size_t)NW * seq_nbufs(K, CH) * seq_buf_bytes(CH) +
+           (size_t)NW * seq_nbufs(K, CH) * 8;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
@@ -74,7 +78,7 @@ __global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(cons
                                                                       const __grid_constant__ JwSteps S, const JwIO io)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int kSeqChunk = CH, kSeqBufBytes = seq_buf_bytes(CH);
+    constexpr int kSeqChunk = CH, kSeqBufBytes = seq_buf_bytes(CH), kSeqBufs = seq_nbufs(K, CH);
     constexpr int CM = CH - 1;                  // row within a chunk: & CM
     constexpr int CS = CH == 16 ? 4 : 3;        // chunk of a sweep position: >> CS
     constexpr int ROWB = CH * 8;                // bytes of a system's row in a box
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(cons
     for (int s = 0; s < KMAX; ++s) Ms[s] = s < K ? (int)S.st[s].M : 0;
     const int64_t nblk = (io.nsys + 31) / 32;
     const uint32_t bufs_u = smem_u32(bufs);
-    uint32_t seq = 0;  // chunk loads issued by this warp so far (buffer seq & 3)
+    uint32_t seq = 0;  // chunk loads issued by this warp so far (buffer seq % kSeqBufs)
     bool ok = true;
 
     auto lds = [](uint32_t a) -> double {
@@ -155,9 +159,9 @@ __global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(cons
     auto lane_off = [&](int rb) -> uint32_t {
         return (uint32_t)(lane * ROWB + ((((rb >> 1) ^ sw)) << 4) + ((rb & 1) << 3));
     };
-    auto buf_of = [&](int k) -> uint32_t { return bufs_u + ((seq + (uint32_t)k) & 3) * kSeqBufBytes; };
+    auto buf_of = [&](int k) -> uint32_t { return bufs_u + ((seq + (uint32_t)k) % kSeqBufs) * kSeqBufBytes; };
     auto issue = [&](int k, int sys0) {
-        const uint32_t b = (seq + (uint32_t)k) & 3;
+        const uint32_t b = (seq + (uint32_t)k) % kSeqBufs;
         const uint32_t bar = smem_u32(&bars[b]);
         mbar_arrive_expect_tx(bar, kSeqBufBytes);
         tma_load_2d(bufs_u + b * kSeqBufBytes, &tm_in, chunk_row0(k), sys0, bar);
@@ -188,7 +192,7 @@ __global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(cons
         const int sys0 = (int)(blk * 32);
         if (lane == 0) {
             bulk_wait_read_all();  // the previous block's stores have read their buffers
-            for (int k = 0; k < 3 && k < NK; ++k) issue(k, sys0);
+            for (int k = 0; k < kSeqBufs - 1 && k < NK; ++k) issue(k, sys0);
         }
         __syncwarp();
         double xa[KMAX], zp[KMAX];
@@ -198,13 +202,16 @@ __global__ void __launch_bounds__(SeqThreads<K, CH>::v) jw_steps_seq_kernel(cons
             zp[s] = 0.0;
         }
         for (int k = 0; k < NK; ++k) {
-            // chunk k: its load was issued two chunks ahead (or before the sweep)
+            // chunk k: its load was issued kSeqBufs - 2 chunks ahead (or
+            // before the sweep)
             if (lane == 0 && k >= 1) {
-                bulk_wait_read_all();  // chunk k-2's store has read buffer (k+2) & 3
-                if (k + 2 < NK) issue(k + 2, sys0);
+                // chunk k-2's store (issued during chunk k-1) has read the
+                // buffer that chunk k + kSeqBufs - 2 takes
+                bulk_wait_read_all();
+                if (k + kSeqBufs - 2 < NK) issue(k + kSeqBufs - 2, sys0);
             }
-            const uint32_t b = (seq + (uint32_t)k) & 3;
-            bool w = mbar_wait_bounded(smem_u32(&bars[b]), ((seq + (uint32_t)k) >> 2) & 1);
+            const uint32_t b = (seq + (uint32_t)k) % kSeqBufs;
+            bool w = mbar_wait_bounded(smem_u32(&bars[b]), ((seq + (uint32_t)k) / kSeqBufs) & 1);
             w = __all_sync(FULL, w);
             if (!w) {
                 if (lane == 0) atomicOr(&g_stream_status, kStatusWaitTimeout);

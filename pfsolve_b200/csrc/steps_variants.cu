@@ -56,11 +56,11 @@ static void seq_launch_fn(dim3 grid, dim3 block, size_t smem, cudaStream_t st, c
     SeqStepsVariant{UB, MV, SV, K, CH, SeqThreads<K, CH>::v, (const void*)&jw_steps_seq_kernel<UB, MV, SV, K, CH>, \
                     &seq_launch_fn<UB, MV, SV, K, CH>}
 #define PFB_SQ(UB, MV, SV, K) PFB_SQC(UB, MV, SV, K, 8), PFB_SQC(UB, MV, SV, K, 16)
-// one instance per step count, 2..8: 16-row boxes up to 4 steps (the default
+// one instance per step count, 2..8: 16-row boxes up to 6 steps (the default
 // there), 8-row boxes at every count
 #define PFB_SQ3(UB, MV, SV)                                                                               \
-    PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 3), PFB_SQ(UB, MV, SV, 4), PFB_SQC(UB, MV, SV, 5, 8),        \
-        PFB_SQC(UB, MV, SV, 6, 8), PFB_SQC(UB, MV, SV, 7, 8), PFB_SQC(UB, MV, SV, 8, 8)
+    PFB_SQ(UB, MV, SV, 2), PFB_SQ(UB, MV, SV, 3), PFB_SQ(UB, MV, SV, 4), PFB_SQ(UB, MV, SV, 5),            \
+        PFB_SQ(UB, MV, SV, 6), PFB_SQC(UB, MV, SV, 7, 8), PFB_SQC(UB, MV, SV, 8, 8)
 
 static const SeqStepsVariant kSeqVariants[] = {
     PFB_SQ3(1, true, true), PFB_SQ3(1, true, false), PFB_SQ3(1, false, true),
