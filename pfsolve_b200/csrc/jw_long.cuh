@@ -637,7 +637,14 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                 const double nn = (k == R - 1) ? nl_after : nlv[k + 1];
                 beta = __fma_rn(nn, beta, gam[k]);
                 if (k < R - 1) alpha *= nlv[k + 1];
-                ab_g[k * T + t] = make_double2(BC::FWD ? alpha : 0.0, BC::BWD ? beta : 0.0);
+                // a one-band matvec (g_k = w_k b_k) folds into the weights:
+                // pass 1 then reduces the staged rows b directly
+                double wk = 1.0;
+                if constexpr (NB == 1) {
+                    const double2 w2 = coef(0, k >> 1);
+                    wk = (k & 1) ? w2.y : w2.x;
+                }
+                ab_g[k * T + t] = make_double2(BC::FWD ? alpha * wk : 0.0, BC::BWD ? beta * wk : 0.0);
             }
         }
         return;
@@ -1061,18 +1068,22 @@ __global__ void __launch_bounds__(C::NT) jw_long_kernel(const __grid_constant__ 
                     if (row < io.iz0 || row >= io.iz1) be[i] = 0.0;
                 }
             }
+            // the matvec (pass 1 with a one-band matvec: folded into its
+            // weights by the table pass)
+            if constexpr (!(PASS == 1 && NB == 1)) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                double2 wc[NB];
+                for (int u = 0; u < U; ++u) {
+                    double2 wc[NB];
 #pragma unroll
-                for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
+                    for (int q = 0; q < NB; ++q) wc[q] = coef(q, u);
 #pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int j = 2 * u + e;
-                    double acc = (e ? wc[0].y : wc[0].x) * be[j];
+                    for (int e = 0; e < 2; ++e) {
+                        const int j = 2 * u + e;
+                        double acc = (e ? wc[0].y : wc[0].x) * be[j];
 #pragma unroll
-                    for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
-                    be[j] = acc;
+                        for (int q = 1; q < NB; ++q) acc = __fma_rn(e ? wc[q].y : wc[q].x, be[j + q], acc);
+                        be[j] = acc;
+                    }
                 }
             }
             double (&x)[R + KL + KU] = be;
