@@ -703,7 +703,7 @@ def dct_measure(N, B, dct_type=2, steps=10, warmup=3):
             "gbs": 2.0 * N * 8 * B / (ms * 1e-3) / 1e9}
 
 
-def alt_measure(M, B, steps=10, warmup=3, path=0):
+def alt_measure(M, B, steps=10, warmup=3, path=0, rows=0):
     """ALT stride-2 mode (jw_type 113: the even and the odd rows of each row
     set are two tridiagonal systems), M rows per row set, B real row sets in
     place, FP64: the streaming kernel (path 1: the group kernel).  Algorithmic
@@ -717,7 +717,7 @@ def alt_measure(M, B, steps=10, warmup=3, path=0):
     tb = torch.from_numpy(WL.alt_bands(rng, M, 2)).cuda()
     x = torch.from_numpy(rng.uniform(-1, 1, M * B)).cuda()
     app = App(buffer=tb, outputBuffer=x, M_size=M, size=(M, B), upperBanded=2, jw_type=113, doublePrecision=1,
-              scaleC=1.0, kernelPath=path)
+              scaleC=1.0, kernelPath=path, rowsPerThread=rows)
     for _ in range(max(1, warmup)):
         app.append()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -918,7 +918,8 @@ def main():
                                                                  steps=args.steps, warmup=args.warmup))), flush=True)
         return
     if args.profile and args.workload == "alt":
-        print(json.dumps(alt_measure(args.m, args.ncplx, steps=args.steps, warmup=args.warmup, path=args.path)),
+        print(json.dumps(alt_measure(args.m, args.ncplx, steps=args.steps, warmup=args.warmup, path=args.path,
+                                     rows=args.rows)),
               flush=True)
         return
     try:
