@@ -263,7 +263,9 @@ typedef struct {
                                      waits between CTAs); 4: long systems in the single pass only */
     int stagingBuffers;           /* streaming kernel: TMA staging buffers per group of warps, 2..4, so
                                      that up to stagingBuffers - 1 systems' loads are in flight while
-                                     one is solved (0: 2); more buffers can mean fewer groups per CTA */
+                                     one is solved (0: 2, or 3 for FP32 storage and arithmetic where
+                                     they fit beside as many groups); more buffers can mean fewer
+                                     groups per CTA */
 } PfSolveConfiguration;
 
 /* Launch-time values (pfSolve_Structs.h:383-449). */

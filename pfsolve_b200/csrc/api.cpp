@@ -188,11 +188,14 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
             find_stream_variant(cand[i][0], cand[i][1], s->KL, s->KU, s->sv, LIN, LOUT, SCALE, s->prec, alt);
         if (!v) continue;
         const int T = 32 * v->W;
-        // Most groups first, two staging buffers per group (a caller's
-        // request: the most groups that fit with it).  Measured at N = 512
-        // (131 072 systems): 3 or 4 buffers per group were no faster for FP64
-        // or the mixed mode and at most 4 % faster for FP32 storage, and
-        // where they cost groups (the config-2 chain) much slower.
+        // Most groups first, two staging buffers per group -- three for FP32
+        // storage and arithmetic where they fit beside as many groups -- (a
+        // caller's request: the most groups that fit with it).  Measured at
+        // N = 512 (131 072 systems): 3 or 4 buffers per group were no faster
+        // for FP64, the mixed mode or FP64 arithmetic on FP32 storage, 3 %
+        // faster for FP32 (its 2-KB systems, solved fastest, need more of them
+        // in flight), and where they cost groups (the config-2 chain) much
+        // slower.
         auto fits = [&](int G, int nb, int* blocks) {
             const size_t smem = v->smem_bytes(G, nb);
             if (smem > 227 * 1024 || !allow_max_smem(v->func)) return false;
@@ -202,7 +205,8 @@ bool choose_stream(AppState* s, int64_t M, int LIN, int LOUT, int SCALE, bool al
         const bool req = s->nbuf_req >= 2 && s->nbuf_req <= kStMaxBuffers;
         for (int G = std::min(v->max_threads / T, 15); G >= 1; --G) {
             int blocks = 0;
-            const int nb = req ? s->nbuf_req : 2;
+            int nb = req ? s->nbuf_req : 2;
+            if (!req && s->prec == PREC_F32 && fits(G, 3, &blocks)) nb = 3;
             if (!fits(G, nb, &blocks)) continue;
             s->stream_v = v;
             s->stream_G = G;

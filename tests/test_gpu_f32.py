@@ -75,6 +75,20 @@ def test_jw_modes(prec, ub, jwt, M):
 
 
 @pytest.mark.parametrize("prec", [F32, F32MEM])
+@pytest.mark.parametrize("nb", [0, 2, 3, 4])
+def test_staging_buffers(prec, nb):
+    """stagingBuffers 2-4 (0: the default, three for FP32 storage and
+    arithmetic where they fit beside as many groups as two) on the streaming
+    kernel's steady state."""
+    rng = np.random.default_rng(610 + nb)
+    case, bands, rhs = jw_case32(rng, 512, 8193, 2, 13)
+    x, info = run_f32(case, bands, rhs, prec, stagingBuffers=nb)
+    assert info["kernel"] == capi.PFSOLVE_KERNEL_STREAMING, info
+    ref = O.jw_step(case, bands, rhs, "f32", nthreads=8)
+    assert rel(x, ref, case) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [F32, F32MEM])
 @pytest.mark.parametrize("M,B", [(512, 4097), (2048, 300), (4096, 150)])
 @pytest.mark.parametrize("path", [0, 1])
 def test_streaming_and_group_kernels(prec, M, B, path):

@@ -227,3 +227,19 @@ def test_streaming_mixed_chain_config2_form():
     got = got.reshape(Y, M, 2)
     e = max(np.linalg.norm(got[k] - ref[k]) / np.linalg.norm(ref[k]) for k in range(Y))
     assert e <= 1e-12, e
+
+
+@pytest.mark.parametrize("nb", [0, 2, 3, 4])
+@pytest.mark.parametrize("refine", [0, 2])
+@pytest.mark.parametrize("M,B,ub,jwt", [(512, 4097, 2, 13), (1024, 3001, 1, 10), (256, 6000, 0, 13)])
+def test_staging_buffers(nb, refine, M, B, ub, jwt):
+    """stagingBuffers (TMA staging buffers per group, 2-4; 0: the default):
+    enough systems that every group cycles through its buffers many times,
+    FP64 and the mixed mode (2 refinement sweeps), against the __float128
+    oracle (1e-13; mixed: 1e-12)."""
+    rng = np.random.default_rng(M + B + nb + refine)
+    case, bands, rhs = _case(rng, M, B, ub, jwt)
+    x, n = _run(case, bands, rhs, stagingBuffers=nb, mixedPrecisionRefinement=refine)
+    assert n == 1, "the launch did not run on the streaming kernel"
+    e, emax = J.rel_err(x, O.jw_step(case, bands, rhs, "q", nthreads=8), case)
+    assert e <= (1e-12 if refine else TOL), (e, emax)
