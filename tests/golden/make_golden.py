@@ -279,8 +279,10 @@ def long_cases():
             case = O.Case(M=M, batch=2, upperBanded=ub, jw_type=jwt)
             rhs = rng.uniform(-1, 1, case.rhs_len())
             out.append((f"long_ub{ub}_t{jwt}_M{M}", case, bands, rhs, "f64"))
-    # beyond one cluster of 8 x 2048 rows: up to 64 slices of 1024 rows
-    for M in (20000, 32768, 65536):
+    # beyond one cluster of 8 x 2048 rows: up to 64 slices of 1024 rows; and
+    # lengths that are not a multiple of 16 rows (an even one, whose rows are
+    # 16-byte aligned at the packed stride, and an odd one)
+    for M in (20000, 32768, 65536, 20002, 12345):
         rng = np.random.default_rng(17500 + M)
         bands = WL.permute_bands(jw_bands(rng, M, 2), M)
         case = O.Case(M=M, batch=2, upperBanded=2, jw_type=13)

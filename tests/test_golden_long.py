@@ -69,8 +69,10 @@ def test_oracle_against_reference(path):
 def test_kernel_against_reference(path, kernel_path):
     import jwcases as J
     case, buf, rhs, ref = load(path)
-    if kernel_path == 2 and case.M > 16384:
-        pytest.skip("the cluster kernel holds one system on 8 CTAs of 2048 rows at most")
+    if kernel_path == 2 and (case.M > 16384 or case.M % 8):
+        pytest.skip("the cluster kernel holds one system of at most 8 x 2048 rows, a multiple of 8")
+    if kernel_path == 3 and case.M % 2:
+        pytest.skip("odd M at the packed stride: rows no tensor map can describe, which two passes alone refuse")
     name = os.path.basename(path)[:-4]
     got = J.run_app(case, buf, rhs, kernelPath=kernel_path)
     if name in LONG_REFERENCE_DEFECTS:
