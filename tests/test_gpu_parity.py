@@ -280,8 +280,8 @@ def test_config3_full_size_sampled():
 # ---------------------------------------------------------------------------
 # Mixed precision: FP32 factor-solve + FP64 residual refinement (FP64 storage).
 # Bound: 1e-12 relative L2 against the __float128 oracle after 2 refinement
-# sweeps on the weakly dominant config-3 system; one sweep
-# is allowed 1e-10.
+# sweeps on the weakly dominant config-3 system (the accuracy the mixed mode
+# is meant to reach); one sweep is allowed 1e-10.
 
 @pytest.mark.parametrize("refine,tol", [(1, 1e-10), (2, 1e-12), (3, 1e-12)])
 def test_mixed_precision_config3(refine, tol):
